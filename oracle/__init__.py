@@ -1,0 +1,211 @@
+"""Oracle for the CUDA path: ctypes front-ends of two CPU libraries.
+
+TEST INFRASTRUCTURE ONLY.  Only ``tests/``, ``__graft_entry__.smoke()`` and
+``bench.py``'s CPU-baseline leg (and its ``--impl reference`` arm) import this
+package; the product library never does.
+
+* :class:`Oracle` drives ``libsvof_oracle.so``, this repository's C
+  restatement of the reference algorithm (``oracle/svof_oracle.c``).
+* :func:`run_reference` drives ``_ref/libsvof_ref[_c0].so``, the reference's
+  own ``src/*.c`` compiled against single-rank shims, in a fresh process (the
+  reference keeps solver state in process-wide statics).
+
+Storage layouts are the reference's (``include/array_macros/**``): x fastest,
+x ghost cells and y halo rows included.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_LIB = os.path.join(HERE, "libsvof_oracle.so")
+REF_LIBS = {"ref": os.path.join(HERE, "_ref", "libsvof_ref.so"),
+            "c0": os.path.join(HERE, "_ref", "libsvof_ref_c0.so")}
+
+# halo rows per field (y) and storage shape (rows, cols[, comps]) for nx, ny
+NHALO = {"ux": 1, "uy": 1, "p": 1, "psi": 1, "t": 1, "vof": 2, "curv": 1}
+
+
+def storage_shape(name: str, nx: int, ny: int):
+    if name == "ux":
+        return (ny + 2, nx + 1)
+    if name in ("uy", "p", "psi", "t", "curv"):
+        return (ny + 2, nx + 2)
+    if name == "vof":
+        return (ny + 4, nx + 2)
+    if name == "dvof":
+        return (ny + 3, nx + 1, 2)
+    if name == "normal":
+        return (ny + 2, nx, 3)
+    if name == "flxx":
+        return (ny, nx + 1)
+    if name == "flxy":
+        return (ny + 1, nx)
+    if name in ("ifrcx",) or name.startswith("srcux"):
+        return (ny, nx - 1)
+    if name in ("ifrcy", "src0", "src1") or name.startswith("srcuy") or name.startswith("srct"):
+        return (ny, nx)
+    raise KeyError(name)
+
+
+def interior_rows(name: str, arr: np.ndarray, ny: int) -> np.ndarray:
+    """rows j = 1..ny of a halo'd field (the part the NPY restart files hold)"""
+    h = NHALO[name]
+    return arr[h:h + ny]
+
+
+class _Params(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int),
+                ("lx", ctypes.c_double), ("ly", ctypes.c_double),
+                ("m_dif", ctypes.c_double), ("t_dif", ctypes.c_double),
+                ("tension", ctypes.c_double),
+                ("coef_dt_adv", ctypes.c_double), ("coef_dt_dif", ctypes.c_double),
+                ("add_buoyancy", ctypes.c_int),
+                ("uy_xm", ctypes.c_double), ("uy_xp", ctypes.c_double),
+                ("t_xm", ctypes.c_double), ("t_xp", ctypes.c_double)]
+
+
+_lib = None
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(ORACLE_LIB):
+            raise RuntimeError(f"{ORACLE_LIB} missing: run 'make -C oracle oracle'")
+        L = ctypes.CDLL(ORACLE_LIB)
+        L.svo_create.restype = ctypes.c_void_p
+        L.svo_create.argtypes = [ctypes.POINTER(_Params), ctypes.c_void_p, ctypes.c_void_p]
+        L.svo_destroy.argtypes = [ctypes.c_void_p]
+        L.svo_field.restype = ctypes.POINTER(ctypes.c_double)
+        L.svo_field.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_long)]
+        for fn in ("svo_init_boundaries", "svo_curvature_tensor", "svo_force", "svo_x_grid_is_uniform"):
+            getattr(L, fn).argtypes = [ctypes.c_void_p]
+        L.svo_decide_dt.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+        for fn in ("svo_update_vof", "svo_predict", "svo_potential_dct", "svo_potential_dft",
+                   "svo_correct", "svo_update_pressure"):
+            getattr(L, fn).argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double]
+        L.svo_integrate.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+        L.svo_run.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        _lib = L
+    return _lib
+
+
+FIELD_NAMES = ["ux", "uy", "p", "psi", "t", "srcux0", "srcux1", "srcux2", "srcuy0", "srcuy1",
+               "srcuy2", "srct0", "srct1", "srct2", "vof", "ifrcx", "ifrcy", "dvof", "normal",
+               "curv", "flxx", "flxy", "src0", "src1"]
+
+
+class Oracle:
+    """The C restatement, 2D FP64.  ``params`` holds m_dif, t_dif, tension,
+    coef_dt_adv, coef_dt_dif (see simplevofsolver_b200.workloads.physical_params)."""
+
+    def __init__(self, ic, params: dict, add_buoyancy: bool = False,
+                 uy_walls=(0.0, 0.0), t_walls=(0.0, 0.0)):
+        L = _load()
+        self.nx, self.ny = int(ic.nx), int(ic.ny)
+        pr = _Params(self.nx, self.ny, float(ic.lx), float(ic.ly), params["m_dif"], params["t_dif"],
+                     params["tension"], params["coef_dt_adv"], params["coef_dt_dif"],
+                     int(bool(add_buoyancy)), float(uy_walls[0]), float(uy_walls[1]),
+                     float(t_walls[0]), float(t_walls[1]))
+        xf = np.ascontiguousarray(ic.xf, dtype=np.float64)
+        xc = np.ascontiguousarray(ic.xc, dtype=np.float64)
+        self._h = L.svo_create(ctypes.byref(pr), xf.ctypes.data, xc.ctypes.data)
+        if not self._h:
+            raise ValueError("svo_create failed")
+        for k, v in ic.fields().items():
+            interior_rows(k, self.field(k), self.ny)[...] = v
+        L.svo_init_boundaries(self._h)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            _load().svo_destroy(self._h)
+            self._h = None
+
+    def field(self, name: str) -> np.ndarray:
+        """live view of a field's storage"""
+        n = ctypes.c_long(0)
+        ptr = _load().svo_field(self._h, name.encode(), ctypes.byref(n))
+        if not ptr:
+            raise KeyError(name)
+        return np.ctypeslib.as_array(ptr, shape=(n.value,)).reshape(storage_shape(name, self.nx, self.ny))
+
+    def snapshot(self, names=("ux", "uy", "p", "psi", "t", "vof")):
+        return {k: self.field(k).copy() for k in names}
+
+    @property
+    def uniform(self):
+        return bool(_load().svo_x_grid_is_uniform(self._h))
+
+    def decide_dt(self):
+        dt = ctypes.c_double(0.0)
+        _load().svo_decide_dt(self._h, ctypes.byref(dt))
+        return dt.value
+
+    def curvature_tensor(self):
+        _load().svo_curvature_tensor(self._h)
+
+    def force(self):
+        _load().svo_force(self._h)
+
+    def update_vof(self, rk, dt):
+        _load().svo_update_vof(self._h, rk, dt)
+
+    def predict(self, rk, dt):
+        _load().svo_predict(self._h, rk, dt)
+
+    def potential(self, rk, dt):
+        if self.uniform:
+            _load().svo_potential_dct(self._h, rk, dt)
+        else:
+            _load().svo_potential_dft(self._h, rk, dt)
+
+    def correct(self, rk, dt):
+        _load().svo_correct(self._h, rk, dt)
+
+    def update_pressure(self, rk, dt):
+        _load().svo_update_pressure(self._h, rk, dt)
+
+    def run(self, nsteps: int) -> np.ndarray:
+        dts = np.zeros(max(nsteps, 1))
+        if _load().svo_run(self._h, int(nsteps), dts.ctypes.data) != 0:
+            raise RuntimeError("svo_run failed")
+        return dts[:nsteps]
+
+
+# ---------------------------------------------------------------- reference
+
+def reference_available(variant: str = "c0") -> bool:
+    return os.path.exists(REF_LIBS[variant])
+
+
+def run_reference(ic, env: dict, nsteps: int, variant: str = "c0",
+                  names=("ux", "uy", "p", "psi", "t", "vof"), timeout: float = 1800.0):
+    """Run the compiled reference for ``nsteps`` steps from ``ic`` (written to a
+    temporary NPY directory and read back by the reference's own fluid_init /
+    interface_init) in a fresh Python process (``oracle/_ref_runner.py``).
+    Returns {name: storage array (reshaped), 'dts': ..., 'seconds': ...}."""
+    import subprocess
+    import sys
+    from simplevofsolver_b200.workloads import write_npy_dir
+    if not reference_available(variant):
+        raise RuntimeError(f"{REF_LIBS[variant]} missing: run 'make -C oracle ref'")
+    with tempfile.TemporaryDirectory() as d:
+        icdir = os.path.join(d, "ic")
+        write_npy_dir(ic, icdir)
+        out_npz = os.path.join(d, "out.npz")
+        envs = dict(os.environ)
+        envs.update({k: repr(float(v)) for k, v in env.items()})
+        cmd = [sys.executable, os.path.join(HERE, "_ref_runner.py"), REF_LIBS[variant], icdir,
+               str(int(nsteps)), out_npz, ",".join(names)]
+        subprocess.run(cmd, check=True, env=envs, timeout=timeout,
+                       stdout=subprocess.DEVNULL)
+        res = dict(np.load(out_npz))
+    out = {"dts": res["dts"], "seconds": float(res["seconds"])}
+    for k in names:
+        out[k] = res[k].reshape(storage_shape(k, ic.nx, ic.ny))
+    return out

@@ -1,0 +1,69 @@
+/*
+ * svof_oracle.h -- CPU restatement of SimpleVOFSolver's per-step hot path
+ * (2D, FP64).  TEST INFRASTRUCTURE ONLY: this is the checker for the CUDA
+ * library; only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
+ * leg may load it.
+ *
+ * Every array is stored exactly as the reference stores it (the index maps of
+ * include/array_macros/** in the reference): x fastest, one row per y index,
+ * x ghost cells and y halo rows included.  With nx, ny the interior sizes:
+ *
+ *   ux    (nx+1) x (ny+2)   i in [1, nx+1], j in [0, ny+1]
+ *   uy, p, psi, t, curv
+ *         (nx+2) x (ny+2)   i in [0, nx+1], j in [0, ny+1]
+ *   vof   (nx+2) x (ny+4)   i in [0, nx+1], j in [-1, ny+2]
+ *   dvof  2 x (nx+1) x (ny+3)   corners, i in [1, nx+1], j in [0, ny+2]
+ *   normal 3 x nx x (ny+2)      i in [1, nx], j in [0, ny+1]
+ *   flxx  (nx+1) x ny,  flxy nx x (ny+1)
+ *   ifrcx, srcux[3]  (nx-1) x ny  (i in [2, nx]);  ifrcy, srcuy[3], srct[3],
+ *   src[2]  nx x ny
+ */
+#ifndef SVOF_ORACLE_H
+#define SVOF_ORACLE_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+  int nx, ny;
+  double lx, ly;
+  double m_dif, t_dif;       /* sqrt(Pr)/sqrt(Ra), 1/(sqrt(Pr) sqrt(Ra)) */
+  double tension;            /* 1 / We */
+  double coef_dt_adv, coef_dt_dif;
+  int add_buoyancy;          /* reference param_add_buoyancy */
+  double uy_xm, uy_xp;       /* wall velocities (param_uy_x[mp]) */
+  double t_xm, t_xp;         /* wall temperatures (param_t_x[mp]) */
+} svo_params_t;
+
+typedef struct svo_ctx svo_ctx_t;
+
+svo_ctx_t *svo_create(const svo_params_t *params, const double *xf, const double *xc);
+void svo_destroy(svo_ctx_t *ctx);
+/* pointer to the storage of a field (names as the reference's members:
+ * ux uy p psi t srcux0..2 srcuy0..2 srct0..2 vof ifrcx ifrcy dvof normal curv
+ * flxx flxy src0 src1); *count receives the number of doubles */
+double *svo_field(svo_ctx_t *ctx, const char *name, long *count);
+/* boundary/halo update of ux uy p t vof, as fluid_init/interface_init do */
+int svo_init_boundaries(svo_ctx_t *ctx);
+int svo_x_grid_is_uniform(svo_ctx_t *ctx);
+
+int svo_decide_dt(svo_ctx_t *ctx, double *dt);
+int svo_curvature_tensor(svo_ctx_t *ctx);
+int svo_force(svo_ctx_t *ctx);
+int svo_update_vof(svo_ctx_t *ctx, int rkstep, double dt);
+int svo_predict(svo_ctx_t *ctx, int rkstep, double dt);
+int svo_potential_dct(svo_ctx_t *ctx, int rkstep, double dt);
+int svo_potential_dft(svo_ctx_t *ctx, int rkstep, double dt);
+int svo_correct(svo_ctx_t *ctx, int rkstep, double dt);
+int svo_update_pressure(svo_ctx_t *ctx, int rkstep, double dt);
+int svo_integrate(svo_ctx_t *ctx, double *dt);
+int svo_run(svo_ctx_t *ctx, int nsteps, double *dts);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
