@@ -1,0 +1,329 @@
+#!/usr/bin/env python3
+"""Throughput of SimpleVOFSolver's per-step hot path on B200.
+
+A step is one call of integrate() (src/integrate.c:11-68): the CFL time step
+and three Runge-Kutta substeps of interface geometry, CSF force, THINC/QQ
+advection, momentum prediction with implicit-x Thomas solves, the Poisson
+solve and the projection.  Metric: Mcell-steps/s = cells x steps / seconds.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME]
+                  [--impl ours|reference]
+
+Our arm (default) prints one JSON line with the device-timed throughput
+(inputs resident in HBM, L2 flushed between timed steps), the end-to-end
+throughput through the C ABI with host buffers (restart fields copied in and
+out every step), the roofline of the dominant kernel, the reference's CPU
+throughput on a bounded sample, and the SM clocks seen during the timed
+region.  The path does not shard (one domain per GPU): with N GPUs every rank
+runs an independent replica ("weak" scaling, no collective on the data path).
+
+--impl reference times the reference's own C implementation (its src/*.c
+compiled against single-rank shims, oracle/_ref) on all host cores: one
+single-rank process per core, each a replica of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "Mcell-steps/s"
+# 2D FP64 algorithmic HBM bytes per cell-step (103 eight-byte words: the
+# compulsory reads/writes of the reference dataflow with stencil-internal
+# intermediates on chip)
+ALG_BYTES_CELL_STEP_2D = 824.0
+# algorithmic 8-byte words per interior cell for one launch of each kernel
+# kind, averaged over the three substeps (src_b is not read at substep 0)
+ALG_WORDS = {
+    "dt": 2.0,                 # R ux, uy
+    "geom": 2.0,               # R vof, W curv (normals of interfacial cells only)
+    "force": 4.0,              # R vof, curv; W ifrcx, ifrcy
+    "vof": 5.0 + 2.0 / 3.0,    # R vof, ux, uy, (src_b); W vof, src_a
+    "predict": 12.0 + 2.0,     # R ux uy p t ifrcx ifrcy (3 src_b); W ux uy t, 3 src_a
+    "poisson_fwd": 3.0,        # R ux, uy; W spectrum
+    "poisson_solve": 2.0,      # R, W spectrum
+    "poisson_inv": 2.0,        # R spectrum; W psi
+    "project": 7.0,            # R psi ux uy p; W ux uy p
+}
+KERNELS_PER_STEP = 2 + 3 * 8
+
+WORKLOADS = {
+    # the reference's runnable configuration: one elliptical droplet,
+    # 128 x 128, uniform x (DCT Poisson path), Re = 100, We = 10
+    "droplet2d_128": dict(nx=128, ny=128, uniform=True),
+    "droplet2d_1024": dict(nx=1024, ny=1024, uniform=True),
+    "droplet2d_2048": dict(nx=2048, ny=2048, uniform=True),
+    "droplet2d_stretched_512": dict(nx=512, ny=512, uniform=False),
+}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region"""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.idx = device_index
+        self.proc = None
+        self.f = None
+
+    def __enter__(self):
+        try:
+            self.f = tempfile.TemporaryFile(mode="w+")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or self.f is None:
+            return None
+        self.f.seek(0)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_reference(ic, env, steps, warmup, replicas):
+    import oracle
+    secs = oracle.run_reference_replicas(ic, env, steps, warmup, replicas)
+    return secs
+
+
+def run_reference_arm(args, wl, ic, env, rank):
+    """the reference's own C path on the host cores (rank 0 only)"""
+    if rank != 0:
+        return
+    ncpu = os.cpu_count() or 1
+    replicas = max(1, min(ncpu, 64))
+    cells = wl["nx"] * wl["ny"]
+    try:
+        secs = cpu_reference(ic, env, args.steps, args.warmup, replicas)
+    except Exception as e:  # the build of the reference is missing
+        print(json.dumps({"impl": "reference", "unavailable": f"reference CPU build failed to run: {e}"}))
+        return
+    t = max(secs)
+    value = replicas * cells * args.steps / t / 1e6
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded droplet field)",
+        "config": {"workload": args.workload, "nx": wl["nx"], "ny": wl["ny"],
+                   "uniform_x": wl["uniform"], "replicas": replicas},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": replicas, "kind": "reference",
+                         "sample": f"{replicas} single-rank processes x {args.steps} steps of {args.workload}"},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--workload", default="droplet2d_128", choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-sample-steps", type=int, default=1000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    from simplevofsolver_b200.workloads import DROPLET2D_ENV, droplet2d, physical_params
+    wl = WORKLOADS[args.workload]
+    ic = droplet2d(wl["nx"], wl["ny"], uniform=wl["uniform"])
+    env = DROPLET2D_ENV
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference_arm(args, wl, ic, env, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    import simplevofsolver_b200 as svof
+    phys = physical_params(env)
+    solver = svof.Solver(ic, phys)
+    cells = wl["nx"] * wl["ny"]
+    stream = torch.cuda.ExternalStream(solver.stream())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # > 126 MB L2
+
+    # warm-up (also captures the step graphs)
+    solver.run(args.warmup)
+    torch.cuda.synchronize()
+
+    # ---- device-timed region: inputs resident in HBM, L2 flushed between steps
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        with torch.cuda.stream(stream):
+            for k in range(args.steps):
+                flush.zero_()
+                starts[k].record(stream)
+                solver.enqueue_steps(1)
+                ends[k].record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = float(sum(step_ms))
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * cells * args.steps / (total_ms * 1e-3) / 1e6
+    clocks = clk.summary()
+
+    # ---- end to end through the C ABI with host buffers: the restart fields
+    # are copied in from pinned host memory and out again every step
+    names = ["ux", "uy", "p", "t", "vof"]
+    host_in = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory().numpy()
+               for k, v in ic.fields().items()}
+    host_out = {k: torch.empty(v.shape, dtype=torch.float64).pin_memory().numpy() for k, v in host_in.items()}
+    h2d = sum(v.nbytes for v in host_in.values())
+    d2h = sum(v.nbytes for v in host_out.values()) + 8
+    e2e_steps = max(1, min(args.steps, 50))
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for k in range(e2e_steps):
+        for n in names:
+            solver.load_interior(n, host_in[n])
+        solver.integrate()
+        for n in names:
+            out = host_out[n]
+            svof._check(svof.lib().svof_store_interior(solver._h, svof.FIELDS[n], out.ctypes.data, out.size))
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * cells * e2e_steps / e2e_s / 1e6
+
+    # ---- per-kernel device times (kernel by kernel, events between launches;
+    # a long memset ahead lets the host enqueue the whole step first)
+    prof = {}
+    nprof = 5
+    for _ in range(nprof):
+        with torch.cuda.stream(stream):
+            big = torch.empty(1024 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+            big.zero_()
+        r = solver.profile_step()
+        del big
+        for k, (ms, n) in r.items():
+            a = prof.setdefault(k, [0.0, 0])
+            a[0] += ms
+            a[1] += n
+    dom = max(prof, key=lambda k: prof[k][0])
+    dom_ms = prof[dom][0] / max(prof[dom][1], 1)
+    peak, peak_kind = peaks()
+    alg_bytes = ALG_WORDS[dom] * 8.0 * cells
+    achieved = alg_bytes / (dom_ms * 1e-3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            tj = json.load(f)
+        traffic = tj.get(args.workload, {}).get(dom)
+    total_prof = sum(v[0] for v in prof.values())
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            secs = cpu_reference(ic, env, args.cpu_sample_steps, 2, 1)
+            cpu = {"value": cells * args.cpu_sample_steps / secs[0] / 1e6, "unit": METRIC, "cores": 1,
+                   "kind": "reference",
+                   "sample": f"{args.cpu_sample_steps} steps of {args.workload}, one single-rank process"}
+        except Exception as e:
+            cpu = {"value": None, "unit": METRIC, "cores": 0, "kind": "reference",
+                   "sample": f"unavailable: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded droplet field, workloads.droplet2d)",
+            "config": {"workload": args.workload, "nx": wl["nx"], "ny": wl["ny"], "uniform_x": wl["uniform"],
+                       "poisson": "dct-x + periodic thomas-y" if wl["uniform"] else "r2c-y + thomas-x",
+                       "l2": "flushed between timed steps (256 MB write)", "parallelism": f"replicas{world}"},
+            "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "steps": e2e_steps},
+            "gpu_launches": KERNELS_PER_STEP * args.steps,
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
+                         "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": dom_ms,
+                         "step_frac": value * 1e6 * ALG_BYTES_CELL_STEP_2D / 1e9 / peak},
+            "kernel_ms_per_step": {k: v[0] / nprof for k, v in prof.items()},
+            "kernel_share": {k: v[0] / total_prof for k, v in prof.items()},
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+        print(json.dumps(line))
+    solver.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

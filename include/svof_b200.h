@@ -1,0 +1,181 @@
+/*
+ * svof_b200.h -- C ABI of the B200 (sm_100a) implementation of
+ * SimpleVOFSolver's per-step hot path.
+ *
+ * Plain pointers and sizes only.  All entry points return 0 on success and a
+ * non-zero code on failure (the reference's convention, src/main.c:66-99);
+ * svof_last_error() describes the last failure of the calling thread.
+ *
+ * Data layout: every field is stored on the device exactly as the reference
+ * stores it in memory (reference include/array_macros/**): float64, x
+ * fastest, x ghost cells and y halo rows included.  For nx x ny interior
+ * cells:
+ *   SVOF_UX                    (ny+2) rows x (nx+1)
+ *   SVOF_UY, SVOF_P, SVOF_PSI, SVOF_T, SVOF_CURV
+ *                              (ny+2) rows x (nx+2)
+ *   SVOF_VOF                   (ny+4) rows x (nx+2)
+ *   SVOF_NORMAL                (ny+2) rows x nx x 3   (nx, ny, intercept)
+ *   SVOF_IFRCX, SVOF_SRCUX_A/B ny rows x (nx-1)
+ *   SVOF_IFRCY, SVOF_SRCUY_A/B, SVOF_SRCT_A/B, SVOF_SRC_A/B
+ *                              ny rows x nx
+ * The restart (NPY) files of the reference hold rows 1..ny of ux, uy, p, t,
+ * vof (src/array.c:80-206); svof_load_interior() accepts exactly that part.
+ *
+ * Threading: one solver is used by one host thread at a time; all device
+ * work is issued on the solver's own CUDA stream.
+ */
+#ifndef SVOF_B200_H
+#define SVOF_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct svof_solver svof_solver_t;
+
+/* run-time form of the reference's compile-time and env parameters:
+ * include/param.h:10-34 (buoyancy, wall values), src/fluid/init.c:90-93
+ * (m_dif = sqrt(Pr)/sqrt(Ra), t_dif = 1/(sqrt(Pr) sqrt(Ra))),
+ * src/interface/init.c:66-68 (tension = 1/We),
+ * src/fluid/decide_dt.c:109-112 (coef_dt_adv, coef_dt_dif).
+ * Diffusion is implicit in x and explicit in y (src/param/implicit.c:3-7). */
+typedef struct {
+  int nx, ny;             /* interior cells; the FFT direction must be a power of two */
+  double lx, ly;          /* domain lengths */
+  double m_dif, t_dif;    /* momentum / temperature diffusivities */
+  double tension;         /* surface tension coefficient, 1/We */
+  double coef_dt_adv;     /* CFL safety factors */
+  double coef_dt_dif;
+  int add_buoyancy;       /* add +T to the ux source (Boussinesq) */
+  double uy_xm, uy_xp;    /* wall velocity in y at x = 0, x = lx */
+  double t_xm, t_xp;      /* wall temperature at x = 0, x = lx */
+} svof_params_t;
+
+enum {
+  SVOF_UX = 0,
+  SVOF_UY = 1,
+  SVOF_P = 2,
+  SVOF_PSI = 3,
+  SVOF_T = 4,
+  SVOF_VOF = 5,
+  SVOF_CURV = 6,
+  SVOF_NORMAL = 7,
+  SVOF_IFRCX = 8,
+  SVOF_IFRCY = 9,
+  SVOF_SRCUX_A = 10, /* current RK source (explicit part), srcux[rk_a] */
+  SVOF_SRCUX_B = 11, /* previous RK source, srcux[rk_b] */
+  SVOF_SRCUY_A = 12,
+  SVOF_SRCUY_B = 13,
+  SVOF_SRCT_A = 14,
+  SVOF_SRCT_B = 15,
+  SVOF_SRC_A = 16,   /* vof sources, interface src[rk_a], src[rk_b] */
+  SVOF_SRC_B = 17,
+  SVOF_NFIELDS = 18
+};
+
+/* Creates a solver for the grid xf[nx+1], xc[nx+2] (reference domain_t,
+ * include/domain.h:19-28; dxf, dxc and dy are derived as src/domain.c:170-209
+ * does).  Allocates all device memory.  Replaces the allocation and set-up
+ * parts of fluid_init (include/fluid_solver.h:10-14), interface_init
+ * (include/interface_solver.h:8-12) and linear_system_init
+ * (include/linear_system.h:37-42). */
+int svof_create(const svof_params_t *params, const double *xf, const double *xc,
+                svof_solver_t **solver);
+/* replaces linear_system_finalise (include/linear_system.h:44-46) and frees
+ * everything svof_create allocated */
+int svof_destroy(svof_solver_t *solver);
+
+/* number of doubles in a field's device storage (layout above) */
+int svof_field_count(const svof_solver_t *solver, int field, size_t *count);
+/* whole-storage copies between host memory and the device field */
+int svof_upload_field(svof_solver_t *solver, int field, const double *host, size_t count);
+int svof_download_field(svof_solver_t *solver, int field, double *host, size_t count);
+/* device address of a field's current storage (valid until the next call
+ * that advances the solution) */
+int svof_device_field(svof_solver_t *solver, int field, double **device_ptr);
+/* Loads rows 1..ny (the restart-file part, shape (ny, nx+nadds)) of ux, uy,
+ * p, t or vof from host memory and imposes that field's boundary and halo
+ * values, as array.load + fluid_update_boundaries_* / interface_update_
+ * boundaries_vof do in fluid_init (src/fluid/init.c:82-88) and
+ * interface_init (src/interface/init.c:60-63). */
+int svof_load_interior(svof_solver_t *solver, int field, const double *host, size_t count);
+/* copies rows 1..ny of ux, uy, p, t or vof to host memory (the part
+ * fluid_save / interface_save write, src/fluid/save.c:18-25) */
+int svof_store_interior(svof_solver_t *solver, int field, double *host, size_t count);
+
+/* 1 if |max dxf - min dxf| < 1e-15 (src/domain.c:75-98): the Poisson solve
+ * uses the DCT path, otherwise the DFT path (src/integrate.c:49-57) */
+int svof_x_grid_is_uniform(const svof_solver_t *solver, int *is_uniform);
+
+/* ---- the reference's solver entry points (include/fluid_solver.h,
+ *      include/interface_solver.h), one kernel sequence each ---- */
+/* fluid_decide_dt (include/fluid_solver.h:24-28); *dt is read back */
+int svof_fluid_decide_dt(svof_solver_t *solver, double *dt);
+/* interface_compute_curvature_tensor (include/interface_solver.h:20-23) */
+int svof_interface_compute_curvature_tensor(svof_solver_t *solver);
+/* interface_compute_force (include/interface_solver.h:25-28) */
+int svof_interface_compute_force(svof_solver_t *solver);
+/* interface_update_vof (include/interface_solver.h:30-36) */
+int svof_interface_update_vof(svof_solver_t *solver, size_t rkstep, double dt);
+/* fluid_predict_field (include/fluid_solver.h:31-37) */
+int svof_fluid_predict_field(svof_solver_t *solver, size_t rkstep, double dt);
+/* fluid_compute_potential_dct / _dft (include/fluid_solver.h:41-55) */
+int svof_fluid_compute_potential_dct(svof_solver_t *solver, size_t rkstep, double dt);
+int svof_fluid_compute_potential_dft(svof_solver_t *solver, size_t rkstep, double dt);
+/* fluid_correct_velocity (include/fluid_solver.h:58-63) */
+int svof_fluid_correct_velocity(svof_solver_t *solver, size_t rkstep, double dt);
+/* fluid_update_pressure (include/fluid_solver.h:66-71) */
+int svof_fluid_update_pressure(svof_solver_t *solver, size_t rkstep, double dt);
+
+/* integrate (reference include/integrate.h:5-10): one full time step
+ * (dt + 3 Runge-Kutta substeps) as one CUDA-graph launch; *dt is read back */
+int svof_integrate(svof_solver_t *solver, double *dt);
+/* nsteps calls of svof_integrate without host synchronisation between
+ * steps; dts (optional, nsteps entries) receives every dt */
+int svof_run(svof_solver_t *solver, int nsteps, double *dts);
+
+/* enqueues nsteps time steps (graph launches plus the 8-byte dt read-back)
+ * on the solver's stream and returns without waiting; svof_last_dt waits and
+ * returns the last dt.  Same semantics as svof_run, for callers that overlap
+ * host work or time the device with events. */
+int svof_enqueue_steps(svof_solver_t *solver, int nsteps);
+int svof_last_dt(svof_solver_t *solver, double *dt);
+
+/* diagnostics of src/logging/divergence.c:36-50 and src/logging/interface.c:
+ * 22-39 computed on the device: max |div u|, and vof min, max and
+ * sum(vof dx dy) / sum(dx dy) */
+int svof_diagnostics(svof_solver_t *solver, double *divmax, double *vofmin, double *vofmax,
+                     double *vofmean);
+
+/* kernel kinds of svof_profile_step */
+enum {
+  SVOF_K_DT = 0,            /* CFL reduction + dt (2 launches) */
+  SVOF_K_GEOM = 1,          /* normals, intercept, curvature */
+  SVOF_K_FORCE = 2,         /* CSF force */
+  SVOF_K_VOF = 3,           /* THINC fluxes + vof update */
+  SVOF_K_PREDICT = 4,       /* momentum / scalar RHS + x Thomas + update */
+  SVOF_K_POISSON_FWD = 5,   /* divergence + forward transform */
+  SVOF_K_POISSON_SOLVE = 6, /* spectral line solves */
+  SVOF_K_POISSON_INV = 7,   /* inverse transform + psi boundaries */
+  SVOF_K_PROJECT = 8,       /* velocity correction + pressure update */
+  SVOF_NKINDS = 9
+};
+/* One time step launched kernel by kernel (no graph), timed with CUDA events
+ * on the solver's stream: ms[k] / launches[k] accumulate per kind k.  The
+ * solution advances exactly as with svof_integrate.  No reference
+ * counterpart (measurement aid). */
+int svof_profile_step(svof_solver_t *solver, double *ms, int *launches, int nkinds);
+
+/* wait for all work of the solver's stream */
+int svof_synchronize(svof_solver_t *solver);
+/* CUDA stream the solver issues its work on (cudaStream_t) */
+int svof_stream(svof_solver_t *solver, void **stream);
+const char *svof_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

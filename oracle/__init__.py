@@ -209,3 +209,35 @@ def run_reference(ic, env: dict, nsteps: int, variant: str = "c0",
     for k in names:
         out[k] = res[k].reshape(storage_shape(k, ic.nx, ic.ny))
     return out
+
+
+def run_reference_replicas(ic, env: dict, nsteps: int, warmup: int, replicas: int, variant: str = "c0",
+                           timeout: float = 1800.0):
+    """``replicas`` independent processes of the compiled reference, each
+    integrating ``warmup`` untimed then ``nsteps`` timed steps from ``ic``, all
+    started together (one process per host core).  Returns the per-replica
+    seconds of the timed steps."""
+    import subprocess
+    import sys
+    from simplevofsolver_b200.workloads import write_npy_dir
+    if not reference_available(variant):
+        raise RuntimeError(f"{REF_LIBS[variant]} missing: run 'make -C oracle ref'")
+    with tempfile.TemporaryDirectory() as d:
+        icdir = os.path.join(d, "ic")
+        write_npy_dir(ic, icdir)
+        envs = dict(os.environ)
+        envs.update({k: repr(float(v)) for k, v in env.items()})
+        envs["OMP_NUM_THREADS"] = "1"
+        procs = []
+        for r in range(replicas):
+            out_npz = os.path.join(d, f"out{r}.npz")
+            cmd = [sys.executable, os.path.join(HERE, "_ref_runner.py"), REF_LIBS[variant], icdir,
+                   str(int(nsteps)), out_npz, "", str(int(warmup))]
+            procs.append((subprocess.Popen(cmd, env=envs, stdout=subprocess.DEVNULL), out_npz))
+        secs = []
+        for pr, out_npz in procs:
+            pr.wait(timeout=timeout)
+            if pr.returncode != 0:
+                raise RuntimeError("reference replica failed")
+            secs.append(float(np.load(out_npz)["seconds"]))
+    return secs

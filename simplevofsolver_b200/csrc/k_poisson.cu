@@ -1,0 +1,339 @@
+// k_poisson.cu -- pressure Poisson solve of the FP64 2D path.
+//
+// Uniform x grid (src/fluid/compute_potential/dct.c:373-421):
+//   k_dct_fwd     divergence right-hand side of one row, FFTW_REDFT10 along x
+//   k_dct_ysolve  periodic tri-diagonal system along y for every x wavenumber
+//                 (Sherman-Morrison, src/tdm.c:78-99), one wavenumber per thread
+//   k_dct_inv     FFTW_REDFT01 along x, psi row with halo and Neumann walls
+// Stretched x grid (src/fluid/compute_potential/dft.c:406-468):
+//   k_dft_fwd     right-hand side of a tile of columns, r2c along y
+//   k_dft_xsolve  complex Neumann tri-diagonal system along x for every y
+//                 wavenumber (src/tdm.c:17-50, component-wise)
+//   k_dft_inv     c2r along y, psi columns with halo and walls
+//
+// The reference transposes between x- and y-pencils around every transform;
+// on one device the spectral array is instead laid out so that each line
+// solve reads it coalesced: DCT path [j][kx] (threads over kx walk j), DFT
+// path [i][ky] (threads over ky walk i).  No transpose pass exists.
+//
+// The transforms are the radix-2 decimation-in-time FFT of the oracle
+// (oracle/svof_fft.c) with the same butterflies and the same twiddle tables,
+// so with FMA contraction disabled they agree with it bit for bit.  Lengths
+// must be powers of two.
+#include "svof_internal.cuh"
+
+namespace svof {
+
+__device__ __forceinline__ int bitrev(int q, int log2n) { return (int)(__brev((unsigned)q) >> (32 - log2n)); }
+
+// butterfly stages on interleaved complex data already in bit-reversed order;
+// `lines` independent transforms of length n = 2^log2n stored back to back
+__device__ __forceinline__ void fft_stages(double *z, int log2n, int lines, const double *__restrict__ tw) {
+  const int n = 1 << log2n;
+  const int nb = lines * (n >> 1);
+  for (int s = 1; s <= log2n; s++) {
+    const int half = 1 << (s - 1);
+    const int len = half << 1;
+    const int step = n >> s;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+      const int line = b / (n >> 1);
+      const int bb = b - line * (n >> 1);
+      const int grp = bb >> (s - 1);
+      const int k = bb & (half - 1);
+      double *zz = z + 2 * line * n;
+      const int ia = grp * len + k, ib = ia + half;
+      const double wr = tw[2 * (k * step) + 0];
+      const double wi = tw[2 * (k * step) + 1];
+      const double xr = zz[2 * ib], xi = zz[2 * ib + 1];
+      const double tr = wr * xr - wi * xi;
+      const double ti = wr * xi + wi * xr;
+      const double ur = zz[2 * ia], ui = zz[2 * ia + 1];
+      zz[2 * ia] = ur + tr;
+      zz[2 * ia + 1] = ui + ti;
+      zz[2 * ib] = ur - tr;
+      zz[2 * ib + 1] = ui - ti;
+    }
+    __syncthreads();
+  }
+}
+
+// assign_input, dct.c:285-315 / dft.c:315-345
+__device__ __forceinline__ double poisson_rhs(const double *__restrict__ ux, const double *__restrict__ uy,
+                                              const Grid2 &g, int i, int j, double prefactor) {
+  const int nx = g.nx;
+  const double dx = g.dxf[i - 1];
+  const double ux_xm = ux[ix_ux(nx, i, j)];
+  const double ux_xp = ux[ix_ux(nx, i + 1, j)];
+  const double uy_ym = uy[ix_cc(nx, i, j)];
+  const double uy_yp = uy[ix_cc(nx, i, j + 1)];
+  return prefactor * (+(ux_xp - ux_xm) / dx + (uy_yp - uy_ym) / g.dy);
+}
+
+// ---------------------------------------------------------------- DCT path
+// one block per row j; dynamic shared memory 2 nx doubles
+__global__ void k_dct_fwd(const double *__restrict__ ux, const double *__restrict__ uy,
+                          double *__restrict__ spec, const double *__restrict__ tw,
+                          const double *__restrict__ cs, const double *__restrict__ dtp,
+                          double gam, int log2n, Grid2 g) {
+  extern __shared__ double z[];
+  const int n = g.nx;
+  const int j = 1 + blockIdx.x;
+  const double dt = *dtp;
+  const double prefactor = 1. / (gam * dt) / (2. * n);
+  // Makhoul reordering v_m = x_{2m}, v_{n-1-m} = x_{2m+1}, stored bit-reversed
+  for (int q = threadIdx.x; q < n; q += blockDim.x) {
+    const int m = bitrev(q, log2n);
+    const int src = (m < n / 2) ? 2 * m : 2 * (n - 1 - m) + 1;
+    z[2 * q] = poisson_rhs(ux, uy, g, src + 1, j, prefactor);
+    z[2 * q + 1] = 0.;
+  }
+  __syncthreads();
+  fft_stages(z, log2n, 1, tw);
+  double *out = spec + (size_t)(j - 1) * n;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    const double c = cs[2 * k], s = cs[2 * k + 1];
+    out[k] = 2.0 * (c * z[2 * k] + s * z[2 * k + 1]);
+  }
+}
+
+// periodic tri-diagonal solve along y per wavenumber k (src/tdm.c:78-99 with
+// gtsv :17-50); vt, q1t ([j][k]) and den[k] are the k-dependent but
+// time-independent quantities of the reference's per-call recomputation
+__global__ void k_dct_ysolve(double *__restrict__ spec, const double *__restrict__ vt,
+                             const double *__restrict__ q1t, const double *__restrict__ ck,
+                             const double *__restrict__ den, double lap, int nx, int ny) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nx) return;
+  const int n = ny;
+  const double l = lap, u = lap, c = ck[k];
+#define Q(jj) spec[(size_t)(jj) * nx + k]
+#define V(jj) vt[(size_t)(jj) * nx + k]
+  // gtsv of size n-1 on rows 0 .. n-2
+  double qprev = Q(0) / c;
+  Q(0) = qprev;
+  for (int i = 1; i < n - 2; i++) {
+    const double val = 1. / (c - l * V(i - 1));
+    qprev = val * (Q(i) - l * qprev);
+    Q(i) = qprev;
+  }
+  {
+    const double val = c - l * V(n - 3);
+    Q(n - 2) = fabs(val) > kDblEpsilon ? 1. / val * (Q(n - 2) - l * qprev) : 0.;
+  }
+  double qn = Q(n - 2);
+  for (int i = n - 3; i >= 0; i--) {
+    qn = Q(i) - V(i) * qn;
+    Q(i) = qn;
+  }
+  // Sherman-Morrison correction
+  const double num = Q(n - 1) - u * qn - l * Q(n - 2);
+  const double d = den[k];
+  const double qlast = fabs(d) < kDblEpsilon ? 0. : num / d;
+  Q(n - 1) = qlast;
+  for (int i = 0; i < n - 1; i++) Q(i) = Q(i) + qlast * q1t[(size_t)i * nx + k];
+#undef Q
+#undef V
+}
+
+// one block per row j: REDFT01 then extract_output + fluid_update_boundaries_psi
+__global__ void k_dct_inv(const double *__restrict__ spec, double *__restrict__ psi,
+                          const double *__restrict__ tw, const double *__restrict__ cs,
+                          int log2n, Grid2 g) {
+  extern __shared__ double z[];
+  const int n = g.nx, nx = g.nx, ny = g.ny;
+  const int j = 1 + blockIdx.x;
+  const double *in = spec + (size_t)(j - 1) * n;
+  // old wall values of the rows that feed the halo (read before any write)
+  double wl = 0., wr = 0.;
+  if (0 == threadIdx.x && (1 == j || ny == j)) {
+    wl = psi[ix_cc(nx, 0, j)];
+    wr = psi[ix_cc(nx, nx + 1, j)];
+  }
+  for (int q = threadIdx.x; q < n; q += blockDim.x) {
+    const int m = bitrev(q, log2n);
+    const double a = in[m];
+    const double b = (0 == m) ? 0. : in[n - m];
+    const double c = cs[2 * m], s = cs[2 * m + 1];
+    z[2 * q] = c * a + s * b;
+    z[2 * q + 1] = s * a - c * b;
+  }
+  __syncthreads();
+  fft_stages(z, log2n, 1, tw);
+  for (int o = threadIdx.x; o < n; o += blockDim.x) {
+    const double y = (0 == (o & 1)) ? z[2 * (o >> 1)] : z[2 * (n - 1 - (o >> 1))];
+    const int i = o + 1;
+    psi[ix_cc(nx, i, j)] = y;
+    if (ny == j) psi[ix_cc(nx, i, 0)] = y;
+    if (1 == j) psi[ix_cc(nx, i, ny + 1)] = y;
+  }
+  if (0 == threadIdx.x) {
+    if (ny == j) {
+      psi[ix_cc(nx, 0, 0)] = wl;
+      psi[ix_cc(nx, nx + 1, 0)] = wr;
+    }
+    if (1 == j) {
+      psi[ix_cc(nx, 0, ny + 1)] = wl;
+      psi[ix_cc(nx, nx + 1, ny + 1)] = wr;
+    }
+    // Neumann walls, psi.c:7-20
+    psi[ix_cc(nx, 0, j)] = z[0];
+    psi[ix_cc(nx, nx + 1, j)] = z[2 * (n - 1 - ((n - 1) >> 1))];
+  }
+}
+
+// ---------------------------------------------------------------- DFT path
+// a block owns `cols` consecutive columns i0 .. i0+cols-1 and all ny rows;
+// dynamic shared memory cols * 2 ny doubles
+__global__ void k_dft_fwd(const double *__restrict__ ux, const double *__restrict__ uy,
+                          double *__restrict__ spec, const double *__restrict__ tw,
+                          const double *__restrict__ dtp, double gam, int log2n, int cols, Grid2 g) {
+  extern __shared__ double z[];
+  const int n = g.ny, nx = g.nx;
+  const int nky = n / 2 + 1;
+  const int i0 = 1 + blockIdx.x * cols;
+  const int nc = min(cols, nx - i0 + 1);
+  const double dt = *dtp;
+  const double prefactor = 1. / (gam * dt) / (1. * n);
+  for (int w = threadIdx.x; w < cols * n; w += blockDim.x) {
+    const int q = w / cols, col = w % cols;
+    const int m = bitrev(q, log2n);
+    double v = 0.;
+    if (col < nc) v = poisson_rhs(ux, uy, g, i0 + col, m + 1, prefactor);
+    z[2 * (col * n + q)] = v;
+    z[2 * (col * n + q) + 1] = 0.;
+  }
+  __syncthreads();
+  fft_stages(z, log2n, cols, tw);
+  for (int w = threadIdx.x; w < nc * nky; w += blockDim.x) {
+    const int col = w / nky, k = w % nky;
+    const size_t o = 2 * ((size_t)(i0 - 1 + col) * nky + k);
+    spec[o] = z[2 * (col * n + k)];
+    spec[o + 1] = z[2 * (col * n + k) + 1];
+  }
+}
+
+// complex Neumann Thomas along x per ky (dft.c:364-395); spec layout [i][ky],
+// vt[i][ky] holds the reference's v for each ky
+__global__ void k_dft_xsolve(double *__restrict__ spec, const double *__restrict__ vt,
+                             const double *__restrict__ pl, const double *__restrict__ pu,
+                             const double *__restrict__ evals, int nx, int nky) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nky) return;
+  const int n = nx;
+  const double ev = evals[k];
+#define QR(ii) spec[2 * ((size_t)(ii) * nky + k)]
+#define QI(ii) spec[2 * ((size_t)(ii) * nky + k) + 1]
+#define V(ii) vt[(size_t)(ii) * nky + k]
+  // tdm_c with the Neumann boundary rows
+  double c0 = -pl[0] - pu[0] + ev;
+  c0 += pl[0];
+  double pr = QR(0) / c0, pi = QI(0) / c0;
+  QR(0) = pr;
+  QI(0) = pi;
+  for (int i = 1; i < n - 1; i++) {
+    const double l = pl[i];
+    const double c = -l - pu[i] + ev;
+    const double val = 1. / (c - l * V(i - 1));
+    pr = val * (QR(i) - l * pr);
+    pi = val * (QI(i) - l * pi);
+    QR(i) = pr;
+    QI(i) = pi;
+  }
+  {
+    const double l = pl[n - 1];
+    double c = -l - pu[n - 1] + ev;
+    c += pu[n - 1];
+    const double val = c - l * V(n - 2);
+    if (fabs(val) > kDblEpsilon) {
+      QR(n - 1) = 1. / val * (QR(n - 1) - l * pr);
+      QI(n - 1) = 1. / val * (QI(n - 1) - l * pi);
+    } else {
+      QR(n - 1) = 0.;
+      QI(n - 1) = 0.;
+    }
+  }
+  double nr = QR(n - 1), ni = QI(n - 1);
+  for (int i = n - 2; i >= 0; i--) {
+    const double v = V(i);
+    nr = QR(i) - v * nr;
+    ni = QI(i) - v * ni;
+    QR(i) = nr;
+    QI(i) = ni;
+  }
+#undef QR
+#undef QI
+#undef V
+}
+
+// c2r along y for a tile of columns, extract_output and the psi boundaries
+__global__ void k_dft_inv(const double *__restrict__ spec, double *__restrict__ psi,
+                          const double *__restrict__ tw, int log2n, int cols, Grid2 g) {
+  extern __shared__ double z[];
+  const int n = g.ny, nx = g.nx, ny = g.ny;
+  const int nky = n / 2 + 1;
+  const int i0 = 1 + blockIdx.x * cols;
+  const int nc = min(cols, nx - i0 + 1);
+  const bool has_left = (1 == i0), has_right = (i0 + nc - 1 == nx);
+  // old wall values feeding the halo rows (read before any write)
+  double wl1 = 0., wln = 0., wr1 = 0., wrn = 0.;
+  if (0 == threadIdx.x) {
+    if (has_left) {
+      wl1 = psi[ix_cc(nx, 0, 1)];
+      wln = psi[ix_cc(nx, 0, ny)];
+    }
+    if (has_right) {
+      wr1 = psi[ix_cc(nx, nx + 1, 1)];
+      wrn = psi[ix_cc(nx, nx + 1, ny)];
+    }
+  }
+  // Hermitian extension as FFTW's c2r reads it: Im of X_0 and X_{n/2} ignored
+  for (int w = threadIdx.x; w < cols * n; w += blockDim.x) {
+    const int q = w / cols, col = w % cols;
+    const int m = bitrev(q, log2n);
+    double re = 0., im = 0.;
+    if (col < nc) {
+      const size_t base = 2 * ((size_t)(i0 - 1 + col) * nky);
+      if (0 == m) {
+        re = spec[base];
+      } else if (2 * m < n) {
+        re = spec[base + 2 * m];
+        im = spec[base + 2 * m + 1];
+      } else if (2 * m == n) {
+        re = spec[base + 2 * m];
+      } else {
+        re = spec[base + 2 * (n - m)];
+        im = -spec[base + 2 * (n - m) + 1];
+      }
+    }
+    z[2 * (col * n + q)] = re;
+    z[2 * (col * n + q) + 1] = im;
+  }
+  __syncthreads();
+  fft_stages(z, log2n, cols, tw);
+  for (int w = threadIdx.x; w < nc * n; w += blockDim.x) {
+    const int r = w / nc, col = w % nc;
+    const int i = i0 + col, j = r + 1;
+    const double y = z[2 * (col * n + r)];
+    psi[ix_cc(nx, i, j)] = y;
+    if (ny == j) psi[ix_cc(nx, i, 0)] = y;
+    if (1 == j) psi[ix_cc(nx, i, ny + 1)] = y;
+  }
+  __syncthreads();
+  if (0 == threadIdx.x) {
+    if (has_left) {
+      psi[ix_cc(nx, 0, 0)] = wln;
+      psi[ix_cc(nx, 0, ny + 1)] = wl1;
+    }
+    if (has_right) {
+      psi[ix_cc(nx, nx + 1, 0)] = wrn;
+      psi[ix_cc(nx, nx + 1, ny + 1)] = wr1;
+    }
+  }
+  // Neumann walls, psi.c:7-20
+  for (int j = 1 + threadIdx.x; j <= ny; j += blockDim.x) {
+    if (has_left) psi[ix_cc(nx, 0, j)] = z[2 * (0 * n + (j - 1))];
+    if (has_right) psi[ix_cc(nx, nx + 1, j)] = z[2 * ((nc - 1) * n + (j - 1))];
+  }
+}
+
+}  // namespace svof

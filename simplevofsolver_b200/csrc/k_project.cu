@@ -1,0 +1,220 @@
+// k_project.cu -- projection, pressure update, time-step and diagnostics
+// kernels of the FP64 2D path.
+//
+//   k_project   u -= gamma dt grad psi (src/fluid/correct_velocity/{ux,uy}.c)
+//               and p += psi - gamma dt nu / 2 Lx psi (src/fluid/update_pressure.c),
+//               in place, with the halo rows and walls of
+//               fluid_update_boundaries_{ux,uy,p}
+//   k_cfl       min over faces of dx / (|u| + 1e-8) (src/fluid/decide_dt.c:28-64)
+//   k_dt_final  safety factor and explicit-diffusion limits (:66-146)
+//   k_diag      max |div u|, vof min / max / volume (src/logging/divergence.c:36-50,
+//               src/logging/interface.c:22-39)
+#include "svof_internal.cuh"
+
+namespace svof {
+
+// one thread per cell i in [1, nx], j in [1, ny]; the thread at i = nx also
+// owns the ux column i = nx + 1
+__global__ void k_project(double *__restrict__ ux, double *__restrict__ uy, double *__restrict__ p,
+                          const double *__restrict__ psi, const double *__restrict__ dtp, double gam,
+                          double m_dif, double uy_xm, double uy_xp, int do_vel, int do_p, Grid2 g) {
+  const int nx = g.nx, ny = g.ny;
+  const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+  if (i > nx || j > ny) return;
+  const double dt = *dtp;
+  const bool top = (1 == j), bottom = (ny == j);
+  if (do_vel) {
+    const double prefactor = gam * dt;  // correct_velocity/main.c:21-23
+    // ux, correct_velocity/ux.c:16-41
+    if (i >= 2) {
+      const double dx = g.dxc[i - 1];
+      const double psi_xm = psi[ix_cc(nx, i - 1, j)];
+      const double psi_xp = psi[ix_cc(nx, i, j)];
+      double v = ux[ix_ux(nx, i, j)];
+      v -= prefactor / dx * (+psi_xp - psi_xm);
+      ux[ix_ux(nx, i, j)] = v;
+      if (bottom) ux[ix_ux(nx, i, 0)] = v;
+      if (top) ux[ix_ux(nx, i, ny + 1)] = v;
+    } else {
+      // wall i = 1: halo rows take the value before the wall assignment
+      const double w = ux[ix_ux(nx, 1, j)];
+      if (bottom) ux[ix_ux(nx, 1, 0)] = w;
+      if (top) ux[ix_ux(nx, 1, ny + 1)] = w;
+      ux[ix_ux(nx, 1, j)] = 0.;
+    }
+    if (nx == i) {
+      const double w = ux[ix_ux(nx, nx + 1, j)];
+      if (bottom) ux[ix_ux(nx, nx + 1, 0)] = w;
+      if (top) ux[ix_ux(nx, nx + 1, ny + 1)] = w;
+      ux[ix_ux(nx, nx + 1, j)] = 0.;
+    }
+    // uy, correct_velocity/uy.c:15-39
+    {
+      const double psi_ym = psi[ix_cc(nx, i, j - 1)];
+      const double psi_yp = psi[ix_cc(nx, i, j)];
+      double v = uy[ix_cc(nx, i, j)];
+      v -= prefactor / g.dy * (+psi_yp - psi_ym);
+      uy[ix_cc(nx, i, j)] = v;
+      if (bottom) uy[ix_cc(nx, i, 0)] = v;
+      if (top) uy[ix_cc(nx, i, ny + 1)] = v;
+    }
+    if (1 == i) {
+      const double w = uy[ix_cc(nx, 0, j)];
+      if (bottom) uy[ix_cc(nx, 0, 0)] = w;
+      if (top) uy[ix_cc(nx, 0, ny + 1)] = w;
+      uy[ix_cc(nx, 0, j)] = uy_xm;
+    }
+    if (nx == i) {
+      const double w = uy[ix_cc(nx, nx + 1, j)];
+      if (bottom) uy[ix_cc(nx, nx + 1, 0)] = w;
+      if (top) uy[ix_cc(nx, nx + 1, ny + 1)] = w;
+      uy[ix_cc(nx, nx + 1, j)] = uy_xp;
+    }
+  }
+  if (do_p) {
+    // update_pressure.c:12-109 (x implicit)
+    const double psi_c = psi[ix_cc(nx, i, j)];
+    double v = p[ix_cc(nx, i, j)];
+    v += psi_c;
+    const double prefactor = 0.5 * gam * dt * m_dif;
+    const double dpsidx_xm = (-psi[ix_cc(nx, i - 1, j)] + psi_c) / g.dxc[i - 1];
+    const double dpsidx_xp = (-psi_c + psi[ix_cc(nx, i + 1, j)]) / g.dxc[i];
+    v -= prefactor / g.dxf[i - 1] * (-dpsidx_xm + dpsidx_xp);
+    p[ix_cc(nx, i, j)] = v;
+    if (bottom) p[ix_cc(nx, i, 0)] = v;
+    if (top) p[ix_cc(nx, i, ny + 1)] = v;
+    // Neumann walls, boundary/p.c:7-20
+    if (1 == i) {
+      const double w = p[ix_cc(nx, 0, j)];
+      if (bottom) p[ix_cc(nx, 0, 0)] = w;
+      if (top) p[ix_cc(nx, 0, ny + 1)] = w;
+      p[ix_cc(nx, 0, j)] = v;
+    }
+    if (nx == i) {
+      const double w = p[ix_cc(nx, nx + 1, j)];
+      if (bottom) p[ix_cc(nx, nx + 1, 0)] = w;
+      if (top) p[ix_cc(nx, nx + 1, ny + 1)] = w;
+      p[ix_cc(nx, nx + 1, j)] = v;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// k_cfl: grid-stride over the ux faces i in [2, nx] and the uy faces
+// i in [1, nx] of rows 1..ny.  All candidates are positive, so the minimum
+// of their IEEE bit patterns (as unsigned integers) is the bit pattern of
+// the minimum; NaN candidates sort above every finite value and are ignored,
+// like fmin ignores them in the reference.
+__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+    v = w < v ? w : v;
+  }
+  return v;
+}
+
+__global__ void k_cfl(const double *__restrict__ ux, const double *__restrict__ uy,
+                      unsigned long long *__restrict__ minbits, Grid2 g) {
+  const int nx = g.nx, ny = g.ny;
+  const double small = 1.e-8;
+  unsigned long long best = 0x7ff0000000000000ull;  // +inf
+  const long nfx = (long)(nx - 1) * ny, nfy = (long)nx * ny;
+  const long stride = (long)gridDim.x * blockDim.x;
+  for (long w = (long)blockIdx.x * blockDim.x + threadIdx.x; w < nfx + nfy; w += stride) {
+    double cand;
+    if (w < nfx) {
+      const int i = 2 + (int)(w % (nx - 1));
+      const int j = 1 + (int)(w / (nx - 1));
+      const double dx = g.dxc[i - 1];
+      const double vel = fabs(ux[ix_ux(nx, i, j)]) + small;
+      cand = dx / vel;
+    } else {
+      const long v = w - nfx;
+      const int i = 1 + (int)(v % nx);
+      const int j = 1 + (int)(v / nx);
+      const double vel = fabs(uy[ix_cc(nx, i, j)]) + small;
+      cand = g.dy / vel;
+    }
+    const unsigned long long b = (unsigned long long)__double_as_longlong(cand);
+    best = b < best ? b : best;
+  }
+  best = warp_min_u64(best);
+  __shared__ unsigned long long sbest[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (0 == lane) sbest[warp] = best;
+  __syncthreads();
+  if (0 == warp) {
+    best = lane < (int)(blockDim.x >> 5) ? sbest[lane] : 0x7ff0000000000000ull;
+    best = warp_min_u64(best);
+    if (0 == lane) atomicMin(minbits, best);
+  }
+}
+
+// decide_dt_adv tail and fluid_decide_dt (src/fluid/decide_dt.c:61-63, 129-143);
+// dif_m_y, dif_t_y are decide_dt_dif's y limits, computed on the host.
+// Resets the accumulator to the bit pattern of 1.0 (the initial *dt = 1.).
+__global__ void k_dt_final(unsigned long long *minbits, double *dt, double coef_adv, double dif_m_y,
+                           double dif_t_y) {
+  double dta = fmin(1., __longlong_as_double((long long)*minbits));
+  dta *= coef_adv;
+  double r = dta;
+  r = fmin(r, dif_m_y);
+  r = fmin(r, dif_t_y);
+  *dt = r;
+  *minbits = (unsigned long long)__double_as_longlong(1.);
+}
+
+// ---------------------------------------------------------------------------
+// k_diag: one block, deterministic order; out = {divmax, vofmin, vofmax,
+// sum vof dx dy, sum dx dy}.  Sums use a TwoSum-compensated accumulation.
+__device__ __forceinline__ void two_sum_acc(double &s, double &c, double x) {
+  const double t = s + x;
+  const double bp = t - s;
+  const double err = (s - (t - bp)) + (x - bp);
+  s = t;
+  c += err;
+}
+
+__global__ void k_diag(const double *__restrict__ ux, const double *__restrict__ uy,
+                       const double *__restrict__ vof, double *__restrict__ out, Grid2 g) {
+  const int nx = g.nx, ny = g.ny;
+  double dmax = 0., vmin = 1., vmax = 0., s0 = 0., c0 = 0., s1 = 0., c1 = 0.;
+  for (long w = threadIdx.x; w < (long)nx * ny; w += blockDim.x) {
+    const int i = 1 + (int)(w % nx), j = 1 + (int)(w / nx);
+    const double dx = g.dxf[i - 1];
+    const double div = +(ux[ix_ux(nx, i + 1, j)] - ux[ix_ux(nx, i, j)]) / dx +
+                       (uy[ix_cc(nx, i, j + 1)] - uy[ix_cc(nx, i, j)]) / g.dy;
+    dmax = fmax(dmax, fabs(div));
+    const double lv = vof[ix_vof(nx, i, j)];
+    vmin = fmin(vmin, lv);
+    vmax = fmax(vmax, lv);
+    two_sum_acc(s0, c0, lv * (dx * g.dy));
+    two_sum_acc(s1, c1, dx * g.dy);
+  }
+  __shared__ double red[5][1024];
+  red[0][threadIdx.x] = dmax;
+  red[1][threadIdx.x] = vmin;
+  red[2][threadIdx.x] = vmax;
+  red[3][threadIdx.x] = s0 + c0;
+  red[4][threadIdx.x] = s1 + c1;
+  __syncthreads();
+  if (0 == threadIdx.x) {
+    double a = 0., b = 1., c = 0., ss0 = 0., cc0 = 0., ss1 = 0., cc1 = 0.;
+    for (int t = 0; t < (int)blockDim.x; t++) {
+      a = fmax(a, red[0][t]);
+      b = fmin(b, red[1][t]);
+      c = fmax(c, red[2][t]);
+      two_sum_acc(ss0, cc0, red[3][t]);
+      two_sum_acc(ss1, cc1, red[4][t]);
+    }
+    out[0] = a;
+    out[1] = b;
+    out[2] = c;
+    out[3] = ss0 + cc0;
+    out[4] = ss1 + cc1;
+  }
+}
+
+}  // namespace svof

@@ -1,0 +1,880 @@
+// solver.cu -- host engine and C ABI (include/svof_b200.h) of the FP64 2D path.
+//
+// Owns the device fields (reference layouts), the grid and line-solver tables,
+// the ping-pong buffers and one CUDA stream.  A full time step
+// (src/integrate.c:11-68) is captured once per buffer parity into a CUDA
+// graph and replayed; the only device->host traffic of a step is the 8-byte
+// dt the reference's integrate() returns.
+//
+// Tables that the reference recomputes on every call from time-independent
+// data (Laplacian coefficients, the Poisson tri-diagonal recurrences, FFT
+// twiddles) are computed here once, on the host, with the reference's
+// expressions, and uploaded; the values are therefore the ones the
+// reference uses.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/svof_b200.h"
+#include "svof_internal.cuh"
+
+using namespace svof;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return 1;
+}
+
+#define CK(x)                                                                  \
+  do {                                                                         \
+    cudaError_t e_ = (x);                                                      \
+    if (cudaSuccess != e_) return fail("%s: %s", #x, cudaGetErrorString(e_));  \
+  } while (0)
+
+#define CK_LAUNCH() CK(cudaGetLastError())
+
+constexpr double kPi = 3.14159265358979323846;        // oracle/svof_fft.c
+constexpr double kGPi = 3.14159265358979324;          // src/fluid/compute_potential/dct.c:20
+constexpr double RK_A[3] = {32. / 60., 25. / 60., 45. / 60.};
+constexpr double RK_B[3] = {0. / 60., -17. / 60., -25. / 60.};
+
+int ilog2_exact(int n) {
+  int l = 0;
+  while ((1 << l) < n) l++;
+  return ((1 << l) == n) ? l : -1;
+}
+
+// gtsv of src/tdm.c:17-50 on the host (used for the table set-up)
+void host_gtsv(int n, const double *l, const double *c, const double *u, double *v, double *q) {
+  v[0] = u[0] / c[0];
+  q[0] = q[0] / c[0];
+  for (int i = 1; i < n - 1; i++) {
+    const double val = 1. / (c[i] - l[i] * v[i - 1]);
+    v[i] = val * (u[i]);
+    q[i] = val * (q[i] - l[i] * q[i - 1]);
+  }
+  const double val = c[n - 1] - l[n - 1] * v[n - 2];
+  if (std::fabs(val) > kDblEpsilon) {
+    q[n - 1] = 1. / val * (q[n - 1] - l[n - 1] * q[n - 2]);
+  } else {
+    q[n - 1] = 0.;
+  }
+  for (int i = n - 2; i >= 0; i--) q[i] -= v[i] * q[i + 1];
+}
+
+struct DevBuf {
+  double *p = nullptr;
+  size_t n = 0;
+};
+
+}  // namespace
+
+struct svof_solver {
+  svof_params_t prm{};
+  int nx = 0, ny = 0;
+  double dy = 0.;
+  bool uniform = false;
+  int log2fft = 0;          // log2 of the FFT length (nx for DCT, ny for DFT)
+  cudaStream_t stream = nullptr;
+  // fields (two buffers where a kernel writes a new copy)
+  DevBuf ux[2], uy[2], t[2], vof[2];
+  DevBuf p, psi, curv, normal, ifrcx, ifrcy;
+  DevBuf sux[2], suy[2], st[2], svof[2];
+  int cur_u = 0;   // which of ux/uy/t[] is current
+  int cur_v = 0;   // which of vof[] is current
+  int sa_f = 0;    // which of sux/suy/st[] is src[rk_a]
+  int sa_v = 0;    // which of svof[] is src[rk_a]
+  // grid tables
+  DevBuf dxf, dxc, lap_ux, lap_uy, lap_t;
+  double lapy[3] = {0., 0., 0.};
+  double dif_m_y = 0., dif_t_y = 0.;
+  // Poisson
+  DevBuf spec, twf, twb, cs, vt, q1t, ck, den, pl, pu, evals;
+  // predict launch shape
+  int pred_rows = 1;
+  size_t pred_smem = 0;
+  int dft_cols = 1;
+  // time step
+  double *d_dt = nullptr;
+  unsigned long long *d_minbits = nullptr;
+  double *h_dt = nullptr;   // pinned, many slots for svof_run
+  int h_dt_slots = 0;
+  DevBuf diag;
+  std::vector<double> xf, xc, dxf_h, dxc_h;
+  // graphs keyed by the buffer state at the start of a step
+  std::map<int, cudaGraphExec_t> graphs;
+
+  Grid2 grid() const { return Grid2{nx, ny, dy, dxf.p, dxc.p}; }
+};
+
+namespace {
+
+int dalloc(DevBuf &b, size_t n) {
+  b.n = n;
+  CK(cudaMalloc(&b.p, sizeof(double) * (n ? n : 1)));
+  CK(cudaMemset(b.p, 0, sizeof(double) * (n ? n : 1)));
+  return 0;
+}
+
+int upload(DevBuf &b, const std::vector<double> &h) {
+  if (dalloc(b, h.size())) return 1;
+  CK(cudaMemcpy(b.p, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
+  return 0;
+}
+
+void dfree(DevBuf &b) {
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.n = 0;
+}
+
+// ---- launch helpers: each issues the kernels of one reference function ----
+
+int launch_halo_bc(svof_solver *s, double *a, int field) {
+  const int nx = s->nx, ny = s->ny;
+  int width, nh, kind;
+  double lo = 0., hi = 0.;
+  switch (field) {
+    case SVOF_UX: width = nx + 1; nh = 1; kind = BC_ZERO_UX; break;
+    case SVOF_UY: width = nx + 2; nh = 1; kind = BC_DIRICHLET; lo = s->prm.uy_xm; hi = s->prm.uy_xp; break;
+    case SVOF_T: width = nx + 2; nh = 1; kind = BC_DIRICHLET; lo = s->prm.t_xm; hi = s->prm.t_xp; break;
+    case SVOF_P: case SVOF_PSI: width = nx + 2; nh = 1; kind = BC_NEUMANN; break;
+    case SVOF_VOF: width = nx + 2; nh = 2; kind = BC_VOF; break;
+    default: return fail("no boundary rule for field %d", field);
+  }
+  k_halo_bc<<<(width + 127) / 128, 128, 0, s->stream>>>(a, width, nh, ny, kind, lo, hi);
+  CK_LAUNCH();
+  return 0;
+}
+
+int launch_dt(svof_solver *s) {
+  const long nf = (long)(s->nx - 1) * s->ny + (long)s->nx * s->ny;
+  int blocks = (int)std::min<long>((nf + 255) / 256, 148L * 8);
+  k_cfl<<<blocks, 256, 0, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->d_minbits, s->grid());
+  CK_LAUNCH();
+  k_dt_final<<<1, 1, 0, s->stream>>>(s->d_minbits, s->d_dt, s->prm.coef_dt_adv, s->dif_m_y, s->dif_t_y);
+  CK_LAUNCH();
+  return 0;
+}
+
+int launch_geom(svof_solver *s) {
+  dim3 b(32, 8), gr((s->nx + 31) / 32, (s->ny + 2 + 7) / 8);
+  k_geom<<<gr, b, 0, s->stream>>>(s->vof[s->cur_v].p, s->normal.p, s->curv.p, s->grid());
+  CK_LAUNCH();
+  return 0;
+}
+
+int launch_force(svof_solver *s) {
+  dim3 b(32, 8), gr((s->nx + 31) / 32, (s->ny + 7) / 8);
+  k_force<<<gr, b, 0, s->stream>>>(s->vof[s->cur_v].p, s->curv.p, s->ifrcx.p, s->ifrcy.p, s->prm.tension,
+                                   s->grid());
+  CK_LAUNCH();
+  return 0;
+}
+
+int launch_vof(svof_solver *s, int rk) {
+  if (0 != rk) s->sa_v ^= 1;  // reset_srcs, src/interface/update/main.c:28-45
+  dim3 b(32, 8), gr((s->nx + 31) / 32, (s->ny + 7) / 8);
+  RK c{RK_A[rk], RK_B[rk], RK_A[rk] + RK_B[rk]};
+  k_vof_advect<<<gr, b, 0, s->stream>>>(s->vof[s->cur_v].p, s->vof[1 - s->cur_v].p, s->ux[s->cur_u].p,
+                                        s->uy[s->cur_u].p, s->normal.p, s->svof[s->sa_v].p,
+                                        s->svof[1 - s->sa_v].p, s->d_dt, c, rk != 0, s->grid());
+  CK_LAUNCH();
+  s->cur_v ^= 1;
+  return 0;
+}
+
+int launch_predict(svof_solver *s, int rk) {
+  if (0 != rk) s->sa_f ^= 1;  // reset_srcs, src/fluid/predict/main.c:9-29
+  PredictArgs a{};
+  const int cu = s->cur_u;
+  a.ux = s->ux[cu].p;
+  a.uy = s->uy[cu].p;
+  a.t = s->t[cu].p;
+  a.p = s->p.p;
+  a.ifrcx = s->ifrcx.p;
+  a.ifrcy = s->ifrcy.p;
+  a.ux_new = s->ux[1 - cu].p;
+  a.uy_new = s->uy[1 - cu].p;
+  a.t_new = s->t[1 - cu].p;
+  a.sux_a = s->sux[s->sa_f].p;
+  a.suy_a = s->suy[s->sa_f].p;
+  a.st_a = s->st[s->sa_f].p;
+  a.sux_b = s->sux[1 - s->sa_f].p;
+  a.suy_b = s->suy[1 - s->sa_f].p;
+  a.st_b = s->st[1 - s->sa_f].p;
+  a.lap_ux = s->lap_ux.p;
+  a.lap_uy = s->lap_uy.p;
+  a.lap_t = s->lap_t.p;
+  a.dtp = s->d_dt;
+  a.m_dif = s->prm.m_dif;
+  a.t_dif = s->prm.t_dif;
+  a.lapy0 = s->lapy[0];
+  a.lapy1 = s->lapy[1];
+  a.lapy2 = s->lapy[2];
+  a.rk = RK{RK_A[rk], RK_B[rk], RK_A[rk] + RK_B[rk]};
+  a.use_b = rk != 0;
+  a.add_buoyancy = s->prm.add_buoyancy;
+  a.uy_xm = s->prm.uy_xm;
+  a.uy_xp = s->prm.uy_xp;
+  a.t_xm = s->prm.t_xm;
+  a.t_xp = s->prm.t_xp;
+  a.rows_per_block = s->pred_rows;
+  a.g = s->grid();
+  const int blocks = (s->ny + s->pred_rows - 1) / s->pred_rows;
+  k_predict<<<blocks, 256, s->pred_smem, s->stream>>>(a);
+  CK_LAUNCH();
+  s->cur_u ^= 1;
+  return 0;
+}
+
+int launch_potential(svof_solver *s, int rk, int want_dct) {
+  const double gam = RK_A[rk] + RK_B[rk];
+  const Grid2 g = s->grid();
+  if (want_dct != (int)s->uniform) {
+    return fail(want_dct ? "DCT Poisson path needs a uniform x grid" : "DFT path requested on a uniform grid");
+  }
+  if (s->uniform) {
+    const int nthr = std::min(256, std::max(32, s->nx / 2));
+    const size_t smem = sizeof(double) * 2 * s->nx;
+    k_dct_fwd<<<s->ny, nthr, smem, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->spec.p, s->twf.p,
+                                                s->cs.p, s->d_dt, gam, s->log2fft, g);
+    CK_LAUNCH();
+    k_dct_ysolve<<<(s->nx + 127) / 128, 128, 0, s->stream>>>(s->spec.p, s->vt.p, s->q1t.p, s->ck.p, s->den.p,
+                                                             1. / s->dy / s->dy, s->nx, s->ny);
+    CK_LAUNCH();
+    k_dct_inv<<<s->ny, nthr, smem, s->stream>>>(s->spec.p, s->psi.p, s->twb.p, s->cs.p, s->log2fft, g);
+    CK_LAUNCH();
+  } else {
+    const int cols = s->dft_cols;
+    const int blocks = (s->nx + cols - 1) / cols;
+    const size_t smem = sizeof(double) * 2 * s->ny * cols;
+    const int nky = s->ny / 2 + 1;
+    k_dft_fwd<<<blocks, 256, smem, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->spec.p, s->twf.p,
+                                                s->d_dt, gam, s->log2fft, cols, g);
+    CK_LAUNCH();
+    k_dft_xsolve<<<(nky + 127) / 128, 128, 0, s->stream>>>(s->spec.p, s->vt.p, s->pl.p, s->pu.p, s->evals.p,
+                                                            s->nx, nky);
+    CK_LAUNCH();
+    k_dft_inv<<<blocks, 256, smem, s->stream>>>(s->spec.p, s->psi.p, s->twb.p, s->log2fft, cols, g);
+    CK_LAUNCH();
+  }
+  return 0;
+}
+
+int launch_project(svof_solver *s, int rk, int do_vel, int do_p) {
+  dim3 b(32, 8), gr((s->nx + 31) / 32, (s->ny + 7) / 8);
+  k_project<<<gr, b, 0, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->p.p, s->psi.p, s->d_dt,
+                                     RK_A[rk] + RK_B[rk], s->prm.m_dif, s->prm.uy_xm, s->prm.uy_xp, do_vel,
+                                     do_p, s->grid());
+  CK_LAUNCH();
+  return 0;
+}
+
+// the kernel sequence of integrate(), src/integrate.c:11-68
+int launch_step(svof_solver *s) {
+  if (launch_dt(s)) return 1;
+  for (int rk = 0; rk < 3; rk++) {
+    if (launch_geom(s)) return 1;
+    if (launch_force(s)) return 1;
+    if (launch_vof(s, rk)) return 1;
+    if (launch_predict(s, rk)) return 1;
+    if (launch_potential(s, rk, s->uniform)) return 1;
+    if (launch_project(s, rk, 1, 1)) return 1;
+  }
+  return 0;
+}
+
+int state_key(const svof_solver *s) { return s->cur_u | (s->cur_v << 1) | (s->sa_f << 2) | (s->sa_v << 3); }
+
+int step_graph(svof_solver *s, cudaGraphExec_t *exec) {
+  const int key = state_key(s);
+  auto it = s->graphs.find(key);
+  if (it != s->graphs.end()) {
+    *exec = it->second;
+    // advance the host-side buffer state as the captured step does: three
+    // field swaps per step (odd), two source swaps (even)
+    s->cur_u ^= 1;
+    s->cur_v ^= 1;
+    return 0;
+  }
+  cudaGraph_t graph;
+  CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+  const int rc = launch_step(s);
+  cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
+  if (rc) return 1;
+  if (cudaSuccess != e) return fail("cudaStreamEndCapture: %s", cudaGetErrorString(e));
+  cudaGraphExec_t ge;
+  CK(cudaGraphInstantiate(&ge, graph, 0));
+  cudaGraphDestroy(graph);
+  s->graphs[key] = ge;
+  *exec = ge;
+  return 0;
+}
+
+int field_buf(svof_solver *s, int field, DevBuf **b) {
+  switch (field) {
+    case SVOF_UX: *b = &s->ux[s->cur_u]; break;
+    case SVOF_UY: *b = &s->uy[s->cur_u]; break;
+    case SVOF_T: *b = &s->t[s->cur_u]; break;
+    case SVOF_VOF: *b = &s->vof[s->cur_v]; break;
+    case SVOF_P: *b = &s->p; break;
+    case SVOF_PSI: *b = &s->psi; break;
+    case SVOF_CURV: *b = &s->curv; break;
+    case SVOF_NORMAL: *b = &s->normal; break;
+    case SVOF_IFRCX: *b = &s->ifrcx; break;
+    case SVOF_IFRCY: *b = &s->ifrcy; break;
+    case SVOF_SRCUX_A: *b = &s->sux[s->sa_f]; break;
+    case SVOF_SRCUX_B: *b = &s->sux[1 - s->sa_f]; break;
+    case SVOF_SRCUY_A: *b = &s->suy[s->sa_f]; break;
+    case SVOF_SRCUY_B: *b = &s->suy[1 - s->sa_f]; break;
+    case SVOF_SRCT_A: *b = &s->st[s->sa_f]; break;
+    case SVOF_SRCT_B: *b = &s->st[1 - s->sa_f]; break;
+    case SVOF_SRC_A: *b = &s->svof[s->sa_v]; break;
+    case SVOF_SRC_B: *b = &s->svof[1 - s->sa_v]; break;
+    default: return fail("unknown field id %d", field);
+  }
+  return 0;
+}
+
+// number of halo rows and row width of the restart-file fields
+int interior_layout(const svof_solver *s, int field, int *nh, int *width) {
+  switch (field) {
+    case SVOF_UX: *nh = 1; *width = s->nx + 1; return 0;
+    case SVOF_UY: case SVOF_P: case SVOF_T: case SVOF_PSI: *nh = 1; *width = s->nx + 2; return 0;
+    case SVOF_VOF: *nh = 2; *width = s->nx + 2; return 0;
+    default: return fail("field %d has no restart-file layout", field);
+  }
+}
+
+int build_tables(svof_solver *s, const double *xf, const double *xc) {
+  const int nx = s->nx, ny = s->ny;
+  s->xf.assign(xf, xf + nx + 1);
+  s->xc.assign(xc, xc + nx + 2);
+  // src/domain.c:107-143, :190-192, :75-98
+  std::vector<double> dxf(nx), dxc(nx + 1);
+  for (int i = 1; i <= nx; i++) dxf[i - 1] = xf[i] - xf[i - 1];
+  for (int i = 1; i <= nx + 1; i++) dxc[i - 1] = xc[i] - xc[i - 1];
+  s->dxf_h = dxf;
+  s->dxc_h = dxc;
+  s->dy = s->prm.ly / ny;
+  {
+    double mn = +1. * 1.7976931348623157e308, mx = -1. * 1.7976931348623157e308;
+    for (int i = 0; i < nx; i++) {
+      mn = std::fmin(mn, dxf[i]);
+      mx = std::fmax(mx, dxf[i]);
+    }
+    s->uniform = std::fabs(mx - mn) < 1.e-15;
+  }
+  if (upload(s->dxf, dxf) || upload(s->dxc, dxc)) return 1;
+  auto DXF = [&](int i) { return dxf[i - 1]; };
+  auto DXC = [&](int i) { return dxc[i - 1]; };
+  // Laplacians, src/fluid/predict/{ux,uy,t}.c init_lap
+  std::vector<double> lux(3 * (nx - 1)), luy(3 * nx);
+  for (int i = 2; i <= nx; i++) {
+    const double l = 1. / DXF(i - 1) / DXC(i);
+    const double u = 1. / DXF(i) / DXC(i);
+    const double c = -l - u;
+    lux[3 * (i - 2) + 0] = l;
+    lux[3 * (i - 2) + 1] = c;
+    lux[3 * (i - 2) + 2] = u;
+  }
+  for (int i = 1; i <= nx; i++) {
+    const double l = 1. / DXC(i) / DXF(i);
+    const double u = 1. / DXC(i + 1) / DXF(i);
+    const double c = -l - u;
+    luy[3 * (i - 1) + 0] = l;
+    luy[3 * (i - 1) + 1] = c;
+    luy[3 * (i - 1) + 2] = u;
+  }
+  if (upload(s->lap_ux, lux) || upload(s->lap_uy, luy) || upload(s->lap_t, luy)) return 1;
+  s->lapy[0] = +1. / s->dy / s->dy;
+  s->lapy[1] = -2. / s->dy / s->dy;
+  s->lapy[2] = +1. / s->dy / s->dy;
+  // decide_dt_dif y limits, src/fluid/decide_dt.c:73-94
+  const int ndims = 2;
+  s->dif_m_y = s->prm.coef_dt_dif / s->prm.m_dif * 0.5 / ndims * std::pow(s->dy, 2.);
+  s->dif_t_y = s->prm.coef_dt_dif / s->prm.t_dif * 0.5 / ndims * std::pow(s->dy, 2.);
+  // FFT twiddles (oracle/svof_fft.c svof_fft_twiddles / svof_dct_twiddles)
+  const int nfft = s->uniform ? nx : ny;
+  s->log2fft = ilog2_exact(nfft);
+  if (s->log2fft < 1) {
+    return fail("the %s direction needs a power-of-two size (got %d)", s->uniform ? "x" : "y", nfft);
+  }
+  {
+    std::vector<double> twf(2 * (nfft / 2)), twb(2 * (nfft / 2)), cs(2 * nfft);
+    for (int m = 0; m < nfft / 2; m++) {
+      const double ang = 2.0 * kPi * (double)m / (double)nfft;
+      twf[2 * m] = std::cos(ang);
+      twf[2 * m + 1] = -std::sin(ang);
+      twb[2 * m] = std::cos(ang);
+      twb[2 * m + 1] = std::sin(ang);
+    }
+    for (int k = 0; k < nfft; k++) {
+      const double ang = kPi * (double)k / (2.0 * (double)nfft);
+      cs[2 * k] = std::cos(ang);
+      cs[2 * k + 1] = std::sin(ang);
+    }
+    if (upload(s->twf, twf) || upload(s->twb, twb) || upload(s->cs, cs)) return 1;
+  }
+  if (s->uniform) {
+    // src/fluid/compute_potential/dct.c:142-178 and :233-261
+    const int n = ny;
+    const double lap = 1. / s->dy / s->dy;
+    std::vector<double> l(n, lap), u(n, lap), c(n), v(n), q1(n);
+    std::vector<double> vt((size_t)n * nx, 0.), q1t((size_t)n * nx, 0.), ck(nx), den(nx);
+    const double signal_length = 2. * nx;
+    const double gridsize = s->prm.lx / nx;
+    for (size_t k = 0; k < (size_t)nx; k++) {
+      const double ev = -4. / std::pow(gridsize, 2.) * std::pow(std::sin(kGPi * k / signal_length), 2.);
+      for (int r = 0; r < n; r++) c[r] = -l[r] - u[r] + ev;
+      for (int i = 0; i < n - 1; i++) q1[i] = i == 0 ? -l[i] : i == n - 2 ? -u[i] : 0.;
+      host_gtsv(n - 1, l.data(), c.data(), u.data(), v.data(), q1.data());
+      for (int i = 0; i < n - 1; i++) {
+        vt[(size_t)i * nx + k] = v[i];
+        q1t[(size_t)i * nx + k] = q1[i];
+      }
+      ck[k] = c[0];
+      den[k] = c[n - 1] + u[n - 1] * q1[0] + l[n - 1] * q1[n - 2];
+    }
+    if (upload(s->vt, vt) || upload(s->q1t, q1t) || upload(s->ck, ck) || upload(s->den, den)) return 1;
+    if (dalloc(s->spec, (size_t)nx * ny)) return 1;
+  } else {
+    // src/fluid/compute_potential/dft.c:142-198 and :263-291
+    const int n = nx, nky = ny / 2 + 1;
+    std::vector<double> pl(n), pu(n), ev(nky), c(n), v(n), vt((size_t)n * nky, 0.);
+    for (int i = 1; i <= n; i++) {
+      pl[i - 1] = 1. / DXC(i) / DXF(i);
+      pu[i - 1] = 1. / DXC(i + 1) / DXF(i);
+    }
+    const double signal_length = (double)ny;
+    const double gridsize = s->prm.ly / ny;
+    for (size_t j = 0; j < (size_t)nky; j++) {
+      ev[j] = -4. / std::pow(gridsize, 2.) * std::pow(std::sin(kGPi * j / signal_length), 2.);
+    }
+    for (int k = 0; k < nky; k++) {
+      for (int i = 0; i < n; i++) c[i] = -pl[i] - pu[i] + ev[k];
+      c[0] += pl[0];
+      c[n - 1] += pu[n - 1];
+      v[0] = pu[0] / c[0];
+      for (int i = 1; i < n - 1; i++) {
+        const double val = 1. / (c[i] - pl[i] * v[i - 1]);
+        v[i] = val * (pu[i]);
+      }
+      for (int i = 0; i < n - 1; i++) vt[(size_t)i * nky + k] = v[i];
+    }
+    if (upload(s->pl, pl) || upload(s->pu, pu) || upload(s->evals, ev) || upload(s->vt, vt)) return 1;
+    if (dalloc(s->spec, 2 * (size_t)nx * nky)) return 1;
+  }
+  return 0;
+}
+
+}  // namespace
+
+// =========================================================================== C ABI
+extern "C" {
+
+const char *svof_last_error(void) { return g_err.c_str(); }
+
+int svof_create(const svof_params_t *prm, const double *xf, const double *xc, svof_solver_t **out) {
+  if (!prm || !xf || !xc || !out) return fail("svof_create: null argument");
+  *out = nullptr;
+  if (prm->nx < 4 || prm->ny < 4) return fail("svof_create: nx and ny must be at least 4");
+  if (!(prm->m_dif > 0.) || !(prm->t_dif > 0.)) return fail("svof_create: diffusivities must be positive");
+  svof_solver *s = new svof_solver();
+  s->prm = *prm;
+  s->nx = prm->nx;
+  s->ny = prm->ny;
+  auto bail = [&]() {
+    std::string e = g_err;
+    svof_destroy(s);
+    g_err = e;
+    return 1;
+  };
+  if (cudaSuccess != cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) {
+    delete s;
+    return fail("svof_create: no CUDA device available (%s)", cudaGetErrorString(cudaGetLastError()));
+  }
+  const int nx = s->nx, ny = s->ny;
+  const size_t n_ux = (size_t)(nx + 1) * (ny + 2), n_cc = (size_t)(nx + 2) * (ny + 2);
+  const size_t n_vof = (size_t)(nx + 2) * (ny + 4), n_src = (size_t)nx * ny, n_srcx = (size_t)(nx - 1) * ny;
+  for (int k = 0; k < 2; k++) {
+    if (dalloc(s->ux[k], n_ux) || dalloc(s->uy[k], n_cc) || dalloc(s->t[k], n_cc) || dalloc(s->vof[k], n_vof))
+      return bail();
+    if (dalloc(s->sux[k], n_srcx) || dalloc(s->suy[k], n_src) || dalloc(s->st[k], n_src) ||
+        dalloc(s->svof[k], n_src))
+      return bail();
+  }
+  if (dalloc(s->p, n_cc) || dalloc(s->psi, n_cc) || dalloc(s->curv, n_cc) ||
+      dalloc(s->normal, 3 * (size_t)nx * (ny + 2)) || dalloc(s->ifrcx, n_srcx) || dalloc(s->ifrcy, n_src) ||
+      dalloc(s->diag, 8))
+    return bail();
+  if (build_tables(s, xf, xc)) return bail();
+  // predict launch shape: R rows per block within 200 KB of shared memory
+  {
+    const long per_row = 3L * (nx + 1);
+    long r = (200L * 1024 / 8 - per_row) / per_row;
+    r = std::max(1L, std::min(8L, r));
+    s->pred_rows = (int)r;
+    s->pred_smem = predict_smem_bytes(nx, s->pred_rows);
+    if (s->pred_smem > 227 * 1024) return fail("svof_create: nx = %d too large for the x line solver", nx), bail();
+    if (cudaSuccess != cudaFuncSetAttribute(k_predict, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)s->pred_smem))
+      return fail("cudaFuncSetAttribute(k_predict): %s", cudaGetErrorString(cudaGetLastError())), bail();
+  }
+  {
+    const size_t dct_smem = sizeof(double) * 2 * nx;
+    if (s->uniform && dct_smem > 48 * 1024) {
+      cudaFuncSetAttribute(k_dct_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dct_smem);
+      cudaFuncSetAttribute(k_dct_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dct_smem);
+    }
+    int cols = 16;
+    while (cols > 1 && sizeof(double) * 2 * (size_t)ny * cols > 100 * 1024) cols >>= 1;
+    s->dft_cols = cols;
+    const size_t dft_smem = sizeof(double) * 2 * (size_t)ny * cols;
+    if (!s->uniform && dft_smem > 48 * 1024) {
+      cudaFuncSetAttribute(k_dft_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dft_smem);
+      cudaFuncSetAttribute(k_dft_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dft_smem);
+    }
+    if (sizeof(double) * 2 * (size_t)(s->uniform ? nx : ny) > 200 * 1024)
+      return fail("svof_create: FFT length too large for one block"), bail();
+  }
+  if (cudaSuccess != cudaMalloc(&s->d_dt, sizeof(double))) return fail("cudaMalloc dt"), bail();
+  if (cudaSuccess != cudaMalloc(&s->d_minbits, sizeof(unsigned long long))) return fail("cudaMalloc"), bail();
+  {
+    const double one = 1.;
+    unsigned long long bits;
+    std::memcpy(&bits, &one, sizeof(bits));
+    cudaMemcpy(s->d_minbits, &bits, sizeof(bits), cudaMemcpyHostToDevice);
+    cudaMemset(s->d_dt, 0, sizeof(double));
+  }
+  s->h_dt_slots = 1024;
+  if (cudaSuccess != cudaMallocHost(&s->h_dt, sizeof(double) * s->h_dt_slots)) return fail("cudaMallocHost"), bail();
+  if (cudaSuccess != cudaDeviceSynchronize()) return fail("svof_create: %s", cudaGetErrorString(cudaGetLastError())), bail();
+  *out = s;
+  return 0;
+}
+
+int svof_destroy(svof_solver_t *s) {
+  if (!s) return 0;
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  for (auto &kv : s->graphs) cudaGraphExecDestroy(kv.second);
+  s->graphs.clear();
+  for (int k = 0; k < 2; k++) {
+    dfree(s->ux[k]); dfree(s->uy[k]); dfree(s->t[k]); dfree(s->vof[k]);
+    dfree(s->sux[k]); dfree(s->suy[k]); dfree(s->st[k]); dfree(s->svof[k]);
+  }
+  DevBuf *bufs[] = {&s->p, &s->psi, &s->curv, &s->normal, &s->ifrcx, &s->ifrcy, &s->dxf, &s->dxc,
+                    &s->lap_ux, &s->lap_uy, &s->lap_t, &s->spec, &s->twf, &s->twb, &s->cs, &s->vt,
+                    &s->q1t, &s->ck, &s->den, &s->pl, &s->pu, &s->evals, &s->diag};
+  for (DevBuf *b : bufs) dfree(*b);
+  if (s->d_dt) cudaFree(s->d_dt);
+  if (s->d_minbits) cudaFree(s->d_minbits);
+  if (s->h_dt) cudaFreeHost(s->h_dt);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+  return 0;
+}
+
+int svof_field_count(const svof_solver_t *cs, int field, size_t *count) {
+  svof_solver *s = const_cast<svof_solver *>(cs);
+  DevBuf *b;
+  if (!s || !count) return fail("null argument");
+  if (field_buf(s, field, &b)) return 1;
+  *count = b->n;
+  return 0;
+}
+
+int svof_upload_field(svof_solver_t *s, int field, const double *host, size_t count) {
+  DevBuf *b;
+  if (!s || !host) return fail("null argument");
+  if (field_buf(s, field, &b)) return 1;
+  if (count != b->n) return fail("field %d holds %zu doubles, got %zu", field, b->n, count);
+  CK(cudaMemcpyAsync(b->p, host, sizeof(double) * count, cudaMemcpyHostToDevice, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+int svof_download_field(svof_solver_t *s, int field, double *host, size_t count) {
+  DevBuf *b;
+  if (!s || !host) return fail("null argument");
+  if (field_buf(s, field, &b)) return 1;
+  if (count != b->n) return fail("field %d holds %zu doubles, got %zu", field, b->n, count);
+  CK(cudaMemcpyAsync(host, b->p, sizeof(double) * count, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+int svof_device_field(svof_solver_t *s, int field, double **dptr) {
+  DevBuf *b;
+  if (!s || !dptr) return fail("null argument");
+  if (field_buf(s, field, &b)) return 1;
+  *dptr = b->p;
+  return 0;
+}
+
+int svof_load_interior(svof_solver_t *s, int field, const double *host, size_t count) {
+  int nh, width;
+  DevBuf *b;
+  if (!s || !host) return fail("null argument");
+  if (interior_layout(s, field, &nh, &width) || field_buf(s, field, &b)) return 1;
+  const size_t n = (size_t)width * s->ny;
+  if (count != n) return fail("field %d: restart layout holds %zu doubles, got %zu", field, n, count);
+  CK(cudaMemcpyAsync(b->p + (size_t)nh * width, host, sizeof(double) * n, cudaMemcpyHostToDevice, s->stream));
+  if (launch_halo_bc(s, b->p, field)) return 1;
+  CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+int svof_store_interior(svof_solver_t *s, int field, double *host, size_t count) {
+  int nh, width;
+  DevBuf *b;
+  if (!s || !host) return fail("null argument");
+  if (interior_layout(s, field, &nh, &width) || field_buf(s, field, &b)) return 1;
+  const size_t n = (size_t)width * s->ny;
+  if (count != n) return fail("field %d: restart layout holds %zu doubles, got %zu", field, n, count);
+  CK(cudaMemcpyAsync(host, b->p + (size_t)nh * width, sizeof(double) * n, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+int svof_x_grid_is_uniform(const svof_solver_t *s, int *u) {
+  if (!s || !u) return fail("null argument");
+  *u = s->uniform ? 1 : 0;
+  return 0;
+}
+
+int svof_fluid_decide_dt(svof_solver_t *s, double *dt) {
+  if (!s || !dt) return fail("null argument");
+  if (launch_dt(s)) return 1;
+  CK(cudaMemcpyAsync(s->h_dt, s->d_dt, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  *dt = s->h_dt[0];
+  return 0;
+}
+
+static int set_dt(svof_solver_t *s, double dt) {
+  s->h_dt[0] = dt;
+  CK(cudaMemcpyAsync(s->d_dt, s->h_dt, sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  return 0;
+}
+
+static int check_rk(size_t rkstep) { return rkstep < 3 ? 0 : fail("rkstep %zu out of range", rkstep); }
+
+static int finish(svof_solver_t *s) {
+  CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+int svof_interface_compute_curvature_tensor(svof_solver_t *s) {
+  if (!s) return fail("null argument");
+  if (launch_geom(s)) return 1;
+  return finish(s);
+}
+
+int svof_interface_compute_force(svof_solver_t *s) {
+  if (!s) return fail("null argument");
+  if (launch_force(s)) return 1;
+  return finish(s);
+}
+
+int svof_interface_update_vof(svof_solver_t *s, size_t rk, double dt) {
+  if (!s) return fail("null argument");
+  if (check_rk(rk) || set_dt(s, dt) || launch_vof(s, (int)rk)) return 1;
+  return finish(s);
+}
+
+int svof_fluid_predict_field(svof_solver_t *s, size_t rk, double dt) {
+  if (!s) return fail("null argument");
+  if (check_rk(rk) || set_dt(s, dt) || launch_predict(s, (int)rk)) return 1;
+  return finish(s);
+}
+
+int svof_fluid_compute_potential_dct(svof_solver_t *s, size_t rk, double dt) {
+  if (!s) return fail("null argument");
+  if (check_rk(rk) || set_dt(s, dt) || launch_potential(s, (int)rk, 1)) return 1;
+  return finish(s);
+}
+
+int svof_fluid_compute_potential_dft(svof_solver_t *s, size_t rk, double dt) {
+  if (!s) return fail("null argument");
+  if (check_rk(rk) || set_dt(s, dt) || launch_potential(s, (int)rk, 0)) return 1;
+  return finish(s);
+}
+
+int svof_fluid_correct_velocity(svof_solver_t *s, size_t rk, double dt) {
+  if (!s) return fail("null argument");
+  if (check_rk(rk) || set_dt(s, dt) || launch_project(s, (int)rk, 1, 0)) return 1;
+  return finish(s);
+}
+
+int svof_fluid_update_pressure(svof_solver_t *s, size_t rk, double dt) {
+  if (!s) return fail("null argument");
+  if (check_rk(rk) || set_dt(s, dt) || launch_project(s, (int)rk, 0, 1)) return 1;
+  return finish(s);
+}
+
+int svof_run(svof_solver_t *s, int nsteps, double *dts) {
+  if (!s) return fail("null argument");
+  if (nsteps < 0) return fail("nsteps must be non-negative");
+  for (int n = 0; n < nsteps; n++) {
+    cudaGraphExec_t ge;
+    if (step_graph(s, &ge)) return 1;
+    CK(cudaGraphLaunch(ge, s->stream));
+    if (dts) {
+      const int slot = n % s->h_dt_slots;
+      if (0 == slot && n > 0) {
+        CK(cudaStreamSynchronize(s->stream));
+        std::memcpy(dts + n - s->h_dt_slots, s->h_dt, sizeof(double) * s->h_dt_slots);
+      }
+      CK(cudaMemcpyAsync(s->h_dt + slot, s->d_dt, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    }
+  }
+  CK(cudaStreamSynchronize(s->stream));
+  if (dts && nsteps > 0) {
+    const int done = ((nsteps - 1) / s->h_dt_slots) * s->h_dt_slots;
+    std::memcpy(dts + done, s->h_dt, sizeof(double) * (nsteps - done));
+  }
+  return 0;
+}
+
+int svof_enqueue_steps(svof_solver_t *s, int nsteps) {
+  if (!s) return fail("null argument");
+  if (nsteps < 0) return fail("nsteps must be non-negative");
+  for (int n = 0; n < nsteps; n++) {
+    cudaGraphExec_t ge;
+    if (step_graph(s, &ge)) return 1;
+    CK(cudaGraphLaunch(ge, s->stream));
+    CK(cudaMemcpyAsync(s->h_dt, s->d_dt, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  }
+  return 0;
+}
+
+int svof_last_dt(svof_solver_t *s, double *dt) {
+  if (!s || !dt) return fail("null argument");
+  CK(cudaStreamSynchronize(s->stream));
+  *dt = s->h_dt[0];
+  return 0;
+}
+
+int svof_integrate(svof_solver_t *s, double *dt) {
+  double d = 0.;
+  if (svof_run(s, 1, &d)) return 1;
+  if (dt) *dt = d;
+  return 0;
+}
+
+// one time step launched kernel by kernel (no graph) with CUDA events between
+// the launches; ms[k] and launches[k] accumulate per kernel kind k (see
+// svof_b200.h).  Advances the solution exactly as svof_integrate does.
+int svof_profile_step(svof_solver_t *s, double *ms, int *launches, int nkinds) {
+  if (!s || !ms || !launches || nkinds < SVOF_NKINDS) return fail("svof_profile_step: bad arguments");
+  for (int k = 0; k < nkinds; k++) {
+    ms[k] = 0.;
+    launches[k] = 0;
+  }
+  std::vector<cudaEvent_t> ev;
+  std::vector<int> kind;
+  auto mark = [&](int k) -> int {
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    CK(cudaEventRecord(e, s->stream));
+    ev.push_back(e);
+    kind.push_back(k);
+    return 0;
+  };
+  int rc = mark(-1);
+  rc = rc || launch_dt(s) || mark(SVOF_K_DT);
+  for (int rk = 0; rk < 3 && !rc; rk++) {
+    rc = rc || launch_geom(s) || mark(SVOF_K_GEOM);
+    rc = rc || launch_force(s) || mark(SVOF_K_FORCE);
+    rc = rc || launch_vof(s, rk) || mark(SVOF_K_VOF);
+    rc = rc || launch_predict(s, rk) || mark(SVOF_K_PREDICT);
+    if (!rc) {
+      const double gam = RK_A[rk] + RK_B[rk];
+      const Grid2 g = s->grid();
+      if (s->uniform) {
+        const int nthr = std::min(256, std::max(32, s->nx / 2));
+        const size_t smem = sizeof(double) * 2 * s->nx;
+        k_dct_fwd<<<s->ny, nthr, smem, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->spec.p, s->twf.p,
+                                                    s->cs.p, s->d_dt, gam, s->log2fft, g);
+        rc = rc || mark(SVOF_K_POISSON_FWD);
+        k_dct_ysolve<<<(s->nx + 127) / 128, 128, 0, s->stream>>>(s->spec.p, s->vt.p, s->q1t.p, s->ck.p,
+                                                                 s->den.p, 1. / s->dy / s->dy, s->nx, s->ny);
+        rc = rc || mark(SVOF_K_POISSON_SOLVE);
+        k_dct_inv<<<s->ny, nthr, smem, s->stream>>>(s->spec.p, s->psi.p, s->twb.p, s->cs.p, s->log2fft, g);
+        rc = rc || mark(SVOF_K_POISSON_INV);
+      } else {
+        const int cols = s->dft_cols;
+        const int blocks = (s->nx + cols - 1) / cols;
+        const size_t smem = sizeof(double) * 2 * s->ny * cols;
+        const int nky = s->ny / 2 + 1;
+        k_dft_fwd<<<blocks, 256, smem, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->spec.p, s->twf.p,
+                                                    s->d_dt, gam, s->log2fft, cols, g);
+        rc = rc || mark(SVOF_K_POISSON_FWD);
+        k_dft_xsolve<<<(nky + 127) / 128, 128, 0, s->stream>>>(s->spec.p, s->vt.p, s->pl.p, s->pu.p,
+                                                                s->evals.p, s->nx, nky);
+        rc = rc || mark(SVOF_K_POISSON_SOLVE);
+        k_dft_inv<<<blocks, 256, smem, s->stream>>>(s->spec.p, s->psi.p, s->twb.p, s->log2fft, cols, g);
+        rc = rc || mark(SVOF_K_POISSON_INV);
+      }
+      rc = rc || (cudaSuccess != cudaGetLastError());
+    }
+    rc = rc || launch_project(s, rk, 1, 1) || mark(SVOF_K_PROJECT);
+  }
+  cudaError_t e = cudaStreamSynchronize(s->stream);
+  if (!rc && cudaSuccess == e) {
+    for (size_t q = 1; q < ev.size(); q++) {
+      float t = 0.f;
+      cudaEventElapsedTime(&t, ev[q - 1], ev[q]);
+      ms[kind[q]] += t;
+      launches[kind[q]] += (SVOF_K_DT == kind[q]) ? 2 : 1;
+    }
+  }
+  for (cudaEvent_t x : ev) cudaEventDestroy(x);
+  if (rc) return 1;
+  if (cudaSuccess != e) return fail("svof_profile_step: %s", cudaGetErrorString(e));
+  return 0;
+}
+
+int svof_diagnostics(svof_solver_t *s, double *divmax, double *vofmin, double *vofmax, double *vofmean) {
+  if (!s) return fail("null argument");
+  k_diag<<<1, 1024, 0, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->vof[s->cur_v].p, s->diag.p,
+                                    s->grid());
+  CK_LAUNCH();
+  double h[5];
+  CK(cudaMemcpyAsync(h, s->diag.p, sizeof(h), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  if (divmax) *divmax = h[0];
+  if (vofmin) *vofmin = h[1];
+  if (vofmax) *vofmax = h[2];
+  if (vofmean) *vofmean = h[3] / h[4];
+  return 0;
+}
+
+int svof_synchronize(svof_solver_t *s) {
+  if (!s) return fail("null argument");
+  CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+int svof_stream(svof_solver_t *s, void **stream) {
+  if (!s || !stream) return fail("null argument");
+  *stream = (void *)s->stream;
+  return 0;
+}
+
+}  // extern "C"

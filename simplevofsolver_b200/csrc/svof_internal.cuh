@@ -1,0 +1,117 @@
+// svof_internal.cuh -- shared device helpers and kernel declarations of the
+// FP64 2D path.  All kernels of this path are compiled with -fmad=false so
+// that every multiply and add rounds separately, as the reference's C code
+// does on x86-64; together with the reference's operation order this makes
+// the device arithmetic reproduce the reference except where it calls libm
+// exp/log (THINC intercept and indicator), whose CUDA versions may differ in
+// the last bit.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+
+namespace svof {
+
+constexpr double kDblEpsilon = 2.220446049250313080847e-16;  // DBL_EPSILON
+
+// reference include/array_macros/**: index maps of the halo'd arrays
+struct Grid2 {
+  int nx, ny;
+  double dy;
+  const double *dxf;   // [nx]   DXF(i) = dxf[i-1]
+  const double *dxc;   // [nx+1] DXC(i) = dxc[i-1]
+};
+
+__host__ __device__ __forceinline__ long ix_ux(int nx, int i, int j) { return (long)(i - 1) + (long)(nx + 1) * j; }
+__host__ __device__ __forceinline__ long ix_cc(int nx, int i, int j) { return (long)i + (long)(nx + 2) * j; }
+__host__ __device__ __forceinline__ long ix_vof(int nx, int i, int j) { return (long)i + (long)(nx + 2) * (j + 1); }
+__host__ __device__ __forceinline__ long ix_nrm(int nx, int i, int j) { return 3L * ((long)(i - 1) + (long)nx * j); }
+__host__ __device__ __forceinline__ long ix_srcx(int nx, int i, int j) { return (long)(i - 2) + (long)(nx - 1) * (j - 1); }
+__host__ __device__ __forceinline__ long ix_src(int nx, int i, int j) { return (long)(i - 1) + (long)nx * (j - 1); }
+
+// Runge-Kutta coefficients of one substep (src/runge_kutta.c:8-15)
+struct RK {
+  double a, b, g;
+};
+
+// boundary kinds of the halo / wall update
+enum BcKind { BC_ZERO_UX = 0, BC_DIRICHLET = 1, BC_NEUMANN = 2, BC_VOF = 3 };
+
+// ---- kernels (definitions in k_*.cu) ----
+// periodic y halo then x wall values of one field (src/halo.c:18-76 and
+// src/fluid/boundary/*.c, src/interface/boundary.c)
+__global__ void k_halo_bc(double *a, int width, int nh, int ny, int kind, double lo, double hi);
+
+// interface geometry: corner normals in shared memory, cell normal +
+// intercept, curvature (src/interface/curvature_tensor.c:14-186)
+__global__ void k_geom(const double *__restrict__ vof, double *__restrict__ normal,
+                       double *__restrict__ curv, Grid2 g);
+// CSF force (src/interface/force.c:11-76)
+__global__ void k_force(const double *__restrict__ vof, const double *__restrict__ curv,
+                        double *__restrict__ ifrcx, double *__restrict__ ifrcy, double tension, Grid2 g);
+// THINC fluxes, flux divergence and RK update of vof
+// (src/interface/update/*.c, src/interface/boundary.c)
+__global__ void k_vof_advect(const double *__restrict__ vof, double *__restrict__ vof_new,
+                             const double *__restrict__ ux, const double *__restrict__ uy,
+                             const double *__restrict__ normal, double *__restrict__ src_a,
+                             const double *__restrict__ src_b, const double *__restrict__ dtp,
+                             RK rk, int use_b, Grid2 g);
+// fused momentum / scalar right-hand sides, increments, implicit-x Thomas
+// sweeps and field update (src/fluid/predict/*.c, src/tdm.c:17-50)
+struct PredictArgs {
+  const double *ux, *uy, *p, *t, *ifrcx, *ifrcy;
+  double *ux_new, *uy_new, *t_new;
+  double *sux_a, *suy_a, *st_a;
+  const double *sux_b, *suy_b, *st_b;
+  const double *lap_ux, *lap_uy, *lap_t;  // 3 per row
+  const double *dtp;
+  double m_dif, t_dif;
+  double lapy0, lapy1, lapy2;
+  RK rk;
+  int use_b;
+  int add_buoyancy;
+  double uy_xm, uy_xp, t_xm, t_xp;
+  int rows_per_block;
+  Grid2 g;
+};
+__global__ void k_predict(PredictArgs a);
+size_t predict_smem_bytes(int nx, int rows_per_block);
+
+// Poisson, DCT path (src/fluid/compute_potential/dct.c)
+__global__ void k_dct_fwd(const double *__restrict__ ux, const double *__restrict__ uy,
+                          double *__restrict__ spec, const double *__restrict__ tw,
+                          const double *__restrict__ cs, const double *__restrict__ dtp,
+                          double gam, int log2n, Grid2 g);
+__global__ void k_dct_ysolve(double *__restrict__ spec, const double *__restrict__ vt,
+                             const double *__restrict__ q1t, const double *__restrict__ ck,
+                             const double *__restrict__ den, double lap, int nx, int ny);
+__global__ void k_dct_inv(const double *__restrict__ spec, double *__restrict__ psi,
+                          const double *__restrict__ tw, const double *__restrict__ cs,
+                          int log2n, Grid2 g);
+// Poisson, DFT path (src/fluid/compute_potential/dft.c)
+__global__ void k_dft_fwd(const double *__restrict__ ux, const double *__restrict__ uy,
+                          double *__restrict__ spec, const double *__restrict__ tw,
+                          const double *__restrict__ dtp, double gam, int log2n, int cols, Grid2 g);
+__global__ void k_dft_xsolve(double *__restrict__ spec, const double *__restrict__ vt,
+                             const double *__restrict__ pl, const double *__restrict__ pu,
+                             const double *__restrict__ evals, int nx, int nky);
+__global__ void k_dft_inv(const double *__restrict__ spec, double *__restrict__ psi,
+                          const double *__restrict__ tw, int log2n, int cols, Grid2 g);
+
+// projection and pressure update, in place (src/fluid/correct_velocity/*.c,
+// src/fluid/update_pressure.c); do_vel / do_p select the two halves
+__global__ void k_project(double *__restrict__ ux, double *__restrict__ uy, double *__restrict__ p,
+                          const double *__restrict__ psi, const double *__restrict__ dtp, double gam,
+                          double m_dif, double uy_xm, double uy_xp, int do_vel, int do_p, Grid2 g);
+
+// time step (src/fluid/decide_dt.c)
+__global__ void k_cfl(const double *__restrict__ ux, const double *__restrict__ uy,
+                      unsigned long long *__restrict__ minbits, Grid2 g);
+__global__ void k_dt_final(unsigned long long *minbits, double *dt, double coef_adv, double dif_m_y,
+                           double dif_t_y);
+// diagnostics (src/logging/divergence.c, src/logging/interface.c)
+__global__ void k_diag(const double *__restrict__ ux, const double *__restrict__ uy,
+                       const double *__restrict__ vof, double *__restrict__ out, Grid2 g);
+
+}  // namespace svof
