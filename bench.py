@@ -56,7 +56,7 @@ ALG_WORDS = {
     "poisson_inv": 2.0,        # R spectrum; W psi
     "project": 7.0,            # R psi ux uy p; W ux uy p
 }
-KERNELS_PER_STEP = 2 + 3 * 8
+KERNELS_PER_STEP = 2 + 3 * 9  # dt (2), then per substep: coef, geom, force, vof, predict, 3 Poisson, project
 
 WORKLOADS = {
     # the reference's runnable configuration: one elliptical droplet,

@@ -97,42 +97,62 @@ __global__ void k_dct_fwd(const double *__restrict__ ux, const double *__restric
 }
 
 // periodic tri-diagonal solve along y per wavenumber k (src/tdm.c:78-99 with
-// gtsv :17-50); vt, q1t ([j][k]) and den[k] are the k-dependent but
-// time-independent quantities of the reference's per-call recomputation
+// gtsv :17-50).  The k-dependent, time-independent quantities the reference
+// recomputes on every call are tables: vt[j][k] (gtsv's v), rvt[j][k]
+// (gtsv's val = 1 / (c - l v[j-1]), j = 1 .. n-3), lastf[k] (1 / val of the
+// last row, 0 where the reference zeroes that row), q1t[j][k] and den[k]
+// (Sherman-Morrison).  A block owns kt consecutive wavenumbers, one line per
+// thread, staged in shared memory ([j][t], coalesced loads and stores).
 __global__ void k_dct_ysolve(double *__restrict__ spec, const double *__restrict__ vt,
-                             const double *__restrict__ q1t, const double *__restrict__ ck,
+                             const double *__restrict__ rvt, const double *__restrict__ q1t,
+                             const double *__restrict__ ck, const double *__restrict__ lastf,
                              const double *__restrict__ den, double lap, int nx, int ny) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= nx) return;
+  extern __shared__ double sq[];  // [ny][kt]
+  const int kt = blockDim.x;
+  const int t = threadIdx.x;
+  const int k0 = blockIdx.x * kt;
   const int n = ny;
-  const double l = lap, u = lap, c = ck[k];
-#define Q(jj) spec[(size_t)(jj) * nx + k]
-#define V(jj) vt[(size_t)(jj) * nx + k]
-  // gtsv of size n-1 on rows 0 .. n-2
-  double qprev = Q(0) / c;
-  Q(0) = qprev;
-  for (int i = 1; i < n - 2; i++) {
-    const double val = 1. / (c - l * V(i - 1));
-    qprev = val * (Q(i) - l * qprev);
-    Q(i) = qprev;
-  }
-  {
-    const double val = c - l * V(n - 3);
-    Q(n - 2) = fabs(val) > kDblEpsilon ? 1. / val * (Q(n - 2) - l * qprev) : 0.;
-  }
-  double qn = Q(n - 2);
-  for (int i = n - 3; i >= 0; i--) {
-    qn = Q(i) - V(i) * qn;
-    Q(i) = qn;
-  }
-  // Sherman-Morrison correction
-  const double num = Q(n - 1) - u * qn - l * Q(n - 2);
-  const double d = den[k];
-  const double qlast = fabs(d) < kDblEpsilon ? 0. : num / d;
-  Q(n - 1) = qlast;
-  for (int i = 0; i < n - 1; i++) Q(i) = Q(i) + qlast * q1t[(size_t)i * nx + k];
+  const int nk = min(kt, nx - k0);
+  for (int j = 0; j < n; j++) sq[j * kt + t] = (t < nk) ? spec[(size_t)j * nx + k0 + t] : 0.;
+  __syncthreads();
+  __shared__ double sl[1024];
+  if (t < nk) {
+    const int k = k0 + t;
+    const double l = lap, u = lap, c = ck[k];
+    double *q = sq + t;
+#define Q(jj) q[(size_t)(jj) * kt]
+    // gtsv of size n-1 on rows 0 .. n-2
+    double qprev = Q(0) / c;
+    Q(0) = qprev;
+    for (int i = 1; i < n - 2; i++) {
+      qprev = rvt[(size_t)i * nx + k] * (Q(i) - l * qprev);
+      Q(i) = qprev;
+    }
+    {
+      const double lf = lastf[k];
+      Q(n - 2) = (0. != lf) ? lf * (Q(n - 2) - l * qprev) : 0.;
+    }
+    double qn = Q(n - 2);
+    for (int i = n - 3; i >= 0; i--) {
+      qn = Q(i) - vt[(size_t)i * nx + k] * qn;
+      Q(i) = qn;
+    }
+    // Sherman-Morrison correction
+    const double num = Q(n - 1) - u * qn - l * Q(n - 2);
+    const double d = den[k];
+    const double qlast = fabs(d) < kDblEpsilon ? 0. : num / d;
+    Q(n - 1) = qlast;
+    sl[t] = qlast;
 #undef Q
-#undef V
+  }
+  __syncthreads();
+  for (int j = 0; j < n; j++) {
+    if (t < nk) {
+      const int k = k0 + t;
+      const double v = (j < n - 1) ? sq[j * kt + t] + sl[t] * q1t[(size_t)j * nx + k] : sq[j * kt + t];
+      spec[(size_t)j * nx + k] = v;
+    }
+  }
 }
 
 // one block per row j: REDFT01 then extract_output + fluid_update_boundaries_psi
@@ -213,10 +233,11 @@ __global__ void k_dft_fwd(const double *__restrict__ ux, const double *__restric
 }
 
 // complex Neumann Thomas along x per ky (dft.c:364-395); spec layout [i][ky],
-// vt[i][ky] holds the reference's v for each ky
+// vt[i][ky] and rvt[i][ky] hold the reference's v and val for each ky
 __global__ void k_dft_xsolve(double *__restrict__ spec, const double *__restrict__ vt,
-                             const double *__restrict__ pl, const double *__restrict__ pu,
-                             const double *__restrict__ evals, int nx, int nky) {
+                             const double *__restrict__ rvt, const double *__restrict__ pl,
+                             const double *__restrict__ pu, const double *__restrict__ evals, int nx,
+                             int nky) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nky) return;
   const int n = nx;
@@ -232,8 +253,7 @@ __global__ void k_dft_xsolve(double *__restrict__ spec, const double *__restrict
   QI(0) = pi;
   for (int i = 1; i < n - 1; i++) {
     const double l = pl[i];
-    const double c = -l - pu[i] + ev;
-    const double val = 1. / (c - l * V(i - 1));
+    const double val = rvt[(size_t)i * nky + k];  // 1 / (c_i - l_i v_{i-1})
     pr = val * (QR(i) - l * pr);
     pi = val * (QI(i) - l * pi);
     QR(i) = pr;

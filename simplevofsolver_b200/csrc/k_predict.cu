@@ -16,7 +16,51 @@
 namespace svof {
 
 size_t predict_smem_bytes(int nx, int R) {
-  return sizeof(double) * ((size_t)3 * R * (nx + 1) + (size_t)3 * (nx + 1));
+  return sizeof(double) * ((size_t)3 * R * (nx + 1));
+}
+
+// Thomas coefficients of the three implicit-x systems of one substep
+// (solve_in_x of src/fluid/predict/{ux,uy,t}.c and gtsv, src/tdm.c:17-50):
+// they depend on dt and the substep only, so one thread per field computes
+// them once and every line solve reads them.  Layout per field f at
+// coef + 3 f nx:  L[i] = tdm_l[i];  R[0] = tdm_c[0], R[i] = 1 / (c_i - l_i
+// v_{i-1}) for 0 < i < n-1, R[n-1] = 1 / (c - l v) of the last row or 0 when
+// the reference zeroes that row;  V[i] = v_i.
+__global__ void k_tdm_coef(const double *__restrict__ lap_ux, const double *__restrict__ lap_uy,
+                           const double *__restrict__ lap_t, const double *__restrict__ dtp, double gam,
+                           double m_dif, double t_dif, int nx, double *__restrict__ coef) {
+  const int f = threadIdx.x;
+  if (f >= 3) return;
+  const double *lap = (0 == f) ? lap_ux : (1 == f ? lap_uy : lap_t);
+  const double dif = (2 == f) ? t_dif : m_dif;
+  const int n = (0 == f) ? nx - 1 : nx;
+  double *L = coef + (size_t)(3 * f + 0) * nx;
+  double *R = coef + (size_t)(3 * f + 1) * nx;
+  double *V = coef + (size_t)(3 * f + 2) * nx;
+  const double dt = *dtp;
+  const double pf = 0.5 * gam * dt * dif;  // ux.c:330-332
+  const double c0 = 1. - pf * lap[1];
+  double v = (-pf * lap[2]) / c0;
+  L[0] = -pf * lap[0];
+  R[0] = c0;
+  V[0] = v;
+  for (int i = 1; i < n - 1; i++) {
+    const double l = -pf * lap[3 * i + 0];
+    const double c = 1. - pf * lap[3 * i + 1];
+    const double u = -pf * lap[3 * i + 2];
+    const double val = 1. / (c - l * v);
+    v = val * (u);
+    L[i] = l;
+    R[i] = val;
+    V[i] = v;
+  }
+  {
+    const double l = -pf * lap[3 * (n - 1) + 0];
+    const double c = 1. - pf * lap[3 * (n - 1) + 1];
+    const double val = c - l * v;
+    L[n - 1] = l;
+    R[n - 1] = fabs(val) > kDblEpsilon ? 1. / val : 0.;
+  }
 }
 
 __global__ void __launch_bounds__(256) k_predict(PredictArgs a) {
@@ -25,7 +69,6 @@ __global__ void __launch_bounds__(256) k_predict(PredictArgs a) {
   const int nx = g.nx, ny = g.ny, R = a.rows_per_block;
   const int ld = nx + 1;
   double *sd = sm;                  // [3][R][ld] increments
-  double *sv = sm + 3 * R * ld;     // [3][ld] Thomas v (shared by all lines of a field)
   const int j0 = 1 + blockIdx.x * R;
   const int nrows = min(R, ny - j0 + 1);
   const double dt = *a.dtp;
@@ -145,46 +188,32 @@ __global__ void __launch_bounds__(256) k_predict(PredictArgs a) {
   }
   __syncthreads();
 
-  // ---------------- phase 2: Thomas sweeps (gtsv, src/tdm.c:17-50)
+  // ---------------- phase 2: Thomas sweeps (gtsv, src/tdm.c:17-50) with the
+  // coefficients of k_tdm_coef
   const bool line = tid < 3 * nrows;
-  const int f = line ? tid / nrows : 0;
-  const int jj = line ? tid % nrows : 0;
-  const int n = (0 == f) ? nx - 1 : nx;
-  double *q = sd + (f * R + jj) * ld;
-  double *v = sv + f * ld;
   if (line) {
-    const double *lap = (0 == f) ? a.lap_ux : (1 == f ? a.lap_uy : a.lap_t);
-    const double dif = (2 == f) ? a.t_dif : a.m_dif;
-    // prefactor = gamma dt diffusivity / 2 (ux.c:330-332), tdm_[lcu] (ux.c:251-271)
-    const double pf = 0.5 * a.rk.g * dt * dif;
-    const double c0 = 1. - pf * lap[1];
-    const double u0 = -pf * lap[2];
-    double vprev = u0 / c0;
-    double qprev = q[0] / c0;
+    const int f = tid / nrows;
+    const int jj = tid % nrows;
+    const int n = (0 == f) ? nx - 1 : nx;
+    double *q = sd + (f * R + jj) * ld;
+    const double *L = a.coef + (size_t)(3 * f + 0) * nx;
+    const double *Rv = a.coef + (size_t)(3 * f + 1) * nx;
+    const double *V = a.coef + (size_t)(3 * f + 2) * nx;
+    double qprev = q[0] / Rv[0];
     q[0] = qprev;
-    if (0 == jj) v[0] = vprev;
+#pragma unroll 4
     for (int i = 1; i < n - 1; i++) {
-      const double l = -pf * lap[3 * i + 0];
-      const double c = 1. - pf * lap[3 * i + 1];
-      const double u = -pf * lap[3 * i + 2];
-      const double val = 1. / (c - l * vprev);
-      vprev = val * (u);
-      qprev = val * (q[i] - l * qprev);
+      qprev = Rv[i] * (q[i] - L[i] * qprev);
       q[i] = qprev;
-      if (0 == jj) v[i] = vprev;
     }
     {
-      const double l = -pf * lap[3 * (n - 1) + 0];
-      const double c = 1. - pf * lap[3 * (n - 1) + 1];
-      const double val = c - l * vprev;
-      q[n - 1] = fabs(val) > kDblEpsilon ? 1. / val * (q[n - 1] - l * qprev) : 0.;
+      const double rl = Rv[n - 1];
+      q[n - 1] = (0. != rl) ? rl * (q[n - 1] - L[n - 1] * qprev) : 0.;
     }
-  }
-  __syncthreads();
-  if (line) {
     double qn = q[n - 1];
+#pragma unroll 4
     for (int i = n - 2; i >= 0; i--) {
-      qn = q[i] - v[i] * qn;
+      qn = q[i] - V[i] * qn;
       q[i] = qn;
     }
   }

@@ -102,7 +102,14 @@ struct svof_solver {
   double lapy[3] = {0., 0., 0.};
   double dif_m_y = 0., dif_t_y = 0.;
   // Poisson
-  DevBuf spec, twf, twb, cs, vt, q1t, ck, den, pl, pu, evals;
+  DevBuf spec, twf, twb, cs, vt, rvt, q1t, ck, lastf, den, pl, pu, evals;
+  int ysolve_kt = 32;       // wavenumber lines per block of the DCT y solve
+  // predictor Thomas coefficients of the current substep (k_tdm_coef)
+  DevBuf coef;
+  // side stream of the step graph: the coefficient kernel runs beside the
+  // interface kernels
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork[3] = {nullptr, nullptr, nullptr}, ev_join[3] = {nullptr, nullptr, nullptr};
   // predict launch shape
   int pred_rows = 1;
   size_t pred_smem = 0;
@@ -197,7 +204,17 @@ int launch_vof(svof_solver *s, int rk) {
   return 0;
 }
 
-int launch_predict(svof_solver *s, int rk) {
+int launch_coef(svof_solver *s, int rk, cudaStream_t st) {
+  k_tdm_coef<<<1, 32, 0, st>>>(s->lap_ux.p, s->lap_uy.p, s->lap_t.p, s->d_dt, RK_A[rk] + RK_B[rk], s->prm.m_dif,
+                               s->prm.t_dif, s->nx, s->coef.p);
+  CK_LAUNCH();
+  return 0;
+}
+
+// with_coef: launch k_tdm_coef first on the same stream (the step graph
+// launches it on the side stream instead)
+int launch_predict(svof_solver *s, int rk, bool with_coef = true) {
+  if (with_coef && launch_coef(s, rk, s->stream)) return 1;
   if (0 != rk) s->sa_f ^= 1;  // reset_srcs, src/fluid/predict/main.c:9-29
   PredictArgs a{};
   const int cu = s->cur_u;
@@ -219,6 +236,7 @@ int launch_predict(svof_solver *s, int rk) {
   a.lap_ux = s->lap_ux.p;
   a.lap_uy = s->lap_uy.p;
   a.lap_t = s->lap_t.p;
+  a.coef = s->coef.p;
   a.dtp = s->d_dt;
   a.m_dif = s->prm.m_dif;
   a.t_dif = s->prm.t_dif;
@@ -253,8 +271,9 @@ int launch_potential(svof_solver *s, int rk, int want_dct) {
     k_dct_fwd<<<s->ny, nthr, smem, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->spec.p, s->twf.p,
                                                 s->cs.p, s->d_dt, gam, s->log2fft, g);
     CK_LAUNCH();
-    k_dct_ysolve<<<(s->nx + 127) / 128, 128, 0, s->stream>>>(s->spec.p, s->vt.p, s->q1t.p, s->ck.p, s->den.p,
-                                                             1. / s->dy / s->dy, s->nx, s->ny);
+    const int kt = s->ysolve_kt;
+    k_dct_ysolve<<<(s->nx + kt - 1) / kt, kt, sizeof(double) * kt * s->ny, s->stream>>>(
+        s->spec.p, s->vt.p, s->rvt.p, s->q1t.p, s->ck.p, s->lastf.p, s->den.p, 1. / s->dy / s->dy, s->nx, s->ny);
     CK_LAUNCH();
     k_dct_inv<<<s->ny, nthr, smem, s->stream>>>(s->spec.p, s->psi.p, s->twb.p, s->cs.p, s->log2fft, g);
     CK_LAUNCH();
@@ -266,8 +285,8 @@ int launch_potential(svof_solver *s, int rk, int want_dct) {
     k_dft_fwd<<<blocks, 256, smem, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->spec.p, s->twf.p,
                                                 s->d_dt, gam, s->log2fft, cols, g);
     CK_LAUNCH();
-    k_dft_xsolve<<<(nky + 127) / 128, 128, 0, s->stream>>>(s->spec.p, s->vt.p, s->pl.p, s->pu.p, s->evals.p,
-                                                            s->nx, nky);
+    k_dft_xsolve<<<(nky + 127) / 128, 128, 0, s->stream>>>(s->spec.p, s->vt.p, s->rvt.p, s->pl.p, s->pu.p,
+                                                            s->evals.p, s->nx, nky);
     CK_LAUNCH();
     k_dft_inv<<<blocks, 256, smem, s->stream>>>(s->spec.p, s->psi.p, s->twb.p, s->log2fft, cols, g);
     CK_LAUNCH();
@@ -288,10 +307,17 @@ int launch_project(svof_solver *s, int rk, int do_vel, int do_p) {
 int launch_step(svof_solver *s) {
   if (launch_dt(s)) return 1;
   for (int rk = 0; rk < 3; rk++) {
+    // the predictor coefficients need only dt: compute them beside the
+    // interface kernels
+    CK(cudaEventRecord(s->ev_fork[rk], s->stream));
+    CK(cudaStreamWaitEvent(s->side, s->ev_fork[rk], 0));
+    if (launch_coef(s, rk, s->side)) return 1;
+    CK(cudaEventRecord(s->ev_join[rk], s->side));
     if (launch_geom(s)) return 1;
     if (launch_force(s)) return 1;
     if (launch_vof(s, rk)) return 1;
-    if (launch_predict(s, rk)) return 1;
+    CK(cudaStreamWaitEvent(s->stream, s->ev_join[rk], 0));
+    if (launch_predict(s, rk, false)) return 1;
     if (launch_potential(s, rk, s->uniform)) return 1;
     if (launch_project(s, rk, 1, 1)) return 1;
   }
@@ -435,7 +461,8 @@ int build_tables(svof_solver *s, const double *xf, const double *xc) {
     const int n = ny;
     const double lap = 1. / s->dy / s->dy;
     std::vector<double> l(n, lap), u(n, lap), c(n), v(n), q1(n);
-    std::vector<double> vt((size_t)n * nx, 0.), q1t((size_t)n * nx, 0.), ck(nx), den(nx);
+    std::vector<double> vt((size_t)n * nx, 0.), rvt((size_t)n * nx, 0.), q1t((size_t)n * nx, 0.), ck(nx),
+        den(nx), lastf(nx);
     const double signal_length = 2. * nx;
     const double gridsize = s->prm.lx / nx;
     for (size_t k = 0; k < (size_t)nx; k++) {
@@ -447,15 +474,23 @@ int build_tables(svof_solver *s, const double *xf, const double *xc) {
         vt[(size_t)i * nx + k] = v[i];
         q1t[(size_t)i * nx + k] = q1[i];
       }
+      // gtsv's val of the size-(n-1) system, rows 1 .. n-3, and its last row
+      for (int i = 1; i < n - 2; i++) rvt[(size_t)i * nx + k] = 1. / (c[i] - l[i] * v[i - 1]);
+      {
+        const double val = c[n - 2] - l[n - 2] * v[n - 3];
+        lastf[k] = std::fabs(val) > kDblEpsilon ? 1. / val : 0.;
+      }
       ck[k] = c[0];
       den[k] = c[n - 1] + u[n - 1] * q1[0] + l[n - 1] * q1[n - 2];
     }
-    if (upload(s->vt, vt) || upload(s->q1t, q1t) || upload(s->ck, ck) || upload(s->den, den)) return 1;
+    if (upload(s->vt, vt) || upload(s->rvt, rvt) || upload(s->q1t, q1t) || upload(s->ck, ck) ||
+        upload(s->den, den) || upload(s->lastf, lastf))
+      return 1;
     if (dalloc(s->spec, (size_t)nx * ny)) return 1;
   } else {
     // src/fluid/compute_potential/dft.c:142-198 and :263-291
     const int n = nx, nky = ny / 2 + 1;
-    std::vector<double> pl(n), pu(n), ev(nky), c(n), v(n), vt((size_t)n * nky, 0.);
+    std::vector<double> pl(n), pu(n), ev(nky), c(n), v(n), vt((size_t)n * nky, 0.), rvt((size_t)n * nky, 0.);
     for (int i = 1; i <= n; i++) {
       pl[i - 1] = 1. / DXC(i) / DXF(i);
       pu[i - 1] = 1. / DXC(i + 1) / DXF(i);
@@ -473,10 +508,13 @@ int build_tables(svof_solver *s, const double *xf, const double *xc) {
       for (int i = 1; i < n - 1; i++) {
         const double val = 1. / (c[i] - pl[i] * v[i - 1]);
         v[i] = val * (pu[i]);
+        rvt[(size_t)i * nky + k] = val;
       }
       for (int i = 0; i < n - 1; i++) vt[(size_t)i * nky + k] = v[i];
     }
-    if (upload(s->pl, pl) || upload(s->pu, pu) || upload(s->evals, ev) || upload(s->vt, vt)) return 1;
+    if (upload(s->pl, pl) || upload(s->pu, pu) || upload(s->evals, ev) || upload(s->vt, vt) ||
+        upload(s->rvt, rvt))
+      return 1;
     if (dalloc(s->spec, 2 * (size_t)nx * nky)) return 1;
   }
   return 0;
@@ -523,6 +561,23 @@ int svof_create(const svof_params_t *prm, const double *xf, const double *xc, sv
       dalloc(s->diag, 8))
     return bail();
   if (build_tables(s, xf, xc)) return bail();
+  if (dalloc(s->coef, 9 * (size_t)nx)) return bail();
+  if (cudaSuccess != cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking)) return fail("stream"), bail();
+  for (int k = 0; k < 3; k++) {
+    if (cudaSuccess != cudaEventCreateWithFlags(&s->ev_fork[k], cudaEventDisableTiming) ||
+        cudaSuccess != cudaEventCreateWithFlags(&s->ev_join[k], cudaEventDisableTiming))
+      return fail("event"), bail();
+  }
+  if (s->uniform) {
+    int kt = 32;
+    while (kt > 1 && sizeof(double) * (size_t)kt * ny > 160 * 1024) kt >>= 1;
+    s->ysolve_kt = kt;
+    const size_t sm = sizeof(double) * (size_t)kt * ny;
+    if (sm > 227 * 1024) return fail("svof_create: ny = %d too large for the y line solver", ny), bail();
+    if (sm > 48 * 1024 &&
+        cudaSuccess != cudaFuncSetAttribute(k_dct_ysolve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))
+      return fail("cudaFuncSetAttribute(k_dct_ysolve)"), bail();
+  }
   // predict launch shape: R rows per block within 200 KB of shared memory
   {
     const long per_row = 3L * (nx + 1);
@@ -579,11 +634,17 @@ int svof_destroy(svof_solver_t *s) {
   }
   DevBuf *bufs[] = {&s->p, &s->psi, &s->curv, &s->normal, &s->ifrcx, &s->ifrcy, &s->dxf, &s->dxc,
                     &s->lap_ux, &s->lap_uy, &s->lap_t, &s->spec, &s->twf, &s->twb, &s->cs, &s->vt,
-                    &s->q1t, &s->ck, &s->den, &s->pl, &s->pu, &s->evals, &s->diag};
+                    &s->rvt, &s->q1t, &s->ck, &s->lastf, &s->den, &s->pl, &s->pu, &s->evals, &s->diag,
+                    &s->coef};
   for (DevBuf *b : bufs) dfree(*b);
   if (s->d_dt) cudaFree(s->d_dt);
   if (s->d_minbits) cudaFree(s->d_minbits);
   if (s->h_dt) cudaFreeHost(s->h_dt);
+  for (int k = 0; k < 3; k++) {
+    if (s->ev_fork[k]) cudaEventDestroy(s->ev_fork[k]);
+    if (s->ev_join[k]) cudaEventDestroy(s->ev_join[k]);
+  }
+  if (s->side) cudaStreamDestroy(s->side);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
   return 0;
@@ -812,8 +873,10 @@ int svof_profile_step(svof_solver_t *s, double *ms, int *launches, int nkinds) {
         k_dct_fwd<<<s->ny, nthr, smem, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->spec.p, s->twf.p,
                                                     s->cs.p, s->d_dt, gam, s->log2fft, g);
         rc = rc || mark(SVOF_K_POISSON_FWD);
-        k_dct_ysolve<<<(s->nx + 127) / 128, 128, 0, s->stream>>>(s->spec.p, s->vt.p, s->q1t.p, s->ck.p,
-                                                                 s->den.p, 1. / s->dy / s->dy, s->nx, s->ny);
+        const int kt = s->ysolve_kt;
+        k_dct_ysolve<<<(s->nx + kt - 1) / kt, kt, sizeof(double) * kt * s->ny, s->stream>>>(
+            s->spec.p, s->vt.p, s->rvt.p, s->q1t.p, s->ck.p, s->lastf.p, s->den.p, 1. / s->dy / s->dy, s->nx,
+            s->ny);
         rc = rc || mark(SVOF_K_POISSON_SOLVE);
         k_dct_inv<<<s->ny, nthr, smem, s->stream>>>(s->spec.p, s->psi.p, s->twb.p, s->cs.p, s->log2fft, g);
         rc = rc || mark(SVOF_K_POISSON_INV);
@@ -825,7 +888,7 @@ int svof_profile_step(svof_solver_t *s, double *ms, int *launches, int nkinds) {
         k_dft_fwd<<<blocks, 256, smem, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->spec.p, s->twf.p,
                                                     s->d_dt, gam, s->log2fft, cols, g);
         rc = rc || mark(SVOF_K_POISSON_FWD);
-        k_dft_xsolve<<<(nky + 127) / 128, 128, 0, s->stream>>>(s->spec.p, s->vt.p, s->pl.p, s->pu.p,
+        k_dft_xsolve<<<(nky + 127) / 128, 128, 0, s->stream>>>(s->spec.p, s->vt.p, s->rvt.p, s->pl.p, s->pu.p,
                                                                 s->evals.p, s->nx, nky);
         rc = rc || mark(SVOF_K_POISSON_SOLVE);
         k_dft_inv<<<blocks, 256, smem, s->stream>>>(s->spec.p, s->psi.p, s->twb.p, s->log2fft, cols, g);
@@ -841,7 +904,7 @@ int svof_profile_step(svof_solver_t *s, double *ms, int *launches, int nkinds) {
       float t = 0.f;
       cudaEventElapsedTime(&t, ev[q - 1], ev[q]);
       ms[kind[q]] += t;
-      launches[kind[q]] += (SVOF_K_DT == kind[q]) ? 2 : 1;
+      launches[kind[q]] += (SVOF_K_DT == kind[q] || SVOF_K_PREDICT == kind[q]) ? 2 : 1;
     }
   }
   for (cudaEvent_t x : ev) cudaEventDestroy(x);

@@ -65,6 +65,7 @@ struct PredictArgs {
   double *sux_a, *suy_a, *st_a;
   const double *sux_b, *suy_b, *st_b;
   const double *lap_ux, *lap_uy, *lap_t;  // 3 per row
+  const double *coef;                     // k_tdm_coef output, [3 fields][L, R, V][nx]
   const double *dtp;
   double m_dif, t_dif;
   double lapy0, lapy1, lapy2;
@@ -76,6 +77,9 @@ struct PredictArgs {
   Grid2 g;
 };
 __global__ void k_predict(PredictArgs a);
+__global__ void k_tdm_coef(const double *__restrict__ lap_ux, const double *__restrict__ lap_uy,
+                           const double *__restrict__ lap_t, const double *__restrict__ dtp, double gam,
+                           double m_dif, double t_dif, int nx, double *__restrict__ coef);
 size_t predict_smem_bytes(int nx, int rows_per_block);
 
 // Poisson, DCT path (src/fluid/compute_potential/dct.c)
@@ -84,7 +88,8 @@ __global__ void k_dct_fwd(const double *__restrict__ ux, const double *__restric
                           const double *__restrict__ cs, const double *__restrict__ dtp,
                           double gam, int log2n, Grid2 g);
 __global__ void k_dct_ysolve(double *__restrict__ spec, const double *__restrict__ vt,
-                             const double *__restrict__ q1t, const double *__restrict__ ck,
+                             const double *__restrict__ rvt, const double *__restrict__ q1t,
+                             const double *__restrict__ ck, const double *__restrict__ lastf,
                              const double *__restrict__ den, double lap, int nx, int ny);
 __global__ void k_dct_inv(const double *__restrict__ spec, double *__restrict__ psi,
                           const double *__restrict__ tw, const double *__restrict__ cs,
@@ -94,8 +99,9 @@ __global__ void k_dft_fwd(const double *__restrict__ ux, const double *__restric
                           double *__restrict__ spec, const double *__restrict__ tw,
                           const double *__restrict__ dtp, double gam, int log2n, int cols, Grid2 g);
 __global__ void k_dft_xsolve(double *__restrict__ spec, const double *__restrict__ vt,
-                             const double *__restrict__ pl, const double *__restrict__ pu,
-                             const double *__restrict__ evals, int nx, int nky);
+                             const double *__restrict__ rvt, const double *__restrict__ pl,
+                             const double *__restrict__ pu, const double *__restrict__ evals, int nx,
+                             int nky);
 __global__ void k_dft_inv(const double *__restrict__ spec, double *__restrict__ psi,
                           const double *__restrict__ tw, int log2n, int cols, Grid2 g);
 
