@@ -22,32 +22,40 @@ constexpr double kVofBeta = 1.;
 constexpr double kVofMin = 1.e-8;
 
 // ---------------------------------------------------------------------------
-// halo + wall update of one field; one thread per storage column.  Both halo
-// exchanges copy whole rows (x ghost cells included) before the wall values
-// are assigned, as src/halo.c:51-74 followed by assign_boundary_conditions_in_x.
+// halo + wall update of one field; one thread per storage cell of the grid
+// (columns x blockIdx.y = storage row).  Both halo exchanges copy whole rows,
+// x ghost cells included, before the wall values are assigned (src/halo.c:
+// 51-74 followed by assign_boundary_conditions_in_x): interior columns copy
+// their halo rows from the source rows; a wall cell of a source row first
+// hands its pre-assignment value to the halo row, then takes its wall value.
 __global__ void k_halo_bc(double *a, int width, int nh, int ny, int kind, double lo, double hi) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y;  // storage row, 0 .. ny + 2 nh - 1
   if (c >= width) return;
   const long w = width;
-  for (int h = 0; h < nh; h++) a[w * h + c] = a[w * (ny + h) + c];
-  for (int h = 0; h < nh; h++) a[w * (ny + nh + h) + c] = a[w * (nh + h) + c];
   const bool left = (0 == c), right = (width - 1 == c);
-  if (!left && !right) return;
-  if (BC_VOF == kind) {
-    for (int r = 0; r < ny + 2 * nh; r++) a[w * r + c] = 0.;
+  if (!left && !right) {
+    if (r < nh) a[w * r + c] = a[w * (ny + r) + c];
+    else if (r >= ny + nh) a[w * r + c] = a[w * (r - ny) + c];
     return;
   }
-  for (int r = nh; r < nh + ny; r++) {
-    double v;
-    if (BC_ZERO_UX == kind) {
-      v = 0.;
-    } else if (BC_DIRICHLET == kind) {
-      v = left ? lo : hi;
-    } else {
-      v = left ? a[w * r + 1] : a[w * r + width - 2];
-    }
-    a[w * r + c] = v;
+  if (BC_VOF == kind) {
+    a[w * r + c] = 0.;
+    return;
   }
+  if (r < nh || r >= ny + nh) return;
+  const double old = a[w * r + c];
+  if (r >= ny) a[w * (r - ny) + c] = old;
+  if (r < 2 * nh) a[w * (r + ny) + c] = old;
+  double v;
+  if (BC_ZERO_UX == kind) {
+    v = 0.;
+  } else if (BC_DIRICHLET == kind) {
+    v = left ? lo : hi;
+  } else {
+    v = left ? a[w * r + 1] : a[w * r + width - 2];
+  }
+  a[w * r + c] = v;
 }
 
 // ---------------------------------------------------------------------------

@@ -101,56 +101,72 @@ __global__ void k_dct_fwd(const double *__restrict__ ux, const double *__restric
 // recomputes on every call are tables: vt[j][k] (gtsv's v), rvt[j][k]
 // (gtsv's val = 1 / (c - l v[j-1]), j = 1 .. n-3), lastf[k] (1 / val of the
 // last row, 0 where the reference zeroes that row), q1t[j][k] and den[k]
-// (Sherman-Morrison).  A block owns kt consecutive wavenumbers, one line per
-// thread, staged in shared memory ([j][t], coalesced loads and stores).
+// (Sherman-Morrison).  A block owns kt consecutive wavenumbers; all its
+// threads stage the lines and their tables in shared memory ([j][t],
+// coalesced), then one thread per line runs the recurrences on shared memory
+// only, and all threads apply the Sherman-Morrison correction on the way out.
 __global__ void k_dct_ysolve(double *__restrict__ spec, const double *__restrict__ vt,
                              const double *__restrict__ rvt, const double *__restrict__ q1t,
                              const double *__restrict__ ck, const double *__restrict__ lastf,
-                             const double *__restrict__ den, double lap, int nx, int ny) {
-  extern __shared__ double sq[];  // [ny][kt]
-  const int kt = blockDim.x;
-  const int t = threadIdx.x;
+                             const double *__restrict__ den, double lap, int nx, int ny, int kt) {
+  extern __shared__ double sm[];
+  double *sq = sm;                       // [ny][kt] line data
+  double *sv = sm + (size_t)ny * kt;     // [ny][kt] v
+  double *sr = sm + 2 * (size_t)ny * kt; // [ny][kt] val
+  __shared__ double sl[64];
   const int k0 = blockIdx.x * kt;
   const int n = ny;
   const int nk = min(kt, nx - k0);
-  for (int j = 0; j < n; j++) sq[j * kt + t] = (t < nk) ? spec[(size_t)j * nx + k0 + t] : 0.;
+  for (int w = threadIdx.x; w < n * kt; w += blockDim.x) {
+    const int j = w / kt, t = w - j * kt;
+    const size_t g = (size_t)j * nx + k0 + t;
+    const bool ok = t < nk;
+    sq[w] = ok ? spec[g] : 0.;
+    sv[w] = ok ? vt[g] : 0.;
+    sr[w] = ok ? rvt[g] : 0.;
+  }
   __syncthreads();
-  __shared__ double sl[1024];
+  const int t = threadIdx.x;
   if (t < nk) {
     const int k = k0 + t;
     const double l = lap, u = lap, c = ck[k];
+    const double lf = lastf[k];
+    const double d = den[k];
     double *q = sq + t;
+    const double *v = sv + t, *r = sr + t;
 #define Q(jj) q[(size_t)(jj) * kt]
+#define V(jj) v[(size_t)(jj) * kt]
+#define RV(jj) r[(size_t)(jj) * kt]
     // gtsv of size n-1 on rows 0 .. n-2
     double qprev = Q(0) / c;
     Q(0) = qprev;
+#pragma unroll 8
     for (int i = 1; i < n - 2; i++) {
-      qprev = rvt[(size_t)i * nx + k] * (Q(i) - l * qprev);
+      qprev = RV(i) * (Q(i) - l * qprev);
       Q(i) = qprev;
     }
-    {
-      const double lf = lastf[k];
-      Q(n - 2) = (0. != lf) ? lf * (Q(n - 2) - l * qprev) : 0.;
-    }
+    Q(n - 2) = (0. != lf) ? lf * (Q(n - 2) - l * qprev) : 0.;
     double qn = Q(n - 2);
+#pragma unroll 8
     for (int i = n - 3; i >= 0; i--) {
-      qn = Q(i) - vt[(size_t)i * nx + k] * qn;
+      qn = Q(i) - V(i) * qn;
       Q(i) = qn;
     }
     // Sherman-Morrison correction
     const double num = Q(n - 1) - u * qn - l * Q(n - 2);
-    const double d = den[k];
     const double qlast = fabs(d) < kDblEpsilon ? 0. : num / d;
     Q(n - 1) = qlast;
     sl[t] = qlast;
 #undef Q
+#undef V
+#undef RV
   }
   __syncthreads();
-  for (int j = 0; j < n; j++) {
-    if (t < nk) {
-      const int k = k0 + t;
-      const double v = (j < n - 1) ? sq[j * kt + t] + sl[t] * q1t[(size_t)j * nx + k] : sq[j * kt + t];
-      spec[(size_t)j * nx + k] = v;
+  for (int w = threadIdx.x; w < n * kt; w += blockDim.x) {
+    const int j = w / kt, tt = w - j * kt;
+    if (tt < nk) {
+      const size_t g = (size_t)j * nx + k0 + tt;
+      spec[g] = (j < n - 1) ? sq[w] + sl[tt] * q1t[g] : sq[w];
     }
   }
 }
@@ -233,56 +249,89 @@ __global__ void k_dft_fwd(const double *__restrict__ ux, const double *__restric
 }
 
 // complex Neumann Thomas along x per ky (dft.c:364-395); spec layout [i][ky],
-// vt[i][ky] and rvt[i][ky] hold the reference's v and val for each ky
+// vt[i][ky] and rvt[i][ky] hold the reference's v and val for each ky.  A
+// block owns kt consecutive ky lines: all threads stage them and their tables
+// in shared memory, one thread per line runs the recurrences there.
 __global__ void k_dft_xsolve(double *__restrict__ spec, const double *__restrict__ vt,
                              const double *__restrict__ rvt, const double *__restrict__ pl,
                              const double *__restrict__ pu, const double *__restrict__ evals, int nx,
-                             int nky) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= nky) return;
+                             int nky, int kt) {
+  extern __shared__ double sm[];
+  double *sre = sm;                        // [nx][kt]
+  double *sim = sm + (size_t)nx * kt;      // [nx][kt]
+  double *sv = sm + 2 * (size_t)nx * kt;   // [nx][kt]
+  double *sr = sm + 3 * (size_t)nx * kt;   // [nx][kt]
+  const int k0 = blockIdx.x * kt;
+  const int nk = min(kt, nky - k0);
   const int n = nx;
-  const double ev = evals[k];
-#define QR(ii) spec[2 * ((size_t)(ii) * nky + k)]
-#define QI(ii) spec[2 * ((size_t)(ii) * nky + k) + 1]
-#define V(ii) vt[(size_t)(ii) * nky + k]
-  // tdm_c with the Neumann boundary rows
-  double c0 = -pl[0] - pu[0] + ev;
-  c0 += pl[0];
-  double pr = QR(0) / c0, pi = QI(0) / c0;
-  QR(0) = pr;
-  QI(0) = pi;
-  for (int i = 1; i < n - 1; i++) {
-    const double l = pl[i];
-    const double val = rvt[(size_t)i * nky + k];  // 1 / (c_i - l_i v_{i-1})
-    pr = val * (QR(i) - l * pr);
-    pi = val * (QI(i) - l * pi);
-    QR(i) = pr;
-    QI(i) = pi;
+  for (int w = threadIdx.x; w < n * kt; w += blockDim.x) {
+    const int i = w / kt, t = w - i * kt;
+    const size_t g = (size_t)i * nky + k0 + t;
+    const bool ok = t < nk;
+    sre[w] = ok ? spec[2 * g] : 0.;
+    sim[w] = ok ? spec[2 * g + 1] : 0.;
+    sv[w] = ok ? vt[g] : 0.;
+    sr[w] = ok ? rvt[g] : 0.;
   }
-  {
-    const double l = pl[n - 1];
-    double c = -l - pu[n - 1] + ev;
-    c += pu[n - 1];
-    const double val = c - l * V(n - 2);
-    if (fabs(val) > kDblEpsilon) {
-      QR(n - 1) = 1. / val * (QR(n - 1) - l * pr);
-      QI(n - 1) = 1. / val * (QI(n - 1) - l * pi);
-    } else {
-      QR(n - 1) = 0.;
-      QI(n - 1) = 0.;
+  __syncthreads();
+  const int t = threadIdx.x;
+  if (t < nk) {
+    const double ev = evals[k0 + t];
+#define QR(ii) sre[(size_t)(ii) * kt + t]
+#define QI(ii) sim[(size_t)(ii) * kt + t]
+#define V(ii) sv[(size_t)(ii) * kt + t]
+#define RV(ii) sr[(size_t)(ii) * kt + t]
+    // tdm_c with the Neumann boundary rows
+    double c0 = -pl[0] - pu[0] + ev;
+    c0 += pl[0];
+    double pr = QR(0) / c0, pi = QI(0) / c0;
+    QR(0) = pr;
+    QI(0) = pi;
+#pragma unroll 4
+    for (int i = 1; i < n - 1; i++) {
+      const double l = pl[i];
+      const double val = RV(i);  // 1 / (c_i - l_i v_{i-1})
+      pr = val * (QR(i) - l * pr);
+      pi = val * (QI(i) - l * pi);
+      QR(i) = pr;
+      QI(i) = pi;
     }
-  }
-  double nr = QR(n - 1), ni = QI(n - 1);
-  for (int i = n - 2; i >= 0; i--) {
-    const double v = V(i);
-    nr = QR(i) - v * nr;
-    ni = QI(i) - v * ni;
-    QR(i) = nr;
-    QI(i) = ni;
-  }
+    {
+      const double l = pl[n - 1];
+      double c = -l - pu[n - 1] + ev;
+      c += pu[n - 1];
+      const double val = c - l * V(n - 2);
+      if (fabs(val) > kDblEpsilon) {
+        QR(n - 1) = 1. / val * (QR(n - 1) - l * pr);
+        QI(n - 1) = 1. / val * (QI(n - 1) - l * pi);
+      } else {
+        QR(n - 1) = 0.;
+        QI(n - 1) = 0.;
+      }
+    }
+    double nr = QR(n - 1), ni = QI(n - 1);
+#pragma unroll 4
+    for (int i = n - 2; i >= 0; i--) {
+      const double v = V(i);
+      nr = QR(i) - v * nr;
+      ni = QI(i) - v * ni;
+      QR(i) = nr;
+      QI(i) = ni;
+    }
 #undef QR
 #undef QI
 #undef V
+#undef RV
+  }
+  __syncthreads();
+  for (int w = threadIdx.x; w < n * kt; w += blockDim.x) {
+    const int i = w / kt, tt = w - i * kt;
+    if (tt < nk) {
+      const size_t g = (size_t)i * nky + k0 + tt;
+      spec[2 * g] = sre[w];
+      spec[2 * g + 1] = sim[w];
+    }
+  }
 }
 
 // c2r along y for a tile of columns, extract_output and the psi boundaries

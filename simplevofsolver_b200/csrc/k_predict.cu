@@ -15,8 +15,9 @@
 
 namespace svof {
 
+// increments [3][R][nx+1] and the substep's Thomas coefficients [9][nx+1]
 size_t predict_smem_bytes(int nx, int R) {
-  return sizeof(double) * ((size_t)3 * R * (nx + 1));
+  return sizeof(double) * ((size_t)3 * R * (nx + 1) + (size_t)9 * (nx + 1));
 }
 
 // Thomas coefficients of the three implicit-x systems of one substep
@@ -29,9 +30,18 @@ size_t predict_smem_bytes(int nx, int R) {
 __global__ void k_tdm_coef(const double *__restrict__ lap_ux, const double *__restrict__ lap_uy,
                            const double *__restrict__ lap_t, const double *__restrict__ dtp, double gam,
                            double m_dif, double t_dif, int nx, double *__restrict__ coef) {
+  // the Laplacian tables are staged in shared memory first: the recurrence
+  // below then waits on arithmetic only
+  extern __shared__ double slap[];  // [3][3 nx]
+  for (int w = threadIdx.x; w < 3 * nx; w += blockDim.x) {
+    slap[w] = (w < 3 * (nx - 1)) ? lap_ux[w] : 0.;
+    slap[3 * nx + w] = lap_uy[w];
+    slap[6 * nx + w] = lap_t[w];
+  }
+  __syncthreads();
   const int f = threadIdx.x;
   if (f >= 3) return;
-  const double *lap = (0 == f) ? lap_ux : (1 == f ? lap_uy : lap_t);
+  const double *lap = slap + 3 * nx * f;
   const double dif = (2 == f) ? t_dif : m_dif;
   const int n = (0 == f) ? nx - 1 : nx;
   double *L = coef + (size_t)(3 * f + 0) * nx;
@@ -69,6 +79,7 @@ __global__ void __launch_bounds__(256) k_predict(PredictArgs a) {
   const int nx = g.nx, ny = g.ny, R = a.rows_per_block;
   const int ld = nx + 1;
   double *sd = sm;                  // [3][R][ld] increments
+  double *sc = sm + 3 * R * ld;     // [9][ld] Thomas coefficients (L, R, V of ux, uy, t)
   const int j0 = 1 + blockIdx.x * R;
   const int nrows = min(R, ny - j0 + 1);
   const double dt = *a.dtp;
@@ -76,6 +87,8 @@ __global__ void __launch_bounds__(256) k_predict(PredictArgs a) {
   const double dy = g.dy;
   const double *ux = a.ux, *uy = a.uy, *p = a.p, *t = a.t;
   const int tid = threadIdx.x;
+
+  for (int w = tid; w < 9 * nx; w += blockDim.x) sc[(w / nx) * ld + (w % nx)] = a.coef[w];
 
   // ---------------- phase 1: right-hand sides and increments
   for (int w = tid; w < nrows * nx; w += blockDim.x) {
@@ -196,9 +209,9 @@ __global__ void __launch_bounds__(256) k_predict(PredictArgs a) {
     const int jj = tid % nrows;
     const int n = (0 == f) ? nx - 1 : nx;
     double *q = sd + (f * R + jj) * ld;
-    const double *L = a.coef + (size_t)(3 * f + 0) * nx;
-    const double *Rv = a.coef + (size_t)(3 * f + 1) * nx;
-    const double *V = a.coef + (size_t)(3 * f + 2) * nx;
+    const double *L = sc + (3 * f + 0) * ld;
+    const double *Rv = sc + (3 * f + 1) * ld;
+    const double *V = sc + (3 * f + 2) * ld;
     double qprev = q[0] / Rv[0];
     q[0] = qprev;
 #pragma unroll 4

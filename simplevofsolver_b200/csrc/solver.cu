@@ -112,7 +112,9 @@ struct svof_solver {
   cudaEvent_t ev_fork[3] = {nullptr, nullptr, nullptr}, ev_join[3] = {nullptr, nullptr, nullptr};
   // predict launch shape
   int pred_rows = 1;
+  int pred_threads = 256;
   size_t pred_smem = 0;
+  int xsolve_kt = 8;        // ky lines per block of the DFT x solve
   int dft_cols = 1;
   // time step
   double *d_dt = nullptr;
@@ -162,7 +164,8 @@ int launch_halo_bc(svof_solver *s, double *a, int field) {
     case SVOF_VOF: width = nx + 2; nh = 2; kind = BC_VOF; break;
     default: return fail("no boundary rule for field %d", field);
   }
-  k_halo_bc<<<(width + 127) / 128, 128, 0, s->stream>>>(a, width, nh, ny, kind, lo, hi);
+  dim3 gr((width + 127) / 128, ny + 2 * nh);
+  k_halo_bc<<<gr, 128, 0, s->stream>>>(a, width, nh, ny, kind, lo, hi);
   CK_LAUNCH();
   return 0;
 }
@@ -205,8 +208,9 @@ int launch_vof(svof_solver *s, int rk) {
 }
 
 int launch_coef(svof_solver *s, int rk, cudaStream_t st) {
-  k_tdm_coef<<<1, 32, 0, st>>>(s->lap_ux.p, s->lap_uy.p, s->lap_t.p, s->d_dt, RK_A[rk] + RK_B[rk], s->prm.m_dif,
-                               s->prm.t_dif, s->nx, s->coef.p);
+  k_tdm_coef<<<1, 128, sizeof(double) * 9 * s->nx, st>>>(s->lap_ux.p, s->lap_uy.p, s->lap_t.p, s->d_dt,
+                                                           RK_A[rk] + RK_B[rk], s->prm.m_dif, s->prm.t_dif, s->nx,
+                                                           s->coef.p);
   CK_LAUNCH();
   return 0;
 }
@@ -253,7 +257,7 @@ int launch_predict(svof_solver *s, int rk, bool with_coef = true) {
   a.rows_per_block = s->pred_rows;
   a.g = s->grid();
   const int blocks = (s->ny + s->pred_rows - 1) / s->pred_rows;
-  k_predict<<<blocks, 256, s->pred_smem, s->stream>>>(a);
+  k_predict<<<blocks, s->pred_threads, s->pred_smem, s->stream>>>(a);
   CK_LAUNCH();
   s->cur_u ^= 1;
   return 0;
@@ -272,8 +276,9 @@ int launch_potential(svof_solver *s, int rk, int want_dct) {
                                                 s->cs.p, s->d_dt, gam, s->log2fft, g);
     CK_LAUNCH();
     const int kt = s->ysolve_kt;
-    k_dct_ysolve<<<(s->nx + kt - 1) / kt, kt, sizeof(double) * kt * s->ny, s->stream>>>(
-        s->spec.p, s->vt.p, s->rvt.p, s->q1t.p, s->ck.p, s->lastf.p, s->den.p, 1. / s->dy / s->dy, s->nx, s->ny);
+    k_dct_ysolve<<<(s->nx + kt - 1) / kt, 128, sizeof(double) * 3 * kt * s->ny, s->stream>>>(
+        s->spec.p, s->vt.p, s->rvt.p, s->q1t.p, s->ck.p, s->lastf.p, s->den.p, 1. / s->dy / s->dy, s->nx, s->ny,
+        kt);
     CK_LAUNCH();
     k_dct_inv<<<s->ny, nthr, smem, s->stream>>>(s->spec.p, s->psi.p, s->twb.p, s->cs.p, s->log2fft, g);
     CK_LAUNCH();
@@ -285,8 +290,9 @@ int launch_potential(svof_solver *s, int rk, int want_dct) {
     k_dft_fwd<<<blocks, 256, smem, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->spec.p, s->twf.p,
                                                 s->d_dt, gam, s->log2fft, cols, g);
     CK_LAUNCH();
-    k_dft_xsolve<<<(nky + 127) / 128, 128, 0, s->stream>>>(s->spec.p, s->vt.p, s->rvt.p, s->pl.p, s->pu.p,
-                                                            s->evals.p, s->nx, nky);
+    const int xkt = s->xsolve_kt;
+    k_dft_xsolve<<<(nky + xkt - 1) / xkt, 128, sizeof(double) * 4 * xkt * s->nx, s->stream>>>(
+        s->spec.p, s->vt.p, s->rvt.p, s->pl.p, s->pu.p, s->evals.p, s->nx, nky, xkt);
     CK_LAUNCH();
     k_dft_inv<<<blocks, 256, smem, s->stream>>>(s->spec.p, s->psi.p, s->twb.p, s->log2fft, cols, g);
     CK_LAUNCH();
@@ -568,28 +574,26 @@ int svof_create(const svof_params_t *prm, const double *xf, const double *xc, sv
         cudaSuccess != cudaEventCreateWithFlags(&s->ev_join[k], cudaEventDisableTiming))
       return fail("event"), bail();
   }
-  if (s->uniform) {
-    int kt = 32;
-    while (kt > 1 && sizeof(double) * (size_t)kt * ny > 160 * 1024) kt >>= 1;
-    s->ysolve_kt = kt;
-    const size_t sm = sizeof(double) * (size_t)kt * ny;
-    if (sm > 227 * 1024) return fail("svof_create: ny = %d too large for the y line solver", ny), bail();
-    if (sm > 48 * 1024 &&
-        cudaSuccess != cudaFuncSetAttribute(k_dct_ysolve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))
-      return fail("cudaFuncSetAttribute(k_dct_ysolve)"), bail();
-  }
-  // predict launch shape: R rows per block within 200 KB of shared memory
+  // predict launch shape: R rows per block, enough blocks to cover the SMs,
+  // within 200 KB of shared memory
   {
     const long per_row = 3L * (nx + 1);
-    long r = (200L * 1024 / 8 - per_row) / per_row;
-    r = std::max(1L, std::min(8L, r));
+    const long fixed = 9L * (nx + 1);
+    long r = std::max(1, std::min(8, ny / 148));
+    while (r > 1 && (fixed + r * per_row) * 8 > 200L * 1024) r--;
     s->pred_rows = (int)r;
+    s->pred_threads = (r <= 2) ? 128 : 256;
     s->pred_smem = predict_smem_bytes(nx, s->pred_rows);
-    if (s->pred_smem > 227 * 1024) return fail("svof_create: nx = %d too large for the x line solver", nx), bail();
+    if (s->pred_smem > 200 * 1024) return fail("svof_create: nx = %d too large for the x line solver", nx), bail();
     if (cudaSuccess != cudaFuncSetAttribute(k_predict, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)s->pred_smem))
       return fail("cudaFuncSetAttribute(k_predict): %s", cudaGetErrorString(cudaGetLastError())), bail();
+    const size_t coef_smem = sizeof(double) * 9 * nx;
+    if (coef_smem > 48 * 1024 &&
+        cudaSuccess != cudaFuncSetAttribute(k_tdm_coef, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coef_smem))
+      return fail("cudaFuncSetAttribute(k_tdm_coef)"), bail();
   }
+  // transforms: one row (DCT) or a tile of columns (DFT) per block
   {
     const size_t dct_smem = sizeof(double) * 2 * nx;
     if (s->uniform && dct_smem > 48 * 1024) {
@@ -606,6 +610,42 @@ int svof_create(const svof_params_t *prm, const double *xf, const double *xc, sv
     }
     if (sizeof(double) * 2 * (size_t)(s->uniform ? nx : ny) > 200 * 1024)
       return fail("svof_create: FFT length too large for one block"), bail();
+  }
+  // line solves: lines per block so that the blocks cover the SMs, within
+  // 160 KB of staged shared memory
+  auto pick_kt = [](int lines, size_t bytes_per_line) {
+    int kt = 32;
+    while (kt > 4 && lines / kt < 148) kt >>= 1;
+    while (kt > 1 && bytes_per_line * kt > 160 * 1024) kt >>= 1;
+    return kt;
+  };
+  if (s->uniform) {
+    const size_t bpl = sizeof(double) * 3 * (size_t)ny;
+    s->ysolve_kt = pick_kt(nx, bpl);
+    const size_t sm = bpl * s->ysolve_kt;
+    if (sm > 200 * 1024) return fail("svof_create: ny = %d too large for the y line solver", ny), bail();
+    if (sm > 48 * 1024 &&
+        cudaSuccess != cudaFuncSetAttribute(k_dct_ysolve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))
+      return fail("cudaFuncSetAttribute(k_dct_ysolve)"), bail();
+  } else {
+    const size_t bpl = sizeof(double) * 4 * (size_t)nx;
+    s->xsolve_kt = pick_kt(ny / 2 + 1, bpl);
+    const size_t sm = bpl * s->xsolve_kt;
+    if (sm > 200 * 1024) return fail("svof_create: nx = %d too large for the x line solver", nx), bail();
+    if (sm > 48 * 1024 &&
+        cudaSuccess != cudaFuncSetAttribute(k_dft_xsolve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))
+      return fail("cudaFuncSetAttribute(k_dft_xsolve)"), bail();
+  }
+  // launch plan checks: every dynamic shared-memory size covers what the
+  // kernel indexes, every line solve has a thread per line
+  {
+    const size_t need_pred = sizeof(double) * (3 * (size_t)s->pred_rows + 9) * (nx + 1);
+    if (s->pred_smem < need_pred || s->pred_threads < 3 * s->pred_rows || s->pred_rows < 1)
+      return fail("svof_create: inconsistent predictor launch plan"), bail();
+    if (s->uniform && (s->ysolve_kt < 1 || s->ysolve_kt > 64 || s->ysolve_kt > 128))
+      return fail("svof_create: inconsistent y line-solve launch plan"), bail();
+    if (!s->uniform && (s->xsolve_kt < 1 || s->xsolve_kt > 128 || s->dft_cols < 1))
+      return fail("svof_create: inconsistent x line-solve launch plan"), bail();
   }
   if (cudaSuccess != cudaMalloc(&s->d_dt, sizeof(double))) return fail("cudaMalloc dt"), bail();
   if (cudaSuccess != cudaMalloc(&s->d_minbits, sizeof(unsigned long long))) return fail("cudaMalloc"), bail();
@@ -874,9 +914,9 @@ int svof_profile_step(svof_solver_t *s, double *ms, int *launches, int nkinds) {
                                                     s->cs.p, s->d_dt, gam, s->log2fft, g);
         rc = rc || mark(SVOF_K_POISSON_FWD);
         const int kt = s->ysolve_kt;
-        k_dct_ysolve<<<(s->nx + kt - 1) / kt, kt, sizeof(double) * kt * s->ny, s->stream>>>(
+        k_dct_ysolve<<<(s->nx + kt - 1) / kt, 128, sizeof(double) * 3 * kt * s->ny, s->stream>>>(
             s->spec.p, s->vt.p, s->rvt.p, s->q1t.p, s->ck.p, s->lastf.p, s->den.p, 1. / s->dy / s->dy, s->nx,
-            s->ny);
+            s->ny, kt);
         rc = rc || mark(SVOF_K_POISSON_SOLVE);
         k_dct_inv<<<s->ny, nthr, smem, s->stream>>>(s->spec.p, s->psi.p, s->twb.p, s->cs.p, s->log2fft, g);
         rc = rc || mark(SVOF_K_POISSON_INV);
@@ -888,8 +928,9 @@ int svof_profile_step(svof_solver_t *s, double *ms, int *launches, int nkinds) {
         k_dft_fwd<<<blocks, 256, smem, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->spec.p, s->twf.p,
                                                     s->d_dt, gam, s->log2fft, cols, g);
         rc = rc || mark(SVOF_K_POISSON_FWD);
-        k_dft_xsolve<<<(nky + 127) / 128, 128, 0, s->stream>>>(s->spec.p, s->vt.p, s->rvt.p, s->pl.p, s->pu.p,
-                                                                s->evals.p, s->nx, nky);
+        const int xkt = s->xsolve_kt;
+        k_dft_xsolve<<<(nky + xkt - 1) / xkt, 128, sizeof(double) * 4 * xkt * s->nx, s->stream>>>(
+            s->spec.p, s->vt.p, s->rvt.p, s->pl.p, s->pu.p, s->evals.p, s->nx, nky, xkt);
         rc = rc || mark(SVOF_K_POISSON_SOLVE);
         k_dft_inv<<<blocks, 256, smem, s->stream>>>(s->spec.p, s->psi.p, s->twb.p, s->log2fft, cols, g);
         rc = rc || mark(SVOF_K_POISSON_INV);

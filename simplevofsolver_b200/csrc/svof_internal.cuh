@@ -90,7 +90,7 @@ __global__ void k_dct_fwd(const double *__restrict__ ux, const double *__restric
 __global__ void k_dct_ysolve(double *__restrict__ spec, const double *__restrict__ vt,
                              const double *__restrict__ rvt, const double *__restrict__ q1t,
                              const double *__restrict__ ck, const double *__restrict__ lastf,
-                             const double *__restrict__ den, double lap, int nx, int ny);
+                             const double *__restrict__ den, double lap, int nx, int ny, int kt);
 __global__ void k_dct_inv(const double *__restrict__ spec, double *__restrict__ psi,
                           const double *__restrict__ tw, const double *__restrict__ cs,
                           int log2n, Grid2 g);
@@ -101,7 +101,7 @@ __global__ void k_dft_fwd(const double *__restrict__ ux, const double *__restric
 __global__ void k_dft_xsolve(double *__restrict__ spec, const double *__restrict__ vt,
                              const double *__restrict__ rvt, const double *__restrict__ pl,
                              const double *__restrict__ pu, const double *__restrict__ evals, int nx,
-                             int nky);
+                             int nky, int kt);
 __global__ void k_dft_inv(const double *__restrict__ spec, double *__restrict__ psi,
                           const double *__restrict__ tw, int log2n, int cols, Grid2 g);
 
