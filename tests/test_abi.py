@@ -1,0 +1,51 @@
+"""The C-ABI library loads without a GPU and exports every function that
+include/*.h declares; the Python host binds them all.  No compute call is
+made here (that needs a GPU)."""
+import ctypes
+import glob
+import os
+import re
+
+import pytest
+
+import simplevofsolver_b200 as svof
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z0-9_\s\*]*?\b(svof_[A-Za-z0-9_]+)\s*\(",
+                             text, flags=re.M):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def test_headers_declare_the_abi():
+    names = declared_functions()
+    assert "svof_create" in names and "svof_integrate" in names
+    assert len(names) >= 25
+
+
+@pytest.mark.parametrize("name", declared_functions())
+def test_library_exports(name):
+    lib = svof.lib()
+    assert hasattr(lib, name), name
+
+
+def test_python_host_binds_every_exported_entry():
+    declared = set(declared_functions())
+    assert set(svof.EXPORTS) <= declared
+
+
+def test_create_fails_cleanly_without_device():
+    """without a GPU, svof_create reports an error instead of crashing"""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    ic = svof.droplet2d(16, 16)
+    with pytest.raises(svof.SvofError):
+        svof.Solver(ic, svof.physical_params(svof.DROPLET2D_ENV))
