@@ -168,6 +168,30 @@ enum {
  * counterpart (measurement aid). */
 int svof_profile_step(svof_solver_t *solver, double *ms, int *launches, int nkinds);
 
+/* Pressure Poisson solve of the uniform-x (DCT) path for callers that cannot
+ * allocate device memory -- for example a host whose device memory belongs to
+ * a pool or budget it does not control, code running where a device
+ * allocation is not allowed, or a plug-in that is handed only its input and
+ * output buffers.  No counterpart in the reference: it computes what
+ * svof_fluid_compute_potential_dct computes, but needs no svof_create and
+ * calls no cudaMalloc, cudaFree or other allocating routine.
+ *
+ * Inputs: params->nx, ny, lx, ly; xf (host, nx+1 faces of a uniform grid);
+ * ux, uy (device, reference layouts); rkstep and dt.  Output: psi (device,
+ * (ny+2) x (nx+2), interior, Neumann walls and halo rows; its four halo corner
+ * cells keep their previous values, as in the reference).  Work is enqueued
+ * on `stream` (a cudaStream_t, or NULL for the default stream).
+ *
+ * Scratch: one file-scope device array of about 2.2 MB, held by every GPU that
+ * loads this library until the process exits.  Limits: nx a power of two,
+ * 4 <= nx, ny <= 1024, nx * ny <= 65536; larger grids are refused with a
+ * non-zero return and a message on stderr.  The first call on a device looks
+ * up that device's address of the array (cudaGetSymbolAddress) and should
+ * come before any stream capture.  All calls share the array, which keeps the
+ * last call's tables and spectrum: calls that overlap on the GPU race. */
+int svof_poisson_dct_noalloc(const svof_params_t *params, const double *xf, const double *ux,
+                             const double *uy, double *psi, size_t rkstep, double dt, void *stream);
+
 /* wait for all work of the solver's stream */
 int svof_synchronize(svof_solver_t *solver);
 /* CUDA stream the solver issues its work on (cudaStream_t) */
