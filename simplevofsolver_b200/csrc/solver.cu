@@ -84,6 +84,7 @@ struct DevBuf {
 
 struct svof_solver {
   svof_params_t prm{};
+  bool managed = false;     // field buffers in CUDA managed memory
   int nx = 0, ny = 0;
   double dy = 0.;
   bool uniform = false;
@@ -131,9 +132,15 @@ struct svof_solver {
 
 namespace {
 
-int dalloc(DevBuf &b, size_t n) {
+// managed: CUDA managed memory, so that a host program holding the pointer
+// (the reference's logging and save code read the fields directly) can read it
+int dalloc(DevBuf &b, size_t n, bool managed = false) {
   b.n = n;
-  CK(cudaMalloc(&b.p, sizeof(double) * (n ? n : 1)));
+  if (managed) {
+    CK(cudaMallocManaged(&b.p, sizeof(double) * (n ? n : 1)));
+  } else {
+    CK(cudaMalloc(&b.p, sizeof(double) * (n ? n : 1)));
+  }
   CK(cudaMemset(b.p, 0, sizeof(double) * (n ? n : 1)));
   return 0;
 }
@@ -534,12 +541,23 @@ extern "C" {
 const char *svof_last_error(void) { return g_err.c_str(); }
 
 int svof_create(const svof_params_t *prm, const double *xf, const double *xc, svof_solver_t **out) {
+  return svof::engine_create(prm, xf, xc, false, out);
+}
+
+}  // extern "C"
+
+namespace svof {
+
+int engine_create(const svof_params_t *prm, const double *xf, const double *xc, bool managed,
+                  svof_solver_t **out) {
   if (!prm || !xf || !xc || !out) return fail("svof_create: null argument");
   *out = nullptr;
   if (prm->nx < 4 || prm->ny < 4) return fail("svof_create: nx and ny must be at least 4");
   if (!(prm->m_dif > 0.) || !(prm->t_dif > 0.)) return fail("svof_create: diffusivities must be positive");
   svof_solver *s = new svof_solver();
   s->prm = *prm;
+  s->managed = managed;
+  const bool mg = managed;
   s->nx = prm->nx;
   s->ny = prm->ny;
   auto bail = [&]() {
@@ -556,15 +574,16 @@ int svof_create(const svof_params_t *prm, const double *xf, const double *xc, sv
   const size_t n_ux = (size_t)(nx + 1) * (ny + 2), n_cc = (size_t)(nx + 2) * (ny + 2);
   const size_t n_vof = (size_t)(nx + 2) * (ny + 4), n_src = (size_t)nx * ny, n_srcx = (size_t)(nx - 1) * ny;
   for (int k = 0; k < 2; k++) {
-    if (dalloc(s->ux[k], n_ux) || dalloc(s->uy[k], n_cc) || dalloc(s->t[k], n_cc) || dalloc(s->vof[k], n_vof))
+    if (dalloc(s->ux[k], n_ux, mg) || dalloc(s->uy[k], n_cc, mg) || dalloc(s->t[k], n_cc, mg) ||
+        dalloc(s->vof[k], n_vof, mg))
       return bail();
-    if (dalloc(s->sux[k], n_srcx) || dalloc(s->suy[k], n_src) || dalloc(s->st[k], n_src) ||
-        dalloc(s->svof[k], n_src))
+    if (dalloc(s->sux[k], n_srcx, mg) || dalloc(s->suy[k], n_src, mg) || dalloc(s->st[k], n_src, mg) ||
+        dalloc(s->svof[k], n_src, mg))
       return bail();
   }
-  if (dalloc(s->p, n_cc) || dalloc(s->psi, n_cc) || dalloc(s->curv, n_cc) ||
-      dalloc(s->normal, 3 * (size_t)nx * (ny + 2)) || dalloc(s->ifrcx, n_srcx) || dalloc(s->ifrcy, n_src) ||
-      dalloc(s->diag, 8))
+  if (dalloc(s->p, n_cc, mg) || dalloc(s->psi, n_cc, mg) || dalloc(s->curv, n_cc, mg) ||
+      dalloc(s->normal, 3 * (size_t)nx * (ny + 2), mg) || dalloc(s->ifrcx, n_srcx, mg) ||
+      dalloc(s->ifrcy, n_src, mg) || dalloc(s->diag, 8))
     return bail();
   if (build_tables(s, xf, xc)) return bail();
   if (dalloc(s->coef, 9 * (size_t)nx)) return bail();
@@ -662,6 +681,36 @@ int svof_create(const svof_params_t *prm, const double *xf, const double *xc, sv
   *out = s;
   return 0;
 }
+
+// parameters that the reference reads after allocation (We in interface_init,
+// coef_dt_* on the first fluid_decide_dt); the step graphs are rebuilt
+int engine_update_params(svof_solver_t *s, const svof_params_t *prm) {
+  if (!s || !prm) return fail("null argument");
+  if (prm->nx != s->nx || prm->ny != s->ny) return fail("engine_update_params: grid size cannot change");
+  CK(cudaStreamSynchronize(s->stream));
+  s->prm = *prm;
+  const int ndims = 2;
+  s->dif_m_y = s->prm.coef_dt_dif / s->prm.m_dif * 0.5 / ndims * std::pow(s->dy, 2.);
+  s->dif_t_y = s->prm.coef_dt_dif / s->prm.t_dif * 0.5 / ndims * std::pow(s->dy, 2.);
+  for (auto &kv : s->graphs) cudaGraphExecDestroy(kv.second);
+  s->graphs.clear();
+  return 0;
+}
+
+// halo / wall update of one field stored at `ptr` (fluid_update_boundaries_*,
+// interface_update_boundaries_vof); waits for completion
+int engine_apply_bc(svof_solver_t *s, int field, double *ptr) {
+  if (!s || !ptr) return fail("null argument");
+  if (launch_halo_bc(s, ptr, field)) return 1;
+  CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+const svof_params_t *engine_params(const svof_solver_t *s) { return &s->prm; }
+
+}  // namespace svof
+
+extern "C" {
 
 int svof_destroy(svof_solver_t *s) {
   if (!s) return 0;

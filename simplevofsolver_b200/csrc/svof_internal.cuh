@@ -11,6 +11,8 @@
 #include <cstddef>
 #include <cstdint>
 
+#include "../../include/svof_b200.h"
+
 namespace svof {
 
 constexpr double kDblEpsilon = 2.220446049250313080847e-16;  // DBL_EPSILON
@@ -119,5 +121,16 @@ __global__ void k_dt_final(unsigned long long *minbits, double *dt, double coef_
 // diagnostics (src/logging/divergence.c, src/logging/interface.c)
 __global__ void k_diag(const double *__restrict__ ux, const double *__restrict__ uy,
                        const double *__restrict__ vof, double *__restrict__ out, Grid2 g);
+
+// ---- engine internals shared by the C ABI front-ends (solver.cu, dropin.cu) ----
+// svof_create with a choice of field memory: managed = CUDA managed memory,
+// readable by a host program that holds the field pointers
+int engine_create(const svof_params_t *prm, const double *xf, const double *xc, bool managed,
+                  svof_solver_t **out);
+// replace the run-time parameters (same grid); rebuilds the step graphs
+int engine_update_params(svof_solver_t *s, const svof_params_t *prm);
+// halo / wall update of field `field` stored at `ptr`, waited for
+int engine_apply_bc(svof_solver_t *s, int field, double *ptr);
+const svof_params_t *engine_params(const svof_solver_t *s);
 
 }  // namespace svof

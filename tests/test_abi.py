@@ -49,3 +49,24 @@ def test_create_fails_cleanly_without_device():
     ic = svof.droplet2d(16, 16)
     with pytest.raises(svof.SvofError):
         svof.Solver(ic, svof.physical_params(svof.DROPLET2D_ENV))
+
+
+REFERENCE_ENTRY_POINTS = [
+    "fluid_init", "fluid_save", "fluid_decide_dt", "fluid_predict_field", "fluid_compute_potential_dft",
+    "fluid_compute_potential_dct", "fluid_correct_velocity", "fluid_update_pressure",
+    "fluid_update_boundaries_ux", "fluid_update_boundaries_uy", "fluid_update_boundaries_p",
+    "fluid_update_boundaries_psi", "fluid_update_boundaries_t", "interface_init", "interface_save",
+    "interface_compute_curvature_tensor", "interface_compute_force", "interface_update_vof",
+    "interface_update_boundaries_vof", "linear_system_init", "linear_system_finalise", "integrate",
+]
+
+
+def test_reference_signature_header_matches_exports():
+    """include/svof_reference_abi.h declares the reference's solver entry
+    points (include/fluid_solver.h, interface_solver.h, linear_system.h,
+    integrate.h) and the library exports every one of them"""
+    text = open(os.path.join(ROOT, "include", "svof_reference_abi.h")).read()
+    lib = svof.lib()
+    for name in REFERENCE_ENTRY_POINTS:
+        assert re.search(r"\bint\s+" + name + r"\s*\(", text), name
+        assert hasattr(lib, name), name
