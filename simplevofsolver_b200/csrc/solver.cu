@@ -111,6 +111,7 @@ struct svof_solver {
   // interface kernels
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork[3] = {nullptr, nullptr, nullptr}, ev_join[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t ev_geom[3] = {nullptr, nullptr, nullptr};
   // predict launch shape
   int pred_rows = 1;
   int pred_threads = 256;
@@ -194,9 +195,9 @@ int launch_geom(svof_solver *s) {
   return 0;
 }
 
-int launch_force(svof_solver *s) {
+int launch_force(svof_solver *s, cudaStream_t st = nullptr) {
   dim3 b(32, 8), gr((s->nx + 31) / 32, (s->ny + 7) / 8);
-  k_force<<<gr, b, 0, s->stream>>>(s->vof[s->cur_v].p, s->curv.p, s->ifrcx.p, s->ifrcy.p, s->prm.tension,
+  k_force<<<gr, b, 0, st ? st : s->stream>>>(s->vof[s->cur_v].p, s->curv.p, s->ifrcx.p, s->ifrcy.p, s->prm.tension,
                                    s->grid());
   CK_LAUNCH();
   return 0;
@@ -325,9 +326,13 @@ int launch_step(svof_solver *s) {
     CK(cudaEventRecord(s->ev_fork[rk], s->stream));
     CK(cudaStreamWaitEvent(s->side, s->ev_fork[rk], 0));
     if (launch_coef(s, rk, s->side)) return 1;
-    CK(cudaEventRecord(s->ev_join[rk], s->side));
     if (launch_geom(s)) return 1;
-    if (launch_force(s)) return 1;
+    // the CSF force and the vof advection both only need the geometry: the
+    // force runs beside the advection, on the side branch
+    CK(cudaEventRecord(s->ev_geom[rk], s->stream));
+    CK(cudaStreamWaitEvent(s->side, s->ev_geom[rk], 0));
+    if (launch_force(s, s->side)) return 1;
+    CK(cudaEventRecord(s->ev_join[rk], s->side));
     if (launch_vof(s, rk)) return 1;
     CK(cudaStreamWaitEvent(s->stream, s->ev_join[rk], 0));
     if (launch_predict(s, rk, false)) return 1;
@@ -590,6 +595,7 @@ int engine_create(const svof_params_t *prm, const double *xf, const double *xc, 
   if (cudaSuccess != cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking)) return fail("stream"), bail();
   for (int k = 0; k < 3; k++) {
     if (cudaSuccess != cudaEventCreateWithFlags(&s->ev_fork[k], cudaEventDisableTiming) ||
+        cudaSuccess != cudaEventCreateWithFlags(&s->ev_geom[k], cudaEventDisableTiming) ||
         cudaSuccess != cudaEventCreateWithFlags(&s->ev_join[k], cudaEventDisableTiming))
       return fail("event"), bail();
   }
@@ -731,6 +737,7 @@ int svof_destroy(svof_solver_t *s) {
   if (s->h_dt) cudaFreeHost(s->h_dt);
   for (int k = 0; k < 3; k++) {
     if (s->ev_fork[k]) cudaEventDestroy(s->ev_fork[k]);
+    if (s->ev_geom[k]) cudaEventDestroy(s->ev_geom[k]);
     if (s->ev_join[k]) cudaEventDestroy(s->ev_join[k]);
   }
   if (s->side) cudaStreamDestroy(s->side);
