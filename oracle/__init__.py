@@ -5,12 +5,13 @@ TEST INFRASTRUCTURE ONLY.  Only ``tests/``, ``__graft_entry__.smoke()`` and
 package; the product library never does.
 
 * :class:`Oracle` drives ``libsvof_oracle.so``, this repository's C
-  restatement of the reference algorithm (``oracle/svof_oracle.c``).
+  restatement of the reference algorithm (``oracle/svof_oracle.c``);
+  :class:`Oracle3D` its 3D extension (``oracle/svof_oracle3d.c``).
 * :func:`run_reference` drives ``_ref/libsvof_ref[_c0].so``, the reference's
   own ``src/*.c`` compiled against single-rank shims, in a fresh process (the
   reference keeps solver state in process-wide statics).
 
-Storage layouts are the reference's (``include/array_macros/**``): x fastest,
+Storage layouts are the reference's (``include/array_macros/``): x fastest,
 x ghost cells and y halo rows included.
 """
 from __future__ import annotations
@@ -174,6 +175,157 @@ class Oracle:
         dts = np.zeros(max(nsteps, 1))
         if _load().svo_run(self._h, int(nsteps), dts.ctypes.data) != 0:
             raise RuntimeError("svo_run failed")
+        return dts[:nsteps]
+
+
+# ---------------------------------------------------------------- 3D
+
+def storage_shape3d(name: str, nx: int, ny: int, nz: int):
+    """storage shapes of the 3D restatement (z, y, x[, comps]), x fastest"""
+    if name == "ux":
+        return (nz + 2, ny + 2, nx + 1)
+    if name in ("uy", "uz", "p", "psi", "t", "curv"):
+        return (nz + 2, ny + 2, nx + 2)
+    if name == "vof":
+        return (nz + 4, ny + 4, nx + 2)
+    if name == "dvof":
+        return (nz + 3, ny + 3, nx + 1, 3)
+    if name == "normal":
+        return (nz + 2, ny + 2, nx, 4)
+    if name == "ifrcx" or name.startswith("srcux"):
+        return (nz, ny, nx - 1)
+    if name in ("ifrcy", "ifrcz", "src0", "src1") or name[:5] in ("srcuy", "srcuz") or name.startswith("srct"):
+        return (nz, ny, nx)
+    raise KeyError(name)
+
+
+NHALO3D = {"ux": 1, "uy": 1, "uz": 1, "p": 1, "psi": 1, "t": 1, "vof": 2, "curv": 1}
+
+
+def interior3d(name: str, arr: np.ndarray, ny: int, nz: int) -> np.ndarray:
+    """the j = 1..ny, k = 1..nz part of a halo'd 3D field"""
+    h = NHALO3D[name]
+    return arr[h:h + nz, h:h + ny]
+
+
+class _Params3D(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("lx", ctypes.c_double), ("ly", ctypes.c_double), ("lz", ctypes.c_double),
+                ("m_dif", ctypes.c_double), ("t_dif", ctypes.c_double),
+                ("tension", ctypes.c_double),
+                ("coef_dt_adv", ctypes.c_double), ("coef_dt_dif", ctypes.c_double),
+                ("add_buoyancy", ctypes.c_int),
+                ("uy_xm", ctypes.c_double), ("uy_xp", ctypes.c_double),
+                ("uz_xm", ctypes.c_double), ("uz_xp", ctypes.c_double),
+                ("t_xm", ctypes.c_double), ("t_xp", ctypes.c_double)]
+
+
+_lib3 = None
+
+
+def _load3():
+    global _lib3
+    if _lib3 is None:
+        L = _load()
+        L.svo3_create.restype = ctypes.c_void_p
+        L.svo3_create.argtypes = [ctypes.POINTER(_Params3D), ctypes.c_void_p, ctypes.c_void_p]
+        L.svo3_destroy.argtypes = [ctypes.c_void_p]
+        L.svo3_field.restype = ctypes.POINTER(ctypes.c_double)
+        L.svo3_field.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_long)]
+        for fn in ("svo3_init_boundaries", "svo3_curvature_tensor", "svo3_force"):
+            getattr(L, fn).argtypes = [ctypes.c_void_p]
+        L.svo3_decide_dt.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+        for fn in ("svo3_update_vof", "svo3_predict", "svo3_potential", "svo3_correct", "svo3_update_pressure"):
+            getattr(L, fn).argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double]
+        L.svo3_integrate.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+        L.svo3_run.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        _lib3 = L
+    return _lib3
+
+
+FIELD_NAMES3D = ["ux", "uy", "uz", "p", "psi", "t", "vof", "curv", "normal", "dvof", "ifrcx", "ifrcy", "ifrcz",
+                 "srcux0", "srcuy0", "srcuz0", "srct0", "srcux1", "srcuy1", "srcuz1", "srct1", "src0", "src1"]
+
+
+class Oracle3D:
+    """The 3D C restatement (oracle/svof_oracle3d.c), FP64.  ``ic`` is a
+    simplevofsolver_b200.workloads.InitialCondition3D."""
+
+    def __init__(self, ic, params: dict, add_buoyancy: bool = False, uy_walls=(0.0, 0.0),
+                 uz_walls=(0.0, 0.0), t_walls=(0.0, 0.0)):
+        L = _load3()
+        self.nx, self.ny, self.nz = int(ic.nx), int(ic.ny), int(ic.nz)
+        pr = _Params3D(self.nx, self.ny, self.nz, float(ic.lx), float(ic.ly), float(ic.lz),
+                       params["m_dif"], params["t_dif"], params["tension"], params["coef_dt_adv"],
+                       params["coef_dt_dif"], int(bool(add_buoyancy)), float(uy_walls[0]),
+                       float(uy_walls[1]), float(uz_walls[0]), float(uz_walls[1]), float(t_walls[0]),
+                       float(t_walls[1]))
+        xf = np.ascontiguousarray(ic.xf, dtype=np.float64)
+        xc = np.ascontiguousarray(ic.xc, dtype=np.float64)
+        self._h = L.svo3_create(ctypes.byref(pr), xf.ctypes.data, xc.ctypes.data)
+        if not self._h:
+            raise ValueError("svo3_create failed")
+        for k, v in ic.fields().items():
+            interior3d(k, self.field(k), self.ny, self.nz)[...] = v
+        L.svo3_init_boundaries(self._h)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            _load3().svo3_destroy(self._h)
+            self._h = None
+
+    def field(self, name: str) -> np.ndarray:
+        n = ctypes.c_long(0)
+        ptr = _load3().svo3_field(self._h, name.encode(), ctypes.byref(n))
+        if not ptr:
+            raise KeyError(name)
+        return np.ctypeslib.as_array(ptr, shape=(n.value,)).reshape(
+            storage_shape3d(name, self.nx, self.ny, self.nz))
+
+    def snapshot(self, names=("ux", "uy", "uz", "p", "psi", "t", "vof")):
+        return {k: self.field(k).copy() for k in names}
+
+    def decide_dt(self):
+        dt = ctypes.c_double(0.0)
+        _load3().svo3_decide_dt(self._h, ctypes.byref(dt))
+        return dt.value
+
+    def curvature_tensor(self):
+        _load3().svo3_curvature_tensor(self._h)
+
+    def force(self):
+        _load3().svo3_force(self._h)
+
+    def update_vof(self, rk, dt):
+        _load3().svo3_update_vof(self._h, rk, dt)
+
+    def predict(self, rk, dt):
+        _load3().svo3_predict(self._h, rk, dt)
+
+    def potential(self, rk, dt):
+        _load3().svo3_potential(self._h, rk, dt)
+
+    def correct(self, rk, dt):
+        _load3().svo3_correct(self._h, rk, dt)
+
+    def update_pressure(self, rk, dt):
+        _load3().svo3_update_pressure(self._h, rk, dt)
+
+    def substeps(self, dt):
+        """one step's three Runge-Kutta substeps with a given dt"""
+        for rk in range(3):
+            self.curvature_tensor()
+            self.force()
+            self.update_vof(rk, dt)
+            self.predict(rk, dt)
+            self.potential(rk, dt)
+            self.correct(rk, dt)
+            self.update_pressure(rk, dt)
+
+    def run(self, nsteps: int) -> np.ndarray:
+        dts = np.zeros(max(nsteps, 1))
+        if _load3().svo3_run(self._h, int(nsteps), dts.ctypes.data) != 0:
+            raise RuntimeError("svo3_run failed")
         return dts[:nsteps]
 
 

@@ -61,7 +61,7 @@ struct svo_ctx {
   double *plap_l, *plap_u;         /* DFT path x-Laplacian */
 };
 
-/* ---------- index maps (reference include/array_macros/**) ---------- */
+/* ---------- index maps (reference include/array_macros/) ---------- */
 #define NX (c->nx)
 #define NY (c->ny)
 #define UX(i, j) c->ux[(i) - 1 + (NX + 1) * (j)]

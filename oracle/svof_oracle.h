@@ -5,7 +5,7 @@
  * leg may load it.
  *
  * Every array is stored exactly as the reference stores it (the index maps of
- * include/array_macros/** in the reference): x fastest, one row per y index,
+ * include/array_macros/ in the reference): x fastest, one row per y index,
  * x ghost cells and y halo rows included.  With nx, ny the interior sizes:
  *
  *   ux    (nx+1) x (ny+2)   i in [1, nx+1], j in [0, ny+1]

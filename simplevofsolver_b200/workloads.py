@@ -100,6 +100,208 @@ def droplet2d(nx: int = 128, ny: int = 128, lx: float = 1.0, ly: float = 1.0,
     return InitialCondition(nx, ny, lx, ly, xf, xc, ux, uy, p, t, vof)
 
 
+@dataclass
+class InitialCondition3D:
+    """3D restart set: fields hold interior y and z rows and the x ghost
+    cells: ux (nz, ny, nx+1); uy, uz, p, t, vof (nz, ny, nx+2)."""
+    nx: int
+    ny: int
+    nz: int
+    lx: float
+    ly: float
+    lz: float
+    xf: np.ndarray
+    xc: np.ndarray
+    ux: np.ndarray
+    uy: np.ndarray
+    uz: np.ndarray
+    p: np.ndarray
+    t: np.ndarray
+    vof: np.ndarray
+    env: dict = field(default_factory=dict)
+
+    def fields(self):
+        return {"ux": self.ux, "uy": self.uy, "uz": self.uz, "p": self.p, "t": self.t, "vof": self.vof}
+
+
+def place_spheres(n: int, rmin: float, rmax: float, lx: float, ly: float, lz: float, wall_gap: float,
+                  rng, gap: float = 0.0, max_tries: int = 200000):
+    """Seeded rejection sampling of ``n`` non-overlapping spheres (radius
+    uniform in [rmin, rmax]) at least ``wall_gap`` from the x walls; y and z
+    are periodic, so distances use the minimum image."""
+    out = []
+    tries = 0
+    while len(out) < n:
+        tries += 1
+        if tries > max_tries:
+            raise RuntimeError(f"could not place {n} spheres")
+        r = rng.uniform(rmin, rmax)
+        x = rng.uniform(r + wall_gap, lx - r - wall_gap)
+        y = rng.uniform(0.0, ly)
+        z = rng.uniform(0.0, lz)
+        ok = True
+        for (x2, y2, z2, r2) in out:
+            dy = abs(y - y2)
+            dy = min(dy, ly - dy)
+            dz = abs(z - z2)
+            dz = min(dz, lz - dz)
+            if (x - x2) ** 2 + dy ** 2 + dz ** 2 < (r + r2 + gap) ** 2:
+                ok = False
+                break
+        if ok:
+            out.append((x, y, z, r))
+    return out
+
+
+def _sphere_vof(vof, xf, ny, nz, ly, lz, sphere, w, band, nsub):
+    """Adds one sphere's cell-averaged 0.5 (1 - tanh(phi / w)) to ``vof``
+    (nz, ny, nx+2): cells farther than ``band`` from the surface are 0 or 1
+    exactly, the band cells are integrated by an nsub^3 midpoint rule."""
+    x0, y0, z0, r = sphere
+    nx = xf.size - 1
+    dy, dz = ly / ny, lz / nz
+    xcen = 0.5 * (xf[:-1] + xf[1:])
+    i0 = max(int(np.searchsorted(xf, x0 - r - band)) - 1, 0)
+    i1 = min(int(np.searchsorted(xf, x0 + r + band)) + 1, nx)
+    j0 = int(np.floor((y0 - r - band) / dy)) - 1
+    j1 = int(np.ceil((y0 + r + band) / dy)) + 1
+    k0 = int(np.floor((z0 - r - band) / dz)) - 1
+    k1 = int(np.ceil((z0 + r + band) / dz)) + 1
+    ii = np.arange(i0, i1)
+    jj = np.arange(j0, j1)
+    kk = np.arange(k0, k1)
+    X = xcen[ii][None, None, :]
+    Y = ((jj + 0.5) * dy)[None, :, None]
+    Z = ((kk + 0.5) * dz)[:, None, None]
+    phi = np.sqrt((X - x0) ** 2 + (Y - y0) ** 2 + (Z - z0) ** 2) - r
+    inside = phi < -band
+    near = np.abs(phi) <= band
+    val = np.where(inside, 1.0, 0.0)
+    kn, jn, in_ = np.nonzero(near)
+    if kn.size:
+        frac = (np.arange(nsub) + 0.5) / nsub
+        dxc = (xf[1:] - xf[:-1])[ii[in_]]
+        xs = xf[ii[in_]][:, None] + dxc[:, None] * frac[None, :]
+        ys = (jj[jn][:, None] + frac[None, :]) * dy
+        zs = (kk[kn][:, None] + frac[None, :]) * dz
+        acc = np.zeros(kn.size)
+        for a in range(nsub):
+            d2 = (zs[:, a][:, None, None] - z0) ** 2 + (ys[:, :, None] - y0) ** 2 + \
+                 (xs[:, None, :] - x0) ** 2
+            ph = np.sqrt(d2) - r
+            acc += (0.5 * (1.0 - np.tanh(ph / w))).sum(axis=(1, 2))
+        val[kn, jn, in_] = acc / nsub ** 3
+    jm = np.mod(jj, ny)
+    km = np.mod(kk, nz)
+    sub = vof[np.ix_(km, jm, ii + 1)]
+    vof[np.ix_(km, jm, ii + 1)] = np.maximum(sub, val)
+
+
+def random_potential(ny, nz, ly, lz, kmax, rng):
+    """Coefficients of one random Fourier potential: a list of
+    (ky, kz, amplitude, phase) with 0 < ky^2 + kz^2 <= kmax^2, amplitudes
+    standard normal over |k|"""
+    modes = []
+    for ky in range(-kmax, kmax + 1):
+        for kz in range(-kmax, kmax + 1):
+            if ky * ky + kz * kz == 0 or ky * ky + kz * kz > kmax * kmax:
+                continue
+            modes.append((ky, kz, rng.standard_normal() / np.hypot(ky, kz), rng.uniform(0.0, 2.0 * np.pi)))
+    return modes
+
+
+def eval_potential(modes, ny, nz, ly, lz, yoff, zoff):
+    y = (np.arange(ny) + yoff) * (ly / ny)
+    z = (np.arange(nz) + zoff) * (lz / nz)
+    out = np.zeros((nz, ny))
+    for ky, kz, a, th in modes:
+        out += a * np.cos(2.0 * np.pi * (ky * y[None, :] / ly + kz * z[:, None] / lz) + th)
+    return out
+
+
+def droplets3d(nx: int = 256, ny: int = 256, nz: int = 256, lx: float = 1.0, ly: float = 1.0,
+               lz: float = 1.0, uniform: bool = False, stretch: float = 1.5, ndrops: int = 32,
+               radii=(0.04, 0.08), urms: float = 0.5, kmax: int = 4, seed: int = 1, nsub: int = 4,
+               velocity: bool = True) -> InitialCondition3D:
+    """Spherical droplets in a wall-bounded (x), doubly periodic (y, z) box.
+
+    * Spheres: ``place_spheres`` with radii uniform in ``radii``, no overlap,
+      at least two nominal cells from the walls (``numpy.random.default_rng(seed)``).
+    * vof: cell average of 0.5 (1 - tanh(phi / w)), phi the distance to the
+      sphere surface, w = (lx / nx) / 3; cells within 8 w of a surface by an
+      nsub^3 midpoint rule, the rest exactly 0 or 1.
+    * Velocity: the staggered discrete curl of A = (0, f(x) a(y, z), f(x) b(y, z)),
+      f = sin^2(pi x / lx) (zero with its slope at the walls, so ux vanishes
+      there), a and b random Fourier sums over 0 < |k| <= kmax: ux = f (db/dy
+      - da/dz), uy = -(df/dx) b, uz = (df/dx) a, differenced on the grid so
+      the discrete divergence vanishes to round-off; scaled so that
+      sqrt(mean(ux^2 + uy^2 + uz^2) / 3) = urms.  p and t are zero.
+    """
+    rng = np.random.default_rng(seed)
+    xf, xc = x_grid(nx, lx, uniform, stretch)
+    h = lx / nx
+    w = h / 3.0
+    spheres = place_spheres(ndrops, radii[0], radii[1], lx, ly, lz, 2.0 * h, rng)
+    vof = np.zeros((nz, ny, nx + 2))
+    for sp in spheres:
+        _sphere_vof(vof, xf, ny, nz, ly, lz, sp, w, 8.0 * w, nsub)
+    ux = np.zeros((nz, ny, nx + 1))
+    uy = np.zeros((nz, ny, nx + 2))
+    uz = np.zeros((nz, ny, nx + 2))
+    if velocity and urms > 0.0:
+        dy, dz = ly / ny, lz / nz
+        ma = random_potential(ny, nz, ly, lz, kmax, rng)
+        mb = random_potential(ny, nz, ly, lz, kmax, rng)
+        # Ay on (x face, y centre, z face), Az on (x face, y face, z centre)
+        a = eval_potential(ma, ny, nz, ly, lz, 0.5, 0.0)
+        b = eval_potential(mb, ny, nz, ly, lz, 0.0, 0.5)
+        f = np.sin(np.pi * xf / lx) ** 2                       # at x faces, f(0) = f(lx) = 0
+        f[0] = 0.0
+        f[-1] = 0.0
+        # ux at (x face i, y centre j, z centre k): dAz/dy - dAy/dz
+        dbdy = (np.roll(b, -1, axis=1) - b) / dy               # (nz, ny): b(j+1) - b(j)
+        dadz = (np.roll(a, -1, axis=0) - a) / dz
+        ux[...] = f[None, None, :] * (dbdy - dadz)[:, :, None]
+        # uy at (x centre, y face j, z centre): -dAz/dx; uz at (x centre, y centre, z face k): dAy/dx
+        dfdx = (f[1:] - f[:-1]) / (xf[1:] - xf[:-1])           # (nx,)
+        uy[:, :, 1:-1] = -dfdx[None, None, :] * b[:, :, None]
+        uz[:, :, 1:-1] = dfdx[None, None, :] * a[:, :, None]
+        rms = np.sqrt((np.mean(ux[:, :, 1:-1] ** 2) + np.mean(uy[:, :, 1:-1] ** 2) +
+                       np.mean(uz[:, :, 1:-1] ** 2)) / 3.0)
+        s = urms / rms
+        ux *= s
+        uy *= s
+        uz *= s
+    p = np.zeros((nz, ny, nx + 2))
+    t = np.zeros((nz, ny, nx + 2))
+    ic = InitialCondition3D(nx, ny, nz, lx, ly, lz, xf, xc, ux, uy, uz, p, t, vof)
+    ic.spheres = spheres
+    return ic
+
+
+def extrude_z(ic: InitialCondition, nz: int, lz: float = 1.0) -> InitialCondition3D:
+    """A 2D set repeated along z (uz = 0): the 3D solver on it reproduces the
+    2D solver."""
+    rep = lambda a: np.ascontiguousarray(np.broadcast_to(a[None], (nz,) + a.shape))
+    return InitialCondition3D(ic.nx, ic.ny, nz, ic.lx, ic.ly, lz, ic.xf.copy(), ic.xc.copy(),
+                              rep(ic.ux), rep(ic.uy), np.zeros((nz, ic.ny, ic.nx + 2)), rep(ic.p),
+                              rep(ic.t), rep(ic.vof))
+
+
+def extrude_y(ic: InitialCondition, ny: int, ly: float = 1.0) -> InitialCondition3D:
+    """A 2D set laid in the x-z plane and repeated along y (uy = 0, the 2D
+    y velocity becomes uz)."""
+    rep = lambda a: np.ascontiguousarray(np.broadcast_to(a[:, None, :], (a.shape[0], ny, a.shape[1])))
+    return InitialCondition3D(ic.nx, ny, ic.ny, ic.lx, ly, ic.ly, ic.xf.copy(), ic.xc.copy(),
+                              rep(ic.ux), np.zeros((ic.ny, ny, ic.nx + 2)), rep(ic.uy), rep(ic.p),
+                              rep(ic.t), rep(ic.vof))
+
+
+# Environment of the 3D droplet workloads: Re = 500 (m_dif = 1 / Re through
+# Ra = 2.5e5, Pr = 1), We = 20, CFL safety 0.5.
+DROPLETS3D_ENV = {"Ra": 2.5e5, "Pr": 1.0, "We": 20.0, "coef_dt_adv": 0.5, "coef_dt_dif": 0.95}
+
+
 # Environment of the 2D droplet workload: Re = sqrt(Ra)/sqrt(Pr) = 100 gives
 # nu = m_dif = 0.01, We = 10, CFL safety 0.5 (src/fluid/init.c:90-93,
 # src/interface/init.c:66-68, src/fluid/decide_dt.c:109-112).
