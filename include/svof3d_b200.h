@@ -1,0 +1,138 @@
+/*
+ * svof3d_b200.h -- C ABI of the B200 library's 3D path (FP64).
+ *
+ * The 3D solver's step functions, with the reference 2D entry points'
+ * semantics and call order (include/fluid_solver.h:10-99,
+ * include/interface_solver.h:8-41, include/integrate.h:5-10), carried to a
+ * third, periodic z direction that is treated like y.  The mounted reference is
+ * its 2D branch, so no reference 3D entry point is replaced one to one.  The
+ * field layouts follow the reference's 3D layout generator
+ * (tools/define_arrays.py:192-229): x fastest, then y, then z, with halo
+ * widths ux (0,1)(1,1)(1,1), uy uz p psi t curv (1,1)(1,1)(1,1),
+ * vof (1,1)(2,2)(2,2) in (x)(y)(z).
+ *
+ *   ux        (nz+2) x (ny+2) x (nx+1)    UX(i,j,k), i = 1 .. nx+1
+ *   uy uz p t psi curv
+ *             (nz+2) x (ny+2) x (nx+2)    i = 0 .. nx+1
+ *   vof       (nz+4) x (ny+4) x (nx+2)    j, k = -1 .. n+2
+ *   normal    (nz+2) x (ny+2) x nx x 4    (nx, ny, nz, intercept) per cell
+ *   ifrcx, srcux_*   nz x ny x (nx-1)     i = 2 .. nx
+ *   ifrcy, ifrcz, srcuy_*, srcuz_*, srct_*, src_*   nz x ny x nx
+ *
+ * Every function returns 0 on success and non-zero on failure, with a message
+ * in svof3d_last_error().  All device work runs on the solver's own stream.
+ * A solver is not reentrant: one host thread drives it at a time.
+ */
+#ifndef SVOF3D_B200_H
+#define SVOF3D_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct svof3d_solver svof3d_solver_t;
+
+typedef struct {
+  int nx, ny, nz;               /* cells; ny and nz powers of two, nx >= 4 */
+  double lx, ly, lz;            /* domain lengths */
+  double m_dif, t_dif;          /* momentum and thermal diffusivities */
+  double tension;               /* surface tension coefficient 1 / We */
+  double coef_dt_adv, coef_dt_dif;
+  int add_buoyancy;             /* +T on the x momentum */
+  double uy_xm, uy_xp;          /* wall values of uy at x = 0, lx */
+  double uz_xm, uz_xp;          /* wall values of uz */
+  double t_xm, t_xp;            /* wall values of t */
+} svof3d_params_t;
+
+enum {
+  SVOF3_UX = 0,
+  SVOF3_UY,
+  SVOF3_UZ,
+  SVOF3_P,
+  SVOF3_T,
+  SVOF3_VOF,
+  SVOF3_PSI,
+  SVOF3_CURV,
+  SVOF3_NORMAL,
+  SVOF3_IFRCX,
+  SVOF3_IFRCY,
+  SVOF3_IFRCZ,
+  SVOF3_SRCUX_A,  /* momentum / scalar sources of the current substep (src_a) */
+  SVOF3_SRCUX_B,  /* ... and of the previous substep (src_b) */
+  SVOF3_SRCUY_A,
+  SVOF3_SRCUY_B,
+  SVOF3_SRCUZ_A,
+  SVOF3_SRCUZ_B,
+  SVOF3_SRCT_A,
+  SVOF3_SRCT_B,
+  SVOF3_SRC_A,    /* vof sources */
+  SVOF3_SRC_B,
+  SVOF3_NFIELDS
+};
+
+/* kernel kinds of svof3d_profile_step */
+enum {
+  SVOF3_K_DT = 0,
+  SVOF3_K_GEOM,
+  SVOF3_K_FORCE,
+  SVOF3_K_VOF,
+  SVOF3_K_PREDICT,
+  SVOF3_K_POISSON_FWD,   /* divergence + r2c along y */
+  SVOF3_K_POISSON_Z,     /* complex DFT along z, both directions */
+  SVOF3_K_POISSON_SOLVE, /* complex Thomas along x */
+  SVOF3_K_POISSON_INV,   /* c2r along y + psi boundaries */
+  SVOF3_K_PROJECT,
+  SVOF3_NKINDS
+};
+
+const char *svof3d_last_error(void);
+
+/* xf: nx+1 face positions, xc: nx+2 centre positions (restart-file xf, xc) */
+int svof3d_create(const svof3d_params_t *params, const double *xf, const double *xc, svof3d_solver_t **out);
+int svof3d_destroy(svof3d_solver_t *s);
+
+/* whole storage arrays (layouts above) */
+int svof3d_field_count(const svof3d_solver_t *s, int field, size_t *count);
+int svof3d_upload_field(svof3d_solver_t *s, int field, const double *host, size_t count);
+int svof3d_download_field(svof3d_solver_t *s, int field, double *host, size_t count);
+int svof3d_device_field(svof3d_solver_t *s, int field, double **dptr);
+
+/* restart-file layout: interior y and z rows, x ghost cells included,
+ * nz x ny x (nx+1) for ux and nz x ny x (nx+2) for uy, uz, p, t, psi, vof;
+ * loading applies the field's halo and wall update */
+int svof3d_load_interior(svof3d_solver_t *s, int field, const double *host, size_t count);
+int svof3d_store_interior(svof3d_solver_t *s, int field, double *host, size_t count);
+
+/* the step functions; rkstep in 0 .. 2 */
+int svof3d_fluid_decide_dt(svof3d_solver_t *s, double *dt);
+int svof3d_interface_compute_curvature_tensor(svof3d_solver_t *s);
+int svof3d_interface_compute_force(svof3d_solver_t *s);
+int svof3d_interface_update_vof(svof3d_solver_t *s, size_t rkstep, double dt);
+int svof3d_fluid_predict_field(svof3d_solver_t *s, size_t rkstep, double dt);
+int svof3d_fluid_compute_potential_dft(svof3d_solver_t *s, size_t rkstep, double dt);
+int svof3d_fluid_correct_velocity(svof3d_solver_t *s, size_t rkstep, double dt);
+int svof3d_fluid_update_pressure(svof3d_solver_t *s, size_t rkstep, double dt);
+
+/* one full step (decide_dt + 3 substeps) as one CUDA graph launch */
+int svof3d_integrate(svof3d_solver_t *s, double *dt);
+/* nsteps steps; dts (may be NULL) receives each step's dt */
+int svof3d_run(svof3d_solver_t *s, int nsteps, double *dts);
+/* nsteps steps queued on the solver's stream without waiting */
+int svof3d_enqueue_steps(svof3d_solver_t *s, int nsteps);
+/* dt of the last completed step; waits for the stream */
+int svof3d_last_dt(svof3d_solver_t *s, double *dt);
+
+/* max |div u| over the interior cells, vof min / max and total volume sum(vof dx dy dz) */
+int svof3d_diagnostics(svof3d_solver_t *s, double *divmax, double *vofmin, double *vofmax, double *volume);
+/* one step launched kernel by kernel with events between; ms[k], launches[k] per kind */
+int svof3d_profile_step(svof3d_solver_t *s, double *ms, int *launches, int nkinds);
+int svof3d_synchronize(svof3d_solver_t *s);
+int svof3d_stream(svof3d_solver_t *s, void **stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

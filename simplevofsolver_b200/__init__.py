@@ -288,3 +288,8 @@ class Solver:
 
     def synchronize(self):
         _check(lib().svof_synchronize(self._h))
+
+
+# the 3D path (include/svof3d_b200.h)
+from .solver3d import (EXPORTS3D, FIELDS3D, Solver3D, interior_shape3d, storage_shape3d)  # noqa: E402,F401
+from .workloads import DROPLETS3D_ENV, InitialCondition3D, droplets3d  # noqa: E402,F401

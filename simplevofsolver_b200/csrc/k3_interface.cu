@@ -1,0 +1,393 @@
+// k3_interface.cu -- boundary and interface (VOF) kernels of the FP64 3D path.
+//
+//   k3_halo_bc     periodic y and z halos + x wall values of one field
+//   k3_geom        corner normals (2x2x2 differences), cell normal and THINC
+//                  intercept (2x2x2 Gauss points), curvature
+//   k3_force       CSF surface-tension force in x, y, z
+//   k3_vof_advect  THINC/QQ face fluxes, flux divergence, RK update of vof
+//                  with its two-layer halo and zero walls
+//
+// The arithmetic is that of oracle/svof_oracle3d.c, which carries the
+// reference's 2D expressions (src/interface/curvature_tensor.c:14-186,
+// force.c:11-76, update/{flxx,flxy,main}.c) to z.  Geometry and advection
+// march along z through a 32 x 4 tile: each plane's inputs are read once,
+// the corner normals of the plane below and the z-face flux of the cell below
+// are kept from the previous plane.
+#include "svof3d_internal.cuh"
+
+namespace svof3 {
+
+__constant__ double c3_gauss_p[2] = {-0.2886751345948129, +0.2886751345948129};
+__constant__ double c3_gauss_w[2] = {+0.5, +0.5};
+constexpr double kVofBeta = 1.;
+constexpr double kVofMin = 1.e-8;
+
+// ---------------------------------------------------------------------------
+// k3_halo_bc: one thread per storage cell c of an interior row (j, k).  The
+// restatement copies the y halo rows of every interior plane, then whole z
+// halo planes, then assigns the x wall values of the interior rows; vof walls
+// are zero in every row.  A halo row therefore holds the values its source
+// row had before the wall assignment.
+__global__ void k3_halo_bc(double *a, int width, int nh, int ny, int nz, int kind, double lo, double hi) {
+  const long w = width;
+  const long tot = w * ny * nz;
+  const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= tot) return;
+  const int c = (int)(id % w);
+  const long row = id / w;
+  const int r = nh + (int)(row % ny);  // stored y index of the interior row
+  const int q = nh + (int)(row / ny);  // stored z index
+  const long rows = ny + 2 * nh;
+  auto at = [&](int rr, int qq) -> double & { return a[w * (rr + rows * qq) + c]; };
+  const double old = at(r, q);
+  int rs[2], qs[2], nr = 1, nq = 1;
+  rs[0] = r;
+  qs[0] = q;
+  if (r - ny >= 0 && r - ny < nh) rs[nr++] = r - ny;
+  if (r + ny >= ny + nh && r + ny < ny + 2 * nh) rs[nr++] = r + ny;
+  if (q - nz >= 0 && q - nz < nh) qs[nq++] = q - nz;
+  if (q + nz >= nz + nh && q + nz < nz + 2 * nh) qs[nq++] = q + nz;
+  const bool left = (0 == c), right = (width - 1 == c);
+  double val = old, img = old;
+  if (BC3_VOF == kind) {
+    if (left || right) val = img = 0.;
+  } else if (left || right) {
+    if (BC3_ZERO == kind) val = 0.;
+    else if (BC3_DIRICHLET == kind) val = left ? lo : hi;
+    else val = left ? a[w * (r + rows * q) + 1] : a[w * (r + rows * q) + width - 2];
+  }
+  for (int x = 0; x < nq; x++)
+    for (int y = 0; y < nr; y++) {
+      if (0 == x && 0 == y) continue;
+      at(rs[y], qs[x]) = img;
+    }
+  at(r, q) = val;
+}
+
+__device__ __forceinline__ double plane_dx(double v00, double v10, double v01, double v11) {
+  return -v00 + v10 - v01 + v11;
+}
+__device__ __forceinline__ double plane_dy(double v00, double v10, double v01, double v11) {
+  return -v00 - v10 + v01 + v11;
+}
+__device__ __forceinline__ double plane_sum(double v00, double v10, double v01, double v11) {
+  return +v00 + v10 + v01 + v11;
+}
+
+// THINC intercept with 2 x 2 x 2 Gauss points (compute_intercept3 of the
+// restatement; src/interface/curvature_tensor.c:50-92 in 2D)
+__device__ __forceinline__ double thinc_intercept3(const double vof, const double n0, const double n1,
+                                                   const double n2) {
+  const int cntmax = 8;
+  const double resmax = 1.e-12;
+  double exps[8];
+#pragma unroll
+  for (int kk = 0; kk < 2; kk++)
+#pragma unroll
+    for (int jj = 0; jj < 2; jj++)
+#pragma unroll
+      for (int ii = 0; ii < 2; ii++)
+        exps[(kk * 2 + jj) * 2 + ii] =
+            exp(-2. * kVofBeta * (+n0 * c3_gauss_p[ii] + n1 * c3_gauss_p[jj] + n2 * c3_gauss_p[kk]));
+  double val = 1. / vof - 1.;
+  for (int cnt = 0; cnt < cntmax; cnt++) {
+    double f0 = -1. * vof;
+    double f1 = 0.;
+#pragma unroll
+    for (int kk = 0; kk < 2; kk++) {
+#pragma unroll
+      for (int jj = 0; jj < 2; jj++) {
+#pragma unroll
+        for (int ii = 0; ii < 2; ii++) {
+          const double weight = c3_gauss_w[ii] * c3_gauss_w[jj] * c3_gauss_w[kk];
+          const double p = exps[(kk * 2 + jj) * 2 + ii];
+          const double denom = 1. / (1. + p * val);
+          f0 += weight * denom;
+          f1 -= weight * p * denom * denom;
+        }
+      }
+    }
+    val -= f0 / f1;
+    if (fabs(f0) < resmax) break;
+  }
+  return -0.5 / kVofBeta * log(val);
+}
+
+// ---------------------------------------------------------------------------
+// k3_geom: cells i in [1, nx], j in [0, ny+1], k in [0, nz+1] (halo cells
+// included, as the restatement computes them).  Block: 32 x 4 cells of one
+// plane, marching over G3Z planes; shared memory holds two vof planes
+// (34 x 6) and two planes of corner normals (33 x 5 x 3).
+constexpr int G3X = 32, G3Y = 4, G3Z = 8;
+
+__global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ vof, double *__restrict__ normal,
+                                                    double *__restrict__ curv, Grid3 g) {
+  __shared__ double sv[2][G3Y + 2][G3X + 2];
+  __shared__ double sc[2][3][G3Y + 1][G3X + 1];
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int i0 = 1 + blockIdx.x * G3X;
+  const int j0 = blockIdx.y * G3Y;
+  const int k0 = blockIdx.z * G3Z;
+  const int kend = min(k0 + G3Z, nz + 2);  // cells k in [k0, kend)
+  const int tid = threadIdx.x;
+  const int tx = tid % G3X, ty = tid / G3X;
+  auto load_plane = [&](int buf, int k) {
+    for (int t = tid; t < (G3X + 2) * (G3Y + 2); t += G3X * G3Y) {
+      const int li = t % (G3X + 2), lj = t / (G3X + 2);
+      const int i = i0 - 1 + li, j = j0 - 1 + lj;
+      sv[buf][lj][li] = (i <= nx + 1 && j <= ny + 2) ? vof[ix_vof(g, i, j, k)] : 0.;
+    }
+  };
+  load_plane(0, k0 - 1);
+  for (int kc = k0; kc <= kend; kc++) {
+    const int bcur = (kc - k0 + 1) & 1, bprev = bcur ^ 1;
+    const int ccur = (kc - k0) & 1, cprev = ccur ^ 1;
+    load_plane(bcur, kc);
+    __syncthreads();
+    // compute_gradient at corners (ic, jc, kc): planes kc-1 (bprev) and kc (bcur)
+    for (int t = tid; t < (G3X + 1) * (G3Y + 1); t += G3X * G3Y) {
+      const int li = t % (G3X + 1), lj = t / (G3X + 1);
+      const int ic = i0 + li, jc = j0 + lj;
+      double d0 = 0., d1 = 0., d2 = 0.;
+      if (ic <= nx + 1 && jc <= ny + 2) {
+        const double a00 = sv[bprev][lj][li], a10 = sv[bprev][lj][li + 1];
+        const double a01 = sv[bprev][lj + 1][li], a11 = sv[bprev][lj + 1][li + 1];
+        const double b00 = sv[bcur][lj][li], b10 = sv[bcur][lj][li + 1];
+        const double b01 = sv[bcur][lj + 1][li], b11 = sv[bcur][lj + 1][li + 1];
+        const double dvofdx = 1. / g.dxc[ic - 1] * (plane_dx(a00, a10, a01, a11) + plane_dx(b00, b10, b01, b11));
+        const double dvofdy = 1. / g.dy * (plane_dy(a00, a10, a01, a11) + plane_dy(b00, b10, b01, b11));
+        const double dvofdz = 1. / g.dz * (plane_sum(b00, b10, b01, b11) - plane_sum(a00, a10, a01, a11));
+        const double norm = sqrt(+dvofdx * dvofdx + dvofdy * dvofdy + dvofdz * dvofdz);
+        const double norminv = 1. / fmax(norm, kDblEpsilon);
+        d0 = dvofdx * norminv;
+        d1 = dvofdy * norminv;
+        d2 = dvofdz * norminv;
+      }
+      sc[ccur][0][lj][li] = d0;
+      sc[ccur][1][lj][li] = d1;
+      sc[ccur][2][lj][li] = d2;
+    }
+    __syncthreads();
+    if (kc > k0) {
+      // cells of plane k = kc - 1: corners kc - 1 (cprev, lower) and kc (ccur, upper)
+      const int i = i0 + tx, j = j0 + ty, k = kc - 1;
+      if (i <= nx && j <= ny + 1) {
+        const double dxf = g.dxf[i - 1];
+#define CL(m, a, b) sc[cprev][m][ty + (b)][tx + (a)]
+#define CU(m, a, b) sc[ccur][m][ty + (b)][tx + (a)]
+        const double dnxdx = 1. / dxf * (plane_dx(CL(0, 0, 0), CL(0, 1, 0), CL(0, 0, 1), CL(0, 1, 1)) +
+                                         plane_dx(CU(0, 0, 0), CU(0, 1, 0), CU(0, 0, 1), CU(0, 1, 1)));
+        const double dnydy = 1. / g.dy * (plane_dy(CL(1, 0, 0), CL(1, 1, 0), CL(1, 0, 1), CL(1, 1, 1)) +
+                                          plane_dy(CU(1, 0, 0), CU(1, 1, 0), CU(1, 0, 1), CU(1, 1, 1)));
+        const double dnzdz = 1. / g.dz * (plane_sum(CU(2, 0, 0), CU(2, 1, 0), CU(2, 0, 1), CU(2, 1, 1)) -
+                                          plane_sum(CL(2, 0, 0), CL(2, 1, 0), CL(2, 0, 1), CL(2, 1, 1)));
+        curv[ix_cc(g, i, j, k)] = 0.25 * (-dnxdx - dnydy - dnzdz);
+        const double lvof = sv[bprev][ty + 1][tx + 1];
+        if (!(lvof < kVofMin || 1. - kVofMin < lvof)) {
+          double n0 = plane_sum(CL(0, 0, 0), CL(0, 1, 0), CL(0, 0, 1), CL(0, 1, 1)) +
+                      plane_sum(CU(0, 0, 0), CU(0, 1, 0), CU(0, 0, 1), CU(0, 1, 1));
+          double n1 = plane_sum(CL(1, 0, 0), CL(1, 1, 0), CL(1, 0, 1), CL(1, 1, 1)) +
+                      plane_sum(CU(1, 0, 0), CU(1, 1, 0), CU(1, 0, 1), CU(1, 1, 1));
+          double n2 = plane_sum(CL(2, 0, 0), CL(2, 1, 0), CL(2, 0, 1), CL(2, 1, 1)) +
+                      plane_sum(CU(2, 0, 0), CU(2, 1, 0), CU(2, 0, 1), CU(2, 1, 1));
+          n0 /= dxf;
+          n1 /= g.dy;
+          n2 /= g.dz;
+          const double norm = sqrt(+n0 * n0 + n1 * n1 + n2 * n2);
+          const double norminv = 1. / fmax(norm, kDblEpsilon);
+          n0 *= norminv;
+          n1 *= norminv;
+          n2 *= norminv;
+          const double d = thinc_intercept3(lvof, n0, n1, n2);
+          double2 *o = reinterpret_cast<double2 *>(normal + ix_nrm(g, i, j, k));
+          o[0] = make_double2(n0, n1);
+          o[1] = make_double2(n2, d);
+        }
+#undef CL
+#undef CU
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// k3_force: one thread per interior cell
+__global__ void k3_force(const double *__restrict__ vof, const double *__restrict__ curv,
+                         double *__restrict__ ifrcx, double *__restrict__ ifrcy, double *__restrict__ ifrcz,
+                         double tension, Grid3 g) {
+  const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = 1 + blockIdx.z;
+  if (i > g.nx || j > g.ny) return;
+  const double vc = vof[ix_vof(g, i, j, k)];
+  const double cc = curv[ix_cc(g, i, j, k)];
+  if (i >= 2) {
+    const double grad = 1. / g.dxc[i - 1] * (-vof[ix_vof(g, i - 1, j, k)] + vc);
+    const double kappa = 0.5 * (+curv[ix_cc(g, i - 1, j, k)] + cc);
+    ifrcx[ix_srcx(g, i, j, k)] = tension * grad * kappa;
+  }
+  {
+    const double grad = 1. / g.dy * (-vof[ix_vof(g, i, j - 1, k)] + vc);
+    const double kappa = 0.5 * (+curv[ix_cc(g, i, j - 1, k)] + cc);
+    ifrcy[ix_src(g, i, j, k)] = tension * grad * kappa;
+  }
+  {
+    const double grad = 1. / g.dz * (-vof[ix_vof(g, i, j, k - 1)] + vc);
+    const double kappa = 0.5 * (+curv[ix_cc(g, i, j, k - 1)] + cc);
+    ifrcz[ix_src(g, i, j, k)] = tension * grad * kappa;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// THINC/QQ flux helpers (indicator3 and the face fluxes of the restatement)
+__device__ __forceinline__ double indicator3(const double *n, double x0, double x1, double x2) {
+  return 1. / (1. + exp(-2. * kVofBeta * (+n[0] * x0 + n[1] * x1 + n[2] * x2 + n[3])));
+}
+
+__device__ __forceinline__ void load_normal(const double *__restrict__ normal, long idx, double *n) {
+  const double2 *p = reinterpret_cast<const double2 *>(normal + idx);
+  const double2 a = p[0], b = p[1];
+  n[0] = a.x;
+  n[1] = a.y;
+  n[2] = b.x;
+  n[3] = b.y;
+}
+
+// flux through the x face i (i in [2, nx]) of row (j, k)
+__device__ __forceinline__ double flux_x(const double *__restrict__ vof, const double *__restrict__ ux,
+                                         const double *__restrict__ normal, const Grid3 &g, int i, int j, int k) {
+  const double vel = ux[ix_ux(g, i, j, k)];
+  const int ii = vel < 0. ? i : i - 1;
+  const double x = vel < 0. ? -0.5 : +0.5;
+  const double lvof = vof[ix_vof(g, ii, j, k)];
+  if (lvof < kVofMin || 1. - kVofMin < lvof) return vel * lvof;
+  double n[4];
+  load_normal(normal, ix_nrm(g, ii, j, k), n);
+  double flux = 0.;
+#pragma unroll
+  for (int kk = 0; kk < 2; kk++)
+#pragma unroll
+    for (int jj = 0; jj < 2; jj++)
+      flux += c3_gauss_w[jj] * c3_gauss_w[kk] * indicator3(n, x, c3_gauss_p[jj], c3_gauss_p[kk]);
+  return vel * flux;
+}
+
+// flux through the y face j (j in [1, ny+1]) of column (i, k)
+__device__ __forceinline__ double flux_y(const double *__restrict__ vof, const double *__restrict__ uy,
+                                         const double *__restrict__ normal, const Grid3 &g, int i, int j, int k) {
+  const double vel = uy[ix_cc(g, i, j, k)];
+  const int jj = vel < 0. ? j : j - 1;
+  const double y = vel < 0. ? -0.5 : +0.5;
+  const double lvof = vof[ix_vof(g, i, jj, k)];
+  if (lvof < kVofMin || 1. - kVofMin < lvof) return vel * lvof;
+  double n[4];
+  load_normal(normal, ix_nrm(g, i, jj, k), n);
+  double flux = 0.;
+#pragma unroll
+  for (int kk = 0; kk < 2; kk++)
+#pragma unroll
+    for (int ii = 0; ii < 2; ii++)
+      flux += c3_gauss_w[ii] * c3_gauss_w[kk] * indicator3(n, c3_gauss_p[ii], y, c3_gauss_p[kk]);
+  return vel * flux;
+}
+
+// flux through the z face k (k in [1, nz+1]) of column (i, j)
+__device__ __forceinline__ double flux_z(const double *__restrict__ vof, const double *__restrict__ uz,
+                                         const double *__restrict__ normal, const Grid3 &g, int i, int j, int k) {
+  const double vel = uz[ix_cc(g, i, j, k)];
+  const int kk = vel < 0. ? k : k - 1;
+  const double z = vel < 0. ? -0.5 : +0.5;
+  const double lvof = vof[ix_vof(g, i, j, kk)];
+  if (lvof < kVofMin || 1. - kVofMin < lvof) return vel * lvof;
+  double n[4];
+  load_normal(normal, ix_nrm(g, i, j, kk), n);
+  double flux = 0.;
+#pragma unroll
+  for (int jj = 0; jj < 2; jj++)
+#pragma unroll
+    for (int ii = 0; ii < 2; ii++)
+      flux += c3_gauss_w[ii] * c3_gauss_w[jj] * indicator3(n, c3_gauss_p[ii], c3_gauss_p[jj], z);
+  return vel * flux;
+}
+
+// k3_vof_advect: cells i in [1, nx], j in [1, ny], k in [1, nz]; block 32 x 4
+// cells marching over V3Z planes.  x and y face fluxes of a plane are staged
+// in shared memory; the z-face flux below a cell is the one above it in the
+// previous plane.  Writes vof_new with its halo images (two layers) and zero
+// x walls, and src_a.
+constexpr int V3X = 32, V3Y = 4, V3Z = 8;
+
+__global__ void __launch_bounds__(V3X * V3Y) k3_vof_advect(const double *__restrict__ vof,
+                                                          double *__restrict__ vof_new,
+                                                          const double *__restrict__ ux,
+                                                          const double *__restrict__ uy,
+                                                          const double *__restrict__ uz,
+                                                          const double *__restrict__ normal,
+                                                          double *__restrict__ src_a,
+                                                          const double *__restrict__ src_b,
+                                                          const double *__restrict__ dtp, RK rk, int use_b,
+                                                          Grid3 g) {
+  __shared__ double fx[V3Y][V3X + 1];
+  __shared__ double fy[V3Y + 1][V3X];
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int i0 = 1 + blockIdx.x * V3X;
+  const int j0 = 1 + blockIdx.y * V3Y;
+  const int k0 = 1 + blockIdx.z * V3Z;
+  const int kend = min(k0 + V3Z, nz + 1);
+  const int tid = threadIdx.x;
+  const int tx = tid % V3X, ty = tid / V3X;
+  const int i = i0 + tx, j = j0 + ty;
+  const bool mine = (i <= nx && j <= ny);
+  const double dt = *dtp;
+  double fz_lo = 0.;
+  if (mine) fz_lo = flux_z(vof, uz, normal, g, i, j, k0);
+  for (int k = k0; k < kend; k++) {
+    for (int t = tid; t < V3Y * (V3X + 1); t += V3X * V3Y) {
+      const int li = t % (V3X + 1), lj = t / (V3X + 1);
+      const int fi = i0 + li, fj = j0 + lj;
+      double f = 0.;
+      if (fi >= 2 && fi <= nx && fj <= ny) f = flux_x(vof, ux, normal, g, fi, fj, k);
+      fx[lj][li] = f;
+    }
+    for (int t = tid; t < (V3Y + 1) * V3X; t += V3X * V3Y) {
+      const int li = t % V3X, lj = t / V3X;
+      const int fi = i0 + li, fj = j0 + lj;
+      double f = 0.;
+      if (fi <= nx && fj <= ny + 1) f = flux_y(vof, uy, normal, g, fi, fj, k);
+      fy[lj][li] = f;
+    }
+    double fz_hi = 0.;
+    if (mine) fz_hi = flux_z(vof, uz, normal, g, i, j, k + 1);
+    __syncthreads();
+    if (mine) {
+      double s = 0.;
+      s += 1. / g.dxf[i - 1] * (+fx[ty][tx] - fx[ty][tx + 1]);
+      s += 1. / g.dy * (+fy[ty][tx] - fy[ty + 1][tx]);
+      s += 1. / g.dz * (+fz_lo - fz_hi);
+      const long is = ix_src(g, i, j, k);
+      src_a[is] = s;
+      double v = vof[ix_vof(g, i, j, k)];
+      v += dt * rk.a * s;
+      if (use_b) v += dt * rk.b * src_b[is];
+      // images: two halo layers in y and z
+      int js[2], ks[2], nj = 1, nk = 1;
+      js[0] = j;
+      ks[0] = k;
+      if (j >= ny - 1) js[nj++] = j - ny;
+      else if (j <= 2) js[nj++] = j + ny;
+      if (k >= nz - 1) ks[nk++] = k - nz;
+      else if (k <= 2) ks[nk++] = k + nz;
+      for (int a = 0; a < nk; a++)
+        for (int b = 0; b < nj; b++) {
+          vof_new[ix_vof(g, i, js[b], ks[a])] = v;
+          if (1 == i) vof_new[ix_vof(g, 0, js[b], ks[a])] = 0.;
+          if (nx == i) vof_new[ix_vof(g, nx + 1, js[b], ks[a])] = 0.;
+        }
+    }
+    fz_lo = fz_hi;
+    __syncthreads();
+  }
+}
+
+}  // namespace svof3

@@ -20,42 +20,13 @@
 // (oracle/svof_fft.c) with the same butterflies and the same twiddle tables,
 // so with FMA contraction disabled they agree with it bit for bit.  Lengths
 // must be powers of two.
+#include "fft_device.cuh"
 #include "svof_internal.cuh"
 
 namespace svof {
 
-__device__ __forceinline__ int bitrev(int q, int log2n) { return (int)(__brev((unsigned)q) >> (32 - log2n)); }
-
-// butterfly stages on interleaved complex data already in bit-reversed order;
-// `lines` independent transforms of length n = 2^log2n stored back to back
-__device__ __forceinline__ void fft_stages(double *z, int log2n, int lines, const double *__restrict__ tw) {
-  const int n = 1 << log2n;
-  const int nb = lines * (n >> 1);
-  for (int s = 1; s <= log2n; s++) {
-    const int half = 1 << (s - 1);
-    const int len = half << 1;
-    const int step = n >> s;
-    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-      const int line = b / (n >> 1);
-      const int bb = b - line * (n >> 1);
-      const int grp = bb >> (s - 1);
-      const int k = bb & (half - 1);
-      double *zz = z + 2 * line * n;
-      const int ia = grp * len + k, ib = ia + half;
-      const double wr = tw[2 * (k * step) + 0];
-      const double wi = tw[2 * (k * step) + 1];
-      const double xr = zz[2 * ib], xi = zz[2 * ib + 1];
-      const double tr = wr * xr - wi * xi;
-      const double ti = wr * xi + wi * xr;
-      const double ur = zz[2 * ia], ui = zz[2 * ia + 1];
-      zz[2 * ia] = ur + tr;
-      zz[2 * ia + 1] = ui + ti;
-      zz[2 * ib] = ur - tr;
-      zz[2 * ib + 1] = ui - ti;
-    }
-    __syncthreads();
-  }
-}
+using svof_fft_dev::bitrev;
+using svof_fft_dev::fft_stages;
 
 // assign_input, dct.c:285-315 / dft.c:315-345
 __device__ __forceinline__ double poisson_rhs(const double *__restrict__ ux, const double *__restrict__ uy,

@@ -1,0 +1,810 @@
+// solver3d.cu -- host engine and C ABI (include/svof3d_b200.h) of the FP64 3D
+// path.
+//
+// Owns the device fields (layouts of tools/define_arrays.py:192-229), the
+// grid and line-solver tables, the ping-pong buffers, the line-solve scratch
+// and one CUDA stream.  A full step (decide_dt and three Runge-Kutta
+// substeps, src/integrate.c:11-68) is captured once per buffer state into a
+// CUDA graph and replayed; the only device->host traffic of a step is the
+// 8-byte dt.  Tables the reference recomputes on every call (Laplacian
+// coefficients, eigenvalues, FFT twiddles) are computed here once, on the
+// host, with the restatement's expressions.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/svof3d_b200.h"
+#include "svof3d_internal.cuh"
+
+using namespace svof3;
+
+namespace {
+
+thread_local std::string g_err3;
+
+int fail(const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err3 = buf;
+  return 1;
+}
+
+#define CK(x)                                                                  \
+  do {                                                                         \
+    cudaError_t e_ = (x);                                                      \
+    if (cudaSuccess != e_) return fail("%s: %s", #x, cudaGetErrorString(e_));  \
+  } while (0)
+
+#define CK_LAUNCH() CK(cudaGetLastError())
+
+constexpr double kPi = 3.14159265358979323846;   // oracle/svof_fft.c twiddles
+constexpr double kGPi = 3.14159265358979324;     // eigenvalues, as src/fluid/compute_potential/dft.c:20
+constexpr double RK_A[3] = {32. / 60., 25. / 60., 45. / 60.};
+constexpr double RK_B[3] = {0. / 60., -17. / 60., -25. / 60.};
+
+int ilog2_exact(int n) {
+  int l = 0;
+  while ((1 << l) < n) l++;
+  return ((1 << l) == n) ? l : -1;
+}
+
+struct DevBuf {
+  double *p = nullptr;
+  size_t n = 0;
+};
+
+int dalloc(DevBuf &b, size_t n) {
+  b.n = n;
+  CK(cudaMalloc(&b.p, sizeof(double) * (n ? n : 1)));
+  CK(cudaMemset(b.p, 0, sizeof(double) * (n ? n : 1)));
+  return 0;
+}
+
+int upload(DevBuf &b, const std::vector<double> &h) {
+  if (dalloc(b, h.size())) return 1;
+  CK(cudaMemcpy(b.p, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
+  return 0;
+}
+
+void dfree(DevBuf &b) {
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.n = 0;
+}
+
+}  // namespace
+
+struct svof3d_solver {
+  svof3d_params_t prm{};
+  int nx = 0, ny = 0, nz = 0;
+  double dy = 0., dz = 0.;
+  int log2ny = 0, log2nz = 0;
+  cudaStream_t stream = nullptr;
+  DevBuf ux[2], uy[2], uz[2], t[2], vof[2];
+  DevBuf p, psi, curv, normal, ifrcx, ifrcy, ifrcz;
+  DevBuf sux[2], suy[2], suz[2], st[2], svof[2];
+  int cur_u = 0, cur_v = 0, sa_f = 0, sa_v = 0;
+  DevBuf dxf, dxc, lap_ux, lap_cc, coef;
+  double lapy[3] = {0., 0., 0.}, lapz[3] = {0., 0., 0.};
+  double lims[4] = {0., 0., 0., 0.};  // explicit diffusive dt limits: m y, m z, t y, t z
+  // Poisson
+  DevBuf spec, xscratch, twf_y, twb_y, twf_z, twb_z, pl, pu, evy, evz;
+  int cols_y = 8, cols_z = 8;
+  // predictor forward-sweep scratch
+  DevBuf fw;
+  // time step
+  double *d_dt = nullptr;
+  unsigned long long *d_minbits = nullptr;
+  double *h_dt = nullptr;
+  int h_dt_slots = 0;
+  DevBuf diag;
+  std::map<int, cudaGraphExec_t> graphs;
+
+  Grid3 grid() const { return Grid3{nx, ny, nz, dy, dz, dxf.p, dxc.p}; }
+};
+
+namespace {
+
+int launch_halo_bc(svof3d_solver *s, double *a, int field) {
+  const int nx = s->nx;
+  int width, nh, kind;
+  double lo = 0., hi = 0.;
+  switch (field) {
+    case SVOF3_UX: width = nx + 1; nh = 1; kind = BC3_ZERO; break;
+    case SVOF3_UY: width = nx + 2; nh = 1; kind = BC3_DIRICHLET; lo = s->prm.uy_xm; hi = s->prm.uy_xp; break;
+    case SVOF3_UZ: width = nx + 2; nh = 1; kind = BC3_DIRICHLET; lo = s->prm.uz_xm; hi = s->prm.uz_xp; break;
+    case SVOF3_T: width = nx + 2; nh = 1; kind = BC3_DIRICHLET; lo = s->prm.t_xm; hi = s->prm.t_xp; break;
+    case SVOF3_P: case SVOF3_PSI: width = nx + 2; nh = 1; kind = BC3_NEUMANN; break;
+    case SVOF3_VOF: width = nx + 2; nh = 2; kind = BC3_VOF; break;
+    default: return fail("no boundary rule for field %d", field);
+  }
+  const long tot = (long)width * s->ny * s->nz;
+  k3_halo_bc<<<(unsigned)((tot + 255) / 256), 256, 0, s->stream>>>(a, width, nh, s->ny, s->nz, kind, lo, hi);
+  CK_LAUNCH();
+  return 0;
+}
+
+int launch_dt(svof3d_solver *s) {
+  const long nc = (long)s->nx * s->ny * s->nz;
+  const int blocks = (int)std::min<long>((nc + 255) / 256, 148L * 8);
+  k3_cfl<<<blocks, 256, 0, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->uz[s->cur_u].p, s->d_minbits,
+                                        s->grid());
+  CK_LAUNCH();
+  k3_dt_final<<<1, 1, 0, s->stream>>>(s->d_minbits, s->d_dt, s->prm.coef_dt_adv, s->lims[0], s->lims[1],
+                                      s->lims[2], s->lims[3]);
+  CK_LAUNCH();
+  return 0;
+}
+
+int launch_geom(svof3d_solver *s) {
+  dim3 gr((s->nx + 31) / 32, (s->ny + 2 + 3) / 4, (s->nz + 2 + 7) / 8);
+  k3_geom<<<gr, 128, 0, s->stream>>>(s->vof[s->cur_v].p, s->normal.p, s->curv.p, s->grid());
+  CK_LAUNCH();
+  return 0;
+}
+
+int launch_force(svof3d_solver *s) {
+  dim3 b(32, 8), gr((s->nx + 31) / 32, (s->ny + 7) / 8, s->nz);
+  k3_force<<<gr, b, 0, s->stream>>>(s->vof[s->cur_v].p, s->curv.p, s->ifrcx.p, s->ifrcy.p, s->ifrcz.p,
+                                    s->prm.tension, s->grid());
+  CK_LAUNCH();
+  return 0;
+}
+
+int launch_vof(svof3d_solver *s, int rk) {
+  if (0 != rk) s->sa_v ^= 1;
+  dim3 gr((s->nx + 31) / 32, (s->ny + 3) / 4, (s->nz + 7) / 8);
+  RK c{RK_A[rk], RK_B[rk], RK_A[rk] + RK_B[rk]};
+  k3_vof_advect<<<gr, 128, 0, s->stream>>>(s->vof[s->cur_v].p, s->vof[1 - s->cur_v].p, s->ux[s->cur_u].p,
+                                           s->uy[s->cur_u].p, s->uz[s->cur_u].p, s->normal.p, s->svof[s->sa_v].p,
+                                           s->svof[1 - s->sa_v].p, s->d_dt, c, rk != 0, s->grid());
+  CK_LAUNCH();
+  s->cur_v ^= 1;
+  return 0;
+}
+
+int launch_predict(svof3d_solver *s, int rk) {
+  k3_tdm_coef<<<1, 128, sizeof(double) * 6 * s->nx, s->stream>>>(s->lap_ux.p, s->lap_cc.p, s->d_dt,
+                                                                 RK_A[rk] + RK_B[rk], s->prm.m_dif, s->prm.t_dif,
+                                                                 s->nx, s->coef.p);
+  CK_LAUNCH();
+  if (0 != rk) s->sa_f ^= 1;
+  Predict3Args a{};
+  const int cu = s->cur_u;
+  a.ux = s->ux[cu].p;
+  a.uy = s->uy[cu].p;
+  a.uz = s->uz[cu].p;
+  a.t = s->t[cu].p;
+  a.p = s->p.p;
+  a.ifrcx = s->ifrcx.p;
+  a.ifrcy = s->ifrcy.p;
+  a.ifrcz = s->ifrcz.p;
+  a.ux_new = s->ux[1 - cu].p;
+  a.uy_new = s->uy[1 - cu].p;
+  a.uz_new = s->uz[1 - cu].p;
+  a.t_new = s->t[1 - cu].p;
+  DevBuf *srcs[4][2] = {{&s->sux[0], &s->sux[1]}, {&s->suy[0], &s->suy[1]}, {&s->suz[0], &s->suz[1]},
+                        {&s->st[0], &s->st[1]}};
+  for (int f = 0; f < 4; f++) {
+    a.sa[f] = srcs[f][s->sa_f]->p;
+    a.sb[f] = srcs[f][1 - s->sa_f]->p;
+  }
+  a.fw = s->fw.p;
+  a.lap_ux = s->lap_ux.p;
+  a.lap_cc = s->lap_cc.p;
+  a.coef = s->coef.p;
+  a.dtp = s->d_dt;
+  a.m_dif = s->prm.m_dif;
+  a.t_dif = s->prm.t_dif;
+  for (int q = 0; q < 3; q++) {
+    a.lapy[q] = s->lapy[q];
+    a.lapz[q] = s->lapz[q];
+  }
+  a.rk = RK{RK_A[rk], RK_B[rk], RK_A[rk] + RK_B[rk]};
+  a.use_b = rk != 0;
+  a.add_buoyancy = s->prm.add_buoyancy;
+  a.uy_xm = s->prm.uy_xm;
+  a.uy_xp = s->prm.uy_xp;
+  a.uz_xm = s->prm.uz_xm;
+  a.uz_xp = s->prm.uz_xp;
+  a.t_xm = s->prm.t_xm;
+  a.t_xp = s->prm.t_xp;
+  a.g = s->grid();
+  const long nlines = (long)s->ny * s->nz;
+  k3_predict<<<(unsigned)((nlines + kPredLines - 1) / kPredLines), 256, 0, s->stream>>>(a);
+  CK_LAUNCH();
+  s->cur_u ^= 1;
+  return 0;
+}
+
+// the four Poisson stages; `marks` (may be null) records an event after each
+int launch_potential(svof3d_solver *s, int rk, const std::vector<cudaEvent_t> *marks = nullptr) {
+  const double gam = RK_A[rk] + RK_B[rk];
+  const Grid3 g = s->grid();
+  const int nky = s->ny / 2 + 1;
+  auto mark = [&](int q) -> int {
+    if (marks) CK(cudaEventRecord((*marks)[q], s->stream));
+    return 0;
+  };
+  {
+    dim3 gr((s->nx + s->cols_y - 1) / s->cols_y, s->nz);
+    const size_t sm = sizeof(double) * 2 * (size_t)s->ny * s->cols_y;
+    k3_pois_fwd_y<<<gr, 256, sm, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->uz[s->cur_u].p, s->spec.p,
+                                              s->twf_y.p, s->d_dt, gam, s->log2ny, s->cols_y, g);
+    CK_LAUNCH();
+    if (mark(0)) return 1;
+  }
+  dim3 grz((s->nx + s->cols_z - 1) / s->cols_z, nky);
+  const size_t smz = sizeof(double) * 2 * (size_t)s->nz * s->cols_z;
+  k3_pois_z<<<grz, 256, smz, s->stream>>>(s->spec.p, s->twf_z.p, s->log2nz, s->cols_z, g);
+  CK_LAUNCH();
+  if (mark(1)) return 1;
+  {
+    const long nlines = (long)nky * s->nz;
+    k3_pois_x<<<(unsigned)((nlines + kXsLines - 1) / kXsLines), 256, 0, s->stream>>>(
+        s->spec.p, s->xscratch.p, s->pl.p, s->pu.p, s->evy.p, s->evz.p, g);
+    CK_LAUNCH();
+    if (mark(2)) return 1;
+  }
+  k3_pois_z<<<grz, 256, smz, s->stream>>>(s->spec.p, s->twb_z.p, s->log2nz, s->cols_z, g);
+  CK_LAUNCH();
+  if (mark(3)) return 1;
+  {
+    dim3 gr((s->nx + s->cols_y - 1) / s->cols_y, s->nz);
+    const size_t sm = sizeof(double) * 2 * (size_t)s->ny * s->cols_y;
+    k3_pois_inv_y<<<gr, 256, sm, s->stream>>>(s->spec.p, s->psi.p, s->twb_y.p, s->log2ny, s->cols_y, g);
+    CK_LAUNCH();
+    if (mark(4)) return 1;
+  }
+  return 0;
+}
+
+int launch_project(svof3d_solver *s, int rk, int do_vel, int do_p) {
+  dim3 b(32, 8), gr((s->nx + 31) / 32, (s->ny + 7) / 8, s->nz);
+  k3_project<<<gr, b, 0, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->uz[s->cur_u].p, s->p.p, s->psi.p,
+                                      s->d_dt, RK_A[rk] + RK_B[rk], s->prm.m_dif, s->prm.uy_xm, s->prm.uy_xp,
+                                      s->prm.uz_xm, s->prm.uz_xp, do_vel, do_p, s->grid());
+  CK_LAUNCH();
+  return 0;
+}
+
+int launch_step(svof3d_solver *s) {
+  if (launch_dt(s)) return 1;
+  for (int rk = 0; rk < 3; rk++) {
+    if (launch_geom(s) || launch_force(s) || launch_vof(s, rk) || launch_predict(s, rk) ||
+        launch_potential(s, rk) || launch_project(s, rk, 1, 1))
+      return 1;
+  }
+  return 0;
+}
+
+int state_key(const svof3d_solver *s) { return s->cur_u | (s->cur_v << 1) | (s->sa_f << 2) | (s->sa_v << 3); }
+
+int step_graph(svof3d_solver *s, cudaGraphExec_t *exec) {
+  const int key = state_key(s);
+  auto it = s->graphs.find(key);
+  if (it != s->graphs.end()) {
+    *exec = it->second;
+    s->cur_u ^= 1;  // three field swaps per step (odd), two source swaps (even)
+    s->cur_v ^= 1;
+    return 0;
+  }
+  cudaGraph_t graph;
+  CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+  const int rc = launch_step(s);
+  cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
+  if (rc) return 1;
+  if (cudaSuccess != e) return fail("cudaStreamEndCapture: %s", cudaGetErrorString(e));
+  cudaGraphExec_t ge;
+  CK(cudaGraphInstantiate(&ge, graph, 0));
+  cudaGraphDestroy(graph);
+  s->graphs[key] = ge;
+  *exec = ge;
+  return 0;
+}
+
+int field_buf(svof3d_solver *s, int field, DevBuf **b) {
+  switch (field) {
+    case SVOF3_UX: *b = &s->ux[s->cur_u]; break;
+    case SVOF3_UY: *b = &s->uy[s->cur_u]; break;
+    case SVOF3_UZ: *b = &s->uz[s->cur_u]; break;
+    case SVOF3_T: *b = &s->t[s->cur_u]; break;
+    case SVOF3_VOF: *b = &s->vof[s->cur_v]; break;
+    case SVOF3_P: *b = &s->p; break;
+    case SVOF3_PSI: *b = &s->psi; break;
+    case SVOF3_CURV: *b = &s->curv; break;
+    case SVOF3_NORMAL: *b = &s->normal; break;
+    case SVOF3_IFRCX: *b = &s->ifrcx; break;
+    case SVOF3_IFRCY: *b = &s->ifrcy; break;
+    case SVOF3_IFRCZ: *b = &s->ifrcz; break;
+    case SVOF3_SRCUX_A: *b = &s->sux[s->sa_f]; break;
+    case SVOF3_SRCUX_B: *b = &s->sux[1 - s->sa_f]; break;
+    case SVOF3_SRCUY_A: *b = &s->suy[s->sa_f]; break;
+    case SVOF3_SRCUY_B: *b = &s->suy[1 - s->sa_f]; break;
+    case SVOF3_SRCUZ_A: *b = &s->suz[s->sa_f]; break;
+    case SVOF3_SRCUZ_B: *b = &s->suz[1 - s->sa_f]; break;
+    case SVOF3_SRCT_A: *b = &s->st[s->sa_f]; break;
+    case SVOF3_SRCT_B: *b = &s->st[1 - s->sa_f]; break;
+    case SVOF3_SRC_A: *b = &s->svof[s->sa_v]; break;
+    case SVOF3_SRC_B: *b = &s->svof[1 - s->sa_v]; break;
+    default: return fail("unknown field id %d", field);
+  }
+  return 0;
+}
+
+// halo width (y and z) and x width of the restart-layout fields
+int interior_layout(const svof3d_solver *s, int field, int *nh, int *width) {
+  switch (field) {
+    case SVOF3_UX: *nh = 1; *width = s->nx + 1; return 0;
+    case SVOF3_UY: case SVOF3_UZ: case SVOF3_P: case SVOF3_T: case SVOF3_PSI: *nh = 1; *width = s->nx + 2; return 0;
+    case SVOF3_VOF: *nh = 2; *width = s->nx + 2; return 0;
+    default: return fail("field %d has no restart-file layout", field);
+  }
+}
+
+int build_tables(svof3d_solver *s, const double *xf, const double *xc) {
+  const int nx = s->nx, ny = s->ny, nz = s->nz;
+  std::vector<double> dxf(nx), dxc(nx + 1);
+  for (int i = 1; i <= nx; i++) dxf[i - 1] = xf[i] - xf[i - 1];
+  for (int i = 1; i <= nx + 1; i++) dxc[i - 1] = xc[i] - xc[i - 1];
+  s->dy = s->prm.ly / ny;
+  s->dz = s->prm.lz / nz;
+  if (upload(s->dxf, dxf) || upload(s->dxc, dxc)) return 1;
+  auto DXF = [&](int i) { return dxf[i - 1]; };
+  auto DXC = [&](int i) { return dxc[i - 1]; };
+  std::vector<double> lux(3 * (nx - 1)), lcc(3 * nx);
+  for (int i = 2; i <= nx; i++) {
+    const double l = 1. / DXF(i - 1) / DXC(i);
+    const double u = 1. / DXF(i) / DXC(i);
+    lux[3 * (i - 2) + 0] = l;
+    lux[3 * (i - 2) + 1] = -l - u;
+    lux[3 * (i - 2) + 2] = u;
+  }
+  for (int i = 1; i <= nx; i++) {
+    const double l = 1. / DXC(i) / DXF(i);
+    const double u = 1. / DXC(i + 1) / DXF(i);
+    lcc[3 * (i - 1) + 0] = l;
+    lcc[3 * (i - 1) + 1] = -l - u;
+    lcc[3 * (i - 1) + 2] = u;
+  }
+  if (upload(s->lap_ux, lux) || upload(s->lap_cc, lcc)) return 1;
+  s->lapy[0] = +1. / s->dy / s->dy;
+  s->lapy[1] = -2. / s->dy / s->dy;
+  s->lapy[2] = +1. / s->dy / s->dy;
+  s->lapz[0] = +1. / s->dz / s->dz;
+  s->lapz[1] = -2. / s->dz / s->dz;
+  s->lapz[2] = +1. / s->dz / s->dz;
+  const int ndims = 3;
+  const double cd = s->prm.coef_dt_dif;
+  s->lims[0] = cd / s->prm.m_dif * 0.5 / ndims * std::pow(s->dy, 2.);
+  s->lims[1] = cd / s->prm.m_dif * 0.5 / ndims * std::pow(s->dz, 2.);
+  s->lims[2] = cd / s->prm.t_dif * 0.5 / ndims * std::pow(s->dy, 2.);
+  s->lims[3] = cd / s->prm.t_dif * 0.5 / ndims * std::pow(s->dz, 2.);
+  s->log2ny = ilog2_exact(ny);
+  s->log2nz = ilog2_exact(nz);
+  if (s->log2ny < 1 || s->log2nz < 1) return fail("svof3d_create: ny and nz must be powers of two (got %d, %d)", ny, nz);
+  auto twiddles = [&](int n, DevBuf &f, DevBuf &b) -> int {
+    std::vector<double> twf(2 * (n / 2)), twb(2 * (n / 2));
+    for (int m = 0; m < n / 2; m++) {
+      const double ang = 2.0 * kPi * (double)m / (double)n;
+      twf[2 * m] = std::cos(ang);
+      twf[2 * m + 1] = -std::sin(ang);
+      twb[2 * m] = std::cos(ang);
+      twb[2 * m + 1] = std::sin(ang);
+    }
+    return upload(f, twf) || upload(b, twb);
+  };
+  if (twiddles(ny, s->twf_y, s->twb_y) || twiddles(nz, s->twf_z, s->twb_z)) return 1;
+  const int nky = ny / 2 + 1;
+  std::vector<double> evy(nky), evz(nz), pl(nx), pu(nx);
+  for (size_t j = 0; j < (size_t)nky; j++)
+    evy[j] = -4. / std::pow(s->prm.ly / ny, 2.) * std::pow(std::sin(kGPi * j / (double)ny), 2.);
+  for (size_t k = 0; k < (size_t)nz; k++)
+    evz[k] = -4. / std::pow(s->prm.lz / nz, 2.) * std::pow(std::sin(kGPi * k / (double)nz), 2.);
+  for (int i = 1; i <= nx; i++) {
+    pl[i - 1] = 1. / DXC(i) / DXF(i);
+    pu[i - 1] = 1. / DXC(i + 1) / DXF(i);
+  }
+  if (upload(s->evy, evy) || upload(s->evz, evz) || upload(s->pl, pl) || upload(s->pu, pu)) return 1;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *svof3d_last_error(void) { return g_err3.c_str(); }
+
+int svof3d_destroy(svof3d_solver_t *s) {
+  if (!s) return 0;
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  for (auto &kv : s->graphs) cudaGraphExecDestroy(kv.second);
+  s->graphs.clear();
+  for (int k = 0; k < 2; k++) {
+    dfree(s->ux[k]); dfree(s->uy[k]); dfree(s->uz[k]); dfree(s->t[k]); dfree(s->vof[k]);
+    dfree(s->sux[k]); dfree(s->suy[k]); dfree(s->suz[k]); dfree(s->st[k]); dfree(s->svof[k]);
+  }
+  DevBuf *bufs[] = {&s->p, &s->psi, &s->curv, &s->normal, &s->ifrcx, &s->ifrcy, &s->ifrcz, &s->dxf, &s->dxc,
+                    &s->lap_ux, &s->lap_cc, &s->coef, &s->spec, &s->xscratch, &s->twf_y, &s->twb_y, &s->twf_z,
+                    &s->twb_z, &s->pl, &s->pu, &s->evy, &s->evz, &s->fw, &s->diag};
+  for (DevBuf *b : bufs) dfree(*b);
+  if (s->d_dt) cudaFree(s->d_dt);
+  if (s->d_minbits) cudaFree(s->d_minbits);
+  if (s->h_dt) cudaFreeHost(s->h_dt);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+  return 0;
+}
+
+int svof3d_create(const svof3d_params_t *prm, const double *xf, const double *xc, svof3d_solver_t **out) {
+  if (!prm || !xf || !xc || !out) return fail("svof3d_create: null argument");
+  *out = nullptr;
+  if (prm->nx < 4 || prm->ny < 4 || prm->nz < 4) return fail("svof3d_create: nx, ny and nz must be at least 4");
+  if (!(prm->m_dif > 0.) || !(prm->t_dif > 0.)) return fail("svof3d_create: diffusivities must be positive");
+  if (prm->ny > 4096 || prm->nz > 4096) return fail("svof3d_create: ny and nz must be at most 4096");
+  svof3d_solver *s = new svof3d_solver();
+  s->prm = *prm;
+  s->nx = prm->nx;
+  s->ny = prm->ny;
+  s->nz = prm->nz;
+  auto bail = [&]() {
+    std::string e = g_err3;
+    svof3d_destroy(s);
+    g_err3 = e;
+    return 1;
+  };
+  if (cudaSuccess != cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) {
+    delete s;
+    return fail("svof3d_create: no CUDA device available (%s)", cudaGetErrorString(cudaGetLastError()));
+  }
+  const size_t nx = s->nx, ny = s->ny, nz = s->nz;
+  const size_t n_ux = (nx + 1) * (ny + 2) * (nz + 2), n_cc = (nx + 2) * (ny + 2) * (nz + 2);
+  const size_t n_vof = (nx + 2) * (ny + 4) * (nz + 4), n_src = nx * ny * nz, n_srcx = (nx - 1) * ny * nz;
+  for (int k = 0; k < 2; k++) {
+    if (dalloc(s->ux[k], n_ux) || dalloc(s->uy[k], n_cc) || dalloc(s->uz[k], n_cc) || dalloc(s->t[k], n_cc) ||
+        dalloc(s->vof[k], n_vof))
+      return bail();
+    if (dalloc(s->sux[k], n_srcx) || dalloc(s->suy[k], n_src) || dalloc(s->suz[k], n_src) ||
+        dalloc(s->st[k], n_src) || dalloc(s->svof[k], n_src))
+      return bail();
+  }
+  if (dalloc(s->p, n_cc) || dalloc(s->psi, n_cc) || dalloc(s->curv, n_cc) ||
+      dalloc(s->normal, 4 * nx * (ny + 2) * (nz + 2)) || dalloc(s->ifrcx, n_srcx) || dalloc(s->ifrcy, n_src) ||
+      dalloc(s->ifrcz, n_src) || dalloc(s->diag, 8))
+    return bail();
+  if (build_tables(s, xf, xc)) return bail();
+  if (dalloc(s->coef, 9 * nx)) return bail();
+  const size_t nky = ny / 2 + 1;
+  if (dalloc(s->spec, 2 * nx * nky * nz) || dalloc(s->xscratch, nx * nky * nz) || dalloc(s->fw, 4 * nx * ny * nz))
+    return bail();
+  // transforms: `cols` lines per block within 64 KB of shared memory
+  auto pick_cols = [](int n) {
+    int c = 16;
+    while (c > 1 && sizeof(double) * 2 * (size_t)n * c > 64 * 1024) c >>= 1;
+    return c;
+  };
+  s->cols_y = pick_cols(s->ny);
+  s->cols_z = pick_cols(s->nz);
+  {
+    const size_t smy = sizeof(double) * 2 * ny * s->cols_y, smz = sizeof(double) * 2 * nz * s->cols_z;
+    if (smy > 200 * 1024 || smz > 200 * 1024) return fail("svof3d_create: FFT length too large"), bail();
+    if (cudaSuccess != cudaFuncSetAttribute(k3_pois_fwd_y, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy) ||
+        cudaSuccess != cudaFuncSetAttribute(k3_pois_inv_y, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy) ||
+        cudaSuccess != cudaFuncSetAttribute(k3_pois_z, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz))
+      return fail("cudaFuncSetAttribute(Poisson): %s", cudaGetErrorString(cudaGetLastError())), bail();
+    const size_t coef_smem = sizeof(double) * 6 * nx;
+    if (coef_smem > 200 * 1024) return fail("svof3d_create: nx too large"), bail();
+    if (cudaSuccess !=
+        cudaFuncSetAttribute(k3_tdm_coef, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coef_smem))
+      return fail("cudaFuncSetAttribute(k3_tdm_coef)"), bail();
+  }
+  if (cudaSuccess != cudaMalloc(&s->d_dt, sizeof(double))) return fail("cudaMalloc dt"), bail();
+  if (cudaSuccess != cudaMalloc(&s->d_minbits, sizeof(unsigned long long))) return fail("cudaMalloc"), bail();
+  {
+    const double one = 1.;
+    unsigned long long bits;
+    std::memcpy(&bits, &one, sizeof(bits));
+    cudaMemcpy(s->d_minbits, &bits, sizeof(bits), cudaMemcpyHostToDevice);
+    cudaMemset(s->d_dt, 0, sizeof(double));
+  }
+  s->h_dt_slots = 1024;
+  if (cudaSuccess != cudaMallocHost(&s->h_dt, sizeof(double) * s->h_dt_slots)) return fail("cudaMallocHost"), bail();
+  if (cudaSuccess != cudaDeviceSynchronize())
+    return fail("svof3d_create: %s", cudaGetErrorString(cudaGetLastError())), bail();
+  *out = s;
+  return 0;
+}
+
+int svof3d_field_count(const svof3d_solver_t *cs, int field, size_t *count) {
+  svof3d_solver *s = const_cast<svof3d_solver *>(cs);
+  DevBuf *b;
+  if (!s || !count) return fail("null argument");
+  if (field_buf(s, field, &b)) return 1;
+  *count = b->n;
+  return 0;
+}
+
+int svof3d_upload_field(svof3d_solver_t *s, int field, const double *host, size_t count) {
+  DevBuf *b;
+  if (!s || !host) return fail("null argument");
+  if (field_buf(s, field, &b)) return 1;
+  if (count != b->n) return fail("field %d holds %zu doubles, got %zu", field, b->n, count);
+  CK(cudaMemcpyAsync(b->p, host, sizeof(double) * count, cudaMemcpyHostToDevice, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+int svof3d_download_field(svof3d_solver_t *s, int field, double *host, size_t count) {
+  DevBuf *b;
+  if (!s || !host) return fail("null argument");
+  if (field_buf(s, field, &b)) return 1;
+  if (count != b->n) return fail("field %d holds %zu doubles, got %zu", field, b->n, count);
+  CK(cudaMemcpyAsync(host, b->p, sizeof(double) * count, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+int svof3d_device_field(svof3d_solver_t *s, int field, double **dptr) {
+  DevBuf *b;
+  if (!s || !dptr) return fail("null argument");
+  if (field_buf(s, field, &b)) return 1;
+  *dptr = b->p;
+  return 0;
+}
+
+// the restart layout is nz x ny x width; in storage each interior plane k has
+// nh halo rows below and above, so the copy is one 2D memcpy of nz planes
+int svof3d_load_interior(svof3d_solver_t *s, int field, const double *host, size_t count) {
+  int nh, width;
+  DevBuf *b;
+  if (!s || !host) return fail("null argument");
+  if (interior_layout(s, field, &nh, &width) || field_buf(s, field, &b)) return 1;
+  const size_t plane = (size_t)width * s->ny;
+  if (count != plane * s->nz) return fail("field %d: restart layout holds %zu doubles, got %zu", field,
+                                          plane * s->nz, count);
+  const size_t spitch = sizeof(double) * plane;
+  const size_t dpitch = sizeof(double) * (size_t)width * (s->ny + 2 * nh);
+  double *dst = b->p + (size_t)width * (s->ny + 2 * nh) * nh + (size_t)width * nh;
+  CK(cudaMemcpy2DAsync(dst, dpitch, host, spitch, spitch, s->nz, cudaMemcpyHostToDevice, s->stream));
+  if (launch_halo_bc(s, b->p, field)) return 1;
+  CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+int svof3d_store_interior(svof3d_solver_t *s, int field, double *host, size_t count) {
+  int nh, width;
+  DevBuf *b;
+  if (!s || !host) return fail("null argument");
+  if (interior_layout(s, field, &nh, &width) || field_buf(s, field, &b)) return 1;
+  const size_t plane = (size_t)width * s->ny;
+  if (count != plane * s->nz) return fail("field %d: restart layout holds %zu doubles, got %zu", field,
+                                          plane * s->nz, count);
+  const size_t dpitch = sizeof(double) * plane;
+  const size_t spitch = sizeof(double) * (size_t)width * (s->ny + 2 * nh);
+  const double *src = b->p + (size_t)width * (s->ny + 2 * nh) * nh + (size_t)width * nh;
+  CK(cudaMemcpy2DAsync(host, dpitch, src, spitch, dpitch, s->nz, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+int svof3d_fluid_decide_dt(svof3d_solver_t *s, double *dt) {
+  if (!s || !dt) return fail("null argument");
+  if (launch_dt(s)) return 1;
+  CK(cudaMemcpyAsync(s->h_dt, s->d_dt, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  *dt = s->h_dt[0];
+  return 0;
+}
+
+static int set_dt(svof3d_solver_t *s, double dt) {
+  s->h_dt[0] = dt;
+  CK(cudaMemcpyAsync(s->d_dt, s->h_dt, sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  return 0;
+}
+
+static int check_rk(size_t rk) { return rk < 3 ? 0 : fail("rkstep %zu out of range", rk); }
+
+static int finish(svof3d_solver_t *s) {
+  CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+int svof3d_interface_compute_curvature_tensor(svof3d_solver_t *s) {
+  if (!s) return fail("null argument");
+  if (launch_geom(s)) return 1;
+  return finish(s);
+}
+
+int svof3d_interface_compute_force(svof3d_solver_t *s) {
+  if (!s) return fail("null argument");
+  if (launch_force(s)) return 1;
+  return finish(s);
+}
+
+int svof3d_interface_update_vof(svof3d_solver_t *s, size_t rk, double dt) {
+  if (!s) return fail("null argument");
+  if (check_rk(rk) || set_dt(s, dt) || launch_vof(s, (int)rk)) return 1;
+  return finish(s);
+}
+
+int svof3d_fluid_predict_field(svof3d_solver_t *s, size_t rk, double dt) {
+  if (!s) return fail("null argument");
+  if (check_rk(rk) || set_dt(s, dt) || launch_predict(s, (int)rk)) return 1;
+  return finish(s);
+}
+
+int svof3d_fluid_compute_potential_dft(svof3d_solver_t *s, size_t rk, double dt) {
+  if (!s) return fail("null argument");
+  if (check_rk(rk) || set_dt(s, dt) || launch_potential(s, (int)rk)) return 1;
+  return finish(s);
+}
+
+int svof3d_fluid_correct_velocity(svof3d_solver_t *s, size_t rk, double dt) {
+  if (!s) return fail("null argument");
+  if (check_rk(rk) || set_dt(s, dt) || launch_project(s, (int)rk, 1, 0)) return 1;
+  return finish(s);
+}
+
+int svof3d_fluid_update_pressure(svof3d_solver_t *s, size_t rk, double dt) {
+  if (!s) return fail("null argument");
+  if (check_rk(rk) || set_dt(s, dt) || launch_project(s, (int)rk, 0, 1)) return 1;
+  return finish(s);
+}
+
+int svof3d_run(svof3d_solver_t *s, int nsteps, double *dts) {
+  if (!s) return fail("null argument");
+  if (nsteps < 0) return fail("nsteps must be non-negative");
+  for (int n = 0; n < nsteps; n++) {
+    cudaGraphExec_t ge;
+    if (step_graph(s, &ge)) return 1;
+    CK(cudaGraphLaunch(ge, s->stream));
+    if (dts) {
+      const int slot = n % s->h_dt_slots;
+      if (0 == slot && n > 0) {
+        CK(cudaStreamSynchronize(s->stream));
+        std::memcpy(dts + n - s->h_dt_slots, s->h_dt, sizeof(double) * s->h_dt_slots);
+      }
+      CK(cudaMemcpyAsync(s->h_dt + slot, s->d_dt, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    }
+  }
+  CK(cudaStreamSynchronize(s->stream));
+  if (dts && nsteps > 0) {
+    const int done = ((nsteps - 1) / s->h_dt_slots) * s->h_dt_slots;
+    std::memcpy(dts + done, s->h_dt, sizeof(double) * (nsteps - done));
+  }
+  return 0;
+}
+
+int svof3d_enqueue_steps(svof3d_solver_t *s, int nsteps) {
+  if (!s) return fail("null argument");
+  if (nsteps < 0) return fail("nsteps must be non-negative");
+  for (int n = 0; n < nsteps; n++) {
+    cudaGraphExec_t ge;
+    if (step_graph(s, &ge)) return 1;
+    CK(cudaGraphLaunch(ge, s->stream));
+    CK(cudaMemcpyAsync(s->h_dt, s->d_dt, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  }
+  return 0;
+}
+
+int svof3d_last_dt(svof3d_solver_t *s, double *dt) {
+  if (!s || !dt) return fail("null argument");
+  CK(cudaStreamSynchronize(s->stream));
+  *dt = s->h_dt[0];
+  return 0;
+}
+
+int svof3d_integrate(svof3d_solver_t *s, double *dt) {
+  double d = 0.;
+  if (svof3d_run(s, 1, &d)) return 1;
+  if (dt) *dt = d;
+  return 0;
+}
+
+int svof3d_profile_step(svof3d_solver_t *s, double *ms, int *launches, int nkinds) {
+  if (!s || !ms || !launches || nkinds < SVOF3_NKINDS) return fail("svof3d_profile_step: bad arguments");
+  for (int k = 0; k < nkinds; k++) {
+    ms[k] = 0.;
+    launches[k] = 0;
+  }
+  std::vector<cudaEvent_t> ev;
+  std::vector<int> kind;
+  auto mark = [&](int k) -> int {
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    CK(cudaEventRecord(e, s->stream));
+    ev.push_back(e);
+    kind.push_back(k);
+    return 0;
+  };
+  std::vector<cudaEvent_t> pev(5);
+  for (auto &e : pev) cudaEventCreate(&e);
+  int rc = mark(-1);
+  rc = rc || launch_dt(s) || mark(SVOF3_K_DT);
+  std::vector<float> pms(5, 0.f);
+  for (int rk = 0; rk < 3 && !rc; rk++) {
+    rc = rc || launch_geom(s) || mark(SVOF3_K_GEOM);
+    rc = rc || launch_force(s) || mark(SVOF3_K_FORCE);
+    rc = rc || launch_vof(s, rk) || mark(SVOF3_K_VOF);
+    rc = rc || launch_predict(s, rk) || mark(SVOF3_K_PREDICT);
+    // the Poisson stages: events after each, start = the predictor's mark
+    cudaEvent_t start = ev.empty() ? nullptr : ev.back();
+    rc = rc || launch_potential(s, rk, &pev);
+    if (!rc) {
+      CK(cudaStreamSynchronize(s->stream));
+      float t;
+      cudaEventElapsedTime(&t, start, pev[0]);
+      ms[SVOF3_K_POISSON_FWD] += t;
+      cudaEventElapsedTime(&t, pev[0], pev[1]);
+      ms[SVOF3_K_POISSON_Z] += t;
+      cudaEventElapsedTime(&t, pev[1], pev[2]);
+      ms[SVOF3_K_POISSON_SOLVE] += t;
+      cudaEventElapsedTime(&t, pev[2], pev[3]);
+      ms[SVOF3_K_POISSON_Z] += t;
+      cudaEventElapsedTime(&t, pev[3], pev[4]);
+      ms[SVOF3_K_POISSON_INV] += t;
+      launches[SVOF3_K_POISSON_FWD] += 1;
+      launches[SVOF3_K_POISSON_Z] += 2;
+      launches[SVOF3_K_POISSON_SOLVE] += 1;
+      launches[SVOF3_K_POISSON_INV] += 1;
+      // restart the chain of marks after the Poisson stages
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      cudaEventRecord(e, s->stream);
+      ev.push_back(e);
+      kind.push_back(-1);
+    }
+    rc = rc || launch_project(s, rk, 1, 1) || mark(SVOF3_K_PROJECT);
+  }
+  cudaError_t e = cudaStreamSynchronize(s->stream);
+  if (!rc && cudaSuccess == e) {
+    for (size_t q = 1; q < ev.size(); q++) {
+      if (kind[q] < 0) continue;
+      float t = 0.f;
+      cudaEventElapsedTime(&t, ev[q - 1], ev[q]);
+      ms[kind[q]] += t;
+      launches[kind[q]] += (SVOF3_K_DT == kind[q] || SVOF3_K_PREDICT == kind[q]) ? 2 : 1;
+    }
+  }
+  for (cudaEvent_t x : ev) cudaEventDestroy(x);
+  for (cudaEvent_t x : pev) cudaEventDestroy(x);
+  if (rc) return 1;
+  if (cudaSuccess != e) return fail("svof3d_profile_step: %s", cudaGetErrorString(e));
+  return 0;
+}
+
+int svof3d_diagnostics(svof3d_solver_t *s, double *divmax, double *vofmin, double *vofmax, double *volume) {
+  if (!s) return fail("null argument");
+  k3_diag<<<1, 1024, 0, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->uz[s->cur_u].p,
+                                     s->vof[s->cur_v].p, s->diag.p, s->grid());
+  CK_LAUNCH();
+  double h[4];
+  CK(cudaMemcpyAsync(h, s->diag.p, sizeof(h), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  if (divmax) *divmax = h[0];
+  if (vofmin) *vofmin = h[1];
+  if (vofmax) *vofmax = h[2];
+  if (volume) *volume = h[3];
+  return 0;
+}
+
+int svof3d_synchronize(svof3d_solver_t *s) {
+  if (!s) return fail("null argument");
+  CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+int svof3d_stream(svof3d_solver_t *s, void **stream) {
+  if (!s || !stream) return fail("null argument");
+  *stream = (void *)s->stream;
+  return 0;
+}
+
+}  // extern "C"

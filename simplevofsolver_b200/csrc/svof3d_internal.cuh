@@ -1,0 +1,147 @@
+// svof3d_internal.cuh -- device helpers and kernel declarations of the FP64
+// 3D path.  Compiled with -fmad=false like the 2D path: every expression keeps
+// the restatement's association (oracle/svof_oracle3d.c), so the device
+// reproduces it except where CUDA's exp / log differ in the last bit (THINC).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+
+#include "../../include/svof3d_b200.h"
+
+namespace svof3 {
+
+constexpr double kDblEpsilon = 2.220446049250313080847e-16;  // DBL_EPSILON
+
+struct Grid3 {
+  int nx, ny, nz;
+  double dy, dz;
+  const double *dxf;  // [nx]   DXF(i) = dxf[i-1]
+  const double *dxc;  // [nx+1] DXC(i) = dxc[i-1]
+};
+
+// index maps of the halo'd arrays (tools/define_arrays.py:192-229)
+__host__ __device__ __forceinline__ long ix_ux(const Grid3 &g, int i, int j, int k) {
+  return (long)(i - 1) + (long)(g.nx + 1) * ((long)j + (long)(g.ny + 2) * k);
+}
+__host__ __device__ __forceinline__ long ix_cc(const Grid3 &g, int i, int j, int k) {
+  return (long)i + (long)(g.nx + 2) * ((long)j + (long)(g.ny + 2) * k);
+}
+__host__ __device__ __forceinline__ long ix_vof(const Grid3 &g, int i, int j, int k) {
+  return (long)i + (long)(g.nx + 2) * ((long)(j + 1) + (long)(g.ny + 4) * (k + 1));
+}
+__host__ __device__ __forceinline__ long ix_nrm(const Grid3 &g, int i, int j, int k) {
+  return 4L * ((long)(i - 1) + (long)g.nx * ((long)j + (long)(g.ny + 2) * k));
+}
+__host__ __device__ __forceinline__ long ix_srcx(const Grid3 &g, int i, int j, int k) {
+  return (long)(i - 2) + (long)(g.nx - 1) * ((long)(j - 1) + (long)g.ny * (k - 1));
+}
+__host__ __device__ __forceinline__ long ix_src(const Grid3 &g, int i, int j, int k) {
+  return (long)(i - 1) + (long)g.nx * ((long)(j - 1) + (long)g.ny * (k - 1));
+}
+
+// periodic images of an interior row (j, k): the row itself and the halo rows
+// that copy it (one halo layer); returns the count, writes up to 4 (j, k)
+__device__ __forceinline__ int halo_images(int j, int k, int ny, int nz, int *jj, int *kk) {
+  int js[2], ks[2], nj = 1, nk = 1;
+  js[0] = j;
+  ks[0] = k;
+  if (1 == j) js[nj++] = ny + 1;
+  else if (ny == j) js[nj++] = 0;
+  if (1 == k) ks[nk++] = nz + 1;
+  else if (nz == k) ks[nk++] = 0;
+  int n = 0;
+  for (int a = 0; a < nk; a++)
+    for (int b = 0; b < nj; b++) {
+      jj[n] = js[b];
+      kk[n] = ks[a];
+      n++;
+    }
+  return n;
+}
+
+struct RK {
+  double a, b, g;
+};
+
+enum BcKind3 { BC3_ZERO = 0, BC3_DIRICHLET = 1, BC3_NEUMANN = 2, BC3_VOF = 3 };
+
+// ---- kernels ----
+// periodic y then z halo and x wall values of one field (restatement of the
+// 2D boundary update with z after y); one thread per storage cell of the
+// interior rows
+__global__ void k3_halo_bc(double *a, int width, int nh, int ny, int nz, int kind, double lo, double hi);
+
+// interface geometry: corner normals, cell normal + intercept, curvature
+__global__ void k3_geom(const double *__restrict__ vof, double *__restrict__ normal, double *__restrict__ curv,
+                        Grid3 g);
+// CSF force
+__global__ void k3_force(const double *__restrict__ vof, const double *__restrict__ curv,
+                         double *__restrict__ ifrcx, double *__restrict__ ifrcy, double *__restrict__ ifrcz,
+                         double tension, Grid3 g);
+// THINC fluxes, divergence, RK update of vof with halo and walls
+__global__ void k3_vof_advect(const double *__restrict__ vof, double *__restrict__ vof_new,
+                              const double *__restrict__ ux, const double *__restrict__ uy,
+                              const double *__restrict__ uz, const double *__restrict__ normal,
+                              double *__restrict__ src_a, const double *__restrict__ src_b,
+                              const double *__restrict__ dtp, RK rk, int use_b, Grid3 g);
+
+// momentum / scalar predictor: right-hand sides, increments and the forward
+// Thomas sweep in x-chunks, then the backward sweep and the update
+struct Predict3Args {
+  const double *ux, *uy, *uz, *p, *t, *ifrcx, *ifrcy, *ifrcz;
+  double *ux_new, *uy_new, *uz_new, *t_new;
+  double *sa[4];        // src_a of ux, uy, uz, t
+  const double *sb[4];  // src_b
+  double *fw;           // forward-sweep scratch, [4][ny nz][nx]
+  const double *lap_ux, *lap_cc;  // 3 per row
+  const double *coef;   // [3 sets (ux, uy/uz, t)][L, R, V][nx]
+  const double *dtp;
+  double m_dif, t_dif;
+  double lapy[3], lapz[3];
+  RK rk;
+  int use_b, add_buoyancy;
+  double uy_xm, uy_xp, uz_xm, uz_xp, t_xm, t_xp;
+  Grid3 g;
+};
+__global__ void k3_predict(Predict3Args a);
+// Thomas coefficients of one substep for the three distinct systems
+__global__ void k3_tdm_coef(const double *__restrict__ lap_ux, const double *__restrict__ lap_cc,
+                            const double *__restrict__ dtp, double gam, double m_dif, double t_dif, int nx,
+                            double *__restrict__ coef);
+
+// Poisson: spectral array S[kz][ky][i] (complex, i fastest)
+__global__ void k3_pois_fwd_y(const double *__restrict__ ux, const double *__restrict__ uy,
+                              const double *__restrict__ uz, double *__restrict__ spec,
+                              const double *__restrict__ tw, const double *__restrict__ dtp, double gam,
+                              int log2n, int cols, Grid3 g);
+__global__ void k3_pois_z(double *__restrict__ spec, const double *__restrict__ tw, int log2n, int cols, Grid3 g);
+__global__ void k3_pois_x(double *__restrict__ spec, double *__restrict__ scratch, const double *__restrict__ pl,
+                          const double *__restrict__ pu, const double *__restrict__ evy,
+                          const double *__restrict__ evz, Grid3 g);
+__global__ void k3_pois_inv_y(const double *__restrict__ spec, double *__restrict__ psi,
+                              const double *__restrict__ tw, int log2n, int cols, Grid3 g);
+
+// projection and pressure update, in place
+__global__ void k3_project(double *__restrict__ ux, double *__restrict__ uy, double *__restrict__ uz,
+                           double *__restrict__ p, const double *__restrict__ psi, const double *__restrict__ dtp,
+                           double gam, double m_dif, double uy_xm, double uy_xp, double uz_xm, double uz_xp,
+                           int do_vel, int do_p, Grid3 g);
+
+// time step
+__global__ void k3_cfl(const double *__restrict__ ux, const double *__restrict__ uy, const double *__restrict__ uz,
+                       unsigned long long *__restrict__ minbits, Grid3 g);
+__global__ void k3_dt_final(unsigned long long *minbits, double *dt, double coef_adv, double l0, double l1,
+                            double l2, double l3);
+// diagnostics: out = {max |div u|, vof min, vof max, sum vof dx dy dz}
+__global__ void k3_diag(const double *__restrict__ ux, const double *__restrict__ uy, const double *__restrict__ uz,
+                        const double *__restrict__ vof, double *__restrict__ out, Grid3 g);
+
+// launch constants shared by the kernels and the host
+constexpr int kPredLines = 32;  // lines per predictor block
+constexpr int kPredChunk = 32;  // x positions per chunk
+constexpr int kXsLines = 32;    // lines per Poisson x-solve block
+constexpr int kXsChunk = 32;
+
+}  // namespace svof3

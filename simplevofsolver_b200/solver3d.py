@@ -1,0 +1,242 @@
+"""The 3D path of libsvof_b200.so through its C ABI (``include/svof3d_b200.h``).
+
+:class:`Solver3D` mirrors the 2D :class:`simplevofsolver_b200.Solver`: the
+reference's entry-point names (``fluid_decide_dt``,
+``interface_compute_curvature_tensor``, ..., ``integrate``) with a third,
+periodic z direction.  Storage shapes are (z, y, x[, comps]), x fastest.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import SvofError, lib
+from .workloads import InitialCondition3D
+
+
+class Params3D(ctypes.Structure):
+    """svof3d_params_t"""
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("lx", ctypes.c_double), ("ly", ctypes.c_double), ("lz", ctypes.c_double),
+                ("m_dif", ctypes.c_double), ("t_dif", ctypes.c_double),
+                ("tension", ctypes.c_double),
+                ("coef_dt_adv", ctypes.c_double), ("coef_dt_dif", ctypes.c_double),
+                ("add_buoyancy", ctypes.c_int),
+                ("uy_xm", ctypes.c_double), ("uy_xp", ctypes.c_double),
+                ("uz_xm", ctypes.c_double), ("uz_xp", ctypes.c_double),
+                ("t_xm", ctypes.c_double), ("t_xp", ctypes.c_double)]
+
+
+FIELDS3D = {"ux": 0, "uy": 1, "uz": 2, "p": 3, "t": 4, "vof": 5, "psi": 6, "curv": 7, "normal": 8,
+            "ifrcx": 9, "ifrcy": 10, "ifrcz": 11, "srcux_a": 12, "srcux_b": 13, "srcuy_a": 14, "srcuy_b": 15,
+            "srcuz_a": 16, "srcuz_b": 17, "srct_a": 18, "srct_b": 19, "src_a": 20, "src_b": 21}
+
+EXPORTS3D = ["svof3d_create", "svof3d_destroy", "svof3d_field_count", "svof3d_upload_field",
+             "svof3d_download_field", "svof3d_device_field", "svof3d_load_interior", "svof3d_store_interior",
+             "svof3d_fluid_decide_dt", "svof3d_interface_compute_curvature_tensor",
+             "svof3d_interface_compute_force", "svof3d_interface_update_vof", "svof3d_fluid_predict_field",
+             "svof3d_fluid_compute_potential_dft", "svof3d_fluid_correct_velocity",
+             "svof3d_fluid_update_pressure", "svof3d_integrate", "svof3d_run", "svof3d_enqueue_steps",
+             "svof3d_last_dt", "svof3d_diagnostics", "svof3d_profile_step", "svof3d_synchronize",
+             "svof3d_stream", "svof3d_last_error"]
+
+
+def storage_shape3d(name: str, nx: int, ny: int, nz: int):
+    if name == "ux":
+        return (nz + 2, ny + 2, nx + 1)
+    if name in ("uy", "uz", "p", "psi", "t", "curv"):
+        return (nz + 2, ny + 2, nx + 2)
+    if name == "vof":
+        return (nz + 4, ny + 4, nx + 2)
+    if name == "normal":
+        return (nz + 2, ny + 2, nx, 4)
+    if name in ("ifrcx", "srcux_a", "srcux_b"):
+        return (nz, ny, nx - 1)
+    if name in FIELDS3D:
+        return (nz, ny, nx)
+    raise KeyError(name)
+
+
+def interior_shape3d(name: str, nx: int, ny: int, nz: int):
+    return (nz, ny, nx + 1) if name == "ux" else (nz, ny, nx + 2)
+
+
+_bound = False
+
+
+def lib3() -> ctypes.CDLL:
+    global _bound
+    L = lib()
+    if not _bound:
+        vp, dp, sz, i, d = ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_double
+        pd = ctypes.POINTER(ctypes.c_double)
+        L.svof3d_create.argtypes = [ctypes.POINTER(Params3D), dp, dp, ctypes.POINTER(vp)]
+        L.svof3d_destroy.argtypes = [vp]
+        L.svof3d_field_count.argtypes = [vp, i, ctypes.POINTER(sz)]
+        for fn in ("svof3d_upload_field", "svof3d_download_field", "svof3d_load_interior", "svof3d_store_interior"):
+            getattr(L, fn).argtypes = [vp, i, dp, sz]
+        L.svof3d_device_field.argtypes = [vp, i, ctypes.POINTER(vp)]
+        L.svof3d_fluid_decide_dt.argtypes = [vp, pd]
+        L.svof3d_interface_compute_curvature_tensor.argtypes = [vp]
+        L.svof3d_interface_compute_force.argtypes = [vp]
+        for fn in ("svof3d_interface_update_vof", "svof3d_fluid_predict_field", "svof3d_fluid_compute_potential_dft",
+                   "svof3d_fluid_correct_velocity", "svof3d_fluid_update_pressure"):
+            getattr(L, fn).argtypes = [vp, sz, d]
+        L.svof3d_integrate.argtypes = [vp, pd]
+        L.svof3d_run.argtypes = [vp, i, dp]
+        L.svof3d_enqueue_steps.argtypes = [vp, i]
+        L.svof3d_last_dt.argtypes = [vp, pd]
+        L.svof3d_diagnostics.argtypes = [vp, pd, pd, pd, pd]
+        L.svof3d_profile_step.argtypes = [vp, dp, dp, i]
+        L.svof3d_synchronize.argtypes = [vp]
+        L.svof3d_stream.argtypes = [vp, ctypes.POINTER(vp)]
+        L.svof3d_last_error.restype = ctypes.c_char_p
+        _bound = True
+    return L
+
+
+def _check(rc: int):
+    if rc != 0:
+        raise SvofError(lib3().svof3d_last_error().decode())
+
+
+def _c(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Solver3D:
+    """One 3D domain on the GPU (FP64).  ``physical`` as for the 2D Solver."""
+
+    KERNEL_KINDS = ["dt", "geom", "force", "vof", "predict", "poisson_fwd", "poisson_z", "poisson_solve",
+                    "poisson_inv", "project"]
+
+    def __init__(self, ic: InitialCondition3D, physical: dict, add_buoyancy: bool = False,
+                 uy_walls=(0.0, 0.0), uz_walls=(0.0, 0.0), t_walls=(0.0, 0.0)):
+        L = lib3()
+        self.nx, self.ny, self.nz = int(ic.nx), int(ic.ny), int(ic.nz)
+        self.params = Params3D(self.nx, self.ny, self.nz, float(ic.lx), float(ic.ly), float(ic.lz),
+                               physical["m_dif"], physical["t_dif"], physical["tension"],
+                               physical["coef_dt_adv"], physical["coef_dt_dif"], int(bool(add_buoyancy)),
+                               float(uy_walls[0]), float(uy_walls[1]), float(uz_walls[0]), float(uz_walls[1]),
+                               float(t_walls[0]), float(t_walls[1]))
+        self._h = ctypes.c_void_p()
+        xf, xc = _c(ic.xf), _c(ic.xc)
+        _check(L.svof3d_create(ctypes.byref(self.params), xf.ctypes.data, xc.ctypes.data, ctypes.byref(self._h)))
+        for k, v in ic.fields().items():
+            self.load_interior(k, v)
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib3().svof3d_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _shape(self, name):
+        return storage_shape3d(name, self.nx, self.ny, self.nz)
+
+    def field(self, name: str) -> np.ndarray:
+        out = np.empty(self._shape(name))
+        _check(lib3().svof3d_download_field(self._h, FIELDS3D[name], out.ctypes.data, out.size))
+        return out
+
+    def set_field(self, name: str, a: np.ndarray):
+        a = _c(a)
+        if a.shape != self._shape(name):
+            raise ValueError(f"{name}: expected shape {self._shape(name)}, got {a.shape}")
+        _check(lib3().svof3d_upload_field(self._h, FIELDS3D[name], a.ctypes.data, a.size))
+
+    def load_interior(self, name: str, a: np.ndarray):
+        a = _c(a)
+        want = interior_shape3d(name, self.nx, self.ny, self.nz)
+        if a.shape != want:
+            raise ValueError(f"{name}: expected shape {want}, got {a.shape}")
+        _check(lib3().svof3d_load_interior(self._h, FIELDS3D[name], a.ctypes.data, a.size))
+
+    def interior(self, name: str) -> np.ndarray:
+        out = np.empty(interior_shape3d(name, self.nx, self.ny, self.nz))
+        _check(lib3().svof3d_store_interior(self._h, FIELDS3D[name], out.ctypes.data, out.size))
+        return out
+
+    def device_ptr(self, name: str) -> int:
+        p = ctypes.c_void_p()
+        _check(lib3().svof3d_device_field(self._h, FIELDS3D[name], ctypes.byref(p)))
+        return int(p.value)
+
+    def stream(self) -> int:
+        p = ctypes.c_void_p()
+        _check(lib3().svof3d_stream(self._h, ctypes.byref(p)))
+        return int(p.value or 0)
+
+    # ------------------------------------------------------------ step functions
+    def fluid_decide_dt(self) -> float:
+        dt = ctypes.c_double(0.0)
+        _check(lib3().svof3d_fluid_decide_dt(self._h, ctypes.byref(dt)))
+        return dt.value
+
+    def interface_compute_curvature_tensor(self):
+        _check(lib3().svof3d_interface_compute_curvature_tensor(self._h))
+
+    def interface_compute_force(self):
+        _check(lib3().svof3d_interface_compute_force(self._h))
+
+    def interface_update_vof(self, rkstep: int, dt: float):
+        _check(lib3().svof3d_interface_update_vof(self._h, rkstep, dt))
+
+    def fluid_predict_field(self, rkstep: int, dt: float):
+        _check(lib3().svof3d_fluid_predict_field(self._h, rkstep, dt))
+
+    def fluid_compute_potential_dft(self, rkstep: int, dt: float):
+        _check(lib3().svof3d_fluid_compute_potential_dft(self._h, rkstep, dt))
+
+    fluid_compute_potential = fluid_compute_potential_dft
+
+    def fluid_correct_velocity(self, rkstep: int, dt: float):
+        _check(lib3().svof3d_fluid_correct_velocity(self._h, rkstep, dt))
+
+    def fluid_update_pressure(self, rkstep: int, dt: float):
+        _check(lib3().svof3d_fluid_update_pressure(self._h, rkstep, dt))
+
+    def integrate(self) -> float:
+        dt = ctypes.c_double(0.0)
+        _check(lib3().svof3d_integrate(self._h, ctypes.byref(dt)))
+        return dt.value
+
+    def run(self, nsteps: int) -> np.ndarray:
+        dts = np.zeros(max(int(nsteps), 1))
+        _check(lib3().svof3d_run(self._h, int(nsteps), dts.ctypes.data))
+        return dts[:nsteps]
+
+    def enqueue_steps(self, nsteps: int):
+        _check(lib3().svof3d_enqueue_steps(self._h, int(nsteps)))
+
+    def last_dt(self) -> float:
+        dt = ctypes.c_double(0.0)
+        _check(lib3().svof3d_last_dt(self._h, ctypes.byref(dt)))
+        return dt.value
+
+    def diagnostics(self) -> dict:
+        v = [ctypes.c_double() for _ in range(4)]
+        _check(lib3().svof3d_diagnostics(self._h, *[ctypes.byref(x) for x in v]))
+        return dict(divmax=v[0].value, vofmin=v[1].value, vofmax=v[2].value, volume=v[3].value)
+
+    def profile_step(self) -> dict:
+        n = len(self.KERNEL_KINDS)
+        ms = np.zeros(n)
+        cnt = np.zeros(n, dtype=np.int32)
+        _check(lib3().svof3d_profile_step(self._h, ms.ctypes.data, cnt.ctypes.data, n))
+        return {k: (float(ms[q]), int(cnt[q])) for q, k in enumerate(self.KERNEL_KINDS)}
+
+    def synchronize(self):
+        _check(lib3().svof3d_synchronize(self._h))

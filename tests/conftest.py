@@ -14,9 +14,8 @@ def pytest_configure(config):
 
 
 def _ensure_oracle():
-    lib = os.path.join(ROOT, "oracle", "libsvof_oracle.so")
-    if not os.path.exists(lib):
-        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "oracle"], check=True)
+    # make rebuilds the oracle library only when its sources are newer
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "oracle"], check=True)
 
 
 _ensure_oracle()

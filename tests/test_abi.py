@@ -18,7 +18,7 @@ def declared_functions():
     for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
         text = open(h).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-        for m in re.finditer(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z0-9_\s\*]*?\b(svof_[A-Za-z0-9_]+)\s*\(",
+        for m in re.finditer(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z0-9_\s\*]*?\b(svof(?:3d)?_[A-Za-z0-9_]+)\s*\(",
                              text, flags=re.M):
             names.add(m.group(1))
     return sorted(names)
@@ -39,6 +39,8 @@ def test_library_exports(name):
 def test_python_host_binds_every_exported_entry():
     declared = set(declared_functions())
     assert set(svof.EXPORTS) <= declared
+    assert set(svof.EXPORTS3D) <= declared
+    assert {n for n in declared if n.startswith("svof3d_")} == set(svof.EXPORTS3D)
 
 
 def test_create_fails_cleanly_without_device():
