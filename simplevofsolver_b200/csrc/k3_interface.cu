@@ -121,7 +121,8 @@ __device__ __forceinline__ double thinc_intercept3(const double vof, const doubl
 constexpr int G3X = 32, G3Y = 4, G3Z = 8;
 
 __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ vof, double *__restrict__ normal,
-                                                    double *__restrict__ curv, Grid3 g) {
+                                                    double *__restrict__ curv, unsigned *__restrict__ work,
+                                                    unsigned *__restrict__ nwork, Grid3 g) {
   __shared__ double sv[2][G3Y + 2][G3X + 2];
   __shared__ double sc[2][3][G3Y + 1][G3X + 1];
   const int nx = g.nx, ny = g.ny, nz = g.nz;
@@ -135,7 +136,7 @@ __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ 
     for (int t = tid; t < (G3X + 2) * (G3Y + 2); t += G3X * G3Y) {
       const int li = t % (G3X + 2), lj = t / (G3X + 2);
       const int i = i0 - 1 + li, j = j0 - 1 + lj;
-      sv[buf][lj][li] = (i <= nx + 1 && j <= ny + 2) ? vof[ix_vof(g, i, j, k)] : 0.;
+      sv[buf][lj][li] = (i <= nx + 1 && j <= ny + 2) ? ldg(vof + ix_vof(g, i, j, k)) : 0.;
     }
   };
   load_plane(0, k0 - 1);
@@ -154,7 +155,7 @@ __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ 
         const double a01 = sv[bprev][lj + 1][li], a11 = sv[bprev][lj + 1][li + 1];
         const double b00 = sv[bcur][lj][li], b10 = sv[bcur][lj][li + 1];
         const double b01 = sv[bcur][lj + 1][li], b11 = sv[bcur][lj + 1][li + 1];
-        const double dvofdx = 1. / g.dxc[ic - 1] * (plane_dx(a00, a10, a01, a11) + plane_dx(b00, b10, b01, b11));
+        const double dvofdx = 1. / ldg(g.dxc + ic - 1) * (plane_dx(a00, a10, a01, a11) + plane_dx(b00, b10, b01, b11));
         const double dvofdy = 1. / g.dy * (plane_dy(a00, a10, a01, a11) + plane_dy(b00, b10, b01, b11));
         const double dvofdz = 1. / g.dz * (plane_sum(b00, b10, b01, b11) - plane_sum(a00, a10, a01, a11));
         const double norm = sqrt(+dvofdx * dvofdx + dvofdy * dvofdy + dvofdz * dvofdz);
@@ -171,8 +172,9 @@ __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ 
     if (kc > k0) {
       // cells of plane k = kc - 1: corners kc - 1 (cprev, lower) and kc (ccur, upper)
       const int i = i0 + tx, j = j0 + ty, k = kc - 1;
+      bool inter = false;
       if (i <= nx && j <= ny + 1) {
-        const double dxf = g.dxf[i - 1];
+        const double dxf = ldg(g.dxf + i - 1);
 #define CL(m, a, b) sc[cprev][m][ty + (b)][tx + (a)]
 #define CU(m, a, b) sc[ccur][m][ty + (b)][tx + (a)]
         const double dnxdx = 1. / dxf * (plane_dx(CL(0, 0, 0), CL(0, 1, 0), CL(0, 0, 1), CL(0, 1, 1)) +
@@ -198,16 +200,48 @@ __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ 
           n0 *= norminv;
           n1 *= norminv;
           n2 *= norminv;
-          const double d = thinc_intercept3(lvof, n0, n1, n2);
           double2 *o = reinterpret_cast<double2 *>(normal + ix_nrm(g, i, j, k));
           o[0] = make_double2(n0, n1);
-          o[1] = make_double2(n2, d);
+          o[1].x = n2;
+          inter = true;
         }
 #undef CL
 #undef CU
       }
+      // the intercept's Newton iteration runs in k3_intercept over a compacted
+      // list of the interfacial cells (warp-aggregated append)
+      const unsigned mask = __ballot_sync(0xffffffffu, inter);
+      if (mask) {
+        const int lane = tid & 31;
+        unsigned base = 0;
+        if (lane == __ffs(mask) - 1) base = atomicAdd(nwork, (unsigned)__popc(mask));
+        base = __shfl_sync(0xffffffffu, base, __ffs(mask) - 1);
+        if (inter) {
+          const unsigned rank = __popc(mask & ((1u << lane) - 1u));
+          work[base + rank] = (unsigned)(ix_nrm(g, i, j, k) >> 2);
+        }
+      }
     }
     __syncthreads();
+  }
+}
+
+// k3_intercept: THINC intercept of every listed interfacial cell (the normal
+// vector is already stored); one thread per cell, grid-stride over the list
+__global__ void __launch_bounds__(256) k3_intercept(const double *__restrict__ vof, double *__restrict__ normal,
+                                                   const unsigned *__restrict__ work,
+                                                   const unsigned *__restrict__ nwork, Grid3 g) {
+  const unsigned n = *nwork;
+  const int nx = g.nx, rows = g.ny + 2;
+  for (unsigned w = blockIdx.x * blockDim.x + threadIdx.x; w < n; w += gridDim.x * blockDim.x) {
+    const unsigned c = work[w];
+    const int i = 1 + (int)(c % (unsigned)nx);
+    const unsigned r = c / (unsigned)nx;
+    const int j = (int)(r % (unsigned)rows), k = (int)(r / (unsigned)rows);
+    double *o = normal + 4L * c;
+    const double2 a = *reinterpret_cast<const double2 *>(o);
+    const double n2 = o[2];
+    o[3] = thinc_intercept3(ldg(vof + ix_vof(g, i, j, k)), a.x, a.y, n2);
   }
 }
 
@@ -220,21 +254,21 @@ __global__ void k3_force(const double *__restrict__ vof, const double *__restric
   const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
   const int k = 1 + blockIdx.z;
   if (i > g.nx || j > g.ny) return;
-  const double vc = vof[ix_vof(g, i, j, k)];
-  const double cc = curv[ix_cc(g, i, j, k)];
+  const double vc = ldg(vof + ix_vof(g, i, j, k));
+  const double cc = ldg(curv + ix_cc(g, i, j, k));
   if (i >= 2) {
-    const double grad = 1. / g.dxc[i - 1] * (-vof[ix_vof(g, i - 1, j, k)] + vc);
-    const double kappa = 0.5 * (+curv[ix_cc(g, i - 1, j, k)] + cc);
+    const double grad = 1. / ldg(g.dxc + i - 1) * (-ldg(vof + ix_vof(g, i - 1, j, k)) + vc);
+    const double kappa = 0.5 * (+ldg(curv + ix_cc(g, i - 1, j, k)) + cc);
     ifrcx[ix_srcx(g, i, j, k)] = tension * grad * kappa;
   }
   {
-    const double grad = 1. / g.dy * (-vof[ix_vof(g, i, j - 1, k)] + vc);
-    const double kappa = 0.5 * (+curv[ix_cc(g, i, j - 1, k)] + cc);
+    const double grad = 1. / g.dy * (-ldg(vof + ix_vof(g, i, j - 1, k)) + vc);
+    const double kappa = 0.5 * (+ldg(curv + ix_cc(g, i, j - 1, k)) + cc);
     ifrcy[ix_src(g, i, j, k)] = tension * grad * kappa;
   }
   {
-    const double grad = 1. / g.dz * (-vof[ix_vof(g, i, j, k - 1)] + vc);
-    const double kappa = 0.5 * (+curv[ix_cc(g, i, j, k - 1)] + cc);
+    const double grad = 1. / g.dz * (-ldg(vof + ix_vof(g, i, j, k - 1)) + vc);
+    const double kappa = 0.5 * (+ldg(curv + ix_cc(g, i, j, k - 1)) + cc);
     ifrcz[ix_src(g, i, j, k)] = tension * grad * kappa;
   }
 }
@@ -247,7 +281,7 @@ __device__ __forceinline__ double indicator3(const double *n, double x0, double 
 
 __device__ __forceinline__ void load_normal(const double *__restrict__ normal, long idx, double *n) {
   const double2 *p = reinterpret_cast<const double2 *>(normal + idx);
-  const double2 a = p[0], b = p[1];
+  const double2 a = __ldg(p), b = __ldg(p + 1);
   n[0] = a.x;
   n[1] = a.y;
   n[2] = b.x;
@@ -257,10 +291,10 @@ __device__ __forceinline__ void load_normal(const double *__restrict__ normal, l
 // flux through the x face i (i in [2, nx]) of row (j, k)
 __device__ __forceinline__ double flux_x(const double *__restrict__ vof, const double *__restrict__ ux,
                                          const double *__restrict__ normal, const Grid3 &g, int i, int j, int k) {
-  const double vel = ux[ix_ux(g, i, j, k)];
+  const double vel = ldg(ux + ix_ux(g, i, j, k));
   const int ii = vel < 0. ? i : i - 1;
   const double x = vel < 0. ? -0.5 : +0.5;
-  const double lvof = vof[ix_vof(g, ii, j, k)];
+  const double lvof = ldg(vof + ix_vof(g, ii, j, k));
   if (lvof < kVofMin || 1. - kVofMin < lvof) return vel * lvof;
   double n[4];
   load_normal(normal, ix_nrm(g, ii, j, k), n);
@@ -276,10 +310,10 @@ __device__ __forceinline__ double flux_x(const double *__restrict__ vof, const d
 // flux through the y face j (j in [1, ny+1]) of column (i, k)
 __device__ __forceinline__ double flux_y(const double *__restrict__ vof, const double *__restrict__ uy,
                                          const double *__restrict__ normal, const Grid3 &g, int i, int j, int k) {
-  const double vel = uy[ix_cc(g, i, j, k)];
+  const double vel = ldg(uy + ix_cc(g, i, j, k));
   const int jj = vel < 0. ? j : j - 1;
   const double y = vel < 0. ? -0.5 : +0.5;
-  const double lvof = vof[ix_vof(g, i, jj, k)];
+  const double lvof = ldg(vof + ix_vof(g, i, jj, k));
   if (lvof < kVofMin || 1. - kVofMin < lvof) return vel * lvof;
   double n[4];
   load_normal(normal, ix_nrm(g, i, jj, k), n);
@@ -295,10 +329,10 @@ __device__ __forceinline__ double flux_y(const double *__restrict__ vof, const d
 // flux through the z face k (k in [1, nz+1]) of column (i, j)
 __device__ __forceinline__ double flux_z(const double *__restrict__ vof, const double *__restrict__ uz,
                                          const double *__restrict__ normal, const Grid3 &g, int i, int j, int k) {
-  const double vel = uz[ix_cc(g, i, j, k)];
+  const double vel = ldg(uz + ix_cc(g, i, j, k));
   const int kk = vel < 0. ? k : k - 1;
   const double z = vel < 0. ? -0.5 : +0.5;
-  const double lvof = vof[ix_vof(g, i, j, kk)];
+  const double lvof = ldg(vof + ix_vof(g, i, j, kk));
   if (lvof < kVofMin || 1. - kVofMin < lvof) return vel * lvof;
   double n[4];
   load_normal(normal, ix_nrm(g, i, j, kk), n);
@@ -339,7 +373,7 @@ __global__ void __launch_bounds__(V3X * V3Y) k3_vof_advect(const double *__restr
   const int tx = tid % V3X, ty = tid / V3X;
   const int i = i0 + tx, j = j0 + ty;
   const bool mine = (i <= nx && j <= ny);
-  const double dt = *dtp;
+  const double dt = ldg(dtp);
   double fz_lo = 0.;
   if (mine) fz_lo = flux_z(vof, uz, normal, g, i, j, k0);
   for (int k = k0; k < kend; k++) {
@@ -362,28 +396,29 @@ __global__ void __launch_bounds__(V3X * V3Y) k3_vof_advect(const double *__restr
     __syncthreads();
     if (mine) {
       double s = 0.;
-      s += 1. / g.dxf[i - 1] * (+fx[ty][tx] - fx[ty][tx + 1]);
+      s += 1. / ldg(g.dxf + i - 1) * (+fx[ty][tx] - fx[ty][tx + 1]);
       s += 1. / g.dy * (+fy[ty][tx] - fy[ty + 1][tx]);
       s += 1. / g.dz * (+fz_lo - fz_hi);
       const long is = ix_src(g, i, j, k);
       src_a[is] = s;
-      double v = vof[ix_vof(g, i, j, k)];
+      double v = ldg(vof + ix_vof(g, i, j, k));
       v += dt * rk.a * s;
-      if (use_b) v += dt * rk.b * src_b[is];
+      if (use_b) v += dt * rk.b * ldg(src_b + is);
       // images: two halo layers in y and z
-      int js[2], ks[2], nj = 1, nk = 1;
-      js[0] = j;
-      ks[0] = k;
-      if (j >= ny - 1) js[nj++] = j - ny;
-      else if (j <= 2) js[nj++] = j + ny;
-      if (k >= nz - 1) ks[nk++] = k - nz;
-      else if (k <= 2) ks[nk++] = k + nz;
-      for (int a = 0; a < nk; a++)
-        for (int b = 0; b < nj; b++) {
-          vof_new[ix_vof(g, i, js[b], ks[a])] = v;
-          if (1 == i) vof_new[ix_vof(g, 0, js[b], ks[a])] = 0.;
-          if (nx == i) vof_new[ix_vof(g, nx + 1, js[b], ks[a])] = 0.;
-        }
+      const bool hj = (j >= ny - 1) || (j <= 2), hk = (k >= nz - 1) || (k <= 2);
+      const int j2 = (j >= ny - 1) ? j - ny : j + ny;
+      const int k2 = (k >= nz - 1) ? k - nz : k + nz;
+      auto put = [&](int jj, int kk) {
+        vof_new[ix_vof(g, i, jj, kk)] = v;
+        if (1 == i) vof_new[ix_vof(g, 0, jj, kk)] = 0.;
+        if (nx == i) vof_new[ix_vof(g, nx + 1, jj, kk)] = 0.;
+      };
+      put(j, k);
+      if (hj) put(j2, k);
+      if (hk) {
+        put(j, k2);
+        if (hj) put(j2, k2);
+      }
     }
     fz_lo = fz_hi;
     __syncthreads();

@@ -76,10 +76,10 @@ __global__ void k3_tdm_coef(const double *__restrict__ lap_ux, const double *__r
 __device__ __forceinline__ void rhs_ux(const Predict3Args &a, const Grid3 &g, int i, int j, int k, double &sa,
                                        double &sg) {
   const double *ux = a.ux, *uy = a.uy, *uz = a.uz;
-  const double dxc = g.dxc[i - 1], dxf = g.dxf[i - 1];
-  const double xm = ux[ix_ux(g, i - 1, j, k)], xc = ux[ix_ux(g, i, j, k)], xp = ux[ix_ux(g, i + 1, j, k)];
-  const double ys = ux[ix_ux(g, i, j - 1, k)], yn = ux[ix_ux(g, i, j + 1, k)];
-  const double zs = ux[ix_ux(g, i, j, k - 1)], zn = ux[ix_ux(g, i, j, k + 1)];
+  const double dxc = ldg(g.dxc + i - 1), dxf = ldg(g.dxf + i - 1);
+  const double xm = ldg(ux + ix_ux(g, i - 1, j, k)), xc = ldg(ux + ix_ux(g, i, j, k)), xp = ldg(ux + ix_ux(g, i + 1, j, k));
+  const double ys = ldg(ux + ix_ux(g, i, j - 1, k)), yn = ldg(ux + ix_ux(g, i, j + 1, k));
+  const double zs = ldg(ux + ix_ux(g, i, j, k - 1)), zn = ldg(ux + ix_ux(g, i, j, k + 1));
   sa = 0.;
   sg = 0.;
   {
@@ -87,40 +87,40 @@ __device__ __forceinline__ void rhs_ux(const Predict3Args &a, const Grid3 &g, in
     const double l = +0.5 / dxc * ul, u = -0.5 / dxc * uu, cc = -l - u;
     sa += +l * xm + cc * xc + u * xp;
   }
-  const double w_xm = 0.5 * g.dxf[i - 2] / dxc, w_xp = 0.5 * dxf / dxc;
+  const double w_xm = 0.5 * ldg(g.dxf + i - 2) / dxc, w_xp = 0.5 * dxf / dxc;
   {
-    const double ul = w_xm * uy[ix_cc(g, i - 1, j, k)] + w_xp * uy[ix_cc(g, i, j, k)];
-    const double uu = w_xm * uy[ix_cc(g, i - 1, j + 1, k)] + w_xp * uy[ix_cc(g, i, j + 1, k)];
+    const double ul = w_xm * ldg(uy + ix_cc(g, i - 1, j, k)) + w_xp * ldg(uy + ix_cc(g, i, j, k));
+    const double uu = w_xm * ldg(uy + ix_cc(g, i - 1, j + 1, k)) + w_xp * ldg(uy + ix_cc(g, i, j + 1, k));
     const double l = +0.5 / g.dy * ul, u = -0.5 / g.dy * uu, cc = -l - u;
     sa += +l * ys + cc * xc + u * yn;
   }
   {
-    const double ul = w_xm * uz[ix_cc(g, i - 1, j, k)] + w_xp * uz[ix_cc(g, i, j, k)];
-    const double uu = w_xm * uz[ix_cc(g, i - 1, j, k + 1)] + w_xp * uz[ix_cc(g, i, j, k + 1)];
+    const double ul = w_xm * ldg(uz + ix_cc(g, i - 1, j, k)) + w_xp * ldg(uz + ix_cc(g, i, j, k));
+    const double uu = w_xm * ldg(uz + ix_cc(g, i - 1, j, k + 1)) + w_xp * ldg(uz + ix_cc(g, i, j, k + 1));
     const double l = +0.5 / g.dz * ul, u = -0.5 / g.dz * uu, cc = -l - u;
     sa += +l * zs + cc * xc + u * zn;
   }
   const double *lx = a.lap_ux + 3 * (i - 2);
-  sg += a.m_dif * (+lx[0] * xm + lx[1] * xc + lx[2] * xp);
+  sg += a.m_dif * (+ldg(lx + 0) * xm + ldg(lx + 1) * xc + ldg(lx + 2) * xp);
   sa += a.m_dif * (+a.lapy[0] * ys + a.lapy[1] * xc + a.lapy[2] * yn);
   sa += a.m_dif * (+a.lapz[0] * zs + a.lapz[1] * xc + a.lapz[2] * zn);
-  sg -= 1. / dxc * (-a.p[ix_cc(g, i - 1, j, k)] + a.p[ix_cc(g, i, j, k)]);
-  if (a.add_buoyancy) sa += +0.5 * a.t[ix_cc(g, i - 1, j, k)] + 0.5 * a.t[ix_cc(g, i, j, k)];
-  sa += a.ifrcx[ix_srcx(g, i, j, k)];
+  sg -= 1. / dxc * (-ldg(a.p + ix_cc(g, i - 1, j, k)) + ldg(a.p + ix_cc(g, i, j, k)));
+  if (a.add_buoyancy) sa += +0.5 * ldg(a.t + ix_cc(g, i - 1, j, k)) + 0.5 * ldg(a.t + ix_cc(g, i, j, k));
+  sa += ldg(a.ifrcx + ix_srcx(g, i, j, k));
 }
 
 __device__ __forceinline__ void rhs_uy(const Predict3Args &a, const Grid3 &g, int i, int j, int k, double &sa,
                                        double &sg) {
   const double *ux = a.ux, *uy = a.uy, *uz = a.uz;
-  const double dxf = g.dxf[i - 1];
-  const double xm = uy[ix_cc(g, i - 1, j, k)], xc = uy[ix_cc(g, i, j, k)], xp = uy[ix_cc(g, i + 1, j, k)];
-  const double ys = uy[ix_cc(g, i, j - 1, k)], yn = uy[ix_cc(g, i, j + 1, k)];
-  const double zs = uy[ix_cc(g, i, j, k - 1)], zn = uy[ix_cc(g, i, j, k + 1)];
+  const double dxf = ldg(g.dxf + i - 1);
+  const double xm = ldg(uy + ix_cc(g, i - 1, j, k)), xc = ldg(uy + ix_cc(g, i, j, k)), xp = ldg(uy + ix_cc(g, i + 1, j, k));
+  const double ys = ldg(uy + ix_cc(g, i, j - 1, k)), yn = ldg(uy + ix_cc(g, i, j + 1, k));
+  const double zs = ldg(uy + ix_cc(g, i, j, k - 1)), zn = ldg(uy + ix_cc(g, i, j, k + 1));
   sa = 0.;
   sg = 0.;
   {
-    const double ul = +0.5 * ux[ix_ux(g, i, j - 1, k)] + 0.5 * ux[ix_ux(g, i, j, k)];
-    const double uu = +0.5 * ux[ix_ux(g, i + 1, j - 1, k)] + 0.5 * ux[ix_ux(g, i + 1, j, k)];
+    const double ul = +0.5 * ldg(ux + ix_ux(g, i, j - 1, k)) + 0.5 * ldg(ux + ix_ux(g, i, j, k));
+    const double uu = +0.5 * ldg(ux + ix_ux(g, i + 1, j - 1, k)) + 0.5 * ldg(ux + ix_ux(g, i + 1, j, k));
     const double l = +0.5 / dxf * ul, u = -0.5 / dxf * uu, cc = -l - u;
     sa += +l * xm + cc * xc + u * xp;
   }
@@ -130,37 +130,37 @@ __device__ __forceinline__ void rhs_uy(const Predict3Args &a, const Grid3 &g, in
     sa += +l * ys + cc * xc + u * yn;
   }
   {
-    const double ul = +0.5 * uz[ix_cc(g, i, j - 1, k)] + 0.5 * uz[ix_cc(g, i, j, k)];
-    const double uu = +0.5 * uz[ix_cc(g, i, j - 1, k + 1)] + 0.5 * uz[ix_cc(g, i, j, k + 1)];
+    const double ul = +0.5 * ldg(uz + ix_cc(g, i, j - 1, k)) + 0.5 * ldg(uz + ix_cc(g, i, j, k));
+    const double uu = +0.5 * ldg(uz + ix_cc(g, i, j - 1, k + 1)) + 0.5 * ldg(uz + ix_cc(g, i, j, k + 1));
     const double l = +0.5 / g.dz * ul, u = -0.5 / g.dz * uu, cc = -l - u;
     sa += +l * zs + cc * xc + u * zn;
   }
   const double *lx = a.lap_cc + 3 * (i - 1);
-  sg += a.m_dif * (+lx[0] * xm + lx[1] * xc + lx[2] * xp);
+  sg += a.m_dif * (+ldg(lx + 0) * xm + ldg(lx + 1) * xc + ldg(lx + 2) * xp);
   sa += a.m_dif * (+a.lapy[0] * ys + a.lapy[1] * xc + a.lapy[2] * yn);
   sa += a.m_dif * (+a.lapz[0] * zs + a.lapz[1] * xc + a.lapz[2] * zn);
-  sg -= 1. / g.dy * (-a.p[ix_cc(g, i, j - 1, k)] + a.p[ix_cc(g, i, j, k)]);
-  sa += a.ifrcy[ix_src(g, i, j, k)];
+  sg -= 1. / g.dy * (-ldg(a.p + ix_cc(g, i, j - 1, k)) + ldg(a.p + ix_cc(g, i, j, k)));
+  sa += ldg(a.ifrcy + ix_src(g, i, j, k));
 }
 
 __device__ __forceinline__ void rhs_uz(const Predict3Args &a, const Grid3 &g, int i, int j, int k, double &sa,
                                        double &sg) {
   const double *ux = a.ux, *uy = a.uy, *uz = a.uz;
-  const double dxf = g.dxf[i - 1];
-  const double xm = uz[ix_cc(g, i - 1, j, k)], xc = uz[ix_cc(g, i, j, k)], xp = uz[ix_cc(g, i + 1, j, k)];
-  const double ys = uz[ix_cc(g, i, j - 1, k)], yn = uz[ix_cc(g, i, j + 1, k)];
-  const double zs = uz[ix_cc(g, i, j, k - 1)], zn = uz[ix_cc(g, i, j, k + 1)];
+  const double dxf = ldg(g.dxf + i - 1);
+  const double xm = ldg(uz + ix_cc(g, i - 1, j, k)), xc = ldg(uz + ix_cc(g, i, j, k)), xp = ldg(uz + ix_cc(g, i + 1, j, k));
+  const double ys = ldg(uz + ix_cc(g, i, j - 1, k)), yn = ldg(uz + ix_cc(g, i, j + 1, k));
+  const double zs = ldg(uz + ix_cc(g, i, j, k - 1)), zn = ldg(uz + ix_cc(g, i, j, k + 1));
   sa = 0.;
   sg = 0.;
   {
-    const double ul = +0.5 * ux[ix_ux(g, i, j, k - 1)] + 0.5 * ux[ix_ux(g, i, j, k)];
-    const double uu = +0.5 * ux[ix_ux(g, i + 1, j, k - 1)] + 0.5 * ux[ix_ux(g, i + 1, j, k)];
+    const double ul = +0.5 * ldg(ux + ix_ux(g, i, j, k - 1)) + 0.5 * ldg(ux + ix_ux(g, i, j, k));
+    const double uu = +0.5 * ldg(ux + ix_ux(g, i + 1, j, k - 1)) + 0.5 * ldg(ux + ix_ux(g, i + 1, j, k));
     const double l = +0.5 / dxf * ul, u = -0.5 / dxf * uu, cc = -l - u;
     sa += +l * xm + cc * xc + u * xp;
   }
   {
-    const double ul = +0.5 * uy[ix_cc(g, i, j, k - 1)] + 0.5 * uy[ix_cc(g, i, j, k)];
-    const double uu = +0.5 * uy[ix_cc(g, i, j + 1, k - 1)] + 0.5 * uy[ix_cc(g, i, j + 1, k)];
+    const double ul = +0.5 * ldg(uy + ix_cc(g, i, j, k - 1)) + 0.5 * ldg(uy + ix_cc(g, i, j, k));
+    const double uu = +0.5 * ldg(uy + ix_cc(g, i, j + 1, k - 1)) + 0.5 * ldg(uy + ix_cc(g, i, j + 1, k));
     const double l = +0.5 / g.dy * ul, u = -0.5 / g.dy * uu, cc = -l - u;
     sa += +l * ys + cc * xc + u * yn;
   }
@@ -170,38 +170,38 @@ __device__ __forceinline__ void rhs_uz(const Predict3Args &a, const Grid3 &g, in
     sa += +l * zs + cc * xc + u * zn;
   }
   const double *lx = a.lap_cc + 3 * (i - 1);
-  sg += a.m_dif * (+lx[0] * xm + lx[1] * xc + lx[2] * xp);
+  sg += a.m_dif * (+ldg(lx + 0) * xm + ldg(lx + 1) * xc + ldg(lx + 2) * xp);
   sa += a.m_dif * (+a.lapy[0] * ys + a.lapy[1] * xc + a.lapy[2] * yn);
   sa += a.m_dif * (+a.lapz[0] * zs + a.lapz[1] * xc + a.lapz[2] * zn);
-  sg -= 1. / g.dz * (-a.p[ix_cc(g, i, j, k - 1)] + a.p[ix_cc(g, i, j, k)]);
-  sa += a.ifrcz[ix_src(g, i, j, k)];
+  sg -= 1. / g.dz * (-ldg(a.p + ix_cc(g, i, j, k - 1)) + ldg(a.p + ix_cc(g, i, j, k)));
+  sa += ldg(a.ifrcz + ix_src(g, i, j, k));
 }
 
 __device__ __forceinline__ void rhs_t(const Predict3Args &a, const Grid3 &g, int i, int j, int k, double &sa,
                                       double &sg) {
   const double *ux = a.ux, *uy = a.uy, *uz = a.uz, *t = a.t;
-  const double dxf = g.dxf[i - 1];
-  const double xm = t[ix_cc(g, i - 1, j, k)], xc = t[ix_cc(g, i, j, k)], xp = t[ix_cc(g, i + 1, j, k)];
-  const double ys = t[ix_cc(g, i, j - 1, k)], yn = t[ix_cc(g, i, j + 1, k)];
-  const double zs = t[ix_cc(g, i, j, k - 1)], zn = t[ix_cc(g, i, j, k + 1)];
+  const double dxf = ldg(g.dxf + i - 1);
+  const double xm = ldg(t + ix_cc(g, i - 1, j, k)), xc = ldg(t + ix_cc(g, i, j, k)), xp = ldg(t + ix_cc(g, i + 1, j, k));
+  const double ys = ldg(t + ix_cc(g, i, j - 1, k)), yn = ldg(t + ix_cc(g, i, j + 1, k));
+  const double zs = ldg(t + ix_cc(g, i, j, k - 1)), zn = ldg(t + ix_cc(g, i, j, k + 1));
   sa = 0.;
   sg = 0.;
   {
-    const double l = +0.5 / dxf * ux[ix_ux(g, i, j, k)], u = -0.5 / dxf * ux[ix_ux(g, i + 1, j, k)], cc = -l - u;
+    const double l = +0.5 / dxf * ldg(ux + ix_ux(g, i, j, k)), u = -0.5 / dxf * ldg(ux + ix_ux(g, i + 1, j, k)), cc = -l - u;
     sa += +l * xm + cc * xc + u * xp;
   }
   {
-    const double l = +0.5 / g.dy * uy[ix_cc(g, i, j, k)], u = -0.5 / g.dy * uy[ix_cc(g, i, j + 1, k)];
+    const double l = +0.5 / g.dy * ldg(uy + ix_cc(g, i, j, k)), u = -0.5 / g.dy * ldg(uy + ix_cc(g, i, j + 1, k));
     const double cc = -l - u;
     sa += +l * ys + cc * xc + u * yn;
   }
   {
-    const double l = +0.5 / g.dz * uz[ix_cc(g, i, j, k)], u = -0.5 / g.dz * uz[ix_cc(g, i, j, k + 1)];
+    const double l = +0.5 / g.dz * ldg(uz + ix_cc(g, i, j, k)), u = -0.5 / g.dz * ldg(uz + ix_cc(g, i, j, k + 1));
     const double cc = -l - u;
     sa += +l * zs + cc * xc + u * zn;
   }
   const double *lx = a.lap_cc + 3 * (i - 1);
-  sg += a.t_dif * (+lx[0] * xm + lx[1] * xc + lx[2] * xp);
+  sg += a.t_dif * (+ldg(lx + 0) * xm + ldg(lx + 1) * xc + ldg(lx + 2) * xp);
   sa += a.t_dif * (+a.lapy[0] * ys + a.lapy[1] * xc + a.lapy[2] * yn);
   sa += a.t_dif * (+a.lapz[0] * zs + a.lapz[1] * xc + a.lapz[2] * zn);
 }
@@ -233,7 +233,7 @@ __global__ void __launch_bounds__(256) k3_predict(Predict3Args a) {
     const int p0 = c * PC;
     for (int w = tid; w < 9 * PC; w += 256) {
       const int r = w / PC, q = w - r * PC;
-      sco[r][q] = (p0 + q < nx) ? a.coef[(size_t)r * nx + p0 + q] : 0.;
+      sco[r][q] = (p0 + q < nx) ? ldg(a.coef + (size_t)r * nx + p0 + q) : 0.;
     }
 #pragma unroll 1
     for (int m = 0; m < 4; m++) {
@@ -248,7 +248,7 @@ __global__ void __launch_bounds__(256) k3_predict(Predict3Args a) {
         rhs_ux(a, g, i, j, k, sa, sg);
         const long is = ix_srcx(g, i, j, k);
         a.sa[0][is] = sa;
-        const double sb = a.use_b ? cb * a.sb[0][is] : 0.;
+        const double sb = a.use_b ? cb * ldg(a.sb[0] + is) : 0.;
         sd[0][ll][tx] = +ca * sa + sb + cg * sg;
       }
       if (p < nx) {
@@ -257,15 +257,15 @@ __global__ void __launch_bounds__(256) k3_predict(Predict3Args a) {
         double sa, sg;
         rhs_uy(a, g, i, j, k, sa, sg);
         a.sa[1][is] = sa;
-        double sb = a.use_b ? cb * a.sb[1][is] : 0.;
+        double sb = a.use_b ? cb * ldg(a.sb[1] + is) : 0.;
         sd[1][ll][tx] = +ca * sa + sb + cg * sg;
         rhs_uz(a, g, i, j, k, sa, sg);
         a.sa[2][is] = sa;
-        sb = a.use_b ? cb * a.sb[2][is] : 0.;
+        sb = a.use_b ? cb * ldg(a.sb[2] + is) : 0.;
         sd[2][ll][tx] = +ca * sa + sb + cg * sg;
         rhs_t(a, g, i, j, k, sa, sg);
         a.sa[3][is] = sa;
-        sb = a.use_b ? cb * a.sb[3][is] : 0.;
+        sb = a.use_b ? cb * ldg(a.sb[3] + is) : 0.;
         sd[3][ll][tx] = +ca * sa + sb + cg * sg;
       }
     }
@@ -310,7 +310,7 @@ __global__ void __launch_bounds__(256) k3_predict(Predict3Args a) {
     const int p0 = c * PC;
     for (int w = tid; w < 3 * PC; w += 256) {
       const int r = w / PC, q = w - r * PC;
-      sco[3 * r + 2][q] = (p0 + q < nx) ? a.coef[(size_t)(3 * r + 2) * nx + p0 + q] : 0.;
+      sco[3 * r + 2][q] = (p0 + q < nx) ? ldg(a.coef + (size_t)(3 * r + 2) * nx + p0 + q) : 0.;
     }
 #pragma unroll 1
     for (int m = 0; m < 4; m++) {
@@ -348,25 +348,23 @@ __global__ void __launch_bounds__(256) k3_predict(Predict3Args a) {
       const int p = p0 + tx;
       if (l >= nlines || p >= nx) continue;
       const int j = 1 + (int)(l % ny), k = 1 + (int)(l / ny);
-      int js[4], ks[4];
-      const int nimg = halo_images(j, k, ny, nz, js, ks);
       if (p < nx - 1) {
         const int i = p + 2;
-        const double v = a.ux[ix_ux(g, i, j, k)] + sd[0][ll][tx];
-        for (int q = 0; q < nimg; q++) a.ux_new[ix_ux(g, i, js[q], ks[q])] = v;
+        const double v = ldg(a.ux + ix_ux(g, i, j, k)) + sd[0][ll][tx];
+        for_images(j, k, ny, nz, true, [&](int jj, int kk) { a.ux_new[ix_ux(g, i, jj, kk)] = v; });
       }
       {
         const int i = p + 1;
         const long ic = ix_cc(g, i, j, k);
-        const double vy = a.uy[ic] + sd[1][ll][tx];
-        const double vz = a.uz[ic] + sd[2][ll][tx];
-        const double vt = a.t[ic] + sd[3][ll][tx];
-        for (int q = 0; q < nimg; q++) {
-          const long o = ix_cc(g, i, js[q], ks[q]);
+        const double vy = ldg(a.uy + ic) + sd[1][ll][tx];
+        const double vz = ldg(a.uz + ic) + sd[2][ll][tx];
+        const double vt = ldg(a.t + ic) + sd[3][ll][tx];
+        for_images(j, k, ny, nz, true, [&](int jj, int kk) {
+          const long o = ix_cc(g, i, jj, kk);
           a.uy_new[o] = vy;
           a.uz_new[o] = vz;
           a.t_new[o] = vt;
-        }
+        });
       }
     }
     __syncthreads();
@@ -380,27 +378,25 @@ __global__ void __launch_bounds__(256) k3_predict(Predict3Args a) {
     const long l = l0 + ll;
     if (l >= nlines) continue;
     const int j = 1 + (int)(l % ny), k = 1 + (int)(l / ny);
-    int js[4], ks[4];
-    const int nimg = halo_images(j, k, ny, nz, js, ks);
     {
       const int i = side ? nx + 1 : 1;
-      const double old = a.ux[ix_ux(g, i, j, k)];
+      const double old = ldg(a.ux + ix_ux(g, i, j, k));
       a.ux_new[ix_ux(g, i, j, k)] = 0.;
-      for (int q = 1; q < nimg; q++) a.ux_new[ix_ux(g, i, js[q], ks[q])] = old;
+      for_images(j, k, ny, nz, false, [&](int jj, int kk) { a.ux_new[ix_ux(g, i, jj, kk)] = old; });
     }
     {
       const int i = side ? nx + 1 : 0;
       const long ic = ix_cc(g, i, j, k);
-      const double oy = a.uy[ic], oz = a.uz[ic], ot = a.t[ic];
+      const double oy = ldg(a.uy + ic), oz = ldg(a.uz + ic), ot = ldg(a.t + ic);
       a.uy_new[ic] = side ? a.uy_xp : a.uy_xm;
       a.uz_new[ic] = side ? a.uz_xp : a.uz_xm;
       a.t_new[ic] = side ? a.t_xp : a.t_xm;
-      for (int q = 1; q < nimg; q++) {
-        const long o = ix_cc(g, i, js[q], ks[q]);
+      for_images(j, k, ny, nz, false, [&](int jj, int kk) {
+        const long o = ix_cc(g, i, jj, kk);
         a.uy_new[o] = oy;
         a.uz_new[o] = oz;
         a.t_new[o] = ot;
-      }
+      });
     }
   }
 }

@@ -14,70 +14,70 @@ namespace svof3 {
 
 // one thread per interior cell; the threads at i = 1 and i = nx also own the
 // wall cells of their row
-__global__ void k3_project(double *__restrict__ ux, double *__restrict__ uy, double *__restrict__ uz,
-                           double *__restrict__ p, const double *__restrict__ psi, const double *__restrict__ dtp,
-                           double gam, double m_dif, double uy_xm, double uy_xp, double uz_xm, double uz_xp,
-                           int do_vel, int do_p, Grid3 g) {
+__global__ void __launch_bounds__(256) k3_project(double *__restrict__ ux, double *__restrict__ uy,
+                                                  double *__restrict__ uz, double *__restrict__ p,
+                                                  const double *__restrict__ psi, const double *__restrict__ dtp,
+                                                  double gam, double m_dif, double uy_xm, double uy_xp,
+                                                  double uz_xm, double uz_xp, int do_vel, int do_p, Grid3 g) {
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
   const int k = 1 + blockIdx.z;
   if (i > nx || j > ny) return;
-  const double dt = *dtp;
-  int js[4], ks[4];
-  const int nimg = halo_images(j, k, ny, nz, js, ks);
-  const double psc = psi[ix_cc(g, i, j, k)];
+  const double dt = ldg(dtp);
+  const double psc = ldg(psi + ix_cc(g, i, j, k));
+  const bool wall = (1 == i || nx == i);
   if (do_vel) {
     const double prefactor = gam * dt;
+    const double pxm = ldg(psi + ix_cc(g, i - 1, j, k));
+    const double pym = ldg(psi + ix_cc(g, i, j - 1, k));
+    const double pzm = ldg(psi + ix_cc(g, i, j, k - 1));
+    const double dxc = ldg(g.dxc + i - 1);
+    const long iu = ix_ux(g, i, j, k), ic = ix_cc(g, i, j, k);
+    const double ux0 = ux[iu], uy0 = uy[ic], uz0 = uz[ic];
     // ux
     if (i >= 2) {
-      double v = ux[ix_ux(g, i, j, k)];
-      v -= prefactor / g.dxc[i - 1] * (+psc - psi[ix_cc(g, i - 1, j, k)]);
-      for (int q = 0; q < nimg; q++) ux[ix_ux(g, i, js[q], ks[q])] = v;
+      double v = ux0;
+      v -= prefactor / dxc * (+psc - pxm);
+      for_images(j, k, ny, nz, true, [&](int jj, int kk) { ux[ix_ux(g, i, jj, kk)] = v; });
     }
-    if (1 == i || nx == i) {
-      const int iw = (1 == i) ? 1 : nx + 1;
-      const double old = ux[ix_ux(g, iw, j, k)];
-      ux[ix_ux(g, iw, j, k)] = 0.;
-      for (int q = 1; q < nimg; q++) ux[ix_ux(g, iw, js[q], ks[q])] = old;
-    }
-    // uy
-    {
-      double v = uy[ix_cc(g, i, j, k)];
-      v -= prefactor / g.dy * (+psc - psi[ix_cc(g, i, j - 1, k)]);
-      for (int q = 0; q < nimg; q++) uy[ix_cc(g, i, js[q], ks[q])] = v;
-    }
-    // uz
-    {
-      double v = uz[ix_cc(g, i, j, k)];
-      v -= prefactor / g.dz * (+psc - psi[ix_cc(g, i, j, k - 1)]);
-      for (int q = 0; q < nimg; q++) uz[ix_cc(g, i, js[q], ks[q])] = v;
-    }
-    if (1 == i || nx == i) {
+    double vy = uy0;
+    vy -= prefactor / g.dy * (+psc - pym);
+    for_images(j, k, ny, nz, true, [&](int jj, int kk) { uy[ix_cc(g, i, jj, kk)] = vy; });
+    double vz = uz0;
+    vz -= prefactor / g.dz * (+psc - pzm);
+    for_images(j, k, ny, nz, true, [&](int jj, int kk) { uz[ix_cc(g, i, jj, kk)] = vz; });
+    if (wall) {
+      const int iwu = (1 == i) ? 1 : nx + 1;
+      const double old = ux[ix_ux(g, iwu, j, k)];
+      ux[ix_ux(g, iwu, j, k)] = 0.;
+      for_images(j, k, ny, nz, false, [&](int jj, int kk) { ux[ix_ux(g, iwu, jj, kk)] = old; });
       const int iw = (1 == i) ? 0 : nx + 1;
       const long o = ix_cc(g, iw, j, k);
       const double oy = uy[o], oz = uz[o];
       uy[o] = (1 == i) ? uy_xm : uy_xp;
       uz[o] = (1 == i) ? uz_xm : uz_xp;
-      for (int q = 1; q < nimg; q++) {
-        uy[ix_cc(g, iw, js[q], ks[q])] = oy;
-        uz[ix_cc(g, iw, js[q], ks[q])] = oz;
-      }
+      for_images(j, k, ny, nz, false, [&](int jj, int kk) {
+        uy[ix_cc(g, iw, jj, kk)] = oy;
+        uz[ix_cc(g, iw, jj, kk)] = oz;
+      });
     }
   }
   if (do_p) {
     const double prefactor = 0.5 * gam * dt * m_dif;
+    const double pxm = ldg(psi + ix_cc(g, i - 1, j, k));
+    const double pxp = ldg(psi + ix_cc(g, i + 1, j, k));
     double v = p[ix_cc(g, i, j, k)];
     v += psc;
-    const double dm = (-psi[ix_cc(g, i - 1, j, k)] + psc) / g.dxc[i - 1];
-    const double dp = (-psc + psi[ix_cc(g, i + 1, j, k)]) / g.dxc[i];
-    v -= prefactor / g.dxf[i - 1] * (-dm + dp);
-    for (int q = 0; q < nimg; q++) p[ix_cc(g, i, js[q], ks[q])] = v;
-    if (1 == i || nx == i) {
+    const double dm = (-pxm + psc) / ldg(g.dxc + i - 1);
+    const double dp = (-psc + pxp) / ldg(g.dxc + i);
+    v -= prefactor / ldg(g.dxf + i - 1) * (-dm + dp);
+    for_images(j, k, ny, nz, true, [&](int jj, int kk) { p[ix_cc(g, i, jj, kk)] = v; });
+    if (wall) {
       const int iw = (1 == i) ? 0 : nx + 1;
       const double old = p[ix_cc(g, iw, j, k)];
       p[ix_cc(g, iw, j, k)] = v;
-      for (int q = 1; q < nimg; q++) p[ix_cc(g, iw, js[q], ks[q])] = old;
+      for_images(j, k, ny, nz, false, [&](int jj, int kk) { p[ix_cc(g, iw, jj, kk)] = old; });
     }
   }
 }
@@ -147,9 +147,11 @@ __device__ __forceinline__ void two_sum_acc(double &s, double &c, double x) {
   c += err;
 }
 
-// out = {max |div u|, vof min, vof max, sum vof dx dy dz}; one block of 1024
-// threads, deterministic order
-__global__ void k3_diag(const double *__restrict__ ux, const double *__restrict__ uy, const double *__restrict__ uz,
+// out = {max |div u|, vof min, vof max, sum vof dx dy dz}; one block of
+// kDiagThreads threads, deterministic order
+constexpr int kDiagThreads = 512;
+
+__global__ void __launch_bounds__(kDiagThreads) k3_diag(const double *__restrict__ ux, const double *__restrict__ uy, const double *__restrict__ uz,
                         const double *__restrict__ vof, double *__restrict__ out, Grid3 g) {
   const int nx = g.nx, ny = g.ny;
   const long ncell = (long)nx * ny * g.nz;
@@ -168,7 +170,7 @@ __global__ void k3_diag(const double *__restrict__ ux, const double *__restrict_
     vmax = fmax(vmax, lv);
     two_sum_acc(s0, c0, lv * (dx * g.dy * g.dz));
   }
-  __shared__ double red[4][1024];
+  __shared__ double red[4][kDiagThreads];
   red[0][threadIdx.x] = dmax;
   red[1][threadIdx.x] = vmin;
   red[2][threadIdx.x] = vmax;

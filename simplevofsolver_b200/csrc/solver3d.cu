@@ -105,6 +105,8 @@ struct svof3d_solver {
   double *h_dt = nullptr;
   int h_dt_slots = 0;
   DevBuf diag;
+  // interfacial-cell worklist of the geometry kernels
+  unsigned *d_work = nullptr, *d_nwork = nullptr;
   std::map<int, cudaGraphExec_t> graphs;
 
   Grid3 grid() const { return Grid3{nx, ny, nz, dy, dz, dxf.p, dxc.p}; }
@@ -144,8 +146,12 @@ int launch_dt(svof3d_solver *s) {
 }
 
 int launch_geom(svof3d_solver *s) {
+  CK(cudaMemsetAsync(s->d_nwork, 0, sizeof(unsigned), s->stream));
   dim3 gr((s->nx + 31) / 32, (s->ny + 2 + 3) / 4, (s->nz + 2 + 7) / 8);
-  k3_geom<<<gr, 128, 0, s->stream>>>(s->vof[s->cur_v].p, s->normal.p, s->curv.p, s->grid());
+  k3_geom<<<gr, 128, 0, s->stream>>>(s->vof[s->cur_v].p, s->normal.p, s->curv.p, s->d_work, s->d_nwork,
+                                     s->grid());
+  CK_LAUNCH();
+  k3_intercept<<<148 * 8, 256, 0, s->stream>>>(s->vof[s->cur_v].p, s->normal.p, s->d_work, s->d_nwork, s->grid());
   CK_LAUNCH();
   return 0;
 }
@@ -233,19 +239,21 @@ int launch_potential(svof3d_solver *s, int rk, const std::vector<cudaEvent_t> *m
     if (marks) CK(cudaEventRecord((*marks)[q], s->stream));
     return 0;
   };
-  {
-    dim3 gr((s->nx + s->cols_y - 1) / s->cols_y, s->nz);
-    const size_t sm = sizeof(double) * 2 * (size_t)s->ny * s->cols_y;
-    k3_pois_fwd_y<<<gr, 256, sm, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->uz[s->cur_u].p, s->spec.p,
-                                              s->twf_y.p, s->d_dt, gam, s->log2ny, s->cols_y, g);
-    CK_LAUNCH();
-    if (mark(0)) return 1;
-  }
-  dim3 grz((s->nx + s->cols_z - 1) / s->cols_z, nky);
-  const size_t smz = sizeof(double) * 2 * (size_t)s->nz * s->cols_z;
-  k3_pois_z<<<grz, 256, smz, s->stream>>>(s->spec.p, s->twf_z.p, s->log2nz, s->cols_z, g);
-  CK_LAUNCH();
-  if (mark(1)) return 1;
+  auto fwd_y = [&]() -> int {
+    CK(pois_fwd_y(s->cols_y, s->stream, s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->uz[s->cur_u].p, s->spec.p,
+                  s->twf_y.p, s->d_dt, gam, s->log2ny, g));
+    return 0;
+  };
+  auto fft_z = [&](const double *tw) -> int {
+    CK(pois_z(s->cols_z, s->stream, s->spec.p, tw, s->log2nz, g));
+    return 0;
+  };
+  auto inv_y = [&]() -> int {
+    CK(pois_inv_y(s->cols_y, s->stream, s->spec.p, s->psi.p, s->twb_y.p, s->log2ny, g));
+    return 0;
+  };
+  if (fwd_y() || mark(0)) return 1;
+  if (fft_z(s->twf_z.p) || mark(1)) return 1;
   {
     const long nlines = (long)nky * s->nz;
     k3_pois_x<<<(unsigned)((nlines + kXsLines - 1) / kXsLines), 256, 0, s->stream>>>(
@@ -253,16 +261,8 @@ int launch_potential(svof3d_solver *s, int rk, const std::vector<cudaEvent_t> *m
     CK_LAUNCH();
     if (mark(2)) return 1;
   }
-  k3_pois_z<<<grz, 256, smz, s->stream>>>(s->spec.p, s->twb_z.p, s->log2nz, s->cols_z, g);
-  CK_LAUNCH();
-  if (mark(3)) return 1;
-  {
-    dim3 gr((s->nx + s->cols_y - 1) / s->cols_y, s->nz);
-    const size_t sm = sizeof(double) * 2 * (size_t)s->ny * s->cols_y;
-    k3_pois_inv_y<<<gr, 256, sm, s->stream>>>(s->spec.p, s->psi.p, s->twb_y.p, s->log2ny, s->cols_y, g);
-    CK_LAUNCH();
-    if (mark(4)) return 1;
-  }
+  if (fft_z(s->twb_z.p) || mark(3)) return 1;
+  if (inv_y() || mark(4)) return 1;
   return 0;
 }
 
@@ -437,6 +437,8 @@ int svof3d_destroy(svof3d_solver_t *s) {
   for (DevBuf *b : bufs) dfree(*b);
   if (s->d_dt) cudaFree(s->d_dt);
   if (s->d_minbits) cudaFree(s->d_minbits);
+  if (s->d_work) cudaFree(s->d_work);
+  if (s->d_nwork) cudaFree(s->d_nwork);
   if (s->h_dt) cudaFreeHost(s->h_dt);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
@@ -448,7 +450,9 @@ int svof3d_create(const svof3d_params_t *prm, const double *xf, const double *xc
   *out = nullptr;
   if (prm->nx < 4 || prm->ny < 4 || prm->nz < 4) return fail("svof3d_create: nx, ny and nz must be at least 4");
   if (!(prm->m_dif > 0.) || !(prm->t_dif > 0.)) return fail("svof3d_create: diffusivities must be positive");
-  if (prm->ny > 4096 || prm->nz > 4096) return fail("svof3d_create: ny and nz must be at most 4096");
+  if (prm->ny > 2048 || prm->nz > 2048) return fail("svof3d_create: ny and nz must be at most 2048");
+  if ((double)prm->nx * (prm->ny + 4) * (prm->nz + 4) > 4.0e9)
+    return fail("svof3d_create: %d x %d x %d cells exceed the 32-bit cell index", prm->nx, prm->ny, prm->nz);
   svof3d_solver *s = new svof3d_solver();
   s->prm = *prm;
   s->nx = prm->nx;
@@ -484,20 +488,14 @@ int svof3d_create(const svof3d_params_t *prm, const double *xf, const double *xc
   const size_t nky = ny / 2 + 1;
   if (dalloc(s->spec, 2 * nx * nky * nz) || dalloc(s->xscratch, nx * nky * nz) || dalloc(s->fw, 4 * nx * ny * nz))
     return bail();
-  // transforms: `cols` lines per block within 64 KB of shared memory
-  auto pick_cols = [](int n) {
-    int c = 16;
-    while (c > 1 && sizeof(double) * 2 * (size_t)n * c > 64 * 1024) c >>= 1;
-    return c;
-  };
+  // transforms: one line per warp, 16 / 8 / 4 lines per block by length
+  auto pick_cols = [](int n) { return n <= 128 ? 16 : (n <= 256 ? 8 : 4); };
   s->cols_y = pick_cols(s->ny);
   s->cols_z = pick_cols(s->nz);
   {
-    const size_t smy = sizeof(double) * 2 * ny * s->cols_y, smz = sizeof(double) * 2 * nz * s->cols_z;
+    const size_t smy = sizeof(double) * 2 * (ny + 1) * s->cols_y, smz = sizeof(double) * 2 * (nz + 1) * s->cols_z;
     if (smy > 200 * 1024 || smz > 200 * 1024) return fail("svof3d_create: FFT length too large"), bail();
-    if (cudaSuccess != cudaFuncSetAttribute(k3_pois_fwd_y, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy) ||
-        cudaSuccess != cudaFuncSetAttribute(k3_pois_inv_y, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy) ||
-        cudaSuccess != cudaFuncSetAttribute(k3_pois_z, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz))
+    if (cudaSuccess != pois_prepare(s->ny, s->cols_y, s->nz, s->cols_z))
       return fail("cudaFuncSetAttribute(Poisson): %s", cudaGetErrorString(cudaGetLastError())), bail();
     const size_t coef_smem = sizeof(double) * 6 * nx;
     if (coef_smem > 200 * 1024) return fail("svof3d_create: nx too large"), bail();
@@ -506,6 +504,9 @@ int svof3d_create(const svof3d_params_t *prm, const double *xf, const double *xc
       return fail("cudaFuncSetAttribute(k3_tdm_coef)"), bail();
   }
   if (cudaSuccess != cudaMalloc(&s->d_dt, sizeof(double))) return fail("cudaMalloc dt"), bail();
+  if (cudaSuccess != cudaMalloc(&s->d_work, sizeof(unsigned) * nx * (ny + 2) * (nz + 2)) ||
+      cudaSuccess != cudaMalloc(&s->d_nwork, sizeof(unsigned)))
+    return fail("cudaMalloc worklist"), bail();
   if (cudaSuccess != cudaMalloc(&s->d_minbits, sizeof(unsigned long long))) return fail("cudaMalloc"), bail();
   {
     const double one = 1.;
@@ -770,7 +771,7 @@ int svof3d_profile_step(svof3d_solver_t *s, double *ms, int *launches, int nkind
       float t = 0.f;
       cudaEventElapsedTime(&t, ev[q - 1], ev[q]);
       ms[kind[q]] += t;
-      launches[kind[q]] += (SVOF3_K_DT == kind[q] || SVOF3_K_PREDICT == kind[q]) ? 2 : 1;
+      launches[kind[q]] += (SVOF3_K_DT == kind[q] || SVOF3_K_PREDICT == kind[q] || SVOF3_K_GEOM == kind[q]) ? 2 : 1;
     }
   }
   for (cudaEvent_t x : ev) cudaEventDestroy(x);
@@ -782,7 +783,7 @@ int svof3d_profile_step(svof3d_solver_t *s, double *ms, int *launches, int nkind
 
 int svof3d_diagnostics(svof3d_solver_t *s, double *divmax, double *vofmin, double *vofmax, double *volume) {
   if (!s) return fail("null argument");
-  k3_diag<<<1, 1024, 0, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->uz[s->cur_u].p,
+  k3_diag<<<1, 512, 0, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->uz[s->cur_u].p,
                                      s->vof[s->cur_v].p, s->diag.p, s->grid());
   CK_LAUNCH();
   double h[4];

@@ -61,6 +61,23 @@ __device__ __forceinline__ int halo_images(int j, int k, int ny, int nz, int *jj
   return n;
 }
 
+// the same, as a visitor: f(j', k') for the row itself (when `self`) and for
+// each halo row that copies it; no local arrays
+template <class F>
+__device__ __forceinline__ void for_images(int j, int k, int ny, int nz, bool self, F f) {
+  const int j2 = (1 == j) ? ny + 1 : ((ny == j) ? 0 : -1);
+  const int k2 = (1 == k) ? nz + 1 : ((nz == k) ? 0 : -1);
+  if (self) f(j, k);
+  if (j2 >= 0) f(j2, k);
+  if (k2 >= 0) {
+    f(j, k2);
+    if (j2 >= 0) f(j2, k2);
+  }
+}
+
+// read-only global load through the non-coherent path
+__device__ __forceinline__ double ldg(const double *p) { return __ldg(p); }
+
 struct RK {
   double a, b, g;
 };
@@ -73,9 +90,13 @@ enum BcKind3 { BC3_ZERO = 0, BC3_DIRICHLET = 1, BC3_NEUMANN = 2, BC3_VOF = 3 };
 // interior rows
 __global__ void k3_halo_bc(double *a, int width, int nh, int ny, int nz, int kind, double lo, double hi);
 
-// interface geometry: corner normals, cell normal + intercept, curvature
+// interface geometry: corner normals, cell normal, curvature; appends the
+// interfacial cells (normal index / 4) to `work`
 __global__ void k3_geom(const double *__restrict__ vof, double *__restrict__ normal, double *__restrict__ curv,
-                        Grid3 g);
+                        unsigned *__restrict__ work, unsigned *__restrict__ nwork, Grid3 g);
+// THINC intercept of the listed cells
+__global__ void k3_intercept(const double *__restrict__ vof, double *__restrict__ normal,
+                             const unsigned *__restrict__ work, const unsigned *__restrict__ nwork, Grid3 g);
 // CSF force
 __global__ void k3_force(const double *__restrict__ vof, const double *__restrict__ curv,
                          double *__restrict__ ifrcx, double *__restrict__ ifrcy, double *__restrict__ ifrcz,
@@ -112,17 +133,17 @@ __global__ void k3_tdm_coef(const double *__restrict__ lap_ux, const double *__r
                             double *__restrict__ coef);
 
 // Poisson: spectral array S[kz][ky][i] (complex, i fastest)
-__global__ void k3_pois_fwd_y(const double *__restrict__ ux, const double *__restrict__ uy,
-                              const double *__restrict__ uz, double *__restrict__ spec,
-                              const double *__restrict__ tw, const double *__restrict__ dtp, double gam,
-                              int log2n, int cols, Grid3 g);
-__global__ void k3_pois_z(double *__restrict__ spec, const double *__restrict__ tw, int log2n, int cols, Grid3 g);
+// transforms, one warp per line, `cols` (16, 8 or 4) lines per block; the
+// launchers live beside their templates in k3_poisson.cu
+cudaError_t pois_prepare(int ny, int cols_y, int nz, int cols_z);
+cudaError_t pois_fwd_y(int cols, cudaStream_t st, const double *ux, const double *uy, const double *uz, double *spec,
+                       const double *tw, const double *dtp, double gam, int log2n, Grid3 g);
+cudaError_t pois_z(int cols, cudaStream_t st, double *spec, const double *tw, int log2n, Grid3 g);
+cudaError_t pois_inv_y(int cols, cudaStream_t st, const double *spec, double *psi, const double *tw, int log2n,
+                       Grid3 g);
 __global__ void k3_pois_x(double *__restrict__ spec, double *__restrict__ scratch, const double *__restrict__ pl,
                           const double *__restrict__ pu, const double *__restrict__ evy,
                           const double *__restrict__ evz, Grid3 g);
-__global__ void k3_pois_inv_y(const double *__restrict__ spec, double *__restrict__ psi,
-                              const double *__restrict__ tw, int log2n, int cols, Grid3 g);
-
 // projection and pressure update, in place
 __global__ void k3_project(double *__restrict__ ux, double *__restrict__ uy, double *__restrict__ uz,
                            double *__restrict__ p, const double *__restrict__ psi, const double *__restrict__ dtp,
