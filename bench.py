@@ -6,6 +6,11 @@ and three Runge-Kutta substeps of interface geometry, CSF force, THINC/QQ
 advection, momentum prediction with implicit-x Thomas solves, the Poisson
 solve and the projection.  Metric: Mcell-steps/s = cells x steps / seconds.
 
+Default workload: 512^3 cells, 128 seeded spherical droplets (radii 0.02 ..
+0.05), tanh-stretched x grid, divergence-free random velocity (rms 0.5),
+Re = 500, We = 20, FP64 (workloads.droplets3d).  The 2D workloads (the
+reference's own runnable 128 x 128 droplet and larger) stay selectable.
+
   python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME]
                   [--impl ours|reference]
 
@@ -19,7 +24,11 @@ runs an independent replica ("weak" scaling, no collective on the data path).
 
 --impl reference times the reference's own C implementation (its src/*.c
 compiled against single-rank shims, oracle/_ref) on all host cores: one
-single-rank process per core, each a replica of the same workload.
+single-rank process per core, each a replica of the same workload.  The
+reference's 3D code is not part of the mounted sources, so for the 3D
+workloads the CPU arms run the 3D restatement (oracle/svof_oracle3d.c) on a
+bounded sample of the same generator (128^3 for the baseline line, 64^3 per
+replica for the reference arm), one process per core.
 """
 from __future__ import annotations
 
@@ -57,6 +66,35 @@ ALG_WORDS = {
     "project": 7.0,            # R psi ux uy p; W ux uy p
 }
 KERNELS_PER_STEP = 2 + 3 * 9  # dt (2), then per substep: coef, geom, force, vof, predict, 3 Poisson, project
+
+# 3D FP64: the ideal dataflow's compulsory 8-byte words per cell-step (145:
+# per substep interface 10, momentum + scalar 20, Poisson 4 + 2 + 2 + 2 + 9,
+# minus the src_b reads of substep 0, plus the CFL pass) and the words each
+# kernel of this implementation moves per interior cell and launch
+ALG_BYTES_CELL_STEP_3D = 1160.0
+ALG_WORDS_3D = {
+    "dt": 3.0,                 # R ux, uy, uz
+    "geom": 2.0,               # R vof, W curv (normals of interfacial cells only)
+    "force": 5.0,              # R vof, curv; W ifrcx, ifrcy, ifrcz
+    "vof": 6.0 + 2.0 / 3.0,    # R vof, ux, uy, uz, (src_b); W vof, src_a
+    "predict": 16.0 + 8.0 / 3.0,  # R ux uy uz p t ifrc x3 (4 src_b); W ux uy uz t, 4 src_a
+    "poisson_fwd": 4.0,        # R ux, uy, uz; W half spectrum (~1 word)
+    "poisson_z": 2.0,          # R, W spectrum
+    "poisson_solve": 2.0,      # R, W spectrum
+    "poisson_inv": 2.0,        # R spectrum; W psi
+    "project": 9.0,            # R psi ux uy uz p; W ux uy uz p
+}
+# dt (2), then per substep: geom + intercept, force, vof, coef + predict,
+# 5 Poisson stages, project
+KERNELS_PER_STEP_3D = 2 + 3 * 12
+
+WORKLOADS3D = {
+    # the headline configuration: 512^3, 128 droplets, radii 0.02 .. 0.05
+    "droplets3d_512": dict(n=512, ndrops=128, radii=(0.02, 0.05)),
+    # 256^3, 32 droplets, radii 0.04 .. 0.08
+    "droplets3d_256": dict(n=256, ndrops=32, radii=(0.04, 0.08)),
+    "droplets3d_128": dict(n=128, ndrops=32, radii=(0.04, 0.08)),
+}
 
 WORKLOADS = {
     # the reference's runnable configuration: one elliptical droplet,
@@ -138,6 +176,37 @@ def cpu_reference(ic, env, steps, warmup, replicas):
     return secs
 
 
+def run_reference_arm_3d(args, wl, rank):
+    """the 3D restatement on the host cores: one single-core replica per core
+    on a 64^3 sample of the workload's generator (rank 0 only)"""
+    if rank != 0:
+        return
+    import oracle
+    ncpu = os.cpu_count() or 1
+    replicas = max(1, min(ncpu, 64))
+    n = 64
+    try:
+        secs = oracle.run_oracle3d_replicas(n, wl["ndrops"], wl["radii"], 1, args.steps, args.warmup, replicas)
+    except Exception as e:
+        print(json.dumps({"impl": "reference", "unavailable": f"3D CPU restatement failed to run: {e}"}))
+        return
+    t = max(secs)
+    value = replicas * n ** 3 * args.steps / t / 1e6
+    sample = (f"{replicas} single-core processes x {args.steps} steps of the {args.workload} generator at "
+              f"{n}^3 (3D restatement oracle/svof_oracle3d.c; the reference's 3D code is not in the mounted sources)")
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded droplet field, workloads.droplets3d)",
+        "config": {"workload": args.workload, "nx": wl["n"], "ny": wl["n"], "nz": wl["n"], "sample_n": n,
+                   "replicas": replicas},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": replicas, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
 def run_reference_arm(args, wl, ic, env, rank):
     """the reference's own C path on the host cores (rank 0 only)"""
     if rank != 0:
@@ -166,30 +235,56 @@ def run_reference_arm(args, wl, ic, env, rank):
     print(json.dumps(line))
 
 
+def _max_over_ranks(x: float, world: int) -> float:
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
-    ap.add_argument("--warmup", type=int, default=10)
-    ap.add_argument("--workload", default="droplet2d_128", choices=sorted(WORKLOADS))
+    ap.add_argument("--steps", type=int, default=None)
+    ap.add_argument("--warmup", type=int, default=None)
+    ap.add_argument("--workload", default="droplets3d_512", choices=sorted(WORKLOADS) + sorted(WORKLOADS3D))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--cpu-sample-steps", type=int, default=1000)
+    ap.add_argument("--cpu-sample-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    three_d = args.workload in WORKLOADS3D
+    if args.steps is None:
+        args.steps = 20 if three_d else 200
+    if args.warmup is None:
+        args.warmup = 3 if three_d else 10
     args.warmup = max(args.warmup, 3)
 
-    from simplevofsolver_b200.workloads import DROPLET2D_ENV, droplet2d, physical_params
-    wl = WORKLOADS[args.workload]
-    ic = droplet2d(wl["nx"], wl["ny"], uniform=wl["uniform"])
-    env = DROPLET2D_ENV
-
+    from simplevofsolver_b200.workloads import (DROPLET2D_ENV, DROPLETS3D_ENV, droplet2d, droplets3d,
+                                                physical_params)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
 
-    if args.impl == "reference":
-        run_reference_arm(args, wl, ic, env, rank)
-        return
+    if three_d:
+        wl = WORKLOADS3D[args.workload]
+        env = DROPLETS3D_ENV
+        if args.impl == "reference":
+            run_reference_arm_3d(args, wl, rank)
+            return
+        n = wl["n"]
+        ic = droplets3d(n, n, n, ndrops=wl["ndrops"], radii=wl["radii"])
+        cells = n ** 3
+    else:
+        wl = WORKLOADS[args.workload]
+        ic = droplet2d(wl["nx"], wl["ny"], uniform=wl["uniform"])
+        env = DROPLET2D_ENV
+        if args.impl == "reference":
+            run_reference_arm(args, wl, ic, env, rank)
+            return
+        cells = wl["nx"] * wl["ny"]
 
     import torch
     import torch.distributed as dist
@@ -200,16 +295,26 @@ def main():
 
     import simplevofsolver_b200 as svof
     phys = physical_params(env)
-    solver = svof.Solver(ic, phys)
-    cells = wl["nx"] * wl["ny"]
+    if three_d:
+        solver = svof.Solver3D(ic, phys)
+        names = ["ux", "uy", "uz", "p", "t", "vof"]
+        lib, store, fields = svof.solver3d.lib3(), "svof3d_store_interior", svof.FIELDS3D
+        alg_words, kernels_per_step, alg_step = ALG_WORDS_3D, KERNELS_PER_STEP_3D, ALG_BYTES_CELL_STEP_3D
+    else:
+        solver = svof.Solver(ic, phys)
+        names = ["ux", "uy", "p", "t", "vof"]
+        lib, store, fields = svof.lib(), "svof_store_interior", svof.FIELDS
+        alg_words, kernels_per_step, alg_step = ALG_WORDS, KERNELS_PER_STEP, ALG_BYTES_CELL_STEP_2D
     stream = torch.cuda.ExternalStream(solver.stream())
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # > 126 MB L2
+    # 3D: every field exceeds the 126 MB L2 many times over together; 2D:
+    # flush L2 between timed steps with a 256 MB write
+    flush = None if three_d else torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     # warm-up (also captures the step graphs)
     solver.run(args.warmup)
     torch.cuda.synchronize()
 
-    # ---- device-timed region: inputs resident in HBM, L2 flushed between steps
+    # ---- device-timed region: inputs resident in HBM
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     if world > 1:
@@ -218,66 +323,62 @@ def main():
     with ClockSampler(local_rank) as clk:
         with torch.cuda.stream(stream):
             for k in range(args.steps):
-                flush.zero_()
+                if flush is not None:
+                    flush.zero_()
                 starts[k].record(stream)
                 solver.enqueue_steps(1)
                 ends[k].record(stream)
         torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    total_ms = float(sum(step_ms))
-    if world > 1:
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    step_ms = [s_.elapsed_time(e_) for s_, e_ in zip(starts, ends)]
+    total_ms = _max_over_ranks(float(sum(step_ms)), world)
     value = world * cells * args.steps / (total_ms * 1e-3) / 1e6
     clocks = clk.summary()
 
     # ---- end to end through the C ABI with host buffers: the restart fields
     # are copied in from pinned host memory and out again every step
-    names = ["ux", "uy", "p", "t", "vof"]
-    host_in = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory().numpy()
-               for k, v in ic.fields().items()}
-    host_out = {k: torch.empty(v.shape, dtype=torch.float64).pin_memory().numpy() for k, v in host_in.items()}
-    h2d = sum(v.nbytes for v in host_in.values())
-    d2h = sum(v.nbytes for v in host_out.values()) + 8
-    e2e_steps = max(1, min(args.steps, 50))
+    host = {k: torch.from_numpy(np.ascontiguousarray(ic.fields()[k])).pin_memory().numpy() for k in names}
+    h2d = sum(v.nbytes for v in host.values())
+    d2h = h2d + 8
+    e2e_steps = max(1, min(args.steps, 3 if three_d else 50))
+    store_fn = getattr(lib, store)
     if world > 1:
         dist.barrier()
     t0 = time.perf_counter()
     for k in range(e2e_steps):
-        for n in names:
-            solver.load_interior(n, host_in[n])
+        for nm in names:
+            solver.load_interior(nm, host[nm])
         solver.integrate()
-        for n in names:
-            out = host_out[n]
-            svof._check(svof.lib().svof_store_interior(solver._h, svof.FIELDS[n], out.ctypes.data, out.size))
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+        for nm in names:
+            out = host[nm]
+            rc = store_fn(solver._h, fields[nm], out.ctypes.data, out.size)
+            if rc != 0:
+                raise RuntimeError(f"{store} failed")
+    e2e_s = _max_over_ranks(time.perf_counter() - t0, world)
     e2e_value = world * cells * e2e_steps / e2e_s / 1e6
 
     # ---- per-kernel device times (kernel by kernel, events between launches;
     # a long memset ahead lets the host enqueue the whole step first)
     prof = {}
-    nprof = 5
+    nprof = 3 if three_d else 5
     for _ in range(nprof):
         with torch.cuda.stream(stream):
             big = torch.empty(1024 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
             big.zero_()
         r = solver.profile_step()
         del big
-        for k, (ms, n) in r.items():
-            a = prof.setdefault(k, [0.0, 0])
-            a[0] += ms
-            a[1] += n
+        for k, (ms, cnt) in r.items():
+            acc = prof.setdefault(k, [0.0, 0])
+            acc[0] += ms
+            acc[1] += cnt
     dom = max(prof, key=lambda k: prof[k][0])
-    dom_ms = prof[dom][0] / max(prof[dom][1], 1)
+    # per launch of the dominant kind (predict: coefficient kernel + predictor
+    # count as one launch of the pair)
+    pair = 2 if dom in ("predict", "dt", "geom") else 1
+    dom_ms = prof[dom][0] / max(prof[dom][1] // pair, 1)
     peak, peak_kind = peaks()
-    alg_bytes = ALG_WORDS[dom] * 8.0 * cells
+    alg_bytes = alg_words[dom] * 8.0 * cells
     achieved = alg_bytes / (dom_ms * 1e-3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
@@ -290,30 +391,50 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            secs = cpu_reference(ic, env, args.cpu_sample_steps, 2, 1)
-            cpu = {"value": cells * args.cpu_sample_steps / secs[0] / 1e6, "unit": METRIC, "cores": 1,
-                   "kind": "reference",
-                   "sample": f"{args.cpu_sample_steps} steps of {args.workload}, one single-rank process"}
+            if three_d:
+                import oracle
+                sn = 128
+                ssteps = args.cpu_sample_steps or 3
+                secs = oracle.run_oracle3d_replicas(sn, wl["ndrops"], wl["radii"], 1, ssteps, 1, 1)
+                cpu = {"value": sn ** 3 * ssteps / secs[0] / 1e6, "unit": METRIC, "cores": 1, "kind": "port",
+                       "sample": (f"{ssteps} steps of the {args.workload} generator at {sn}^3 on one core (3D "
+                                  "restatement oracle/svof_oracle3d.c; the reference's 3D code is not in the "
+                                  "mounted sources)")}
+            else:
+                ssteps = args.cpu_sample_steps or 1000
+                secs = cpu_reference(ic, env, ssteps, 2, 1)
+                cpu = {"value": cells * ssteps / secs[0] / 1e6, "unit": METRIC, "cores": 1, "kind": "reference",
+                       "sample": f"{ssteps} steps of {args.workload}, one single-rank process"}
         except Exception as e:
-            cpu = {"value": None, "unit": METRIC, "cores": 0, "kind": "reference",
+            cpu = {"value": None, "unit": METRIC, "cores": 0, "kind": "port" if three_d else "reference",
                    "sample": f"unavailable: {e}"}
 
     if rank == 0:
+        if three_d:
+            config = {"workload": args.workload, "nx": wl["n"], "ny": wl["n"], "nz": wl["n"],
+                      "droplets": wl["ndrops"], "radii": list(wl["radii"]), "x_grid": "tanh-stretched (1.5)",
+                      "poisson": "r2c-y + dft-z + thomas-x", "precision": "fp64",
+                      "l2": "not flushed: inputs larger than L2 (%.1f GB of fields resident)" % (
+                          35.5 * cells * 8 / 1e9),
+                      "parallelism": f"replicas{world}"}
+        else:
+            config = {"workload": args.workload, "nx": wl["nx"], "ny": wl["ny"], "uniform_x": wl["uniform"],
+                      "poisson": "dct-x + periodic thomas-y" if wl["uniform"] else "r2c-y + thomas-x",
+                      "l2": "flushed between timed steps (256 MB write)", "parallelism": f"replicas{world}"}
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded droplet field, workloads.droplet2d)",
-            "config": {"workload": args.workload, "nx": wl["nx"], "ny": wl["ny"], "uniform_x": wl["uniform"],
-                       "poisson": "dct-x + periodic thomas-y" if wl["uniform"] else "r2c-y + thomas-x",
-                       "l2": "flushed between timed steps (256 MB write)", "parallelism": f"replicas{world}"},
+            "data": ("synthetic (seeded droplet field, workloads.droplets3d)" if three_d else
+                     "synthetic (seeded droplet field, workloads.droplet2d)"),
+            "config": config,
             "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "steps": e2e_steps},
-            "gpu_launches": KERNELS_PER_STEP * args.steps,
+            "gpu_launches": kernels_per_step * args.steps,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
                          "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": dom_ms,
-                         "step_frac": value * 1e6 * ALG_BYTES_CELL_STEP_2D / 1e9 / peak},
+                         "step_frac": value * 1e6 * alg_step / 1e9 / peak},
             "kernel_ms_per_step": {k: v[0] / nprof for k, v in prof.items()},
             "kernel_share": {k: v[0] / total_prof for k, v in prof.items()},
             "cpu_baseline": cpu,

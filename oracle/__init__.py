@@ -393,3 +393,28 @@ def run_reference_replicas(ic, env: dict, nsteps: int, warmup: int, replicas: in
                 raise RuntimeError("reference replica failed")
             secs.append(float(np.load(out_npz)["seconds"]))
     return secs
+
+
+def run_oracle3d_replicas(n: int, ndrops: int, radii, seed: int, nsteps: int, warmup: int, replicas: int,
+                          timeout: float = 3600.0):
+    """``replicas`` independent single-core processes of the 3D restatement on
+    the seeded droplet field at n^3 (``_oracle3d_runner.py``), started
+    together; returns the per-replica seconds of the ``nsteps`` timed steps."""
+    import subprocess
+    import sys
+    with tempfile.TemporaryDirectory() as d:
+        envs = dict(os.environ)
+        envs["OMP_NUM_THREADS"] = "1"
+        procs = []
+        for r in range(replicas):
+            out = os.path.join(d, f"o{r}.npz")
+            cmd = [sys.executable, os.path.join(HERE, "_oracle3d_runner.py"), str(n), str(ndrops), repr(radii[0]),
+                   repr(radii[1]), str(seed), str(nsteps), str(warmup), out]
+            procs.append((subprocess.Popen(cmd, env=envs, stdout=subprocess.DEVNULL), out))
+        secs = []
+        for pr, out in procs:
+            pr.wait(timeout=timeout)
+            if pr.returncode != 0:
+                raise RuntimeError("3D oracle replica failed")
+            secs.append(float(np.load(out)["seconds"]))
+    return secs

@@ -70,145 +70,176 @@ __global__ void k3_tdm_coef(const double *__restrict__ lap_ux, const double *__r
   }
 }
 
-// right-hand sides at (i, j, k): the explicit part into sa, the x-implicit
-// diffusion and the pressure gradient into sg, in the restatement's order
-// (advection x, y, z; diffusion x, y, z; pressure; buoyancy; surface)
-__device__ __forceinline__ void rhs_ux(const Predict3Args &a, const Grid3 &g, int i, int j, int k, double &sa,
-                                       double &sg) {
-  const double *ux = a.ux, *uy = a.uy, *uz = a.uz;
-  const double dxc = ldg(g.dxc + i - 1), dxf = ldg(g.dxf + i - 1);
-  const double xm = ldg(ux + ix_ux(g, i - 1, j, k)), xc = ldg(ux + ix_ux(g, i, j, k)), xp = ldg(ux + ix_ux(g, i + 1, j, k));
-  const double ys = ldg(ux + ix_ux(g, i, j - 1, k)), yn = ldg(ux + ix_ux(g, i, j + 1, k));
-  const double zs = ldg(ux + ix_ux(g, i, j, k - 1)), zn = ldg(ux + ix_ux(g, i, j, k + 1));
-  sa = 0.;
-  sg = 0.;
-  {
-    const double ul = +0.5 * xm + 0.5 * xc, uu = +0.5 * xc + 0.5 * xp;
-    const double l = +0.5 / dxc * ul, u = -0.5 / dxc * uu, cc = -l - u;
-    sa += +l * xm + cc * xc + u * xp;
+// Right-hand sides of one thread's cell: uy, uz and t at cell i and ux at the
+// face i + 1 (do_ux: i < nx).  The explicit part goes to sa[f], the
+// x-implicit diffusion and the pressure gradient to sg[f], in the
+// restatement's order (advection x, y, z; diffusion x, y, z; pressure;
+// buoyancy; surface).  All stencil values are loaded before any arithmetic,
+// so that the ~50 loads of a cell are in flight together.
+// Field order: 0 ux, 1 uy, 2 uz, 3 t.
+__device__ __forceinline__ void rhs4(const Predict3Args &a, const Grid3 &g, int i, int j, int k, bool do_ux,
+                                     double *sa, double *sg) {
+  const double *ux = a.ux, *uy = a.uy, *uz = a.uz, *t = a.t, *p = a.p;
+  // ---- loads
+  const double u00 = ldg(ux + ix_ux(g, i, j, k)), u10 = ldg(ux + ix_ux(g, i + 1, j, k));
+  const double u0s = ldg(ux + ix_ux(g, i, j - 1, k)), u1s = ldg(ux + ix_ux(g, i + 1, j - 1, k));
+  const double u0b = ldg(ux + ix_ux(g, i, j, k - 1)), u1b = ldg(ux + ix_ux(g, i + 1, j, k - 1));
+  const double vc = ldg(uy + ix_cc(g, i, j, k)), vxm = ldg(uy + ix_cc(g, i - 1, j, k));
+  const double vxp = ldg(uy + ix_cc(g, i + 1, j, k));
+  const double vs = ldg(uy + ix_cc(g, i, j - 1, k)), vn = ldg(uy + ix_cc(g, i, j + 1, k));
+  const double vb = ldg(uy + ix_cc(g, i, j, k - 1)), vt = ldg(uy + ix_cc(g, i, j, k + 1));
+  const double vnb = ldg(uy + ix_cc(g, i, j + 1, k - 1));
+  const double wc = ldg(uz + ix_cc(g, i, j, k)), wxm = ldg(uz + ix_cc(g, i - 1, j, k));
+  const double wxp = ldg(uz + ix_cc(g, i + 1, j, k));
+  const double ws = ldg(uz + ix_cc(g, i, j - 1, k)), wn = ldg(uz + ix_cc(g, i, j + 1, k));
+  const double wb = ldg(uz + ix_cc(g, i, j, k - 1)), wt = ldg(uz + ix_cc(g, i, j, k + 1));
+  const double wst = ldg(uz + ix_cc(g, i, j - 1, k + 1));
+  const double tc = ldg(t + ix_cc(g, i, j, k)), txm = ldg(t + ix_cc(g, i - 1, j, k));
+  const double txp = ldg(t + ix_cc(g, i + 1, j, k));
+  const double ts = ldg(t + ix_cc(g, i, j - 1, k)), tn = ldg(t + ix_cc(g, i, j + 1, k));
+  const double tb = ldg(t + ix_cc(g, i, j, k - 1)), tt = ldg(t + ix_cc(g, i, j, k + 1));
+  const double pc = ldg(p + ix_cc(g, i, j, k)), ps = ldg(p + ix_cc(g, i, j - 1, k));
+  const double pb = ldg(p + ix_cc(g, i, j, k - 1));
+  const double ify = ldg(a.ifrcy + ix_src(g, i, j, k)), ifz = ldg(a.ifrcz + ix_src(g, i, j, k));
+  const double dxf_i = ldg(g.dxf + i - 1);
+  const double lc0 = ldg(a.lap_cc + 3 * (i - 1) + 0), lc1 = ldg(a.lap_cc + 3 * (i - 1) + 1);
+  const double lc2 = ldg(a.lap_cc + 3 * (i - 1) + 2);
+  double u20 = 0., u1n = 0., u1t = 0., v1n = 0., w1t = 0., pxp = 0., ifx = 0., dxf_i1 = 1., dxc_i1 = 1.;
+  double lu0 = 0., lu1 = 0., lu2 = 0.;
+  if (do_ux) {
+    u20 = ldg(ux + ix_ux(g, i + 2, j, k));
+    u1n = ldg(ux + ix_ux(g, i + 1, j + 1, k));
+    u1t = ldg(ux + ix_ux(g, i + 1, j, k + 1));
+    v1n = ldg(uy + ix_cc(g, i + 1, j + 1, k));
+    w1t = ldg(uz + ix_cc(g, i + 1, j, k + 1));
+    pxp = ldg(p + ix_cc(g, i + 1, j, k));
+    ifx = ldg(a.ifrcx + ix_srcx(g, i + 1, j, k));
+    dxf_i1 = ldg(g.dxf + i);
+    dxc_i1 = ldg(g.dxc + i);
+    lu0 = ldg(a.lap_ux + 3 * (i - 1) + 0);
+    lu1 = ldg(a.lap_ux + 3 * (i - 1) + 1);
+    lu2 = ldg(a.lap_ux + 3 * (i - 1) + 2);
   }
-  const double w_xm = 0.5 * ldg(g.dxf + i - 2) / dxc, w_xp = 0.5 * dxf / dxc;
-  {
-    const double ul = w_xm * ldg(uy + ix_cc(g, i - 1, j, k)) + w_xp * ldg(uy + ix_cc(g, i, j, k));
-    const double uu = w_xm * ldg(uy + ix_cc(g, i - 1, j + 1, k)) + w_xp * ldg(uy + ix_cc(g, i, j + 1, k));
-    const double l = +0.5 / g.dy * ul, u = -0.5 / g.dy * uu, cc = -l - u;
-    sa += +l * ys + cc * xc + u * yn;
+  const double md = a.m_dif, td = a.t_dif, dy = g.dy, dz = g.dz;
+  const double *ly = a.lapy, *lz = a.lapz;
+  // ---- ux at the face iu = i + 1: xm = UX(iu-1), xc = UX(iu), xp = UX(iu+1)
+  if (do_ux) {
+    const double xm = u00, xc = u10, xp = u20, ys = u1s, yn = u1n, zs = u1b, zn = u1t;
+    const double dxc = dxc_i1;
+    double ra = 0., rg = 0.;
+    {
+      const double ul = +0.5 * xm + 0.5 * xc, uu = +0.5 * xc + 0.5 * xp;
+      const double l = +0.5 / dxc * ul, u = -0.5 / dxc * uu, cc = -l - u;
+      ra += +l * xm + cc * xc + u * xp;
+    }
+    const double w_xm = 0.5 * dxf_i / dxc, w_xp = 0.5 * dxf_i1 / dxc;
+    {
+      const double ul = w_xm * vc + w_xp * vxp;
+      const double uu = w_xm * vn + w_xp * v1n;
+      const double l = +0.5 / dy * ul, u = -0.5 / dy * uu, cc = -l - u;
+      ra += +l * ys + cc * xc + u * yn;
+    }
+    {
+      const double ul = w_xm * wc + w_xp * wxp;
+      const double uu = w_xm * wt + w_xp * w1t;
+      const double l = +0.5 / dz * ul, u = -0.5 / dz * uu, cc = -l - u;
+      ra += +l * zs + cc * xc + u * zn;
+    }
+    rg += md * (+lu0 * xm + lu1 * xc + lu2 * xp);
+    ra += md * (+ly[0] * ys + ly[1] * xc + ly[2] * yn);
+    ra += md * (+lz[0] * zs + lz[1] * xc + lz[2] * zn);
+    rg -= 1. / dxc * (-pc + pxp);
+    if (a.add_buoyancy) ra += +0.5 * tc + 0.5 * txp;
+    ra += ifx;
+    sa[0] = ra;
+    sg[0] = rg;
   }
+  const double dxf = dxf_i;
+  // ---- uy at cell i
   {
-    const double ul = w_xm * ldg(uz + ix_cc(g, i - 1, j, k)) + w_xp * ldg(uz + ix_cc(g, i, j, k));
-    const double uu = w_xm * ldg(uz + ix_cc(g, i - 1, j, k + 1)) + w_xp * ldg(uz + ix_cc(g, i, j, k + 1));
-    const double l = +0.5 / g.dz * ul, u = -0.5 / g.dz * uu, cc = -l - u;
-    sa += +l * zs + cc * xc + u * zn;
+    const double xm = vxm, xc = vc, xp = vxp, ys = vs, yn = vn, zs = vb, zn = vt;
+    double ra = 0., rg = 0.;
+    {
+      const double ul = +0.5 * u0s + 0.5 * u00;
+      const double uu = +0.5 * u1s + 0.5 * u10;
+      const double l = +0.5 / dxf * ul, u = -0.5 / dxf * uu, cc = -l - u;
+      ra += +l * xm + cc * xc + u * xp;
+    }
+    {
+      const double ul = +0.5 * ys + 0.5 * xc, uu = +0.5 * xc + 0.5 * yn;
+      const double l = +0.5 / dy * ul, u = -0.5 / dy * uu, cc = -l - u;
+      ra += +l * ys + cc * xc + u * yn;
+    }
+    {
+      const double ul = +0.5 * ws + 0.5 * wc;
+      const double uu = +0.5 * wst + 0.5 * wt;
+      const double l = +0.5 / dz * ul, u = -0.5 / dz * uu, cc = -l - u;
+      ra += +l * zs + cc * xc + u * zn;
+    }
+    rg += md * (+lc0 * xm + lc1 * xc + lc2 * xp);
+    ra += md * (+ly[0] * ys + ly[1] * xc + ly[2] * yn);
+    ra += md * (+lz[0] * zs + lz[1] * xc + lz[2] * zn);
+    rg -= 1. / dy * (-ps + pc);
+    ra += ify;
+    sa[1] = ra;
+    sg[1] = rg;
   }
-  const double *lx = a.lap_ux + 3 * (i - 2);
-  sg += a.m_dif * (+ldg(lx + 0) * xm + ldg(lx + 1) * xc + ldg(lx + 2) * xp);
-  sa += a.m_dif * (+a.lapy[0] * ys + a.lapy[1] * xc + a.lapy[2] * yn);
-  sa += a.m_dif * (+a.lapz[0] * zs + a.lapz[1] * xc + a.lapz[2] * zn);
-  sg -= 1. / dxc * (-ldg(a.p + ix_cc(g, i - 1, j, k)) + ldg(a.p + ix_cc(g, i, j, k)));
-  if (a.add_buoyancy) sa += +0.5 * ldg(a.t + ix_cc(g, i - 1, j, k)) + 0.5 * ldg(a.t + ix_cc(g, i, j, k));
-  sa += ldg(a.ifrcx + ix_srcx(g, i, j, k));
-}
-
-__device__ __forceinline__ void rhs_uy(const Predict3Args &a, const Grid3 &g, int i, int j, int k, double &sa,
-                                       double &sg) {
-  const double *ux = a.ux, *uy = a.uy, *uz = a.uz;
-  const double dxf = ldg(g.dxf + i - 1);
-  const double xm = ldg(uy + ix_cc(g, i - 1, j, k)), xc = ldg(uy + ix_cc(g, i, j, k)), xp = ldg(uy + ix_cc(g, i + 1, j, k));
-  const double ys = ldg(uy + ix_cc(g, i, j - 1, k)), yn = ldg(uy + ix_cc(g, i, j + 1, k));
-  const double zs = ldg(uy + ix_cc(g, i, j, k - 1)), zn = ldg(uy + ix_cc(g, i, j, k + 1));
-  sa = 0.;
-  sg = 0.;
+  // ---- uz at cell i
   {
-    const double ul = +0.5 * ldg(ux + ix_ux(g, i, j - 1, k)) + 0.5 * ldg(ux + ix_ux(g, i, j, k));
-    const double uu = +0.5 * ldg(ux + ix_ux(g, i + 1, j - 1, k)) + 0.5 * ldg(ux + ix_ux(g, i + 1, j, k));
-    const double l = +0.5 / dxf * ul, u = -0.5 / dxf * uu, cc = -l - u;
-    sa += +l * xm + cc * xc + u * xp;
+    const double xm = wxm, xc = wc, xp = wxp, ys = ws, yn = wn, zs = wb, zn = wt;
+    double ra = 0., rg = 0.;
+    {
+      const double ul = +0.5 * u0b + 0.5 * u00;
+      const double uu = +0.5 * u1b + 0.5 * u10;
+      const double l = +0.5 / dxf * ul, u = -0.5 / dxf * uu, cc = -l - u;
+      ra += +l * xm + cc * xc + u * xp;
+    }
+    {
+      const double ul = +0.5 * vb + 0.5 * vc;
+      const double uu = +0.5 * vnb + 0.5 * vn;
+      const double l = +0.5 / dy * ul, u = -0.5 / dy * uu, cc = -l - u;
+      ra += +l * ys + cc * xc + u * yn;
+    }
+    {
+      const double ul = +0.5 * zs + 0.5 * xc, uu = +0.5 * xc + 0.5 * zn;
+      const double l = +0.5 / dz * ul, u = -0.5 / dz * uu, cc = -l - u;
+      ra += +l * zs + cc * xc + u * zn;
+    }
+    rg += md * (+lc0 * xm + lc1 * xc + lc2 * xp);
+    ra += md * (+ly[0] * ys + ly[1] * xc + ly[2] * yn);
+    ra += md * (+lz[0] * zs + lz[1] * xc + lz[2] * zn);
+    rg -= 1. / dz * (-pb + pc);
+    ra += ifz;
+    sa[2] = ra;
+    sg[2] = rg;
   }
+  // ---- t at cell i
   {
-    const double ul = +0.5 * ys + 0.5 * xc, uu = +0.5 * xc + 0.5 * yn;
-    const double l = +0.5 / g.dy * ul, u = -0.5 / g.dy * uu, cc = -l - u;
-    sa += +l * ys + cc * xc + u * yn;
+    const double xm = txm, xc = tc, xp = txp, ys = ts, yn = tn, zs = tb, zn = tt;
+    double ra = 0., rg = 0.;
+    {
+      const double l = +0.5 / dxf * u00, u = -0.5 / dxf * u10, cc = -l - u;
+      ra += +l * xm + cc * xc + u * xp;
+    }
+    {
+      const double l = +0.5 / dy * vc, u = -0.5 / dy * vn, cc = -l - u;
+      ra += +l * ys + cc * xc + u * yn;
+    }
+    {
+      const double l = +0.5 / dz * wc, u = -0.5 / dz * wt, cc = -l - u;
+      ra += +l * zs + cc * xc + u * zn;
+    }
+    rg += td * (+lc0 * xm + lc1 * xc + lc2 * xp);
+    ra += td * (+ly[0] * ys + ly[1] * xc + ly[2] * yn);
+    ra += td * (+lz[0] * zs + lz[1] * xc + lz[2] * zn);
+    sa[3] = ra;
+    sg[3] = rg;
   }
-  {
-    const double ul = +0.5 * ldg(uz + ix_cc(g, i, j - 1, k)) + 0.5 * ldg(uz + ix_cc(g, i, j, k));
-    const double uu = +0.5 * ldg(uz + ix_cc(g, i, j - 1, k + 1)) + 0.5 * ldg(uz + ix_cc(g, i, j, k + 1));
-    const double l = +0.5 / g.dz * ul, u = -0.5 / g.dz * uu, cc = -l - u;
-    sa += +l * zs + cc * xc + u * zn;
-  }
-  const double *lx = a.lap_cc + 3 * (i - 1);
-  sg += a.m_dif * (+ldg(lx + 0) * xm + ldg(lx + 1) * xc + ldg(lx + 2) * xp);
-  sa += a.m_dif * (+a.lapy[0] * ys + a.lapy[1] * xc + a.lapy[2] * yn);
-  sa += a.m_dif * (+a.lapz[0] * zs + a.lapz[1] * xc + a.lapz[2] * zn);
-  sg -= 1. / g.dy * (-ldg(a.p + ix_cc(g, i, j - 1, k)) + ldg(a.p + ix_cc(g, i, j, k)));
-  sa += ldg(a.ifrcy + ix_src(g, i, j, k));
-}
-
-__device__ __forceinline__ void rhs_uz(const Predict3Args &a, const Grid3 &g, int i, int j, int k, double &sa,
-                                       double &sg) {
-  const double *ux = a.ux, *uy = a.uy, *uz = a.uz;
-  const double dxf = ldg(g.dxf + i - 1);
-  const double xm = ldg(uz + ix_cc(g, i - 1, j, k)), xc = ldg(uz + ix_cc(g, i, j, k)), xp = ldg(uz + ix_cc(g, i + 1, j, k));
-  const double ys = ldg(uz + ix_cc(g, i, j - 1, k)), yn = ldg(uz + ix_cc(g, i, j + 1, k));
-  const double zs = ldg(uz + ix_cc(g, i, j, k - 1)), zn = ldg(uz + ix_cc(g, i, j, k + 1));
-  sa = 0.;
-  sg = 0.;
-  {
-    const double ul = +0.5 * ldg(ux + ix_ux(g, i, j, k - 1)) + 0.5 * ldg(ux + ix_ux(g, i, j, k));
-    const double uu = +0.5 * ldg(ux + ix_ux(g, i + 1, j, k - 1)) + 0.5 * ldg(ux + ix_ux(g, i + 1, j, k));
-    const double l = +0.5 / dxf * ul, u = -0.5 / dxf * uu, cc = -l - u;
-    sa += +l * xm + cc * xc + u * xp;
-  }
-  {
-    const double ul = +0.5 * ldg(uy + ix_cc(g, i, j, k - 1)) + 0.5 * ldg(uy + ix_cc(g, i, j, k));
-    const double uu = +0.5 * ldg(uy + ix_cc(g, i, j + 1, k - 1)) + 0.5 * ldg(uy + ix_cc(g, i, j + 1, k));
-    const double l = +0.5 / g.dy * ul, u = -0.5 / g.dy * uu, cc = -l - u;
-    sa += +l * ys + cc * xc + u * yn;
-  }
-  {
-    const double ul = +0.5 * zs + 0.5 * xc, uu = +0.5 * xc + 0.5 * zn;
-    const double l = +0.5 / g.dz * ul, u = -0.5 / g.dz * uu, cc = -l - u;
-    sa += +l * zs + cc * xc + u * zn;
-  }
-  const double *lx = a.lap_cc + 3 * (i - 1);
-  sg += a.m_dif * (+ldg(lx + 0) * xm + ldg(lx + 1) * xc + ldg(lx + 2) * xp);
-  sa += a.m_dif * (+a.lapy[0] * ys + a.lapy[1] * xc + a.lapy[2] * yn);
-  sa += a.m_dif * (+a.lapz[0] * zs + a.lapz[1] * xc + a.lapz[2] * zn);
-  sg -= 1. / g.dz * (-ldg(a.p + ix_cc(g, i, j, k - 1)) + ldg(a.p + ix_cc(g, i, j, k)));
-  sa += ldg(a.ifrcz + ix_src(g, i, j, k));
-}
-
-__device__ __forceinline__ void rhs_t(const Predict3Args &a, const Grid3 &g, int i, int j, int k, double &sa,
-                                      double &sg) {
-  const double *ux = a.ux, *uy = a.uy, *uz = a.uz, *t = a.t;
-  const double dxf = ldg(g.dxf + i - 1);
-  const double xm = ldg(t + ix_cc(g, i - 1, j, k)), xc = ldg(t + ix_cc(g, i, j, k)), xp = ldg(t + ix_cc(g, i + 1, j, k));
-  const double ys = ldg(t + ix_cc(g, i, j - 1, k)), yn = ldg(t + ix_cc(g, i, j + 1, k));
-  const double zs = ldg(t + ix_cc(g, i, j, k - 1)), zn = ldg(t + ix_cc(g, i, j, k + 1));
-  sa = 0.;
-  sg = 0.;
-  {
-    const double l = +0.5 / dxf * ldg(ux + ix_ux(g, i, j, k)), u = -0.5 / dxf * ldg(ux + ix_ux(g, i + 1, j, k)), cc = -l - u;
-    sa += +l * xm + cc * xc + u * xp;
-  }
-  {
-    const double l = +0.5 / g.dy * ldg(uy + ix_cc(g, i, j, k)), u = -0.5 / g.dy * ldg(uy + ix_cc(g, i, j + 1, k));
-    const double cc = -l - u;
-    sa += +l * ys + cc * xc + u * yn;
-  }
-  {
-    const double l = +0.5 / g.dz * ldg(uz + ix_cc(g, i, j, k)), u = -0.5 / g.dz * ldg(uz + ix_cc(g, i, j, k + 1));
-    const double cc = -l - u;
-    sa += +l * zs + cc * xc + u * zn;
-  }
-  const double *lx = a.lap_cc + 3 * (i - 1);
-  sg += a.t_dif * (+ldg(lx + 0) * xm + ldg(lx + 1) * xc + ldg(lx + 2) * xp);
-  sa += a.t_dif * (+a.lapy[0] * ys + a.lapy[1] * xc + a.lapy[2] * yn);
-  sa += a.t_dif * (+a.lapz[0] * zs + a.lapz[1] * xc + a.lapz[2] * zn);
 }
 
 constexpr int PL = kPredLines, PC = kPredChunk;
 
-__global__ void __launch_bounds__(256) k3_predict(Predict3Args a) {
+__global__ void __launch_bounds__(256, 2) k3_predict(Predict3Args a) {
   __shared__ double sd[4][PL][PC + 1];  // the four fields' increments of one tile
   __shared__ double sco[9][PC];         // L, R, V of the three systems, one chunk
   const Grid3 g = a.g;
@@ -242,31 +273,25 @@ __global__ void __launch_bounds__(256) k3_predict(Predict3Args a) {
       if (l >= nlines) continue;
       const int j = 1 + (int)(l % ny), k = 1 + (int)(l / ny);
       const int p = p0 + tx;
-      if (p < nx - 1) {
-        const int i = p + 2;
-        double sa, sg;
-        rhs_ux(a, g, i, j, k, sa, sg);
-        const long is = ix_srcx(g, i, j, k);
-        a.sa[0][is] = sa;
+      if (p >= nx) continue;
+      // cell i = p + 1 for uy, uz, t (line position p) and face i + 1 for ux
+      // (line position p of the ux system, which has nx - 1 unknowns)
+      const int i = p + 1;
+      const bool do_ux = p < nx - 1;
+      double sa[4], sg[4];
+      rhs4(a, g, i, j, k, do_ux, sa, sg);
+      if (do_ux) {
+        const long is = ix_srcx(g, i + 1, j, k);
+        a.sa[0][is] = sa[0];
         const double sb = a.use_b ? cb * ldg(a.sb[0] + is) : 0.;
-        sd[0][ll][tx] = +ca * sa + sb + cg * sg;
+        sd[0][ll][tx] = +ca * sa[0] + sb + cg * sg[0];
       }
-      if (p < nx) {
-        const int i = p + 1;
-        const long is = ix_src(g, i, j, k);
-        double sa, sg;
-        rhs_uy(a, g, i, j, k, sa, sg);
-        a.sa[1][is] = sa;
-        double sb = a.use_b ? cb * ldg(a.sb[1] + is) : 0.;
-        sd[1][ll][tx] = +ca * sa + sb + cg * sg;
-        rhs_uz(a, g, i, j, k, sa, sg);
-        a.sa[2][is] = sa;
-        sb = a.use_b ? cb * ldg(a.sb[2] + is) : 0.;
-        sd[2][ll][tx] = +ca * sa + sb + cg * sg;
-        rhs_t(a, g, i, j, k, sa, sg);
-        a.sa[3][is] = sa;
-        sb = a.use_b ? cb * ldg(a.sb[3] + is) : 0.;
-        sd[3][ll][tx] = +ca * sa + sb + cg * sg;
+      const long is = ix_src(g, i, j, k);
+#pragma unroll
+      for (int q = 1; q < 4; q++) {
+        a.sa[q][is] = sa[q];
+        const double sb = a.use_b ? cb * ldg(a.sb[q] + is) : 0.;
+        sd[q][ll][tx] = +ca * sa[q] + sb + cg * sg[q];
       }
     }
     __syncthreads();

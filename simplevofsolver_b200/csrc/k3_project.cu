@@ -22,9 +22,12 @@ __global__ void __launch_bounds__(256) k3_project(double *__restrict__ ux, doubl
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = 1 + blockIdx.z;
   if (i > nx || j > ny) return;
   const double dt = ldg(dtp);
+#pragma unroll 2
+  for (int kz = 0; kz < kProjectPlanes; kz++) {
+  const int k = 1 + blockIdx.z * kProjectPlanes + kz;
+  if (k > nz) break;
   const double psc = ldg(psi + ix_cc(g, i, j, k));
   const bool wall = (1 == i || nx == i);
   if (do_vel) {
@@ -79,6 +82,7 @@ __global__ void __launch_bounds__(256) k3_project(double *__restrict__ ux, doubl
       p[ix_cc(g, iw, j, k)] = v;
       for_images(j, k, ny, nz, false, [&](int jj, int kk) { p[ix_cc(g, iw, jj, kk)] = old; });
     }
+  }
   }
 }
 

@@ -267,7 +267,7 @@ int launch_potential(svof3d_solver *s, int rk, const std::vector<cudaEvent_t> *m
 }
 
 int launch_project(svof3d_solver *s, int rk, int do_vel, int do_p) {
-  dim3 b(32, 8), gr((s->nx + 31) / 32, (s->ny + 7) / 8, s->nz);
+  dim3 b(32, 8), gr((s->nx + 31) / 32, (s->ny + 7) / 8, (s->nz + kProjectPlanes - 1) / kProjectPlanes);
   k3_project<<<gr, b, 0, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->uz[s->cur_u].p, s->p.p, s->psi.p,
                                       s->d_dt, RK_A[rk] + RK_B[rk], s->prm.m_dif, s->prm.uy_xm, s->prm.uy_xp,
                                       s->prm.uz_xm, s->prm.uz_xp, do_vel, do_p, s->grid());
