@@ -1,4 +1,11 @@
-// k3_interface.cu -- boundary and interface (VOF) kernels of the FP64 3D path.
+// k3_interface.cu -- boundary and interface (VOF) kernels of the 3D path.
+//
+// The kernels are templates on R, the type of the interface intermediates
+// (curvature, normals, forces) and of the geometry and THINC arithmetic:
+// R = double is the FP64 path, which follows the restatement bit for bit
+// except for exp / log; R = float is the mixed path, where vof, the
+// velocities and the vof sources stay FP64 and only the geometry and the
+// THINC evaluations run in FP32.
 //
 //   k3_halo_bc     periodic y and z halos + x wall values of one field
 //   k3_geom        corner normals (2x2x2 differences), cell normal and THINC
@@ -64,44 +71,49 @@ __global__ void k3_halo_bc(double *a, int width, int nh, int ny, int nz, int kin
   at(r, q) = val;
 }
 
-__device__ __forceinline__ double plane_dx(double v00, double v10, double v01, double v11) {
+template <class T>
+__device__ __forceinline__ T plane_dx(T v00, T v10, T v01, T v11) {
   return -v00 + v10 - v01 + v11;
 }
-__device__ __forceinline__ double plane_dy(double v00, double v10, double v01, double v11) {
+template <class T>
+__device__ __forceinline__ T plane_dy(T v00, T v10, T v01, T v11) {
   return -v00 - v10 + v01 + v11;
 }
-__device__ __forceinline__ double plane_sum(double v00, double v10, double v01, double v11) {
+template <class T>
+__device__ __forceinline__ T plane_sum(T v00, T v10, T v01, T v11) {
   return +v00 + v10 + v01 + v11;
 }
 
 // THINC intercept with 2 x 2 x 2 Gauss points (compute_intercept3 of the
-// restatement; src/interface/curvature_tensor.c:50-92 in 2D)
-__device__ __forceinline__ double thinc_intercept3(const double vof, const double n0, const double n1,
-                                                   const double n2) {
+// restatement; src/interface/curvature_tensor.c:50-92 in 2D).  The Newton
+// tolerance is the reference's 1e-12 in FP64 and 1e-6 in FP32.
+template <class R>
+__device__ __forceinline__ R thinc_intercept3(const R vof, const R n0, const R n1, const R n2) {
   const int cntmax = 8;
-  const double resmax = 1.e-12;
-  double exps[8];
+  const R resmax = sizeof(R) == 8 ? R(1.e-12) : R(1.e-6);
+  const R gp0 = R(c3_gauss_p[0]), gp1 = R(c3_gauss_p[1]), gw = R(c3_gauss_w[0]);
+  const R gp[2] = {gp0, gp1};
+  R exps[8];
 #pragma unroll
   for (int kk = 0; kk < 2; kk++)
 #pragma unroll
     for (int jj = 0; jj < 2; jj++)
 #pragma unroll
       for (int ii = 0; ii < 2; ii++)
-        exps[(kk * 2 + jj) * 2 + ii] =
-            exp(-2. * kVofBeta * (+n0 * c3_gauss_p[ii] + n1 * c3_gauss_p[jj] + n2 * c3_gauss_p[kk]));
-  double val = 1. / vof - 1.;
+        exps[(kk * 2 + jj) * 2 + ii] = exp(R(-2.) * R(kVofBeta) * (+n0 * gp[ii] + n1 * gp[jj] + n2 * gp[kk]));
+  R val = R(1.) / vof - R(1.);
   for (int cnt = 0; cnt < cntmax; cnt++) {
-    double f0 = -1. * vof;
-    double f1 = 0.;
+    R f0 = R(-1.) * vof;
+    R f1 = R(0.);
 #pragma unroll
     for (int kk = 0; kk < 2; kk++) {
 #pragma unroll
       for (int jj = 0; jj < 2; jj++) {
 #pragma unroll
         for (int ii = 0; ii < 2; ii++) {
-          const double weight = c3_gauss_w[ii] * c3_gauss_w[jj] * c3_gauss_w[kk];
-          const double p = exps[(kk * 2 + jj) * 2 + ii];
-          const double denom = 1. / (1. + p * val);
+          const R weight = gw * gw * gw;
+          const R p = exps[(kk * 2 + jj) * 2 + ii];
+          const R denom = R(1.) / (R(1.) + p * val);
           f0 += weight * denom;
           f1 -= weight * p * denom * denom;
         }
@@ -110,21 +122,48 @@ __device__ __forceinline__ double thinc_intercept3(const double vof, const doubl
     val -= f0 / f1;
     if (fabs(f0) < resmax) break;
   }
-  return -0.5 / kVofBeta * log(val);
+  return R(-0.5) / R(kVofBeta) * log(val);
+}
+
+// four normal components per cell: two double2 / one float4
+__device__ __forceinline__ void store_normal3(double *o, double n0, double n1, double n2) {
+  reinterpret_cast<double2 *>(o)[0] = make_double2(n0, n1);
+  o[2] = n2;
+}
+__device__ __forceinline__ void store_normal3(float *o, float n0, float n1, float n2) {
+  reinterpret_cast<float2 *>(o)[0] = make_float2(n0, n1);
+  o[2] = n2;
+}
+__device__ __forceinline__ void load_normal(const double *__restrict__ normal, long idx, double *n) {
+  const double2 *p = reinterpret_cast<const double2 *>(normal + idx);
+  const double2 a = __ldg(p), b = __ldg(p + 1);
+  n[0] = a.x;
+  n[1] = a.y;
+  n[2] = b.x;
+  n[3] = b.y;
+}
+__device__ __forceinline__ void load_normal(const float *__restrict__ normal, long idx, float *n) {
+  const float4 a = __ldg(reinterpret_cast<const float4 *>(normal + idx));
+  n[0] = a.x;
+  n[1] = a.y;
+  n[2] = a.z;
+  n[3] = a.w;
 }
 
 // ---------------------------------------------------------------------------
 // k3_geom: cells i in [1, nx], j in [0, ny+1], k in [0, nz+1] (halo cells
 // included, as the restatement computes them).  Block: 32 x 4 cells of one
 // plane, marching over G3Z planes; shared memory holds two vof planes
-// (34 x 6) and two planes of corner normals (33 x 5 x 3).
+// (34 x 6, FP64) and two planes of corner normals (33 x 5 x 3, R).  The vof
+// differences are taken in FP64 and then carried in R.
 constexpr int G3X = 32, G3Y = 4, G3Z = 8;
 
-__global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ vof, double *__restrict__ normal,
-                                                    double *__restrict__ curv, unsigned *__restrict__ work,
+template <class R>
+__global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ vof, R *__restrict__ normal,
+                                                    R *__restrict__ curv, unsigned *__restrict__ work,
                                                     unsigned *__restrict__ nwork, Grid3 g) {
   __shared__ double sv[2][G3Y + 2][G3X + 2];
-  __shared__ double sc[2][3][G3Y + 1][G3X + 1];
+  __shared__ R sc[2][3][G3Y + 1][G3X + 1];
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int i0 = 1 + blockIdx.x * G3X;
   const int j0 = blockIdx.y * G3Y;
@@ -132,6 +171,8 @@ __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ 
   const int kend = min(k0 + G3Z, nz + 2);  // cells k in [k0, kend)
   const int tid = threadIdx.x;
   const int tx = tid % G3X, ty = tid / G3X;
+  const R eps = R(kDblEpsilon);
+  const R rdy = R(1.) / R(g.dy), rdz = R(1.) / R(g.dz);
   auto load_plane = [&](int buf, int k) {
     for (int t = tid; t < (G3X + 2) * (G3Y + 2); t += G3X * G3Y) {
       const int li = t % (G3X + 2), lj = t / (G3X + 2);
@@ -149,17 +190,17 @@ __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ 
     for (int t = tid; t < (G3X + 1) * (G3Y + 1); t += G3X * G3Y) {
       const int li = t % (G3X + 1), lj = t / (G3X + 1);
       const int ic = i0 + li, jc = j0 + lj;
-      double d0 = 0., d1 = 0., d2 = 0.;
+      R d0 = R(0.), d1 = R(0.), d2 = R(0.);
       if (ic <= nx + 1 && jc <= ny + 2) {
         const double a00 = sv[bprev][lj][li], a10 = sv[bprev][lj][li + 1];
         const double a01 = sv[bprev][lj + 1][li], a11 = sv[bprev][lj + 1][li + 1];
         const double b00 = sv[bcur][lj][li], b10 = sv[bcur][lj][li + 1];
         const double b01 = sv[bcur][lj + 1][li], b11 = sv[bcur][lj + 1][li + 1];
-        const double dvofdx = 1. / ldg(g.dxc + ic - 1) * (plane_dx(a00, a10, a01, a11) + plane_dx(b00, b10, b01, b11));
-        const double dvofdy = 1. / g.dy * (plane_dy(a00, a10, a01, a11) + plane_dy(b00, b10, b01, b11));
-        const double dvofdz = 1. / g.dz * (plane_sum(b00, b10, b01, b11) - plane_sum(a00, a10, a01, a11));
-        const double norm = sqrt(+dvofdx * dvofdx + dvofdy * dvofdy + dvofdz * dvofdz);
-        const double norminv = 1. / fmax(norm, kDblEpsilon);
+        const R dvofdx = R(1.) / R(ldg(g.dxc + ic - 1)) * R(plane_dx(a00, a10, a01, a11) + plane_dx(b00, b10, b01, b11));
+        const R dvofdy = rdy * R(plane_dy(a00, a10, a01, a11) + plane_dy(b00, b10, b01, b11));
+        const R dvofdz = rdz * R(plane_sum(b00, b10, b01, b11) - plane_sum(a00, a10, a01, a11));
+        const R norm = sqrt(+dvofdx * dvofdx + dvofdy * dvofdy + dvofdz * dvofdz);
+        const R norminv = R(1.) / fmax(norm, eps);
         d0 = dvofdx * norminv;
         d1 = dvofdy * norminv;
         d2 = dvofdz * norminv;
@@ -174,35 +215,33 @@ __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ 
       const int i = i0 + tx, j = j0 + ty, k = kc - 1;
       bool inter = false;
       if (i <= nx && j <= ny + 1) {
-        const double dxf = ldg(g.dxf + i - 1);
+        const R dxf = R(ldg(g.dxf + i - 1));
 #define CL(m, a, b) sc[cprev][m][ty + (b)][tx + (a)]
 #define CU(m, a, b) sc[ccur][m][ty + (b)][tx + (a)]
-        const double dnxdx = 1. / dxf * (plane_dx(CL(0, 0, 0), CL(0, 1, 0), CL(0, 0, 1), CL(0, 1, 1)) +
-                                         plane_dx(CU(0, 0, 0), CU(0, 1, 0), CU(0, 0, 1), CU(0, 1, 1)));
-        const double dnydy = 1. / g.dy * (plane_dy(CL(1, 0, 0), CL(1, 1, 0), CL(1, 0, 1), CL(1, 1, 1)) +
-                                          plane_dy(CU(1, 0, 0), CU(1, 1, 0), CU(1, 0, 1), CU(1, 1, 1)));
-        const double dnzdz = 1. / g.dz * (plane_sum(CU(2, 0, 0), CU(2, 1, 0), CU(2, 0, 1), CU(2, 1, 1)) -
-                                          plane_sum(CL(2, 0, 0), CL(2, 1, 0), CL(2, 0, 1), CL(2, 1, 1)));
-        curv[ix_cc(g, i, j, k)] = 0.25 * (-dnxdx - dnydy - dnzdz);
+        const R dnxdx = R(1.) / dxf * (plane_dx(CL(0, 0, 0), CL(0, 1, 0), CL(0, 0, 1), CL(0, 1, 1)) +
+                                       plane_dx(CU(0, 0, 0), CU(0, 1, 0), CU(0, 0, 1), CU(0, 1, 1)));
+        const R dnydy = rdy * (plane_dy(CL(1, 0, 0), CL(1, 1, 0), CL(1, 0, 1), CL(1, 1, 1)) +
+                               plane_dy(CU(1, 0, 0), CU(1, 1, 0), CU(1, 0, 1), CU(1, 1, 1)));
+        const R dnzdz = rdz * (plane_sum(CU(2, 0, 0), CU(2, 1, 0), CU(2, 0, 1), CU(2, 1, 1)) -
+                               plane_sum(CL(2, 0, 0), CL(2, 1, 0), CL(2, 0, 1), CL(2, 1, 1)));
+        curv[ix_cc(g, i, j, k)] = R(0.25) * (-dnxdx - dnydy - dnzdz);
         const double lvof = sv[bprev][ty + 1][tx + 1];
         if (!(lvof < kVofMin || 1. - kVofMin < lvof)) {
-          double n0 = plane_sum(CL(0, 0, 0), CL(0, 1, 0), CL(0, 0, 1), CL(0, 1, 1)) +
-                      plane_sum(CU(0, 0, 0), CU(0, 1, 0), CU(0, 0, 1), CU(0, 1, 1));
-          double n1 = plane_sum(CL(1, 0, 0), CL(1, 1, 0), CL(1, 0, 1), CL(1, 1, 1)) +
-                      plane_sum(CU(1, 0, 0), CU(1, 1, 0), CU(1, 0, 1), CU(1, 1, 1));
-          double n2 = plane_sum(CL(2, 0, 0), CL(2, 1, 0), CL(2, 0, 1), CL(2, 1, 1)) +
-                      plane_sum(CU(2, 0, 0), CU(2, 1, 0), CU(2, 0, 1), CU(2, 1, 1));
+          R n0 = plane_sum(CL(0, 0, 0), CL(0, 1, 0), CL(0, 0, 1), CL(0, 1, 1)) +
+                 plane_sum(CU(0, 0, 0), CU(0, 1, 0), CU(0, 0, 1), CU(0, 1, 1));
+          R n1 = plane_sum(CL(1, 0, 0), CL(1, 1, 0), CL(1, 0, 1), CL(1, 1, 1)) +
+                 plane_sum(CU(1, 0, 0), CU(1, 1, 0), CU(1, 0, 1), CU(1, 1, 1));
+          R n2 = plane_sum(CL(2, 0, 0), CL(2, 1, 0), CL(2, 0, 1), CL(2, 1, 1)) +
+                 plane_sum(CU(2, 0, 0), CU(2, 1, 0), CU(2, 0, 1), CU(2, 1, 1));
           n0 /= dxf;
-          n1 /= g.dy;
-          n2 /= g.dz;
-          const double norm = sqrt(+n0 * n0 + n1 * n1 + n2 * n2);
-          const double norminv = 1. / fmax(norm, kDblEpsilon);
+          n1 /= R(g.dy);
+          n2 /= R(g.dz);
+          const R norm = sqrt(+n0 * n0 + n1 * n1 + n2 * n2);
+          const R norminv = R(1.) / fmax(norm, eps);
           n0 *= norminv;
           n1 *= norminv;
           n2 *= norminv;
-          double2 *o = reinterpret_cast<double2 *>(normal + ix_nrm(g, i, j, k));
-          o[0] = make_double2(n0, n1);
-          o[1].x = n2;
+          store_normal3(normal + ix_nrm(g, i, j, k), n0, n1, n2);
           inter = true;
         }
 #undef CL
@@ -228,7 +267,8 @@ __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ 
 
 // k3_intercept: THINC intercept of every listed interfacial cell (the normal
 // vector is already stored); one thread per cell, grid-stride over the list
-__global__ void __launch_bounds__(256) k3_intercept(const double *__restrict__ vof, double *__restrict__ normal,
+template <class R>
+__global__ void __launch_bounds__(256) k3_intercept(const double *__restrict__ vof, R *__restrict__ normal,
                                                    const unsigned *__restrict__ work,
                                                    const unsigned *__restrict__ nwork, Grid3 g) {
   const unsigned n = *nwork;
@@ -238,126 +278,122 @@ __global__ void __launch_bounds__(256) k3_intercept(const double *__restrict__ v
     const int i = 1 + (int)(c % (unsigned)nx);
     const unsigned r = c / (unsigned)nx;
     const int j = (int)(r % (unsigned)rows), k = (int)(r / (unsigned)rows);
-    double *o = normal + 4L * c;
-    const double2 a = *reinterpret_cast<const double2 *>(o);
-    const double n2 = o[2];
-    o[3] = thinc_intercept3(ldg(vof + ix_vof(g, i, j, k)), a.x, a.y, n2);
+    R *o = normal + 4L * c;
+    o[3] = thinc_intercept3<R>(R(ldg(vof + ix_vof(g, i, j, k))), o[0], o[1], o[2]);
   }
 }
 
 // ---------------------------------------------------------------------------
-// k3_force: one thread per interior cell
-__global__ void k3_force(const double *__restrict__ vof, const double *__restrict__ curv,
-                         double *__restrict__ ifrcx, double *__restrict__ ifrcy, double *__restrict__ ifrcz,
-                         double tension, Grid3 g) {
+// k3_force: one thread per interior cell; FP64 arithmetic, R output
+template <class R>
+__global__ void k3_force(const double *__restrict__ vof, const R *__restrict__ curv, R *__restrict__ ifrcx,
+                         R *__restrict__ ifrcy, R *__restrict__ ifrcz, double tension, Grid3 g) {
   const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
   const int k = 1 + blockIdx.z;
   if (i > g.nx || j > g.ny) return;
   const double vc = ldg(vof + ix_vof(g, i, j, k));
-  const double cc = ldg(curv + ix_cc(g, i, j, k));
+  const double cc = (double)__ldg(curv + ix_cc(g, i, j, k));
   if (i >= 2) {
     const double grad = 1. / ldg(g.dxc + i - 1) * (-ldg(vof + ix_vof(g, i - 1, j, k)) + vc);
-    const double kappa = 0.5 * (+ldg(curv + ix_cc(g, i - 1, j, k)) + cc);
-    ifrcx[ix_srcx(g, i, j, k)] = tension * grad * kappa;
+    const double kappa = 0.5 * (+(double)__ldg(curv + ix_cc(g, i - 1, j, k)) + cc);
+    ifrcx[ix_srcx(g, i, j, k)] = R(tension * grad * kappa);
   }
   {
     const double grad = 1. / g.dy * (-ldg(vof + ix_vof(g, i, j - 1, k)) + vc);
-    const double kappa = 0.5 * (+ldg(curv + ix_cc(g, i, j - 1, k)) + cc);
-    ifrcy[ix_src(g, i, j, k)] = tension * grad * kappa;
+    const double kappa = 0.5 * (+(double)__ldg(curv + ix_cc(g, i, j - 1, k)) + cc);
+    ifrcy[ix_src(g, i, j, k)] = R(tension * grad * kappa);
   }
   {
     const double grad = 1. / g.dz * (-ldg(vof + ix_vof(g, i, j, k - 1)) + vc);
-    const double kappa = 0.5 * (+ldg(curv + ix_cc(g, i, j, k - 1)) + cc);
-    ifrcz[ix_src(g, i, j, k)] = tension * grad * kappa;
+    const double kappa = 0.5 * (+(double)__ldg(curv + ix_cc(g, i, j, k - 1)) + cc);
+    ifrcz[ix_src(g, i, j, k)] = R(tension * grad * kappa);
   }
 }
 
 // ---------------------------------------------------------------------------
-// THINC/QQ flux helpers (indicator3 and the face fluxes of the restatement)
-__device__ __forceinline__ double indicator3(const double *n, double x0, double x1, double x2) {
-  return 1. / (1. + exp(-2. * kVofBeta * (+n[0] * x0 + n[1] * x1 + n[2] * x2 + n[3])));
-}
-
-__device__ __forceinline__ void load_normal(const double *__restrict__ normal, long idx, double *n) {
-  const double2 *p = reinterpret_cast<const double2 *>(normal + idx);
-  const double2 a = __ldg(p), b = __ldg(p + 1);
-  n[0] = a.x;
-  n[1] = a.y;
-  n[2] = b.x;
-  n[3] = b.y;
+// THINC/QQ flux helpers (indicator3 and the face fluxes of the restatement):
+// the indicator sums run in R, the flux vel * sum in FP64
+template <class R>
+__device__ __forceinline__ R indicator3(const R *n, R x0, R x1, R x2) {
+  return R(1.) / (R(1.) + exp(R(-2.) * R(kVofBeta) * (+n[0] * x0 + n[1] * x1 + n[2] * x2 + n[3])));
 }
 
 // flux through the x face i (i in [2, nx]) of row (j, k)
+template <class R>
 __device__ __forceinline__ double flux_x(const double *__restrict__ vof, const double *__restrict__ ux,
-                                         const double *__restrict__ normal, const Grid3 &g, int i, int j, int k) {
+                                         const R *__restrict__ normal, const Grid3 &g, int i, int j, int k) {
   const double vel = ldg(ux + ix_ux(g, i, j, k));
   const int ii = vel < 0. ? i : i - 1;
-  const double x = vel < 0. ? -0.5 : +0.5;
+  const R x = vel < 0. ? R(-0.5) : R(+0.5);
   const double lvof = ldg(vof + ix_vof(g, ii, j, k));
   if (lvof < kVofMin || 1. - kVofMin < lvof) return vel * lvof;
-  double n[4];
+  R n[4];
   load_normal(normal, ix_nrm(g, ii, j, k), n);
-  double flux = 0.;
+  R flux = R(0.);
 #pragma unroll
   for (int kk = 0; kk < 2; kk++)
 #pragma unroll
     for (int jj = 0; jj < 2; jj++)
-      flux += c3_gauss_w[jj] * c3_gauss_w[kk] * indicator3(n, x, c3_gauss_p[jj], c3_gauss_p[kk]);
-  return vel * flux;
+      flux += R(c3_gauss_w[jj]) * R(c3_gauss_w[kk]) * indicator3<R>(n, x, R(c3_gauss_p[jj]), R(c3_gauss_p[kk]));
+  return vel * (double)flux;
 }
 
 // flux through the y face j (j in [1, ny+1]) of column (i, k)
+template <class R>
 __device__ __forceinline__ double flux_y(const double *__restrict__ vof, const double *__restrict__ uy,
-                                         const double *__restrict__ normal, const Grid3 &g, int i, int j, int k) {
+                                         const R *__restrict__ normal, const Grid3 &g, int i, int j, int k) {
   const double vel = ldg(uy + ix_cc(g, i, j, k));
   const int jj = vel < 0. ? j : j - 1;
-  const double y = vel < 0. ? -0.5 : +0.5;
+  const R y = vel < 0. ? R(-0.5) : R(+0.5);
   const double lvof = ldg(vof + ix_vof(g, i, jj, k));
   if (lvof < kVofMin || 1. - kVofMin < lvof) return vel * lvof;
-  double n[4];
+  R n[4];
   load_normal(normal, ix_nrm(g, i, jj, k), n);
-  double flux = 0.;
+  R flux = R(0.);
 #pragma unroll
   for (int kk = 0; kk < 2; kk++)
 #pragma unroll
     for (int ii = 0; ii < 2; ii++)
-      flux += c3_gauss_w[ii] * c3_gauss_w[kk] * indicator3(n, c3_gauss_p[ii], y, c3_gauss_p[kk]);
-  return vel * flux;
+      flux += R(c3_gauss_w[ii]) * R(c3_gauss_w[kk]) * indicator3<R>(n, R(c3_gauss_p[ii]), y, R(c3_gauss_p[kk]));
+  return vel * (double)flux;
 }
 
 // flux through the z face k (k in [1, nz+1]) of column (i, j)
+template <class R>
 __device__ __forceinline__ double flux_z(const double *__restrict__ vof, const double *__restrict__ uz,
-                                         const double *__restrict__ normal, const Grid3 &g, int i, int j, int k) {
+                                         const R *__restrict__ normal, const Grid3 &g, int i, int j, int k) {
   const double vel = ldg(uz + ix_cc(g, i, j, k));
   const int kk = vel < 0. ? k : k - 1;
-  const double z = vel < 0. ? -0.5 : +0.5;
+  const R z = vel < 0. ? R(-0.5) : R(+0.5);
   const double lvof = ldg(vof + ix_vof(g, i, j, kk));
   if (lvof < kVofMin || 1. - kVofMin < lvof) return vel * lvof;
-  double n[4];
+  R n[4];
   load_normal(normal, ix_nrm(g, i, j, kk), n);
-  double flux = 0.;
+  R flux = R(0.);
 #pragma unroll
   for (int jj = 0; jj < 2; jj++)
 #pragma unroll
     for (int ii = 0; ii < 2; ii++)
-      flux += c3_gauss_w[ii] * c3_gauss_w[jj] * indicator3(n, c3_gauss_p[ii], c3_gauss_p[jj], z);
-  return vel * flux;
+      flux += R(c3_gauss_w[ii]) * R(c3_gauss_w[jj]) * indicator3<R>(n, R(c3_gauss_p[ii]), R(c3_gauss_p[jj]), z);
+  return vel * (double)flux;
 }
 
 // k3_vof_advect: cells i in [1, nx], j in [1, ny], k in [1, nz]; block 32 x 4
 // cells marching over V3Z planes.  x and y face fluxes of a plane are staged
 // in shared memory; the z-face flux below a cell is the one above it in the
 // previous plane.  Writes vof_new with its halo images (two layers) and zero
-// x walls, and src_a.
+// x walls, and src_a.  The flux divergence and the update are FP64 in both
+// precisions, so that the update conserves volume to FP64 round-off.
 constexpr int V3X = 32, V3Y = 4, V3Z = 8;
 
+template <class R>
 __global__ void __launch_bounds__(V3X * V3Y) k3_vof_advect(const double *__restrict__ vof,
                                                           double *__restrict__ vof_new,
                                                           const double *__restrict__ ux,
                                                           const double *__restrict__ uy,
                                                           const double *__restrict__ uz,
-                                                          const double *__restrict__ normal,
+                                                          const R *__restrict__ normal,
                                                           double *__restrict__ src_a,
                                                           const double *__restrict__ src_b,
                                                           const double *__restrict__ dtp, RK rk, int use_b,
@@ -375,24 +411,24 @@ __global__ void __launch_bounds__(V3X * V3Y) k3_vof_advect(const double *__restr
   const bool mine = (i <= nx && j <= ny);
   const double dt = ldg(dtp);
   double fz_lo = 0.;
-  if (mine) fz_lo = flux_z(vof, uz, normal, g, i, j, k0);
+  if (mine) fz_lo = flux_z<R>(vof, uz, normal, g, i, j, k0);
   for (int k = k0; k < kend; k++) {
     for (int t = tid; t < V3Y * (V3X + 1); t += V3X * V3Y) {
       const int li = t % (V3X + 1), lj = t / (V3X + 1);
       const int fi = i0 + li, fj = j0 + lj;
       double f = 0.;
-      if (fi >= 2 && fi <= nx && fj <= ny) f = flux_x(vof, ux, normal, g, fi, fj, k);
+      if (fi >= 2 && fi <= nx && fj <= ny) f = flux_x<R>(vof, ux, normal, g, fi, fj, k);
       fx[lj][li] = f;
     }
     for (int t = tid; t < (V3Y + 1) * V3X; t += V3X * V3Y) {
       const int li = t % V3X, lj = t / V3X;
       const int fi = i0 + li, fj = j0 + lj;
       double f = 0.;
-      if (fi <= nx && fj <= ny + 1) f = flux_y(vof, uy, normal, g, fi, fj, k);
+      if (fi <= nx && fj <= ny + 1) f = flux_y<R>(vof, uy, normal, g, fi, fj, k);
       fy[lj][li] = f;
     }
     double fz_hi = 0.;
-    if (mine) fz_hi = flux_z(vof, uz, normal, g, i, j, k + 1);
+    if (mine) fz_hi = flux_z<R>(vof, uz, normal, g, i, j, k + 1);
     __syncthreads();
     if (mine) {
       double s = 0.;
@@ -424,5 +460,45 @@ __global__ void __launch_bounds__(V3X * V3Y) k3_vof_advect(const double *__restr
     __syncthreads();
   }
 }
+
+// ---- host-side launchers
+template <class R>
+cudaError_t interface_geom(cudaStream_t st, const double *vof, R *normal, R *curv, unsigned *work,
+                           unsigned *nwork, Grid3 g) {
+  cudaError_t e = cudaMemsetAsync(nwork, 0, sizeof(unsigned), st);
+  if (cudaSuccess != e) return e;
+  dim3 gr((g.nx + G3X - 1) / G3X, (g.ny + 2 + G3Y - 1) / G3Y, (g.nz + 2 + G3Z - 1) / G3Z);
+  k3_geom<R><<<gr, G3X * G3Y, 0, st>>>(vof, normal, curv, work, nwork, g);
+  if (cudaSuccess != (e = cudaGetLastError())) return e;
+  k3_intercept<R><<<148 * 8, 256, 0, st>>>(vof, normal, work, nwork, g);
+  return cudaGetLastError();
+}
+
+template <class R>
+cudaError_t interface_force(cudaStream_t st, const double *vof, const R *curv, R *ifrcx, R *ifrcy, R *ifrcz,
+                            double tension, Grid3 g) {
+  dim3 b(32, 8), gr((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz);
+  k3_force<R><<<gr, b, 0, st>>>(vof, curv, ifrcx, ifrcy, ifrcz, tension, g);
+  return cudaGetLastError();
+}
+
+template <class R>
+cudaError_t interface_advect(cudaStream_t st, const double *vof, double *vof_new, const double *ux,
+                             const double *uy, const double *uz, const R *normal, double *src_a,
+                             const double *src_b, const double *dtp, RK rk, int use_b, Grid3 g) {
+  dim3 gr((g.nx + V3X - 1) / V3X, (g.ny + V3Y - 1) / V3Y, (g.nz + V3Z - 1) / V3Z);
+  k3_vof_advect<R><<<gr, V3X * V3Y, 0, st>>>(vof, vof_new, ux, uy, uz, normal, src_a, src_b, dtp, rk, use_b, g);
+  return cudaGetLastError();
+}
+
+#define SVOF3_INTERFACE_INST(R)                                                                                \
+  template cudaError_t interface_geom<R>(cudaStream_t, const double *, R *, R *, unsigned *, unsigned *, Grid3); \
+  template cudaError_t interface_force<R>(cudaStream_t, const double *, const R *, R *, R *, R *, double, Grid3); \
+  template cudaError_t interface_advect<R>(cudaStream_t, const double *, double *, const double *, const double *, \
+                                           const double *, const R *, double *, const double *, const double *,   \
+                                           RK, int, Grid3);
+SVOF3_INTERFACE_INST(double)
+SVOF3_INTERFACE_INST(float)
+#undef SVOF3_INTERFACE_INST
 
 }  // namespace svof3

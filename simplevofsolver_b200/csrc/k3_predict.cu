@@ -77,7 +77,8 @@ __global__ void k3_tdm_coef(const double *__restrict__ lap_ux, const double *__r
 // buoyancy; surface).  All stencil values are loaded before any arithmetic,
 // so that the ~50 loads of a cell are in flight together.
 // Field order: 0 ux, 1 uy, 2 uz, 3 t.
-__device__ __forceinline__ void rhs4(const Predict3Args &a, const Grid3 &g, int i, int j, int k, bool do_ux,
+template <class R>
+__device__ __forceinline__ void rhs4(const Predict3Args<R> &a, const Grid3 &g, int i, int j, int k, bool do_ux,
                                      double *sa, double *sg) {
   const double *ux = a.ux, *uy = a.uy, *uz = a.uz, *t = a.t, *p = a.p;
   // ---- loads
@@ -239,7 +240,8 @@ __device__ __forceinline__ void rhs4(const Predict3Args &a, const Grid3 &g, int 
 
 constexpr int PL = kPredLines, PC = kPredChunk;
 
-__global__ void __launch_bounds__(256, 2) k3_predict(Predict3Args a) {
+template <class R>
+__global__ void __launch_bounds__(256, 2) k3_predict(Predict3Args<R> a) {
   __shared__ double sd[4][PL][PC + 1];  // the four fields' increments of one tile
   __shared__ double sco[9][PC];         // L, R, V of the three systems, one chunk
   const Grid3 g = a.g;
@@ -249,7 +251,7 @@ __global__ void __launch_bounds__(256, 2) k3_predict(Predict3Args a) {
   const int tid = threadIdx.x;
   const int tx = tid & 31, ty = tid >> 5;
   const int nchunks = (nx + PC - 1) / PC;
-  const double dt = *a.dtp;
+  const double dt = ldg(a.dtp);
   const double ca = a.rk.a * dt, cb = a.rk.b * dt, cg = a.rk.g * dt;
   // the sweeping warps: warp f < 4 owns field f, lane = line of the block
   const int f = ty;
@@ -282,14 +284,14 @@ __global__ void __launch_bounds__(256, 2) k3_predict(Predict3Args a) {
       rhs4(a, g, i, j, k, do_ux, sa, sg);
       if (do_ux) {
         const long is = ix_srcx(g, i + 1, j, k);
-        a.sa[0][is] = sa[0];
+        a.sa[0][is] = R(sa[0]);
         const double sb = a.use_b ? cb * ldg(a.sb[0] + is) : 0.;
         sd[0][ll][tx] = +ca * sa[0] + sb + cg * sg[0];
       }
       const long is = ix_src(g, i, j, k);
 #pragma unroll
       for (int q = 1; q < 4; q++) {
-        a.sa[q][is] = sa[q];
+        a.sa[q][is] = R(sa[q]);
         const double sb = a.use_b ? cb * ldg(a.sb[q] + is) : 0.;
         sd[q][ll][tx] = +ca * sa[q] + sb + cg * sg[q];
       }
@@ -320,11 +322,11 @@ __global__ void __launch_bounds__(256, 2) k3_predict(Predict3Args a) {
       const long l = l0 + ll;
       const int p = p0 + tx;
       if (l >= nlines || p >= nx) continue;
-      double *fw = a.fw + (size_t)l * nx + p;
-      if (p < nx - 1) fw[0] = sd[0][ll][tx];
-      fw[fstride] = sd[1][ll][tx];
-      fw[2 * fstride] = sd[2][ll][tx];
-      fw[3 * fstride] = sd[3][ll][tx];
+      R *fw = a.fw + (size_t)l * nx + p;
+      if (p < nx - 1) fw[0] = R(sd[0][ll][tx]);
+      fw[fstride] = R(sd[1][ll][tx]);
+      fw[2 * fstride] = R(sd[2][ll][tx]);
+      fw[3 * fstride] = R(sd[3][ll][tx]);
     }
     __syncthreads();
   }
@@ -343,7 +345,7 @@ __global__ void __launch_bounds__(256, 2) k3_predict(Predict3Args a) {
       const long l = l0 + ll;
       const int p = p0 + tx;
       if (l >= nlines || p >= nx) continue;
-      const double *fw = a.fw + (size_t)l * nx + p;
+      const R *fw = a.fw + (size_t)l * nx + p;
       sd[0][ll][tx] = (p < nx - 1) ? fw[0] : 0.;
       sd[1][ll][tx] = fw[fstride];
       sd[2][ll][tx] = fw[2 * fstride];
@@ -425,5 +427,14 @@ __global__ void __launch_bounds__(256, 2) k3_predict(Predict3Args a) {
     }
   }
 }
+
+template <class R>
+cudaError_t predict_launch(cudaStream_t st, const Predict3Args<R> &a) {
+  const long nlines = (long)a.g.ny * a.g.nz;
+  k3_predict<R><<<(unsigned)((nlines + PL - 1) / PL), 256, 0, st>>>(a);
+  return cudaGetLastError();
+}
+template cudaError_t predict_launch<double>(cudaStream_t, const Predict3Args<double> &);
+template cudaError_t predict_launch<float>(cudaStream_t, const Predict3Args<float> &);
 
 }  // namespace svof3

@@ -13,6 +13,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <string>
 #include <vector>
@@ -55,21 +56,35 @@ int ilog2_exact(int n) {
   return ((1 << l) == n) ? l : -1;
 }
 
+// a device array of n elements of es bytes (8: double, 4: float)
 struct DevBuf {
   double *p = nullptr;
   size_t n = 0;
+  size_t es = 8;
+  template <class T>
+  T *as() const {
+    return reinterpret_cast<T *>(p);
+  }
 };
 
-int dalloc(DevBuf &b, size_t n) {
+int dalloc(DevBuf &b, size_t n, size_t es = 8) {
   b.n = n;
-  CK(cudaMalloc(&b.p, sizeof(double) * (n ? n : 1)));
-  CK(cudaMemset(b.p, 0, sizeof(double) * (n ? n : 1)));
+  b.es = es;
+  CK(cudaMalloc(&b.p, es * (n ? n : 1)));
+  CK(cudaMemset(b.p, 0, es * (n ? n : 1)));
   return 0;
 }
 
 int upload(DevBuf &b, const std::vector<double> &h) {
   if (dalloc(b, h.size())) return 1;
   CK(cudaMemcpy(b.p, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
+  return 0;
+}
+
+int upload_f(DevBuf &b, const std::vector<double> &h) {
+  std::vector<float> f(h.begin(), h.end());
+  if (dalloc(b, h.size(), 4)) return 1;
+  CK(cudaMemcpy(b.p, f.data(), sizeof(float) * f.size(), cudaMemcpyHostToDevice));
   return 0;
 }
 
@@ -83,6 +98,7 @@ void dfree(DevBuf &b) {
 
 struct svof3d_solver {
   svof3d_params_t prm{};
+  bool mixed = false;  // SVOF3_MIXED: FP32 intermediates (see svof3d_b200.h)
   int nx = 0, ny = 0, nz = 0;
   double dy = 0., dz = 0.;
   int log2ny = 0, log2nz = 0;
@@ -96,6 +112,7 @@ struct svof3d_solver {
   double lims[4] = {0., 0., 0., 0.};  // explicit diffusive dt limits: m y, m z, t y, t z
   // Poisson
   DevBuf spec, xscratch, twf_y, twb_y, twf_z, twb_z, pl, pu, evy, evz;
+  DevBuf twf_y32, twb_y32, twf_z32, twb_z32;  // FP32 twiddles of the mixed path
   int cols_y = 8, cols_z = 8;
   // predictor forward-sweep scratch
   DevBuf fw;
@@ -145,53 +162,51 @@ int launch_dt(svof3d_solver *s) {
   return 0;
 }
 
-int launch_geom(svof3d_solver *s) {
-  CK(cudaMemsetAsync(s->d_nwork, 0, sizeof(unsigned), s->stream));
-  dim3 gr((s->nx + 31) / 32, (s->ny + 2 + 3) / 4, (s->nz + 2 + 7) / 8);
-  k3_geom<<<gr, 128, 0, s->stream>>>(s->vof[s->cur_v].p, s->normal.p, s->curv.p, s->d_work, s->d_nwork,
-                                     s->grid());
-  CK_LAUNCH();
-  k3_intercept<<<148 * 8, 256, 0, s->stream>>>(s->vof[s->cur_v].p, s->normal.p, s->d_work, s->d_nwork, s->grid());
-  CK_LAUNCH();
+template <class R>
+int launch_geom_t(svof3d_solver *s) {
+  CK(interface_geom<R>(s->stream, s->vof[s->cur_v].p, s->normal.as<R>(), s->curv.as<R>(), s->d_work, s->d_nwork,
+                       s->grid()));
   return 0;
 }
+int launch_geom(svof3d_solver *s) { return s->mixed ? launch_geom_t<float>(s) : launch_geom_t<double>(s); }
 
-int launch_force(svof3d_solver *s) {
-  dim3 b(32, 8), gr((s->nx + 31) / 32, (s->ny + 7) / 8, s->nz);
-  k3_force<<<gr, b, 0, s->stream>>>(s->vof[s->cur_v].p, s->curv.p, s->ifrcx.p, s->ifrcy.p, s->ifrcz.p,
-                                    s->prm.tension, s->grid());
-  CK_LAUNCH();
+template <class R>
+int launch_force_t(svof3d_solver *s) {
+  CK(interface_force<R>(s->stream, s->vof[s->cur_v].p, s->curv.as<R>(), s->ifrcx.as<R>(), s->ifrcy.as<R>(),
+                        s->ifrcz.as<R>(), s->prm.tension, s->grid()));
   return 0;
 }
+int launch_force(svof3d_solver *s) { return s->mixed ? launch_force_t<float>(s) : launch_force_t<double>(s); }
 
 int launch_vof(svof3d_solver *s, int rk) {
   if (0 != rk) s->sa_v ^= 1;
-  dim3 gr((s->nx + 31) / 32, (s->ny + 3) / 4, (s->nz + 7) / 8);
   RK c{RK_A[rk], RK_B[rk], RK_A[rk] + RK_B[rk]};
-  k3_vof_advect<<<gr, 128, 0, s->stream>>>(s->vof[s->cur_v].p, s->vof[1 - s->cur_v].p, s->ux[s->cur_u].p,
-                                           s->uy[s->cur_u].p, s->uz[s->cur_u].p, s->normal.p, s->svof[s->sa_v].p,
-                                           s->svof[1 - s->sa_v].p, s->d_dt, c, rk != 0, s->grid());
-  CK_LAUNCH();
+  const int cv = s->cur_v, cu = s->cur_u;
+  if (s->mixed) {
+    CK(interface_advect<float>(s->stream, s->vof[cv].p, s->vof[1 - cv].p, s->ux[cu].p, s->uy[cu].p, s->uz[cu].p,
+                               s->normal.as<float>(), s->svof[s->sa_v].p, s->svof[1 - s->sa_v].p, s->d_dt, c,
+                               rk != 0, s->grid()));
+  } else {
+    CK(interface_advect<double>(s->stream, s->vof[cv].p, s->vof[1 - cv].p, s->ux[cu].p, s->uy[cu].p, s->uz[cu].p,
+                                s->normal.as<double>(), s->svof[s->sa_v].p, s->svof[1 - s->sa_v].p, s->d_dt, c,
+                                rk != 0, s->grid()));
+  }
   s->cur_v ^= 1;
   return 0;
 }
 
-int launch_predict(svof3d_solver *s, int rk) {
-  k3_tdm_coef<<<1, 128, sizeof(double) * 6 * s->nx, s->stream>>>(s->lap_ux.p, s->lap_cc.p, s->d_dt,
-                                                                 RK_A[rk] + RK_B[rk], s->prm.m_dif, s->prm.t_dif,
-                                                                 s->nx, s->coef.p);
-  CK_LAUNCH();
-  if (0 != rk) s->sa_f ^= 1;
-  Predict3Args a{};
+template <class R>
+int launch_predict_t(svof3d_solver *s, int rk) {
+  Predict3Args<R> a{};
   const int cu = s->cur_u;
   a.ux = s->ux[cu].p;
   a.uy = s->uy[cu].p;
   a.uz = s->uz[cu].p;
   a.t = s->t[cu].p;
   a.p = s->p.p;
-  a.ifrcx = s->ifrcx.p;
-  a.ifrcy = s->ifrcy.p;
-  a.ifrcz = s->ifrcz.p;
+  a.ifrcx = s->ifrcx.as<R>();
+  a.ifrcy = s->ifrcy.as<R>();
+  a.ifrcz = s->ifrcz.as<R>();
   a.ux_new = s->ux[1 - cu].p;
   a.uy_new = s->uy[1 - cu].p;
   a.uz_new = s->uz[1 - cu].p;
@@ -199,10 +214,10 @@ int launch_predict(svof3d_solver *s, int rk) {
   DevBuf *srcs[4][2] = {{&s->sux[0], &s->sux[1]}, {&s->suy[0], &s->suy[1]}, {&s->suz[0], &s->suz[1]},
                         {&s->st[0], &s->st[1]}};
   for (int f = 0; f < 4; f++) {
-    a.sa[f] = srcs[f][s->sa_f]->p;
-    a.sb[f] = srcs[f][1 - s->sa_f]->p;
+    a.sa[f] = srcs[f][s->sa_f]->as<R>();
+    a.sb[f] = srcs[f][1 - s->sa_f]->as<R>();
   }
-  a.fw = s->fw.p;
+  a.fw = s->fw.as<R>();
   a.lap_ux = s->lap_ux.p;
   a.lap_cc = s->lap_cc.p;
   a.coef = s->coef.p;
@@ -223,47 +238,58 @@ int launch_predict(svof3d_solver *s, int rk) {
   a.t_xm = s->prm.t_xm;
   a.t_xp = s->prm.t_xp;
   a.g = s->grid();
-  const long nlines = (long)s->ny * s->nz;
-  k3_predict<<<(unsigned)((nlines + kPredLines - 1) / kPredLines), 256, 0, s->stream>>>(a);
+  CK(predict_launch<R>(s->stream, a));
+  return 0;
+}
+
+int launch_predict(svof3d_solver *s, int rk) {
+  k3_tdm_coef<<<1, 128, sizeof(double) * 6 * s->nx, s->stream>>>(s->lap_ux.p, s->lap_cc.p, s->d_dt,
+                                                                 RK_A[rk] + RK_B[rk], s->prm.m_dif, s->prm.t_dif,
+                                                                 s->nx, s->coef.p);
   CK_LAUNCH();
+  if (0 != rk) s->sa_f ^= 1;
+  const int rc = s->mixed ? launch_predict_t<float>(s, rk) : launch_predict_t<double>(s, rk);
+  if (rc) return 1;
   s->cur_u ^= 1;
   return 0;
 }
 
-// the four Poisson stages; `marks` (may be null) records an event after each
-int launch_potential(svof3d_solver *s, int rk, const std::vector<cudaEvent_t> *marks = nullptr) {
+// the Poisson stages; `mark` (may be empty) is called with the kernel kind
+// after each launch
+using Marker = std::function<int(int)>;
+
+template <class R>
+int launch_potential_t(svof3d_solver *s, int rk, const Marker &mark, const R *twfy, const R *twby, const R *twfz,
+                       const R *twbz) {
   const double gam = RK_A[rk] + RK_B[rk];
   const Grid3 g = s->grid();
-  const int nky = s->ny / 2 + 1;
-  auto mark = [&](int q) -> int {
-    if (marks) CK(cudaEventRecord((*marks)[q], s->stream));
-    return 0;
-  };
-  auto fwd_y = [&]() -> int {
-    CK(pois_fwd_y(s->cols_y, s->stream, s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->uz[s->cur_u].p, s->spec.p,
-                  s->twf_y.p, s->d_dt, gam, s->log2ny, g));
-    return 0;
-  };
-  auto fft_z = [&](const double *tw) -> int {
-    CK(pois_z(s->cols_z, s->stream, s->spec.p, tw, s->log2nz, g));
-    return 0;
-  };
-  auto inv_y = [&]() -> int {
-    CK(pois_inv_y(s->cols_y, s->stream, s->spec.p, s->psi.p, s->twb_y.p, s->log2ny, g));
-    return 0;
-  };
-  if (fwd_y() || mark(0)) return 1;
-  if (fft_z(s->twf_z.p) || mark(1)) return 1;
-  {
-    const long nlines = (long)nky * s->nz;
-    k3_pois_x<<<(unsigned)((nlines + kXsLines - 1) / kXsLines), 256, 0, s->stream>>>(
-        s->spec.p, s->xscratch.p, s->pl.p, s->pu.p, s->evy.p, s->evz.p, g);
-    CK_LAUNCH();
-    if (mark(2)) return 1;
+  auto m = [&](int kind) { return mark ? mark(kind) : 0; };
+  const int passes = s->mixed ? 2 : 1;
+  for (int pass = 0; pass < passes; pass++) {
+    const bool second = pass > 0;
+    const int cu = s->cur_u;
+    CK(pois_fwd_y<R>(s->cols_y, second, s->stream, s->ux[cu].p, s->uy[cu].p, s->uz[cu].p, s->psi.p, s->pl.p,
+                     s->pu.p, s->spec.as<R>(), twfy, s->d_dt, gam, s->log2ny, g));
+    if (m(SVOF3_K_POISSON_FWD)) return 1;
+    CK(pois_z<R>(s->cols_z, s->stream, s->spec.as<R>(), twfz, s->log2nz, g));
+    if (m(SVOF3_K_POISSON_Z)) return 1;
+    CK(pois_x<R>(s->stream, s->spec.as<R>(), s->xscratch.as<R>(), s->pl.p, s->pu.p, s->evy.p, s->evz.p,
+                 s->mixed ? 1 : 0, g));
+    if (m(SVOF3_K_POISSON_SOLVE)) return 1;
+    CK(pois_z<R>(s->cols_z, s->stream, s->spec.as<R>(), twbz, s->log2nz, g));
+    if (m(SVOF3_K_POISSON_Z)) return 1;
+    CK(pois_inv_y<R>(s->cols_y, second, s->stream, s->spec.as<R>(), s->psi.p, twby, s->log2ny, g));
+    if (m(SVOF3_K_POISSON_INV)) return 1;
   }
-  if (fft_z(s->twb_z.p) || mark(3)) return 1;
-  if (inv_y() || mark(4)) return 1;
   return 0;
+}
+
+int launch_potential(svof3d_solver *s, int rk, const Marker &mark = Marker()) {
+  if (s->mixed) {
+    return launch_potential_t<float>(s, rk, mark, s->twf_y32.as<float>(), s->twb_y32.as<float>(),
+                                     s->twf_z32.as<float>(), s->twb_z32.as<float>());
+  }
+  return launch_potential_t<double>(s, rk, mark, s->twf_y.p, s->twb_y.p, s->twf_z.p, s->twb_z.p);
 }
 
 int launch_project(svof3d_solver *s, int rk, int do_vel, int do_p) {
@@ -402,6 +428,15 @@ int build_tables(svof3d_solver *s, const double *xf, const double *xc) {
     return upload(f, twf) || upload(b, twb);
   };
   if (twiddles(ny, s->twf_y, s->twb_y) || twiddles(nz, s->twf_z, s->twb_z)) return 1;
+  // FP32 copies for the mixed path (the FP64 tables rounded once)
+  auto twiddles32 = [&](const DevBuf &src, DevBuf &dst) -> int {
+    std::vector<double> h(src.n);
+    CK(cudaMemcpy(h.data(), src.p, sizeof(double) * src.n, cudaMemcpyDeviceToHost));
+    return upload_f(dst, h);
+  };
+  if (twiddles32(s->twf_y, s->twf_y32) || twiddles32(s->twb_y, s->twb_y32) || twiddles32(s->twf_z, s->twf_z32) ||
+      twiddles32(s->twb_z, s->twb_z32))
+    return 1;
   const int nky = ny / 2 + 1;
   std::vector<double> evy(nky), evz(nz), pl(nx), pu(nx);
   for (size_t j = 0; j < (size_t)nky; j++)
@@ -433,7 +468,8 @@ int svof3d_destroy(svof3d_solver_t *s) {
   }
   DevBuf *bufs[] = {&s->p, &s->psi, &s->curv, &s->normal, &s->ifrcx, &s->ifrcy, &s->ifrcz, &s->dxf, &s->dxc,
                     &s->lap_ux, &s->lap_cc, &s->coef, &s->spec, &s->xscratch, &s->twf_y, &s->twb_y, &s->twf_z,
-                    &s->twb_z, &s->pl, &s->pu, &s->evy, &s->evz, &s->fw, &s->diag};
+                    &s->twb_z, &s->pl, &s->pu, &s->evy, &s->evz, &s->fw, &s->diag, &s->twf_y32, &s->twb_y32,
+                    &s->twf_z32, &s->twb_z32};
   for (DevBuf *b : bufs) dfree(*b);
   if (s->d_dt) cudaFree(s->d_dt);
   if (s->d_minbits) cudaFree(s->d_minbits);
@@ -453,8 +489,11 @@ int svof3d_create(const svof3d_params_t *prm, const double *xf, const double *xc
   if (prm->ny > 2048 || prm->nz > 2048) return fail("svof3d_create: ny and nz must be at most 2048");
   if ((double)prm->nx * (prm->ny + 4) * (prm->nz + 4) > 4.0e9)
     return fail("svof3d_create: %d x %d x %d cells exceed the 32-bit cell index", prm->nx, prm->ny, prm->nz);
+  if (SVOF3_FP64 != prm->precision && SVOF3_MIXED != prm->precision)
+    return fail("svof3d_create: precision must be SVOF3_FP64 or SVOF3_MIXED (got %d)", prm->precision);
   svof3d_solver *s = new svof3d_solver();
   s->prm = *prm;
+  s->mixed = SVOF3_MIXED == prm->precision;
   s->nx = prm->nx;
   s->ny = prm->ny;
   s->nz = prm->nz;
@@ -469,33 +508,37 @@ int svof3d_create(const svof3d_params_t *prm, const double *xf, const double *xc
     return fail("svof3d_create: no CUDA device available (%s)", cudaGetErrorString(cudaGetLastError()));
   }
   const size_t nx = s->nx, ny = s->ny, nz = s->nz;
+  const size_t es = s->mixed ? sizeof(float) : sizeof(double);  // intermediates
   const size_t n_ux = (nx + 1) * (ny + 2) * (nz + 2), n_cc = (nx + 2) * (ny + 2) * (nz + 2);
   const size_t n_vof = (nx + 2) * (ny + 4) * (nz + 4), n_src = nx * ny * nz, n_srcx = (nx - 1) * ny * nz;
   for (int k = 0; k < 2; k++) {
     if (dalloc(s->ux[k], n_ux) || dalloc(s->uy[k], n_cc) || dalloc(s->uz[k], n_cc) || dalloc(s->t[k], n_cc) ||
         dalloc(s->vof[k], n_vof))
       return bail();
-    if (dalloc(s->sux[k], n_srcx) || dalloc(s->suy[k], n_src) || dalloc(s->suz[k], n_src) ||
-        dalloc(s->st[k], n_src) || dalloc(s->svof[k], n_src))
+    if (dalloc(s->sux[k], n_srcx, es) || dalloc(s->suy[k], n_src, es) || dalloc(s->suz[k], n_src, es) ||
+        dalloc(s->st[k], n_src, es) || dalloc(s->svof[k], n_src))
       return bail();
   }
-  if (dalloc(s->p, n_cc) || dalloc(s->psi, n_cc) || dalloc(s->curv, n_cc) ||
-      dalloc(s->normal, 4 * nx * (ny + 2) * (nz + 2)) || dalloc(s->ifrcx, n_srcx) || dalloc(s->ifrcy, n_src) ||
-      dalloc(s->ifrcz, n_src) || dalloc(s->diag, 8))
+  if (dalloc(s->p, n_cc) || dalloc(s->psi, n_cc) || dalloc(s->curv, n_cc, es) ||
+      dalloc(s->normal, 4 * nx * (ny + 2) * (nz + 2), es) || dalloc(s->ifrcx, n_srcx, es) ||
+      dalloc(s->ifrcy, n_src, es) || dalloc(s->ifrcz, n_src, es) || dalloc(s->diag, 8))
     return bail();
   if (build_tables(s, xf, xc)) return bail();
   if (dalloc(s->coef, 9 * nx)) return bail();
   const size_t nky = ny / 2 + 1;
-  if (dalloc(s->spec, 2 * nx * nky * nz) || dalloc(s->xscratch, nx * nky * nz) || dalloc(s->fw, 4 * nx * ny * nz))
+  if (dalloc(s->spec, 2 * nx * nky * nz, es) || dalloc(s->xscratch, nx * nky * nz, es) ||
+      dalloc(s->fw, 4 * nx * ny * nz, es))
     return bail();
   // transforms: one line per warp, 16 / 8 / 4 lines per block by length
   auto pick_cols = [](int n) { return n <= 128 ? 16 : (n <= 256 ? 8 : 4); };
   s->cols_y = pick_cols(s->ny);
   s->cols_z = pick_cols(s->nz);
   {
-    const size_t smy = sizeof(double) * 2 * (ny + 1) * s->cols_y, smz = sizeof(double) * 2 * (nz + 1) * s->cols_z;
+    const size_t smy = es * 2 * (ny + 1) * s->cols_y, smz = es * 2 * (nz + 1) * s->cols_z;
     if (smy > 200 * 1024 || smz > 200 * 1024) return fail("svof3d_create: FFT length too large"), bail();
-    if (cudaSuccess != pois_prepare(s->ny, s->cols_y, s->nz, s->cols_z))
+    const cudaError_t pe = s->mixed ? pois_prepare<float>(s->ny, s->cols_y, s->nz, s->cols_z)
+                                    : pois_prepare<double>(s->ny, s->cols_y, s->nz, s->cols_z);
+    if (cudaSuccess != pe)
       return fail("cudaFuncSetAttribute(Poisson): %s", cudaGetErrorString(cudaGetLastError())), bail();
     const size_t coef_smem = sizeof(double) * 6 * nx;
     if (coef_smem > 200 * 1024) return fail("svof3d_create: nx too large"), bail();
@@ -536,7 +579,13 @@ int svof3d_upload_field(svof3d_solver_t *s, int field, const double *host, size_
   DevBuf *b;
   if (!s || !host) return fail("null argument");
   if (field_buf(s, field, &b)) return 1;
-  if (count != b->n) return fail("field %d holds %zu doubles, got %zu", field, b->n, count);
+  if (count != b->n) return fail("field %d holds %zu values, got %zu", field, b->n, count);
+  if (4 == b->es) {
+    std::vector<float> f(host, host + count);
+    CK(cudaMemcpyAsync(b->p, f.data(), sizeof(float) * count, cudaMemcpyHostToDevice, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return 0;
+  }
   CK(cudaMemcpyAsync(b->p, host, sizeof(double) * count, cudaMemcpyHostToDevice, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   return 0;
@@ -546,7 +595,14 @@ int svof3d_download_field(svof3d_solver_t *s, int field, double *host, size_t co
   DevBuf *b;
   if (!s || !host) return fail("null argument");
   if (field_buf(s, field, &b)) return 1;
-  if (count != b->n) return fail("field %d holds %zu doubles, got %zu", field, b->n, count);
+  if (count != b->n) return fail("field %d holds %zu values, got %zu", field, b->n, count);
+  if (4 == b->es) {
+    std::vector<float> f(count);
+    CK(cudaMemcpyAsync(f.data(), b->p, sizeof(float) * count, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    for (size_t q = 0; q < count; q++) host[q] = (double)f[q];
+    return 0;
+  }
   CK(cudaMemcpyAsync(host, b->p, sizeof(double) * count, cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   return 0;
@@ -717,7 +773,7 @@ int svof3d_profile_step(svof3d_solver_t *s, double *ms, int *launches, int nkind
   }
   std::vector<cudaEvent_t> ev;
   std::vector<int> kind;
-  auto mark = [&](int k) -> int {
+  Marker mark = [&](int k) -> int {
     cudaEvent_t e;
     CK(cudaEventCreate(&e));
     CK(cudaEventRecord(e, s->stream));
@@ -725,49 +781,19 @@ int svof3d_profile_step(svof3d_solver_t *s, double *ms, int *launches, int nkind
     kind.push_back(k);
     return 0;
   };
-  std::vector<cudaEvent_t> pev(5);
-  for (auto &e : pev) cudaEventCreate(&e);
   int rc = mark(-1);
   rc = rc || launch_dt(s) || mark(SVOF3_K_DT);
-  std::vector<float> pms(5, 0.f);
   for (int rk = 0; rk < 3 && !rc; rk++) {
     rc = rc || launch_geom(s) || mark(SVOF3_K_GEOM);
     rc = rc || launch_force(s) || mark(SVOF3_K_FORCE);
     rc = rc || launch_vof(s, rk) || mark(SVOF3_K_VOF);
     rc = rc || launch_predict(s, rk) || mark(SVOF3_K_PREDICT);
-    // the Poisson stages: events after each, start = the predictor's mark
-    cudaEvent_t start = ev.empty() ? nullptr : ev.back();
-    rc = rc || launch_potential(s, rk, &pev);
-    if (!rc) {
-      CK(cudaStreamSynchronize(s->stream));
-      float t;
-      cudaEventElapsedTime(&t, start, pev[0]);
-      ms[SVOF3_K_POISSON_FWD] += t;
-      cudaEventElapsedTime(&t, pev[0], pev[1]);
-      ms[SVOF3_K_POISSON_Z] += t;
-      cudaEventElapsedTime(&t, pev[1], pev[2]);
-      ms[SVOF3_K_POISSON_SOLVE] += t;
-      cudaEventElapsedTime(&t, pev[2], pev[3]);
-      ms[SVOF3_K_POISSON_Z] += t;
-      cudaEventElapsedTime(&t, pev[3], pev[4]);
-      ms[SVOF3_K_POISSON_INV] += t;
-      launches[SVOF3_K_POISSON_FWD] += 1;
-      launches[SVOF3_K_POISSON_Z] += 2;
-      launches[SVOF3_K_POISSON_SOLVE] += 1;
-      launches[SVOF3_K_POISSON_INV] += 1;
-      // restart the chain of marks after the Poisson stages
-      cudaEvent_t e;
-      cudaEventCreate(&e);
-      cudaEventRecord(e, s->stream);
-      ev.push_back(e);
-      kind.push_back(-1);
-    }
+    rc = rc || launch_potential(s, rk, mark);
     rc = rc || launch_project(s, rk, 1, 1) || mark(SVOF3_K_PROJECT);
   }
   cudaError_t e = cudaStreamSynchronize(s->stream);
   if (!rc && cudaSuccess == e) {
     for (size_t q = 1; q < ev.size(); q++) {
-      if (kind[q] < 0) continue;
       float t = 0.f;
       cudaEventElapsedTime(&t, ev[q - 1], ev[q]);
       ms[kind[q]] += t;
@@ -775,7 +801,6 @@ int svof3d_profile_step(svof3d_solver_t *s, double *ms, int *launches, int nkind
     }
   }
   for (cudaEvent_t x : ev) cudaEventDestroy(x);
-  for (cudaEvent_t x : pev) cudaEventDestroy(x);
   if (rc) return 1;
   if (cudaSuccess != e) return fail("svof3d_profile_step: %s", cudaGetErrorString(e));
   return 0;

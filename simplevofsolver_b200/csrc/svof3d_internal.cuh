@@ -77,6 +77,7 @@ __device__ __forceinline__ void for_images(int j, int k, int ny, int nz, bool se
 
 // read-only global load through the non-coherent path
 __device__ __forceinline__ double ldg(const double *p) { return __ldg(p); }
+__device__ __forceinline__ float ldg(const float *p) { return __ldg(p); }
 
 struct RK {
   double a, b, g;
@@ -90,32 +91,36 @@ enum BcKind3 { BC3_ZERO = 0, BC3_DIRICHLET = 1, BC3_NEUMANN = 2, BC3_VOF = 3 };
 // interior rows
 __global__ void k3_halo_bc(double *a, int width, int nh, int ny, int nz, int kind, double lo, double hi);
 
-// interface geometry: corner normals, cell normal, curvature; appends the
-// interfacial cells (normal index / 4) to `work`
-__global__ void k3_geom(const double *__restrict__ vof, double *__restrict__ normal, double *__restrict__ curv,
-                        unsigned *__restrict__ work, unsigned *__restrict__ nwork, Grid3 g);
-// THINC intercept of the listed cells
-__global__ void k3_intercept(const double *__restrict__ vof, double *__restrict__ normal,
-                             const unsigned *__restrict__ work, const unsigned *__restrict__ nwork, Grid3 g);
+// interface kernels (k3_interface.cu), templates on R = double (FP64 path) or
+// float (mixed path): R is the type of curv, normal, ifrc* and of the
+// geometry / THINC arithmetic; vof, velocities and vof sources are FP64.
+// geometry: corner normals, cell normals, curvature (clears and fills the
+// interfacial-cell worklist), then the THINC intercepts of the listed cells
+template <class R>
+cudaError_t interface_geom(cudaStream_t st, const double *vof, R *normal, R *curv, unsigned *work,
+                           unsigned *nwork, Grid3 g);
 // CSF force
-__global__ void k3_force(const double *__restrict__ vof, const double *__restrict__ curv,
-                         double *__restrict__ ifrcx, double *__restrict__ ifrcy, double *__restrict__ ifrcz,
-                         double tension, Grid3 g);
+template <class R>
+cudaError_t interface_force(cudaStream_t st, const double *vof, const R *curv, R *ifrcx, R *ifrcy, R *ifrcz,
+                            double tension, Grid3 g);
 // THINC fluxes, divergence, RK update of vof with halo and walls
-__global__ void k3_vof_advect(const double *__restrict__ vof, double *__restrict__ vof_new,
-                              const double *__restrict__ ux, const double *__restrict__ uy,
-                              const double *__restrict__ uz, const double *__restrict__ normal,
-                              double *__restrict__ src_a, const double *__restrict__ src_b,
-                              const double *__restrict__ dtp, RK rk, int use_b, Grid3 g);
+template <class R>
+cudaError_t interface_advect(cudaStream_t st, const double *vof, double *vof_new, const double *ux,
+                             const double *uy, const double *uz, const R *normal, double *src_a,
+                             const double *src_b, const double *dtp, RK rk, int use_b, Grid3 g);
 
 // momentum / scalar predictor: right-hand sides, increments and the forward
-// Thomas sweep in x-chunks, then the backward sweep and the update
+// Thomas sweep in x-chunks, then the backward sweep and the update.  R is the
+// storage type of the forces, the momentum sources and the sweep scratch; the
+// arithmetic is FP64 in both precisions.
+template <class R>
 struct Predict3Args {
-  const double *ux, *uy, *uz, *p, *t, *ifrcx, *ifrcy, *ifrcz;
+  const double *ux, *uy, *uz, *p, *t;
+  const R *ifrcx, *ifrcy, *ifrcz;
   double *ux_new, *uy_new, *uz_new, *t_new;
-  double *sa[4];        // src_a of ux, uy, uz, t
-  const double *sb[4];  // src_b
-  double *fw;           // forward-sweep scratch, [4][ny nz][nx]
+  R *sa[4];        // src_a of ux, uy, uz, t
+  const R *sb[4];  // src_b
+  R *fw;           // forward-sweep scratch, [4][ny nz][nx]
   const double *lap_ux, *lap_cc;  // 3 per row
   const double *coef;   // [3 sets (ux, uy/uz, t)][L, R, V][nx]
   const double *dtp;
@@ -126,24 +131,35 @@ struct Predict3Args {
   double uy_xm, uy_xp, uz_xm, uz_xp, t_xm, t_xp;
   Grid3 g;
 };
-__global__ void k3_predict(Predict3Args a);
+template <class R>
+cudaError_t predict_launch(cudaStream_t st, const Predict3Args<R> &a);
 // Thomas coefficients of one substep for the three distinct systems
 __global__ void k3_tdm_coef(const double *__restrict__ lap_ux, const double *__restrict__ lap_cc,
                             const double *__restrict__ dtp, double gam, double m_dif, double t_dif, int nx,
                             double *__restrict__ coef);
 
 // Poisson: spectral array S[kz][ky][i] (complex, i fastest)
-// transforms, one warp per line, `cols` (16, 8 or 4) lines per block; the
-// launchers live beside their templates in k3_poisson.cu
+// Poisson stages (k3_poisson.cu), templates on R = double (FP64 path) or float
+// (mixed path): R is the type of the spectrum, the twiddles and the transform
+// arithmetic; the x line solve is FP64.  `cols` (16, 8 or 4) lines per block,
+// one warp per line.  resid: transform the residual b - A psi instead of b;
+// accum: psi += the inverse; pin_gauge: zero the last unknown of the singular
+// (ky, kz) = (0, 0) line.
+template <class R>
 cudaError_t pois_prepare(int ny, int cols_y, int nz, int cols_z);
-cudaError_t pois_fwd_y(int cols, cudaStream_t st, const double *ux, const double *uy, const double *uz, double *spec,
-                       const double *tw, const double *dtp, double gam, int log2n, Grid3 g);
-cudaError_t pois_z(int cols, cudaStream_t st, double *spec, const double *tw, int log2n, Grid3 g);
-cudaError_t pois_inv_y(int cols, cudaStream_t st, const double *spec, double *psi, const double *tw, int log2n,
+template <class R>
+cudaError_t pois_fwd_y(int cols, bool resid, cudaStream_t st, const double *ux, const double *uy, const double *uz,
+                       const double *psi, const double *pl, const double *pu, R *spec, const R *tw,
+                       const double *dtp, double gam, int log2n, Grid3 g);
+template <class R>
+cudaError_t pois_z(int cols, cudaStream_t st, R *spec, const R *tw, int log2n, Grid3 g);
+template <class R>
+cudaError_t pois_x(cudaStream_t st, R *spec, R *scratch, const double *pl, const double *pu, const double *evy,
+                   const double *evz, int pin_gauge, Grid3 g);
+template <class R>
+cudaError_t pois_inv_y(int cols, bool accum, cudaStream_t st, const R *spec, double *psi, const R *tw, int log2n,
                        Grid3 g);
-__global__ void k3_pois_x(double *__restrict__ spec, double *__restrict__ scratch, const double *__restrict__ pl,
-                          const double *__restrict__ pu, const double *__restrict__ evy,
-                          const double *__restrict__ evz, Grid3 g);
+
 // projection and pressure update, in place
 __global__ void k3_project(double *__restrict__ ux, double *__restrict__ uy, double *__restrict__ uz,
                            double *__restrict__ p, const double *__restrict__ psi, const double *__restrict__ dtp,

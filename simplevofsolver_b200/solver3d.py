@@ -25,8 +25,11 @@ class Params3D(ctypes.Structure):
                 ("add_buoyancy", ctypes.c_int),
                 ("uy_xm", ctypes.c_double), ("uy_xp", ctypes.c_double),
                 ("uz_xm", ctypes.c_double), ("uz_xp", ctypes.c_double),
-                ("t_xm", ctypes.c_double), ("t_xp", ctypes.c_double)]
+                ("t_xm", ctypes.c_double), ("t_xp", ctypes.c_double),
+                ("precision", ctypes.c_int)]
 
+
+FP64, MIXED = 0, 1
 
 FIELDS3D = {"ux": 0, "uy": 1, "uz": 2, "p": 3, "t": 4, "vof": 5, "psi": 6, "curv": 7, "normal": 8,
             "ifrcx": 9, "ifrcy": 10, "ifrcz": 11, "srcux_a": 12, "srcux_b": 13, "srcuy_a": 14, "srcuy_b": 15,
@@ -112,14 +115,18 @@ class Solver3D:
                     "poisson_inv", "project"]
 
     def __init__(self, ic: InitialCondition3D, physical: dict, add_buoyancy: bool = False,
-                 uy_walls=(0.0, 0.0), uz_walls=(0.0, 0.0), t_walls=(0.0, 0.0)):
+                 uy_walls=(0.0, 0.0), uz_walls=(0.0, 0.0), t_walls=(0.0, 0.0), precision: str = "fp64"):
+        """precision: "fp64" or "mixed" (see svof3d_b200.h)"""
+        if precision not in ("fp64", "mixed"):
+            raise ValueError(f"precision must be 'fp64' or 'mixed', not {precision!r}")
         L = lib3()
+        self.precision = precision
         self.nx, self.ny, self.nz = int(ic.nx), int(ic.ny), int(ic.nz)
         self.params = Params3D(self.nx, self.ny, self.nz, float(ic.lx), float(ic.ly), float(ic.lz),
                                physical["m_dif"], physical["t_dif"], physical["tension"],
                                physical["coef_dt_adv"], physical["coef_dt_dif"], int(bool(add_buoyancy)),
                                float(uy_walls[0]), float(uy_walls[1]), float(uz_walls[0]), float(uz_walls[1]),
-                               float(t_walls[0]), float(t_walls[1]))
+                               float(t_walls[0]), float(t_walls[1]), MIXED if precision == "mixed" else FP64)
         self._h = ctypes.c_void_p()
         xf, xc = _c(ic.xf), _c(ic.xc)
         _check(L.svof3d_create(ctypes.byref(self.params), xf.ctypes.data, xc.ctypes.data, ctypes.byref(self._h)))
