@@ -4,8 +4,8 @@
 // (curvature, normals, forces) and of the geometry and THINC arithmetic:
 // R = double is the FP64 path, which follows the restatement bit for bit
 // except for exp / log; R = float is the mixed path, where vof, the
-// velocities and the vof sources stay FP64 and only the geometry and the
-// THINC evaluations run in FP32.
+// velocities and the vof sources stay FP64, the geometry and the THINC flux
+// evaluations run in FP32 and the intercept's Newton iteration in FP64.
 //
 //   k3_halo_bc     periodic y and z halos + x wall values of one field
 //   k3_geom        corner normals (2x2x2 differences), cell normal and THINC
@@ -84,13 +84,22 @@ __device__ __forceinline__ T plane_sum(T v00, T v10, T v01, T v11) {
   return +v00 + v10 + v01 + v11;
 }
 
+// 1 / max(|v|, eps) for |v|^2 = s: the restatement's form in FP64; in FP32 a
+// reciprocal square root of max(s, eps^2), which stays on the fast path for
+// the vanishing gradients of the vof tails
+__device__ __forceinline__ double rnorm(double s, double eps) { return 1. / fmax(sqrt(s), eps); }
+__device__ __forceinline__ float rnorm(float s, float eps) { return rsqrtf(fmaxf(s, eps * eps)); }
+// x / y: a division in FP64, a multiplication by the reciprocal in FP32
+__device__ __forceinline__ double div_by(double x, double y) { return x / y; }
+__device__ __forceinline__ float div_by(float x, float y) { return x * (1.f / y); }
+
 // THINC intercept with 2 x 2 x 2 Gauss points (compute_intercept3 of the
-// restatement; src/interface/curvature_tensor.c:50-92 in 2D).  The Newton
-// tolerance is the reference's 1e-12 in FP64 and 1e-6 in FP32.
+// restatement; src/interface/curvature_tensor.c:50-92 in 2D), Newton
+// tolerance 1e-12.
 template <class R>
 __device__ __forceinline__ R thinc_intercept3(const R vof, const R n0, const R n1, const R n2) {
   const int cntmax = 8;
-  const R resmax = sizeof(R) == 8 ? R(1.e-12) : R(1.e-6);
+  const R resmax = R(1.e-12);
   const R gp0 = R(c3_gauss_p[0]), gp1 = R(c3_gauss_p[1]), gw = R(c3_gauss_w[0]);
   const R gp[2] = {gp0, gp1};
   R exps[8];
@@ -199,8 +208,7 @@ __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ 
         const R dvofdx = R(1.) / R(ldg(g.dxc + ic - 1)) * R(plane_dx(a00, a10, a01, a11) + plane_dx(b00, b10, b01, b11));
         const R dvofdy = rdy * R(plane_dy(a00, a10, a01, a11) + plane_dy(b00, b10, b01, b11));
         const R dvofdz = rdz * R(plane_sum(b00, b10, b01, b11) - plane_sum(a00, a10, a01, a11));
-        const R norm = sqrt(+dvofdx * dvofdx + dvofdy * dvofdy + dvofdz * dvofdz);
-        const R norminv = R(1.) / fmax(norm, eps);
+        const R norminv = rnorm(+dvofdx * dvofdx + dvofdy * dvofdy + dvofdz * dvofdz, eps);
         d0 = dvofdx * norminv;
         d1 = dvofdy * norminv;
         d2 = dvofdz * norminv;
@@ -233,11 +241,10 @@ __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ 
                  plane_sum(CU(1, 0, 0), CU(1, 1, 0), CU(1, 0, 1), CU(1, 1, 1));
           R n2 = plane_sum(CL(2, 0, 0), CL(2, 1, 0), CL(2, 0, 1), CL(2, 1, 1)) +
                  plane_sum(CU(2, 0, 0), CU(2, 1, 0), CU(2, 0, 1), CU(2, 1, 1));
-          n0 /= dxf;
-          n1 /= R(g.dy);
-          n2 /= R(g.dz);
-          const R norm = sqrt(+n0 * n0 + n1 * n1 + n2 * n2);
-          const R norminv = R(1.) / fmax(norm, eps);
+          n0 = div_by(n0, dxf);
+          n1 = div_by(n1, R(g.dy));
+          n2 = div_by(n2, R(g.dz));
+          const R norminv = rnorm(+n0 * n0 + n1 * n1 + n2 * n2, eps);
           n0 *= norminv;
           n1 *= norminv;
           n2 *= norminv;
@@ -266,7 +273,10 @@ __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ 
 }
 
 // k3_intercept: THINC intercept of every listed interfacial cell (the normal
-// vector is already stored); one thread per cell, grid-stride over the list
+// vector is already stored); one thread per cell, grid-stride over the list.
+// The Newton iteration runs in FP64 in both precisions: near-full cells
+// (1 - vof below FP32 resolution) have no FP32 solution, and the list holds
+// only the interfacial cells.
 template <class R>
 __global__ void __launch_bounds__(256) k3_intercept(const double *__restrict__ vof, R *__restrict__ normal,
                                                    const unsigned *__restrict__ work,
@@ -279,7 +289,7 @@ __global__ void __launch_bounds__(256) k3_intercept(const double *__restrict__ v
     const unsigned r = c / (unsigned)nx;
     const int j = (int)(r % (unsigned)rows), k = (int)(r / (unsigned)rows);
     R *o = normal + 4L * c;
-    o[3] = thinc_intercept3<R>(R(ldg(vof + ix_vof(g, i, j, k))), o[0], o[1], o[2]);
+    o[3] = R(thinc_intercept3<double>(ldg(vof + ix_vof(g, i, j, k)), (double)o[0], (double)o[1], (double)o[2]));
   }
 }
 
@@ -314,9 +324,11 @@ __global__ void k3_force(const double *__restrict__ vof, const R *__restrict__ c
 // ---------------------------------------------------------------------------
 // THINC/QQ flux helpers (indicator3 and the face fluxes of the restatement):
 // the indicator sums run in R, the flux vel * sum in FP64
-template <class R>
-__device__ __forceinline__ R indicator3(const R *n, R x0, R x1, R x2) {
-  return R(1.) / (R(1.) + exp(R(-2.) * R(kVofBeta) * (+n[0] * x0 + n[1] * x1 + n[2] * x2 + n[3])));
+__device__ __forceinline__ double indicator3(const double *n, double x0, double x1, double x2) {
+  return 1. / (1. + exp(-2. * kVofBeta * (+n[0] * x0 + n[1] * x1 + n[2] * x2 + n[3])));
+}
+__device__ __forceinline__ float indicator3(const float *n, float x0, float x1, float x2) {
+  return __fdividef(1.f, 1.f + expf(-2.f * (float)kVofBeta * (+n[0] * x0 + n[1] * x1 + n[2] * x2 + n[3])));
 }
 
 // flux through the x face i (i in [2, nx]) of row (j, k)
@@ -335,7 +347,7 @@ __device__ __forceinline__ double flux_x(const double *__restrict__ vof, const d
   for (int kk = 0; kk < 2; kk++)
 #pragma unroll
     for (int jj = 0; jj < 2; jj++)
-      flux += R(c3_gauss_w[jj]) * R(c3_gauss_w[kk]) * indicator3<R>(n, x, R(c3_gauss_p[jj]), R(c3_gauss_p[kk]));
+      flux += R(c3_gauss_w[jj]) * R(c3_gauss_w[kk]) * indicator3(n, x, R(c3_gauss_p[jj]), R(c3_gauss_p[kk]));
   return vel * (double)flux;
 }
 
@@ -355,7 +367,7 @@ __device__ __forceinline__ double flux_y(const double *__restrict__ vof, const d
   for (int kk = 0; kk < 2; kk++)
 #pragma unroll
     for (int ii = 0; ii < 2; ii++)
-      flux += R(c3_gauss_w[ii]) * R(c3_gauss_w[kk]) * indicator3<R>(n, R(c3_gauss_p[ii]), y, R(c3_gauss_p[kk]));
+      flux += R(c3_gauss_w[ii]) * R(c3_gauss_w[kk]) * indicator3(n, R(c3_gauss_p[ii]), y, R(c3_gauss_p[kk]));
   return vel * (double)flux;
 }
 
@@ -375,7 +387,7 @@ __device__ __forceinline__ double flux_z(const double *__restrict__ vof, const d
   for (int jj = 0; jj < 2; jj++)
 #pragma unroll
     for (int ii = 0; ii < 2; ii++)
-      flux += R(c3_gauss_w[ii]) * R(c3_gauss_w[jj]) * indicator3<R>(n, R(c3_gauss_p[ii]), R(c3_gauss_p[jj]), z);
+      flux += R(c3_gauss_w[ii]) * R(c3_gauss_w[jj]) * indicator3(n, R(c3_gauss_p[ii]), R(c3_gauss_p[jj]), z);
   return vel * (double)flux;
 }
 
