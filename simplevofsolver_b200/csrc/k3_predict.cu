@@ -1,25 +1,25 @@
-// k3_predict.cu -- momentum / scalar predictor of the FP64 3D path.
+// k3_predict.cu -- momentum / scalar predictor of the 3D path.
 //
-// ux, uy, uz and t each take dt (alpha src_a + beta src_b + gamma src_g),
-// solve (1 - gamma dt nu / 2 Lx) delta' = delta along x, and update
+// ux, uy, uz and t each take delta = dt (alpha src_a + beta src_b + gamma
+// src_g), solve (1 - gamma dt nu / 2 Lx) delta' = delta along x, and update
 // u += delta' (src/fluid/predict/{ux,uy,t}.c in 2D, carried to z by the
-// restatement oracle/svof_oracle3d.c).  The x lines are short and many
-// (ny nz of them), and the Thomas recurrence is serial along a line, so a
-// block owns 32 lines and walks them in 32-cell x-chunks:
+// restatement oracle/svof_oracle3d.c).  Two kernels:
 //
-//   forward, chunk by chunk: all 256 threads evaluate the four right-hand
-//     sides of a 32 x 32 tile (x coalesced), store src_a, and keep the
-//     increments in shared memory; warps 0..3 (one field each, one line per
-//     lane) continue the forward Thomas recurrence through the chunk with the
-//     carry in a register; the swept chunk goes to a scratch array.
-//   backward, chunk by chunk in reverse: the tile comes back, warps 0..3 run
-//     the back substitution, all threads write u + delta' into the other
-//     buffer of the ping-pong pair together with the halo images.
-//   walls: the x wall values of the four fields and their halo images.
+//   k3_rhs     all right-hand sides and increments: a 2.5D stencil that
+//              marches along z with the state planes staged in shared memory
+//              by cp.async one plane ahead; writes src_a and the increments
+//              in a line layout
+//   k3_xsolve  the x lines (ny nz of them, serial recurrences): a block owns
+//              32 lines, walks them in 32-cell chunks forward and backward
+//              with one line per lane of four sweeping warps, and writes the
+//              updated fields with their halo images and walls
 //
-// The Thomas coefficients depend on the substep only and come from
-// k3_tdm_coef (three distinct systems: ux, uy/uz, t).  The arithmetic keeps
-// the restatement's association, so the result matches it bit for bit.
+// The Thomas coefficients depend on the substep only (k3_tdm_coef: three
+// distinct systems, ux, uy/uz, t).  The arithmetic is FP64 with the
+// restatement's association in both precisions, so the FP64 path matches it
+// bit for bit; R is the storage type of forces, sources and increments.
+#include <cuda_pipeline.h>
+
 #include "svof3d_internal.cuh"
 
 namespace svof3 {
@@ -70,57 +70,39 @@ __global__ void k3_tdm_coef(const double *__restrict__ lap_ux, const double *__r
   }
 }
 
-// Right-hand sides of one thread's cell: uy, uz and t at cell i and ux at the
-// face i + 1 (do_ux: i < nx).  The explicit part goes to sa[f], the
-// x-implicit diffusion and the pressure gradient to sg[f], in the
+// The stencil values one cell's right-hand sides read: uy, uz, t at cell i
+// and ux at the face iu = i + 1 (names: u = ux, v = uy, w = uz, t, p; 0 / 1
+// / 2 the x offset from i, s / n the row j -+ 1, b / t the plane k -+ 1).
+struct Stencil4 {
+  double u00, u10, u20, u0s, u1s, u1n, u0b, u1b, u1t;
+  double vc, vxm, vxp, vs, vn, vb, vt, vnb, v1n;
+  double wc, wxm, wxp, ws, wn, wb, wt, wst, w1t;
+  double tc, txm, txp, ts, tn, tb, tt;
+  double pc, ps, pb, pxp;
+  double ifx, ify, ifz;
+  double dxf_i, dxf_i1, dxc_i1;
+  double lu0, lu1, lu2, lc0, lc1, lc2;
+};
+
+// Right-hand sides of one cell (src/fluid/predict/{ux,uy,t}.c compute_rhs_*
+// in 2D, carried to z by the restatement): the explicit part into sa[f], the
+// x-implicit diffusion and the pressure gradient into sg[f], in the
 // restatement's order (advection x, y, z; diffusion x, y, z; pressure;
-// buoyancy; surface).  All stencil values are loaded before any arithmetic,
-// so that the ~50 loads of a cell are in flight together.
-// Field order: 0 ux, 1 uy, 2 uz, 3 t.
+// buoyancy; surface).  Fields 0 ux (do_ux: the face exists), 1 uy, 2 uz, 3 t.
 template <class R>
-__device__ __forceinline__ void rhs4(const Predict3Args<R> &a, const Grid3 &g, int i, int j, int k, bool do_ux,
-                                     double *sa, double *sg) {
-  const double *ux = a.ux, *uy = a.uy, *uz = a.uz, *t = a.t, *p = a.p;
-  // ---- loads
-  const double u00 = ldg(ux + ix_ux(g, i, j, k)), u10 = ldg(ux + ix_ux(g, i + 1, j, k));
-  const double u0s = ldg(ux + ix_ux(g, i, j - 1, k)), u1s = ldg(ux + ix_ux(g, i + 1, j - 1, k));
-  const double u0b = ldg(ux + ix_ux(g, i, j, k - 1)), u1b = ldg(ux + ix_ux(g, i + 1, j, k - 1));
-  const double vc = ldg(uy + ix_cc(g, i, j, k)), vxm = ldg(uy + ix_cc(g, i - 1, j, k));
-  const double vxp = ldg(uy + ix_cc(g, i + 1, j, k));
-  const double vs = ldg(uy + ix_cc(g, i, j - 1, k)), vn = ldg(uy + ix_cc(g, i, j + 1, k));
-  const double vb = ldg(uy + ix_cc(g, i, j, k - 1)), vt = ldg(uy + ix_cc(g, i, j, k + 1));
-  const double vnb = ldg(uy + ix_cc(g, i, j + 1, k - 1));
-  const double wc = ldg(uz + ix_cc(g, i, j, k)), wxm = ldg(uz + ix_cc(g, i - 1, j, k));
-  const double wxp = ldg(uz + ix_cc(g, i + 1, j, k));
-  const double ws = ldg(uz + ix_cc(g, i, j - 1, k)), wn = ldg(uz + ix_cc(g, i, j + 1, k));
-  const double wb = ldg(uz + ix_cc(g, i, j, k - 1)), wt = ldg(uz + ix_cc(g, i, j, k + 1));
-  const double wst = ldg(uz + ix_cc(g, i, j - 1, k + 1));
-  const double tc = ldg(t + ix_cc(g, i, j, k)), txm = ldg(t + ix_cc(g, i - 1, j, k));
-  const double txp = ldg(t + ix_cc(g, i + 1, j, k));
-  const double ts = ldg(t + ix_cc(g, i, j - 1, k)), tn = ldg(t + ix_cc(g, i, j + 1, k));
-  const double tb = ldg(t + ix_cc(g, i, j, k - 1)), tt = ldg(t + ix_cc(g, i, j, k + 1));
-  const double pc = ldg(p + ix_cc(g, i, j, k)), ps = ldg(p + ix_cc(g, i, j - 1, k));
-  const double pb = ldg(p + ix_cc(g, i, j, k - 1));
-  const double ify = ldg(a.ifrcy + ix_src(g, i, j, k)), ifz = ldg(a.ifrcz + ix_src(g, i, j, k));
-  const double dxf_i = ldg(g.dxf + i - 1);
-  const double lc0 = ldg(a.lap_cc + 3 * (i - 1) + 0), lc1 = ldg(a.lap_cc + 3 * (i - 1) + 1);
-  const double lc2 = ldg(a.lap_cc + 3 * (i - 1) + 2);
-  double u20 = 0., u1n = 0., u1t = 0., v1n = 0., w1t = 0., pxp = 0., ifx = 0., dxf_i1 = 1., dxc_i1 = 1.;
-  double lu0 = 0., lu1 = 0., lu2 = 0.;
-  if (do_ux) {
-    u20 = ldg(ux + ix_ux(g, i + 2, j, k));
-    u1n = ldg(ux + ix_ux(g, i + 1, j + 1, k));
-    u1t = ldg(ux + ix_ux(g, i + 1, j, k + 1));
-    v1n = ldg(uy + ix_cc(g, i + 1, j + 1, k));
-    w1t = ldg(uz + ix_cc(g, i + 1, j, k + 1));
-    pxp = ldg(p + ix_cc(g, i + 1, j, k));
-    ifx = ldg(a.ifrcx + ix_srcx(g, i + 1, j, k));
-    dxf_i1 = ldg(g.dxf + i);
-    dxc_i1 = ldg(g.dxc + i);
-    lu0 = ldg(a.lap_ux + 3 * (i - 1) + 0);
-    lu1 = ldg(a.lap_ux + 3 * (i - 1) + 1);
-    lu2 = ldg(a.lap_ux + 3 * (i - 1) + 2);
-  }
+__device__ __forceinline__ void rhs4_values(const Predict3Args<R> &a, const Grid3 &g, const Stencil4 &S, bool do_ux,
+                                            double *sa, double *sg) {
+  const double u00 = S.u00, u10 = S.u10, u20 = S.u20, u0s = S.u0s, u1s = S.u1s, u1n = S.u1n, u0b = S.u0b,
+               u1b = S.u1b, u1t = S.u1t;
+  const double vc = S.vc, vxm = S.vxm, vxp = S.vxp, vs = S.vs, vn = S.vn, vb = S.vb, vt = S.vt, vnb = S.vnb,
+               v1n = S.v1n;
+  const double wc = S.wc, wxm = S.wxm, wxp = S.wxp, ws = S.ws, wn = S.wn, wb = S.wb, wt = S.wt, wst = S.wst,
+               w1t = S.w1t;
+  const double tc = S.tc, txm = S.txm, txp = S.txp, ts = S.ts, tn = S.tn, tb = S.tb, tt = S.tt;
+  const double pc = S.pc, ps = S.ps, pb = S.pb, pxp = S.pxp;
+  const double ifx = S.ifx, ify = S.ify, ifz = S.ifz;
+  const double dxf_i = S.dxf_i, dxf_i1 = S.dxf_i1, dxc_i1 = S.dxc_i1;
+  const double lu0 = S.lu0, lu1 = S.lu1, lu2 = S.lu2, lc0 = S.lc0, lc1 = S.lc1, lc2 = S.lc2;
   const double md = a.m_dif, td = a.t_dif, dy = g.dy, dz = g.dz;
   const double *ly = a.lapy, *lz = a.lapz;
   // ---- ux at the face iu = i + 1: xm = UX(iu-1), xc = UX(iu), xp = UX(iu+1)
@@ -238,11 +220,172 @@ __device__ __forceinline__ void rhs4(const Predict3Args<R> &a, const Grid3 &g, i
   }
 }
 
-constexpr int PL = kPredLines, PC = kPredChunk;
+// ---------------------------------------------------------------------------
+// k3_rhs: the right-hand sides and increments of all cells.  A block owns a
+// 32 x 8 tile of (i, j) and marches along z over RZ planes.  The five state
+// fields ux, uy, uz, t, p live in a ring of four shared-memory planes (a
+// 34 x 10 window each, the tile with its x and y neighbours): planes k - 1,
+// k, k + 1 are read by the stencil while plane k + 2 arrives by cp.async.
+// Writes src_a and the increment delta = dt (alpha src_a + beta src_b +
+// gamma src_g) in the line layout [field][j - 1 + ny (k - 1)][x position]
+// that the line solver reads.
+constexpr int RX = 32, RY = 8, RZ = 16;
+constexpr int WX = RX + 2, WY = RY + 2, NSLOT = 4, NFLD = 5;
+constexpr size_t kRhsSmem = sizeof(double) * NFLD * NSLOT * WY * WX;
+
+size_t rhs_smem_bytes() { return kRhsSmem; }
 
 template <class R>
-__global__ void __launch_bounds__(256, 2) k3_predict(Predict3Args<R> a) {
-  __shared__ double sd[4][PL][PC + 1];  // the four fields' increments of one tile
+__global__ void __launch_bounds__(RX * RY, 2) k3_rhs(Predict3Args<R> a) {
+  extern __shared__ double ring[];  // [NFLD][NSLOT][WY][WX]
+  const Grid3 g = a.g;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int tid = threadIdx.x, tx = tid % RX, ty = tid / RX;
+  const int i0 = 1 + blockIdx.x * RX, j0 = 1 + blockIdx.y * RY, k0 = 1 + blockIdx.z * RZ;
+  const int kend = min(k0 + RZ, nz + 1);  // cells k in [k0, kend)
+  const int i = i0 + tx, j = j0 + ty;
+  const bool mine = i <= nx && j <= ny;
+  const bool do_ux = i < nx;
+  const double *fld[NFLD] = {a.ux, a.uy, a.uz, a.t, a.p};
+  const long width[NFLD] = {nx + 1, nx + 2, nx + 2, nx + 2, nx + 2};
+  const long plane_rows = ny + 2;
+  // window column c <-> storage x = i0 - 1 + c; row r <-> j = j0 - 1 + r
+  auto load_plane = [&](int kk) {
+    const int slot = kk & (NSLOT - 1);
+    for (int f = 0; f < NFLD; f++) {
+      double *dst = ring + ((size_t)f * NSLOT + slot) * WY * WX;
+      const double *src = fld[f] + width[f] * plane_rows * kk;
+      for (int e = tid; e < WY * WX; e += RX * RY) {
+        const int r = e / WX, c = e - r * WX;
+        const long x = i0 - 1 + c;
+        const int jj = j0 - 1 + r;
+        if (x < width[f] && jj <= ny + 1) {
+          __pipeline_memcpy_async(dst + e, src + x + width[f] * jj, sizeof(double));
+        } else {
+          dst[e] = 0.;
+        }
+      }
+    }
+    __pipeline_commit();
+  };
+  load_plane(k0 - 1);
+  load_plane(k0);
+  load_plane(k0 + 1);
+  __pipeline_wait_prior(0);
+  __syncthreads();
+  const double dt = ldg(a.dtp);
+  const double ca = a.rk.a * dt, cb = a.rk.b * dt, cg = a.rk.g * dt;
+  const size_t fstride = (size_t)ny * nz * nx;
+  // per-column constants
+  double dxf_i = 1., dxf_i1 = 1., dxc_i1 = 1., lu0 = 0., lu1 = 0., lu2 = 0., lc0 = 0., lc1 = 0., lc2 = 0.;
+  if (mine) {
+    dxf_i = ldg(g.dxf + i - 1);
+    lc0 = ldg(a.lap_cc + 3 * (i - 1) + 0);
+    lc1 = ldg(a.lap_cc + 3 * (i - 1) + 1);
+    lc2 = ldg(a.lap_cc + 3 * (i - 1) + 2);
+    if (do_ux) {
+      dxf_i1 = ldg(g.dxf + i);
+      dxc_i1 = ldg(g.dxc + i);
+      lu0 = ldg(a.lap_ux + 3 * (i - 1) + 0);
+      lu1 = ldg(a.lap_ux + 3 * (i - 1) + 1);
+      lu2 = ldg(a.lap_ux + 3 * (i - 1) + 2);
+    }
+  }
+  for (int k = k0; k < kend; k++) {
+    if (k + 2 <= min(kend, nz + 1)) load_plane(k + 2);
+    if (mine) {
+      const int sm = (k - 1) & (NSLOT - 1), s0 = k & (NSLOT - 1), sp = (k + 1) & (NSLOT - 1);
+#define RING(f, slot, r, c) ring[(((size_t)(f) * NSLOT + (slot)) * WY + (r)) * WX + (c)]
+      Stencil4 S;
+      // ux (f 0): face iu <-> column iu - i0, i.e. face i <-> tx
+      S.u00 = RING(0, s0, ty + 1, tx);
+      S.u10 = RING(0, s0, ty + 1, tx + 1);
+      S.u20 = RING(0, s0, ty + 1, tx + 2);
+      S.u0s = RING(0, s0, ty, tx);
+      S.u1s = RING(0, s0, ty, tx + 1);
+      S.u1n = RING(0, s0, ty + 2, tx + 1);
+      S.u0b = RING(0, sm, ty + 1, tx);
+      S.u1b = RING(0, sm, ty + 1, tx + 1);
+      S.u1t = RING(0, sp, ty + 1, tx + 1);
+      // cell-centred fields: cell i <-> column tx + 1
+      S.vc = RING(1, s0, ty + 1, tx + 1);
+      S.vxm = RING(1, s0, ty + 1, tx);
+      S.vxp = RING(1, s0, ty + 1, tx + 2);
+      S.vs = RING(1, s0, ty, tx + 1);
+      S.vn = RING(1, s0, ty + 2, tx + 1);
+      S.vb = RING(1, sm, ty + 1, tx + 1);
+      S.vt = RING(1, sp, ty + 1, tx + 1);
+      S.vnb = RING(1, sm, ty + 2, tx + 1);
+      S.v1n = RING(1, s0, ty + 2, tx + 2);
+      S.wc = RING(2, s0, ty + 1, tx + 1);
+      S.wxm = RING(2, s0, ty + 1, tx);
+      S.wxp = RING(2, s0, ty + 1, tx + 2);
+      S.ws = RING(2, s0, ty, tx + 1);
+      S.wn = RING(2, s0, ty + 2, tx + 1);
+      S.wb = RING(2, sm, ty + 1, tx + 1);
+      S.wt = RING(2, sp, ty + 1, tx + 1);
+      S.wst = RING(2, sp, ty, tx + 1);
+      S.w1t = RING(2, sp, ty + 1, tx + 2);
+      S.tc = RING(3, s0, ty + 1, tx + 1);
+      S.txm = RING(3, s0, ty + 1, tx);
+      S.txp = RING(3, s0, ty + 1, tx + 2);
+      S.ts = RING(3, s0, ty, tx + 1);
+      S.tn = RING(3, s0, ty + 2, tx + 1);
+      S.tb = RING(3, sm, ty + 1, tx + 1);
+      S.tt = RING(3, sp, ty + 1, tx + 1);
+      S.pc = RING(4, s0, ty + 1, tx + 1);
+      S.ps = RING(4, s0, ty, tx + 1);
+      S.pb = RING(4, sm, ty + 1, tx + 1);
+      S.pxp = RING(4, s0, ty + 1, tx + 2);
+#undef RING
+      const long is = ix_src(g, i, j, k);
+      S.ify = (double)ldg(a.ifrcy + is);
+      S.ifz = (double)ldg(a.ifrcz + is);
+      S.ifx = do_ux ? (double)ldg(a.ifrcx + ix_srcx(g, i + 1, j, k)) : 0.;
+      S.dxf_i = dxf_i;
+      S.dxf_i1 = dxf_i1;
+      S.dxc_i1 = dxc_i1;
+      S.lu0 = lu0;
+      S.lu1 = lu1;
+      S.lu2 = lu2;
+      S.lc0 = lc0;
+      S.lc1 = lc1;
+      S.lc2 = lc2;
+      double sa[4], sg[4];
+      rhs4_values(a, g, S, do_ux, sa, sg);
+      const size_t line = (size_t)(j - 1) + (size_t)ny * (k - 1);
+      R *dl = a.fw + line * nx + (i - 1);
+      if (do_ux) {
+        const long isx = ix_srcx(g, i + 1, j, k);
+        a.sa[0][isx] = R(sa[0]);
+        const double sb = a.use_b ? cb * (double)ldg(a.sb[0] + isx) : 0.;
+        dl[0] = R(+ca * sa[0] + sb + cg * sg[0]);
+      }
+#pragma unroll
+      for (int q = 1; q < 4; q++) {
+        a.sa[q][is] = R(sa[q]);
+        const double sb = a.use_b ? cb * (double)ldg(a.sb[q] + is) : 0.;
+        dl[q * fstride] = R(+ca * sa[q] + sb + cg * sg[q]);
+      }
+    }
+    __pipeline_wait_prior(0);
+    __syncthreads();
+  }
+}
+
+constexpr int PL = kPredLines, PC = kPredChunk;
+
+// ---------------------------------------------------------------------------
+// k3_xsolve: the implicit-x Thomas sweeps of the four fields and the update.
+// A block owns 32 lines, walked in 32-cell x-chunks: forward (the increments
+// come in from the line array, warps 0..3 continue the recurrence with the
+// carry in a register, one field per warp and one line per lane, the swept
+// values go back), then backward in reverse chunk order with the update
+// u + delta' into the other buffer of the ping-pong pair, halo images
+// included, then the walls.
+template <class R>
+__global__ void __launch_bounds__(256) k3_xsolve(Predict3Args<R> a) {
+  __shared__ double sd[4][PL][PC + 1];  // the four fields' values of one tile
   __shared__ double sco[9][PC];         // L, R, V of the three systems, one chunk
   const Grid3 g = a.g;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
@@ -251,14 +394,12 @@ __global__ void __launch_bounds__(256, 2) k3_predict(Predict3Args<R> a) {
   const int tid = threadIdx.x;
   const int tx = tid & 31, ty = tid >> 5;
   const int nchunks = (nx + PC - 1) / PC;
-  const double dt = ldg(a.dtp);
-  const double ca = a.rk.a * dt, cb = a.rk.b * dt, cg = a.rk.g * dt;
   // the sweeping warps: warp f < 4 owns field f, lane = line of the block
   const int f = ty;
   const bool sweeper = f < 4 && (l0 + tx < nlines);
   const int set = (0 == f) ? 0 : (3 == f ? 2 : 1);
   const int nf = (0 == f) ? nx - 1 : nx;
-  const size_t fstride = (size_t)nlines * nx;  // scratch per field
+  const size_t fstride = (size_t)nlines * nx;  // line array per field
   double carry = 0.;
 
   // ------------------------------------------------------------ forward
@@ -272,45 +413,29 @@ __global__ void __launch_bounds__(256, 2) k3_predict(Predict3Args<R> a) {
     for (int m = 0; m < 4; m++) {
       const int ll = ty + 8 * m;
       const long l = l0 + ll;
-      if (l >= nlines) continue;
-      const int j = 1 + (int)(l % ny), k = 1 + (int)(l / ny);
       const int p = p0 + tx;
-      if (p >= nx) continue;
-      // cell i = p + 1 for uy, uz, t (line position p) and face i + 1 for ux
-      // (line position p of the ux system, which has nx - 1 unknowns)
-      const int i = p + 1;
-      const bool do_ux = p < nx - 1;
-      double sa[4], sg[4];
-      rhs4(a, g, i, j, k, do_ux, sa, sg);
-      if (do_ux) {
-        const long is = ix_srcx(g, i + 1, j, k);
-        a.sa[0][is] = R(sa[0]);
-        const double sb = a.use_b ? cb * ldg(a.sb[0] + is) : 0.;
-        sd[0][ll][tx] = +ca * sa[0] + sb + cg * sg[0];
-      }
-      const long is = ix_src(g, i, j, k);
-#pragma unroll
-      for (int q = 1; q < 4; q++) {
-        a.sa[q][is] = R(sa[q]);
-        const double sb = a.use_b ? cb * ldg(a.sb[q] + is) : 0.;
-        sd[q][ll][tx] = +ca * sa[q] + sb + cg * sg[q];
-      }
+      if (l >= nlines || p >= nx) continue;
+      const R *fw = a.fw + (size_t)l * nx + p;
+      sd[0][ll][tx] = (p < nx - 1) ? (double)fw[0] : 0.;
+      sd[1][ll][tx] = fw[fstride];
+      sd[2][ll][tx] = fw[2 * fstride];
+      sd[3][ll][tx] = fw[3 * fstride];
     }
     __syncthreads();
     if (sweeper) {
       double *q = sd[f][tx];
-      const double *L = sco[3 * set], *R = sco[3 * set + 1];
+      const double *L = sco[3 * set], *Rr = sco[3 * set + 1];
       const int smax = min(PC, nf - p0);
 #pragma unroll 4
       for (int s = 0; s < smax; s++) {
         const int pp = p0 + s;
         const double x = q[s];
         if (0 == pp) {
-          carry = x / R[s];
+          carry = x / Rr[s];
         } else if (pp < nf - 1) {
-          carry = R[s] * (x - L[s] * carry);
+          carry = Rr[s] * (x - L[s] * carry);
         } else {
-          carry = (0. != R[s]) ? R[s] * (x - L[s] * carry) : 0.;
+          carry = (0. != Rr[s]) ? Rr[s] * (x - L[s] * carry) : 0.;
         }
         q[s] = carry;
       }
@@ -430,9 +555,20 @@ __global__ void __launch_bounds__(256, 2) k3_predict(Predict3Args<R> a) {
 
 template <class R>
 cudaError_t predict_launch(cudaStream_t st, const Predict3Args<R> &a) {
-  const long nlines = (long)a.g.ny * a.g.nz;
-  k3_predict<R><<<(unsigned)((nlines + PL - 1) / PL), 256, 0, st>>>(a);
+  const Grid3 &g = a.g;
+  dim3 gr((g.nx + RX - 1) / RX, (g.ny + RY - 1) / RY, (g.nz + RZ - 1) / RZ);
+  k3_rhs<R><<<gr, RX * RY, kRhsSmem, st>>>(a);
+  cudaError_t e = cudaGetLastError();
+  if (cudaSuccess != e) return e;
+  const long nlines = (long)g.ny * g.nz;
+  k3_xsolve<R><<<(unsigned)((nlines + PL - 1) / PL), 256, 0, st>>>(a);
   return cudaGetLastError();
+}
+
+cudaError_t predict_prepare() {
+  cudaError_t e = cudaFuncSetAttribute(k3_rhs<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRhsSmem);
+  if (cudaSuccess != e) return e;
+  return cudaFuncSetAttribute(k3_rhs<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRhsSmem);
 }
 template cudaError_t predict_launch<double>(cudaStream_t, const Predict3Args<double> &);
 template cudaError_t predict_launch<float>(cudaStream_t, const Predict3Args<float> &);

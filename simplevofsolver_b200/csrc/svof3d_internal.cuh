@@ -133,6 +133,8 @@ struct Predict3Args {
 };
 template <class R>
 cudaError_t predict_launch(cudaStream_t st, const Predict3Args<R> &a);
+// opt-in shared memory of the right-hand-side kernel (once per device)
+cudaError_t predict_prepare();
 // Thomas coefficients of one substep for the three distinct systems
 __global__ void k3_tdm_coef(const double *__restrict__ lap_ux, const double *__restrict__ lap_cc,
                             const double *__restrict__ dtp, double gam, double m_dif, double t_dif, int nx,
