@@ -20,6 +20,8 @@
 // march along z through a 32 x 4 tile: each plane's inputs are read once,
 // the corner normals of the plane below and the z-face flux of the cell below
 // are kept from the previous plane.
+#include <cuda_pipeline.h>
+
 #include "svof3d_internal.cuh"
 
 namespace svof3 {
@@ -171,7 +173,7 @@ template <class R>
 __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ vof, R *__restrict__ normal,
                                                     R *__restrict__ curv, unsigned *__restrict__ work,
                                                     unsigned *__restrict__ nwork, Grid3 g) {
-  __shared__ double sv[2][G3Y + 2][G3X + 2];
+  __shared__ double sv[3][G3Y + 2][G3X + 2];  // vof planes, plane p in slot (p - k0 + 1) % 3
   __shared__ R sc[2][3][G3Y + 1][G3X + 1];
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int i0 = 1 + blockIdx.x * G3X;
@@ -182,19 +184,25 @@ __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ 
   const int tx = tid % G3X, ty = tid / G3X;
   const R eps = R(kDblEpsilon);
   const R rdy = R(1.) / R(g.dy), rdz = R(1.) / R(g.dz);
-  auto load_plane = [&](int buf, int k) {
+  // cp.async: the next plane arrives while the current one is processed
+  auto load_plane = [&](int k) {
+    const int buf = (k - k0 + 1) % 3;
     for (int t = tid; t < (G3X + 2) * (G3Y + 2); t += G3X * G3Y) {
       const int li = t % (G3X + 2), lj = t / (G3X + 2);
       const int i = i0 - 1 + li, j = j0 - 1 + lj;
-      sv[buf][lj][li] = (i <= nx + 1 && j <= ny + 2) ? ldg(vof + ix_vof(g, i, j, k)) : 0.;
+      if (i <= nx + 1 && j <= ny + 2) __pipeline_memcpy_async(&sv[buf][lj][li], vof + ix_vof(g, i, j, k), 8);
+      else sv[buf][lj][li] = 0.;
     }
+    __pipeline_commit();
   };
-  load_plane(0, k0 - 1);
+  load_plane(k0 - 1);
+  load_plane(k0);
+  __pipeline_wait_prior(0);
+  __syncthreads();
   for (int kc = k0; kc <= kend; kc++) {
-    const int bcur = (kc - k0 + 1) & 1, bprev = bcur ^ 1;
+    const int bcur = (kc - k0 + 1) % 3, bprev = (kc - k0) % 3;
     const int ccur = (kc - k0) & 1, cprev = ccur ^ 1;
-    load_plane(bcur, kc);
-    __syncthreads();
+    if (kc + 1 <= kend) load_plane(kc + 1);
     // compute_gradient at corners (ic, jc, kc): planes kc-1 (bprev) and kc (bcur)
     for (int t = tid; t < (G3X + 1) * (G3Y + 1); t += G3X * G3Y) {
       const int li = t % (G3X + 1), lj = t / (G3X + 1);
@@ -268,6 +276,7 @@ __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ 
         }
       }
     }
+    __pipeline_wait_prior(0);
     __syncthreads();
   }
 }
@@ -331,127 +340,153 @@ __device__ __forceinline__ float indicator3(const float *n, float x0, float x1, 
   return __fdividef(1.f, 1.f + expf(-2.f * (float)kVofBeta * (+n[0] * x0 + n[1] * x1 + n[2] * x2 + n[3])));
 }
 
-// flux through the x face i (i in [2, nx]) of row (j, k)
-template <class R>
-__device__ __forceinline__ double flux_x(const double *__restrict__ vof, const double *__restrict__ ux,
-                                         const R *__restrict__ normal, const Grid3 &g, int i, int j, int k) {
-  const double vel = ldg(ux + ix_ux(g, i, j, k));
-  const int ii = vel < 0. ? i : i - 1;
-  const R x = vel < 0. ? R(-0.5) : R(+0.5);
-  const double lvof = ldg(vof + ix_vof(g, ii, j, k));
+// flux through one face given its velocity and the vof of the cells below
+// (lo) and above (hi) it along the face normal, AXIS 0 / 1 / 2 = x / y / z
+// (update/flx{x,y}.c and the restatement's z face): the upwind cell's
+// vof times the velocity outside the interface, else the velocity times the
+// 2 x 2 Gauss-point THINC indicator of the upwind cell on the face
+template <class R, int AXIS>
+__device__ __forceinline__ double face_flux(double vel, double vlo, double vhi, const R *__restrict__ normal,
+                                            long nrm_lo, long nrm_hi) {
+  const bool neg = vel < 0.;
+  const double lvof = neg ? vhi : vlo;
   if (lvof < kVofMin || 1. - kVofMin < lvof) return vel * lvof;
+  const R c = neg ? R(-0.5) : R(+0.5);
   R n[4];
-  load_normal(normal, ix_nrm(g, ii, j, k), n);
+  load_normal(normal, neg ? nrm_hi : nrm_lo, n);
   R flux = R(0.);
 #pragma unroll
-  for (int kk = 0; kk < 2; kk++)
+  for (int b = 0; b < 2; b++)
 #pragma unroll
-    for (int jj = 0; jj < 2; jj++)
-      flux += R(c3_gauss_w[jj]) * R(c3_gauss_w[kk]) * indicator3(n, x, R(c3_gauss_p[jj]), R(c3_gauss_p[kk]));
+    for (int a = 0; a < 2; a++) {
+      const R pa = R(c3_gauss_p[a]), pb = R(c3_gauss_p[b]);
+      const R wgt = R(c3_gauss_w[a]) * R(c3_gauss_w[b]);
+      if (0 == AXIS) flux += wgt * indicator3(n, c, pa, pb);
+      else if (1 == AXIS) flux += wgt * indicator3(n, pa, c, pb);
+      else flux += wgt * indicator3(n, pa, pb, c);
+    }
   return vel * (double)flux;
 }
 
-// flux through the y face j (j in [1, ny+1]) of column (i, k)
-template <class R>
-__device__ __forceinline__ double flux_y(const double *__restrict__ vof, const double *__restrict__ uy,
-                                         const R *__restrict__ normal, const Grid3 &g, int i, int j, int k) {
-  const double vel = ldg(uy + ix_cc(g, i, j, k));
-  const int jj = vel < 0. ? j : j - 1;
-  const R y = vel < 0. ? R(-0.5) : R(+0.5);
-  const double lvof = ldg(vof + ix_vof(g, i, jj, k));
-  if (lvof < kVofMin || 1. - kVofMin < lvof) return vel * lvof;
-  R n[4];
-  load_normal(normal, ix_nrm(g, i, jj, k), n);
-  R flux = R(0.);
-#pragma unroll
-  for (int kk = 0; kk < 2; kk++)
-#pragma unroll
-    for (int ii = 0; ii < 2; ii++)
-      flux += R(c3_gauss_w[ii]) * R(c3_gauss_w[kk]) * indicator3(n, R(c3_gauss_p[ii]), y, R(c3_gauss_p[kk]));
-  return vel * (double)flux;
-}
-
-// flux through the z face k (k in [1, nz+1]) of column (i, j)
-template <class R>
-__device__ __forceinline__ double flux_z(const double *__restrict__ vof, const double *__restrict__ uz,
-                                         const R *__restrict__ normal, const Grid3 &g, int i, int j, int k) {
-  const double vel = ldg(uz + ix_cc(g, i, j, k));
-  const int kk = vel < 0. ? k : k - 1;
-  const R z = vel < 0. ? R(-0.5) : R(+0.5);
-  const double lvof = ldg(vof + ix_vof(g, i, j, kk));
-  if (lvof < kVofMin || 1. - kVofMin < lvof) return vel * lvof;
-  R n[4];
-  load_normal(normal, ix_nrm(g, i, j, kk), n);
-  R flux = R(0.);
-#pragma unroll
-  for (int jj = 0; jj < 2; jj++)
-#pragma unroll
-    for (int ii = 0; ii < 2; ii++)
-      flux += R(c3_gauss_w[ii]) * R(c3_gauss_w[jj]) * indicator3(n, R(c3_gauss_p[ii]), R(c3_gauss_p[jj]), z);
-  return vel * (double)flux;
-}
-
-// k3_vof_advect: cells i in [1, nx], j in [1, ny], k in [1, nz]; block 32 x 4
-// cells marching over V3Z planes.  x and y face fluxes of a plane are staged
-// in shared memory; the z-face flux below a cell is the one above it in the
-// previous plane.  Writes vof_new with its halo images (two layers) and zero
-// x walls, and src_a.  The flux divergence and the update are FP64 in both
+// k3_vof_advect: cells i in [1, nx], j in [1, ny], k in [1, nz].  A block
+// owns a 32 x 8 tile of (i, j) and marches along z over AZ planes; vof (34 x
+// 10 windows), the x and y face velocities of the tile, the z face velocities
+// and src_b live in a ring of four shared-memory planes that cp.async fills
+// two planes ahead.  The x and y face fluxes of a plane are staged in shared
+// memory; the z-face flux below a cell is the one above it in the previous
+// plane.  Writes vof_new with its halo images (two layers) and zero x walls,
+// and src_a.  The flux divergence and the update are FP64 in both
 // precisions, so that the update conserves volume to FP64 round-off.
-constexpr int V3X = 32, V3Y = 4, V3Z = 8;
+constexpr int AX = 32, AY = 8, AZ = 16, AWX = AX + 2, AWY = AY + 2, ASLOT = 4;
+constexpr int kVofRing = ASLOT * AWY * AWX, kUxRing = ASLOT * AY * (AX + 1), kUyRing = ASLOT * (AY + 1) * AX;
+constexpr int kUzRing = ASLOT * AY * AX, kSbRing = ASLOT * AY * AX;
+constexpr size_t kAdvectSmem =
+    sizeof(double) * (kVofRing + kUxRing + kUyRing + kUzRing + kSbRing + AY * (AX + 1) + (AY + 1) * AX);
 
 template <class R>
-__global__ void __launch_bounds__(V3X * V3Y) k3_vof_advect(const double *__restrict__ vof,
-                                                          double *__restrict__ vof_new,
-                                                          const double *__restrict__ ux,
-                                                          const double *__restrict__ uy,
-                                                          const double *__restrict__ uz,
-                                                          const R *__restrict__ normal,
-                                                          double *__restrict__ src_a,
-                                                          const double *__restrict__ src_b,
-                                                          const double *__restrict__ dtp, RK rk, int use_b,
-                                                          Grid3 g) {
-  __shared__ double fx[V3Y][V3X + 1];
-  __shared__ double fy[V3Y + 1][V3X];
+__global__ void __launch_bounds__(AX * AY) k3_vof_advect(const double *__restrict__ vof, double *__restrict__ vof_new,
+                                                        const double *__restrict__ ux, const double *__restrict__ uy,
+                                                        const double *__restrict__ uz, const R *__restrict__ normal,
+                                                        double *__restrict__ src_a, const double *__restrict__ src_b,
+                                                        const double *__restrict__ dtp, RK rk, int use_b, Grid3 g) {
+  extern __shared__ double sm[];
+  double *vr = sm;                  // [ASLOT][AWY][AWX]  vof, rows j0-1.., cols i0-1..
+  double *xr = vr + kVofRing;       // [ASLOT][AY][AX+1]  ux faces i0 .. i0+32
+  double *yr = xr + kUxRing;        // [ASLOT][AY+1][AX]  uy faces j0 .. j0+8
+  double *zr = yr + kUyRing;        // [ASLOT][AY][AX]    uz face k (plane k)
+  double *br = zr + kUzRing;        // [ASLOT][AY][AX]    src_b
+  double *fx = br + kSbRing;        // [AY][AX+1]
+  double *fy = fx + AY * (AX + 1);  // [AY+1][AX]
   const int nx = g.nx, ny = g.ny, nz = g.nz;
-  const int i0 = 1 + blockIdx.x * V3X;
-  const int j0 = 1 + blockIdx.y * V3Y;
-  const int k0 = 1 + blockIdx.z * V3Z;
-  const int kend = min(k0 + V3Z, nz + 1);
-  const int tid = threadIdx.x;
-  const int tx = tid % V3X, ty = tid / V3X;
+  const int tid = threadIdx.x, tx = tid % AX, ty = tid / AX;
+  const int i0 = 1 + blockIdx.x * AX, j0 = 1 + blockIdx.y * AY, k0 = 1 + blockIdx.z * AZ;
+  const int kend = min(k0 + AZ, nz + 1);  // cells k in [k0, kend)
   const int i = i0 + tx, j = j0 + ty;
   const bool mine = (i <= nx && j <= ny);
-  const double dt = ldg(dtp);
-  double fz_lo = 0.;
-  if (mine) fz_lo = flux_z<R>(vof, uz, normal, g, i, j, k0);
-  for (int k = k0; k < kend; k++) {
-    for (int t = tid; t < V3Y * (V3X + 1); t += V3X * V3Y) {
-      const int li = t % (V3X + 1), lj = t / (V3X + 1);
-      const int fi = i0 + li, fj = j0 + lj;
-      double f = 0.;
-      if (fi >= 2 && fi <= nx && fj <= ny) f = flux_x<R>(vof, ux, normal, g, fi, fj, k);
-      fx[lj][li] = f;
+  const long vw = nx + 2, vrows = ny + 4, uw = nx + 1, crow = ny + 2;
+  auto cp = [](double *dst, const double *src) { __pipeline_memcpy_async(dst, src, sizeof(double)); };
+  auto load_plane = [&](int kk) {
+    const int sl = kk & (ASLOT - 1);
+    // vof window, planes k0 - 1 .. kend + 1
+    for (int e = tid; e < AWY * AWX; e += AX * AY) {
+      const int r = e / AWX, c = e - r * AWX;
+      const int x = i0 - 1 + c, jj = j0 - 1 + r;
+      double *d = vr + (size_t)sl * AWY * AWX + e;
+      if (x <= nx + 1 && jj <= ny + 2) cp(d, vof + x + vw * ((jj + 1) + vrows * (kk + 1)));
+      else *d = 0.;
     }
-    for (int t = tid; t < (V3Y + 1) * V3X; t += V3X * V3Y) {
-      const int li = t % V3X, lj = t / V3X;
-      const int fi = i0 + li, fj = j0 + lj;
+    // z face velocities of planes k0 .. kend (the top face of the last cell)
+    if (kk >= k0 && kk <= kend && mine) cp(zr + (size_t)sl * AY * AX + tid, uz + ix_cc(g, i, j, kk));
+    if (kk >= k0 && kk < kend) {
+      for (int e = tid; e < AY * (AX + 1); e += AX * AY) {
+        const int r = e / (AX + 1), c = e - r * (AX + 1);
+        const int fi = i0 + c, jj = j0 + r;  // face fi, storage fi - 1
+        double *d = xr + (size_t)sl * AY * (AX + 1) + e;
+        if (fi <= nx + 1 && jj <= ny) cp(d, ux + (fi - 1) + uw * (jj + crow * kk));
+        else *d = 0.;
+      }
+      for (int e = tid; e < (AY + 1) * AX; e += AX * AY) {
+        const int r = e / AX, c = e - r * AX;
+        const int ii = i0 + c, fj = j0 + r;
+        double *d = yr + (size_t)sl * (AY + 1) * AX + e;
+        if (ii <= nx && fj <= ny + 1) cp(d, uy + ii + vw * (fj + crow * kk));
+        else *d = 0.;
+      }
+      if (use_b && mine) cp(br + (size_t)sl * AY * AX + tid, src_b + ix_src(g, i, j, kk));
+    }
+    __pipeline_commit();
+  };
+  load_plane(k0 - 1);
+  load_plane(k0);
+  load_plane(k0 + 1);
+  __pipeline_wait_prior(0);
+  __syncthreads();
+  const double dt = ldg(dtp);
+  // 1 / dx of the flux divergence, once per thread (same values)
+  const double rdx = mine ? 1. / ldg(g.dxf + i - 1) : 0., rdy = 1. / g.dy, rdz = 1. / g.dz;
+#define VR(sl, r, c) vr[((size_t)(sl) * AWY + (r)) * AWX + (c)]
+  double fz_lo = 0.;
+  if (mine) {
+    const int sm1 = (k0 - 1) & (ASLOT - 1), s0 = k0 & (ASLOT - 1);
+    fz_lo = face_flux<R, 2>(zr[(size_t)s0 * AY * AX + tid], VR(sm1, ty + 1, tx + 1), VR(s0, ty + 1, tx + 1), normal,
+                            ix_nrm(g, i, j, k0 - 1), ix_nrm(g, i, j, k0));
+  }
+  for (int k = k0; k < kend; k++) {
+    if (k + 2 <= kend + 1) load_plane(k + 2);
+    const int s0 = k & (ASLOT - 1), sp = (k + 1) & (ASLOT - 1);
+    for (int e = tid; e < AY * (AX + 1); e += AX * AY) {
+      const int r = e / (AX + 1), c = e - r * (AX + 1);
+      const int fi = i0 + c, fj = j0 + r;
       double f = 0.;
-      if (fi <= nx && fj <= ny + 1) f = flux_y<R>(vof, uy, normal, g, fi, fj, k);
-      fy[lj][li] = f;
+      if (fi >= 2 && fi <= nx && fj <= ny)
+        f = face_flux<R, 0>(xr[((size_t)s0 * AY + r) * (AX + 1) + c], VR(s0, r + 1, c), VR(s0, r + 1, c + 1), normal,
+                            ix_nrm(g, fi - 1, fj, k), ix_nrm(g, fi, fj, k));
+      fx[r * (AX + 1) + c] = f;
+    }
+    for (int e = tid; e < (AY + 1) * AX; e += AX * AY) {
+      const int r = e / AX, c = e - r * AX;
+      const int fi = i0 + c, fj = j0 + r;
+      double f = 0.;
+      if (fi <= nx && fj <= ny + 1)
+        f = face_flux<R, 1>(yr[((size_t)s0 * (AY + 1) + r) * AX + c], VR(s0, r, c + 1), VR(s0, r + 1, c + 1), normal,
+                            ix_nrm(g, fi, fj - 1, k), ix_nrm(g, fi, fj, k));
+      fy[r * AX + c] = f;
     }
     double fz_hi = 0.;
-    if (mine) fz_hi = flux_z<R>(vof, uz, normal, g, i, j, k + 1);
+    if (mine)
+      fz_hi = face_flux<R, 2>(zr[(size_t)sp * AY * AX + tid], VR(s0, ty + 1, tx + 1), VR(sp, ty + 1, tx + 1), normal,
+                              ix_nrm(g, i, j, k), ix_nrm(g, i, j, k + 1));
     __syncthreads();
     if (mine) {
       double s = 0.;
-      s += 1. / ldg(g.dxf + i - 1) * (+fx[ty][tx] - fx[ty][tx + 1]);
-      s += 1. / g.dy * (+fy[ty][tx] - fy[ty + 1][tx]);
-      s += 1. / g.dz * (+fz_lo - fz_hi);
+      s += rdx * (+fx[ty * (AX + 1) + tx] - fx[ty * (AX + 1) + tx + 1]);
+      s += rdy * (+fy[ty * AX + tx] - fy[(ty + 1) * AX + tx]);
+      s += rdz * (+fz_lo - fz_hi);
       const long is = ix_src(g, i, j, k);
       src_a[is] = s;
-      double v = ldg(vof + ix_vof(g, i, j, k));
+      double v = VR(s0, ty + 1, tx + 1);
       v += dt * rk.a * s;
-      if (use_b) v += dt * rk.b * ldg(src_b + is);
+      if (use_b) v += dt * rk.b * br[(size_t)s0 * AY * AX + tid];
       // images: two halo layers in y and z
       const bool hj = (j >= ny - 1) || (j <= 2), hk = (k >= nz - 1) || (k <= 2);
       const int j2 = (j >= ny - 1) ? j - ny : j + ny;
@@ -469,8 +504,10 @@ __global__ void __launch_bounds__(V3X * V3Y) k3_vof_advect(const double *__restr
       }
     }
     fz_lo = fz_hi;
+    __pipeline_wait_prior(0);
     __syncthreads();
   }
+#undef VR
 }
 
 // ---- host-side launchers
@@ -498,9 +535,16 @@ template <class R>
 cudaError_t interface_advect(cudaStream_t st, const double *vof, double *vof_new, const double *ux,
                              const double *uy, const double *uz, const R *normal, double *src_a,
                              const double *src_b, const double *dtp, RK rk, int use_b, Grid3 g) {
-  dim3 gr((g.nx + V3X - 1) / V3X, (g.ny + V3Y - 1) / V3Y, (g.nz + V3Z - 1) / V3Z);
-  k3_vof_advect<R><<<gr, V3X * V3Y, 0, st>>>(vof, vof_new, ux, uy, uz, normal, src_a, src_b, dtp, rk, use_b, g);
+  dim3 gr((g.nx + AX - 1) / AX, (g.ny + AY - 1) / AY, (g.nz + AZ - 1) / AZ);
+  k3_vof_advect<R><<<gr, AX * AY, kAdvectSmem, st>>>(vof, vof_new, ux, uy, uz, normal, src_a, src_b, dtp, rk, use_b, g);
   return cudaGetLastError();
+}
+
+cudaError_t interface_prepare() {
+  cudaError_t e =
+      cudaFuncSetAttribute(k3_vof_advect<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAdvectSmem);
+  if (cudaSuccess != e) return e;
+  return cudaFuncSetAttribute(k3_vof_advect<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAdvectSmem);
 }
 
 #define SVOF3_INTERFACE_INST(R)                                                                                \

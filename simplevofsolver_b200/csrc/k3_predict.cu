@@ -84,14 +84,42 @@ struct Stencil4 {
   double lu0, lu1, lu2, lc0, lc1, lc2;
 };
 
+// The quotients of grid spacings the right-hand sides use, each evaluated
+// once (per column for the x ones) with the expression the restatement
+// evaluates per cell, hence the same values: h.. = +-0.5 / d., r.. = 1 / d.,
+// w_xm / w_xp the x interpolation weights of the ux face.
+struct RhsCoef {
+  double hxc0, hxc1, w_xm, w_xp, rdxc;  // face iu = i + 1
+  double hxf0, hxf1;                    // cell i
+  double hy0, hy1, hz0, hz1, rdy, rdz;
+};
+
+__device__ __forceinline__ RhsCoef rhs_coef(double dxf_i, double dxf_i1, double dxc_i1, double dy, double dz) {
+  RhsCoef c;
+  c.hxc0 = +0.5 / dxc_i1;
+  c.hxc1 = -0.5 / dxc_i1;
+  c.w_xm = 0.5 * dxf_i / dxc_i1;
+  c.w_xp = 0.5 * dxf_i1 / dxc_i1;
+  c.rdxc = 1. / dxc_i1;
+  c.hxf0 = +0.5 / dxf_i;
+  c.hxf1 = -0.5 / dxf_i;
+  c.hy0 = +0.5 / dy;
+  c.hy1 = -0.5 / dy;
+  c.hz0 = +0.5 / dz;
+  c.hz1 = -0.5 / dz;
+  c.rdy = 1. / dy;
+  c.rdz = 1. / dz;
+  return c;
+}
+
 // Right-hand sides of one cell (src/fluid/predict/{ux,uy,t}.c compute_rhs_*
 // in 2D, carried to z by the restatement): the explicit part into sa[f], the
 // x-implicit diffusion and the pressure gradient into sg[f], in the
 // restatement's order (advection x, y, z; diffusion x, y, z; pressure;
 // buoyancy; surface).  Fields 0 ux (do_ux: the face exists), 1 uy, 2 uz, 3 t.
 template <class R>
-__device__ __forceinline__ void rhs4_values(const Predict3Args<R> &a, const Grid3 &g, const Stencil4 &S, bool do_ux,
-                                            double *sa, double *sg) {
+__device__ __forceinline__ void rhs4_values(const Predict3Args<R> &a, const Grid3 &g, const Stencil4 &S,
+                                            const RhsCoef &K, bool do_ux, double *sa, double *sg) {
   const double u00 = S.u00, u10 = S.u10, u20 = S.u20, u0s = S.u0s, u1s = S.u1s, u1n = S.u1n, u0b = S.u0b,
                u1b = S.u1b, u1t = S.u1t;
   const double vc = S.vc, vxm = S.vxm, vxp = S.vxp, vs = S.vs, vn = S.vn, vb = S.vb, vt = S.vt, vnb = S.vnb,
@@ -112,26 +140,26 @@ __device__ __forceinline__ void rhs4_values(const Predict3Args<R> &a, const Grid
     double ra = 0., rg = 0.;
     {
       const double ul = +0.5 * xm + 0.5 * xc, uu = +0.5 * xc + 0.5 * xp;
-      const double l = +0.5 / dxc * ul, u = -0.5 / dxc * uu, cc = -l - u;
+      const double l = K.hxc0 * ul, u = K.hxc1 * uu, cc = -l - u;
       ra += +l * xm + cc * xc + u * xp;
     }
-    const double w_xm = 0.5 * dxf_i / dxc, w_xp = 0.5 * dxf_i1 / dxc;
+    const double w_xm = K.w_xm, w_xp = K.w_xp;
     {
       const double ul = w_xm * vc + w_xp * vxp;
       const double uu = w_xm * vn + w_xp * v1n;
-      const double l = +0.5 / dy * ul, u = -0.5 / dy * uu, cc = -l - u;
+      const double l = K.hy0 * ul, u = K.hy1 * uu, cc = -l - u;
       ra += +l * ys + cc * xc + u * yn;
     }
     {
       const double ul = w_xm * wc + w_xp * wxp;
       const double uu = w_xm * wt + w_xp * w1t;
-      const double l = +0.5 / dz * ul, u = -0.5 / dz * uu, cc = -l - u;
+      const double l = K.hz0 * ul, u = K.hz1 * uu, cc = -l - u;
       ra += +l * zs + cc * xc + u * zn;
     }
     rg += md * (+lu0 * xm + lu1 * xc + lu2 * xp);
     ra += md * (+ly[0] * ys + ly[1] * xc + ly[2] * yn);
     ra += md * (+lz[0] * zs + lz[1] * xc + lz[2] * zn);
-    rg -= 1. / dxc * (-pc + pxp);
+    rg -= K.rdxc * (-pc + pxp);
     if (a.add_buoyancy) ra += +0.5 * tc + 0.5 * txp;
     ra += ifx;
     sa[0] = ra;
@@ -145,24 +173,24 @@ __device__ __forceinline__ void rhs4_values(const Predict3Args<R> &a, const Grid
     {
       const double ul = +0.5 * u0s + 0.5 * u00;
       const double uu = +0.5 * u1s + 0.5 * u10;
-      const double l = +0.5 / dxf * ul, u = -0.5 / dxf * uu, cc = -l - u;
+      const double l = K.hxf0 * ul, u = K.hxf1 * uu, cc = -l - u;
       ra += +l * xm + cc * xc + u * xp;
     }
     {
       const double ul = +0.5 * ys + 0.5 * xc, uu = +0.5 * xc + 0.5 * yn;
-      const double l = +0.5 / dy * ul, u = -0.5 / dy * uu, cc = -l - u;
+      const double l = K.hy0 * ul, u = K.hy1 * uu, cc = -l - u;
       ra += +l * ys + cc * xc + u * yn;
     }
     {
       const double ul = +0.5 * ws + 0.5 * wc;
       const double uu = +0.5 * wst + 0.5 * wt;
-      const double l = +0.5 / dz * ul, u = -0.5 / dz * uu, cc = -l - u;
+      const double l = K.hz0 * ul, u = K.hz1 * uu, cc = -l - u;
       ra += +l * zs + cc * xc + u * zn;
     }
     rg += md * (+lc0 * xm + lc1 * xc + lc2 * xp);
     ra += md * (+ly[0] * ys + ly[1] * xc + ly[2] * yn);
     ra += md * (+lz[0] * zs + lz[1] * xc + lz[2] * zn);
-    rg -= 1. / dy * (-ps + pc);
+    rg -= K.rdy * (-ps + pc);
     ra += ify;
     sa[1] = ra;
     sg[1] = rg;
@@ -174,24 +202,24 @@ __device__ __forceinline__ void rhs4_values(const Predict3Args<R> &a, const Grid
     {
       const double ul = +0.5 * u0b + 0.5 * u00;
       const double uu = +0.5 * u1b + 0.5 * u10;
-      const double l = +0.5 / dxf * ul, u = -0.5 / dxf * uu, cc = -l - u;
+      const double l = K.hxf0 * ul, u = K.hxf1 * uu, cc = -l - u;
       ra += +l * xm + cc * xc + u * xp;
     }
     {
       const double ul = +0.5 * vb + 0.5 * vc;
       const double uu = +0.5 * vnb + 0.5 * vn;
-      const double l = +0.5 / dy * ul, u = -0.5 / dy * uu, cc = -l - u;
+      const double l = K.hy0 * ul, u = K.hy1 * uu, cc = -l - u;
       ra += +l * ys + cc * xc + u * yn;
     }
     {
       const double ul = +0.5 * zs + 0.5 * xc, uu = +0.5 * xc + 0.5 * zn;
-      const double l = +0.5 / dz * ul, u = -0.5 / dz * uu, cc = -l - u;
+      const double l = K.hz0 * ul, u = K.hz1 * uu, cc = -l - u;
       ra += +l * zs + cc * xc + u * zn;
     }
     rg += md * (+lc0 * xm + lc1 * xc + lc2 * xp);
     ra += md * (+ly[0] * ys + ly[1] * xc + ly[2] * yn);
     ra += md * (+lz[0] * zs + lz[1] * xc + lz[2] * zn);
-    rg -= 1. / dz * (-pb + pc);
+    rg -= K.rdz * (-pb + pc);
     ra += ifz;
     sa[2] = ra;
     sg[2] = rg;
@@ -201,15 +229,15 @@ __device__ __forceinline__ void rhs4_values(const Predict3Args<R> &a, const Grid
     const double xm = txm, xc = tc, xp = txp, ys = ts, yn = tn, zs = tb, zn = tt;
     double ra = 0., rg = 0.;
     {
-      const double l = +0.5 / dxf * u00, u = -0.5 / dxf * u10, cc = -l - u;
+      const double l = K.hxf0 * u00, u = K.hxf1 * u10, cc = -l - u;
       ra += +l * xm + cc * xc + u * xp;
     }
     {
-      const double l = +0.5 / dy * vc, u = -0.5 / dy * vn, cc = -l - u;
+      const double l = K.hy0 * vc, u = K.hy1 * vn, cc = -l - u;
       ra += +l * ys + cc * xc + u * yn;
     }
     {
-      const double l = +0.5 / dz * wc, u = -0.5 / dz * wt, cc = -l - u;
+      const double l = K.hz0 * wc, u = K.hz1 * wt, cc = -l - u;
       ra += +l * zs + cc * xc + u * zn;
     }
     rg += td * (+lc0 * xm + lc1 * xc + lc2 * xp);
@@ -230,8 +258,10 @@ __device__ __forceinline__ void rhs4_values(const Predict3Args<R> &a, const Grid
 // gamma src_g) in the line layout [field][j - 1 + ny (k - 1)][x position]
 // that the line solver reads.
 constexpr int RX = 32, RY = 8, RZ = 16;
-constexpr int WX = RX + 2, WY = RY + 2, NSLOT = 4, NFLD = 5;
-constexpr size_t kRhsSmem = sizeof(double) * NFLD * NSLOT * WY * WX;
+constexpr int WX = RX + 2, WY = RY + 2, NSLOT = 4, NFLD = 5, NCEN = 7;
+// the state windows (FP64) and the per-cell inputs ifrcx / ifrcy / ifrcz and
+// src_b of the four fields (R; sized for FP64)
+constexpr size_t kRhsSmem = sizeof(double) * (NFLD * NSLOT * WY * WX + NCEN * NSLOT * RY * RX);
 
 size_t rhs_smem_bytes() { return kRhsSmem; }
 
@@ -250,8 +280,22 @@ __global__ void __launch_bounds__(RX * RY, 2) k3_rhs(Predict3Args<R> a) {
   const long width[NFLD] = {nx + 1, nx + 2, nx + 2, nx + 2, nx + 2};
   const long plane_rows = ny + 2;
   // window column c <-> storage x = i0 - 1 + c; row r <-> j = j0 - 1 + r
+  R *cen = reinterpret_cast<R *>(ring + (size_t)NFLD * NSLOT * WY * WX);  // [NCEN][NSLOT][RY][RX]
+  const R *cen_src[NCEN] = {a.ifrcx, a.ifrcy, a.ifrcz, a.sb[0], a.sb[1], a.sb[2], a.sb[3]};
+  const int ncen = a.use_b ? NCEN : 3;
   auto load_plane = [&](int kk) {
     const int slot = kk & (NSLOT - 1);
+    // per-cell inputs of the interior planes: thread (tx, ty) copies its own
+    if (kk >= k0 && kk < kend && mine) {
+      const long is = ix_src(g, i, j, kk);
+      const long isx = (long)(i - 1) + (long)(nx - 1) * ((long)(j - 1) + (long)ny * (kk - 1));  // face i + 1
+      for (int q = 0; q < ncen; q++) {
+        const bool xface = (0 == q || 3 == q);
+        if (xface && !do_ux) continue;
+        __pipeline_memcpy_async(cen + ((size_t)(q * NSLOT + slot) * RY + ty) * RX + tx,
+                                cen_src[q] + (xface ? isx : is), sizeof(R));
+      }
+    }
     for (int f = 0; f < NFLD; f++) {
       double *dst = ring + ((size_t)f * NSLOT + slot) * WY * WX;
       const double *src = fld[f] + width[f] * plane_rows * kk;
@@ -291,6 +335,7 @@ __global__ void __launch_bounds__(RX * RY, 2) k3_rhs(Predict3Args<R> a) {
       lu2 = ldg(a.lap_ux + 3 * (i - 1) + 2);
     }
   }
+  const RhsCoef K = rhs_coef(dxf_i, dxf_i1, dxc_i1, g.dy, g.dz);
   for (int k = k0; k < kend; k++) {
     if (k + 2 <= min(kend, nz + 1)) load_plane(k + 2);
     if (mine) {
@@ -339,9 +384,10 @@ __global__ void __launch_bounds__(RX * RY, 2) k3_rhs(Predict3Args<R> a) {
       S.pxp = RING(4, s0, ty + 1, tx + 2);
 #undef RING
       const long is = ix_src(g, i, j, k);
-      S.ify = (double)ldg(a.ifrcy + is);
-      S.ifz = (double)ldg(a.ifrcz + is);
-      S.ifx = do_ux ? (double)ldg(a.ifrcx + ix_srcx(g, i + 1, j, k)) : 0.;
+#define CEN(q) (double)cen[((size_t)((q) * NSLOT + s0) * RY + ty) * RX + tx]
+      S.ify = CEN(1);
+      S.ifz = CEN(2);
+      S.ifx = do_ux ? CEN(0) : 0.;
       S.dxf_i = dxf_i;
       S.dxf_i1 = dxf_i1;
       S.dxc_i1 = dxc_i1;
@@ -352,21 +398,22 @@ __global__ void __launch_bounds__(RX * RY, 2) k3_rhs(Predict3Args<R> a) {
       S.lc1 = lc1;
       S.lc2 = lc2;
       double sa[4], sg[4];
-      rhs4_values(a, g, S, do_ux, sa, sg);
+      rhs4_values(a, g, S, K, do_ux, sa, sg);
       const size_t line = (size_t)(j - 1) + (size_t)ny * (k - 1);
       R *dl = a.fw + line * nx + (i - 1);
       if (do_ux) {
         const long isx = ix_srcx(g, i + 1, j, k);
         a.sa[0][isx] = R(sa[0]);
-        const double sb = a.use_b ? cb * (double)ldg(a.sb[0] + isx) : 0.;
+        const double sb = a.use_b ? cb * CEN(3) : 0.;
         dl[0] = R(+ca * sa[0] + sb + cg * sg[0]);
       }
 #pragma unroll
       for (int q = 1; q < 4; q++) {
         a.sa[q][is] = R(sa[q]);
-        const double sb = a.use_b ? cb * (double)ldg(a.sb[q] + is) : 0.;
+        const double sb = a.use_b ? cb * CEN(3 + q) : 0.;
         dl[q * fstride] = R(+ca * sa[q] + sb + cg * sg[q]);
       }
+#undef CEN
     }
     __pipeline_wait_prior(0);
     __syncthreads();

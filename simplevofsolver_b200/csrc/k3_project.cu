@@ -24,6 +24,10 @@ __global__ void __launch_bounds__(256) k3_project(double *__restrict__ ux, doubl
   const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
   if (i > nx || j > ny) return;
   const double dt = ldg(dtp);
+  // quotients the restatement evaluates per cell, once per thread (same values)
+  const double pv = gam * dt, pp = 0.5 * gam * dt * m_dif;
+  const double cvx = pv / ldg(g.dxc + i - 1), cvy = pv / g.dy, cvz = pv / g.dz;
+  const double cpx = pp / ldg(g.dxf + i - 1);
 #pragma unroll 2
   for (int kz = 0; kz < kProjectPlanes; kz++) {
   const int k = 1 + blockIdx.z * kProjectPlanes + kz;
@@ -31,24 +35,22 @@ __global__ void __launch_bounds__(256) k3_project(double *__restrict__ ux, doubl
   const double psc = ldg(psi + ix_cc(g, i, j, k));
   const bool wall = (1 == i || nx == i);
   if (do_vel) {
-    const double prefactor = gam * dt;
     const double pxm = ldg(psi + ix_cc(g, i - 1, j, k));
     const double pym = ldg(psi + ix_cc(g, i, j - 1, k));
     const double pzm = ldg(psi + ix_cc(g, i, j, k - 1));
-    const double dxc = ldg(g.dxc + i - 1);
     const long iu = ix_ux(g, i, j, k), ic = ix_cc(g, i, j, k);
     const double ux0 = ux[iu], uy0 = uy[ic], uz0 = uz[ic];
     // ux
     if (i >= 2) {
       double v = ux0;
-      v -= prefactor / dxc * (+psc - pxm);
+      v -= cvx * (+psc - pxm);
       for_images(j, k, ny, nz, true, [&](int jj, int kk) { ux[ix_ux(g, i, jj, kk)] = v; });
     }
     double vy = uy0;
-    vy -= prefactor / g.dy * (+psc - pym);
+    vy -= cvy * (+psc - pym);
     for_images(j, k, ny, nz, true, [&](int jj, int kk) { uy[ix_cc(g, i, jj, kk)] = vy; });
     double vz = uz0;
-    vz -= prefactor / g.dz * (+psc - pzm);
+    vz -= cvz * (+psc - pzm);
     for_images(j, k, ny, nz, true, [&](int jj, int kk) { uz[ix_cc(g, i, jj, kk)] = vz; });
     if (wall) {
       const int iwu = (1 == i) ? 1 : nx + 1;
@@ -67,14 +69,13 @@ __global__ void __launch_bounds__(256) k3_project(double *__restrict__ ux, doubl
     }
   }
   if (do_p) {
-    const double prefactor = 0.5 * gam * dt * m_dif;
     const double pxm = ldg(psi + ix_cc(g, i - 1, j, k));
     const double pxp = ldg(psi + ix_cc(g, i + 1, j, k));
     double v = p[ix_cc(g, i, j, k)];
     v += psc;
     const double dm = (-pxm + psc) / ldg(g.dxc + i - 1);
     const double dp = (-psc + pxp) / ldg(g.dxc + i);
-    v -= prefactor / ldg(g.dxf + i - 1) * (-dm + dp);
+    v -= cpx * (-dm + dp);
     for_images(j, k, ny, nz, true, [&](int jj, int kk) { p[ix_cc(g, i, jj, kk)] = v; });
     if (wall) {
       const int iw = (1 == i) ? 0 : nx + 1;

@@ -538,7 +538,7 @@ int svof3d_create(const svof3d_params_t *prm, const double *xf, const double *xc
     if (smy > 200 * 1024 || smz > 200 * 1024) return fail("svof3d_create: FFT length too large"), bail();
     const cudaError_t pe = s->mixed ? pois_prepare<float>(s->ny, s->cols_y, s->nz, s->cols_z)
                                     : pois_prepare<double>(s->ny, s->cols_y, s->nz, s->cols_z);
-    if (cudaSuccess != pe || cudaSuccess != predict_prepare())
+    if (cudaSuccess != pe || cudaSuccess != predict_prepare() || cudaSuccess != interface_prepare())
       return fail("cudaFuncSetAttribute(Poisson): %s", cudaGetErrorString(cudaGetLastError())), bail();
     const size_t coef_smem = sizeof(double) * 6 * nx;
     if (coef_smem > 200 * 1024) return fail("svof3d_create: nx too large"), bail();

@@ -103,6 +103,8 @@ cudaError_t interface_geom(cudaStream_t st, const double *vof, R *normal, R *cur
 template <class R>
 cudaError_t interface_force(cudaStream_t st, const double *vof, const R *curv, R *ifrcx, R *ifrcy, R *ifrcz,
                             double tension, Grid3 g);
+// opt-in shared memory of the interface kernels (once per device)
+cudaError_t interface_prepare();
 // THINC fluxes, divergence, RK update of vof with halo and walls
 template <class R>
 cudaError_t interface_advect(cudaStream_t st, const double *vof, double *vof_new, const double *ux,
