@@ -46,36 +46,74 @@ struct Cplx<float> {
   static __device__ __forceinline__ T make(float a, float b) { return make_float2(a, b); }
 };
 
-// One warp per line.  Lines are stored re / im separately in shared memory
-// with a row stride of n + 1, so that the column-wise loads and stores
-// (consecutive threads on consecutive lines) and the butterflies (consecutive
-// lanes on consecutive positions) are free of bank conflicts.  The butterflies
-// are those of the oracle's radix-2 FFT (same pairs, same twiddles, same
-// association).
+// One warp per line.  Lines are stored re / im separately in shared memory,
+// position p at padded index pad(p) = p + p / 8 and lines ld = n + n / 8 + 1
+// apart, which keeps the column-wise loads and stores (consecutive threads on
+// consecutive lines) and the register passes below free of bank conflicts.
+// The transform is the oracle's radix-2 decimation in time (same butterfly
+// pairs, same twiddles, same association), executed in passes of up to three
+// stages: a lane loads the 2^ns points a pass combines, runs their butterflies
+// in registers and stores them back, so shared memory is touched once per
+// pass instead of once per stage.
+__device__ __forceinline__ int fpad(int p) { return p + (p >> 3); }
+__host__ __device__ __forceinline__ int fft_ld(int n) { return n + (n >> 3) + 1; }
+
+template <class R, int NS>
+__device__ __forceinline__ void fft_pass(R *__restrict__ re, R *__restrict__ im, int log2n, int s0,
+                                         const R *__restrict__ tw) {
+  using C2 = typename Cplx<R>::T;
+  constexpr int G = 1 << NS;
+  const int lane = threadIdx.x & 31;
+  const int h = 1 << (s0 - 1);
+  const int ngroups = (1 << log2n) >> NS;
+  for (int gi = lane; gi < ngroups; gi += 32) {
+    const int base = (gi & (h - 1)) + ((gi >> (s0 - 1)) << (s0 - 1 + NS));
+    R xr[G], xi[G];
+#pragma unroll
+    for (int m = 0; m < G; m++) {
+      const int q = fpad(base + m * h);
+      xr[m] = re[q];
+      xi[m] = im[q];
+    }
+#pragma unroll
+    for (int t = 0; t < NS; t++) {
+      const int st = s0 + t, dist = 1 << t;
+#pragma unroll
+      for (int m = 0; m < G; m++) {
+        if (m & dist) continue;
+        const int pa = base + m * h;
+        const int kk = pa & ((h << t) - 1);
+        const C2 w = __ldg(reinterpret_cast<const C2 *>(tw) + (kk << (log2n - st)));
+        const R br = xr[m + dist], bi = xi[m + dist];
+        const R tr = w.x * br - w.y * bi;
+        const R ti = w.x * bi + w.y * br;
+        const R ur = xr[m], ui = xi[m];
+        xr[m] = ur + tr;
+        xi[m] = ui + ti;
+        xr[m + dist] = ur - tr;
+        xi[m + dist] = ui - ti;
+      }
+    }
+#pragma unroll
+    for (int m = 0; m < G; m++) {
+      const int q = fpad(base + m * h);
+      re[q] = xr[m];
+      im[q] = xi[m];
+    }
+  }
+  __syncwarp();
+}
+
 template <class R>
 __device__ __forceinline__ void warp_fft_line(R *__restrict__ re, R *__restrict__ im, int log2n,
                                               const R *__restrict__ tw) {
-  using C2 = typename Cplx<R>::T;
-  const int lane = threadIdx.x & 31;
-  const int nb = 1 << (log2n - 1);
-  for (int st = 1; st <= log2n; st++) {
-    const int half = 1 << (st - 1);
-    const int sh = log2n - st;
-    for (int b = lane; b < nb; b += 32) {
-      const int grp = b >> (st - 1);
-      const int kk = b & (half - 1);
-      const int ia = (grp << st) + kk, ib = ia + half;
-      const C2 w = __ldg(reinterpret_cast<const C2 *>(tw) + (kk << sh));
-      const R xr = re[ib], xi = im[ib];
-      const R tr = w.x * xr - w.y * xi;
-      const R ti = w.x * xi + w.y * xr;
-      const R ur = re[ia], ui = im[ia];
-      re[ia] = ur + tr;
-      im[ia] = ui + ti;
-      re[ib] = ur - tr;
-      im[ib] = ui - ti;
-    }
-    __syncwarp();
+  int s0 = 1;
+  while (s0 <= log2n) {
+    const int ns = min(3, log2n - s0 + 1);
+    if (3 == ns) fft_pass<R, 3>(re, im, log2n, s0, tw);
+    else if (2 == ns) fft_pass<R, 2>(re, im, log2n, s0, tw);
+    else fft_pass<R, 1>(re, im, log2n, s0, tw);
+    s0 += ns;
   }
 }
 
@@ -109,7 +147,7 @@ __global__ void __launch_bounds__(32 * COLS) k3_pois_fwd_y(const double *__restr
                                                           double gam, int log2n, Grid3 g) {
   extern __shared__ unsigned char smraw[];
   R *re = reinterpret_cast<R *>(smraw);
-  const int n = 1 << log2n, ld = n + 1, nx = g.nx, nky = n / 2 + 1;
+  const int n = 1 << log2n, ld = fft_ld(n), nx = g.nx, nky = n / 2 + 1;
   R *im = re + COLS * ld;
   const int i0 = 1 + blockIdx.x * COLS;
   const int k = 1 + blockIdx.y;
@@ -122,8 +160,8 @@ __global__ void __launch_bounds__(32 * COLS) k3_pois_fwd_y(const double *__restr
     const int m = bitrev(q, log2n);
     double v = 0.;
     if (col < nc) v = pois_rhs<RESID>(ux, uy, uz, psi, pl, pu, g, i0 + col, m + 1, k, prefactor, gdt);
-    re[col * ld + q] = R(v);
-    im[col * ld + q] = R(0.);
+    re[col * ld + fpad(q)] = R(v);
+    im[col * ld + fpad(q)] = R(0.);
   }
   __syncthreads();
   {
@@ -136,7 +174,7 @@ __global__ void __launch_bounds__(32 * COLS) k3_pois_fwd_y(const double *__restr
     const int ky = w / COLS, col = w % COLS;
     if (col < nc) {
       reinterpret_cast<C2 *>(spec)[((size_t)(k - 1) * nky + ky) * nx + (i0 - 1 + col)] =
-          Cplx<R>::make(re[col * ld + ky], im[col * ld + ky]);
+          Cplx<R>::make(re[col * ld + fpad(ky)], im[col * ld + fpad(ky)]);
     }
   }
 }
@@ -148,7 +186,7 @@ __global__ void __launch_bounds__(32 * COLS) k3_pois_z(R *__restrict__ spec, con
                                                       Grid3 g) {
   extern __shared__ unsigned char smraw[];
   R *re = reinterpret_cast<R *>(smraw);
-  const int n = 1 << log2n, ld = n + 1, nx = g.nx, nky = g.ny / 2 + 1;
+  const int n = 1 << log2n, ld = fft_ld(n), nx = g.nx, nky = g.ny / 2 + 1;
   R *im = re + COLS * ld;
   const int i0 = blockIdx.x * COLS;
   const int ky = blockIdx.y;
@@ -160,8 +198,8 @@ __global__ void __launch_bounds__(32 * COLS) k3_pois_z(R *__restrict__ spec, con
     const int m = bitrev(q, log2n);
     C2 v = Cplx<R>::make(R(0.), R(0.));
     if (col < nc) v = sp[((size_t)m * nky + ky) * nx + (i0 + col)];
-    re[col * ld + q] = v.x;
-    im[col * ld + q] = v.y;
+    re[col * ld + fpad(q)] = v.x;
+    im[col * ld + fpad(q)] = v.y;
   }
   __syncthreads();
   {
@@ -171,7 +209,8 @@ __global__ void __launch_bounds__(32 * COLS) k3_pois_z(R *__restrict__ spec, con
   __syncthreads();
   for (int w = threadIdx.x; w < COLS * n; w += 32 * COLS) {
     const int kz = w / COLS, col = w % COLS;
-    if (col < nc) sp[((size_t)kz * nky + ky) * nx + (i0 + col)] = Cplx<R>::make(re[col * ld + kz], im[col * ld + kz]);
+    if (col < nc)
+      sp[((size_t)kz * nky + ky) * nx + (i0 + col)] = Cplx<R>::make(re[col * ld + fpad(kz)], im[col * ld + fpad(kz)]);
   }
 }
 
@@ -322,7 +361,7 @@ __global__ void __launch_bounds__(32 * COLS) k3_pois_inv_y(const R *__restrict__
                                                           const R *__restrict__ tw, int log2n, Grid3 g) {
   extern __shared__ unsigned char smraw[];
   R *re = reinterpret_cast<R *>(smraw);
-  const int n = 1 << log2n, ld = n + 1, nx = g.nx, ny = g.ny, nz = g.nz, nky = n / 2 + 1;
+  const int n = 1 << log2n, ld = fft_ld(n), nx = g.nx, ny = g.ny, nz = g.nz, nky = n / 2 + 1;
   R *im = re + COLS * ld;
   const int i0 = 1 + blockIdx.x * COLS;
   const int k = 1 + blockIdx.y;
@@ -349,8 +388,8 @@ __global__ void __launch_bounds__(32 * COLS) k3_pois_inv_y(const R *__restrict__
         x = -v.y;
       }
     }
-    re[col * ld + q] = r;
-    im[col * ld + q] = x;
+    re[col * ld + fpad(q)] = r;
+    im[col * ld + fpad(q)] = x;
   }
   __syncthreads();
   {
@@ -362,7 +401,7 @@ __global__ void __launch_bounds__(32 * COLS) k3_pois_inv_y(const R *__restrict__
     const int r = w / COLS, col = w % COLS;
     if (col >= nc) continue;
     const int i = i0 + col, j = r + 1;
-    double y = (double)re[col * ld + r];
+    double y = (double)re[col * ld + fpad(r)];
     if (ACCUM) y += psi[ix_cc(g, i, j, k)];
     for_images(j, k, ny, nz, true, [&](int jj, int kk) { psi[ix_cc(g, i, jj, kk)] = y; });
   }
@@ -375,7 +414,7 @@ __global__ void __launch_bounds__(32 * COLS) k3_pois_inv_y(const R *__restrict__
     if ((0 == side && !has_left) || (1 == side && !has_right)) continue;
     const int iw = side ? nx + 1 : 0;
     const int col = side ? nc - 1 : 0;
-    const double nv = ACCUM ? psi[ix_cc(g, i0 + col, j, k)] : (double)re[col * ld + (j - 1)];
+    const double nv = ACCUM ? psi[ix_cc(g, i0 + col, j, k)] : (double)re[col * ld + fpad(j - 1)];
     const double old = psi[ix_cc(g, iw, j, k)];
     psi[ix_cc(g, iw, j, k)] = nv;
     for_images(j, k, ny, nz, false, [&](int jj, int kk) { psi[ix_cc(g, iw, jj, kk)] = old; });
@@ -395,7 +434,7 @@ cudaError_t by_cols(int cols, F f) {
 }
 template <class R>
 size_t fft_smem(int n, int cols) {
-  return sizeof(R) * 2 * (size_t)(n + 1) * cols;
+  return sizeof(R) * 2 * (size_t)fft_ld(n) * cols;
 }
 }  // namespace
 
