@@ -48,6 +48,10 @@ if ROOT not in sys.path:
 import numpy as np  # noqa: E402
 
 METRIC = "Mcell-steps/s"
+# the headline metric of the 3D workloads: the mixed-precision path's
+# throughput at 512^3, reported beside the FP64 path's on the same GPU with
+# the mixed path's error against it
+METRIC3D = "Mcell-steps/s 512^3 mixed vs FP64 (same GPU, stated error)"
 # 2D FP64 algorithmic HBM bytes per cell-step (103 eight-byte words: the
 # compulsory reads/writes of the reference dataflow with stencil-internal
 # intermediates on chip)
@@ -84,9 +88,21 @@ ALG_WORDS_3D = {
     "poisson_inv": 2.0,        # R spectrum; W psi
     "project": 9.0,            # R psi ux uy uz p; W ux uy uz p
 }
-# dt (2), then per substep: geom + intercept, force, vof, coef + predict,
-# 5 Poisson stages, project
-KERNELS_PER_STEP_3D = 2 + 3 * 12
+# the mixed path's bytes per interior cell and launch: the state (velocities,
+# p, t, vof, vof sources, psi) stays FP64, curvature, forces, momentum
+# sources, increments and spectra are FP32; the Poisson kinds average its
+# two passes (the second also reads psi)
+ALG_BYTES_3D_MIXED = {
+    "dt": 24.0, "geom": 12.0, "force": 24.0, "vof": 48.0 + 16.0 / 3.0,
+    "predict": 40.0 + 12.0 + 32.0 / 3.0 + 32.0 + 16.0,
+    "poisson_fwd": 32.0, "poisson_z": 8.0, "poisson_solve": 8.0, "poisson_inv": 16.0, "project": 72.0,
+}
+# dt (2), then per substep: geom + intercept, force, vof, coef + rhs +
+# line solve, 5 Poisson stages (10 in the mixed path), project
+KERNELS_PER_STEP_3D = 2 + 3 * 13
+# kernels launched per launch of a kind (profile counts kernels)
+KERNELS_PER_KIND_3D = {"dt": 2, "geom": 2, "predict": 3}
+KERNELS_PER_STEP_3D_MIXED = 2 + 3 * 18
 
 WORKLOADS3D = {
     # the headline configuration: 512^3, 128 droplets, radii 0.02 .. 0.05
@@ -245,6 +261,174 @@ def _max_over_ranks(x: float, world: int) -> float:
     return float(t.item())
 
 
+def _timed_steps(solver, steps, world, local_rank, flush=None):
+    """device time of `steps` steps enqueued back to back (events on the
+    solver's stream), the max over ranks, and the clocks seen meanwhile"""
+    import torch
+    import torch.distributed as dist
+    stream = torch.cuda.ExternalStream(solver.stream())
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        with torch.cuda.stream(stream):
+            for k in range(steps):
+                if flush is not None:
+                    flush.zero_()
+                starts[k].record(stream)
+                solver.enqueue_steps(1)
+                ends[k].record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    total_ms = _max_over_ranks(float(sum(s_.elapsed_time(e_) for s_, e_ in zip(starts, ends))), world)
+    return total_ms, clk.summary()
+
+
+def _profile(solver, nprof):
+    """per-kernel-kind device time of `nprof` steps launched kernel by kernel;
+    a long memset ahead lets the host enqueue the whole step first"""
+    import torch
+    stream = torch.cuda.ExternalStream(solver.stream())
+    prof = {}
+    for _ in range(nprof):
+        with torch.cuda.stream(stream):
+            big = torch.empty(1024 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+            big.zero_()
+        r = solver.profile_step()
+        del big
+        for k, (ms, cnt) in r.items():
+            acc = prof.setdefault(k, [0.0, 0])
+            acc[0] += ms
+            acc[1] += cnt
+    return prof
+
+
+def _roofline(prof, alg_bytes_cell, cells, nprof):
+    """roofline of the dominant kernel kind: algorithmic bytes per launch over
+    its average device time per launch (coefficient + predictor, geometry +
+    intercept and dt + final count as one launch each)"""
+    dom = max(prof, key=lambda k: prof[k][0])
+    nl = max(prof[dom][1] // KERNELS_PER_KIND_3D.get(dom, 1), 1)
+    dom_ms = prof[dom][0] / nl
+    peak, peak_kind = peaks()
+    alg = alg_bytes_cell[dom] * cells
+    achieved = alg / (dom_ms * 1e-3) / 1e9
+    return {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": peak_kind, "alg_bytes_per_launch": alg,
+            "avg_launch_ms": dom_ms}
+
+
+def run3d(args, wl, ic, env, world, rank, local_rank):
+    """the 3D workloads: the mixed path (the headline value) and the FP64 path
+    on the same GPU, the mixed path's error against the FP64 one after the
+    same steps, end-to-end throughput, rooflines and the CPU baseline"""
+    import torch
+    import simplevofsolver_b200 as svof
+    from simplevofsolver_b200.workloads import physical_params
+    phys = physical_params(env)
+    n = wl["n"]
+    cells = n ** 3
+    dxf = np.diff(ic.xf)
+    vol0 = float(np.sum(ic.vof[:, :, 1:-1] * dxf)) * (ic.ly / ic.ny) * (ic.lz / ic.nz)
+    res = {}
+    for prec in ("fp64", "mixed"):
+        solver = svof.Solver3D(ic, phys, precision=prec)
+        solver.run(args.warmup)
+        torch.cuda.synchronize()
+        total_ms, clocks = _timed_steps(solver, args.steps, world, local_rank)
+        diag = solver.diagnostics()
+        fields = {k: solver.interior(k) for k in ("ux", "uy", "uz")}
+        prof = _profile(solver, 3)
+        alg = ALG_BYTES_3D_MIXED if prec == "mixed" else {k: 8.0 * v for k, v in ALG_WORDS_3D.items()}
+        step_alg = sum(alg[k] * (v[1] / 3) / KERNELS_PER_KIND_3D.get(k, 1) for k, v in prof.items())
+        res[prec] = dict(total_ms=total_ms, clocks=clocks, diag=diag, fields=fields, prof=prof,
+                         value=world * cells * args.steps / (total_ms * 1e-3) / 1e6,
+                         roofline=_roofline(prof, alg, cells, 3), step_alg_bytes=step_alg)
+        if prec == "mixed":
+            # end to end through the C ABI with host buffers: the restart
+            # fields copied in from pinned host memory and out again every step
+            names = ["ux", "uy", "uz", "p", "t", "vof"]
+            host = {k: torch.from_numpy(np.ascontiguousarray(ic.fields()[k])).pin_memory().numpy() for k in names}
+            h2d = sum(v.nbytes for v in host.values())
+            e2e_steps = max(1, min(args.steps, 3))
+            store = svof.solver3d.lib3().svof3d_store_interior
+            t0 = time.perf_counter()
+            for _ in range(e2e_steps):
+                for nm in names:
+                    solver.load_interior(nm, host[nm])
+                solver.integrate()
+                for nm in names:
+                    out = host[nm]
+                    if store(solver._h, svof.FIELDS3D[nm], out.ctypes.data, out.size) != 0:
+                        raise RuntimeError("svof3d_store_interior failed")
+            e2e_s = _max_over_ranks(time.perf_counter() - t0, world)
+            res[prec]["e2e"] = {"value": world * cells * e2e_steps / e2e_s / 1e6, "unit": METRIC,
+                                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d + 8, "steps": e2e_steps}
+            del host
+        solver.close()
+        torch.cuda.synchronize()
+    m, f = res["mixed"], res["fp64"]
+    err = {}
+    for k in ("ux", "uy", "uz"):
+        a, b = m["fields"][k][:, :, 1:-1], f["fields"][k][:, :, 1:-1]
+        err[f"{k}_rel_l2"] = float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+    err["divmax"] = m["diag"]["divmax"]
+    err["volume_drift"] = abs(m["diag"]["volume"] - vol0) / vol0
+    err["fp64_divmax"] = f["diag"]["divmax"]
+    err["fp64_volume_drift"] = abs(f["diag"]["volume"] - vol0) / vol0
+    err["after_steps"] = args.warmup + args.steps
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            import oracle
+            sn = 128
+            ssteps = args.cpu_sample_steps or 3
+            secs = oracle.run_oracle3d_replicas(sn, wl["ndrops"], wl["radii"], 1, ssteps, 1, 1)
+            cpu = {"value": sn ** 3 * ssteps / secs[0] / 1e6, "unit": METRIC, "cores": 1, "kind": "port",
+                   "sample": (f"{ssteps} steps of the {args.workload} generator at {sn}^3 on one core (3D "
+                              "restatement oracle/svof_oracle3d.c in FP64; the reference's 3D code is not in the "
+                              "mounted sources)")}
+        except Exception as e:
+            cpu = {"value": None, "unit": METRIC, "cores": 0, "kind": "port", "sample": f"unavailable: {e}"}
+
+    if rank == 0:
+        peak, _ = peaks()
+        line = {
+            "metric": METRIC3D, "value": m["value"], "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": m["total_ms"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64 (mixed)",
+            "data": "synthetic (seeded droplet field, workloads.droplets3d)",
+            "config": {"workload": args.workload, "nx": n, "ny": n, "nz": n, "droplets": wl["ndrops"],
+                       "radii": list(wl["radii"]), "x_grid": "tanh-stretched (1.5)",
+                       "poisson": "r2c-y + dft-z + thomas-x (mixed: two passes, FP64 residual)",
+                       "precision": "mixed (FP32 intermediates and transforms, FP64 state and x line solves)",
+                       "l2": "not flushed: inputs larger than L2 (fields of %.1f GB resident)" % (
+                           35.5 * cells * 8 / 1e9),
+                       "parallelism": f"replicas{world}"},
+            "fp64": {"value": f["value"], "unit": METRIC, "ms_per_step": f["total_ms"] / args.steps,
+                     "roofline": f["roofline"],
+                     "step_frac": f["value"] * 1e6 * ALG_BYTES_CELL_STEP_3D / 1e9 / peak,
+                     "kernel_ms_per_step": {k: v[0] / 3 for k, v in f["prof"].items()},
+                     "clocks": f["clocks"]},
+            "mixed_over_fp64": m["value"] / f["value"],
+            "mixed_error": err,
+            "e2e": m["e2e"],
+            "gpu_launches": KERNELS_PER_STEP_3D_MIXED * args.steps,
+            "roofline": dict(m["roofline"], traffic=None,
+                             step_frac=m["value"] * 1e6 * m["step_alg_bytes"] / 1e9 / peak,
+                             step_alg_bytes_per_cell=m["step_alg_bytes"]),
+            "kernel_ms_per_step": {k: v[0] / 3 for k, v in m["prof"].items()},
+            "kernel_share": {k: v[0] / sum(x[0] for x in m["prof"].values()) for k, v in m["prof"].items()},
+            "cpu_baseline": cpu,
+            "clocks": m["clocks"],
+        }
+        print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -296,10 +480,10 @@ def main():
     import simplevofsolver_b200 as svof
     phys = physical_params(env)
     if three_d:
-        solver = svof.Solver3D(ic, phys)
-        names = ["ux", "uy", "uz", "p", "t", "vof"]
-        lib, store, fields = svof.solver3d.lib3(), "svof3d_store_interior", svof.FIELDS3D
-        alg_words, kernels_per_step, alg_step = ALG_WORDS_3D, KERNELS_PER_STEP_3D, ALG_BYTES_CELL_STEP_3D
+        run3d(args, wl, ic, env, world, rank, local_rank)
+        if world > 1:
+            dist.destroy_process_group()
+        return
     else:
         solver = svof.Solver(ic, phys)
         names = ["ux", "uy", "p", "t", "vof"]

@@ -797,7 +797,7 @@ int svof3d_profile_step(svof3d_solver_t *s, double *ms, int *launches, int nkind
       float t = 0.f;
       cudaEventElapsedTime(&t, ev[q - 1], ev[q]);
       ms[kind[q]] += t;
-      launches[kind[q]] += (SVOF3_K_DT == kind[q] || SVOF3_K_PREDICT == kind[q] || SVOF3_K_GEOM == kind[q]) ? 2 : 1;
+      launches[kind[q]] += (SVOF3_K_PREDICT == kind[q]) ? 3 : ((SVOF3_K_DT == kind[q] || SVOF3_K_GEOM == kind[q]) ? 2 : 1);
     }
   }
   for (cudaEvent_t x : ev) cudaEventDestroy(x);
