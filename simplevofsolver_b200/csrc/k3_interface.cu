@@ -197,6 +197,14 @@ __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ 
   };
   load_plane(k0 - 1);
   load_plane(k0);
+  // 1 / dxc of the (up to two) corner columns this thread handles and 1 / dxf
+  // of its cell column, once (the same values as per corner / cell)
+  R rdxc[2] = {R(0.), R(0.)};
+  for (int t = tid, q = 0; t < (G3X + 1) * (G3Y + 1) && q < 2; t += G3X * G3Y, q++) {
+    const int ic = i0 + t % (G3X + 1);
+    if (ic <= nx + 1) rdxc[q] = R(1.) / R(ldg(g.dxc + ic - 1));
+  }
+  const R rdxf = (i0 + tx <= nx) ? R(1.) / R(ldg(g.dxf + i0 + tx - 1)) : R(0.);
   __pipeline_wait_prior(0);
   __syncthreads();
   for (int kc = k0; kc <= kend; kc++) {
@@ -204,7 +212,7 @@ __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ 
     const int ccur = (kc - k0) & 1, cprev = ccur ^ 1;
     if (kc + 1 <= kend) load_plane(kc + 1);
     // compute_gradient at corners (ic, jc, kc): planes kc-1 (bprev) and kc (bcur)
-    for (int t = tid; t < (G3X + 1) * (G3Y + 1); t += G3X * G3Y) {
+    for (int t = tid, q = 0; t < (G3X + 1) * (G3Y + 1); t += G3X * G3Y, q++) {
       const int li = t % (G3X + 1), lj = t / (G3X + 1);
       const int ic = i0 + li, jc = j0 + lj;
       R d0 = R(0.), d1 = R(0.), d2 = R(0.);
@@ -213,7 +221,7 @@ __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ 
         const double a01 = sv[bprev][lj + 1][li], a11 = sv[bprev][lj + 1][li + 1];
         const double b00 = sv[bcur][lj][li], b10 = sv[bcur][lj][li + 1];
         const double b01 = sv[bcur][lj + 1][li], b11 = sv[bcur][lj + 1][li + 1];
-        const R dvofdx = R(1.) / R(ldg(g.dxc + ic - 1)) * R(plane_dx(a00, a10, a01, a11) + plane_dx(b00, b10, b01, b11));
+        const R dvofdx = rdxc[q] * R(plane_dx(a00, a10, a01, a11) + plane_dx(b00, b10, b01, b11));
         const R dvofdy = rdy * R(plane_dy(a00, a10, a01, a11) + plane_dy(b00, b10, b01, b11));
         const R dvofdz = rdz * R(plane_sum(b00, b10, b01, b11) - plane_sum(a00, a10, a01, a11));
         const R norminv = rnorm(+dvofdx * dvofdx + dvofdy * dvofdy + dvofdz * dvofdz, eps);
@@ -234,7 +242,7 @@ __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ 
         const R dxf = R(ldg(g.dxf + i - 1));
 #define CL(m, a, b) sc[cprev][m][ty + (b)][tx + (a)]
 #define CU(m, a, b) sc[ccur][m][ty + (b)][tx + (a)]
-        const R dnxdx = R(1.) / dxf * (plane_dx(CL(0, 0, 0), CL(0, 1, 0), CL(0, 0, 1), CL(0, 1, 1)) +
+        const R dnxdx = rdxf * (plane_dx(CL(0, 0, 0), CL(0, 1, 0), CL(0, 0, 1), CL(0, 1, 1)) +
                                        plane_dx(CU(0, 0, 0), CU(0, 1, 0), CU(0, 0, 1), CU(0, 1, 1)));
         const R dnydy = rdy * (plane_dy(CL(1, 0, 0), CL(1, 1, 0), CL(1, 0, 1), CL(1, 1, 1)) +
                                plane_dy(CU(1, 0, 0), CU(1, 1, 0), CU(1, 0, 1), CU(1, 1, 1)));

@@ -129,14 +129,12 @@ __device__ __forceinline__ void rhs4_values(const Predict3Args<R> &a, const Grid
   const double tc = S.tc, txm = S.txm, txp = S.txp, ts = S.ts, tn = S.tn, tb = S.tb, tt = S.tt;
   const double pc = S.pc, ps = S.ps, pb = S.pb, pxp = S.pxp;
   const double ifx = S.ifx, ify = S.ify, ifz = S.ifz;
-  const double dxf_i = S.dxf_i, dxf_i1 = S.dxf_i1, dxc_i1 = S.dxc_i1;
   const double lu0 = S.lu0, lu1 = S.lu1, lu2 = S.lu2, lc0 = S.lc0, lc1 = S.lc1, lc2 = S.lc2;
-  const double md = a.m_dif, td = a.t_dif, dy = g.dy, dz = g.dz;
+  const double md = a.m_dif, td = a.t_dif;
   const double *ly = a.lapy, *lz = a.lapz;
   // ---- ux at the face iu = i + 1: xm = UX(iu-1), xc = UX(iu), xp = UX(iu+1)
   if (do_ux) {
     const double xm = u00, xc = u10, xp = u20, ys = u1s, yn = u1n, zs = u1b, zn = u1t;
-    const double dxc = dxc_i1;
     double ra = 0., rg = 0.;
     {
       const double ul = +0.5 * xm + 0.5 * xc, uu = +0.5 * xc + 0.5 * xp;
@@ -165,7 +163,6 @@ __device__ __forceinline__ void rhs4_values(const Predict3Args<R> &a, const Grid
     sa[0] = ra;
     sg[0] = rg;
   }
-  const double dxf = dxf_i;
   // ---- uy at cell i
   {
     const double xm = vxm, xc = vc, xp = vxp, ys = vs, yn = vn, zs = vb, zn = vt;

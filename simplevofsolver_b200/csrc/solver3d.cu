@@ -529,8 +529,9 @@ int svof3d_create(const svof3d_params_t *prm, const double *xf, const double *xc
   if (dalloc(s->spec, 2 * nx * nky * nz, es) || dalloc(s->xscratch, nx * nky * nz, es) ||
       dalloc(s->fw, 4 * nx * ny * nz, es))
     return bail();
-  // transforms: one line per warp, 16 / 8 / 4 lines per block by length
-  auto pick_cols = [](int n) { return n <= 128 ? 16 : (n <= 256 ? 8 : 4); };
+  // transforms: one line per warp, 16 / 8 / 4 lines per block by length (the
+  // y transforms read rows of 16 / 8 / 4 consecutive i)
+  auto pick_cols = [](int n) { return n <= 256 ? 16 : (n <= 512 ? 8 : 4); };
   s->cols_y = pick_cols(s->ny);
   s->cols_z = pick_cols(s->nz);
   {
