@@ -46,74 +46,96 @@ struct Cplx<float> {
   static __device__ __forceinline__ T make(float a, float b) { return make_float2(a, b); }
 };
 
-// One warp per line.  Lines are stored re / im separately in shared memory,
-// position p at padded index pad(p) = p + p / 8 and lines ld = n + n / 8 + 1
-// apart, which keeps the column-wise loads and stores (consecutive threads on
-// consecutive lines) and the register passes below free of bank conflicts.
-// The transform is the oracle's radix-2 decimation in time (same butterfly
-// pairs, same twiddles, same association), executed in passes of up to three
-// stages: a lane loads the 2^ns points a pass combines, runs their butterflies
-// in registers and stores them back, so shared memory is touched once per
-// pass instead of once per stage.
+// One warp per line, the line length N = 2^L2N a compile-time constant.
+// Lines are stored re / im separately in shared memory, position p at padded
+// index pad(p) = p + p / 8 and lines LD = N + N / 8 + 1 apart, which keeps the
+// column-wise loads and stores (consecutive threads on consecutive lines) and
+// the register passes below free of bank conflicts.  The transform is the
+// oracle's radix-2 decimation in time (same butterfly pairs, same twiddles,
+// same association), executed in passes of up to three stages: a lane loads
+// the 2^NS points a pass combines, runs their butterflies in registers and
+// stores them back, so shared memory is touched once per pass instead of once
+// per stage.
 __device__ __forceinline__ int fpad(int p) { return p + (p >> 3); }
-__host__ __device__ __forceinline__ int fft_ld(int n) { return n + (n >> 3) + 1; }
 
-template <class R, int NS>
-__device__ __forceinline__ void fft_pass(R *__restrict__ re, R *__restrict__ im, int log2n, int s0,
-                                         const R *__restrict__ tw) {
+// Shape of a block of one transform direction: COLS lines of N points, one
+// warp each.  COLS is the widest of 16 / 8 / 4 whose shared memory stays
+// within 80 KB (the rows the y transforms read are COLS x 8 bytes wide and,
+// with the reference's x pitch of nx + 2, not sector aligned: wider rows waste
+// less of each sector), MINB the resident blocks per SM the launch bounds ask
+// for (shared memory permitting, and no fewer than 64 registers a thread).
+constexpr int line_cols(int col_bytes) {
+  return (16 * col_bytes <= 81920) ? 16 : ((8 * col_bytes <= 81920) ? 8 : 4);
+}
+constexpr int line_minb(int smem, int threads) {
+  return (232448 / (smem + 1024) < 1024 / threads) ? ((232448 / (smem + 1024)) < 1 ? 1 : 232448 / (smem + 1024))
+                                                    : ((1024 / threads) < 1 ? 1 : 1024 / threads);
+}
+template <class R, int L2N>
+struct Line {
+  static constexpr int N = 1 << L2N;
+  static constexpr int LD = N + (N >> 3) + 1;
+  static constexpr int COL_BYTES = 2 * (int)sizeof(R) * LD;
+  static constexpr int COLS = line_cols(COL_BYTES);
+  static constexpr int THREADS = 32 * COLS;
+  static constexpr int SMEM = COLS * COL_BYTES;
+  static constexpr int MINB = line_minb(SMEM, THREADS);
+  static constexpr int ITER = (N + 31) / 32;  // points per thread in the load / store loops
+};
+
+template <class R, int L2N, int S0, int NS>
+__device__ __forceinline__ void fft_pass(R *__restrict__ re, R *__restrict__ im, const R *__restrict__ tw) {
   using C2 = typename Cplx<R>::T;
-  constexpr int G = 1 << NS;
+  constexpr int G = 1 << NS, H = 1 << (S0 - 1), NG = (1 << L2N) >> NS;
   const int lane = threadIdx.x & 31;
-  const int h = 1 << (s0 - 1);
-  const int ngroups = (1 << log2n) >> NS;
-  for (int gi = lane; gi < ngroups; gi += 32) {
-    const int base = (gi & (h - 1)) + ((gi >> (s0 - 1)) << (s0 - 1 + NS));
-    R xr[G], xi[G];
 #pragma unroll
-    for (int m = 0; m < G; m++) {
-      const int q = fpad(base + m * h);
-      xr[m] = re[q];
-      xi[m] = im[q];
-    }
-#pragma unroll
-    for (int t = 0; t < NS; t++) {
-      const int st = s0 + t, dist = 1 << t;
+  for (int g0 = 0; g0 < NG; g0 += 32) {
+    const int gi = g0 + lane;
+    if (NG >= 32 || gi < NG) {
+      const int base = (gi & (H - 1)) + ((gi >> (S0 - 1)) << (S0 - 1 + NS));
+      R xr[G], xi[G];
 #pragma unroll
       for (int m = 0; m < G; m++) {
-        if (m & dist) continue;
-        const int pa = base + m * h;
-        const int kk = pa & ((h << t) - 1);
-        const C2 w = __ldg(reinterpret_cast<const C2 *>(tw) + (kk << (log2n - st)));
-        const R br = xr[m + dist], bi = xi[m + dist];
-        const R tr = w.x * br - w.y * bi;
-        const R ti = w.x * bi + w.y * br;
-        const R ur = xr[m], ui = xi[m];
-        xr[m] = ur + tr;
-        xi[m] = ui + ti;
-        xr[m + dist] = ur - tr;
-        xi[m + dist] = ui - ti;
+        const int q = fpad(base + m * H);
+        xr[m] = re[q];
+        xi[m] = im[q];
       }
-    }
 #pragma unroll
-    for (int m = 0; m < G; m++) {
-      const int q = fpad(base + m * h);
-      re[q] = xr[m];
-      im[q] = xi[m];
+      for (int t = 0; t < NS; t++) {
+        const int st = S0 + t, dist = 1 << t;
+#pragma unroll
+        for (int m = 0; m < G; m++) {
+          if (m & dist) continue;
+          // twiddle index of the pair (base + m H, base + (m + dist) H) at stage st
+          const int kk = (gi & (H - 1)) + (m & (dist - 1)) * H;
+          const C2 w = __ldg(reinterpret_cast<const C2 *>(tw) + (kk << (L2N - st)));
+          const R br = xr[m + dist], bi = xi[m + dist];
+          const R tr = w.x * br - w.y * bi;
+          const R ti = w.x * bi + w.y * br;
+          const R ur = xr[m], ui = xi[m];
+          xr[m] = ur + tr;
+          xi[m] = ui + ti;
+          xr[m + dist] = ur - tr;
+          xi[m + dist] = ui - ti;
+        }
+      }
+#pragma unroll
+      for (int m = 0; m < G; m++) {
+        const int q = fpad(base + m * H);
+        re[q] = xr[m];
+        im[q] = xi[m];
+      }
     }
   }
   __syncwarp();
 }
 
-template <class R>
-__device__ __forceinline__ void warp_fft_line(R *__restrict__ re, R *__restrict__ im, int log2n,
-                                              const R *__restrict__ tw) {
-  int s0 = 1;
-  while (s0 <= log2n) {
-    const int ns = min(3, log2n - s0 + 1);
-    if (3 == ns) fft_pass<R, 3>(re, im, log2n, s0, tw);
-    else if (2 == ns) fft_pass<R, 2>(re, im, log2n, s0, tw);
-    else fft_pass<R, 1>(re, im, log2n, s0, tw);
-    s0 += ns;
+template <class R, int L2N, int S0 = 1>
+__device__ __forceinline__ void warp_fft_line(R *__restrict__ re, R *__restrict__ im, const R *__restrict__ tw) {
+  if constexpr (S0 <= L2N) {
+    constexpr int NS = (L2N - S0 + 1) < 3 ? (L2N - S0 + 1) : 3;
+    fft_pass<R, L2N, S0, NS>(re, im, tw);
+    warp_fft_line<R, L2N, S0 + NS>(re, im, tw);
   }
 }
 
@@ -136,81 +158,97 @@ __device__ __forceinline__ double pois_rhs(const double *__restrict__ ux, const 
   return (div / gdt - ap) / (1. * g.ny * g.nz);
 }
 
-template <int COLS, class R, bool RESID>
-__global__ void __launch_bounds__(32 * COLS) k3_pois_fwd_y(const double *__restrict__ ux,
-                                                          const double *__restrict__ uy,
-                                                          const double *__restrict__ uz,
-                                                          const double *__restrict__ psi,
-                                                          const double *__restrict__ pl,
-                                                          const double *__restrict__ pu, R *__restrict__ spec,
-                                                          const R *__restrict__ tw, const double *__restrict__ dtp,
-                                                          double gam, int log2n, Grid3 g) {
+// forward transform along y of COLS consecutive i of plane k: the right-hand
+// side (RESID: the residual) of each point, in bit-reversed order, then the
+// warp transforms, then the ky = 0 .. N/2 half of the spectrum
+template <int L2N, class R, bool RESID>
+__global__ void __launch_bounds__(Line<R, L2N>::THREADS, Line<R, L2N>::MINB)
+    k3_pois_fwd_y(const double *__restrict__ ux, const double *__restrict__ uy, const double *__restrict__ uz,
+                  const double *__restrict__ psi, const double *__restrict__ pl, const double *__restrict__ pu,
+                  R *__restrict__ spec, const R *__restrict__ tw, const double *__restrict__ dtp, double gam,
+                  Grid3 g) {
+  using L = Line<R, L2N>;
+  constexpr int N = L::N, LD = L::LD, COLS = L::COLS, NKY = N / 2 + 1;
   extern __shared__ unsigned char smraw[];
   R *re = reinterpret_cast<R *>(smraw);
-  const int n = 1 << log2n, ld = fft_ld(n), nx = g.nx, nky = n / 2 + 1;
-  R *im = re + COLS * ld;
+  R *im = re + COLS * LD;
+  const int nx = g.nx;
   const int i0 = 1 + blockIdx.x * COLS;
   const int k = 1 + blockIdx.y;
   const int nc = min(COLS, nx - i0 + 1);
   const double dt = ldg(dtp);
   const double prefactor = 1. / (gam * dt) / (1. * g.ny * g.nz);
   const double gdt = gam * dt;
-  for (int w = threadIdx.x; w < COLS * n; w += 32 * COLS) {
-    const int q = w / COLS, col = w % COLS;
-    const int m = bitrev(q, log2n);
-    double v = 0.;
-    if (col < nc) v = pois_rhs<RESID>(ux, uy, uz, psi, pl, pu, g, i0 + col, m + 1, k, prefactor, gdt);
-    re[col * ld + fpad(q)] = R(v);
-    im[col * ld + fpad(q)] = R(0.);
+#pragma unroll 4
+  for (int it = 0; it < L::ITER; it++) {
+    const int w = threadIdx.x + it * L::THREADS;
+    if (N >= 32 || w < COLS * N) {
+      const int q = w / COLS, col = w % COLS;
+      const int m = bitrev(q, L2N);
+      double v = 0.;
+      if (col < nc) v = pois_rhs<RESID>(ux, uy, uz, psi, pl, pu, g, i0 + col, m + 1, k, prefactor, gdt);
+      re[col * LD + fpad(q)] = R(v);
+      im[col * LD + fpad(q)] = R(0.);
+    }
   }
   __syncthreads();
   {
     const int col = threadIdx.x >> 5;
-    warp_fft_line<R>(re + col * ld, im + col * ld, log2n, tw);
+    warp_fft_line<R, L2N>(re + col * LD, im + col * LD, tw);
   }
   __syncthreads();
   using C2 = typename Cplx<R>::T;
-  for (int w = threadIdx.x; w < nky * COLS; w += 32 * COLS) {
+  C2 *out = reinterpret_cast<C2 *>(spec) + (size_t)(k - 1) * NKY * nx + (i0 - 1);
+#pragma unroll 4
+  for (int it = 0; it < (NKY * COLS + L::THREADS - 1) / L::THREADS; it++) {
+    const int w = threadIdx.x + it * L::THREADS;
     const int ky = w / COLS, col = w % COLS;
-    if (col < nc) {
-      reinterpret_cast<C2 *>(spec)[((size_t)(k - 1) * nky + ky) * nx + (i0 - 1 + col)] =
-          Cplx<R>::make(re[col * ld + fpad(ky)], im[col * ld + fpad(ky)]);
-    }
+    if (ky < NKY && col < nc) out[(size_t)ky * nx + col] = Cplx<R>::make(re[col * LD + fpad(ky)], im[col * LD + fpad(ky)]);
   }
 }
 
 // complex DFT along z, in place, for COLS consecutive i of one ky; the sign is
 // the twiddle table's
-template <int COLS, class R>
-__global__ void __launch_bounds__(32 * COLS) k3_pois_z(R *__restrict__ spec, const R *__restrict__ tw, int log2n,
-                                                      Grid3 g) {
+template <int L2N, class R>
+__global__ void __launch_bounds__(Line<R, L2N>::THREADS, Line<R, L2N>::MINB)
+    k3_pois_z(R *__restrict__ spec, const R *__restrict__ tw, Grid3 g) {
+  using L = Line<R, L2N>;
+  constexpr int N = L::N, LD = L::LD, COLS = L::COLS;
   extern __shared__ unsigned char smraw[];
   R *re = reinterpret_cast<R *>(smraw);
-  const int n = 1 << log2n, ld = fft_ld(n), nx = g.nx, nky = g.ny / 2 + 1;
-  R *im = re + COLS * ld;
+  R *im = re + COLS * LD;
+  const int nx = g.nx, nky = g.ny / 2 + 1;
   const int i0 = blockIdx.x * COLS;
   const int ky = blockIdx.y;
   const int nc = min(COLS, nx - i0);
   using C2 = typename Cplx<R>::T;
-  C2 *sp = reinterpret_cast<C2 *>(spec);
-  for (int w = threadIdx.x; w < COLS * n; w += 32 * COLS) {
-    const int q = w / COLS, col = w % COLS;
-    const int m = bitrev(q, log2n);
-    C2 v = Cplx<R>::make(R(0.), R(0.));
-    if (col < nc) v = sp[((size_t)m * nky + ky) * nx + (i0 + col)];
-    re[col * ld + fpad(q)] = v.x;
-    im[col * ld + fpad(q)] = v.y;
+  C2 *sp = reinterpret_cast<C2 *>(spec) + (size_t)ky * nx + i0;
+  const size_t rs = (size_t)nky * nx;  // stride of kz
+#pragma unroll 4
+  for (int it = 0; it < L::ITER; it++) {
+    const int w = threadIdx.x + it * L::THREADS;
+    if (N >= 32 || w < COLS * N) {
+      const int q = w / COLS, col = w % COLS;
+      const int m = bitrev(q, L2N);
+      C2 v = Cplx<R>::make(R(0.), R(0.));
+      if (col < nc) v = sp[m * rs + col];
+      re[col * LD + fpad(q)] = v.x;
+      im[col * LD + fpad(q)] = v.y;
+    }
   }
   __syncthreads();
   {
     const int col = threadIdx.x >> 5;
-    warp_fft_line<R>(re + col * ld, im + col * ld, log2n, tw);
+    warp_fft_line<R, L2N>(re + col * LD, im + col * LD, tw);
   }
   __syncthreads();
-  for (int w = threadIdx.x; w < COLS * n; w += 32 * COLS) {
-    const int kz = w / COLS, col = w % COLS;
-    if (col < nc)
-      sp[((size_t)kz * nky + ky) * nx + (i0 + col)] = Cplx<R>::make(re[col * ld + fpad(kz)], im[col * ld + fpad(kz)]);
+#pragma unroll 4
+  for (int it = 0; it < L::ITER; it++) {
+    const int w = threadIdx.x + it * L::THREADS;
+    if (N >= 32 || w < COLS * N) {
+      const int kz = w / COLS, col = w % COLS;
+      if (col < nc) sp[kz * rs + col] = Cplx<R>::make(re[col * LD + fpad(kz)], im[col * LD + fpad(kz)]);
+    }
   }
 }
 
@@ -356,65 +394,68 @@ __global__ void __launch_bounds__(256) k3_pois_x(R *__restrict__ spec, R *__rest
 // X_{ny/2} ignored), psi of COLS consecutive i of plane k (ACCUM: psi +=) with
 // the halo images; the Neumann walls take the new neighbour value and hand
 // their old value to the halo images
-template <int COLS, class R, bool ACCUM>
-__global__ void __launch_bounds__(32 * COLS) k3_pois_inv_y(const R *__restrict__ spec, double *__restrict__ psi,
-                                                          const R *__restrict__ tw, int log2n, Grid3 g) {
+template <int L2N, class R, bool ACCUM>
+__global__ void __launch_bounds__(Line<R, L2N>::THREADS, Line<R, L2N>::MINB)
+    k3_pois_inv_y(const R *__restrict__ spec, double *__restrict__ psi, const R *__restrict__ tw, Grid3 g) {
+  using L = Line<R, L2N>;
+  constexpr int N = L::N, LD = L::LD, COLS = L::COLS, NKY = N / 2 + 1;
   extern __shared__ unsigned char smraw[];
   R *re = reinterpret_cast<R *>(smraw);
-  const int n = 1 << log2n, ld = fft_ld(n), nx = g.nx, ny = g.ny, nz = g.nz, nky = n / 2 + 1;
-  R *im = re + COLS * ld;
+  R *im = re + COLS * LD;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int i0 = 1 + blockIdx.x * COLS;
   const int k = 1 + blockIdx.y;
   const int nc = min(COLS, nx - i0 + 1);
   using C2 = typename Cplx<R>::T;
-  const C2 *sp = reinterpret_cast<const C2 *>(spec);
-  for (int w = threadIdx.x; w < COLS * n; w += 32 * COLS) {
-    const int q = w / COLS, col = w % COLS;
-    const int m = bitrev(q, log2n);
-    R r = R(0.), x = R(0.);
-    if (col < nc) {
-      const size_t base = ((size_t)(k - 1) * nky) * nx + (i0 - 1 + col);
-      if (0 == m) {
-        r = __ldg(&sp[base].x);
-      } else if (2 * m < n) {
-        const C2 v = __ldg(&sp[base + (size_t)m * nx]);
+  const C2 *sp = reinterpret_cast<const C2 *>(spec) + (size_t)(k - 1) * NKY * nx + (i0 - 1);
+#pragma unroll 4
+  for (int it = 0; it < L::ITER; it++) {
+    const int w = threadIdx.x + it * L::THREADS;
+    if (N >= 32 || w < COLS * N) {
+      const int q = w / COLS, col = w % COLS;
+      const int m = bitrev(q, L2N);
+      R r = R(0.), x = R(0.);
+      if (col < nc) {
+        // X_m for m <= N/2, conj(X_{N-m}) above; Im of X_0 and X_{N/2} ignored
+        const int row = (2 * m <= N) ? m : N - m;
+        const C2 v = __ldg(&sp[(size_t)row * nx + col]);
         r = v.x;
-        x = v.y;
-      } else if (2 * m == n) {
-        r = __ldg(&sp[base + (size_t)m * nx].x);
-      } else {
-        const C2 v = __ldg(&sp[base + (size_t)(n - m) * nx]);
-        r = v.x;
-        x = -v.y;
+        x = (0 == m || 2 * m == N) ? R(0.) : ((2 * m < N) ? v.y : -v.y);
       }
+      re[col * LD + fpad(q)] = r;
+      im[col * LD + fpad(q)] = x;
     }
-    re[col * ld + fpad(q)] = r;
-    im[col * ld + fpad(q)] = x;
   }
   __syncthreads();
   {
     const int col = threadIdx.x >> 5;
-    warp_fft_line<R>(re + col * ld, im + col * ld, log2n, tw);
+    warp_fft_line<R, L2N>(re + col * LD, im + col * LD, tw);
   }
   __syncthreads();
-  for (int w = threadIdx.x; w < n * COLS; w += 32 * COLS) {
-    const int r = w / COLS, col = w % COLS;
-    if (col >= nc) continue;
-    const int i = i0 + col, j = r + 1;
-    double y = (double)re[col * ld + fpad(r)];
-    if (ACCUM) y += psi[ix_cc(g, i, j, k)];
-    for_images(j, k, ny, nz, true, [&](int jj, int kk) { psi[ix_cc(g, i, jj, kk)] = y; });
+#pragma unroll 4
+  for (int it = 0; it < L::ITER; it++) {
+    const int w = threadIdx.x + it * L::THREADS;
+    if (N >= 32 || w < COLS * N) {
+      const int r = w / COLS, col = w % COLS;
+      if (col < nc) {
+        const int i = i0 + col, j = r + 1;
+        double y = (double)re[col * LD + fpad(r)];
+        if (ACCUM) y += psi[ix_cc(g, i, j, k)];
+        for_images(j, k, ny, nz, true, [&](int jj, int kk) { psi[ix_cc(g, i, jj, kk)] = y; });
+      }
+    }
   }
   // (ACCUM: the walls below read the accumulated neighbour values)
   if (ACCUM) __syncthreads();
   // Neumann walls of the interior rows of this plane
   const bool has_left = (1 == i0), has_right = (i0 + nc - 1 == nx);
-  for (int w = threadIdx.x; w < 2 * n; w += 32 * COLS) {
-    const int side = w / n, j = 1 + (w - side * n);
+  if (!has_left && !has_right) return;
+  for (int w = threadIdx.x; w < 2 * N; w += L::THREADS) {
+    const int side = w / N, j = 1 + (w - side * N);
     if ((0 == side && !has_left) || (1 == side && !has_right)) continue;
     const int iw = side ? nx + 1 : 0;
     const int col = side ? nc - 1 : 0;
-    const double nv = ACCUM ? psi[ix_cc(g, i0 + col, j, k)] : (double)re[col * ld + fpad(j - 1)];
+    const double nv = ACCUM ? psi[ix_cc(g, i0 + col, j, k)] : (double)re[col * LD + fpad(j - 1)];
     const double old = psi[ix_cc(g, iw, j, k)];
     psi[ix_cc(g, iw, j, k)] = nv;
     for_images(j, k, ny, nz, false, [&](int jj, int kk) { psi[ix_cc(g, iw, jj, kk)] = old; });
@@ -423,64 +464,75 @@ __global__ void __launch_bounds__(32 * COLS) k3_pois_inv_y(const R *__restrict__
 
 // ---- host-side launchers (the templates stay in this translation unit)
 namespace {
+constexpr int kMinL2N = 1, kMaxL2N = 11;
 template <class F>
-cudaError_t by_cols(int cols, F f) {
-  switch (cols) {
-    case 16: return f(std::integral_constant<int, 16>());
-    case 8: return f(std::integral_constant<int, 8>());
+cudaError_t by_l2n(int l2n, F f) {
+  switch (l2n) {
+    case 1: return f(std::integral_constant<int, 1>());
+    case 2: return f(std::integral_constant<int, 2>());
+    case 3: return f(std::integral_constant<int, 3>());
     case 4: return f(std::integral_constant<int, 4>());
+    case 5: return f(std::integral_constant<int, 5>());
+    case 6: return f(std::integral_constant<int, 6>());
+    case 7: return f(std::integral_constant<int, 7>());
+    case 8: return f(std::integral_constant<int, 8>());
+    case 9: return f(std::integral_constant<int, 9>());
+    case 10: return f(std::integral_constant<int, 10>());
+    case 11: return f(std::integral_constant<int, 11>());
     default: return cudaErrorInvalidValue;
   }
 }
-template <class R>
-size_t fft_smem(int n, int cols) {
-  return sizeof(R) * 2 * (size_t)fft_ld(n) * cols;
+template <class K>
+cudaError_t line_attrs(K kernel, int smem) {
+  cudaError_t r = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (cudaSuccess != r) return r;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
 }
 }  // namespace
 
 template <class R>
-cudaError_t pois_prepare(int ny, int cols_y, int nz, int cols_z) {
-  cudaError_t e = by_cols(cols_y, [&](auto c) {
-    constexpr int C = decltype(c)::value;
-    const int sy = (int)fft_smem<R>(ny, C);
-    const cudaFuncAttribute at = cudaFuncAttributeMaxDynamicSharedMemorySize;
+cudaError_t pois_prepare(int log2ny, int log2nz) {
+  if (log2ny < kMinL2N || log2ny > kMaxL2N || log2nz < kMinL2N || log2nz > kMaxL2N) return cudaErrorInvalidValue;
+  cudaError_t e = by_l2n(log2ny, [&](auto c) {
+    constexpr int L2 = decltype(c)::value;
+    constexpr int sm = Line<R, L2>::SMEM;
     cudaError_t r;
-    if (cudaSuccess != (r = cudaFuncSetAttribute(k3_pois_fwd_y<C, R, false>, at, sy))) return r;
-    if (cudaSuccess != (r = cudaFuncSetAttribute(k3_pois_fwd_y<C, R, true>, at, sy))) return r;
-    if (cudaSuccess != (r = cudaFuncSetAttribute(k3_pois_inv_y<C, R, false>, at, sy))) return r;
-    return cudaFuncSetAttribute(k3_pois_inv_y<C, R, true>, at, sy);
+    if (cudaSuccess != (r = line_attrs(k3_pois_fwd_y<L2, R, false>, sm))) return r;
+    if (cudaSuccess != (r = line_attrs(k3_pois_fwd_y<L2, R, true>, sm))) return r;
+    if (cudaSuccess != (r = line_attrs(k3_pois_inv_y<L2, R, false>, sm))) return r;
+    return line_attrs(k3_pois_inv_y<L2, R, true>, sm);
   });
   if (cudaSuccess != e) return e;
-  return by_cols(cols_z, [&](auto c) {
-    constexpr int C = decltype(c)::value;
-    return cudaFuncSetAttribute(k3_pois_z<C, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)fft_smem<R>(nz, C));
+  return by_l2n(log2nz, [&](auto c) {
+    constexpr int L2 = decltype(c)::value;
+    return line_attrs(k3_pois_z<L2, R>, Line<R, L2>::SMEM);
   });
 }
 
 template <class R>
-cudaError_t pois_fwd_y(int cols, bool resid, cudaStream_t st, const double *ux, const double *uy, const double *uz,
+cudaError_t pois_fwd_y(bool resid, cudaStream_t st, const double *ux, const double *uy, const double *uz,
                        const double *psi, const double *pl, const double *pu, R *spec, const R *tw,
                        const double *dtp, double gam, int log2n, Grid3 g) {
-  return by_cols(cols, [&](auto c) {
-    constexpr int C = decltype(c)::value;
-    dim3 gr((g.nx + C - 1) / C, g.nz);
-    const size_t sm = fft_smem<R>(g.ny, C);
+  return by_l2n(log2n, [&](auto c) {
+    constexpr int L2 = decltype(c)::value;
+    using L = Line<R, L2>;
+    dim3 gr((g.nx + L::COLS - 1) / L::COLS, g.nz);
     if (resid) {
-      k3_pois_fwd_y<C, R, true><<<gr, 32 * C, sm, st>>>(ux, uy, uz, psi, pl, pu, spec, tw, dtp, gam, log2n, g);
+      k3_pois_fwd_y<L2, R, true><<<gr, L::THREADS, L::SMEM, st>>>(ux, uy, uz, psi, pl, pu, spec, tw, dtp, gam, g);
     } else {
-      k3_pois_fwd_y<C, R, false><<<gr, 32 * C, sm, st>>>(ux, uy, uz, psi, pl, pu, spec, tw, dtp, gam, log2n, g);
+      k3_pois_fwd_y<L2, R, false><<<gr, L::THREADS, L::SMEM, st>>>(ux, uy, uz, psi, pl, pu, spec, tw, dtp, gam, g);
     }
     return cudaGetLastError();
   });
 }
 
 template <class R>
-cudaError_t pois_z(int cols, cudaStream_t st, R *spec, const R *tw, int log2n, Grid3 g) {
-  return by_cols(cols, [&](auto c) {
-    constexpr int C = decltype(c)::value;
-    dim3 gr((g.nx + C - 1) / C, g.ny / 2 + 1);
-    k3_pois_z<C, R><<<gr, 32 * C, fft_smem<R>(g.nz, C), st>>>(spec, tw, log2n, g);
+cudaError_t pois_z(cudaStream_t st, R *spec, const R *tw, int log2n, Grid3 g) {
+  return by_l2n(log2n, [&](auto c) {
+    constexpr int L2 = decltype(c)::value;
+    using L = Line<R, L2>;
+    dim3 gr((g.nx + L::COLS - 1) / L::COLS, g.ny / 2 + 1);
+    k3_pois_z<L2, R><<<gr, L::THREADS, L::SMEM, st>>>(spec, tw, g);
     return cudaGetLastError();
   });
 }
@@ -494,30 +546,29 @@ cudaError_t pois_x(cudaStream_t st, R *spec, R *scratch, const double *pl, const
 }
 
 template <class R>
-cudaError_t pois_inv_y(int cols, bool accum, cudaStream_t st, const R *spec, double *psi, const R *tw, int log2n,
-                       Grid3 g) {
-  return by_cols(cols, [&](auto c) {
-    constexpr int C = decltype(c)::value;
-    dim3 gr((g.nx + C - 1) / C, g.nz);
-    const size_t sm = fft_smem<R>(g.ny, C);
+cudaError_t pois_inv_y(bool accum, cudaStream_t st, const R *spec, double *psi, const R *tw, int log2n, Grid3 g) {
+  return by_l2n(log2n, [&](auto c) {
+    constexpr int L2 = decltype(c)::value;
+    using L = Line<R, L2>;
+    dim3 gr((g.nx + L::COLS - 1) / L::COLS, g.nz);
     if (accum) {
-      k3_pois_inv_y<C, R, true><<<gr, 32 * C, sm, st>>>(spec, psi, tw, log2n, g);
+      k3_pois_inv_y<L2, R, true><<<gr, L::THREADS, L::SMEM, st>>>(spec, psi, tw, g);
     } else {
-      k3_pois_inv_y<C, R, false><<<gr, 32 * C, sm, st>>>(spec, psi, tw, log2n, g);
+      k3_pois_inv_y<L2, R, false><<<gr, L::THREADS, L::SMEM, st>>>(spec, psi, tw, g);
     }
     return cudaGetLastError();
   });
 }
 
 #define SVOF3_POISSON_INST(R)                                                                                    \
-  template cudaError_t pois_prepare<R>(int, int, int, int);                                                      \
-  template cudaError_t pois_fwd_y<R>(int, bool, cudaStream_t, const double *, const double *, const double *,   \
+  template cudaError_t pois_prepare<R>(int, int);                                                                \
+  template cudaError_t pois_fwd_y<R>(bool, cudaStream_t, const double *, const double *, const double *,   \
                                      const double *, const double *, const double *, R *, const R *,            \
                                      const double *, double, int, Grid3);                                       \
-  template cudaError_t pois_z<R>(int, cudaStream_t, R *, const R *, int, Grid3);                                 \
+  template cudaError_t pois_z<R>(cudaStream_t, R *, const R *, int, Grid3);                                      \
   template cudaError_t pois_x<R>(cudaStream_t, R *, R *, const double *, const double *, const double *,        \
                                  const double *, int, Grid3);                                                    \
-  template cudaError_t pois_inv_y<R>(int, bool, cudaStream_t, const R *, double *, const R *, int, Grid3);
+  template cudaError_t pois_inv_y<R>(bool, cudaStream_t, const R *, double *, const R *, int, Grid3);
 SVOF3_POISSON_INST(double)
 SVOF3_POISSON_INST(float)
 #undef SVOF3_POISSON_INST

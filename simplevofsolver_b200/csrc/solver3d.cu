@@ -113,7 +113,6 @@ struct svof3d_solver {
   // Poisson
   DevBuf spec, xscratch, twf_y, twb_y, twf_z, twb_z, pl, pu, evy, evz;
   DevBuf twf_y32, twb_y32, twf_z32, twb_z32;  // FP32 twiddles of the mixed path
-  int cols_y = 8, cols_z = 8;
   // predictor forward-sweep scratch
   DevBuf fw;
   // time step
@@ -268,17 +267,17 @@ int launch_potential_t(svof3d_solver *s, int rk, const Marker &mark, const R *tw
   for (int pass = 0; pass < passes; pass++) {
     const bool second = pass > 0;
     const int cu = s->cur_u;
-    CK(pois_fwd_y<R>(s->cols_y, second, s->stream, s->ux[cu].p, s->uy[cu].p, s->uz[cu].p, s->psi.p, s->pl.p,
+    CK(pois_fwd_y<R>(second, s->stream, s->ux[cu].p, s->uy[cu].p, s->uz[cu].p, s->psi.p, s->pl.p,
                      s->pu.p, s->spec.as<R>(), twfy, s->d_dt, gam, s->log2ny, g));
     if (m(SVOF3_K_POISSON_FWD)) return 1;
-    CK(pois_z<R>(s->cols_z, s->stream, s->spec.as<R>(), twfz, s->log2nz, g));
+    CK(pois_z<R>(s->stream, s->spec.as<R>(), twfz, s->log2nz, g));
     if (m(SVOF3_K_POISSON_Z)) return 1;
     CK(pois_x<R>(s->stream, s->spec.as<R>(), s->xscratch.as<R>(), s->pl.p, s->pu.p, s->evy.p, s->evz.p,
                  s->mixed ? 1 : 0, g));
     if (m(SVOF3_K_POISSON_SOLVE)) return 1;
-    CK(pois_z<R>(s->cols_z, s->stream, s->spec.as<R>(), twbz, s->log2nz, g));
+    CK(pois_z<R>(s->stream, s->spec.as<R>(), twbz, s->log2nz, g));
     if (m(SVOF3_K_POISSON_Z)) return 1;
-    CK(pois_inv_y<R>(s->cols_y, second, s->stream, s->spec.as<R>(), s->psi.p, twby, s->log2ny, g));
+    CK(pois_inv_y<R>(second, s->stream, s->spec.as<R>(), s->psi.p, twby, s->log2ny, g));
     if (m(SVOF3_K_POISSON_INV)) return 1;
   }
   return 0;
@@ -416,6 +415,8 @@ int build_tables(svof3d_solver *s, const double *xf, const double *xc) {
   s->log2ny = ilog2_exact(ny);
   s->log2nz = ilog2_exact(nz);
   if (s->log2ny < 1 || s->log2nz < 1) return fail("svof3d_create: ny and nz must be powers of two (got %d, %d)", ny, nz);
+  // (the transforms are compiled for lengths 2 .. 2048)
+  if (s->log2ny > 11 || s->log2nz > 11) return fail("svof3d_create: ny and nz at most 2048 (got %d, %d)", ny, nz);
   auto twiddles = [&](int n, DevBuf &f, DevBuf &b) -> int {
     std::vector<double> twf(2 * (n / 2)), twb(2 * (n / 2));
     for (int m = 0; m < n / 2; m++) {
@@ -529,16 +530,9 @@ int svof3d_create(const svof3d_params_t *prm, const double *xf, const double *xc
   if (dalloc(s->spec, 2 * nx * nky * nz, es) || dalloc(s->xscratch, nx * nky * nz, es) ||
       dalloc(s->fw, 4 * nx * ny * nz, es))
     return bail();
-  // transforms: one line per warp, 16 / 8 / 4 lines per block by length (the
-  // y transforms read rows of 16 / 8 / 4 consecutive i)
-  auto pick_cols = [](int n) { return n <= 256 ? 16 : (n <= 512 ? 8 : 4); };
-  s->cols_y = pick_cols(s->ny);
-  s->cols_z = pick_cols(s->nz);
   {
-    const size_t smy = es * 2 * (ny + 1) * s->cols_y, smz = es * 2 * (nz + 1) * s->cols_z;
-    if (smy > 200 * 1024 || smz > 200 * 1024) return fail("svof3d_create: FFT length too large"), bail();
-    const cudaError_t pe = s->mixed ? pois_prepare<float>(s->ny, s->cols_y, s->nz, s->cols_z)
-                                    : pois_prepare<double>(s->ny, s->cols_y, s->nz, s->cols_z);
+    const cudaError_t pe = s->mixed ? pois_prepare<float>(s->log2ny, s->log2nz)
+                                    : pois_prepare<double>(s->log2ny, s->log2nz);
     if (cudaSuccess != pe || cudaSuccess != predict_prepare() || cudaSuccess != interface_prepare())
       return fail("cudaFuncSetAttribute(Poisson): %s", cudaGetErrorString(cudaGetLastError())), bail();
     const size_t coef_smem = sizeof(double) * 6 * nx;
