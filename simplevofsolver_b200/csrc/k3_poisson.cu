@@ -10,9 +10,11 @@
 //
 //   k3_pois_fwd_y  a block owns COLS consecutive i of one plane k
 //   k3_pois_z      a block owns COLS consecutive i of one ky, both signs
-//   k3_pois_x      a block owns 32 lines (ky, kz), walked in 32-cell chunks:
-//                  forward recurrence (values back into S, v into scratch),
-//                  then back substitution in reverse chunk order
+//                  (in place)
+//   k3_pois_x      a block owns 64 or 128 lines (ky, kz), one per thread,
+//                  walked in 16-cell chunks: forward recurrence (values back
+//                  into S, v into scratch), then back substitution in reverse
+//                  chunk order
 //   k3_pois_inv_y  a block owns COLS consecutive i of one plane k; writes psi
 //                  with its halo images and Neumann walls
 //
@@ -24,6 +26,8 @@
 // adds its solution to psi (ACCUM); its singular (ky, kz) = (0, 0) line has
 // its gauge pinned (last unknown zero) so that the FP32 round-off of the
 // compatibility condition cannot blow the additive constant up.
+#include <cuda_pipeline.h>
+
 #include <type_traits>
 
 #include "fft_device.cuh"
@@ -46,30 +50,31 @@ struct Cplx<float> {
   static __device__ __forceinline__ T make(float a, float b) { return make_float2(a, b); }
 };
 
-// One warp per line, the line length N = 2^L2N a compile-time constant.
-// Lines are stored re / im separately in shared memory, position p at padded
-// index pad(p) = p + p / 8 and lines LD = N + N / 8 + 1 apart, which keeps the
-// column-wise loads and stores (consecutive threads on consecutive lines) and
-// the register passes below free of bank conflicts.  The transform is the
-// oracle's radix-2 decimation in time (same butterfly pairs, same twiddles,
-// same association), executed in passes of up to three stages: a lane loads
-// the 2^NS points a pass combines, runs their butterflies in registers and
-// stores them back, so shared memory is touched once per pass instead of once
-// per stage.
+// The transforms.  A block owns COLS lines of N = 2^L2N points (N a
+// compile-time constant): consecutive i of one plane k for y, of one ky for z.
+// The transform is the oracle's radix-2 decimation in time (same butterfly
+// pairs, same twiddles, same association) run in passes of up to three
+// stages.  In a pass a thread takes (line, group) pairs, lines fastest across
+// the lanes, loads the 2^NS points of its group, runs their butterflies in
+// registers and stores them.  The first pass reads its points (in bit-reversed
+// order) from global memory and the last one writes its results there, so a
+// warp's global accesses are runs of consecutive i; the passes between go
+// through shared memory, re / im separately, point p of line c at
+// c LD + p + p / 8 with LD = N + N / 8 + 1 odd, so the lanes of a half warp,
+// on distinct lines, fall on distinct banks.
 __device__ __forceinline__ int fpad(int p) { return p + (p >> 3); }
 
-// Shape of a block of one transform direction: COLS lines of N points, one
-// warp each.  COLS is the widest of 16 / 8 / 4 whose shared memory stays
-// within 80 KB (the rows the y transforms read are COLS x 8 bytes wide and,
-// with the reference's x pitch of nx + 2, not sector aligned: wider rows waste
-// less of each sector), MINB the resident blocks per SM the launch bounds ask
-// for (shared memory permitting, and no fewer than 64 registers a thread).
+constexpr int kLineThreads = 256;
+// COLS: the widest of 16 / 8 / 4 lines whose shared memory stays within 80 KB
+// (the rows the y transforms read are COLS x 8 bytes wide and, with the
+// reference's x pitch of nx + 2, not sector aligned: wider rows waste less of
+// each sector).  MINB: resident blocks per SM, shared memory permitting, at
+// most 4 (64 registers a thread).
 constexpr int line_cols(int col_bytes) {
   return (16 * col_bytes <= 81920) ? 16 : ((8 * col_bytes <= 81920) ? 8 : 4);
 }
-constexpr int line_minb(int smem, int threads) {
-  return (232448 / (smem + 1024) < 1024 / threads) ? ((232448 / (smem + 1024)) < 1 ? 1 : 232448 / (smem + 1024))
-                                                    : ((1024 / threads) < 1 ? 1 : 1024 / threads);
+constexpr int line_minb(int smem) {
+  return (232448 / (smem + 1024) < 1) ? 1 : ((232448 / (smem + 1024) > 4) ? 4 : 232448 / (smem + 1024));
 }
 template <class R, int L2N>
 struct Line {
@@ -77,101 +82,168 @@ struct Line {
   static constexpr int LD = N + (N >> 3) + 1;
   static constexpr int COL_BYTES = 2 * (int)sizeof(R) * LD;
   static constexpr int COLS = line_cols(COL_BYTES);
-  static constexpr int THREADS = 32 * COLS;
   static constexpr int SMEM = COLS * COL_BYTES;
-  static constexpr int MINB = line_minb(SMEM, THREADS);
-  static constexpr int ITER = (N + 31) / 32;  // points per thread in the load / store loops
+  static constexpr int MINB = line_minb(SMEM);
 };
 
+// twiddle loads: read-only path, kept in L1 ahead of the streaming data
+__device__ __forceinline__ double2 tw_ld(const double2 *p) {
+  double2 v;
+  asm("ld.global.nc.L1::evict_last.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ float2 tw_ld(const float2 *p) {
+  float2 v;
+  asm("ld.global.nc.L1::evict_last.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p));
+  return v;
+}
+
+// the butterflies of stages S0 .. S0 + NS - 1 of group gi, in registers
 template <class R, int L2N, int S0, int NS>
-__device__ __forceinline__ void fft_pass(R *__restrict__ re, R *__restrict__ im, const R *__restrict__ tw) {
+__device__ __forceinline__ void butterflies(int gi, R *xr, R *xi, const R *__restrict__ tw) {
   using C2 = typename Cplx<R>::T;
-  constexpr int G = 1 << NS, H = 1 << (S0 - 1), NG = (1 << L2N) >> NS;
-  const int lane = threadIdx.x & 31;
+  constexpr int G = 1 << NS, H = 1 << (S0 - 1);
 #pragma unroll
-  for (int g0 = 0; g0 < NG; g0 += 32) {
-    const int gi = g0 + lane;
-    if (NG >= 32 || gi < NG) {
-      const int base = (gi & (H - 1)) + ((gi >> (S0 - 1)) << (S0 - 1 + NS));
-      R xr[G], xi[G];
+  for (int t = 0; t < NS; t++) {
+    const int st_ = S0 + t, dist = 1 << t;
 #pragma unroll
-      for (int m = 0; m < G; m++) {
-        const int q = fpad(base + m * H);
-        xr[m] = re[q];
-        xi[m] = im[q];
-      }
-#pragma unroll
-      for (int t = 0; t < NS; t++) {
-        const int st = S0 + t, dist = 1 << t;
-#pragma unroll
-        for (int m = 0; m < G; m++) {
-          if (m & dist) continue;
-          // twiddle index of the pair (base + m H, base + (m + dist) H) at stage st
-          const int kk = (gi & (H - 1)) + (m & (dist - 1)) * H;
-          const C2 w = __ldg(reinterpret_cast<const C2 *>(tw) + (kk << (L2N - st)));
-          const R br = xr[m + dist], bi = xi[m + dist];
-          const R tr = w.x * br - w.y * bi;
-          const R ti = w.x * bi + w.y * br;
-          const R ur = xr[m], ui = xi[m];
-          xr[m] = ur + tr;
-          xi[m] = ui + ti;
-          xr[m + dist] = ur - tr;
-          xi[m + dist] = ui - ti;
-        }
-      }
-#pragma unroll
-      for (int m = 0; m < G; m++) {
-        const int q = fpad(base + m * H);
-        re[q] = xr[m];
-        im[q] = xi[m];
-      }
+    for (int m = 0; m < G; m++) {
+      if (m & dist) continue;
+      // twiddle of the pair (base + m H, base + (m + dist) H) at stage st_
+      const int kk = (gi & (H - 1)) + (m & (dist - 1)) * H;
+      const C2 w = tw_ld(reinterpret_cast<const C2 *>(tw) + (kk << (L2N - st_)));
+      const R br = xr[m + dist], bi = xi[m + dist];
+      const R tr = w.x * br - w.y * bi;
+      const R ti = w.x * bi + w.y * br;
+      const R ur = xr[m], ui = xi[m];
+      xr[m] = ur + tr;
+      xi[m] = ui + ti;
+      xr[m + dist] = ur - tr;
+      xi[m + dist] = ui - ti;
     }
   }
-  __syncwarp();
 }
 
-template <class R, int L2N, int S0 = 1>
-__device__ __forceinline__ void warp_fft_line(R *__restrict__ re, R *__restrict__ im, const R *__restrict__ tw) {
-  if constexpr (S0 <= L2N) {
-    constexpr int NS = (L2N - S0 + 1) < 3 ? (L2N - S0 + 1) : 3;
-    fft_pass<R, L2N, S0, NS>(re, im, tw);
-    warp_fft_line<R, L2N, S0 + NS>(re, im, tw);
+// stages S0 .. S0 + NS - 1 of the block's COLS lines: ld(c, base, G, H, re,
+// im) fetches the G points base + m H (m < G) of line c into re[m], im[m],
+// st(c, base, G, H, re, im) stores them (G and H as integral constants)
+template <class R, int L2N, int COLS, int S0, int NS, class LdF, class StF>
+__device__ __forceinline__ void fft_pass(const R *__restrict__ tw, LdF ld, StF st) {
+  constexpr int G = 1 << NS, H = 1 << (S0 - 1), NG = (1 << L2N) >> NS, PAIRS = COLS * NG;
+  using GC = std::integral_constant<int, G>;
+  using HC = std::integral_constant<int, H>;
+#pragma unroll
+  for (int p0 = 0; p0 < PAIRS; p0 += kLineThreads) {
+    const int pr = p0 + (int)threadIdx.x;
+    if (0 == PAIRS % kLineThreads || pr < PAIRS) {
+      const int c = pr % COLS, gi = pr / COLS;
+      const int base = (gi & (H - 1)) + ((gi >> (S0 - 1)) << (S0 - 1 + NS));
+      R xr[G], xi[G];
+      ld(c, base, GC(), HC(), xr, xi);
+      butterflies<R, L2N, S0, NS>(gi, xr, xi, tw);
+      st(c, base, GC(), HC(), xr, xi);
+    }
   }
 }
 
-// right-hand side (or, RESID, the residual b - A psi) at (i, j, k); FP64
-template <bool RESID>
-__device__ __forceinline__ double pois_rhs(const double *__restrict__ ux, const double *__restrict__ uy,
-                                           const double *__restrict__ uz, const double *__restrict__ psi,
-                                           const double *__restrict__ pl, const double *__restrict__ pu,
-                                           const Grid3 &g, int i, int j, int k, double prefactor, double gdt) {
-  const double dx = ldg(g.dxf + i - 1);
-  const double div = +(ldg(ux + ix_ux(g, i + 1, j, k)) - ldg(ux + ix_ux(g, i, j, k))) / dx +
-                     (ldg(uy + ix_cc(g, i, j + 1, k)) - ldg(uy + ix_cc(g, i, j, k))) / g.dy +
-                     (ldg(uz + ix_cc(g, i, j, k + 1)) - ldg(uz + ix_cc(g, i, j, k))) / g.dz;
-  if (!RESID) return prefactor * div;
-  const double c = ldg(psi + ix_cc(g, i, j, k));
-  const double l = ldg(pl + i - 1), u = ldg(pu + i - 1);
-  const double ap = l * ldg(psi + ix_cc(g, i - 1, j, k)) + (-l - u) * c + u * ldg(psi + ix_cc(g, i + 1, j, k)) +
-                    (ldg(psi + ix_cc(g, i, j - 1, k)) - 2. * c + ldg(psi + ix_cc(g, i, j + 1, k))) / (g.dy * g.dy) +
-                    (ldg(psi + ix_cc(g, i, j, k - 1)) - 2. * c + ldg(psi + ix_cc(g, i, j, k + 1))) / (g.dz * g.dz);
-  return (div / gdt - ap) / (1. * g.ny * g.nz);
+// all passes: the first reads through `first`, the last writes through `last`
+template <class R, int L2N, int COLS, int S0 = 1, class FirstF, class LastF>
+__device__ __forceinline__ void fft_lines(R *__restrict__ re, R *__restrict__ im, const R *__restrict__ tw,
+                                          FirstF first, LastF last) {
+  constexpr int LD = Line<R, L2N>::LD;
+  constexpr int NS = (L2N - S0 + 1) < 3 ? (L2N - S0 + 1) : 3;
+  constexpr bool IS_FIRST = (1 == S0), IS_LAST = (S0 + NS > L2N);
+  auto lds = [&](int c, int base, auto gc, auto hc, R *xr, R *xi) {
+    constexpr int G = decltype(gc)::value, H = decltype(hc)::value;
+#pragma unroll
+    for (int m = 0; m < G; m++) {
+      xr[m] = re[c * LD + fpad(base + m * H)];
+      xi[m] = im[c * LD + fpad(base + m * H)];
+    }
+  };
+  auto sts = [&](int c, int base, auto gc, auto hc, const R *xr, const R *xi) {
+    constexpr int G = decltype(gc)::value, H = decltype(hc)::value;
+#pragma unroll
+    for (int m = 0; m < G; m++) {
+      re[c * LD + fpad(base + m * H)] = xr[m];
+      im[c * LD + fpad(base + m * H)] = xi[m];
+    }
+  };
+  if constexpr (IS_FIRST && IS_LAST) {
+    fft_pass<R, L2N, COLS, S0, NS>(tw, first, last);
+  } else if constexpr (IS_FIRST) {
+    fft_pass<R, L2N, COLS, S0, NS>(tw, first, sts);
+  } else if constexpr (IS_LAST) {
+    fft_pass<R, L2N, COLS, S0, NS>(tw, lds, last);
+  } else {
+    fft_pass<R, L2N, COLS, S0, NS>(tw, lds, sts);
+  }
+  if constexpr (!IS_LAST) {
+    __syncthreads();
+    fft_lines<R, L2N, COLS, S0 + NS>(re, im, tw, first, last);
+  }
 }
 
-// forward transform along y of COLS consecutive i of plane k: the right-hand
-// side (RESID: the residual) of each point, in bit-reversed order, then the
-// warp transforms, then the ky = 0 .. N/2 half of the spectrum
+// right-hand side (or, RESID, the residual b - A psi) at (i, j, k), FP64, in
+// two steps so that a group's loads can all be in flight before its first
+// division: rhs_terms gathers the differences (loads, subtractions and
+// products only), rhs_value forms the quotients and sums, with the
+// association of b = div u / (gamma dt ny nz) and of the 7-point operator
+template <bool RESID>
+struct RhsTerms;
+template <>
+struct RhsTerms<false> {
+  double dux, duy, duz;
+};
+template <>
+struct RhsTerms<true> {
+  double dux, duy, duz, ax, ty, tz;
+};
+
+template <bool RESID>
+__device__ __forceinline__ RhsTerms<RESID> rhs_terms(const double *__restrict__ ux, const double *__restrict__ uy,
+                                                     const double *__restrict__ uz, const double *__restrict__ psi,
+                                                     double l, double u, const Grid3 &g, int i, int j, int k) {
+  RhsTerms<RESID> t;
+  t.dux = ldg(ux + ix_ux(g, i + 1, j, k)) - ldg(ux + ix_ux(g, i, j, k));
+  t.duy = ldg(uy + ix_cc(g, i, j + 1, k)) - ldg(uy + ix_cc(g, i, j, k));
+  t.duz = ldg(uz + ix_cc(g, i, j, k + 1)) - ldg(uz + ix_cc(g, i, j, k));
+  if constexpr (RESID) {
+    const double c = ldg(psi + ix_cc(g, i, j, k));
+    t.ax = l * ldg(psi + ix_cc(g, i - 1, j, k)) + (-l - u) * c + u * ldg(psi + ix_cc(g, i + 1, j, k));
+    t.ty = ldg(psi + ix_cc(g, i, j - 1, k)) - 2. * c + ldg(psi + ix_cc(g, i, j + 1, k));
+    t.tz = ldg(psi + ix_cc(g, i, j, k - 1)) - 2. * c + ldg(psi + ix_cc(g, i, j, k + 1));
+  }
+  return t;
+}
+
+template <bool RESID>
+__device__ __forceinline__ double rhs_value(const RhsTerms<RESID> &t, double dx, const Grid3 &g, double prefactor,
+                                            double gdt) {
+  const double div = +t.dux / dx + t.duy / g.dy + t.duz / g.dz;
+  if constexpr (!RESID) {
+    return prefactor * div;
+  } else {
+    const double ap = t.ax + t.ty / (g.dy * g.dy) + t.tz / (g.dz * g.dz);
+    return (div / gdt - ap) / (1. * g.ny * g.nz);
+  }
+}
+
+// forward transform along y of COLS consecutive i of plane k: the first pass
+// evaluates the right-hand side (RESID: the residual) of its points, the last
+// one writes the ky = 0 .. N/2 half of the spectrum
 template <int L2N, class R, bool RESID>
-__global__ void __launch_bounds__(Line<R, L2N>::THREADS, Line<R, L2N>::MINB)
+__global__ void __launch_bounds__(kLineThreads, Line<R, L2N>::MINB)
     k3_pois_fwd_y(const double *__restrict__ ux, const double *__restrict__ uy, const double *__restrict__ uz,
                   const double *__restrict__ psi, const double *__restrict__ pl, const double *__restrict__ pu,
                   R *__restrict__ spec, const R *__restrict__ tw, const double *__restrict__ dtp, double gam,
                   Grid3 g) {
   using L = Line<R, L2N>;
-  constexpr int N = L::N, LD = L::LD, COLS = L::COLS, NKY = N / 2 + 1;
+  using C2 = typename Cplx<R>::T;
+  constexpr int N = L::N, COLS = L::COLS, NKY = N / 2 + 1;
   extern __shared__ unsigned char smraw[];
   R *re = reinterpret_cast<R *>(smraw);
-  R *im = re + COLS * LD;
+  R *im = re + COLS * L::LD;
   const int nx = g.nx;
   const int i0 = 1 + blockIdx.x * COLS;
   const int k = 1 + blockIdx.y;
@@ -179,128 +251,165 @@ __global__ void __launch_bounds__(Line<R, L2N>::THREADS, Line<R, L2N>::MINB)
   const double dt = ldg(dtp);
   const double prefactor = 1. / (gam * dt) / (1. * g.ny * g.nz);
   const double gdt = gam * dt;
-#pragma unroll 4
-  for (int it = 0; it < L::ITER; it++) {
-    const int w = threadIdx.x + it * L::THREADS;
-    if (N >= 32 || w < COLS * N) {
-      const int q = w / COLS, col = w % COLS;
-      const int m = bitrev(q, L2N);
-      double v = 0.;
-      if (col < nc) v = pois_rhs<RESID>(ux, uy, uz, psi, pl, pu, g, i0 + col, m + 1, k, prefactor, gdt);
-      re[col * LD + fpad(q)] = R(v);
-      im[col * LD + fpad(q)] = R(0.);
-    }
-  }
-  __syncthreads();
-  {
-    const int col = threadIdx.x >> 5;
-    warp_fft_line<R, L2N>(re + col * LD, im + col * LD, tw);
-  }
-  __syncthreads();
-  using C2 = typename Cplx<R>::T;
   C2 *out = reinterpret_cast<C2 *>(spec) + (size_t)(k - 1) * NKY * nx + (i0 - 1);
-#pragma unroll 4
-  for (int it = 0; it < (NKY * COLS + L::THREADS - 1) / L::THREADS; it++) {
-    const int w = threadIdx.x + it * L::THREADS;
-    const int ky = w / COLS, col = w % COLS;
-    if (ky < NKY && col < nc) out[(size_t)ky * nx + col] = Cplx<R>::make(re[col * LD + fpad(ky)], im[col * LD + fpad(ky)]);
-  }
+  auto first = [&](int c, int base, auto gc, auto hc, R *xr, R *xi) {
+    constexpr int G = decltype(gc)::value, H = decltype(hc)::value, BM = RESID ? 2 : 4, B = G < BM ? G : BM;
+    const int i = i0 + c;
+    const bool live = c < nc;
+    double dx = 1., l = 0., u = 0.;
+    if (live) {
+      dx = ldg(g.dxf + i - 1);
+      if (RESID) {
+        l = ldg(pl + i - 1);
+        u = ldg(pu + i - 1);
+      }
+    }
+#pragma unroll
+    for (int b0 = 0; b0 < G; b0 += B) {
+      RhsTerms<RESID> t[B];
+#pragma unroll
+      for (int q = 0; q < B; q++) {
+        if (live) t[q] = rhs_terms<RESID>(ux, uy, uz, psi, l, u, g, i, bitrev(base + (b0 + q) * H, L2N) + 1, k);
+      }
+#pragma unroll
+      for (int q = 0; q < B; q++) {
+        xr[b0 + q] = R(live ? rhs_value<RESID>(t[q], dx, g, prefactor, gdt) : 0.);
+        xi[b0 + q] = R(0.);
+      }
+    }
+  };
+  auto last = [&](int c, int base, auto gc, auto hc, const R *xr, const R *xi) {
+    constexpr int G = decltype(gc)::value, H = decltype(hc)::value;
+    if (c >= nc) return;
+#pragma unroll
+    for (int m = 0; m < G; m++) {
+      const int p = base + m * H;
+      if (p <= N / 2) out[(size_t)p * nx + c] = Cplx<R>::make(xr[m], xi[m]);
+    }
+  };
+  fft_lines<R, L2N, COLS>(re, im, tw, first, last);
 }
 
 // complex DFT along z, in place, for COLS consecutive i of one ky; the sign is
-// the twiddle table's
+// the twiddle table's (every read of the first pass precedes every write of
+// the last, the passes being separated by block barriers; a single-pass
+// length has one group per line)
 template <int L2N, class R>
-__global__ void __launch_bounds__(Line<R, L2N>::THREADS, Line<R, L2N>::MINB)
+__global__ void __launch_bounds__(kLineThreads, Line<R, L2N>::MINB)
     k3_pois_z(R *__restrict__ spec, const R *__restrict__ tw, Grid3 g) {
   using L = Line<R, L2N>;
-  constexpr int N = L::N, LD = L::LD, COLS = L::COLS;
+  using C2 = typename Cplx<R>::T;
+  constexpr int COLS = L::COLS;
   extern __shared__ unsigned char smraw[];
   R *re = reinterpret_cast<R *>(smraw);
-  R *im = re + COLS * LD;
+  R *im = re + COLS * L::LD;
   const int nx = g.nx, nky = g.ny / 2 + 1;
   const int i0 = blockIdx.x * COLS;
   const int ky = blockIdx.y;
   const int nc = min(COLS, nx - i0);
-  using C2 = typename Cplx<R>::T;
   C2 *sp = reinterpret_cast<C2 *>(spec) + (size_t)ky * nx + i0;
   const size_t rs = (size_t)nky * nx;  // stride of kz
-#pragma unroll 4
-  for (int it = 0; it < L::ITER; it++) {
-    const int w = threadIdx.x + it * L::THREADS;
-    if (N >= 32 || w < COLS * N) {
-      const int q = w / COLS, col = w % COLS;
-      const int m = bitrev(q, L2N);
+  auto first = [&](int c, int base, auto gc, auto hc, R *xr, R *xi) {
+    constexpr int G = decltype(gc)::value, H = decltype(hc)::value;
+#pragma unroll
+    for (int m = 0; m < G; m++) {
       C2 v = Cplx<R>::make(R(0.), R(0.));
-      if (col < nc) v = sp[m * rs + col];
-      re[col * LD + fpad(q)] = v.x;
-      im[col * LD + fpad(q)] = v.y;
+      if (c < nc) v = sp[bitrev(base + m * H, L2N) * rs + c];
+      xr[m] = v.x;
+      xi[m] = v.y;
     }
-  }
-  __syncthreads();
-  {
-    const int col = threadIdx.x >> 5;
-    warp_fft_line<R, L2N>(re + col * LD, im + col * LD, tw);
-  }
-  __syncthreads();
-#pragma unroll 4
-  for (int it = 0; it < L::ITER; it++) {
-    const int w = threadIdx.x + it * L::THREADS;
-    if (N >= 32 || w < COLS * N) {
-      const int kz = w / COLS, col = w % COLS;
-      if (col < nc) sp[kz * rs + col] = Cplx<R>::make(re[col * LD + fpad(kz)], im[col * LD + fpad(kz)]);
-    }
-  }
+  };
+  auto last = [&](int c, int base, auto gc, auto hc, const R *xr, const R *xi) {
+    constexpr int G = decltype(gc)::value, H = decltype(hc)::value;
+    if (c >= nc) return;
+#pragma unroll
+    for (int m = 0; m < G; m++) sp[(base + m * H) * rs + c] = Cplx<R>::make(xr[m], xi[m]);
+  };
+  fft_lines<R, L2N, COLS>(re, im, tw, first, last);
 }
 
 // complex Neumann Thomas along x per line (ky, kz): tdm_c = -pl - pu + lambda,
 // lambda = evy[ky] + evz[kz], first / last diagonal + pl[0] / + pu[nx-1], then
-// gtsv component-wise (src/tdm.c:17-50; dft.c:364-395 in 2D).  Warp 0 runs
-// the recurrences with one line per lane; the other warps move the tiles.
-// FP64 arithmetic; the spectrum and the scratch of v are R.
-constexpr int XL = kXsLines, XC = kXsChunk;
+// gtsv component-wise (src/tdm.c:17-50; dft.c:364-395 in 2D).  Every thread
+// sweeps one line of the block's LPB, the recurrence carried in registers in
+// FP64 across chunks of XC points that the block stages in shared memory by
+// cp.async (a warp's copies are runs of XC consecutive points of two lines):
+// forward (values back into S, v into scratch), then back substitution in
+// reverse chunk order.  The spectrum and the scratch of v are R.
+constexpr int XC = 16;
+template <class R, int LPB>
+struct XShape {
+  using C2 = typename Cplx<R>::T;
+  static constexpr size_t SQ = sizeof(C2) * LPB * (XC + 1);
+  static constexpr size_t SMEM = SQ + sizeof(R) * LPB * (XC + 1) + 2 * sizeof(double) * XC;
+};
 
-template <class R>
-__global__ void __launch_bounds__(256) k3_pois_x(R *__restrict__ spec, R *__restrict__ scratch,
+template <class R, int LPB>
+__global__ void __launch_bounds__(LPB) k3_pois_x(R *__restrict__ spec, R *__restrict__ scratch,
                                                  const double *__restrict__ pl, const double *__restrict__ pu,
                                                  const double *__restrict__ evy, const double *__restrict__ evz,
                                                  int pin_gauge, Grid3 g) {
-  __shared__ double sre[XL][XC + 1], sim[XL][XC + 1], sv[XL][XC + 1];
-  __shared__ double spl[XC], spu[XC];
   using C2 = typename Cplx<R>::T;
+  using S = XShape<R, LPB>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C2(*sq)[XC + 1] = reinterpret_cast<C2(*)[XC + 1]>(smraw);
+  R(*sv)[XC + 1] = reinterpret_cast<R(*)[XC + 1]>(smraw + S::SQ);
+  double *spl = reinterpret_cast<double *>(smraw + S::SQ + sizeof(R) * LPB * (XC + 1));
+  double *spu = spl + XC;
   C2 *sp = reinterpret_cast<C2 *>(spec);
   const int nx = g.nx, nky = g.ny / 2 + 1;
   const long nlines = (long)nky * g.nz;
-  const long l0 = (long)blockIdx.x * XL;
-  const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+  const long l0 = (long)blockIdx.x * LPB;
+  const int t = threadIdx.x;
+  const bool live = l0 + t < nlines;
   const int nchunks = (nx + XC - 1) / XC;
-  const bool sweeper = (0 == ty) && (l0 + tx < nlines);
   double lam = 0.;
   bool pinned = false;
-  if (sweeper) {
-    const long l = l0 + tx;
+  if (live) {
+    const long l = l0 + t;
     lam = ldg(evy + l % nky) + ldg(evz + l / nky);
     pinned = pin_gauge && (0 == l);
   }
+  // chunk copies: element e = t + LPB r is point e % XC of line e / XC
+  auto copy_in = [&](int p0, bool with_v) {
+    const int pw = min(XC, nx - p0);
+#pragma unroll 4
+    for (int r = 0; r < XC; r++) {
+      const int e = t + LPB * r, ll = e / XC, q = e % XC;
+      const long l = l0 + ll;
+      if (l < nlines && q < pw) {
+        const size_t o = (size_t)l * nx + p0 + q;
+        __pipeline_memcpy_async(&sq[ll][q], &sp[o], sizeof(C2));
+        if (with_v) __pipeline_memcpy_async(&sv[ll][q], &scratch[o], sizeof(R));
+      }
+    }
+    __pipeline_commit();
+  };
+  auto copy_out = [&](int p0, bool with_v) {
+    const int pw = min(XC, nx - p0);
+#pragma unroll 4
+    for (int r = 0; r < XC; r++) {
+      const int e = t + LPB * r, ll = e / XC, q = e % XC;
+      const long l = l0 + ll;
+      if (l < nlines && q < pw) {
+        const size_t o = (size_t)l * nx + p0 + q;
+        sp[o] = sq[ll][q];
+        if (with_v) scratch[o] = sv[ll][q];
+      }
+    }
+  };
   double vprev = 0., qr = 0., qi = 0.;
   // ---------------------------------------------------------- forward
   for (int c = 0; c < nchunks; c++) {
     const int p0 = c * XC;
-    if (tid < XC) {
-      spl[tid] = (p0 + tid < nx) ? ldg(pl + p0 + tid) : 0.;
-      spu[tid] = (p0 + tid < nx) ? ldg(pu + p0 + tid) : 0.;
+    if (t < XC) {
+      spl[t] = (p0 + t < nx) ? ldg(pl + p0 + t) : 0.;
+      spu[t] = (p0 + t < nx) ? ldg(pu + p0 + t) : 0.;
     }
-    for (int m = 0; m < XL / 8; m++) {
-      const int ll = ty + 8 * m;
-      const long l = l0 + ll;
-      const int p = p0 + tx;
-      if (l < nlines && p < nx) {
-        const C2 v = sp[(size_t)l * nx + p];
-        sre[ll][tx] = v.x;
-        sim[ll][tx] = v.y;
-      }
-    }
+    copy_in(p0, false);
+    __pipeline_wait_prior(0);
     __syncthreads();
-    if (sweeper) {
+    if (live) {
       const int smax = min(XC, nx - p0);
       for (int s = 0; s < smax; s++) {
         const int i = p0 + s;
@@ -308,7 +417,8 @@ __global__ void __launch_bounds__(256) k3_pois_x(R *__restrict__ spec, R *__rest
         double c = -l - u + lam;
         if (0 == i) c += l;
         if (nx - 1 == i) c += u;
-        const double xr = sre[tx][s], xi = sim[tx][s];
+        const C2 x = sq[t][s];
+        const double xr = x.x, xi = x.y;
         if (0 == i) {
           vprev = u / c;
           qr = xr / c;
@@ -328,21 +438,12 @@ __global__ void __launch_bounds__(256) k3_pois_x(R *__restrict__ spec, R *__rest
             qi = 0.;
           }
         }
-        sre[tx][s] = qr;
-        sim[tx][s] = qi;
-        sv[tx][s] = vprev;
+        sq[t][s] = Cplx<R>::make(R(qr), R(qi));
+        sv[t][s] = R(vprev);
       }
     }
     __syncthreads();
-    for (int m = 0; m < XL / 8; m++) {
-      const int ll = ty + 8 * m;
-      const long l = l0 + ll;
-      const int p = p0 + tx;
-      if (l < nlines && p < nx) {
-        sp[(size_t)l * nx + p] = Cplx<R>::make(R(sre[ll][tx]), R(sim[ll][tx]));
-        scratch[(size_t)l * nx + p] = R(sv[ll][tx]);
-      }
-    }
+    copy_out(p0, true);
     __syncthreads();
   }
   // ---------------------------------------------------------- backward
@@ -351,41 +452,27 @@ __global__ void __launch_bounds__(256) k3_pois_x(R *__restrict__ spec, R *__rest
   double nr = 0., ni = 0.;
   for (int c = nchunks - 1; c >= 0; c--) {
     const int p0 = c * XC;
-    for (int m = 0; m < XL / 8; m++) {
-      const int ll = ty + 8 * m;
-      const long l = l0 + ll;
-      const int p = p0 + tx;
-      if (l < nlines && p < nx) {
-        const C2 v = sp[(size_t)l * nx + p];
-        sre[ll][tx] = v.x;
-        sim[ll][tx] = v.y;
-        sv[ll][tx] = scratch[(size_t)l * nx + p];
-      }
-    }
+    copy_in(p0, true);
+    __pipeline_wait_prior(0);
     __syncthreads();
-    if (sweeper) {
+    if (live) {
       const int smax = min(XC, nx - p0);
       for (int s = smax - 1; s >= 0; s--) {
         const int i = p0 + s;
+        const C2 x = sq[t][s];
         if (nx - 1 == i) {
-          nr = sre[tx][s];
-          ni = sim[tx][s];
+          nr = x.x;
+          ni = x.y;
         } else {
-          const double v = sv[tx][s];
-          nr = sre[tx][s] - v * nr;
-          ni = sim[tx][s] - v * ni;
-          sre[tx][s] = nr;
-          sim[tx][s] = ni;
+          const double v = sv[t][s];
+          nr = x.x - v * nr;
+          ni = x.y - v * ni;
+          sq[t][s] = Cplx<R>::make(R(nr), R(ni));
         }
       }
     }
     __syncthreads();
-    for (int m = 0; m < XL / 8; m++) {
-      const int ll = ty + 8 * m;
-      const long l = l0 + ll;
-      const int p = p0 + tx;
-      if (l < nlines && p < nx) sp[(size_t)l * nx + p] = Cplx<R>::make(R(sre[ll][tx]), R(sim[ll][tx]));
-    }
+    copy_out(p0, false);
     __syncthreads();
   }
 }
@@ -395,67 +482,65 @@ __global__ void __launch_bounds__(256) k3_pois_x(R *__restrict__ spec, R *__rest
 // the halo images; the Neumann walls take the new neighbour value and hand
 // their old value to the halo images
 template <int L2N, class R, bool ACCUM>
-__global__ void __launch_bounds__(Line<R, L2N>::THREADS, Line<R, L2N>::MINB)
+__global__ void __launch_bounds__(kLineThreads, Line<R, L2N>::MINB)
     k3_pois_inv_y(const R *__restrict__ spec, double *__restrict__ psi, const R *__restrict__ tw, Grid3 g) {
   using L = Line<R, L2N>;
-  constexpr int N = L::N, LD = L::LD, COLS = L::COLS, NKY = N / 2 + 1;
+  using C2 = typename Cplx<R>::T;
+  constexpr int N = L::N, COLS = L::COLS, NKY = N / 2 + 1;
   extern __shared__ unsigned char smraw[];
   R *re = reinterpret_cast<R *>(smraw);
-  R *im = re + COLS * LD;
+  R *im = re + COLS * L::LD;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int i0 = 1 + blockIdx.x * COLS;
   const int k = 1 + blockIdx.y;
   const int nc = min(COLS, nx - i0 + 1);
-  using C2 = typename Cplx<R>::T;
   const C2 *sp = reinterpret_cast<const C2 *>(spec) + (size_t)(k - 1) * NKY * nx + (i0 - 1);
-#pragma unroll 4
-  for (int it = 0; it < L::ITER; it++) {
-    const int w = threadIdx.x + it * L::THREADS;
-    if (N >= 32 || w < COLS * N) {
-      const int q = w / COLS, col = w % COLS;
-      const int m = bitrev(q, L2N);
+  auto first = [&](int c, int base, auto gc, auto hc, R *xr, R *xi) {
+    constexpr int G = decltype(gc)::value, H = decltype(hc)::value;
+#pragma unroll
+    for (int q = 0; q < G; q++) {
+      const int m = bitrev(base + q * H, L2N);
       R r = R(0.), x = R(0.);
-      if (col < nc) {
+      if (c < nc) {
         // X_m for m <= N/2, conj(X_{N-m}) above; Im of X_0 and X_{N/2} ignored
         const int row = (2 * m <= N) ? m : N - m;
-        const C2 v = __ldg(&sp[(size_t)row * nx + col]);
+        const C2 v = __ldg(&sp[(size_t)row * nx + c]);
         r = v.x;
         x = (0 == m || 2 * m == N) ? R(0.) : ((2 * m < N) ? v.y : -v.y);
       }
-      re[col * LD + fpad(q)] = r;
-      im[col * LD + fpad(q)] = x;
+      xr[q] = r;
+      xi[q] = x;
     }
-  }
-  __syncthreads();
-  {
-    const int col = threadIdx.x >> 5;
-    warp_fft_line<R, L2N>(re + col * LD, im + col * LD, tw);
-  }
-  __syncthreads();
-#pragma unroll 4
-  for (int it = 0; it < L::ITER; it++) {
-    const int w = threadIdx.x + it * L::THREADS;
-    if (N >= 32 || w < COLS * N) {
-      const int r = w / COLS, col = w % COLS;
-      if (col < nc) {
-        const int i = i0 + col, j = r + 1;
-        double y = (double)re[col * LD + fpad(r)];
-        if (ACCUM) y += psi[ix_cc(g, i, j, k)];
-        for_images(j, k, ny, nz, true, [&](int jj, int kk) { psi[ix_cc(g, i, jj, kk)] = y; });
-      }
+  };
+  // psi of rows j = p + 1 with their halo images
+  auto last = [&](int c, int base, auto gc, auto hc, const R *xr, const R *) {
+    constexpr int G = decltype(gc)::value, H = decltype(hc)::value;
+    if (c >= nc) return;
+    const int i = i0 + c;
+    double y[G];
+#pragma unroll
+    for (int q = 0; q < G; q++) {
+      y[q] = (double)xr[q];
+      if (ACCUM) y[q] += psi[ix_cc(g, i, base + q * H + 1, k)];
     }
-  }
-  // (ACCUM: the walls below read the accumulated neighbour values)
-  if (ACCUM) __syncthreads();
-  // Neumann walls of the interior rows of this plane
+#pragma unroll
+    for (int q = 0; q < G; q++) {
+      const double v = y[q];
+      for_images(base + q * H + 1, k, ny, nz, true, [&](int jj, int kk) { psi[ix_cc(g, i, jj, kk)] = v; });
+    }
+  };
+  fft_lines<R, L2N, COLS>(re, im, tw, first, last);
+  // Neumann walls of the interior rows of this plane (the blocks at either end
+  // of x): the wall cell takes its neighbour's new value, read back after the
+  // barrier, and hands its old value to its halo images
   const bool has_left = (1 == i0), has_right = (i0 + nc - 1 == nx);
   if (!has_left && !has_right) return;
-  for (int w = threadIdx.x; w < 2 * N; w += L::THREADS) {
+  __syncthreads();
+  for (int w = threadIdx.x; w < 2 * N; w += kLineThreads) {
     const int side = w / N, j = 1 + (w - side * N);
     if ((0 == side && !has_left) || (1 == side && !has_right)) continue;
     const int iw = side ? nx + 1 : 0;
-    const int col = side ? nc - 1 : 0;
-    const double nv = ACCUM ? psi[ix_cc(g, i0 + col, j, k)] : (double)re[col * LD + fpad(j - 1)];
+    const double nv = psi[ix_cc(g, side ? nx : 1, j, k)];
     const double old = psi[ix_cc(g, iw, j, k)];
     psi[ix_cc(g, iw, j, k)] = nv;
     for_images(j, k, ny, nz, false, [&](int jj, int kk) { psi[ix_cc(g, iw, jj, kk)] = old; });
@@ -503,10 +588,13 @@ cudaError_t pois_prepare(int log2ny, int log2nz) {
     return line_attrs(k3_pois_inv_y<L2, R, true>, sm);
   });
   if (cudaSuccess != e) return e;
-  return by_l2n(log2nz, [&](auto c) {
+  e = by_l2n(log2nz, [&](auto c) {
     constexpr int L2 = decltype(c)::value;
     return line_attrs(k3_pois_z<L2, R>, Line<R, L2>::SMEM);
   });
+  if (cudaSuccess != e) return e;
+  if (cudaSuccess != (e = line_attrs(k3_pois_x<R, 64>, (int)XShape<R, 64>::SMEM))) return e;
+  return line_attrs(k3_pois_x<R, 128>, (int)XShape<R, 128>::SMEM);
 }
 
 template <class R>
@@ -518,9 +606,9 @@ cudaError_t pois_fwd_y(bool resid, cudaStream_t st, const double *ux, const doub
     using L = Line<R, L2>;
     dim3 gr((g.nx + L::COLS - 1) / L::COLS, g.nz);
     if (resid) {
-      k3_pois_fwd_y<L2, R, true><<<gr, L::THREADS, L::SMEM, st>>>(ux, uy, uz, psi, pl, pu, spec, tw, dtp, gam, g);
+      k3_pois_fwd_y<L2, R, true><<<gr, kLineThreads, L::SMEM, st>>>(ux, uy, uz, psi, pl, pu, spec, tw, dtp, gam, g);
     } else {
-      k3_pois_fwd_y<L2, R, false><<<gr, L::THREADS, L::SMEM, st>>>(ux, uy, uz, psi, pl, pu, spec, tw, dtp, gam, g);
+      k3_pois_fwd_y<L2, R, false><<<gr, kLineThreads, L::SMEM, st>>>(ux, uy, uz, psi, pl, pu, spec, tw, dtp, gam, g);
     }
     return cudaGetLastError();
   });
@@ -532,16 +620,25 @@ cudaError_t pois_z(cudaStream_t st, R *spec, const R *tw, int log2n, Grid3 g) {
     constexpr int L2 = decltype(c)::value;
     using L = Line<R, L2>;
     dim3 gr((g.nx + L::COLS - 1) / L::COLS, g.ny / 2 + 1);
-    k3_pois_z<L2, R><<<gr, L::THREADS, L::SMEM, st>>>(spec, tw, g);
+    k3_pois_z<L2, R><<<gr, kLineThreads, L::SMEM, st>>>(spec, tw, g);
     return cudaGetLastError();
   });
 }
+
+// lines per block of the x solve: 128, or 64 when 128 would leave SMs idle
+inline bool pois_x_narrow(long nlines) { return nlines < 148L * 4 * 128; }
 
 template <class R>
 cudaError_t pois_x(cudaStream_t st, R *spec, R *scratch, const double *pl, const double *pu, const double *evy,
                    const double *evz, int pin_gauge, Grid3 g) {
   const long nlines = (long)(g.ny / 2 + 1) * g.nz;
-  k3_pois_x<R><<<(unsigned)((nlines + XL - 1) / XL), 256, 0, st>>>(spec, scratch, pl, pu, evy, evz, pin_gauge, g);
+  if (pois_x_narrow(nlines)) {
+    k3_pois_x<R, 64><<<(unsigned)((nlines + 63) / 64), 64, XShape<R, 64>::SMEM, st>>>(spec, scratch, pl, pu, evy,
+                                                                                      evz, pin_gauge, g);
+  } else {
+    k3_pois_x<R, 128><<<(unsigned)((nlines + 127) / 128), 128, XShape<R, 128>::SMEM, st>>>(spec, scratch, pl, pu,
+                                                                                          evy, evz, pin_gauge, g);
+  }
   return cudaGetLastError();
 }
 
@@ -552,9 +649,9 @@ cudaError_t pois_inv_y(bool accum, cudaStream_t st, const R *spec, double *psi, 
     using L = Line<R, L2>;
     dim3 gr((g.nx + L::COLS - 1) / L::COLS, g.nz);
     if (accum) {
-      k3_pois_inv_y<L2, R, true><<<gr, L::THREADS, L::SMEM, st>>>(spec, psi, tw, g);
+      k3_pois_inv_y<L2, R, true><<<gr, kLineThreads, L::SMEM, st>>>(spec, psi, tw, g);
     } else {
-      k3_pois_inv_y<L2, R, false><<<gr, L::THREADS, L::SMEM, st>>>(spec, psi, tw, g);
+      k3_pois_inv_y<L2, R, false><<<gr, kLineThreads, L::SMEM, st>>>(spec, psi, tw, g);
     }
     return cudaGetLastError();
   });

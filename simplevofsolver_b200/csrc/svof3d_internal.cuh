@@ -182,8 +182,6 @@ __global__ void k3_diag(const double *__restrict__ ux, const double *__restrict_
 // launch constants shared by the kernels and the host
 constexpr int kPredLines = 32;  // lines per predictor block
 constexpr int kPredChunk = 32;  // x positions per chunk
-constexpr int kXsLines = 32;    // lines per Poisson x-solve block
-constexpr int kXsChunk = 32;
 constexpr int kProjectPlanes = 4;  // z planes per thread of k3_project
 
 }  // namespace svof3
