@@ -12,9 +12,13 @@
 
 namespace svof3 {
 
-// one thread per interior cell; the threads at i = 1 and i = nx also own the
-// wall cells of their row
-__global__ void __launch_bounds__(256) k3_project(double *__restrict__ ux, double *__restrict__ uy,
+// one thread per interior (i, j) and kProjectPlanes planes k; the threads at
+// i = 1 and i = nx also own the wall cells of their rows.  The planes go in
+// pairs, every load of a pair issued before its first store; psi at k - 1 is
+// the previous plane's centre value.  A wall cell's old value is read only
+// where the cell has halo images to take it (rows j = 1, ny or planes
+// k = 1, nz).
+__global__ void __launch_bounds__(256, 3) k3_project(double *__restrict__ ux, double *__restrict__ uy,
                                                   double *__restrict__ uz, double *__restrict__ p,
                                                   const double *__restrict__ psi, const double *__restrict__ dtp,
                                                   double gam, double m_dif, double uy_xm, double uy_xp,
@@ -23,67 +27,95 @@ __global__ void __launch_bounds__(256) k3_project(double *__restrict__ ux, doubl
   const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
   if (i > nx || j > ny) return;
+  const int k0 = 1 + blockIdx.z * kProjectPlanes;
+  if (k0 > nz) return;
   const double dt = ldg(dtp);
   // quotients the restatement evaluates per cell, once per thread (same values)
   const double pv = gam * dt, pp = 0.5 * gam * dt * m_dif;
-  const double cvx = pv / ldg(g.dxc + i - 1), cvy = pv / g.dy, cvz = pv / g.dz;
+  const double dxc_m = ldg(g.dxc + i - 1);
+  const double cvx = pv / dxc_m, cvy = pv / g.dy, cvz = pv / g.dz;
   const double cpx = pp / ldg(g.dxf + i - 1);
-#pragma unroll 2
-  for (int kz = 0; kz < kProjectPlanes; kz++) {
-  const int k = 1 + blockIdx.z * kProjectPlanes + kz;
-  if (k > nz) break;
-  const double psc = ldg(psi + ix_cc(g, i, j, k));
+  const double dxc_p = (do_p) ? ldg(g.dxc + i) : 1.;
   const bool wall = (1 == i || nx == i);
-  if (do_vel) {
-    const double pxm = ldg(psi + ix_cc(g, i - 1, j, k));
-    const double pym = ldg(psi + ix_cc(g, i, j - 1, k));
-    const double pzm = ldg(psi + ix_cc(g, i, j, k - 1));
-    const long iu = ix_ux(g, i, j, k), ic = ix_cc(g, i, j, k);
-    const double ux0 = ux[iu], uy0 = uy[ic], uz0 = uz[ic];
-    // ux
-    if (i >= 2) {
-      double v = ux0;
-      v -= cvx * (+psc - pxm);
-      for_images(j, k, ny, nz, true, [&](int jj, int kk) { ux[ix_ux(g, i, jj, kk)] = v; });
+  const int iwu = (1 == i) ? 1 : nx + 1;  // the wall face of ux
+  const int iw = (1 == i) ? 0 : nx + 1;   // the wall cell of the others
+  double pzm_next = do_vel ? ldg(psi + ix_cc(g, i, j, k0 - 1)) : 0.;
+  constexpr int B = 2;
+#pragma unroll
+  for (int kb = 0; kb < kProjectPlanes; kb += B) {
+    double psc[B], pxm[B], pym[B], pxp[B], u0[B], v0[B], w0[B], p0[B];
+    // ---- loads
+#pragma unroll
+    for (int h = 0; h < B; h++) {
+      const int k = k0 + kb + h;
+      if (k > nz) break;
+      const long ic = ix_cc(g, i, j, k);
+      psc[h] = ldg(psi + ic);
+      pxm[h] = ldg(psi + ix_cc(g, i - 1, j, k));
+      if (do_vel) {
+        pym[h] = ldg(psi + ix_cc(g, i, j - 1, k));
+        u0[h] = ux[ix_ux(g, i, j, k)];
+        v0[h] = uy[ic];
+        w0[h] = uz[ic];
+      }
+      if (do_p) {
+        pxp[h] = ldg(psi + ix_cc(g, i + 1, j, k));
+        p0[h] = p[ic];
+      }
     }
-    double vy = uy0;
-    vy -= cvy * (+psc - pym);
-    for_images(j, k, ny, nz, true, [&](int jj, int kk) { uy[ix_cc(g, i, jj, kk)] = vy; });
-    double vz = uz0;
-    vz -= cvz * (+psc - pzm);
-    for_images(j, k, ny, nz, true, [&](int jj, int kk) { uz[ix_cc(g, i, jj, kk)] = vz; });
-    if (wall) {
-      const int iwu = (1 == i) ? 1 : nx + 1;
-      const double old = ux[ix_ux(g, iwu, j, k)];
-      ux[ix_ux(g, iwu, j, k)] = 0.;
-      for_images(j, k, ny, nz, false, [&](int jj, int kk) { ux[ix_ux(g, iwu, jj, kk)] = old; });
-      const int iw = (1 == i) ? 0 : nx + 1;
-      const long o = ix_cc(g, iw, j, k);
-      const double oy = uy[o], oz = uz[o];
-      uy[o] = (1 == i) ? uy_xm : uy_xp;
-      uz[o] = (1 == i) ? uz_xm : uz_xp;
-      for_images(j, k, ny, nz, false, [&](int jj, int kk) {
-        uy[ix_cc(g, iw, jj, kk)] = oy;
-        uz[ix_cc(g, iw, jj, kk)] = oz;
-      });
+    // ---- updates
+#pragma unroll
+    for (int h = 0; h < B; h++) {
+      const int k = k0 + kb + h;
+      if (k > nz) break;
+      const double pzm = pzm_next;
+      pzm_next = psc[h];
+      if (do_vel) {
+        if (i >= 2) {
+          double v = u0[h];
+          v -= cvx * (+psc[h] - pxm[h]);
+          for_images(j, k, ny, nz, true, [&](int jj, int kk) { ux[ix_ux(g, i, jj, kk)] = v; });
+        }
+        double vy = v0[h];
+        vy -= cvy * (+psc[h] - pym[h]);
+        for_images(j, k, ny, nz, true, [&](int jj, int kk) { uy[ix_cc(g, i, jj, kk)] = vy; });
+        double vz = w0[h];
+        vz -= cvz * (+psc[h] - pzm);
+        for_images(j, k, ny, nz, true, [&](int jj, int kk) { uz[ix_cc(g, i, jj, kk)] = vz; });
+        if (wall) {
+          const bool img = (1 == j || ny == j || 1 == k || nz == k);
+          const long o = ix_cc(g, iw, j, k);
+          double old = 0., oy = 0., oz = 0.;
+          if (img) {
+            old = ux[ix_ux(g, iwu, j, k)];
+            oy = uy[o];
+            oz = uz[o];
+          }
+          ux[ix_ux(g, iwu, j, k)] = 0.;
+          for_images(j, k, ny, nz, false, [&](int jj, int kk) { ux[ix_ux(g, iwu, jj, kk)] = old; });
+          uy[o] = (1 == i) ? uy_xm : uy_xp;
+          uz[o] = (1 == i) ? uz_xm : uz_xp;
+          for_images(j, k, ny, nz, false, [&](int jj, int kk) {
+            uy[ix_cc(g, iw, jj, kk)] = oy;
+            uz[ix_cc(g, iw, jj, kk)] = oz;
+          });
+        }
+      }
+      if (do_p) {
+        double v = p0[h];
+        v += psc[h];
+        const double dm = (-pxm[h] + psc[h]) / dxc_m;
+        const double dp = (-psc[h] + pxp[h]) / dxc_p;
+        v -= cpx * (-dm + dp);
+        for_images(j, k, ny, nz, true, [&](int jj, int kk) { p[ix_cc(g, i, jj, kk)] = v; });
+        if (wall) {
+          const bool img = (1 == j || ny == j || 1 == k || nz == k);
+          const double old = img ? p[ix_cc(g, iw, j, k)] : 0.;
+          p[ix_cc(g, iw, j, k)] = v;
+          for_images(j, k, ny, nz, false, [&](int jj, int kk) { p[ix_cc(g, iw, jj, kk)] = old; });
+        }
+      }
     }
-  }
-  if (do_p) {
-    const double pxm = ldg(psi + ix_cc(g, i - 1, j, k));
-    const double pxp = ldg(psi + ix_cc(g, i + 1, j, k));
-    double v = p[ix_cc(g, i, j, k)];
-    v += psc;
-    const double dm = (-pxm + psc) / ldg(g.dxc + i - 1);
-    const double dp = (-psc + pxp) / ldg(g.dxc + i);
-    v -= cpx * (-dm + dp);
-    for_images(j, k, ny, nz, true, [&](int jj, int kk) { p[ix_cc(g, i, jj, kk)] = v; });
-    if (wall) {
-      const int iw = (1 == i) ? 0 : nx + 1;
-      const double old = p[ix_cc(g, iw, j, k)];
-      p[ix_cc(g, iw, j, k)] = v;
-      for_images(j, k, ny, nz, false, [&](int jj, int kk) { p[ix_cc(g, iw, jj, kk)] = old; });
-    }
-  }
   }
 }
 
@@ -96,34 +128,49 @@ __device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v)
   return v;
 }
 
-// grid-stride over the ux faces i in [2, nx], the uy and the uz faces of the
-// interior cells.  All candidates are positive, so the minimum of their IEEE
-// bit patterns as unsigned integers is the bit pattern of the minimum.
-__global__ void k3_cfl(const double *__restrict__ ux, const double *__restrict__ uy, const double *__restrict__ uz,
-                       unsigned long long *__restrict__ minbits, Grid3 g) {
-  const int nx = g.nx, ny = g.ny;
+// one thread per interior (i, j) and kCflPlanes planes k: the ux face i in
+// [2, nx], the uy and the uz faces of each cell.  All candidates are
+// positive, so the minimum of their IEEE bit patterns as unsigned integers is
+// the bit pattern of the minimum (NaN candidates, whose patterns lie above
+// that of +inf, never win, as with fmin).
+__global__ void __launch_bounds__(256) k3_cfl(const double *__restrict__ ux, const double *__restrict__ uy,
+                                              const double *__restrict__ uz, unsigned long long *__restrict__ minbits,
+                                              Grid3 g) {
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k0 = 1 + blockIdx.z * kCflPlanes;
   const double small = 1.e-8;
   unsigned long long best = 0x7ff0000000000000ull;
-  const long ncell = (long)nx * ny * g.nz;
-  const long stride = (long)gridDim.x * blockDim.x;
-  for (long w = (long)blockIdx.x * blockDim.x + threadIdx.x; w < ncell; w += stride) {
-    const int i = 1 + (int)(w % nx);
-    const long r = w / nx;
-    const int j = 1 + (int)(r % ny), k = 1 + (int)(r / ny);
-    double cand = g.dy / (fabs(uy[ix_cc(g, i, j, k)]) + small);
-    const double cz = g.dz / (fabs(uz[ix_cc(g, i, j, k)]) + small);
-    cand = fmin(cand, cz);
-    if (i >= 2) cand = fmin(cand, g.dxc[i - 1] / (fabs(ux[ix_ux(g, i, j, k)]) + small));
-    const unsigned long long b = (unsigned long long)__double_as_longlong(cand);
-    best = b < best ? b : best;
+  if (i <= nx && j <= ny) {
+    const double dxc = (i >= 2) ? ldg(g.dxc + i - 1) : 0.;
+    double vy[kCflPlanes], vz[kCflPlanes], vx[kCflPlanes];
+#pragma unroll
+    for (int h = 0; h < kCflPlanes; h++) {
+      const int k = min(k0 + h, nz);
+      vy[h] = ldg(uy + ix_cc(g, i, j, k));
+      vz[h] = ldg(uz + ix_cc(g, i, j, k));
+      vx[h] = (i >= 2) ? ldg(ux + ix_ux(g, i, j, k)) : 0.;
+    }
+#pragma unroll
+    for (int h = 0; h < kCflPlanes; h++) {
+      if (k0 + h > nz) break;
+      double cand = g.dy / (fabs(vy[h]) + small);
+      const double cz = g.dz / (fabs(vz[h]) + small);
+      cand = fmin(cand, cz);
+      if (i >= 2) cand = fmin(cand, dxc / (fabs(vx[h]) + small));
+      const unsigned long long b = (unsigned long long)__double_as_longlong(cand);
+      best = b < best ? b : best;
+    }
   }
   best = warp_min_u64(best);
-  __shared__ unsigned long long sbest[32];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __shared__ unsigned long long sbest[8];
+  const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+  const int lane = tid & 31, warp = tid >> 5;
   if (0 == lane) sbest[warp] = best;
   __syncthreads();
   if (0 == warp) {
-    best = lane < (int)(blockDim.x >> 5) ? sbest[lane] : 0x7ff0000000000000ull;
+    best = lane < 8 ? sbest[lane] : 0x7ff0000000000000ull;
     best = warp_min_u64(best);
     if (0 == lane) atomicMin(minbits, best);
   }

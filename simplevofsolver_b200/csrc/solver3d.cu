@@ -150,9 +150,8 @@ int launch_halo_bc(svof3d_solver *s, double *a, int field) {
 }
 
 int launch_dt(svof3d_solver *s) {
-  const long nc = (long)s->nx * s->ny * s->nz;
-  const int blocks = (int)std::min<long>((nc + 255) / 256, 148L * 8);
-  k3_cfl<<<blocks, 256, 0, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->uz[s->cur_u].p, s->d_minbits,
+  const dim3 cb(32, 8), cg((s->nx + 31) / 32, (s->ny + 7) / 8, (s->nz + kCflPlanes - 1) / kCflPlanes);
+  k3_cfl<<<cg, cb, 0, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->uz[s->cur_u].p, s->d_minbits,
                                         s->grid());
   CK_LAUNCH();
   k3_dt_final<<<1, 1, 0, s->stream>>>(s->d_minbits, s->d_dt, s->prm.coef_dt_adv, s->lims[0], s->lims[1],

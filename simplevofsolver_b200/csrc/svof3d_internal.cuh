@@ -183,5 +183,6 @@ __global__ void k3_diag(const double *__restrict__ ux, const double *__restrict_
 constexpr int kPredLines = 32;  // lines per predictor block
 constexpr int kPredChunk = 32;  // x positions per chunk
 constexpr int kProjectPlanes = 4;  // z planes per thread of k3_project
+constexpr int kCflPlanes = 8;      // z planes per thread of k3_cfl (blocks of 32 x 8)
 
 }  // namespace svof3
