@@ -184,14 +184,26 @@ __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ 
   const int tx = tid % G3X, ty = tid / G3X;
   const R eps = R(kDblEpsilon);
   const R rdy = R(1.) / R(g.dy), rdz = R(1.) / R(g.dz);
-  // cp.async: the next plane arrives while the current one is processed
+  // cp.async: the next plane arrives while the current one is processed; the
+  // window elements a thread copies are the same on every plane, their
+  // in-plane offsets computed once (-1: zero fill, -2: no element)
+  constexpr int NT = G3X * G3Y, NW = ((G3X + 2) * (G3Y + 2) + NT - 1) / NT;
+  const long vplane = (long)(nx + 2) * (ny + 4);
+  int woff[NW];
+#pragma unroll
+  for (int q = 0; q < NW; q++) {
+    const int t = tid + NT * q, li = t % (G3X + 2), lj = t / (G3X + 2);
+    const int i = i0 - 1 + li, j = j0 - 1 + lj;
+    woff[q] = (t >= (G3X + 2) * (G3Y + 2)) ? -2 : ((i <= nx + 1 && j <= ny + 2) ? i + (nx + 2) * (j + 1) : -1);
+  }
   auto load_plane = [&](int k) {
     const int buf = (k - k0 + 1) % 3;
-    for (int t = tid; t < (G3X + 2) * (G3Y + 2); t += G3X * G3Y) {
-      const int li = t % (G3X + 2), lj = t / (G3X + 2);
-      const int i = i0 - 1 + li, j = j0 - 1 + lj;
-      if (i <= nx + 1 && j <= ny + 2) __pipeline_memcpy_async(&sv[buf][lj][li], vof + ix_vof(g, i, j, k), 8);
-      else sv[buf][lj][li] = 0.;
+    const double *vp = vof + vplane * (k + 1);
+    double *d = &sv[buf][0][0];
+#pragma unroll
+    for (int q = 0; q < NW; q++) {
+      if (woff[q] >= 0) __pipeline_memcpy_async(d + tid + NT * q, vp + woff[q], 8);
+      else if (-1 == woff[q]) d[tid + NT * q] = 0.;
     }
     __pipeline_commit();
   };
@@ -392,7 +404,7 @@ constexpr size_t kAdvectSmem =
     sizeof(double) * (kVofRing + kUxRing + kUyRing + kUzRing + kSbRing + AY * (AX + 1) + (AY + 1) * AX);
 
 template <class R>
-__global__ void __launch_bounds__(AX * AY) k3_vof_advect(const double *__restrict__ vof, double *__restrict__ vof_new,
+__global__ void __launch_bounds__(AX * AY, 4) k3_vof_advect(const double *__restrict__ vof, double *__restrict__ vof_new,
                                                         const double *__restrict__ ux, const double *__restrict__ uy,
                                                         const double *__restrict__ uz, const R *__restrict__ normal,
                                                         double *__restrict__ src_a, const double *__restrict__ src_b,
@@ -412,38 +424,84 @@ __global__ void __launch_bounds__(AX * AY) k3_vof_advect(const double *__restric
   const int i = i0 + tx, j = j0 + ty;
   const bool mine = (i <= nx && j <= ny);
   const long vw = nx + 2, vrows = ny + 4, uw = nx + 1, crow = ny + 2;
+  const long vplane = vw * vrows, uplane = uw * crow, cplane = vw * crow, splane = (long)nx * ny;
+  const long nplane = 4L * nx * crow;  // normal array, per plane k
   auto cp = [](double *dst, const double *src) { __pipeline_memcpy_async(dst, src, sizeof(double)); };
+  // The copies and faces a thread handles are the same on every plane: their
+  // in-plane offsets are computed once (-1: zero fill, -2: no element).
+  constexpr int NT = AX * AY;
+  constexpr int NV = (AWY * AWX + NT - 1) / NT, NXF = (AY * (AX + 1) + NT - 1) / NT,
+                NYF = ((AY + 1) * AX + NT - 1) / NT;
+  int vsrc[NV], xsrc[NXF], ysrc[NYF];
+#pragma unroll
+  for (int q = 0; q < NV; q++) {
+    const int e = tid + NT * q, r = e / AWX, c = e - r * AWX;
+    const int x = i0 - 1 + c, jj = j0 - 1 + r;
+    vsrc[q] = (e >= AWY * AWX) ? -2 : ((x <= nx + 1 && jj <= ny + 2) ? (int)(x + vw * (jj + 1)) : -1);
+  }
+#pragma unroll
+  for (int q = 0; q < NXF; q++) {
+    const int e = tid + NT * q, r = e / (AX + 1), c = e - r * (AX + 1);
+    const int fi = i0 + c, jj = j0 + r;  // face fi, storage fi - 1
+    xsrc[q] = (e >= AY * (AX + 1)) ? -2 : ((fi <= nx + 1 && jj <= ny) ? (int)((fi - 1) + uw * jj) : -1);
+  }
+#pragma unroll
+  for (int q = 0; q < NYF; q++) {
+    const int e = tid + NT * q, r = e / AX, c = e - r * AX;
+    const int ii = i0 + c, fj = j0 + r;
+    ysrc[q] = (e >= (AY + 1) * AX) ? -2 : ((ii <= nx && fj <= ny + 1) ? (int)(ii + vw * fj) : -1);
+  }
+  const int zsrc = (int)(i + vw * j), bsrc = (i - 1) + nx * (j - 1);
   auto load_plane = [&](int kk) {
     const int sl = kk & (ASLOT - 1);
     // vof window, planes k0 - 1 .. kend + 1
-    for (int e = tid; e < AWY * AWX; e += AX * AY) {
-      const int r = e / AWX, c = e - r * AWX;
-      const int x = i0 - 1 + c, jj = j0 - 1 + r;
-      double *d = vr + (size_t)sl * AWY * AWX + e;
-      if (x <= nx + 1 && jj <= ny + 2) cp(d, vof + x + vw * ((jj + 1) + vrows * (kk + 1)));
-      else *d = 0.;
+    const double *vp = vof + vplane * (kk + 1);
+    double *vd = vr + (size_t)sl * AWY * AWX;
+#pragma unroll
+    for (int q = 0; q < NV; q++) {
+      if (vsrc[q] >= 0) cp(vd + tid + NT * q, vp + vsrc[q]);
+      else if (-1 == vsrc[q]) vd[tid + NT * q] = 0.;
     }
     // z face velocities of planes k0 .. kend (the top face of the last cell)
-    if (kk >= k0 && kk <= kend && mine) cp(zr + (size_t)sl * AY * AX + tid, uz + ix_cc(g, i, j, kk));
+    if (kk >= k0 && kk <= kend && mine) cp(zr + (size_t)sl * AY * AX + tid, uz + cplane * kk + zsrc);
     if (kk >= k0 && kk < kend) {
-      for (int e = tid; e < AY * (AX + 1); e += AX * AY) {
-        const int r = e / (AX + 1), c = e - r * (AX + 1);
-        const int fi = i0 + c, jj = j0 + r;  // face fi, storage fi - 1
-        double *d = xr + (size_t)sl * AY * (AX + 1) + e;
-        if (fi <= nx + 1 && jj <= ny) cp(d, ux + (fi - 1) + uw * (jj + crow * kk));
-        else *d = 0.;
+      const double *up = ux + uplane * kk;
+      double *xd = xr + (size_t)sl * AY * (AX + 1);
+#pragma unroll
+      for (int q = 0; q < NXF; q++) {
+        if (xsrc[q] >= 0) cp(xd + tid + NT * q, up + xsrc[q]);
+        else if (-1 == xsrc[q]) xd[tid + NT * q] = 0.;
       }
-      for (int e = tid; e < (AY + 1) * AX; e += AX * AY) {
-        const int r = e / AX, c = e - r * AX;
-        const int ii = i0 + c, fj = j0 + r;
-        double *d = yr + (size_t)sl * (AY + 1) * AX + e;
-        if (ii <= nx && fj <= ny + 1) cp(d, uy + ii + vw * (fj + crow * kk));
-        else *d = 0.;
+      const double *yp = uy + cplane * kk;
+      double *yd = yr + (size_t)sl * (AY + 1) * AX;
+#pragma unroll
+      for (int q = 0; q < NYF; q++) {
+        if (ysrc[q] >= 0) cp(yd + tid + NT * q, yp + ysrc[q]);
+        else if (-1 == ysrc[q]) yd[tid + NT * q] = 0.;
       }
-      if (use_b && mine) cp(br + (size_t)sl * AY * AX + tid, src_b + ix_src(g, i, j, kk));
+      if (use_b && mine) cp(br + (size_t)sl * AY * AX + tid, src_b + splane * (kk - 1) + bsrc);
     }
     __pipeline_commit();
   };
+  // faces: window offsets of the two cells and in-plane normal offsets
+  int xface[NXF], yface[NYF];  // window offset of the lower cell, -1 outside the domain
+  int xnrm[NXF], ynrm[NYF];
+#pragma unroll
+  for (int q = 0; q < NXF; q++) {
+    const int e = tid + NT * q, r = e / (AX + 1), c = e - r * (AX + 1);
+    const int fi = i0 + c, fj = j0 + r;
+    const bool ok = e < AY * (AX + 1) && fi >= 2 && fi <= nx && fj <= ny;
+    xface[q] = ok ? (r + 1) * AWX + c : -1;
+    xnrm[q] = ok ? 4 * ((fi - 2) + nx * fj) : 0;  // normal of cell fi - 1; cell fi is 4 further
+  }
+#pragma unroll
+  for (int q = 0; q < NYF; q++) {
+    const int e = tid + NT * q, r = e / AX, c = e - r * AX;
+    const int fi = i0 + c, fj = j0 + r;
+    const bool ok = e < (AY + 1) * AX && fi <= nx && fj <= ny + 1;
+    yface[q] = ok ? r * AWX + c + 1 : -1;
+    ynrm[q] = ok ? 4 * ((fi - 1) + nx * (fj - 1)) : 0;  // normal of row fj - 1; row fj is 4 nx further
+  }
   load_plane(k0 - 1);
   load_plane(k0);
   load_plane(k0 + 1);
@@ -462,23 +520,27 @@ __global__ void __launch_bounds__(AX * AY) k3_vof_advect(const double *__restric
   for (int k = k0; k < kend; k++) {
     if (k + 2 <= kend + 1) load_plane(k + 2);
     const int s0 = k & (ASLOT - 1), sp = (k + 1) & (ASLOT - 1);
-    for (int e = tid; e < AY * (AX + 1); e += AX * AY) {
-      const int r = e / (AX + 1), c = e - r * (AX + 1);
-      const int fi = i0 + c, fj = j0 + r;
+    const double *vs = vr + (size_t)s0 * AWY * AWX;
+    const long nk = nplane * k;
+#pragma unroll
+    for (int q = 0; q < NXF; q++) {
+      const int e = tid + NT * q;
+      if (e >= AY * (AX + 1)) break;
       double f = 0.;
-      if (fi >= 2 && fi <= nx && fj <= ny)
-        f = face_flux<R, 0>(xr[((size_t)s0 * AY + r) * (AX + 1) + c], VR(s0, r + 1, c), VR(s0, r + 1, c + 1), normal,
-                            ix_nrm(g, fi - 1, fj, k), ix_nrm(g, fi, fj, k));
-      fx[r * (AX + 1) + c] = f;
+      if (xface[q] >= 0)
+        f = face_flux<R, 0>(xr[(size_t)s0 * AY * (AX + 1) + e], vs[xface[q]], vs[xface[q] + 1], normal,
+                            nk + xnrm[q], nk + xnrm[q] + 4);
+      fx[e] = f;
     }
-    for (int e = tid; e < (AY + 1) * AX; e += AX * AY) {
-      const int r = e / AX, c = e - r * AX;
-      const int fi = i0 + c, fj = j0 + r;
+#pragma unroll
+    for (int q = 0; q < NYF; q++) {
+      const int e = tid + NT * q;
+      if (e >= (AY + 1) * AX) break;
       double f = 0.;
-      if (fi <= nx && fj <= ny + 1)
-        f = face_flux<R, 1>(yr[((size_t)s0 * (AY + 1) + r) * AX + c], VR(s0, r, c + 1), VR(s0, r + 1, c + 1), normal,
-                            ix_nrm(g, fi, fj - 1, k), ix_nrm(g, fi, fj, k));
-      fy[r * AX + c] = f;
+      if (yface[q] >= 0)
+        f = face_flux<R, 1>(yr[(size_t)s0 * (AY + 1) * AX + e], vs[yface[q]], vs[yface[q] + AWX], normal,
+                            nk + ynrm[q], nk + ynrm[q] + 4L * nx);
+      fy[e] = f;
     }
     double fz_hi = 0.;
     if (mine)
