@@ -98,11 +98,12 @@ ALG_BYTES_3D_MIXED = {
     "poisson_fwd": 32.0, "poisson_z": 8.0, "poisson_solve": 8.0, "poisson_inv": 16.0, "project": 72.0,
 }
 # dt (2), then per substep: geom + intercept, force, vof, coef + rhs +
-# line solve, 5 Poisson stages (10 in the mixed path), project
-KERNELS_PER_STEP_3D = 2 + 3 * 13
+# line solve, 6 Poisson launches (right-hand side, y, z, x, z, y; 12 in the
+# mixed path), project
+KERNELS_PER_STEP_3D = 2 + 3 * 14
 # kernels launched per launch of a kind (profile counts kernels)
-KERNELS_PER_KIND_3D = {"dt": 2, "geom": 2, "predict": 3}
-KERNELS_PER_STEP_3D_MIXED = 2 + 3 * 18
+KERNELS_PER_KIND_3D = {"dt": 2, "geom": 2, "predict": 3, "poisson_fwd": 2}
+KERNELS_PER_STEP_3D_MIXED = 2 + 3 * 20
 
 WORKLOADS3D = {
     # the headline configuration: 512^3, 128 droplets, radii 0.02 .. 0.05

@@ -8,6 +8,7 @@
 // x fastest: every transform reads and writes runs of consecutive i, and the
 // x line solve reads each line contiguously.  No transpose pass exists.
 //
+//   k3_pois_b      the right-hand side (or residual) of every cell, compact
 //   k3_pois_fwd_y  a block owns COLS consecutive i of one plane k
 //   k3_pois_z      a block owns COLS consecutive i of one ky, both signs
 //                  (in place)
@@ -185,7 +186,7 @@ __device__ __forceinline__ void fft_lines(R *__restrict__ re, R *__restrict__ im
 }
 
 // right-hand side (or, RESID, the residual b - A psi) at (i, j, k), FP64, in
-// two steps so that a group's loads can all be in flight before its first
+// two steps so that a thread's loads can all be in flight before its first
 // division: rhs_terms gathers the differences (loads, subtractions and
 // products only), rhs_value forms the quotients and sums, with the
 // association of b = div u / (gamma dt ny nz) and of the 7-point operator
@@ -229,15 +230,51 @@ __device__ __forceinline__ double rhs_value(const RhsTerms<RESID> &t, double dx,
   }
 }
 
+// the right-hand side (RESID: the residual) of every interior cell into b,
+// compact (x fastest, nx ny per plane): one thread per (i, j) and kBPlanes
+// planes, the loads of a pair of planes issued before their quotients
+constexpr int kBPlanes = 4;
+template <bool RESID>
+__global__ void __launch_bounds__(256) k3_pois_b(const double *__restrict__ ux, const double *__restrict__ uy,
+                                                 const double *__restrict__ uz, const double *__restrict__ psi,
+                                                 const double *__restrict__ pl, const double *__restrict__ pu,
+                                                 double *__restrict__ b, const double *__restrict__ dtp, double gam,
+                                                 Grid3 g) {
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k0 = 1 + blockIdx.z * kBPlanes;
+  if (i > nx || j > ny || k0 > nz) return;
+  const double dt = ldg(dtp);
+  const double prefactor = 1. / (gam * dt) / (1. * g.ny * g.nz);
+  const double gdt = gam * dt;
+  const double dx = ldg(g.dxf + i - 1);
+  const double l = RESID ? ldg(pl + i - 1) : 0., u = RESID ? ldg(pu + i - 1) : 0.;
+  double *bo = b + (i - 1) + (size_t)nx * (j - 1);
+  const size_t bplane = (size_t)nx * ny;
+  constexpr int B = 2;
+#pragma unroll
+  for (int kb = 0; kb < kBPlanes; kb += B) {
+    RhsTerms<RESID> t[B];
+#pragma unroll
+    for (int h = 0; h < B; h++) {
+      const int k = min(k0 + kb + h, nz);
+      t[h] = rhs_terms<RESID>(ux, uy, uz, psi, l, u, g, i, j, k);
+    }
+#pragma unroll
+    for (int h = 0; h < B; h++) {
+      const int k = k0 + kb + h;
+      if (k <= nz) bo[bplane * (k - 1)] = rhs_value<RESID>(t[h], dx, g, prefactor, gdt);
+    }
+  }
+}
+
 // forward transform along y of COLS consecutive i of plane k: the first pass
-// evaluates the right-hand side (RESID: the residual) of its points, the last
-// one writes the ky = 0 .. N/2 half of the spectrum
-template <int L2N, class R, bool RESID>
+// reads the right-hand side b (k3_pois_b), the last one writes the
+// ky = 0 .. N/2 half of the spectrum
+template <int L2N, class R>
 __global__ void __launch_bounds__(kLineThreads, Line<R, L2N>::MINB)
-    k3_pois_fwd_y(const double *__restrict__ ux, const double *__restrict__ uy, const double *__restrict__ uz,
-                  const double *__restrict__ psi, const double *__restrict__ pl, const double *__restrict__ pu,
-                  R *__restrict__ spec, const R *__restrict__ tw, const double *__restrict__ dtp, double gam,
-                  Grid3 g) {
+    k3_pois_fwd_y(const double *__restrict__ b, R *__restrict__ spec, const R *__restrict__ tw, Grid3 g) {
   using L = Line<R, L2N>;
   using C2 = typename Cplx<R>::T;
   constexpr int N = L::N, COLS = L::COLS, NKY = N / 2 + 1;
@@ -248,34 +285,14 @@ __global__ void __launch_bounds__(kLineThreads, Line<R, L2N>::MINB)
   const int i0 = 1 + blockIdx.x * COLS;
   const int k = 1 + blockIdx.y;
   const int nc = min(COLS, nx - i0 + 1);
-  const double dt = ldg(dtp);
-  const double prefactor = 1. / (gam * dt) / (1. * g.ny * g.nz);
-  const double gdt = gam * dt;
+  const double *bp = b + (size_t)nx * N * (k - 1) + (i0 - 1);
   C2 *out = reinterpret_cast<C2 *>(spec) + (size_t)(k - 1) * NKY * nx + (i0 - 1);
   auto first = [&](int c, int base, auto gc, auto hc, R *xr, R *xi) {
-    constexpr int G = decltype(gc)::value, H = decltype(hc)::value, BM = RESID ? 2 : 4, B = G < BM ? G : BM;
-    const int i = i0 + c;
-    const bool live = c < nc;
-    double dx = 1., l = 0., u = 0.;
-    if (live) {
-      dx = ldg(g.dxf + i - 1);
-      if (RESID) {
-        l = ldg(pl + i - 1);
-        u = ldg(pu + i - 1);
-      }
-    }
+    constexpr int G = decltype(gc)::value, H = decltype(hc)::value;
 #pragma unroll
-    for (int b0 = 0; b0 < G; b0 += B) {
-      RhsTerms<RESID> t[B];
-#pragma unroll
-      for (int q = 0; q < B; q++) {
-        if (live) t[q] = rhs_terms<RESID>(ux, uy, uz, psi, l, u, g, i, bitrev(base + (b0 + q) * H, L2N) + 1, k);
-      }
-#pragma unroll
-      for (int q = 0; q < B; q++) {
-        xr[b0 + q] = R(live ? rhs_value<RESID>(t[q], dx, g, prefactor, gdt) : 0.);
-        xi[b0 + q] = R(0.);
-      }
+    for (int m = 0; m < G; m++) {
+      xr[m] = R(c < nc ? ldg(bp + (size_t)nx * bitrev(base + m * H, L2N) + c) : 0.);
+      xi[m] = R(0.);
     }
   };
   auto last = [&](int c, int base, auto gc, auto hc, const R *xr, const R *xi) {
@@ -582,8 +599,7 @@ cudaError_t pois_prepare(int log2ny, int log2nz) {
     constexpr int L2 = decltype(c)::value;
     constexpr int sm = Line<R, L2>::SMEM;
     cudaError_t r;
-    if (cudaSuccess != (r = line_attrs(k3_pois_fwd_y<L2, R, false>, sm))) return r;
-    if (cudaSuccess != (r = line_attrs(k3_pois_fwd_y<L2, R, true>, sm))) return r;
+    if (cudaSuccess != (r = line_attrs(k3_pois_fwd_y<L2, R>, sm))) return r;
     if (cudaSuccess != (r = line_attrs(k3_pois_inv_y<L2, R, false>, sm))) return r;
     return line_attrs(k3_pois_inv_y<L2, R, true>, sm);
   });
@@ -599,17 +615,21 @@ cudaError_t pois_prepare(int log2ny, int log2nz) {
 
 template <class R>
 cudaError_t pois_fwd_y(bool resid, cudaStream_t st, const double *ux, const double *uy, const double *uz,
-                       const double *psi, const double *pl, const double *pu, R *spec, const R *tw,
+                       const double *psi, const double *pl, const double *pu, double *b, R *spec, const R *tw,
                        const double *dtp, double gam, int log2n, Grid3 g) {
+  const dim3 bb(32, 8), bg((g.nx + 31) / 32, (g.ny + 7) / 8, (g.nz + kBPlanes - 1) / kBPlanes);
+  if (resid) {
+    k3_pois_b<true><<<bg, bb, 0, st>>>(ux, uy, uz, psi, pl, pu, b, dtp, gam, g);
+  } else {
+    k3_pois_b<false><<<bg, bb, 0, st>>>(ux, uy, uz, psi, pl, pu, b, dtp, gam, g);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (cudaSuccess != e) return e;
   return by_l2n(log2n, [&](auto c) {
     constexpr int L2 = decltype(c)::value;
     using L = Line<R, L2>;
     dim3 gr((g.nx + L::COLS - 1) / L::COLS, g.nz);
-    if (resid) {
-      k3_pois_fwd_y<L2, R, true><<<gr, kLineThreads, L::SMEM, st>>>(ux, uy, uz, psi, pl, pu, spec, tw, dtp, gam, g);
-    } else {
-      k3_pois_fwd_y<L2, R, false><<<gr, kLineThreads, L::SMEM, st>>>(ux, uy, uz, psi, pl, pu, spec, tw, dtp, gam, g);
-    }
+    k3_pois_fwd_y<L2, R><<<gr, kLineThreads, L::SMEM, st>>>(b, spec, tw, g);
     return cudaGetLastError();
   });
 }
@@ -660,8 +680,8 @@ cudaError_t pois_inv_y(bool accum, cudaStream_t st, const R *spec, double *psi, 
 #define SVOF3_POISSON_INST(R)                                                                                    \
   template cudaError_t pois_prepare<R>(int, int);                                                                \
   template cudaError_t pois_fwd_y<R>(bool, cudaStream_t, const double *, const double *, const double *,   \
-                                     const double *, const double *, const double *, R *, const R *,            \
-                                     const double *, double, int, Grid3);                                       \
+                                     const double *, const double *, const double *, double *, R *,             \
+                                     const R *, const double *, double, int, Grid3);                            \
   template cudaError_t pois_z<R>(cudaStream_t, R *, const R *, int, Grid3);                                      \
   template cudaError_t pois_x<R>(cudaStream_t, R *, R *, const double *, const double *, const double *,        \
                                  const double *, int, Grid3);                                                    \

@@ -266,8 +266,10 @@ int launch_potential_t(svof3d_solver *s, int rk, const Marker &mark, const R *tw
   for (int pass = 0; pass < passes; pass++) {
     const bool second = pass > 0;
     const int cu = s->cur_u;
+    // (the right-hand side goes through the predictor's line scratch, idle
+    // here: 4 nx ny nz elements of 4 or 8 bytes)
     CK(pois_fwd_y<R>(second, s->stream, s->ux[cu].p, s->uy[cu].p, s->uz[cu].p, s->psi.p, s->pl.p,
-                     s->pu.p, s->spec.as<R>(), twfy, s->d_dt, gam, s->log2ny, g));
+                     s->pu.p, s->fw.as<double>(), s->spec.as<R>(), twfy, s->d_dt, gam, s->log2ny, g));
     if (m(SVOF3_K_POISSON_FWD)) return 1;
     CK(pois_z<R>(s->stream, s->spec.as<R>(), twfz, s->log2nz, g));
     if (m(SVOF3_K_POISSON_Z)) return 1;
@@ -791,7 +793,12 @@ int svof3d_profile_step(svof3d_solver_t *s, double *ms, int *launches, int nkind
       float t = 0.f;
       cudaEventElapsedTime(&t, ev[q - 1], ev[q]);
       ms[kind[q]] += t;
-      launches[kind[q]] += (SVOF3_K_PREDICT == kind[q]) ? 3 : ((SVOF3_K_DT == kind[q] || SVOF3_K_GEOM == kind[q]) ? 2 : 1);
+      // kernels per kind: predict = coefficients, right-hand sides, line
+      // solve; dt = reduction + final; geom = geometry + intercept;
+      // poisson_fwd = right-hand side + transform
+      const int kq = kind[q];
+      launches[kq] += (SVOF3_K_PREDICT == kq) ? 3
+                      : ((SVOF3_K_DT == kq || SVOF3_K_GEOM == kq || SVOF3_K_POISSON_FWD == kq) ? 2 : 1);
     }
   }
   for (cudaEvent_t x : ev) cudaEventDestroy(x);

@@ -152,9 +152,10 @@ __global__ void k3_tdm_coef(const double *__restrict__ lap_ux, const double *__r
 // (ky, kz) = (0, 0) line.
 template <class R>
 cudaError_t pois_prepare(int log2ny, int log2nz);
+// (b: scratch of nx ny nz doubles for the right-hand side)
 template <class R>
 cudaError_t pois_fwd_y(bool resid, cudaStream_t st, const double *ux, const double *uy, const double *uz,
-                       const double *psi, const double *pl, const double *pu, R *spec, const R *tw,
+                       const double *psi, const double *pl, const double *pu, double *b, R *spec, const R *tw,
                        const double *dtp, double gam, int log2n, Grid3 g);
 template <class R>
 cudaError_t pois_z(cudaStream_t st, R *spec, const R *tw, int log2n, Grid3 g);
