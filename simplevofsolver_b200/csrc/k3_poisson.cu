@@ -231,11 +231,12 @@ __device__ __forceinline__ double rhs_value(const RhsTerms<RESID> &t, double dx,
 }
 
 // the right-hand side (RESID: the residual) of every interior cell into b,
-// compact (x fastest, nx ny per plane): one thread per (i, j) and kBPlanes
-// planes, the loads of a pair of planes issued before their quotients
+// compact (x fastest, nx ny per plane): one thread per (i, j) walking
+// kBPlanes planes, uz at k + 1 (and psi at k, k + 1) carried to the next
+// plane; the loads of a batch of planes are issued before their quotients
 constexpr int kBPlanes = 4;
 template <bool RESID>
-__global__ void __launch_bounds__(256) k3_pois_b(const double *__restrict__ ux, const double *__restrict__ uy,
+__global__ void __launch_bounds__(256, 4) k3_pois_b(const double *__restrict__ ux, const double *__restrict__ uy,
                                                  const double *__restrict__ uz, const double *__restrict__ psi,
                                                  const double *__restrict__ pl, const double *__restrict__ pu,
                                                  double *__restrict__ b, const double *__restrict__ dtp, double gam,
@@ -252,19 +253,47 @@ __global__ void __launch_bounds__(256) k3_pois_b(const double *__restrict__ ux, 
   const double l = RESID ? ldg(pl + i - 1) : 0., u = RESID ? ldg(pu + i - 1) : 0.;
   double *bo = b + (i - 1) + (size_t)nx * (j - 1);
   const size_t bplane = (size_t)nx * ny;
-  constexpr int B = 2;
+  // carried values: uz at the current plane; psi below and at it
+  double uzk = ldg(uz + ix_cc(g, i, j, k0));
+  double pkm = RESID ? ldg(psi + ix_cc(g, i, j, k0 - 1)) : 0., pk = RESID ? ldg(psi + ix_cc(g, i, j, k0)) : 0.;
+  constexpr int B = RESID ? 2 : kBPlanes;
 #pragma unroll
   for (int kb = 0; kb < kBPlanes; kb += B) {
-    RhsTerms<RESID> t[B];
+    double x0[B], x1[B], y0[B], y1[B], zp[B], pxm[B], pxp[B], pym[B], pyp[B], pzp[B];
 #pragma unroll
     for (int h = 0; h < B; h++) {
       const int k = min(k0 + kb + h, nz);
-      t[h] = rhs_terms<RESID>(ux, uy, uz, psi, l, u, g, i, j, k);
+      x0[h] = ldg(ux + ix_ux(g, i, j, k));
+      x1[h] = ldg(ux + ix_ux(g, i + 1, j, k));
+      y0[h] = ldg(uy + ix_cc(g, i, j, k));
+      y1[h] = ldg(uy + ix_cc(g, i, j + 1, k));
+      zp[h] = ldg(uz + ix_cc(g, i, j, k + 1));
+      if (RESID) {
+        pxm[h] = ldg(psi + ix_cc(g, i - 1, j, k));
+        pxp[h] = ldg(psi + ix_cc(g, i + 1, j, k));
+        pym[h] = ldg(psi + ix_cc(g, i, j - 1, k));
+        pyp[h] = ldg(psi + ix_cc(g, i, j + 1, k));
+        pzp[h] = ldg(psi + ix_cc(g, i, j, k + 1));
+      }
     }
 #pragma unroll
     for (int h = 0; h < B; h++) {
       const int k = k0 + kb + h;
-      if (k <= nz) bo[bplane * (k - 1)] = rhs_value<RESID>(t[h], dx, g, prefactor, gdt);
+      if (k > nz) break;
+      RhsTerms<RESID> t;
+      t.dux = x1[h] - x0[h];
+      t.duy = y1[h] - y0[h];
+      t.duz = zp[h] - uzk;
+      uzk = zp[h];
+      if constexpr (RESID) {
+        const double c = pk;
+        t.ax = l * pxm[h] + (-l - u) * c + u * pxp[h];
+        t.ty = pym[h] - 2. * c + pyp[h];
+        t.tz = pkm - 2. * c + pzp[h];
+        pkm = pk;
+        pk = pzp[h];
+      }
+      bo[bplane * (k - 1)] = rhs_value<RESID>(t, dx, g, prefactor, gdt);
     }
   }
 }

@@ -421,15 +421,17 @@ constexpr int PL = kPredLines, PC = kPredChunk;
 
 // ---------------------------------------------------------------------------
 // k3_xsolve: the implicit-x Thomas sweeps of the four fields and the update.
-// A block owns 32 lines, walked in 32-cell x-chunks: forward (the increments
-// come in from the line array, warps 0..3 continue the recurrence with the
-// carry in a register, one field per warp and one line per lane, the swept
-// values go back), then backward in reverse chunk order with the update
-// u + delta' into the other buffer of the ping-pong pair, halo images
-// included, then the walls.
+// A block owns 32 lines, walked in 32-cell x-chunks staged by cp.async:
+// forward (the increments come in from the line array, warps 0..3 continue
+// the recurrence with the carry in a register in FP64, one field per warp and
+// one line per lane, the swept values go back), then backward in reverse
+// chunk order with the update u + delta' into the other buffer of the
+// ping-pong pair, halo images included, then the walls.  The tile holds the
+// storage type R (in the mixed path the swept increments are FP32, as in the
+// line array).
 template <class R>
 __global__ void __launch_bounds__(256) k3_xsolve(Predict3Args<R> a) {
-  __shared__ double sd[4][PL][PC + 1];  // the four fields' values of one tile
+  __shared__ R sd[4][PL][PC + 1];  // the four fields' values of one tile
   __shared__ double sco[9][PC];         // L, R, V of the three systems, one chunk
   const Grid3 g = a.g;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
@@ -460,14 +462,17 @@ __global__ void __launch_bounds__(256) k3_xsolve(Predict3Args<R> a) {
       const int p = p0 + tx;
       if (l >= nlines || p >= nx) continue;
       const R *fw = a.fw + (size_t)l * nx + p;
-      sd[0][ll][tx] = (p < nx - 1) ? (double)fw[0] : 0.;
-      sd[1][ll][tx] = fw[fstride];
-      sd[2][ll][tx] = fw[2 * fstride];
-      sd[3][ll][tx] = fw[3 * fstride];
+      if (p < nx - 1) __pipeline_memcpy_async(&sd[0][ll][tx], fw, sizeof(R));
+      else sd[0][ll][tx] = R(0.);
+      __pipeline_memcpy_async(&sd[1][ll][tx], fw + fstride, sizeof(R));
+      __pipeline_memcpy_async(&sd[2][ll][tx], fw + 2 * fstride, sizeof(R));
+      __pipeline_memcpy_async(&sd[3][ll][tx], fw + 3 * fstride, sizeof(R));
     }
+    __pipeline_commit();
+    __pipeline_wait_prior(0);
     __syncthreads();
     if (sweeper) {
-      double *q = sd[f][tx];
+      R *q = sd[f][tx];
       const double *L = sco[3 * set], *Rr = sco[3 * set + 1];
       const int smax = min(PC, nf - p0);
 #pragma unroll 4
@@ -481,7 +486,7 @@ __global__ void __launch_bounds__(256) k3_xsolve(Predict3Args<R> a) {
         } else {
           carry = (0. != Rr[s]) ? Rr[s] * (x - L[s] * carry) : 0.;
         }
-        q[s] = carry;
+        q[s] = R(carry);
       }
     }
     __syncthreads();
@@ -515,14 +520,17 @@ __global__ void __launch_bounds__(256) k3_xsolve(Predict3Args<R> a) {
       const int p = p0 + tx;
       if (l >= nlines || p >= nx) continue;
       const R *fw = a.fw + (size_t)l * nx + p;
-      sd[0][ll][tx] = (p < nx - 1) ? fw[0] : 0.;
-      sd[1][ll][tx] = fw[fstride];
-      sd[2][ll][tx] = fw[2 * fstride];
-      sd[3][ll][tx] = fw[3 * fstride];
+      if (p < nx - 1) __pipeline_memcpy_async(&sd[0][ll][tx], fw, sizeof(R));
+      else sd[0][ll][tx] = R(0.);
+      __pipeline_memcpy_async(&sd[1][ll][tx], fw + fstride, sizeof(R));
+      __pipeline_memcpy_async(&sd[2][ll][tx], fw + 2 * fstride, sizeof(R));
+      __pipeline_memcpy_async(&sd[3][ll][tx], fw + 3 * fstride, sizeof(R));
     }
+    __pipeline_commit();
+    __pipeline_wait_prior(0);
     __syncthreads();
     if (sweeper) {
-      double *q = sd[f][tx];
+      R *q = sd[f][tx];
       const double *V = sco[3 * set + 2];
       const int smax = min(PC, nf - p0);
 #pragma unroll 4
@@ -532,7 +540,7 @@ __global__ void __launch_bounds__(256) k3_xsolve(Predict3Args<R> a) {
           nxt = q[s];
         } else {
           nxt = q[s] - V[s] * nxt;
-          q[s] = nxt;
+          q[s] = R(nxt);
         }
       }
     }

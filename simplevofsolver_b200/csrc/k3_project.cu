@@ -129,10 +129,13 @@ __device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v)
 }
 
 // one thread per interior (i, j) and kCflPlanes planes k: the ux face i in
-// [2, nx], the uy and the uz faces of each cell.  All candidates are
-// positive, so the minimum of their IEEE bit patterns as unsigned integers is
-// the bit pattern of the minimum (NaN candidates, whose patterns lie above
-// that of +inf, never win, as with fmin).
+// [2, nx], the uy and the uz faces of each cell.  The candidate d / (|u| +
+// 1e-8) decreases with |u|, and rounded addition and division are monotone,
+// so the thread's minimum over its faces of a kind is the quotient of its
+// maximum |u| (NaN velocities are skipped by fmax, as by the fmin of the
+// per-face form): three divisions a thread instead of three a cell.  All
+// candidates are positive, so the minimum of their IEEE bit patterns as
+// unsigned integers is the bit pattern of the minimum.
 __global__ void __launch_bounds__(256) k3_cfl(const double *__restrict__ ux, const double *__restrict__ uy,
                                               const double *__restrict__ uz, unsigned long long *__restrict__ minbits,
                                               Grid3 g) {
@@ -143,7 +146,6 @@ __global__ void __launch_bounds__(256) k3_cfl(const double *__restrict__ ux, con
   const double small = 1.e-8;
   unsigned long long best = 0x7ff0000000000000ull;
   if (i <= nx && j <= ny) {
-    const double dxc = (i >= 2) ? ldg(g.dxc + i - 1) : 0.;
     double vy[kCflPlanes], vz[kCflPlanes], vx[kCflPlanes];
 #pragma unroll
     for (int h = 0; h < kCflPlanes; h++) {
@@ -152,16 +154,19 @@ __global__ void __launch_bounds__(256) k3_cfl(const double *__restrict__ ux, con
       vz[h] = ldg(uz + ix_cc(g, i, j, k));
       vx[h] = (i >= 2) ? ldg(ux + ix_ux(g, i, j, k)) : 0.;
     }
+    double my = -1., mz = -1., mx = -1.;
 #pragma unroll
     for (int h = 0; h < kCflPlanes; h++) {
       if (k0 + h > nz) break;
-      double cand = g.dy / (fabs(vy[h]) + small);
-      const double cz = g.dz / (fabs(vz[h]) + small);
-      cand = fmin(cand, cz);
-      if (i >= 2) cand = fmin(cand, dxc / (fabs(vx[h]) + small));
-      const unsigned long long b = (unsigned long long)__double_as_longlong(cand);
-      best = b < best ? b : best;
+      my = fmax(my, fabs(vy[h]));
+      mz = fmax(mz, fabs(vz[h]));
+      if (i >= 2) mx = fmax(mx, fabs(vx[h]));
     }
+    double cand = __longlong_as_double(0x7ff0000000000000ll);
+    if (my >= 0.) cand = fmin(cand, g.dy / (my + small));
+    if (mz >= 0.) cand = fmin(cand, g.dz / (mz + small));
+    if (mx >= 0.) cand = fmin(cand, ldg(g.dxc + i - 1) / (mx + small));
+    best = (unsigned long long)__double_as_longlong(cand);
   }
   best = warp_min_u64(best);
   __shared__ unsigned long long sbest[8];
