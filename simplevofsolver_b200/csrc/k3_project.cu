@@ -7,7 +7,8 @@
 //                in 2D, carried to z by oracle/svof_oracle3d.c)
 //   k3_cfl       min over faces of dx / (|u| + 1e-8) (src/fluid/decide_dt.c:28-64)
 //   k3_dt_final  safety factor and the explicit y and z diffusion limits
-//   k3_diag      max |div u|, vof min / max, compensated volume sum
+//   k3_diag_part / k3_diag_final  max |div u|, vof min / max and the
+//                compensated volume sum, in two deterministic stages
 #include "svof3d_internal.cuh"
 
 namespace svof3 {
@@ -204,47 +205,113 @@ __device__ __forceinline__ void two_sum_acc(double &s, double &c, double x) {
   c += err;
 }
 
-// out = {max |div u|, vof min, vof max, sum vof dx dy dz}; one block of
-// kDiagThreads threads, deterministic order
-constexpr int kDiagThreads = 512;
+// compensated pair (s, c) += (s2, c2): s2 added exactly (TwoSum), the
+// correction terms summed
+__device__ __forceinline__ void comp_add(double &s, double &c, double s2, double c2) {
+  two_sum_acc(s, c, s2);
+  c += c2;
+}
 
-__global__ void __launch_bounds__(kDiagThreads) k3_diag(const double *__restrict__ ux, const double *__restrict__ uy, const double *__restrict__ uz,
-                        const double *__restrict__ vof, double *__restrict__ out, Grid3 g) {
-  const int nx = g.nx, ny = g.ny;
-  const long ncell = (long)nx * ny * g.nz;
-  double dmax = 0., vmin = 1., vmax = 0., s0 = 0., c0 = 0.;
-  for (long w = threadIdx.x; w < ncell; w += blockDim.x) {
-    const int i = 1 + (int)(w % nx);
-    const long r = w / nx;
-    const int j = 1 + (int)(r % ny), k = 1 + (int)(r / ny);
-    const double dx = g.dxf[i - 1];
-    const double div = +(ux[ix_ux(g, i + 1, j, k)] - ux[ix_ux(g, i, j, k)]) / dx +
-                       (uy[ix_cc(g, i, j + 1, k)] - uy[ix_cc(g, i, j, k)]) / g.dy +
-                       (uz[ix_cc(g, i, j, k + 1)] - uz[ix_cc(g, i, j, k)]) / g.dz;
-    dmax = fmax(dmax, fabs(div));
-    const double lv = vof[ix_vof(g, i, j, k)];
-    vmin = fmin(vmin, lv);
-    vmax = fmax(vmax, lv);
-    two_sum_acc(s0, c0, lv * (dx * g.dy * g.dz));
+// the five partial values of a thread set, reduced over a warp by a fixed
+// xor-butterfly (the same order on every run)
+struct DiagPart {
+  double dmax, vmin, vmax, s, c;
+};
+__device__ __forceinline__ void warp_reduce_diag(DiagPart &d) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    d.dmax = fmax(d.dmax, __shfl_xor_sync(0xffffffffu, d.dmax, o));
+    d.vmin = fmin(d.vmin, __shfl_xor_sync(0xffffffffu, d.vmin, o));
+    d.vmax = fmax(d.vmax, __shfl_xor_sync(0xffffffffu, d.vmax, o));
+    const double s2 = __shfl_xor_sync(0xffffffffu, d.s, o), c2 = __shfl_xor_sync(0xffffffffu, d.c, o);
+    comp_add(d.s, d.c, s2, c2);
   }
-  __shared__ double red[4][kDiagThreads];
-  red[0][threadIdx.x] = dmax;
-  red[1][threadIdx.x] = vmin;
-  red[2][threadIdx.x] = vmax;
-  red[3][threadIdx.x] = s0 + c0;
+}
+
+// stage 1: one thread per interior (i, j) and kDiagPlanes planes (uz at
+// k + 1 carried to the next plane); each block of 32 x 8 threads writes its
+// partial {max |div u|, vof min, vof max, volume sum, its correction} to
+// part[5 b]
+__global__ void __launch_bounds__(256) k3_diag_part(const double *__restrict__ ux, const double *__restrict__ uy,
+                                                    const double *__restrict__ uz, const double *__restrict__ vof,
+                                                    double *__restrict__ part, Grid3 g) {
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k0 = 1 + blockIdx.z * kDiagPlanes;
+  DiagPart d{0., 1., 0., 0., 0.};
+  if (i <= nx && j <= ny && k0 <= nz) {
+    const double dx = ldg(g.dxf + i - 1);
+    const double cell = dx * g.dy * g.dz;
+    double uzk = ldg(uz + ix_cc(g, i, j, k0));
+#pragma unroll 4
+    for (int h = 0; h < kDiagPlanes; h++) {
+      const int k = k0 + h;
+      if (k > nz) break;
+      const double x0 = ldg(ux + ix_ux(g, i, j, k)), x1 = ldg(ux + ix_ux(g, i + 1, j, k));
+      const double y0 = ldg(uy + ix_cc(g, i, j, k)), y1 = ldg(uy + ix_cc(g, i, j + 1, k));
+      const double zp = ldg(uz + ix_cc(g, i, j, k + 1));
+      const double lv = ldg(vof + ix_vof(g, i, j, k));
+      const double div = +(x1 - x0) / dx + (y1 - y0) / g.dy + (zp - uzk) / g.dz;
+      uzk = zp;
+      d.dmax = fmax(d.dmax, fabs(div));
+      d.vmin = fmin(d.vmin, lv);
+      d.vmax = fmax(d.vmax, lv);
+      two_sum_acc(d.s, d.c, lv * cell);
+    }
+  }
+  warp_reduce_diag(d);
+  __shared__ DiagPart sp[8];
+  const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+  const int lane = tid & 31, warp = tid >> 5;
+  if (0 == lane) sp[warp] = d;
+  __syncthreads();
+  if (0 == tid) {
+    DiagPart r = sp[0];
+    for (int w = 1; w < 8; w++) {
+      r.dmax = fmax(r.dmax, sp[w].dmax);
+      r.vmin = fmin(r.vmin, sp[w].vmin);
+      r.vmax = fmax(r.vmax, sp[w].vmax);
+      comp_add(r.s, r.c, sp[w].s, sp[w].c);
+    }
+    double *o = part + 5 * (size_t)(blockIdx.x + gridDim.x * (blockIdx.y + (size_t)gridDim.y * blockIdx.z));
+    o[0] = r.dmax;
+    o[1] = r.vmin;
+    o[2] = r.vmax;
+    o[3] = r.s;
+    o[4] = r.c;
+  }
+}
+
+// stage 2: one block of kDiagThreads threads folds the nparts partials in a
+// fixed order into out = {max |div u|, vof min, vof max, sum vof dx dy dz}
+__global__ void __launch_bounds__(kDiagThreads) k3_diag_final(const double *__restrict__ part, long nparts,
+                                                               double *__restrict__ out) {
+  DiagPart d{0., 1., 0., 0., 0.};
+  for (long b = threadIdx.x; b < nparts; b += kDiagThreads) {
+    const double *o = part + 5 * b;
+    d.dmax = fmax(d.dmax, o[0]);
+    d.vmin = fmin(d.vmin, o[1]);
+    d.vmax = fmax(d.vmax, o[2]);
+    comp_add(d.s, d.c, o[3], o[4]);
+  }
+  warp_reduce_diag(d);
+  __shared__ DiagPart sp[kDiagThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (0 == lane) sp[warp] = d;
   __syncthreads();
   if (0 == threadIdx.x) {
-    double a = 0., b = 1., c = 0., ss = 0., cc = 0.;
-    for (int t = 0; t < (int)blockDim.x; t++) {
-      a = fmax(a, red[0][t]);
-      b = fmin(b, red[1][t]);
-      c = fmax(c, red[2][t]);
-      two_sum_acc(ss, cc, red[3][t]);
+    DiagPart r = sp[0];
+    for (int w = 1; w < kDiagThreads / 32; w++) {
+      r.dmax = fmax(r.dmax, sp[w].dmax);
+      r.vmin = fmin(r.vmin, sp[w].vmin);
+      r.vmax = fmax(r.vmax, sp[w].vmax);
+      comp_add(r.s, r.c, sp[w].s, sp[w].c);
     }
-    out[0] = a;
-    out[1] = b;
-    out[2] = c;
-    out[3] = ss + cc;
+    out[0] = r.dmax;
+    out[1] = r.vmin;
+    out[2] = r.vmax;
+    out[3] = r.s + r.c;
   }
 }
 

@@ -523,7 +523,8 @@ int svof3d_create(const svof3d_params_t *prm, const double *xf, const double *xc
   }
   if (dalloc(s->p, n_cc) || dalloc(s->psi, n_cc) || dalloc(s->curv, n_cc, es) ||
       dalloc(s->normal, 4 * nx * (ny + 2) * (nz + 2), es) || dalloc(s->ifrcx, n_srcx, es) ||
-      dalloc(s->ifrcy, n_src, es) || dalloc(s->ifrcz, n_src, es) || dalloc(s->diag, 8))
+      dalloc(s->ifrcy, n_src, es) || dalloc(s->ifrcz, n_src, es) ||
+      dalloc(s->diag, 8 + 5 * (size_t)((nx + 31) / 32) * ((ny + 7) / 8) * ((nz + kDiagPlanes - 1) / kDiagPlanes)))
     return bail();
   if (build_tables(s, xf, xc)) return bail();
   if (dalloc(s->coef, 9 * nx)) return bail();
@@ -809,8 +810,11 @@ int svof3d_profile_step(svof3d_solver_t *s, double *ms, int *launches, int nkind
 
 int svof3d_diagnostics(svof3d_solver_t *s, double *divmax, double *vofmin, double *vofmax, double *volume) {
   if (!s) return fail("null argument");
-  k3_diag<<<1, 512, 0, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->uz[s->cur_u].p,
-                                     s->vof[s->cur_v].p, s->diag.p, s->grid());
+  const dim3 db(32, 8), dg((s->nx + 31) / 32, (s->ny + 7) / 8, (s->nz + kDiagPlanes - 1) / kDiagPlanes);
+  k3_diag_part<<<dg, db, 0, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->uz[s->cur_u].p,
+                                         s->vof[s->cur_v].p, s->diag.p + 8, s->grid());
+  CK_LAUNCH();
+  k3_diag_final<<<1, kDiagThreads, 0, s->stream>>>(s->diag.p + 8, (long)dg.x * dg.y * dg.z, s->diag.p);
   CK_LAUNCH();
   double h[4];
   CK(cudaMemcpyAsync(h, s->diag.p, sizeof(h), cudaMemcpyDeviceToHost, s->stream));

@@ -176,9 +176,14 @@ __global__ void k3_cfl(const double *__restrict__ ux, const double *__restrict__
                        unsigned long long *__restrict__ minbits, Grid3 g);
 __global__ void k3_dt_final(unsigned long long *minbits, double *dt, double coef_adv, double l0, double l1,
                             double l2, double l3);
-// diagnostics: out = {max |div u|, vof min, vof max, sum vof dx dy dz}
-__global__ void k3_diag(const double *__restrict__ ux, const double *__restrict__ uy, const double *__restrict__ uz,
-                        const double *__restrict__ vof, double *__restrict__ out, Grid3 g);
+// diagnostics, deterministic two-stage reduction: blocks of 32 x 8 threads
+// over kDiagPlanes planes write 5 partials each; out = {max |div u|, vof min,
+// vof max, sum vof dx dy dz (compensated)}
+constexpr int kDiagPlanes = 8, kDiagThreads = 1024;
+__global__ void k3_diag_part(const double *__restrict__ ux, const double *__restrict__ uy,
+                             const double *__restrict__ uz, const double *__restrict__ vof,
+                             double *__restrict__ part, Grid3 g);
+__global__ void k3_diag_final(const double *__restrict__ part, long nparts, double *__restrict__ out);
 
 // launch constants shared by the kernels and the host
 constexpr int kPredLines = 32;  // lines per predictor block
