@@ -307,6 +307,17 @@ def _profile(solver, nprof):
     return prof
 
 
+def _traffic(workload, prec, kind):
+    """DRAM bytes (read + write) per launch of `kind` from the committed ncu
+    summary profiles/traffic.json, or None"""
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(tpath):
+        return None
+    with open(tpath) as f:
+        tj = json.load(f)
+    return tj.get(workload, {}).get(prec, {}).get(kind)
+
+
 def _roofline(prof, alg_bytes_cell, cells, nprof):
     """roofline of the dominant kernel kind: algorithmic bytes per launch over
     its average device time per launch (coefficient + predictor, geometry +
@@ -411,7 +422,8 @@ def run3d(args, wl, ic, env, world, rank, local_rank):
                            35.5 * cells * 8 / 1e9),
                        "parallelism": f"replicas{world}"},
             "fp64": {"value": f["value"], "unit": METRIC, "ms_per_step": f["total_ms"] / args.steps,
-                     "roofline": f["roofline"],
+                     "roofline": dict(f["roofline"], traffic=_traffic(args.workload, "fp64", f["roofline"]["kernel"]),
+                                      traffic_unit="DRAM bytes per launch (ncu, profiles/traffic.json)"),
                      "step_frac": f["value"] * 1e6 * ALG_BYTES_CELL_STEP_3D / 1e9 / peak,
                      "kernel_ms_per_step": {k: v[0] / 3 for k, v in f["prof"].items()},
                      "clocks": f["clocks"]},
@@ -419,7 +431,8 @@ def run3d(args, wl, ic, env, world, rank, local_rank):
             "mixed_error": err,
             "e2e": m["e2e"],
             "gpu_launches": KERNELS_PER_STEP_3D_MIXED * args.steps,
-            "roofline": dict(m["roofline"], traffic=None,
+            "roofline": dict(m["roofline"], traffic=_traffic(args.workload, "mixed", m["roofline"]["kernel"]),
+                             traffic_unit="DRAM bytes per launch (ncu, profiles/traffic.json)",
                              step_frac=m["value"] * 1e6 * m["step_alg_bytes"] / 1e9 / peak,
                              step_alg_bytes_per_cell=m["step_alg_bytes"]),
             "kernel_ms_per_step": {k: v[0] / 3 for k, v in m["prof"].items()},
