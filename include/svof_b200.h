@@ -149,6 +149,19 @@ int svof_last_dt(svof_solver_t *solver, double *dt);
 int svof_diagnostics(svof_solver_t *solver, double *divmax, double *vofmin, double *vofmax,
                      double *vofmean);
 
+/* the logging reductions of src/logging/momentum.c:38-54, src/logging/
+ * energy.c:41-65 and src/logging/nusselt/ (heat_flux.c:22-41,
+ * kinetic_energy_injection.c:25-49, kinetic_energy_dissipation.c:11-163,
+ * thermal_energy_dissipation.c:10-95, reference.c:4-12) computed on the
+ * device from the current fields, without moving them to the host.  out[0..8]
+ * (nout >= 9) = {x momentum, y momentum, kinetic energy of ux, of uy, thermal
+ * energy, Nusselt number from the wall heat flux, from the kinetic energy
+ * injection, from the kinetic energy dissipation, from the thermal energy
+ * dissipation}: the values the reference writes to momentum.dat, energy.dat
+ * and nusselt.dat.  The sums are compensated (TwoSum) and deterministic; they
+ * differ from the reference's sequential sums only by round-off. */
+int svof_logging_quantities(svof_solver_t *solver, double *out, int nout);
+
 /* kernel kinds of svof_profile_step */
 enum {
   SVOF_K_DT = 0,            /* CFL reduction + dt (2 launches) */

@@ -92,6 +92,7 @@ def _load():
             getattr(L, fn).argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double]
         L.svo_integrate.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
         L.svo_run.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        L.svo_logging.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         _lib = L
     return _lib
 
@@ -176,6 +177,16 @@ class Oracle:
         if _load().svo_run(self._h, int(nsteps), dts.ctypes.data) != 0:
             raise RuntimeError("svo_run failed")
         return dts[:nsteps]
+
+    LOGGING_NAMES = ["momentum_x", "momentum_y", "energy_ux", "energy_uy", "energy_t", "nu_heat_flux",
+                     "nu_kinetic_injection", "nu_kinetic_dissipation", "nu_thermal_dissipation"]
+
+    def logging(self) -> dict:
+        """src/logging/momentum.c, energy.c and nusselt/ on the current fields
+        (svo_logging: the reference's loops and order)"""
+        out = np.zeros(9)
+        _load().svo_logging(self._h, out.ctypes.data)
+        return dict(zip(self.LOGGING_NAMES, out.tolist()))
 
 
 # ---------------------------------------------------------------- 3D

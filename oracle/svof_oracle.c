@@ -997,3 +997,136 @@ int svo_run(svo_ctx_t *c, int nsteps, double *dts) {
   }
   return 0;
 }
+
+/* ---------------- logging reductions: src/logging/{momentum,energy}.c and src/logging/nusselt/ ----------------
+ * out = {x momentum, y momentum (momentum.c:38-54); kinetic energy of ux, of uy,
+ * thermal energy (energy.c:41-65); Nusselt numbers from the wall heat flux
+ * (nusselt/heat_flux.c:22-41), the kinetic energy injection
+ * (kinetic_energy_injection.c:25-49), the kinetic energy dissipation
+ * (kinetic_energy_dissipation.c:11-163) and the thermal energy dissipation
+ * (thermal_energy_dissipation.c:10-95)}, each normalised by the laminar heat
+ * flux t_dif ly (reference.c:4-12); the sums in the reference's loop order */
+int svo_logging(svo_ctx_t *c, double out[9]) {
+  const double dy = c->dy, md = c->prm.m_dif, td = c->prm.t_dif;
+  const double *T = c->t, *UY = c->uy;
+#define TT(i, j) CC(T, i, j)
+#define VY(i, j) CC(UY, i, j)
+  double mx = 0., my = 0.;
+  for (int j = 1; j <= NY; j++)
+    for (int i = 2; i <= NX; i++) mx += UX(i, j) * (DXC(i) * dy);
+  for (int j = 1; j <= NY; j++)
+    for (int i = 1; i <= NX; i++) my += VY(i, j) * (DXF(i) * dy);
+  double ex = 0., ey = 0., et = 0.;
+  for (int j = 1; j <= NY; j++)
+    for (int i = 2; i <= NX; i++) ex += 0.5 * pow(UX(i, j), 2.) * (DXC(i) * dy);
+  for (int j = 1; j <= NY; j++)
+    for (int i = 1; i <= NX; i++) ey += 0.5 * pow(VY(i, j), 2.) * (DXF(i) * dy);
+  for (int j = 1; j <= NY; j++)
+    for (int i = 1; i <= NX; i++) et += 0.5 * pow(TT(i, j), 2.) * (DXF(i) * dy);
+  const double ref = td * c->prm.ly;
+  /* heat flux through the two walls */
+  double hf = 0.;
+  for (int j = 1; j <= NY; j++) {
+    const double dtdx_xm = (+TT(1, j) - TT(0, j)) / DXC(1);
+    const double dtdx_xp = (+TT(NX + 1, j) - TT(NX, j)) / DXC(NX + 1);
+    hf -= 0.5 * td * (dtdx_xm + dtdx_xp) * dy;
+  }
+  /* kinetic energy injection */
+  double inj = 0.;
+  for (int j = 1; j <= NY; j++)
+    for (int i = 2; i <= NX; i++) {
+      const double t_ = +0.5 * TT(i - 1, j) + 0.5 * TT(i, j);
+      inj += UX(i, j) * t_ * (DXC(i) * dy);
+    }
+  /* kinetic energy dissipation: ux-x, ux-y, uy-x, uy-y */
+  double kd[4] = {0., 0., 0., 0.};
+  for (int j = 1; j <= NY; j++)
+    for (int i = 1; i <= NX + 1; i++) {
+      const double cs = DXC(i) * dy;
+      if (1 != i) {
+        const double d = 1. / DXF(i - 1) * (UX(i, j) - UX(i - 1, j));
+        const double w = DXF(i - 1) / DXC(i);
+        kd[0] += md * 0.5 * w * pow(d, 2.) * cs;
+      }
+      if (NX + 1 != i) {
+        const double d = 1. / DXF(i) * (UX(i + 1, j) - UX(i, j));
+        const double w = DXF(i) / DXC(i);
+        kd[0] += md * 0.5 * w * pow(d, 2.) * cs;
+      }
+    }
+  for (int j = 1; j <= NY; j++)
+    for (int i = 1; i <= NX + 1; i++) {
+      const double cs = DXC(i) * dy;
+      const double dm = 1. / dy * (UX(i, j) - UX(i, j - 1));
+      kd[1] += md * 0.5 * pow(dm, 2.) * cs;
+      const double dp = 1. / dy * (UX(i, j + 1) - UX(i, j));
+      kd[1] += md * 0.5 * pow(dp, 2.) * cs;
+    }
+  for (int j = 1; j <= NY; j++)
+    for (int i = 1; i <= NX; i++) {
+      const double cs = DXF(i) * dy;
+      {
+        const double d = 1. / DXC(i) * (VY(i, j) - VY(i - 1, j));
+        const double w0 = DXC(i) / DXF(i), w1 = 1 == i ? 2. : 1.;
+        kd[2] += md * 0.5 * w0 * w1 * pow(d, 2.) * cs;
+      }
+      {
+        const double d = 1. / DXC(i + 1) * (VY(i + 1, j) - VY(i, j));
+        const double w0 = DXC(i + 1) / DXF(i), w1 = NX == i ? 2. : 1.;
+        kd[2] += md * 0.5 * w0 * w1 * pow(d, 2.) * cs;
+      }
+    }
+  for (int j = 1; j <= NY; j++)
+    for (int i = 1; i <= NX; i++) {
+      const double cs = DXF(i) * dy;
+      const double dm = 1. / dy * (VY(i, j) - VY(i, j - 1));
+      kd[3] += md * 0.5 * pow(dm, 2.) * cs;
+      const double dp = 1. / dy * (VY(i, j + 1) - VY(i, j));
+      kd[3] += md * 0.5 * pow(dp, 2.) * cs;
+    }
+  /* thermal energy dissipation: x, y */
+  double th[2] = {0., 0.};
+  for (int j = 1; j <= NY; j++)
+    for (int i = 1; i <= NX; i++) {
+      const double cs = DXF(i) * dy;
+      {
+        const double d = 1. / DXC(i) * (TT(i, j) - TT(i - 1, j));
+        const double w0 = DXC(i) / DXF(i), w1 = 1 == i ? 2. : 1.;
+        th[0] += td * 0.5 * w0 * w1 * pow(d, 2.) * cs;
+      }
+      {
+        const double d = 1. / DXC(i + 1) * (TT(i + 1, j) - TT(i, j));
+        const double w0 = DXC(i + 1) / DXF(i), w1 = NX == i ? 2. : 1.;
+        th[0] += td * 0.5 * w0 * w1 * pow(d, 2.) * cs;
+      }
+    }
+  for (int j = 1; j <= NY; j++)
+    for (int i = 1; i <= NX; i++) {
+      const double cs = DXF(i) * dy;
+      const double dm = 1. / dy * (TT(i, j) - TT(i, j - 1));
+      th[1] += td * 0.5 * pow(dm, 2.) * cs;
+      const double dp = 1. / dy * (TT(i, j + 1) - TT(i, j));
+      th[1] += td * 0.5 * pow(dp, 2.) * cs;
+    }
+#undef TT
+#undef VY
+  double kdis = 0.;
+  kdis += kd[0];
+  kdis += kd[1];
+  kdis += kd[2];
+  kdis += kd[3];
+  double tdis = 0.;
+  tdis += th[0];
+  tdis += th[1];
+  out[0] = mx;
+  out[1] = my;
+  out[2] = ex;
+  out[3] = ey;
+  out[4] = et;
+  out[5] = hf / ref;
+  out[6] = inj / ref + 1.;
+  out[7] = kdis / ref + 1.;
+  out[8] = tdis / ref;
+  return 0;
+}
+

@@ -61,6 +61,11 @@ int svo_correct(svo_ctx_t *ctx, int rkstep, double dt);
 int svo_update_pressure(svo_ctx_t *ctx, int rkstep, double dt);
 int svo_integrate(svo_ctx_t *ctx, double *dt);
 int svo_run(svo_ctx_t *ctx, int nsteps, double *dts);
+/* logging reductions of the current fields (src/logging/momentum.c,
+ * energy.c, nusselt/ sources): out = {momentum x, y; energy ux, uy, t; Nusselt from
+ * the wall heat flux, kinetic energy injection, kinetic and thermal energy
+ * dissipation} */
+int svo_logging(svo_ctx_t *ctx, double out[9]);
 
 #ifdef __cplusplus
 }

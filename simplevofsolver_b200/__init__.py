@@ -112,6 +112,7 @@ def lib() -> ctypes.CDLL:
         L.svof_enqueue_steps.argtypes = [vp, i]
         L.svof_last_dt.argtypes = [vp, pd]
         L.svof_diagnostics.argtypes = [vp, pd, pd, pd, pd]
+        L.svof_logging_quantities.argtypes = [vp, pd, i]
         L.svof_synchronize.argtypes = [vp]
         L.svof_profile_step.argtypes = [vp, dp, dp, i]
         L.svof_stream.argtypes = [vp, ctypes.POINTER(vp)]
@@ -274,6 +275,17 @@ class Solver:
         v = [ctypes.c_double() for _ in range(4)]
         _check(lib().svof_diagnostics(self._h, *[ctypes.byref(x) for x in v]))
         return dict(divmax=v[0].value, vofmin=v[1].value, vofmax=v[2].value, vofmean=v[3].value)
+
+    LOGGING_NAMES = ["momentum_x", "momentum_y", "energy_ux", "energy_uy", "energy_t", "nu_heat_flux",
+                     "nu_kinetic_injection", "nu_kinetic_dissipation", "nu_thermal_dissipation"]
+
+    def logging(self) -> dict:
+        """the logging reductions of src/logging/momentum.c, energy.c and
+        nusselt/ on the device (the quantities of momentum.dat, energy.dat and
+        nusselt.dat)"""
+        out = np.zeros(9)
+        _check(lib().svof_logging_quantities(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 9))
+        return dict(zip(self.LOGGING_NAMES, out.tolist()))
 
     KERNEL_KINDS = ["dt", "geom", "force", "vof", "predict", "poisson_fwd", "poisson_solve",
                     "poisson_inv", "project"]

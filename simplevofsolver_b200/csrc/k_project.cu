@@ -217,4 +217,152 @@ __global__ void k_diag(const double *__restrict__ ux, const double *__restrict__
   }
 }
 
+// ---------------------------------------------------------------------------
+// k_logging: the logging reductions of src/logging/momentum.c:38-54,
+// energy.c:41-65 and nusselt/{heat_flux,kinetic_energy_injection,
+// kinetic_energy_dissipation,thermal_energy_dissipation}.c on the device,
+// every term with the reference's expression and association; the sums are
+// TwoSum-compensated, thread partials folded over a warp by a fixed
+// butterfly and over the block in warp order (deterministic).  One block of
+// kLogThreads threads walks the positions (i, j), i in [1, nx+1], j in
+// [1, ny].  out = {momentum x, y; energy ux, uy, t; Nusselt from the wall
+// heat flux, kinetic energy injection, kinetic and thermal energy
+// dissipation}.
+namespace {
+constexpr int kLogThreads = 1024, kLogSums = 13;
+struct CSum {
+  double s = 0., c = 0.;
+  __device__ __forceinline__ void add(double x) { two_sum_acc(s, c, x); }
+  __device__ __forceinline__ void add(const CSum &o) {
+    two_sum_acc(s, c, o.s);
+    c += o.c;
+  }
+};
+}  // namespace
+
+__global__ void __launch_bounds__(kLogThreads) k_logging(const double *__restrict__ ux, const double *__restrict__ uy,
+                                                         const double *__restrict__ t, double m_dif, double t_dif,
+                                                         double ly, double *__restrict__ out, Grid2 g) {
+  const int nx = g.nx, ny = g.ny;
+  const double dy = g.dy, md = m_dif, td = t_dif;
+  auto UX = [&](int i, int j) { return ux[ix_ux(nx, i, j)]; };
+  auto UY = [&](int i, int j) { return uy[ix_cc(nx, i, j)]; };
+  auto TT = [&](int i, int j) { return t[ix_cc(nx, i, j)]; };
+  auto DXF = [&](int i) { return g.dxf[i - 1]; };
+  auto DXC = [&](int i) { return g.dxc[i - 1]; };
+  // 0 mx, 1 my, 2 ex, 3 ey, 4 et, 5 heat flux, 6 injection, 7..10 kinetic
+  // dissipation (ux-x, ux-y, uy-x, uy-y), 11..12 thermal dissipation (x, y)
+  CSum sum[kLogSums];
+  const int npos = (nx + 1) * ny;
+  for (int w = threadIdx.x; w < npos; w += kLogThreads) {
+    const int i = 1 + w % (nx + 1), j = 1 + w / (nx + 1);
+    // ---- ux faces i in [1, nx+1]
+    {
+      const double cs = DXC(i) * dy;
+      if (2 <= i && i <= nx) {
+        const double u = UX(i, j);
+        sum[0].add(u * (DXC(i) * dy));
+        sum[2].add(0.5 * (u * u) * (DXC(i) * dy));
+        const double t_ = +0.5 * TT(i - 1, j) + 0.5 * TT(i, j);
+        sum[6].add(u * t_ * (DXC(i) * dy));
+      }
+      if (1 != i) {
+        const double d = 1. / DXF(i - 1) * (UX(i, j) - UX(i - 1, j));
+        const double wt = DXF(i - 1) / DXC(i);
+        sum[7].add(md * 0.5 * wt * (d * d) * cs);
+      }
+      if (nx + 1 != i) {
+        const double d = 1. / DXF(i) * (UX(i + 1, j) - UX(i, j));
+        const double wt = DXF(i) / DXC(i);
+        sum[7].add(md * 0.5 * wt * (d * d) * cs);
+      }
+      const double dm = 1. / dy * (UX(i, j) - UX(i, j - 1));
+      sum[8].add(md * 0.5 * (dm * dm) * cs);
+      const double dp = 1. / dy * (UX(i, j + 1) - UX(i, j));
+      sum[8].add(md * 0.5 * (dp * dp) * cs);
+    }
+    // ---- cells i in [1, nx]
+    if (i <= nx) {
+      const double cs = DXF(i) * dy;
+      const double v = UY(i, j), tc = TT(i, j);
+      sum[1].add(v * (DXF(i) * dy));
+      sum[3].add(0.5 * (v * v) * (DXF(i) * dy));
+      sum[4].add(0.5 * (tc * tc) * (DXF(i) * dy));
+      const double w1m = 1 == i ? 2. : 1., w1p = nx == i ? 2. : 1.;
+      {
+        const double d = 1. / DXC(i) * (v - UY(i - 1, j));
+        sum[9].add(md * 0.5 * (DXC(i) / DXF(i)) * w1m * (d * d) * cs);
+      }
+      {
+        const double d = 1. / DXC(i + 1) * (UY(i + 1, j) - v);
+        sum[9].add(md * 0.5 * (DXC(i + 1) / DXF(i)) * w1p * (d * d) * cs);
+      }
+      {
+        const double dm = 1. / dy * (v - UY(i, j - 1));
+        sum[10].add(md * 0.5 * (dm * dm) * cs);
+        const double dp = 1. / dy * (UY(i, j + 1) - v);
+        sum[10].add(md * 0.5 * (dp * dp) * cs);
+      }
+      {
+        const double d = 1. / DXC(i) * (tc - TT(i - 1, j));
+        sum[11].add(td * 0.5 * (DXC(i) / DXF(i)) * w1m * (d * d) * cs);
+      }
+      {
+        const double d = 1. / DXC(i + 1) * (TT(i + 1, j) - tc);
+        sum[11].add(td * 0.5 * (DXC(i + 1) / DXF(i)) * w1p * (d * d) * cs);
+      }
+      {
+        const double dm = 1. / dy * (tc - TT(i, j - 1));
+        sum[12].add(td * 0.5 * (dm * dm) * cs);
+        const double dp = 1. / dy * (TT(i, j + 1) - tc);
+        sum[12].add(td * 0.5 * (dp * dp) * cs);
+      }
+    }
+    // ---- the wall heat flux of row j
+    if (1 == i) {
+      const double dtdx_xm = (+TT(1, j) - TT(0, j)) / DXC(1);
+      const double dtdx_xp = (+TT(nx + 1, j) - TT(nx, j)) / DXC(nx + 1);
+      sum[5].add(-(0.5 * td * (dtdx_xm + dtdx_xp) * dy));
+    }
+  }
+  // warp butterfly, then warp order
+#pragma unroll
+  for (int q = 0; q < kLogSums; q++) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      CSum x;
+      x.s = __shfl_xor_sync(0xffffffffu, sum[q].s, o);
+      x.c = __shfl_xor_sync(0xffffffffu, sum[q].c, o);
+      sum[q].add(x);
+    }
+  }
+  __shared__ CSum red[kLogSums][kLogThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (0 == lane) {
+#pragma unroll
+    for (int q = 0; q < kLogSums; q++) red[q][warp] = sum[q];
+  }
+  __syncthreads();
+  if (threadIdx.x < kLogSums) {
+    const int q = threadIdx.x;
+    CSum r = red[q][0];
+    for (int w = 1; w < kLogThreads / 32; w++) r.add(red[q][w]);
+    red[q][0] = r;
+  }
+  __syncthreads();
+  if (0 == threadIdx.x) {
+    auto v = [&](int q) { return red[q][0].s + red[q][0].c; };
+    const double ref = td * ly;  // laminar heat flux (nusselt/reference.c:4-12)
+    out[0] = v(0);
+    out[1] = v(1);
+    out[2] = v(2);
+    out[3] = v(3);
+    out[4] = v(4);
+    out[5] = v(5) / ref;
+    out[6] = v(6) / ref + 1.;
+    out[7] = (((v(7) + v(8)) + v(9)) + v(10)) / ref + 1.;
+    out[8] = (v(11) + v(12)) / ref;
+  }
+}
+
 }  // namespace svof

@@ -588,7 +588,7 @@ int engine_create(const svof_params_t *prm, const double *xf, const double *xc, 
   }
   if (dalloc(s->p, n_cc, mg) || dalloc(s->psi, n_cc, mg) || dalloc(s->curv, n_cc, mg) ||
       dalloc(s->normal, 3 * (size_t)nx * (ny + 2), mg) || dalloc(s->ifrcx, n_srcx, mg) ||
-      dalloc(s->ifrcy, n_src, mg) || dalloc(s->diag, 8))
+      dalloc(s->ifrcy, n_src, mg) || dalloc(s->diag, 16))
     return bail();
   if (build_tables(s, xf, xc)) return bail();
   if (dalloc(s->coef, 9 * (size_t)nx)) return bail();
@@ -1022,6 +1022,16 @@ int svof_diagnostics(svof_solver_t *s, double *divmax, double *vofmin, double *v
   if (vofmin) *vofmin = h[1];
   if (vofmax) *vofmax = h[2];
   if (vofmean) *vofmean = h[3] / h[4];
+  return 0;
+}
+
+int svof_logging_quantities(svof_solver_t *s, double *out, int nout) {
+  if (!s || !out || nout < 9) return fail("svof_logging_quantities: bad arguments (nout must be >= 9)");
+  k_logging<<<1, 1024, 0, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->t[s->cur_u].p, s->prm.m_dif,
+                                       s->prm.t_dif, s->prm.ly, s->diag.p, s->grid());
+  CK_LAUNCH();
+  CK(cudaMemcpyAsync(out, s->diag.p, 9 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
   return 0;
 }
 

@@ -121,6 +121,10 @@ __global__ void k_dt_final(unsigned long long *minbits, double *dt, double coef_
 // diagnostics (src/logging/divergence.c, src/logging/interface.c)
 __global__ void k_diag(const double *__restrict__ ux, const double *__restrict__ uy,
                        const double *__restrict__ vof, double *__restrict__ out, Grid2 g);
+// logging reductions (src/logging/momentum.c, energy.c, nusselt/); one block
+__global__ void k_logging(const double *__restrict__ ux, const double *__restrict__ uy,
+                          const double *__restrict__ t, double m_dif, double t_dif, double ly,
+                          double *__restrict__ out, Grid2 g);
 
 // ---- engine internals shared by the C ABI front-ends (solver.cu, dropin.cu) ----
 // svof_create with a choice of field memory: managed = CUDA managed memory,
