@@ -149,9 +149,19 @@ class Solver:
                              float(uy_walls[1]), float(t_walls[0]), float(t_walls[1]))
         self._h = ctypes.c_void_p()
         xf, xc = _c(ic.xf), _c(ic.xc)
+        self._grid = (float(ic.lx), float(ic.ly), xf.copy(), xc.copy())
         _check(L.svof_create(ctypes.byref(self.params), xf.ctypes.data, xc.ctypes.data, ctypes.byref(self._h)))
         for k, v in ic.fields().items():
             self.load_interior(k, v)
+
+    @classmethod
+    def from_npy_dir(cls, dirname: str, physical: dict, **kw):
+        """restart from a directory in the reference's save layout (as
+        fluid_init / interface_init read it); returns (solver, step, time)"""
+        ic = read_npy_dir(dirname)
+        step = int(np.load(os.path.join(dirname, "step.npy")))
+        time = float(np.load(os.path.join(dirname, "time.npy")))
+        return cls(ic, physical, **kw), step, time
 
     # ------------------------------------------------------------ lifetime
     def close(self):
@@ -275,6 +285,34 @@ class Solver:
         v = [ctypes.c_double() for _ in range(4)]
         _check(lib().svof_diagnostics(self._h, *[ctypes.byref(x) for x in v]))
         return dict(divmax=v[0].value, vofmin=v[1].value, vofmax=v[2].value, vofmean=v[3].value)
+
+    # ------------------------------------------------------------ restart files
+    def state(self) -> InitialCondition:
+        """the current fields in the restart layout, with the grid"""
+        lx, ly, xf, xc = self._grid
+        return InitialCondition(self.nx, self.ny, lx, ly, xf.copy(), xc.copy(),
+                                *(self.interior(k) for k in ("ux", "uy", "p", "t", "vof")))
+
+    def fluid_save(self, dirname: str):
+        """src/fluid/save.c: m_dif, t_dif and ux, uy, p, t"""
+        os.makedirs(dirname, exist_ok=True)
+        np.save(os.path.join(dirname, "m_dif.npy"), np.array(self.params.m_dif))
+        np.save(os.path.join(dirname, "t_dif.npy"), np.array(self.params.t_dif))
+        for k in ("ux", "uy", "p", "t"):
+            np.save(os.path.join(dirname, f"{k}.npy"), self.interior(k))
+
+    def interface_save(self, dirname: str):
+        """src/interface/save.c: surface_tension and vof"""
+        os.makedirs(dirname, exist_ok=True)
+        np.save(os.path.join(dirname, "surface_tension.npy"), np.array(self.params.tension))
+        np.save(os.path.join(dirname, "vof.npy"), self.interior("vof"))
+
+    def save(self, dirname: str, step: int = 0, time: float = 0.0):
+        """a save / restart directory as the reference's save entry point
+        writes it (src/save.c, src/main.c:64-71, src/domain.c:60-74)"""
+        write_npy_dir(self.state(), dirname, step, time)
+        self.fluid_save(dirname)
+        self.interface_save(dirname)
 
     LOGGING_NAMES = ["momentum_x", "momentum_y", "energy_ux", "energy_uy", "energy_t", "nu_heat_flux",
                      "nu_kinetic_injection", "nu_kinetic_dissipation", "nu_thermal_dissipation"]

@@ -8,11 +8,12 @@ periodic z direction.  Storage shapes are (z, y, x[, comps]), x fastest.
 from __future__ import annotations
 
 import ctypes
+import os
 
 import numpy as np
 
 from . import SvofError, lib
-from .workloads import InitialCondition3D
+from .workloads import InitialCondition3D, read_npy_dir, write_npy_dir
 
 
 class Params3D(ctypes.Structure):
@@ -129,9 +130,48 @@ class Solver3D:
                                float(t_walls[0]), float(t_walls[1]), MIXED if precision == "mixed" else FP64)
         self._h = ctypes.c_void_p()
         xf, xc = _c(ic.xf), _c(ic.xc)
+        self._grid = (float(ic.lx), float(ic.ly), float(ic.lz), xf.copy(), xc.copy())
         _check(L.svof3d_create(ctypes.byref(self.params), xf.ctypes.data, xc.ctypes.data, ctypes.byref(self._h)))
         for k, v in ic.fields().items():
             self.load_interior(k, v)
+
+    @classmethod
+    def from_npy_dir(cls, dirname: str, physical: dict, **kw):
+        """restart from a 3D directory in the save layout; returns (solver,
+        step, time)"""
+        ic = read_npy_dir(dirname)
+        if not isinstance(ic, InitialCondition3D):
+            raise ValueError(f"{dirname} holds a 2D restart set")
+        step = int(np.load(os.path.join(dirname, "step.npy")))
+        time = float(np.load(os.path.join(dirname, "time.npy")))
+        return cls(ic, physical, **kw), step, time
+
+    # ------------------------------------------------------------ restart files
+    def state(self) -> InitialCondition3D:
+        """the current fields in the restart layout, with the grid"""
+        lx, ly, lz, xf, xc = self._grid
+        return InitialCondition3D(self.nx, self.ny, self.nz, lx, ly, lz, xf.copy(), xc.copy(),
+                                  *(self.interior(k) for k in ("ux", "uy", "uz", "p", "t", "vof")))
+
+    def fluid_save(self, dirname: str):
+        """m_dif, t_dif and ux, uy, uz, p, t (src/fluid/save.c with uz)"""
+        os.makedirs(dirname, exist_ok=True)
+        np.save(os.path.join(dirname, "m_dif.npy"), np.array(self.params.m_dif))
+        np.save(os.path.join(dirname, "t_dif.npy"), np.array(self.params.t_dif))
+        for k in ("ux", "uy", "uz", "p", "t"):
+            np.save(os.path.join(dirname, f"{k}.npy"), self.interior(k))
+
+    def interface_save(self, dirname: str):
+        """surface_tension and vof (src/interface/save.c)"""
+        os.makedirs(dirname, exist_ok=True)
+        np.save(os.path.join(dirname, "surface_tension.npy"), np.array(self.params.tension))
+        np.save(os.path.join(dirname, "vof.npy"), self.interior("vof"))
+
+    def save(self, dirname: str, step: int = 0, time: float = 0.0):
+        """a save / restart directory: step, time, the grid, fluid and interface"""
+        write_npy_dir(self.state(), dirname, step, time)
+        self.fluid_save(dirname)
+        self.interface_save(dirname)
 
     def close(self):
         if getattr(self, "_h", None) and self._h.value:

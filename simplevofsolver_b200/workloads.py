@@ -317,22 +317,36 @@ def physical_params(env: dict):
                 coef_dt_adv=float(env["coef_dt_adv"]), coef_dt_dif=float(env["coef_dt_dif"]))
 
 
-def write_npy_dir(ic: InitialCondition, dirname: str, step: int = 0, time: float = 0.0):
+def write_npy_dir(ic, dirname: str, step: int = 0, time: float = 0.0):
+    """a restart directory in the reference's layout (src/main.c:64-71,
+    src/domain.c:60-74, src/fluid/save.c, src/interface/save.c): step, time,
+    glsizes, lengths, xf, xc and the fields' interior rows with their x ghost
+    cells; 2D (InitialCondition) or 3D (InitialCondition3D: one more size and
+    length, uz)"""
     os.makedirs(dirname, exist_ok=True)
+    three = hasattr(ic, "nz")
+    sizes = [ic.nx, ic.ny, ic.nz] if three else [ic.nx, ic.ny]
+    lengths = [ic.lx, ic.ly, ic.lz] if three else [ic.lx, ic.ly]
     np.save(os.path.join(dirname, "step.npy"), np.array(step, dtype=np.uint64))
     np.save(os.path.join(dirname, "time.npy"), np.array(time, dtype=np.float64))
-    np.save(os.path.join(dirname, "glsizes.npy"), np.array([ic.nx, ic.ny], dtype=np.uint64))
-    np.save(os.path.join(dirname, "lengths.npy"), np.array([ic.lx, ic.ly], dtype=np.float64))
+    np.save(os.path.join(dirname, "glsizes.npy"), np.array(sizes, dtype=np.uint64))
+    np.save(os.path.join(dirname, "lengths.npy"), np.array(lengths, dtype=np.float64))
     np.save(os.path.join(dirname, "xf.npy"), ic.xf.astype(np.float64))
     np.save(os.path.join(dirname, "xc.npy"), ic.xc.astype(np.float64))
     for k, v in ic.fields().items():
         np.save(os.path.join(dirname, f"{k}.npy"), np.ascontiguousarray(v, dtype=np.float64))
 
 
-def read_npy_dir(dirname: str) -> InitialCondition:
+def read_npy_dir(dirname: str):
+    """the restart directory written by write_npy_dir or by the reference's
+    save: InitialCondition (2D) or InitialCondition3D (glsizes of 3 items)"""
     ld = lambda k: np.load(os.path.join(dirname, f"{k}.npy"))
     gl = ld("glsizes")
     ln = ld("lengths")
+    if 3 == len(gl):
+        nx, ny, nz = (int(v) for v in gl)
+        return InitialCondition3D(nx, ny, nz, float(ln[0]), float(ln[1]), float(ln[2]), ld("xf"), ld("xc"),
+                                  ld("ux"), ld("uy"), ld("uz"), ld("p"), ld("t"), ld("vof"))
     nx, ny = int(gl[0]), int(gl[1])
     return InitialCondition(nx, ny, float(ln[0]), float(ln[1]), ld("xf"), ld("xc"),
                             ld("ux"), ld("uy"), ld("p"), ld("t"), ld("vof"))
