@@ -219,9 +219,10 @@ __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ 
   const R rdxf = (i0 + tx <= nx) ? R(1.) / R(ldg(g.dxf + i0 + tx - 1)) : R(0.);
   __pipeline_wait_prior(0);
   __syncthreads();
+  R l_dx0 = R(0.), l_dy1 = R(0.), l_s0 = R(0.), l_s1 = R(0.), l_s2 = R(0.);  // lower corner plane
   for (int kc = k0; kc <= kend; kc++) {
     const int bcur = (kc - k0 + 1) % 3, bprev = (kc - k0) % 3;
-    const int ccur = (kc - k0) & 1, cprev = ccur ^ 1;
+    const int ccur = (kc - k0) & 1;
     if (kc + 1 <= kend) load_plane(kc + 1);
     // compute_gradient at corners (ic, jc, kc): planes kc-1 (bprev) and kc (bcur)
     for (int t = tid, q = 0; t < (G3X + 1) * (G3Y + 1); t += G3X * G3Y, q++) {
@@ -246,29 +247,37 @@ __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ 
       sc[ccur][2][lj][li] = d2;
     }
     __syncthreads();
-    if (kc > k0) {
-      // cells of plane k = kc - 1: corners kc - 1 (cprev, lower) and kc (ccur, upper)
-      const int i = i0 + tx, j = j0 + ty, k = kc - 1;
-      bool inter = false;
-      if (i <= nx && j <= ny + 1) {
-        const R dxf = R(ldg(g.dxf + i - 1));
-#define CL(m, a, b) sc[cprev][m][ty + (b)][tx + (a)]
+    // the corner plane kc's 2 x 2 stencils of this thread's cell column: the
+    // upper plane of cell k = kc - 1 now, the lower plane of cell kc next
+    // (carried in registers, so each is formed once, with the same operands
+    // in the same order)
+    const int i = i0 + tx, j = j0 + ty;
+    const bool cell = i <= nx && j <= ny + 1;
+    R u_dx0 = R(0.), u_dy1 = R(0.), u_s0 = R(0.), u_s1 = R(0.), u_s2 = R(0.);
+    if (cell) {
 #define CU(m, a, b) sc[ccur][m][ty + (b)][tx + (a)]
-        const R dnxdx = rdxf * (plane_dx(CL(0, 0, 0), CL(0, 1, 0), CL(0, 0, 1), CL(0, 1, 1)) +
-                                       plane_dx(CU(0, 0, 0), CU(0, 1, 0), CU(0, 0, 1), CU(0, 1, 1)));
-        const R dnydy = rdy * (plane_dy(CL(1, 0, 0), CL(1, 1, 0), CL(1, 0, 1), CL(1, 1, 1)) +
-                               plane_dy(CU(1, 0, 0), CU(1, 1, 0), CU(1, 0, 1), CU(1, 1, 1)));
-        const R dnzdz = rdz * (plane_sum(CU(2, 0, 0), CU(2, 1, 0), CU(2, 0, 1), CU(2, 1, 1)) -
-                               plane_sum(CL(2, 0, 0), CL(2, 1, 0), CL(2, 0, 1), CL(2, 1, 1)));
+      u_dx0 = plane_dx(CU(0, 0, 0), CU(0, 1, 0), CU(0, 0, 1), CU(0, 1, 1));
+      u_dy1 = plane_dy(CU(1, 0, 0), CU(1, 1, 0), CU(1, 0, 1), CU(1, 1, 1));
+      u_s0 = plane_sum(CU(0, 0, 0), CU(0, 1, 0), CU(0, 0, 1), CU(0, 1, 1));
+      u_s1 = plane_sum(CU(1, 0, 0), CU(1, 1, 0), CU(1, 0, 1), CU(1, 1, 1));
+      u_s2 = plane_sum(CU(2, 0, 0), CU(2, 1, 0), CU(2, 0, 1), CU(2, 1, 1));
+#undef CU
+    }
+    if (kc > k0) {
+      // cells of plane k = kc - 1: corners kc - 1 (lower, carried) and kc (upper)
+      const int k = kc - 1;
+      bool inter = false;
+      if (cell) {
+        const R dxf = R(ldg(g.dxf + i - 1));
+        const R dnxdx = rdxf * (l_dx0 + u_dx0);
+        const R dnydy = rdy * (l_dy1 + u_dy1);
+        const R dnzdz = rdz * (u_s2 - l_s2);
         curv[ix_cc(g, i, j, k)] = R(0.25) * (-dnxdx - dnydy - dnzdz);
         const double lvof = sv[bprev][ty + 1][tx + 1];
         if (!(lvof < kVofMin || 1. - kVofMin < lvof)) {
-          R n0 = plane_sum(CL(0, 0, 0), CL(0, 1, 0), CL(0, 0, 1), CL(0, 1, 1)) +
-                 plane_sum(CU(0, 0, 0), CU(0, 1, 0), CU(0, 0, 1), CU(0, 1, 1));
-          R n1 = plane_sum(CL(1, 0, 0), CL(1, 1, 0), CL(1, 0, 1), CL(1, 1, 1)) +
-                 plane_sum(CU(1, 0, 0), CU(1, 1, 0), CU(1, 0, 1), CU(1, 1, 1));
-          R n2 = plane_sum(CL(2, 0, 0), CL(2, 1, 0), CL(2, 0, 1), CL(2, 1, 1)) +
-                 plane_sum(CU(2, 0, 0), CU(2, 1, 0), CU(2, 0, 1), CU(2, 1, 1));
+          R n0 = l_s0 + u_s0;
+          R n1 = l_s1 + u_s1;
+          R n2 = l_s2 + u_s2;
           n0 = div_by(n0, dxf);
           n1 = div_by(n1, R(g.dy));
           n2 = div_by(n2, R(g.dz));
@@ -279,8 +288,6 @@ __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ 
           store_normal3(normal + ix_nrm(g, i, j, k), n0, n1, n2);
           inter = true;
         }
-#undef CL
-#undef CU
       }
       // the intercept's Newton iteration runs in k3_intercept over a compacted
       // list of the interfacial cells (warp-aggregated append)
@@ -296,6 +303,11 @@ __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ 
         }
       }
     }
+    l_dx0 = u_dx0;
+    l_dy1 = u_dy1;
+    l_s0 = u_s0;
+    l_s1 = u_s1;
+    l_s2 = u_s2;
     __pipeline_wait_prior(0);
     __syncthreads();
   }
