@@ -335,30 +335,53 @@ __global__ void __launch_bounds__(256) k3_intercept(const double *__restrict__ v
 }
 
 // ---------------------------------------------------------------------------
-// k3_force: one thread per interior cell; FP64 arithmetic, R output
+// k3_force: one thread per interior (i, j) and kForcePlanes planes k (vof and
+// curvature at k - 1 carried from the previous plane, the loads of the
+// thread's planes issued before its arithmetic); FP64 arithmetic, R output
+constexpr int kForcePlanes = 4;
 template <class R>
-__global__ void k3_force(const double *__restrict__ vof, const R *__restrict__ curv, R *__restrict__ ifrcx,
-                         R *__restrict__ ifrcy, R *__restrict__ ifrcz, double tension, Grid3 g) {
+__global__ void __launch_bounds__(256) k3_force(const double *__restrict__ vof, const R *__restrict__ curv,
+                                                R *__restrict__ ifrcx, R *__restrict__ ifrcy, R *__restrict__ ifrcz,
+                                                double tension, Grid3 g) {
   const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = 1 + blockIdx.z;
-  if (i > g.nx || j > g.ny) return;
-  const double vc = ldg(vof + ix_vof(g, i, j, k));
-  const double cc = (double)__ldg(curv + ix_cc(g, i, j, k));
-  if (i >= 2) {
-    const double grad = 1. / ldg(g.dxc + i - 1) * (-ldg(vof + ix_vof(g, i - 1, j, k)) + vc);
-    const double kappa = 0.5 * (+(double)__ldg(curv + ix_cc(g, i - 1, j, k)) + cc);
-    ifrcx[ix_srcx(g, i, j, k)] = R(tension * grad * kappa);
+  const int k0 = 1 + blockIdx.z * kForcePlanes;
+  if (i > g.nx || j > g.ny || k0 > g.nz) return;
+  const double rdxc = (i >= 2) ? 1. / ldg(g.dxc + i - 1) : 0., rdy = 1. / g.dy, rdz = 1. / g.dz;
+  double vc[kForcePlanes], vxm[kForcePlanes], vym[kForcePlanes], cc[kForcePlanes], cxm[kForcePlanes],
+      cym[kForcePlanes];
+#pragma unroll
+  for (int h = 0; h < kForcePlanes; h++) {
+    const int k = min(k0 + h, g.nz);
+    vc[h] = ldg(vof + ix_vof(g, i, j, k));
+    vxm[h] = ldg(vof + ix_vof(g, i - 1, j, k));
+    vym[h] = ldg(vof + ix_vof(g, i, j - 1, k));
+    cc[h] = (double)__ldg(curv + ix_cc(g, i, j, k));
+    cxm[h] = (double)__ldg(curv + ix_cc(g, i - 1, j, k));
+    cym[h] = (double)__ldg(curv + ix_cc(g, i, j - 1, k));
   }
-  {
-    const double grad = 1. / g.dy * (-ldg(vof + ix_vof(g, i, j - 1, k)) + vc);
-    const double kappa = 0.5 * (+(double)__ldg(curv + ix_cc(g, i, j - 1, k)) + cc);
-    ifrcy[ix_src(g, i, j, k)] = R(tension * grad * kappa);
-  }
-  {
-    const double grad = 1. / g.dz * (-ldg(vof + ix_vof(g, i, j, k - 1)) + vc);
-    const double kappa = 0.5 * (+(double)__ldg(curv + ix_cc(g, i, j, k - 1)) + cc);
-    ifrcz[ix_src(g, i, j, k)] = R(tension * grad * kappa);
+  double vzm = ldg(vof + ix_vof(g, i, j, k0 - 1)), czm = (double)__ldg(curv + ix_cc(g, i, j, k0 - 1));
+#pragma unroll
+  for (int h = 0; h < kForcePlanes; h++) {
+    const int k = k0 + h;
+    if (k > g.nz) break;
+    if (i >= 2) {
+      const double grad = rdxc * (-vxm[h] + vc[h]);
+      const double kappa = 0.5 * (+cxm[h] + cc[h]);
+      ifrcx[ix_srcx(g, i, j, k)] = R(tension * grad * kappa);
+    }
+    {
+      const double grad = rdy * (-vym[h] + vc[h]);
+      const double kappa = 0.5 * (+cym[h] + cc[h]);
+      ifrcy[ix_src(g, i, j, k)] = R(tension * grad * kappa);
+    }
+    {
+      const double grad = rdz * (-vzm + vc[h]);
+      const double kappa = 0.5 * (+czm + cc[h]);
+      ifrcz[ix_src(g, i, j, k)] = R(tension * grad * kappa);
+    }
+    vzm = vc[h];
+    czm = cc[h];
   }
 }
 
@@ -608,7 +631,7 @@ cudaError_t interface_geom(cudaStream_t st, const double *vof, R *normal, R *cur
 template <class R>
 cudaError_t interface_force(cudaStream_t st, const double *vof, const R *curv, R *ifrcx, R *ifrcy, R *ifrcz,
                             double tension, Grid3 g) {
-  dim3 b(32, 8), gr((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz);
+  dim3 b(32, 8), gr((g.nx + 31) / 32, (g.ny + 7) / 8, (g.nz + kForcePlanes - 1) / kForcePlanes);
   k3_force<R><<<gr, b, 0, st>>>(vof, curv, ifrcx, ifrcy, ifrcz, tension, g);
   return cudaGetLastError();
 }
