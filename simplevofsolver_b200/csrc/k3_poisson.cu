@@ -8,7 +8,8 @@
 // x fastest: every transform reads and writes runs of consecutive i, and the
 // x line solve reads each line contiguously.  No transpose pass exists.
 //
-//   k3_pois_b      the right-hand side (or residual) of every cell, compact
+//   k3_pois_b      the right-hand side of every cell, compact (k3_pois_resid:
+//                  the mixed second pass's residual, in place)
 //   k3_pois_fwd_y  a block owns COLS consecutive i of one plane k
 //   k3_pois_z      a block owns COLS consecutive i of one ky, both signs
 //                  (in place)
@@ -23,7 +24,7 @@
 // arithmetic: R = double is the FP64 path (the restatement's butterflies bit
 // for bit); R = float is the mixed path.  The x line solve is FP64 in both.
 // The mixed path solves twice (defect correction): the second pass
-// transforms the FP64 residual b - A psi of the first solution (RESID) and
+// transforms the FP64 residual b - A psi of the first solution (k3_pois_resid) and
 // adds its solution to psi (ACCUM); its singular (ky, kz) = (0, 0) line has
 // its gauge pinned (last unknown zero) so that the FP32 round-off of the
 // compatibility condition cannot blow the additive constant up.
@@ -185,62 +186,15 @@ __device__ __forceinline__ void fft_lines(R *__restrict__ re, R *__restrict__ im
   }
 }
 
-// right-hand side (or, RESID, the residual b - A psi) at (i, j, k), FP64, in
-// two steps so that a thread's loads can all be in flight before its first
-// division: rhs_terms gathers the differences (loads, subtractions and
-// products only), rhs_value forms the quotients and sums, with the
-// association of b = div u / (gamma dt ny nz) and of the 7-point operator
-template <bool RESID>
-struct RhsTerms;
-template <>
-struct RhsTerms<false> {
-  double dux, duy, duz;
-};
-template <>
-struct RhsTerms<true> {
-  double dux, duy, duz, ax, ty, tz;
-};
-
-template <bool RESID>
-__device__ __forceinline__ RhsTerms<RESID> rhs_terms(const double *__restrict__ ux, const double *__restrict__ uy,
-                                                     const double *__restrict__ uz, const double *__restrict__ psi,
-                                                     double l, double u, const Grid3 &g, int i, int j, int k) {
-  RhsTerms<RESID> t;
-  t.dux = ldg(ux + ix_ux(g, i + 1, j, k)) - ldg(ux + ix_ux(g, i, j, k));
-  t.duy = ldg(uy + ix_cc(g, i, j + 1, k)) - ldg(uy + ix_cc(g, i, j, k));
-  t.duz = ldg(uz + ix_cc(g, i, j, k + 1)) - ldg(uz + ix_cc(g, i, j, k));
-  if constexpr (RESID) {
-    const double c = ldg(psi + ix_cc(g, i, j, k));
-    t.ax = l * ldg(psi + ix_cc(g, i - 1, j, k)) + (-l - u) * c + u * ldg(psi + ix_cc(g, i + 1, j, k));
-    t.ty = ldg(psi + ix_cc(g, i, j - 1, k)) - 2. * c + ldg(psi + ix_cc(g, i, j + 1, k));
-    t.tz = ldg(psi + ix_cc(g, i, j, k - 1)) - 2. * c + ldg(psi + ix_cc(g, i, j, k + 1));
-  }
-  return t;
-}
-
-template <bool RESID>
-__device__ __forceinline__ double rhs_value(const RhsTerms<RESID> &t, double dx, const Grid3 &g, double prefactor,
-                                            double gdt) {
-  const double div = +t.dux / dx + t.duy / g.dy + t.duz / g.dz;
-  if constexpr (!RESID) {
-    return prefactor * div;
-  } else {
-    const double ap = t.ax + t.ty / (g.dy * g.dy) + t.tz / (g.dz * g.dz);
-    return (div / gdt - ap) / (1. * g.ny * g.nz);
-  }
-}
-
-// the right-hand side (RESID: the residual) of every interior cell into b,
-// compact (x fastest, nx ny per plane): one thread per (i, j) walking
-// kBPlanes planes, uz at k + 1 (and psi at k, k + 1) carried to the next
-// plane; the loads of a batch of planes are issued before their quotients
+// the right-hand side b = div u / (gamma dt ny nz) of every interior cell,
+// FP64, into a compact array (x fastest, nx ny per plane), with the
+// reference's association: one thread per (i, j) walking kBPlanes planes, uz
+// at k + 1 carried to the next plane, every load of the thread's planes
+// issued before its first division
 constexpr int kBPlanes = 4;
-template <bool RESID>
 __global__ void __launch_bounds__(256, 4) k3_pois_b(const double *__restrict__ ux, const double *__restrict__ uy,
-                                                 const double *__restrict__ uz, const double *__restrict__ psi,
-                                                 const double *__restrict__ pl, const double *__restrict__ pu,
-                                                 double *__restrict__ b, const double *__restrict__ dtp, double gam,
-                                                 Grid3 g) {
+                                                    const double *__restrict__ uz, double *__restrict__ b,
+                                                    const double *__restrict__ dtp, double gam, Grid3 g) {
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
@@ -248,52 +202,73 @@ __global__ void __launch_bounds__(256, 4) k3_pois_b(const double *__restrict__ u
   if (i > nx || j > ny || k0 > nz) return;
   const double dt = ldg(dtp);
   const double prefactor = 1. / (gam * dt) / (1. * g.ny * g.nz);
-  const double gdt = gam * dt;
   const double dx = ldg(g.dxf + i - 1);
-  const double l = RESID ? ldg(pl + i - 1) : 0., u = RESID ? ldg(pu + i - 1) : 0.;
   double *bo = b + (i - 1) + (size_t)nx * (j - 1);
   const size_t bplane = (size_t)nx * ny;
-  // carried values: uz at the current plane; psi below and at it
-  double uzk = ldg(uz + ix_cc(g, i, j, k0));
-  double pkm = RESID ? ldg(psi + ix_cc(g, i, j, k0 - 1)) : 0., pk = RESID ? ldg(psi + ix_cc(g, i, j, k0)) : 0.;
-  constexpr int B = RESID ? 2 : kBPlanes;
+  double uzk = ldg(uz + ix_cc(g, i, j, k0));  // uz at the current plane
+  constexpr int B = kBPlanes;
+  double x0[B], x1[B], y0[B], y1[B], zp[B];
+#pragma unroll
+  for (int h = 0; h < B; h++) {
+    const int k = min(k0 + h, nz);
+    x0[h] = ldg(ux + ix_ux(g, i, j, k));
+    x1[h] = ldg(ux + ix_ux(g, i + 1, j, k));
+    y0[h] = ldg(uy + ix_cc(g, i, j, k));
+    y1[h] = ldg(uy + ix_cc(g, i, j + 1, k));
+    zp[h] = ldg(uz + ix_cc(g, i, j, k + 1));
+  }
+#pragma unroll
+  for (int h = 0; h < B; h++) {
+    const int k = k0 + h;
+    if (k > nz) break;
+    const double div = +(x1[h] - x0[h]) / dx + (y1[h] - y0[h]) / g.dy + (zp[h] - uzk) / g.dz;
+    uzk = zp[h];
+    bo[bplane * (k - 1)] = prefactor * div;
+  }
+}
+
+// the residual of the mixed path's second pass, in place: b - A psi / (ny nz)
+// from the first pass's right-hand side b (still in the scratch) and the first
+// solution psi, FP64: one thread per (i, j) walking kBPlanes planes, psi at
+// k, k + 1 carried to the next plane
+__global__ void __launch_bounds__(256, 4) k3_pois_resid(const double *__restrict__ psi,
+                                                        const double *__restrict__ pl,
+                                                        const double *__restrict__ pu, double *__restrict__ b,
+                                                        Grid3 g) {
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k0 = 1 + blockIdx.z * kBPlanes;
+  if (i > nx || j > ny || k0 > nz) return;
+  const double l = ldg(pl + i - 1), u = ldg(pu + i - 1);
+  const double dy2 = g.dy * g.dy, dz2 = g.dz * g.dz, nn = 1. * g.ny * g.nz;
+  double *bo = b + (i - 1) + (size_t)nx * (j - 1);
+  const size_t bplane = (size_t)nx * ny;
+  double pkm = ldg(psi + ix_cc(g, i, j, k0 - 1)), pk = ldg(psi + ix_cc(g, i, j, k0));
+  constexpr int B = 2;
 #pragma unroll
   for (int kb = 0; kb < kBPlanes; kb += B) {
-    double x0[B], x1[B], y0[B], y1[B], zp[B], pxm[B], pxp[B], pym[B], pyp[B], pzp[B];
+    double bb[B], pxm[B], pxp[B], pym[B], pyp[B], pzp[B];
 #pragma unroll
     for (int h = 0; h < B; h++) {
       const int k = min(k0 + kb + h, nz);
-      x0[h] = ldg(ux + ix_ux(g, i, j, k));
-      x1[h] = ldg(ux + ix_ux(g, i + 1, j, k));
-      y0[h] = ldg(uy + ix_cc(g, i, j, k));
-      y1[h] = ldg(uy + ix_cc(g, i, j + 1, k));
-      zp[h] = ldg(uz + ix_cc(g, i, j, k + 1));
-      if (RESID) {
-        pxm[h] = ldg(psi + ix_cc(g, i - 1, j, k));
-        pxp[h] = ldg(psi + ix_cc(g, i + 1, j, k));
-        pym[h] = ldg(psi + ix_cc(g, i, j - 1, k));
-        pyp[h] = ldg(psi + ix_cc(g, i, j + 1, k));
-        pzp[h] = ldg(psi + ix_cc(g, i, j, k + 1));
-      }
+      bb[h] = bo[bplane * (k - 1)];
+      pxm[h] = ldg(psi + ix_cc(g, i - 1, j, k));
+      pxp[h] = ldg(psi + ix_cc(g, i + 1, j, k));
+      pym[h] = ldg(psi + ix_cc(g, i, j - 1, k));
+      pyp[h] = ldg(psi + ix_cc(g, i, j + 1, k));
+      pzp[h] = ldg(psi + ix_cc(g, i, j, k + 1));
     }
 #pragma unroll
     for (int h = 0; h < B; h++) {
       const int k = k0 + kb + h;
       if (k > nz) break;
-      RhsTerms<RESID> t;
-      t.dux = x1[h] - x0[h];
-      t.duy = y1[h] - y0[h];
-      t.duz = zp[h] - uzk;
-      uzk = zp[h];
-      if constexpr (RESID) {
-        const double c = pk;
-        t.ax = l * pxm[h] + (-l - u) * c + u * pxp[h];
-        t.ty = pym[h] - 2. * c + pyp[h];
-        t.tz = pkm - 2. * c + pzp[h];
-        pkm = pk;
-        pk = pzp[h];
-      }
-      bo[bplane * (k - 1)] = rhs_value<RESID>(t, dx, g, prefactor, gdt);
+      const double c = pk;
+      const double ap = (l * pxm[h] + (-l - u) * c + u * pxp[h]) + (pym[h] - 2. * c + pyp[h]) / dy2 +
+                        (pkm - 2. * c + pzp[h]) / dz2;
+      pkm = pk;
+      pk = pzp[h];
+      bo[bplane * (k - 1)] = bb[h] - ap / nn;
     }
   }
 }
@@ -648,9 +623,10 @@ cudaError_t pois_fwd_y(bool resid, cudaStream_t st, const double *ux, const doub
                        const double *dtp, double gam, int log2n, Grid3 g) {
   const dim3 bb(32, 8), bg((g.nx + 31) / 32, (g.ny + 7) / 8, (g.nz + kBPlanes - 1) / kBPlanes);
   if (resid) {
-    k3_pois_b<true><<<bg, bb, 0, st>>>(ux, uy, uz, psi, pl, pu, b, dtp, gam, g);
+    // the first pass's right-hand side is still in b
+    k3_pois_resid<<<bg, bb, 0, st>>>(psi, pl, pu, b, g);
   } else {
-    k3_pois_b<false><<<bg, bb, 0, st>>>(ux, uy, uz, psi, pl, pu, b, dtp, gam, g);
+    k3_pois_b<<<bg, bb, 0, st>>>(ux, uy, uz, b, dtp, gam, g);
   }
   cudaError_t e = cudaGetLastError();
   if (cudaSuccess != e) return e;

@@ -146,10 +146,11 @@ __global__ void k3_tdm_coef(const double *__restrict__ lap_ux, const double *__r
 // Poisson stages (k3_poisson.cu), templates on R = double (FP64 path) or float
 // (mixed path): R is the type of the spectrum, the twiddles and the transform
 // arithmetic; the x line solve is FP64.  The transforms are compiled for each
-// length 2^1 .. 2^11 (log2n outside that range is an invalid value), one warp
-// per line.  resid: transform the residual b - A psi instead of b; accum:
-// psi += the inverse; pin_gauge: zero the last unknown of the singular
-// (ky, kz) = (0, 0) line.
+// length 2^1 .. 2^11 (log2n outside that range is an invalid value).
+// resid: transform the residual b - A psi of the current psi instead of b,
+// formed in place from the b of the previous (first) pass, which must still
+// be in the scratch; accum: psi += the inverse; pin_gauge: zero the last
+// unknown of the singular (ky, kz) = (0, 0) line.
 template <class R>
 cudaError_t pois_prepare(int log2ny, int log2nz);
 // (b: scratch of nx ny nz doubles for the right-hand side)
