@@ -258,9 +258,14 @@ constexpr int RX = 32, RY = 8, RZ = 16;
 constexpr int WX = RX + 2, WY = RY + 2, NSLOT = 4, NFLD = 5, NCEN = 7;
 // the state windows (FP64) and the per-cell inputs ifrcx / ifrcy / ifrcz and
 // src_b of the four fields (R; sized for FP64)
-constexpr size_t kRhsSmem = sizeof(double) * (NFLD * NSLOT * WY * WX + NCEN * NSLOT * RY * RX);
-
-size_t rhs_smem_bytes() { return kRhsSmem; }
+// FP64: the per-cell inputs are read straight from global memory (they are
+// used by their own thread only, and the FP64 kernel runs faster without
+// their ring); FP32 (mixed): they ride the ring with the state planes
+template <class R>
+constexpr bool kRhsDirect = 8 == sizeof(R);
+template <class R>
+constexpr size_t kRhsSmem =
+    sizeof(double) * (NFLD * NSLOT * WY * WX + (kRhsDirect<R> ? 0 : NCEN * NSLOT * RY * RX));
 
 template <class R>
 __global__ void __launch_bounds__(RX * RY, 2) k3_rhs(Predict3Args<R> a) {
@@ -283,7 +288,7 @@ __global__ void __launch_bounds__(RX * RY, 2) k3_rhs(Predict3Args<R> a) {
   auto load_plane = [&](int kk) {
     const int slot = kk & (NSLOT - 1);
     // per-cell inputs of the interior planes: thread (tx, ty) copies its own
-    if (kk >= k0 && kk < kend && mine) {
+    if (!kRhsDirect<R> && kk >= k0 && kk < kend && mine) {
       const long is = ix_src(g, i, j, kk);
       const long isx = (long)(i - 1) + (long)(nx - 1) * ((long)(j - 1) + (long)ny * (kk - 1));  // face i + 1
       for (int q = 0; q < ncen; q++) {
@@ -336,6 +341,20 @@ __global__ void __launch_bounds__(RX * RY, 2) k3_rhs(Predict3Args<R> a) {
   for (int k = k0; k < kend; k++) {
     if (k + 2 <= min(kend, nz + 1)) load_plane(k + 2);
     if (mine) {
+      // FP64: the per-cell inputs from global memory, issued first
+      double ifx_v = 0., ify_v = 0., ifz_v = 0., sbv[4] = {0., 0., 0., 0.};
+      if constexpr (kRhsDirect<R>) {
+        const long is_ = ix_src(g, i, j, k), isx_ = ix_srcx(g, i + 1, j, k);
+        ifx_v = do_ux ? (double)__ldg(a.ifrcx + isx_) : 0.;
+        ify_v = (double)__ldg(a.ifrcy + is_);
+        ifz_v = (double)__ldg(a.ifrcz + is_);
+        if (a.use_b) {
+          sbv[0] = do_ux ? (double)__ldg(a.sb[0] + isx_) : 0.;
+          sbv[1] = (double)__ldg(a.sb[1] + is_);
+          sbv[2] = (double)__ldg(a.sb[2] + is_);
+          sbv[3] = (double)__ldg(a.sb[3] + is_);
+        }
+      }
       const int sm = (k - 1) & (NSLOT - 1), s0 = k & (NSLOT - 1), sp = (k + 1) & (NSLOT - 1);
 #define RING(f, slot, r, c) ring[(((size_t)(f) * NSLOT + (slot)) * WY + (r)) * WX + (c)]
       Stencil4 S;
@@ -382,9 +401,15 @@ __global__ void __launch_bounds__(RX * RY, 2) k3_rhs(Predict3Args<R> a) {
 #undef RING
       const long is = ix_src(g, i, j, k);
 #define CEN(q) (double)cen[((size_t)((q) * NSLOT + s0) * RY + ty) * RX + tx]
-      S.ify = CEN(1);
-      S.ifz = CEN(2);
-      S.ifx = do_ux ? CEN(0) : 0.;
+      if constexpr (kRhsDirect<R>) {
+        S.ify = ify_v;
+        S.ifz = ifz_v;
+        S.ifx = ifx_v;
+      } else {
+        S.ify = CEN(1);
+        S.ifz = CEN(2);
+        S.ifx = do_ux ? CEN(0) : 0.;
+      }
       S.dxf_i = dxf_i;
       S.dxf_i1 = dxf_i1;
       S.dxc_i1 = dxc_i1;
@@ -401,13 +426,13 @@ __global__ void __launch_bounds__(RX * RY, 2) k3_rhs(Predict3Args<R> a) {
       if (do_ux) {
         const long isx = ix_srcx(g, i + 1, j, k);
         a.sa[0][isx] = R(sa[0]);
-        const double sb = a.use_b ? cb * CEN(3) : 0.;
+        const double sb = a.use_b ? cb * (kRhsDirect<R> ? sbv[0] : CEN(3)) : 0.;
         dl[0] = R(+ca * sa[0] + sb + cg * sg[0]);
       }
 #pragma unroll
       for (int q = 1; q < 4; q++) {
         a.sa[q][is] = R(sa[q]);
-        const double sb = a.use_b ? cb * CEN(3 + q) : 0.;
+        const double sb = a.use_b ? cb * (kRhsDirect<R> ? sbv[q] : CEN(3 + q)) : 0.;
         dl[q * fstride] = R(+ca * sa[q] + sb + cg * sg[q]);
       }
 #undef CEN
@@ -609,7 +634,7 @@ template <class R>
 cudaError_t predict_launch(cudaStream_t st, const Predict3Args<R> &a) {
   const Grid3 &g = a.g;
   dim3 gr((g.nx + RX - 1) / RX, (g.ny + RY - 1) / RY, (g.nz + RZ - 1) / RZ);
-  k3_rhs<R><<<gr, RX * RY, kRhsSmem, st>>>(a);
+  k3_rhs<R><<<gr, RX * RY, kRhsSmem<R>, st>>>(a);
   cudaError_t e = cudaGetLastError();
   if (cudaSuccess != e) return e;
   const long nlines = (long)g.ny * g.nz;
@@ -618,9 +643,9 @@ cudaError_t predict_launch(cudaStream_t st, const Predict3Args<R> &a) {
 }
 
 cudaError_t predict_prepare() {
-  cudaError_t e = cudaFuncSetAttribute(k3_rhs<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRhsSmem);
+  cudaError_t e = cudaFuncSetAttribute(k3_rhs<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRhsSmem<double>);
   if (cudaSuccess != e) return e;
-  return cudaFuncSetAttribute(k3_rhs<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRhsSmem);
+  return cudaFuncSetAttribute(k3_rhs<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRhsSmem<float>);
 }
 template cudaError_t predict_launch<double>(cudaStream_t, const Predict3Args<double> &);
 template cudaError_t predict_launch<float>(cudaStream_t, const Predict3Args<float> &);
