@@ -253,13 +253,22 @@ def run_reference_arm(args, wl, ic, env, rank):
 
 
 def _max_over_ranks(x: float, world: int) -> float:
+    """the maximum of x over the ranks (a device tensor under NCCL, a host
+    tensor under gloo)"""
     if world <= 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], device="cuda", dtype=torch.float64)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], device=dev, dtype=torch.float64)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def _aggregate(cells: int, steps: int, world: int, total_ms: float) -> float:
+    """whole-job Mcell-steps/s of `world` replicas, each `cells` cells for
+    `steps` steps, over the slowest rank's device time"""
+    return world * cells * steps / (total_ms * 1e-3) / 1e6
 
 
 def _timed_steps(solver, steps, world, local_rank, flush=None):
@@ -357,7 +366,7 @@ def run3d(args, wl, ic, env, world, rank, local_rank):
         alg = ALG_BYTES_3D_MIXED if prec == "mixed" else {k: 8.0 * v for k, v in ALG_WORDS_3D.items()}
         step_alg = sum(alg[k] * (v[1] / 3) / KERNELS_PER_KIND_3D.get(k, 1) for k, v in prof.items())
         res[prec] = dict(total_ms=total_ms, clocks=clocks, diag=diag, fields=fields, prof=prof,
-                         value=world * cells * args.steps / (total_ms * 1e-3) / 1e6,
+                         value=_aggregate(cells, args.steps, world, total_ms),
                          roofline=_roofline(prof, alg, cells, 3), step_alg_bytes=step_alg)
         if prec == "mixed":
             # end to end through the C ABI with host buffers: the restart
@@ -531,7 +540,7 @@ def main():
         dist.barrier()
     step_ms = [s_.elapsed_time(e_) for s_, e_ in zip(starts, ends)]
     total_ms = _max_over_ranks(float(sum(step_ms)), world)
-    value = world * cells * args.steps / (total_ms * 1e-3) / 1e6
+    value = _aggregate(cells, args.steps, world, total_ms)
     clocks = clk.summary()
 
     # ---- end to end through the C ABI with host buffers: the restart fields
