@@ -32,7 +32,7 @@ def _rank(rank, world, port, out):
 
 @pytest.mark.parametrize("world", [2])
 def test_replica_timing_is_the_max_over_ranks(world):
-    out = mp.Manager().dict()
+    out = mp.get_context("spawn").Manager().dict()  # (no fork: the parent may hold a CUDA context)
     mp.spawn(_rank, args=(world, _free_port(), out), nprocs=world, join=True)
     slowest = 100.0 + 10.0 * (world - 1)
     for r in range(world):
