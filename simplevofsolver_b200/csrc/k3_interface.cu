@@ -167,7 +167,7 @@ __device__ __forceinline__ void load_normal(const float *__restrict__ normal, lo
 // plane, marching over G3Z planes; shared memory holds two vof planes
 // (34 x 6, FP64) and two planes of corner normals (33 x 5 x 3, R).  The vof
 // differences are taken in FP64 and then carried in R.
-constexpr int G3X = 32, G3Y = 4, G3Z = 8;
+constexpr int G3X = 32, G3Y = 4, G3Z = 16;
 
 template <class R>
 __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ vof, R *__restrict__ normal,
@@ -432,7 +432,7 @@ __device__ __forceinline__ double face_flux(double vel, double vlo, double vhi, 
 // plane.  Writes vof_new with its halo images (two layers) and zero x walls,
 // and src_a.  The flux divergence and the update are FP64 in both
 // precisions, so that the update conserves volume to FP64 round-off.
-constexpr int AX = 32, AY = 8, AZ = 16, AWX = AX + 2, AWY = AY + 2, ASLOT = 4;
+constexpr int AX = 32, AY = 8, AZ = 32, AWX = AX + 2, AWY = AY + 2, ASLOT = 4;
 constexpr int kVofRing = ASLOT * AWY * AWX, kUxRing = ASLOT * AY * (AX + 1), kUyRing = ASLOT * (AY + 1) * AX;
 constexpr int kUzRing = ASLOT * AY * AX, kSbRing = ASLOT * AY * AX;
 constexpr size_t kAdvectSmem =
