@@ -167,7 +167,7 @@ __device__ __forceinline__ void load_normal(const float *__restrict__ normal, lo
 // plane, marching over G3Z planes; shared memory holds two vof planes
 // (34 x 6, FP64) and two planes of corner normals (33 x 5 x 3, R).  The vof
 // differences are taken in FP64 and then carried in R.
-constexpr int G3X = 32, G3Y = 4, G3Z = 16;
+constexpr int G3X = 32, G3Y = 4, G3Z = 32;
 
 template <class R>
 __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ vof, R *__restrict__ normal,

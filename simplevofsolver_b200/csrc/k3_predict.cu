@@ -254,7 +254,7 @@ __device__ __forceinline__ void rhs4_values(const Predict3Args<R> &a, const Grid
 // Writes src_a and the increment delta = dt (alpha src_a + beta src_b +
 // gamma src_g) in the line layout [field][j - 1 + ny (k - 1)][x position]
 // that the line solver reads.
-constexpr int RX = 32, RY = 8, RZ = 32;
+constexpr int RX = 32, RY = 8, RZ = 64;
 constexpr int WX = RX + 2, WY = RY + 2, NSLOT = 4, NFLD = 5, NCEN = 7;
 // the state windows (FP64) and the per-cell inputs ifrcx / ifrcy / ifrcz and
 // src_b of the four fields (R; sized for FP64)
