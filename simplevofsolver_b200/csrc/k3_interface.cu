@@ -338,7 +338,7 @@ __global__ void __launch_bounds__(256) k3_intercept(const double *__restrict__ v
 // k3_force: one thread per interior (i, j) and kForcePlanes planes k (vof and
 // curvature at k - 1 carried from the previous plane, the loads of the
 // thread's planes issued before its arithmetic); FP64 arithmetic, R output
-constexpr int kForcePlanes = 4;
+constexpr int kForcePlanes = 8;
 template <class R>
 __global__ void __launch_bounds__(256) k3_force(const double *__restrict__ vof, const R *__restrict__ curv,
                                                 R *__restrict__ ifrcx, R *__restrict__ ifrcy, R *__restrict__ ifrcz,
