@@ -20,7 +20,9 @@
  *   ifrcy, ifrcz, srcuy_*, srcuz_*, srct_*, src_*   nz x ny x nx
  *
  * Every function returns 0 on success and non-zero on failure, with a message
- * in svof3d_last_error().  All device work runs on the solver's own stream.
+ * in svof3d_last_error().  All device work runs on the solver's own stream,
+ * except the host copies of the queued loads and stores, which run on two
+ * copy streams the solver makes for them.
  * A solver is not reentrant: one host thread drives it at a time.
  */
 #ifndef SVOF3D_B200_H
@@ -119,6 +121,25 @@ int svof3d_device_field(svof3d_solver_t *s, int field, double **dptr);
  * loading applies the field's halo and wall update */
 int svof3d_load_interior(svof3d_solver_t *s, int field, const double *host, size_t count);
 int svof3d_store_interior(svof3d_solver_t *s, int field, double *host, size_t count);
+
+/* Queued forms of the two calls above, for streaming restart states through
+ * one solver (load, enqueue steps, store, repeat) without waiting in between.
+ * Each call returns once its copy is queued; in device order it sits after
+ * the steps queued before it and before the steps queued after it.  The host
+ * copy runs on a copy stream of its own (one per direction) through a
+ * staging buffer in device memory, so host-to-device copies, device-to-host
+ * copies and steps overlap; the host buffer must be page-locked for that and
+ * must stay valid, and a load's buffer unchanged, until svof3d_io_wait()
+ * returns.  The staging buffers (one per field and direction, restart-layout
+ * size) are made on first use and freed by svof3d_destroy().  The restart
+ * files they stand in for are read by fluid_init / interface_init and
+ * written by fluid_save / interface_save (src/fluid/init.c:72,
+ * src/fluid/save.c:8, src/interface/init.c:55, src/interface/save.c:7),
+ * called from src/main.c:29-30 and src/main.c:78-82. */
+int svof3d_load_interior_async(svof3d_solver_t *s, int field, const double *host, size_t count);
+int svof3d_store_interior_async(svof3d_solver_t *s, int field, double *host, size_t count);
+/* waits for every queued load, step and store */
+int svof3d_io_wait(svof3d_solver_t *s);
 
 /* the step functions; rkstep in 0 .. 2 */
 int svof3d_fluid_decide_dt(svof3d_solver_t *s, double *dt);

@@ -124,6 +124,16 @@ struct svof3d_solver {
   // interfacial-cell worklist of the geometry kernels
   unsigned *d_work = nullptr, *d_nwork = nullptr;
   std::map<int, cudaGraphExec_t> graphs;
+  // queued restart-layout copies: a compact staging buffer per field and
+  // direction, a copy stream per direction; `filled` marks a buffer written,
+  // `drained` a buffer read, so that a reuse waits for the previous copy
+  struct IoSlot {
+    double *stage = nullptr;
+    cudaEvent_t filled = nullptr, drained = nullptr;
+    bool pending = false;
+  };
+  cudaStream_t io_h2d = nullptr, io_d2h = nullptr;
+  IoSlot io_in[SVOF3_NFIELDS], io_out[SVOF3_NFIELDS];
 
   Grid3 grid() const { return Grid3{nx, ny, nz, dy, dz, dxf.p, dxc.p}; }
 };
@@ -375,6 +385,34 @@ int interior_layout(const svof3d_solver *s, int field, int *nh, int *width) {
   }
 }
 
+// staging buffer of `count` doubles and its events, made on first use
+int io_slot(svof3d_solver *s, svof3d_solver::IoSlot &q, size_t count) {
+  if (!s->io_h2d) CK(cudaStreamCreateWithFlags(&s->io_h2d, cudaStreamNonBlocking));
+  if (!s->io_d2h) CK(cudaStreamCreateWithFlags(&s->io_d2h, cudaStreamNonBlocking));
+  if (!q.stage) {
+    CK(cudaMalloc(&q.stage, sizeof(double) * count));
+    CK(cudaEventCreateWithFlags(&q.filled, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&q.drained, cudaEventDisableTiming));
+  }
+  return 0;
+}
+
+void io_free(svof3d_solver *s) {
+  if (s->io_h2d) cudaStreamSynchronize(s->io_h2d);
+  if (s->io_d2h) cudaStreamSynchronize(s->io_d2h);
+  for (int f = 0; f < SVOF3_NFIELDS; f++) {
+    for (svof3d_solver::IoSlot *q : {&s->io_in[f], &s->io_out[f]}) {
+      if (q->stage) cudaFree(q->stage);
+      if (q->filled) cudaEventDestroy(q->filled);
+      if (q->drained) cudaEventDestroy(q->drained);
+      *q = svof3d_solver::IoSlot{};
+    }
+  }
+  if (s->io_h2d) cudaStreamDestroy(s->io_h2d);
+  if (s->io_d2h) cudaStreamDestroy(s->io_d2h);
+  s->io_h2d = s->io_d2h = nullptr;
+}
+
 int build_tables(svof3d_solver *s, const double *xf, const double *xc) {
   const int nx = s->nx, ny = s->ny, nz = s->nz;
   std::vector<double> dxf(nx), dxc(nx + 1);
@@ -462,6 +500,7 @@ const char *svof3d_last_error(void) { return g_err3.c_str(); }
 int svof3d_destroy(svof3d_solver_t *s) {
   if (!s) return 0;
   if (s->stream) cudaStreamSynchronize(s->stream);
+  io_free(s);
   for (auto &kv : s->graphs) cudaGraphExecDestroy(kv.second);
   s->graphs.clear();
   for (int k = 0; k < 2; k++) {
@@ -645,6 +684,66 @@ int svof3d_store_interior(svof3d_solver_t *s, int field, double *host, size_t co
   const double *src = b->p + (size_t)width * (s->ny + 2 * nh) * nh + (size_t)width * nh;
   CK(cudaMemcpy2DAsync(host, dpitch, src, spitch, dpitch, s->nz, cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+// queued load: host -> staging on the copy-in stream (one contiguous copy),
+// then staging -> storage and the halo update on the solver's stream, in
+// order with the steps queued around it
+int svof3d_load_interior_async(svof3d_solver_t *s, int field, const double *host, size_t count) {
+  int nh, width;
+  DevBuf *b;
+  if (!s || !host) return fail("null argument");
+  if (interior_layout(s, field, &nh, &width) || field_buf(s, field, &b)) return 1;
+  const size_t plane = (size_t)width * s->ny;
+  if (count != plane * s->nz) return fail("field %d: restart layout holds %zu doubles, got %zu", field,
+                                          plane * s->nz, count);
+  svof3d_solver::IoSlot &q = s->io_in[field];
+  if (io_slot(s, q, count)) return 1;
+  if (q.pending) CK(cudaStreamWaitEvent(s->io_h2d, q.drained, 0));
+  CK(cudaMemcpyAsync(q.stage, host, sizeof(double) * count, cudaMemcpyHostToDevice, s->io_h2d));
+  CK(cudaEventRecord(q.filled, s->io_h2d));
+  CK(cudaStreamWaitEvent(s->stream, q.filled, 0));
+  const size_t spitch = sizeof(double) * plane;
+  const size_t dpitch = sizeof(double) * (size_t)width * (s->ny + 2 * nh);
+  double *dst = b->p + (size_t)width * (s->ny + 2 * nh) * nh + (size_t)width * nh;
+  CK(cudaMemcpy2DAsync(dst, dpitch, q.stage, spitch, spitch, s->nz, cudaMemcpyDeviceToDevice, s->stream));
+  if (launch_halo_bc(s, b->p, field)) return 1;
+  CK(cudaEventRecord(q.drained, s->stream));
+  q.pending = true;
+  return 0;
+}
+
+// queued store: storage -> staging on the solver's stream, then staging ->
+// host on the copy-out stream (one contiguous copy)
+int svof3d_store_interior_async(svof3d_solver_t *s, int field, double *host, size_t count) {
+  int nh, width;
+  DevBuf *b;
+  if (!s || !host) return fail("null argument");
+  if (interior_layout(s, field, &nh, &width) || field_buf(s, field, &b)) return 1;
+  const size_t plane = (size_t)width * s->ny;
+  if (count != plane * s->nz) return fail("field %d: restart layout holds %zu doubles, got %zu", field,
+                                          plane * s->nz, count);
+  svof3d_solver::IoSlot &q = s->io_out[field];
+  if (io_slot(s, q, count)) return 1;
+  if (q.pending) CK(cudaStreamWaitEvent(s->stream, q.drained, 0));
+  const size_t dpitch = sizeof(double) * plane;
+  const size_t spitch = sizeof(double) * (size_t)width * (s->ny + 2 * nh);
+  const double *src = b->p + (size_t)width * (s->ny + 2 * nh) * nh + (size_t)width * nh;
+  CK(cudaMemcpy2DAsync(q.stage, dpitch, src, spitch, dpitch, s->nz, cudaMemcpyDeviceToDevice, s->stream));
+  CK(cudaEventRecord(q.filled, s->stream));
+  CK(cudaStreamWaitEvent(s->io_d2h, q.filled, 0));
+  CK(cudaMemcpyAsync(host, q.stage, sizeof(double) * count, cudaMemcpyDeviceToHost, s->io_d2h));
+  CK(cudaEventRecord(q.drained, s->io_d2h));
+  q.pending = true;
+  return 0;
+}
+
+int svof3d_io_wait(svof3d_solver_t *s) {
+  if (!s) return fail("null argument");
+  if (s->io_h2d) CK(cudaStreamSynchronize(s->io_h2d));
+  CK(cudaStreamSynchronize(s->stream));
+  if (s->io_d2h) CK(cudaStreamSynchronize(s->io_d2h));
   return 0;
 }
 

@@ -38,6 +38,7 @@ FIELDS3D = {"ux": 0, "uy": 1, "uz": 2, "p": 3, "t": 4, "vof": 5, "psi": 6, "curv
 
 EXPORTS3D = ["svof3d_create", "svof3d_destroy", "svof3d_field_count", "svof3d_upload_field",
              "svof3d_download_field", "svof3d_device_field", "svof3d_load_interior", "svof3d_store_interior",
+             "svof3d_load_interior_async", "svof3d_store_interior_async", "svof3d_io_wait",
              "svof3d_fluid_decide_dt", "svof3d_interface_compute_curvature_tensor",
              "svof3d_interface_compute_force", "svof3d_interface_update_vof", "svof3d_fluid_predict_field",
              "svof3d_fluid_compute_potential_dft", "svof3d_fluid_correct_velocity",
@@ -78,8 +79,10 @@ def lib3() -> ctypes.CDLL:
         L.svof3d_create.argtypes = [ctypes.POINTER(Params3D), dp, dp, ctypes.POINTER(vp)]
         L.svof3d_destroy.argtypes = [vp]
         L.svof3d_field_count.argtypes = [vp, i, ctypes.POINTER(sz)]
-        for fn in ("svof3d_upload_field", "svof3d_download_field", "svof3d_load_interior", "svof3d_store_interior"):
+        for fn in ("svof3d_upload_field", "svof3d_download_field", "svof3d_load_interior", "svof3d_store_interior",
+                   "svof3d_load_interior_async", "svof3d_store_interior_async"):
             getattr(L, fn).argtypes = [vp, i, dp, sz]
+        L.svof3d_io_wait.argtypes = [vp]
         L.svof3d_device_field.argtypes = [vp, i, ctypes.POINTER(vp)]
         L.svof3d_fluid_decide_dt.argtypes = [vp, pd]
         L.svof3d_interface_compute_curvature_tensor.argtypes = [vp]
@@ -129,6 +132,7 @@ class Solver3D:
                                float(uy_walls[0]), float(uy_walls[1]), float(uz_walls[0]), float(uz_walls[1]),
                                float(t_walls[0]), float(t_walls[1]), MIXED if precision == "mixed" else FP64)
         self._h = ctypes.c_void_p()
+        self._io_held = []
         xf, xc = _c(ic.xf), _c(ic.xc)
         self._grid = (float(ic.lx), float(ic.ly), float(ic.lz), xf.copy(), xc.copy())
         _check(L.svof3d_create(ctypes.byref(self.params), xf.ctypes.data, xc.ctypes.data, ctypes.byref(self._h)))
@@ -175,8 +179,9 @@ class Solver3D:
 
     def close(self):
         if getattr(self, "_h", None) and self._h.value:
-            lib3().svof3d_destroy(self._h)
+            lib3().svof3d_destroy(self._h)  # waits for queued copies first
             self._h = ctypes.c_void_p()
+            self._io_held = []
 
     def __del__(self):
         try:
@@ -215,6 +220,31 @@ class Solver3D:
         out = np.empty(interior_shape3d(name, self.nx, self.ny, self.nz))
         _check(lib3().svof3d_store_interior(self._h, FIELDS3D[name], out.ctypes.data, out.size))
         return out
+
+    def load_interior_async(self, name: str, a: np.ndarray):
+        """Queue a restart-layout load; `a` (page-locked for overlap) is held
+        until io_wait()."""
+        a = _c(a)
+        want = interior_shape3d(name, self.nx, self.ny, self.nz)
+        if a.shape != want:
+            raise ValueError(f"{name}: expected shape {want}, got {a.shape}")
+        _check(lib3().svof3d_load_interior_async(self._h, FIELDS3D[name], a.ctypes.data, a.size))
+        self._io_held.append(a)
+
+    def store_interior_async(self, name: str, out: np.ndarray):
+        """Queue a restart-layout store into `out`, a C-contiguous float64
+        array of the field's restart shape, complete after io_wait()."""
+        want = interior_shape3d(name, self.nx, self.ny, self.nz)
+        if (not isinstance(out, np.ndarray) or out.dtype != np.float64 or out.shape != want
+                or not out.flags.c_contiguous or not out.flags.writeable):
+            raise ValueError(f"{name}: expected a writeable C-contiguous float64 array of shape {want}")
+        _check(lib3().svof3d_store_interior_async(self._h, FIELDS3D[name], out.ctypes.data, out.size))
+        self._io_held.append(out)
+
+    def io_wait(self):
+        """Wait for every queued load, step and store."""
+        _check(lib3().svof3d_io_wait(self._h))
+        self._io_held.clear()
 
     def device_ptr(self, name: str) -> int:
         p = ctypes.c_void_p()
