@@ -162,6 +162,38 @@ int svof3d_last_dt(svof3d_solver_t *s, double *dt);
 
 /* max |div u| over the interior cells, vof min / max and total volume sum(vof dx dy dz) */
 int svof3d_diagnostics(svof3d_solver_t *s, double *divmax, double *vofmin, double *vofmax, double *volume);
+/* Time-averaged statistics on the device, the 2D collection of
+ * src/statistics.c:117-204 carried to 3D (the reference's 3D statistics code
+ * is not in the mounted sources): each svof3d_statistics_collect() adds one
+ * sample of the current fields, queued on the solver's stream,
+ *   ux1 += ux, ux2 += ux^2, uy1 += uy, uy2 += uy^2, uz1 += uz, uz2 += uz^2,
+ *   t1 += t, t2 += t^2, uxt += ux (t(i-1) + t(i)) / 2
+ * over the interior rows (j = 1 .. ny, k = 1 .. nz), i = 1 .. nx+1 for ux1
+ * ux2 uxt and i = 0 .. nx+1 for the others; arrays nz x ny x (nx+1) or
+ * nz x ny x (nx+2), no halo.  Squares are the correctly rounded products. */
+enum {
+  SVOF3_STAT_UX1 = 0,
+  SVOF3_STAT_UX2,
+  SVOF3_STAT_UY1,
+  SVOF3_STAT_UY2,
+  SVOF3_STAT_UZ1,
+  SVOF3_STAT_UZ2,
+  SVOF3_STAT_T1,
+  SVOF3_STAT_T2,
+  SVOF3_STAT_UXT,
+  SVOF3_NSTATS
+};
+int svof3d_statistics_collect(svof3d_solver_t *s);
+int svof3d_statistics_reset(svof3d_solver_t *s);
+int svof3d_statistics_count(svof3d_solver_t *s, size_t *num);
+/* the reduction of reduce_and_write (src/statistics.c:232-281) over y and z:
+ * out[i] = sum over k = 1 .. nz, in order from zero, of the plane sums (each
+ * the sum over j = 1 .. ny, in order from zero) at column i; count = nx+1
+ * (ux1 ux2 uxt) or nx+2 */
+int svof3d_statistics_reduce(svof3d_solver_t *s, int quantity, double *out, size_t count);
+/* the accumulated array itself */
+int svof3d_statistics_field(svof3d_solver_t *s, int quantity, double *out, size_t count);
+
 /* one step launched kernel by kernel with events between; ms[k], launches[k] per kind */
 int svof3d_profile_step(svof3d_solver_t *s, double *ms, int *launches, int nkinds);
 int svof3d_synchronize(svof3d_solver_t *s);

@@ -162,6 +162,41 @@ int svof_diagnostics(svof_solver_t *solver, double *divmax, double *vofmin, doub
  * differ from the reference's sequential sums only by round-off. */
 int svof_logging_quantities(svof_solver_t *solver, double *out, int nout);
 
+/* Time-averaged statistics on the device (src/statistics.c).  Each
+ * svof_statistics_collect() adds one sample of the current fields to FP64
+ * accumulators (collect_mean_ux, collect_mean_uy, collect_mean_t,
+ * collect_uxt, src/statistics.c:117-204), queued on the solver's stream:
+ *   ux1 += ux, ux2 += ux^2, uy1 += uy, uy2 += uy^2, t1 += t, t2 += t^2,
+ *   uxt += ux (t(i-1) + t(i)) / 2
+ * over the interior rows j = 1 .. ny, for i = 1 .. nx+1 (ux1 ux2 uxt) and
+ * i = 0 .. nx+1 (the others), in the reference's statistics layouts
+ * (include/array_macros/statistics/ux1.h .. uxt.h: ny x (nx+1) and
+ * ny x (nx+2), no halo).  The squares are the correctly rounded products;
+ * the reference's pow(x, 2.) is within one unit in the last place of them.
+ * The caller keeps the sampling schedule, as src/main.c:137-140 does.  The
+ * accumulators (7 arrays) are allocated on the first collection. */
+enum {
+  SVOF_STAT_UX1 = 0,
+  SVOF_STAT_UX2,
+  SVOF_STAT_UY1,
+  SVOF_STAT_UY2,
+  SVOF_STAT_T1,
+  SVOF_STAT_T2,
+  SVOF_STAT_UXT,
+  SVOF_NSTATS
+};
+int svof_statistics_collect(svof_solver_t *solver);
+/* zero the accumulators and the sample count */
+int svof_statistics_reset(svof_solver_t *solver);
+/* samples since creation or the last reset (the reference's g_num) */
+int svof_statistics_count(svof_solver_t *solver, size_t *num);
+/* the reduced output of reduce_and_write (src/statistics.c:232-281):
+ * out[i] = sum over the rows j = 1 .. ny, in that order from zero, of the
+ * accumulated quantity at column i; count = nx+1 (ux1 ux2 uxt) or nx+2 */
+int svof_statistics_reduce(svof_solver_t *solver, int quantity, double *out, size_t count);
+/* the accumulated array itself (the unreduced array.dump output) */
+int svof_statistics_field(svof_solver_t *solver, int quantity, double *out, size_t count);
+
 /* kernel kinds of svof_profile_step */
 enum {
   SVOF_K_DT = 0,            /* CFL reduction + dt (2 launches) */

@@ -93,6 +93,10 @@ def _load():
         L.svo_integrate.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
         L.svo_run.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
         L.svo_logging.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.svo_stat_collect.argtypes = [ctypes.c_void_p]
+        L.svo_stat_reduce.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        L.svo_stat_num.argtypes = [ctypes.c_void_p]
+        L.svo_stat_num.restype = ctypes.c_long
         _lib = L
     return _lib
 
@@ -188,6 +192,23 @@ class Oracle:
         _load().svo_logging(self._h, out.ctypes.data)
         return dict(zip(self.LOGGING_NAMES, out.tolist()))
 
+    STAT_NAMES = ["ux1", "ux2", "uy1", "uy2", "t1", "t2", "uxt"]
+
+    def statistics_collect(self):
+        """one sample of src/statistics.c:117-204 (svo_stat_collect)"""
+        _load().svo_stat_collect(self._h)
+
+    def statistics_reduced(self) -> dict:
+        """reduce_and_write's row sums (src/statistics.c:232-281) of every
+        quantity, plus 'num' the number of samples"""
+        out = {}
+        for q, k in enumerate(self.STAT_NAMES):
+            v = np.zeros(self.nx + (1 if k in ("ux1", "ux2", "uxt") else 2))
+            _load().svo_stat_reduce(self._h, q, v.ctypes.data)
+            out[k] = v
+        out["num"] = int(_load().svo_stat_num(self._h))
+        return out
+
 
 # ---------------------------------------------------------------- 3D
 
@@ -250,6 +271,10 @@ def _load3():
             getattr(L, fn).argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double]
         L.svo3_integrate.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
         L.svo3_run.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        L.svo3_stat_collect.argtypes = [ctypes.c_void_p]
+        L.svo3_stat_reduce.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        L.svo3_stat_num.argtypes = [ctypes.c_void_p]
+        L.svo3_stat_num.restype = ctypes.c_long
         _lib3 = L
     return _lib3
 
@@ -338,6 +363,22 @@ class Oracle3D:
         if _load3().svo3_run(self._h, int(nsteps), dts.ctypes.data) != 0:
             raise RuntimeError("svo3_run failed")
         return dts[:nsteps]
+
+    STAT_NAMES = ["ux1", "ux2", "uy1", "uy2", "uz1", "uz2", "t1", "t2", "uxt"]
+
+    def statistics_collect(self):
+        """one sample of the statistics (svo3_stat_collect)"""
+        _load3().svo3_stat_collect(self._h)
+
+    def statistics_reduced(self) -> dict:
+        """the y-z sums of every quantity, plus 'num'"""
+        out = {}
+        for q, k in enumerate(self.STAT_NAMES):
+            v = np.zeros(self.nx + (1 if k in ("ux1", "ux2", "uxt") else 2))
+            _load3().svo3_stat_reduce(self._h, q, v.ctypes.data)
+            out[k] = v
+        out["num"] = int(_load3().svo3_stat_num(self._h))
+        return out
 
 
 # ---------------------------------------------------------------- reference

@@ -59,6 +59,10 @@ struct svo_ctx {
   svof_fft_plan_t *plan_x, *plan_y;
   double *evals_dct, *evals_dft;
   double *plap_l, *plap_u;         /* DFT path x-Laplacian */
+  /* time-averaged statistics (src/statistics.c:40-47): ux1 ux2 uy1 uy2 t1
+   * t2 uxt, allocated on the first collection */
+  double *stat[7];
+  long stat_num;
 };
 
 /* ---------- index maps (reference include/array_macros/) ---------- */
@@ -204,6 +208,8 @@ svo_ctx_t *svo_create(const svo_params_t *prm, const double *xf, const double *x
 }
 
 void svo_destroy(svo_ctx_t *c) {
+  if (c)
+    for (int q = 0; q < 7; q++) free(c->stat[q]);
   if (!c) return;
   double *bufs[] = {c->xf, c->xc, c->dxf, c->dxc, c->ux, c->uy, c->p, c->psi, c->t,
                     c->vof, c->ifrcx, c->ifrcy, c->dvof, c->normal, c->curv, c->flxx, c->flxy,
@@ -1130,3 +1136,60 @@ int svo_logging(svo_ctx_t *c, double out[9]) {
   return 0;
 }
 
+
+/* ---------- time-averaged statistics (src/statistics.c) ---------- */
+
+/* widths of the statistics arrays (array_macros/statistics/ux1.h .. uxt.h): ux1, ux2
+ * and uxt hold i = 1 .. nx+1, the others i = 0 .. nx+1; rows j = 1 .. ny,
+ * no halo */
+static int stat_width(const svo_ctx_t *c, int q) { return (0 == q || 1 == q || 6 == q) ? NX + 1 : NX + 2; }
+
+/* one sample: collect_mean_ux, collect_mean_uy, collect_mean_t and
+ * collect_uxt (src/statistics.c:117-204), pow() as the reference calls it */
+int svo_stat_collect(svo_ctx_t *c) {
+  if (!c->stat[0])
+    for (int q = 0; q < 7; q++) c->stat[q] = dalloc((long)stat_width(c, q) * NY);
+  const double *T = c->t, *UY = c->uy;
+  double *ux1 = c->stat[0], *ux2 = c->stat[1], *uy1 = c->stat[2], *uy2 = c->stat[3];
+  double *t1 = c->stat[4], *t2 = c->stat[5], *uxt = c->stat[6];
+#define SX(a, i, j) (a)[(i) - 1 + (NX + 1) * ((j) - 1)]
+#define SC(a, i, j) (a)[(i) + (NX + 2) * ((j) - 1)]
+  for (int j = 1; j <= NY; j++)
+    for (int i = 1; i <= NX + 1; i++) {
+      SX(ux1, i, j) += pow(UX(i, j), 1.);
+      SX(ux2, i, j) += pow(UX(i, j), 2.);
+    }
+  for (int j = 1; j <= NY; j++)
+    for (int i = 0; i <= NX + 1; i++) {
+      SC(uy1, i, j) += pow(CC(UY, i, j), 1.);
+      SC(uy2, i, j) += pow(CC(UY, i, j), 2.);
+    }
+  for (int j = 1; j <= NY; j++)
+    for (int i = 0; i <= NX + 1; i++) {
+      SC(t1, i, j) += pow(CC(T, i, j), 1.);
+      SC(t2, i, j) += pow(CC(T, i, j), 2.);
+    }
+  for (int j = 1; j <= NY; j++)
+    for (int i = 1; i <= NX + 1; i++) {
+      const double t_ = +0.5 * CC(T, i - 1, j) + 0.5 * CC(T, i, j);
+      SX(uxt, i, j) += UX(i, j) * t_;
+    }
+#undef SX
+#undef SC
+  c->stat_num += 1;
+  return 0;
+}
+
+/* reduce_and_write (src/statistics.c:232-281): out[i] = sum over the rows in
+ * order, starting from zero; out holds stat_width() values */
+int svo_stat_reduce(const svo_ctx_t *c, int q, double *out) {
+  if (q < 0 || q > 6) return 1;
+  const int w = stat_width(c, q);
+  for (int i = 0; i < w; i++) out[i] = 0.;
+  if (!c->stat[0]) return 0;
+  for (int j = 0; j < NY; j++)
+    for (int i = 0; i < w; i++) out[i] += c->stat[q][(long)j * w + i];
+  return 0;
+}
+
+long svo_stat_num(const svo_ctx_t *c) { return c->stat_num; }

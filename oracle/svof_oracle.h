@@ -66,6 +66,12 @@ int svo_run(svo_ctx_t *ctx, int nsteps, double *dts);
  * the wall heat flux, kinetic energy injection, kinetic and thermal energy
  * dissipation} */
 int svo_logging(svo_ctx_t *ctx, double out[9]);
+/* time-averaged statistics (src/statistics.c:117-281): one sample of ux1 ux2
+ * uy1 uy2 t1 t2 uxt (q = 0 .. 6), the row sum of one quantity (nx+1 values
+ * for ux1 ux2 uxt, nx+2 for the others), the number of samples */
+int svo_stat_collect(svo_ctx_t *ctx);
+int svo_stat_reduce(const svo_ctx_t *ctx, int q, double *out);
+long svo_stat_num(const svo_ctx_t *ctx);
 
 #ifdef __cplusplus
 }

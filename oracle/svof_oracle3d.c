@@ -42,6 +42,10 @@ struct svo3_ctx {
   double *line;               /* 2 * max(ny, nz) */
   svof_fft_plan_t *plan_y, *plan_z;
   double *evy, *evz, *pl, *pu;
+  /* time-averaged statistics: ux1 ux2 uy1 uy2 uz1 uz2 t1 t2 uxt, made on the
+   * first collection */
+  double *stat[9];
+  long stat_num;
 };
 
 #define NX (c->nx)
@@ -164,6 +168,8 @@ svo3_ctx_t *svo3_create(const svo3_params_t *prm, const double *xf, const double
 }
 
 void svo3_destroy(svo3_ctx_t *c) {
+  if (c)
+    for (int q = 0; q < 9; q++) free(c->stat[q]);
   if (!c) return;
   double *bufs[] = {c->xf, c->xc, c->dxf, c->dxc, c->ux, c->uy, c->uz, c->p, c->psi, c->t, c->vof,
                     c->ifrcx, c->ifrcy, c->ifrcz, c->dvof, c->normal, c->curv, c->flxx, c->flxy, c->flxz,
@@ -879,3 +885,65 @@ int svo3_run(svo3_ctx_t *c, int nsteps, double *dts) {
   }
   return 0;
 }
+
+/* ---------- time-averaged statistics ---------- */
+
+/* the 2D collection of src/statistics.c:117-204 with a k loop and uz added;
+ * arrays nz x ny x width, no halo, width nx+1 for ux1 ux2 uxt (q = 0, 1, 8)
+ * and nx+2 for the others */
+static int stat_width3(const svo3_ctx_t *c, int q) { return (0 == q || 1 == q || 8 == q) ? NX + 1 : NX + 2; }
+
+int svo3_stat_collect(svo3_ctx_t *c) {
+  if (!c->stat[0])
+    for (int q = 0; q < 9; q++) c->stat[q] = calloc((size_t)stat_width3(c, q) * NY * NZ, sizeof(double));
+  const double *UY = c->uy, *UZ = c->uz, *T = c->t;
+#define SX(a, i, j, k) (a)[(i) - 1 + (long)(NX + 1) * (((j) - 1) + (long)NY * ((k) - 1))]
+#define SC(a, i, j, k) (a)[(i) + (long)(NX + 2) * (((j) - 1) + (long)NY * ((k) - 1))]
+  for (int k = 1; k <= NZ; k++)
+    for (int j = 1; j <= NY; j++)
+      for (int i = 1; i <= NX + 1; i++) {
+        SX(c->stat[0], i, j, k) += pow(UX(i, j, k), 1.);
+        SX(c->stat[1], i, j, k) += pow(UX(i, j, k), 2.);
+      }
+  for (int k = 1; k <= NZ; k++)
+    for (int j = 1; j <= NY; j++)
+      for (int i = 0; i <= NX + 1; i++) {
+        SC(c->stat[2], i, j, k) += pow(CC(UY, i, j, k), 1.);
+        SC(c->stat[3], i, j, k) += pow(CC(UY, i, j, k), 2.);
+        SC(c->stat[4], i, j, k) += pow(CC(UZ, i, j, k), 1.);
+        SC(c->stat[5], i, j, k) += pow(CC(UZ, i, j, k), 2.);
+        SC(c->stat[6], i, j, k) += pow(CC(T, i, j, k), 1.);
+        SC(c->stat[7], i, j, k) += pow(CC(T, i, j, k), 2.);
+      }
+  for (int k = 1; k <= NZ; k++)
+    for (int j = 1; j <= NY; j++)
+      for (int i = 1; i <= NX + 1; i++) {
+        const double t_ = +0.5 * CC(T, i - 1, j, k) + 0.5 * CC(T, i, j, k);
+        SX(c->stat[8], i, j, k) += UX(i, j, k) * t_;
+      }
+#undef SX
+#undef SC
+  c->stat_num += 1;
+  return 0;
+}
+
+/* reduce_and_write (src/statistics.c:232-281) over y and z: the sum over j of
+ * each z plane, in order from zero, then the sum of the planes in z order
+ * from zero */
+int svo3_stat_reduce(const svo3_ctx_t *c, int q, double *out) {
+  if (q < 0 || q > 8) return 1;
+  const int w = stat_width3(c, q);
+  for (int i = 0; i < w; i++) out[i] = 0.;
+  if (!c->stat[0]) return 0;
+  double *plane = calloc((size_t)w, sizeof(double));
+  for (int k = 0; k < NZ; k++) {
+    for (int i = 0; i < w; i++) plane[i] = 0.;
+    for (int j = 0; j < NY; j++)
+      for (int i = 0; i < w; i++) plane[i] += c->stat[q][((long)k * NY + j) * w + i];
+    for (int i = 0; i < w; i++) out[i] += plane[i];
+  }
+  free(plane);
+  return 0;
+}
+
+long svo3_stat_num(const svo3_ctx_t *c) { return c->stat_num; }

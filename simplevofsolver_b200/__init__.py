@@ -55,7 +55,12 @@ EXPORTS = ["svof_create", "svof_destroy", "svof_field_count", "svof_upload_field
            "svof_fluid_compute_potential_dct", "svof_fluid_compute_potential_dft",
            "svof_fluid_correct_velocity", "svof_fluid_update_pressure", "svof_integrate", "svof_run",
            "svof_enqueue_steps", "svof_last_dt",
-           "svof_diagnostics", "svof_profile_step", "svof_synchronize", "svof_stream", "svof_last_error"]
+           "svof_diagnostics", "svof_profile_step", "svof_synchronize", "svof_stream", "svof_last_error",
+           "svof_logging_quantities", "svof_statistics_collect", "svof_statistics_reset",
+           "svof_statistics_count", "svof_statistics_reduce", "svof_statistics_field"]
+
+# statistics quantities (SVOF_STAT_*), in the reference's order (src/statistics.c:41-47)
+STAT_NAMES = ["ux1", "ux2", "uy1", "uy2", "t1", "t2", "uxt"]
 
 
 def storage_shape(name: str, nx: int, ny: int):
@@ -113,6 +118,11 @@ def lib() -> ctypes.CDLL:
         L.svof_last_dt.argtypes = [vp, pd]
         L.svof_diagnostics.argtypes = [vp, pd, pd, pd, pd]
         L.svof_logging_quantities.argtypes = [vp, pd, i]
+        L.svof_statistics_collect.argtypes = [vp]
+        L.svof_statistics_reset.argtypes = [vp]
+        L.svof_statistics_count.argtypes = [vp, ctypes.POINTER(sz)]
+        L.svof_statistics_reduce.argtypes = [vp, i, dp, sz]
+        L.svof_statistics_field.argtypes = [vp, i, dp, sz]
         L.svof_synchronize.argtypes = [vp]
         L.svof_profile_step.argtypes = [vp, dp, dp, i]
         L.svof_stream.argtypes = [vp, ctypes.POINTER(vp)]
@@ -324,6 +334,38 @@ class Solver:
         out = np.zeros(9)
         _check(lib().svof_logging_quantities(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 9))
         return dict(zip(self.LOGGING_NAMES, out.tolist()))
+
+    # ------------------------------------------------- time-averaged statistics
+    def statistics_collect(self):
+        """add one sample of the current fields to the device accumulators
+        (src/statistics.c:117-204); queued, does not wait"""
+        _check(lib().svof_statistics_collect(self._h))
+
+    def statistics_reset(self):
+        _check(lib().svof_statistics_reset(self._h))
+
+    def statistics_count(self) -> int:
+        n = ctypes.c_size_t(0)
+        _check(lib().svof_statistics_count(self._h, ctypes.byref(n)))
+        return int(n.value)
+
+    def statistics_reduced(self) -> dict:
+        """the row sums reduce_and_write writes (src/statistics.c:232-281), one
+        vector per quantity, plus 'num' the number of samples"""
+        out = {}
+        for q, k in enumerate(STAT_NAMES):
+            v = np.zeros(self.nx + (1 if k in ("ux1", "ux2", "uxt") else 2))
+            _check(lib().svof_statistics_reduce(self._h, q, v.ctypes.data, v.size))
+            out[k] = v
+        out["num"] = self.statistics_count()
+        return out
+
+    def statistics_field(self, name: str) -> np.ndarray:
+        """the accumulated array of one quantity, ny x (nx+1) or ny x (nx+2)"""
+        q = STAT_NAMES.index(name)
+        v = np.zeros((self.ny, self.nx + (1 if name in ("ux1", "ux2", "uxt") else 2)))
+        _check(lib().svof_statistics_field(self._h, q, v.ctypes.data, v.size))
+        return v
 
     KERNEL_KINDS = ["dt", "geom", "force", "vof", "predict", "poisson_fwd", "poisson_solve",
                     "poisson_inv", "project"]

@@ -21,6 +21,7 @@
 
 #include "../../include/svof_b200.h"
 #include "svof_internal.cuh"
+#include "stat_internal.cuh"
 
 using namespace svof;
 
@@ -124,6 +125,10 @@ struct svof_solver {
   double *h_dt = nullptr;   // pinned, many slots for svof_run
   int h_dt_slots = 0;
   DevBuf diag;
+  // time-averaged statistics: accumulators (made on the first collection),
+  // row-sum scratch, samples so far
+  DevBuf stat[SVOF_NSTATS], stat_part;
+  size_t stat_num = 0;
   std::vector<double> xf, xc, dxf_h, dxc_h;
   // graphs keyed by the buffer state at the start of a step
   std::map<int, cudaGraphExec_t> graphs;
@@ -730,8 +735,9 @@ int svof_destroy(svof_solver_t *s) {
   DevBuf *bufs[] = {&s->p, &s->psi, &s->curv, &s->normal, &s->ifrcx, &s->ifrcy, &s->dxf, &s->dxc,
                     &s->lap_ux, &s->lap_uy, &s->lap_t, &s->spec, &s->twf, &s->twb, &s->cs, &s->vt,
                     &s->rvt, &s->q1t, &s->ck, &s->lastf, &s->den, &s->pl, &s->pu, &s->evals, &s->diag,
-                    &s->coef};
+                    &s->coef, &s->stat_part};
   for (DevBuf *b : bufs) dfree(*b);
+  for (DevBuf &b : s->stat) dfree(b);
   if (s->d_dt) cudaFree(s->d_dt);
   if (s->d_minbits) cudaFree(s->d_minbits);
   if (s->h_dt) cudaFreeHost(s->h_dt);
@@ -1031,6 +1037,82 @@ int svof_logging_quantities(svof_solver_t *s, double *out, int nout) {
                                        s->prm.t_dif, s->prm.ly, s->diag.p, s->grid());
   CK_LAUNCH();
   CK(cudaMemcpyAsync(out, s->diag.p, 9 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+// x width of a statistics array (array_macros/statistics/ux1.h .. uxt.h)
+static int stat_width(const svof_solver *s, int q) {
+  return (SVOF_STAT_UX1 == q || SVOF_STAT_UX2 == q || SVOF_STAT_UXT == q) ? s->nx + 1 : s->nx + 2;
+}
+
+int svof_statistics_collect(svof_solver_t *s) {
+  if (!s) return fail("null argument");
+  if (!s->stat[0].p) {
+    for (int q = 0; q < SVOF_NSTATS; q++) {
+      DevBuf &b = s->stat[q];
+      b.n = (size_t)stat_width(s, q) * s->ny;
+      CK(cudaMalloc(&b.p, sizeof(double) * b.n));
+      CK(cudaMemsetAsync(b.p, 0, sizeof(double) * b.n, s->stream));
+    }
+    s->stat_part.n = 2 * (size_t)(s->nx + 2);
+    CK(cudaMalloc(&s->stat_part.p, sizeof(double) * s->stat_part.n));
+  }
+  StatArgs a{s->ux[s->cur_u].p, s->uy[s->cur_u].p, nullptr, s->t[s->cur_u].p,
+             s->stat[SVOF_STAT_UX1].p, s->stat[SVOF_STAT_UX2].p, s->stat[SVOF_STAT_UY1].p,
+             s->stat[SVOF_STAT_UY2].p, nullptr, nullptr, s->stat[SVOF_STAT_T1].p, s->stat[SVOF_STAT_T2].p,
+             s->stat[SVOF_STAT_UXT].p, s->nx, s->ny, 1, 0};
+  const dim3 b(32, 8), g((s->nx + 2 + 31) / 32, (s->ny + 7) / 8, 1);
+  k_stat_collect<<<g, b, 0, s->stream>>>(a);
+  CK_LAUNCH();
+  s->stat_num += 1;
+  return 0;
+}
+
+int svof_statistics_reset(svof_solver_t *s) {
+  if (!s) return fail("null argument");
+  for (DevBuf &b : s->stat)
+    if (b.p) CK(cudaMemsetAsync(b.p, 0, sizeof(double) * b.n, s->stream));
+  s->stat_num = 0;
+  CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+int svof_statistics_count(svof_solver_t *s, size_t *num) {
+  if (!s || !num) return fail("null argument");
+  *num = s->stat_num;
+  return 0;
+}
+
+int svof_statistics_reduce(svof_solver_t *s, int quantity, double *out, size_t count) {
+  if (!s || !out) return fail("null argument");
+  if (quantity < 0 || quantity >= SVOF_NSTATS) return fail("unknown statistics quantity %d", quantity);
+  const int w = stat_width(s, quantity);
+  if (count != (size_t)w) return fail("statistics quantity %d has %d columns, got %zu", quantity, w, count);
+  if (!s->stat[0].p) {
+    for (int i = 0; i < w; i++) out[i] = 0.;
+    return 0;
+  }
+  double *part = s->stat_part.p, *res = s->stat_part.p + w;
+  k_stat_reduce_planes<<<dim3((w + 127) / 128, 1), 128, 0, s->stream>>>(s->stat[quantity].p, w, s->ny, part);
+  CK_LAUNCH();
+  k_stat_reduce_final<<<(w + 127) / 128, 128, 0, s->stream>>>(part, w, 1, res);
+  CK_LAUNCH();
+  CK(cudaMemcpyAsync(out, res, sizeof(double) * w, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+int svof_statistics_field(svof_solver_t *s, int quantity, double *out, size_t count) {
+  if (!s || !out) return fail("null argument");
+  if (quantity < 0 || quantity >= SVOF_NSTATS) return fail("unknown statistics quantity %d", quantity);
+  const size_t n = (size_t)stat_width(s, quantity) * s->ny;
+  if (count != n) return fail("statistics quantity %d holds %zu values, got %zu", quantity, n, count);
+  if (!s->stat[0].p) {
+    for (size_t q = 0; q < n; q++) out[q] = 0.;
+    return 0;
+  }
+  CK(cudaMemcpyAsync(out, s->stat[quantity].p, sizeof(double) * n, cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   return 0;
 }

@@ -20,6 +20,7 @@
 
 #include "../../include/svof3d_b200.h"
 #include "svof3d_internal.cuh"
+#include "stat_internal.cuh"
 
 using namespace svof3;
 
@@ -134,6 +135,10 @@ struct svof3d_solver {
   };
   cudaStream_t io_h2d = nullptr, io_d2h = nullptr;
   IoSlot io_in[SVOF3_NFIELDS], io_out[SVOF3_NFIELDS];
+  // time-averaged statistics: accumulators (made on the first collection),
+  // row-sum scratch (one partial row per z plane, then the result), samples
+  DevBuf stat[SVOF3_NSTATS], stat_part;
+  size_t stat_num = 0;
 
   Grid3 grid() const { return Grid3{nx, ny, nz, dy, dz, dxf.p, dxc.p}; }
 };
@@ -510,8 +515,9 @@ int svof3d_destroy(svof3d_solver_t *s) {
   DevBuf *bufs[] = {&s->p, &s->psi, &s->curv, &s->normal, &s->ifrcx, &s->ifrcy, &s->ifrcz, &s->dxf, &s->dxc,
                     &s->lap_ux, &s->lap_cc, &s->coef, &s->spec, &s->xscratch, &s->twf_y, &s->twb_y, &s->twf_z,
                     &s->twb_z, &s->pl, &s->pu, &s->evy, &s->evz, &s->fw, &s->diag, &s->twf_y32, &s->twb_y32,
-                    &s->twf_z32, &s->twb_z32};
+                    &s->twf_z32, &s->twb_z32, &s->stat_part};
   for (DevBuf *b : bufs) dfree(*b);
+  for (DevBuf &b : s->stat) dfree(b);
   if (s->d_dt) cudaFree(s->d_dt);
   if (s->d_minbits) cudaFree(s->d_minbits);
   if (s->d_work) cudaFree(s->d_work);
@@ -922,6 +928,84 @@ int svof3d_diagnostics(svof3d_solver_t *s, double *divmax, double *vofmin, doubl
   if (vofmin) *vofmin = h[1];
   if (vofmax) *vofmax = h[2];
   if (volume) *volume = h[3];
+  return 0;
+}
+
+// x width of a statistics array: faces for ux1 ux2 uxt, cells otherwise
+static int stat_width(const svof3d_solver *s, int q) {
+  return (SVOF3_STAT_UX1 == q || SVOF3_STAT_UX2 == q || SVOF3_STAT_UXT == q) ? s->nx + 1 : s->nx + 2;
+}
+
+int svof3d_statistics_collect(svof3d_solver_t *s) {
+  if (!s) return fail("null argument");
+  if (!s->stat[0].p) {
+    for (int q = 0; q < SVOF3_NSTATS; q++) {
+      DevBuf &b = s->stat[q];
+      b.n = (size_t)stat_width(s, q) * s->ny * s->nz;
+      CK(cudaMalloc(&b.p, sizeof(double) * b.n));
+      CK(cudaMemsetAsync(b.p, 0, sizeof(double) * b.n, s->stream));
+    }
+    s->stat_part.n = (size_t)(s->nz + 1) * (s->nx + 2);
+    CK(cudaMalloc(&s->stat_part.p, sizeof(double) * s->stat_part.n));
+  }
+  StatArgs a{s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->uz[s->cur_u].p, s->t[s->cur_u].p,
+             s->stat[SVOF3_STAT_UX1].p, s->stat[SVOF3_STAT_UX2].p, s->stat[SVOF3_STAT_UY1].p,
+             s->stat[SVOF3_STAT_UY2].p, s->stat[SVOF3_STAT_UZ1].p, s->stat[SVOF3_STAT_UZ2].p,
+             s->stat[SVOF3_STAT_T1].p, s->stat[SVOF3_STAT_T2].p, s->stat[SVOF3_STAT_UXT].p,
+             s->nx, s->ny, s->nz, 1};
+  const dim3 b(32, 8), g((s->nx + 2 + 31) / 32, (s->ny + 7) / 8, s->nz);
+  k_stat_collect<<<g, b, 0, s->stream>>>(a);
+  CK_LAUNCH();
+  s->stat_num += 1;
+  return 0;
+}
+
+int svof3d_statistics_reset(svof3d_solver_t *s) {
+  if (!s) return fail("null argument");
+  for (DevBuf &b : s->stat)
+    if (b.p) CK(cudaMemsetAsync(b.p, 0, sizeof(double) * b.n, s->stream));
+  s->stat_num = 0;
+  CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+int svof3d_statistics_count(svof3d_solver_t *s, size_t *num) {
+  if (!s || !num) return fail("null argument");
+  *num = s->stat_num;
+  return 0;
+}
+
+int svof3d_statistics_reduce(svof3d_solver_t *s, int quantity, double *out, size_t count) {
+  if (!s || !out) return fail("null argument");
+  if (quantity < 0 || quantity >= SVOF3_NSTATS) return fail("unknown statistics quantity %d", quantity);
+  const int w = stat_width(s, quantity);
+  if (count != (size_t)w) return fail("statistics quantity %d has %d columns, got %zu", quantity, w, count);
+  if (!s->stat[0].p) {
+    for (int i = 0; i < w; i++) out[i] = 0.;
+    return 0;
+  }
+  double *part = s->stat_part.p, *res = s->stat_part.p + (size_t)s->nz * w;
+  k_stat_reduce_planes<<<dim3((w + 127) / 128, s->nz), 128, 0, s->stream>>>(s->stat[quantity].p, w, s->ny,
+                                                                             part);
+  CK_LAUNCH();
+  k_stat_reduce_final<<<(w + 127) / 128, 128, 0, s->stream>>>(part, w, s->nz, res);
+  CK_LAUNCH();
+  CK(cudaMemcpyAsync(out, res, sizeof(double) * w, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return 0;
+}
+
+int svof3d_statistics_field(svof3d_solver_t *s, int quantity, double *out, size_t count) {
+  if (!s || !out) return fail("null argument");
+  if (quantity < 0 || quantity >= SVOF3_NSTATS) return fail("unknown statistics quantity %d", quantity);
+  const size_t n = (size_t)stat_width(s, quantity) * s->ny * s->nz;
+  if (count != n) return fail("statistics quantity %d holds %zu values, got %zu", quantity, n, count);
+  if (!s->stat[0].p) {
+    for (size_t q = 0; q < n; q++) out[q] = 0.;
+    return 0;
+  }
+  CK(cudaMemcpyAsync(out, s->stat[quantity].p, sizeof(double) * n, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
   return 0;
 }
 

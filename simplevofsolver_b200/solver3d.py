@@ -44,7 +44,11 @@ EXPORTS3D = ["svof3d_create", "svof3d_destroy", "svof3d_field_count", "svof3d_up
              "svof3d_fluid_compute_potential_dft", "svof3d_fluid_correct_velocity",
              "svof3d_fluid_update_pressure", "svof3d_integrate", "svof3d_run", "svof3d_enqueue_steps",
              "svof3d_last_dt", "svof3d_diagnostics", "svof3d_profile_step", "svof3d_synchronize",
-             "svof3d_stream", "svof3d_last_error"]
+             "svof3d_stream", "svof3d_last_error", "svof3d_statistics_collect", "svof3d_statistics_reset",
+             "svof3d_statistics_count", "svof3d_statistics_reduce", "svof3d_statistics_field"]
+
+# statistics quantities (SVOF3_STAT_*)
+STAT_NAMES3D = ["ux1", "ux2", "uy1", "uy2", "uz1", "uz2", "t1", "t2", "uxt"]
 
 
 def storage_shape3d(name: str, nx: int, ny: int, nz: int):
@@ -83,6 +87,11 @@ def lib3() -> ctypes.CDLL:
                    "svof3d_load_interior_async", "svof3d_store_interior_async"):
             getattr(L, fn).argtypes = [vp, i, dp, sz]
         L.svof3d_io_wait.argtypes = [vp]
+        L.svof3d_statistics_collect.argtypes = [vp]
+        L.svof3d_statistics_reset.argtypes = [vp]
+        L.svof3d_statistics_count.argtypes = [vp, ctypes.POINTER(sz)]
+        L.svof3d_statistics_reduce.argtypes = [vp, i, dp, sz]
+        L.svof3d_statistics_field.argtypes = [vp, i, dp, sz]
         L.svof3d_device_field.argtypes = [vp, i, ctypes.POINTER(vp)]
         L.svof3d_fluid_decide_dt.argtypes = [vp, pd]
         L.svof3d_interface_compute_curvature_tensor.argtypes = [vp]
@@ -314,6 +323,37 @@ class Solver3D:
         cnt = np.zeros(n, dtype=np.int32)
         _check(lib3().svof3d_profile_step(self._h, ms.ctypes.data, cnt.ctypes.data, n))
         return {k: (float(ms[q]), int(cnt[q])) for q, k in enumerate(self.KERNEL_KINDS)}
+
+    # ------------------------------------------------- time-averaged statistics
+    def statistics_collect(self):
+        """add one sample of the current fields to the device accumulators;
+        queued, does not wait"""
+        _check(lib3().svof3d_statistics_collect(self._h))
+
+    def statistics_reset(self):
+        _check(lib3().svof3d_statistics_reset(self._h))
+
+    def statistics_count(self) -> int:
+        n = ctypes.c_size_t(0)
+        _check(lib3().svof3d_statistics_count(self._h, ctypes.byref(n)))
+        return int(n.value)
+
+    def statistics_reduced(self) -> dict:
+        """the y-z sums of every quantity (one vector along x each), plus 'num'"""
+        out = {}
+        for q, k in enumerate(STAT_NAMES3D):
+            v = np.zeros(self.nx + (1 if k in ("ux1", "ux2", "uxt") else 2))
+            _check(lib3().svof3d_statistics_reduce(self._h, q, v.ctypes.data, v.size))
+            out[k] = v
+        out["num"] = self.statistics_count()
+        return out
+
+    def statistics_field(self, name: str) -> np.ndarray:
+        """the accumulated array of one quantity, nz x ny x (nx+1) or nz x ny x (nx+2)"""
+        q = STAT_NAMES3D.index(name)
+        v = np.zeros((self.nz, self.ny, self.nx + (1 if name in ("ux1", "ux2", "uxt") else 2)))
+        _check(lib3().svof3d_statistics_field(self._h, q, v.ctypes.data, v.size))
+        return v
 
     def synchronize(self):
         _check(lib3().svof3d_synchronize(self._h))
