@@ -23,6 +23,7 @@
 #include <cuda_pipeline.h>
 
 #include "svof3d_internal.cuh"
+#include "smem_limit.cuh"
 
 namespace svof3 {
 
@@ -646,10 +647,9 @@ cudaError_t interface_advect(cudaStream_t st, const double *vof, double *vof_new
 }
 
 cudaError_t interface_prepare() {
-  cudaError_t e =
-      cudaFuncSetAttribute(k3_vof_advect<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAdvectSmem);
+  cudaError_t e = raise_smem_limit(k3_vof_advect<double>, kAdvectSmem);
   if (cudaSuccess != e) return e;
-  return cudaFuncSetAttribute(k3_vof_advect<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAdvectSmem);
+  return raise_smem_limit(k3_vof_advect<float>, kAdvectSmem);
 }
 
 #define SVOF3_INTERFACE_INST(R)                                                                                \

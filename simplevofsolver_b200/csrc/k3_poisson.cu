@@ -34,6 +34,7 @@
 
 #include "fft_device.cuh"
 #include "svof3d_internal.cuh"
+#include "smem_limit.cuh"
 
 namespace svof3 {
 
@@ -590,7 +591,7 @@ cudaError_t by_l2n(int l2n, F f) {
 }
 template <class K>
 cudaError_t line_attrs(K kernel, int smem) {
-  cudaError_t r = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaError_t r = raise_smem_limit(kernel, (size_t)smem);
   if (cudaSuccess != r) return r;
   return cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
 }

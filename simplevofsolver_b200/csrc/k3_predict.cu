@@ -21,6 +21,7 @@
 #include <cuda_pipeline.h>
 
 #include "svof3d_internal.cuh"
+#include "smem_limit.cuh"
 
 namespace svof3 {
 
@@ -643,9 +644,9 @@ cudaError_t predict_launch(cudaStream_t st, const Predict3Args<R> &a) {
 }
 
 cudaError_t predict_prepare() {
-  cudaError_t e = cudaFuncSetAttribute(k3_rhs<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRhsSmem<double>);
+  cudaError_t e = raise_smem_limit(k3_rhs<double>, kRhsSmem<double>);
   if (cudaSuccess != e) return e;
-  return cudaFuncSetAttribute(k3_rhs<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRhsSmem<float>);
+  return raise_smem_limit(k3_rhs<float>, kRhsSmem<float>);
 }
 template cudaError_t predict_launch<double>(cudaStream_t, const Predict3Args<double> &);
 template cudaError_t predict_launch<float>(cudaStream_t, const Predict3Args<float> &);

@@ -98,6 +98,7 @@ __device__ __forceinline__ double thinc_intercept(const double vof, const double
 
 __global__ void __launch_bounds__(GBX * GBY) k_geom(const double *__restrict__ vof, double *__restrict__ normal,
                                                    double *__restrict__ curv, Grid2 g) {
+  pdl_enter();
   __shared__ double sv[GBY + 2][GBX + 2];
   __shared__ double sdx[GBY + 1][GBX + 1];
   __shared__ double sdy[GBY + 1][GBX + 1];
@@ -163,6 +164,7 @@ __global__ void __launch_bounds__(GBX * GBY) k_geom(const double *__restrict__ v
 // k_force: one thread per cell i in [1, nx], j in [1, ny]
 __global__ void k_force(const double *__restrict__ vof, const double *__restrict__ curv,
                         double *__restrict__ ifrcx, double *__restrict__ ifrcy, double tension, Grid2 g) {
+  pdl_enter();
   const int nx = g.nx, ny = g.ny;
   const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
@@ -199,6 +201,7 @@ __global__ void __launch_bounds__(ABX * ABY) k_vof_advect(
     const double *__restrict__ vof, double *__restrict__ vof_new, const double *__restrict__ ux,
     const double *__restrict__ uy, const double *__restrict__ normal, double *__restrict__ src_a,
     const double *__restrict__ src_b, const double *__restrict__ dtp, RK rk, int use_b, Grid2 g) {
+  pdl_enter();
   __shared__ double fx[ABY][ABX + 1];  // faces i0 .. i0+ABX of rows j0 .. j0+ABY-1
   __shared__ double fy[ABY + 1][ABX];  // faces j0 .. j0+ABY of columns i0 .. i0+ABX-1
   const int nx = g.nx, ny = g.ny;

@@ -46,6 +46,7 @@ __global__ void k_dct_fwd(const double *__restrict__ ux, const double *__restric
                           double *__restrict__ spec, const double *__restrict__ tw,
                           const double *__restrict__ cs, const double *__restrict__ dtp,
                           double gam, int log2n, Grid2 g) {
+  pdl_enter();
   extern __shared__ double z[];
   const int n = g.nx;
   const int j = 1 + blockIdx.x;
@@ -80,6 +81,7 @@ __global__ void k_dct_ysolve(double *__restrict__ spec, const double *__restrict
                              const double *__restrict__ rvt, const double *__restrict__ q1t,
                              const double *__restrict__ ck, const double *__restrict__ lastf,
                              const double *__restrict__ den, double lap, int nx, int ny, int kt) {
+  pdl_enter();
   extern __shared__ double sm[];
   double *sq = sm;                       // [ny][kt] line data
   double *sv = sm + (size_t)ny * kt;     // [ny][kt] v
@@ -146,6 +148,7 @@ __global__ void k_dct_ysolve(double *__restrict__ spec, const double *__restrict
 __global__ void k_dct_inv(const double *__restrict__ spec, double *__restrict__ psi,
                           const double *__restrict__ tw, const double *__restrict__ cs,
                           int log2n, Grid2 g) {
+  pdl_enter();
   extern __shared__ double z[];
   const int n = g.nx, nx = g.nx, ny = g.ny;
   const int j = 1 + blockIdx.x;
@@ -194,6 +197,7 @@ __global__ void k_dct_inv(const double *__restrict__ spec, double *__restrict__ 
 __global__ void k_dft_fwd(const double *__restrict__ ux, const double *__restrict__ uy,
                           double *__restrict__ spec, const double *__restrict__ tw,
                           const double *__restrict__ dtp, double gam, int log2n, int cols, Grid2 g) {
+  pdl_enter();
   extern __shared__ double z[];
   const int n = g.ny, nx = g.nx;
   const int nky = n / 2 + 1;
@@ -227,6 +231,7 @@ __global__ void k_dft_xsolve(double *__restrict__ spec, const double *__restrict
                              const double *__restrict__ rvt, const double *__restrict__ pl,
                              const double *__restrict__ pu, const double *__restrict__ evals, int nx,
                              int nky, int kt) {
+  pdl_enter();
   extern __shared__ double sm[];
   double *sre = sm;                        // [nx][kt]
   double *sim = sm + (size_t)nx * kt;      // [nx][kt]
@@ -308,6 +313,7 @@ __global__ void k_dft_xsolve(double *__restrict__ spec, const double *__restrict
 // c2r along y for a tile of columns, extract_output and the psi boundaries
 __global__ void k_dft_inv(const double *__restrict__ spec, double *__restrict__ psi,
                           const double *__restrict__ tw, int log2n, int cols, Grid2 g) {
+  pdl_enter();
   extern __shared__ double z[];
   const int n = g.ny, nx = g.nx, ny = g.ny;
   const int nky = n / 2 + 1;

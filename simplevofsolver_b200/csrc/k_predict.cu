@@ -30,6 +30,7 @@ size_t predict_smem_bytes(int nx, int R) {
 __global__ void k_tdm_coef(const double *__restrict__ lap_ux, const double *__restrict__ lap_uy,
                            const double *__restrict__ lap_t, const double *__restrict__ dtp, double gam,
                            double m_dif, double t_dif, int nx, double *__restrict__ coef) {
+  pdl_enter();
   // the Laplacian tables are staged in shared memory first: the recurrence
   // below then waits on arithmetic only
   extern __shared__ double slap[];  // [3][3 nx]
@@ -74,6 +75,7 @@ __global__ void k_tdm_coef(const double *__restrict__ lap_ux, const double *__re
 }
 
 __global__ void __launch_bounds__(256) k_predict(PredictArgs a) {
+  pdl_enter();
   extern __shared__ double sm[];
   const Grid2 g = a.g;
   const int nx = g.nx, ny = g.ny, R = a.rows_per_block;

@@ -18,6 +18,7 @@ namespace svof {
 __global__ void k_project(double *__restrict__ ux, double *__restrict__ uy, double *__restrict__ p,
                           const double *__restrict__ psi, const double *__restrict__ dtp, double gam,
                           double m_dif, double uy_xm, double uy_xp, int do_vel, int do_p, Grid2 g) {
+  pdl_enter();
   const int nx = g.nx, ny = g.ny;
   const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
@@ -117,6 +118,7 @@ __device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v)
 
 __global__ void k_cfl(const double *__restrict__ ux, const double *__restrict__ uy,
                       unsigned long long *__restrict__ minbits, Grid2 g) {
+  pdl_enter();
   const int nx = g.nx, ny = g.ny;
   const double small = 1.e-8;
   unsigned long long best = 0x7ff0000000000000ull;  // +inf
@@ -157,6 +159,7 @@ __global__ void k_cfl(const double *__restrict__ ux, const double *__restrict__ 
 // Resets the accumulator to the bit pattern of 1.0 (the initial *dt = 1.).
 __global__ void k_dt_final(unsigned long long *minbits, double *dt, double coef_adv, double dif_m_y,
                            double dif_t_y) {
+  pdl_enter();
   double dta = fmin(1., __longlong_as_double((long long)*minbits));
   dta *= coef_adv;
   double r = dta;

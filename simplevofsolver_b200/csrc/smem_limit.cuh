@@ -1,0 +1,29 @@
+// Dynamic shared-memory limits of the kernels whose tiles depend on the grid.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <mutex>
+
+// Raises func's dynamic shared-memory limit to at least `bytes`.  The limit
+// is an attribute of the function, shared by every solver of the process, so
+// it only ever grows: a solver set up later with shorter lines must not take
+// away what an earlier one launches with.  Called for every size, small ones
+// included, since the default limit also counts the kernel's static shared
+// memory.
+inline cudaError_t raise_smem_limit(const void *func, size_t bytes) {
+  static std::mutex mu;
+  static std::map<const void *, size_t> granted;
+  std::lock_guard<std::mutex> lock(mu);
+  size_t &g = granted[func];
+  if (bytes <= g) return cudaSuccess;
+  const cudaError_t e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (cudaSuccess == e) g = bytes;
+  return e;
+}
+
+template <class... A>
+inline cudaError_t raise_smem_limit(void (*func)(A...), size_t bytes) {
+  return raise_smem_limit(reinterpret_cast<const void *>(func), bytes);
+}

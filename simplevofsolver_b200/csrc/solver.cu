@@ -22,6 +22,7 @@
 #include "../../include/svof_b200.h"
 #include "svof_internal.cuh"
 #include "stat_internal.cuh"
+#include "smem_limit.cuh"
 
 using namespace svof;
 
@@ -125,6 +126,10 @@ struct svof_solver {
   double *h_dt = nullptr;   // pinned, many slots for svof_run
   int h_dt_slots = 0;
   DevBuf diag;
+  // set while the step graph of a small grid is captured: its kernels are
+  // launched with programmatic stream serialisation (each starts with
+  // pdl_enter)
+  bool pdl = false;
   // time-averaged statistics: accumulators (made on the first collection),
   // row-sum scratch, samples so far
   DevBuf stat[SVOF_NSTATS], stat_part;
@@ -165,6 +170,28 @@ void dfree(DevBuf &b) {
 
 // ---- launch helpers: each issues the kernels of one reference function ----
 
+// launch k on st; with pdl, as a programmatic dependent of the stream's
+// previous kernel
+template <typename... KArgs, typename... Args>
+cudaError_t launch_k(bool pdl, void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                     Args... args) {
+  if (!pdl) {
+    k<<<grid, block, smem, st>>>(args...);
+    return cudaGetLastError();
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 int launch_halo_bc(svof_solver *s, double *a, int field) {
   const int nx = s->nx, ny = s->ny;
   int width, nh, kind;
@@ -186,25 +213,24 @@ int launch_halo_bc(svof_solver *s, double *a, int field) {
 int launch_dt(svof_solver *s) {
   const long nf = (long)(s->nx - 1) * s->ny + (long)s->nx * s->ny;
   int blocks = (int)std::min<long>((nf + 255) / 256, 148L * 8);
-  k_cfl<<<blocks, 256, 0, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->d_minbits, s->grid());
-  CK_LAUNCH();
-  k_dt_final<<<1, 1, 0, s->stream>>>(s->d_minbits, s->d_dt, s->prm.coef_dt_adv, s->dif_m_y, s->dif_t_y);
-  CK_LAUNCH();
+  CK(launch_k(s->pdl, k_cfl, blocks, 256, 0, s->stream, (const double *)s->ux[s->cur_u].p,
+              (const double *)s->uy[s->cur_u].p, s->d_minbits, s->grid()));
+  CK(launch_k(s->pdl, k_dt_final, 1, 1, 0, s->stream, s->d_minbits, s->d_dt, s->prm.coef_dt_adv, s->dif_m_y,
+              s->dif_t_y));
   return 0;
 }
 
 int launch_geom(svof_solver *s) {
   dim3 b(32, 8), gr((s->nx + 31) / 32, (s->ny + 2 + 7) / 8);
-  k_geom<<<gr, b, 0, s->stream>>>(s->vof[s->cur_v].p, s->normal.p, s->curv.p, s->grid());
-  CK_LAUNCH();
+  CK(launch_k(s->pdl, k_geom, gr, b, 0, s->stream, (const double *)s->vof[s->cur_v].p, s->normal.p, s->curv.p,
+              s->grid()));
   return 0;
 }
 
 int launch_force(svof_solver *s, cudaStream_t st = nullptr) {
   dim3 b(32, 8), gr((s->nx + 31) / 32, (s->ny + 7) / 8);
-  k_force<<<gr, b, 0, st ? st : s->stream>>>(s->vof[s->cur_v].p, s->curv.p, s->ifrcx.p, s->ifrcy.p, s->prm.tension,
-                                   s->grid());
-  CK_LAUNCH();
+  CK(launch_k(s->pdl, k_force, gr, b, 0, st ? st : s->stream, (const double *)s->vof[s->cur_v].p,
+              (const double *)s->curv.p, s->ifrcx.p, s->ifrcy.p, s->prm.tension, s->grid()));
   return 0;
 }
 
@@ -212,19 +238,18 @@ int launch_vof(svof_solver *s, int rk) {
   if (0 != rk) s->sa_v ^= 1;  // reset_srcs, src/interface/update/main.c:28-45
   dim3 b(32, 8), gr((s->nx + 31) / 32, (s->ny + 7) / 8);
   RK c{RK_A[rk], RK_B[rk], RK_A[rk] + RK_B[rk]};
-  k_vof_advect<<<gr, b, 0, s->stream>>>(s->vof[s->cur_v].p, s->vof[1 - s->cur_v].p, s->ux[s->cur_u].p,
-                                        s->uy[s->cur_u].p, s->normal.p, s->svof[s->sa_v].p,
-                                        s->svof[1 - s->sa_v].p, s->d_dt, c, rk != 0, s->grid());
-  CK_LAUNCH();
+  CK(launch_k(s->pdl, k_vof_advect, gr, b, 0, s->stream, (const double *)s->vof[s->cur_v].p, s->vof[1 - s->cur_v].p,
+              (const double *)s->ux[s->cur_u].p, (const double *)s->uy[s->cur_u].p, (const double *)s->normal.p,
+              s->svof[s->sa_v].p, (const double *)s->svof[1 - s->sa_v].p, (const double *)s->d_dt, c, rk != 0,
+              s->grid()));
   s->cur_v ^= 1;
   return 0;
 }
 
 int launch_coef(svof_solver *s, int rk, cudaStream_t st) {
-  k_tdm_coef<<<1, 128, sizeof(double) * 9 * s->nx, st>>>(s->lap_ux.p, s->lap_uy.p, s->lap_t.p, s->d_dt,
-                                                           RK_A[rk] + RK_B[rk], s->prm.m_dif, s->prm.t_dif, s->nx,
-                                                           s->coef.p);
-  CK_LAUNCH();
+  CK(launch_k(s->pdl, k_tdm_coef, 1, 128, sizeof(double) * 9 * s->nx, st, (const double *)s->lap_ux.p,
+              (const double *)s->lap_uy.p, (const double *)s->lap_t.p, (const double *)s->d_dt, RK_A[rk] + RK_B[rk],
+              s->prm.m_dif, s->prm.t_dif, s->nx, s->coef.p));
   return 0;
 }
 
@@ -270,8 +295,7 @@ int launch_predict(svof_solver *s, int rk, bool with_coef = true) {
   a.rows_per_block = s->pred_rows;
   a.g = s->grid();
   const int blocks = (s->ny + s->pred_rows - 1) / s->pred_rows;
-  k_predict<<<blocks, s->pred_threads, s->pred_smem, s->stream>>>(a);
-  CK_LAUNCH();
+  CK(launch_k(s->pdl, k_predict, blocks, s->pred_threads, s->pred_smem, s->stream, a));
   s->cur_u ^= 1;
   return 0;
 }
@@ -285,40 +309,34 @@ int launch_potential(svof_solver *s, int rk, int want_dct) {
   if (s->uniform) {
     const int nthr = std::min(256, std::max(32, s->nx / 2));
     const size_t smem = sizeof(double) * 2 * s->nx;
-    k_dct_fwd<<<s->ny, nthr, smem, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->spec.p, s->twf.p,
-                                                s->cs.p, s->d_dt, gam, s->log2fft, g);
-    CK_LAUNCH();
+    CK(launch_k(s->pdl, k_dct_fwd, s->ny, nthr, smem, s->stream, s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->spec.p,
+                s->twf.p, s->cs.p, s->d_dt, gam, s->log2fft, g));
     const int kt = s->ysolve_kt;
-    k_dct_ysolve<<<(s->nx + kt - 1) / kt, 128, sizeof(double) * 3 * kt * s->ny, s->stream>>>(
-        s->spec.p, s->vt.p, s->rvt.p, s->q1t.p, s->ck.p, s->lastf.p, s->den.p, 1. / s->dy / s->dy, s->nx, s->ny,
-        kt);
-    CK_LAUNCH();
-    k_dct_inv<<<s->ny, nthr, smem, s->stream>>>(s->spec.p, s->psi.p, s->twb.p, s->cs.p, s->log2fft, g);
-    CK_LAUNCH();
+    CK(launch_k(s->pdl, k_dct_ysolve, (s->nx + kt - 1) / kt, 128, sizeof(double) * 3 * kt * s->ny, s->stream,
+                s->spec.p, s->vt.p, s->rvt.p, s->q1t.p, s->ck.p, s->lastf.p, s->den.p, 1. / s->dy / s->dy, s->nx,
+                s->ny, kt));
+    CK(launch_k(s->pdl, k_dct_inv, s->ny, nthr, smem, s->stream, s->spec.p, s->psi.p, s->twb.p, s->cs.p,
+                s->log2fft, g));
   } else {
     const int cols = s->dft_cols;
     const int blocks = (s->nx + cols - 1) / cols;
     const size_t smem = sizeof(double) * 2 * s->ny * cols;
     const int nky = s->ny / 2 + 1;
-    k_dft_fwd<<<blocks, 256, smem, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->spec.p, s->twf.p,
-                                                s->d_dt, gam, s->log2fft, cols, g);
-    CK_LAUNCH();
+    CK(launch_k(s->pdl, k_dft_fwd, blocks, 256, smem, s->stream, s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->spec.p,
+                s->twf.p, s->d_dt, gam, s->log2fft, cols, g));
     const int xkt = s->xsolve_kt;
-    k_dft_xsolve<<<(nky + xkt - 1) / xkt, 128, sizeof(double) * 4 * xkt * s->nx, s->stream>>>(
-        s->spec.p, s->vt.p, s->rvt.p, s->pl.p, s->pu.p, s->evals.p, s->nx, nky, xkt);
-    CK_LAUNCH();
-    k_dft_inv<<<blocks, 256, smem, s->stream>>>(s->spec.p, s->psi.p, s->twb.p, s->log2fft, cols, g);
-    CK_LAUNCH();
+    CK(launch_k(s->pdl, k_dft_xsolve, (nky + xkt - 1) / xkt, 128, sizeof(double) * 4 * xkt * s->nx, s->stream,
+                s->spec.p, s->vt.p, s->rvt.p, s->pl.p, s->pu.p, s->evals.p, s->nx, nky, xkt));
+    CK(launch_k(s->pdl, k_dft_inv, blocks, 256, smem, s->stream, s->spec.p, s->psi.p, s->twb.p, s->log2fft, cols, g));
   }
   return 0;
 }
 
 int launch_project(svof_solver *s, int rk, int do_vel, int do_p) {
   dim3 b(32, 8), gr((s->nx + 31) / 32, (s->ny + 7) / 8);
-  k_project<<<gr, b, 0, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->p.p, s->psi.p, s->d_dt,
-                                     RK_A[rk] + RK_B[rk], s->prm.m_dif, s->prm.uy_xm, s->prm.uy_xp, do_vel,
-                                     do_p, s->grid());
-  CK_LAUNCH();
+  CK(launch_k(s->pdl, k_project, gr, b, 0, s->stream, s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->p.p,
+              (const double *)s->psi.p, (const double *)s->d_dt, RK_A[rk] + RK_B[rk], s->prm.m_dif, s->prm.uy_xm,
+              s->prm.uy_xp, do_vel, do_p, s->grid()));
   return 0;
 }
 
@@ -362,7 +380,11 @@ int step_graph(svof_solver *s, cudaGraphExec_t *exec) {
   }
   cudaGraph_t graph;
   CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+  // launch-bound grids only: at 128^2 and 256^2 cells a step is 3-4 % faster,
+  // at 512^2 and above the attribute gains nothing
+  s->pdl = (long)s->nx * s->ny <= 256L * 256L;
   const int rc = launch_step(s);
+  s->pdl = false;
   cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
   if (rc) return 1;
   if (cudaSuccess != e) return fail("cudaStreamEndCapture: %s", cudaGetErrorString(e));
@@ -615,29 +637,24 @@ int engine_create(const svof_params_t *prm, const double *xf, const double *xc, 
     s->pred_threads = (r <= 2) ? 128 : 256;
     s->pred_smem = predict_smem_bytes(nx, s->pred_rows);
     if (s->pred_smem > 200 * 1024) return fail("svof_create: nx = %d too large for the x line solver", nx), bail();
-    if (cudaSuccess != cudaFuncSetAttribute(k_predict, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)s->pred_smem))
+    if (cudaSuccess != raise_smem_limit(k_predict, s->pred_smem))
       return fail("cudaFuncSetAttribute(k_predict): %s", cudaGetErrorString(cudaGetLastError())), bail();
     const size_t coef_smem = sizeof(double) * 9 * nx;
-    if (coef_smem > 48 * 1024 &&
-        cudaSuccess != cudaFuncSetAttribute(k_tdm_coef, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coef_smem))
-      return fail("cudaFuncSetAttribute(k_tdm_coef)"), bail();
+    if (cudaSuccess != raise_smem_limit(k_tdm_coef, coef_smem)) return fail("cudaFuncSetAttribute(k_tdm_coef)"), bail();
   }
   // transforms: one row (DCT) or a tile of columns (DFT) per block
   {
     const size_t dct_smem = sizeof(double) * 2 * nx;
-    if (s->uniform && dct_smem > 48 * 1024) {
-      cudaFuncSetAttribute(k_dct_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dct_smem);
-      cudaFuncSetAttribute(k_dct_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dct_smem);
-    }
+    if (s->uniform && (cudaSuccess != raise_smem_limit(k_dct_fwd, dct_smem) ||
+                       cudaSuccess != raise_smem_limit(k_dct_inv, dct_smem)))
+      return fail("cudaFuncSetAttribute(k_dct_fwd, k_dct_inv)"), bail();
     int cols = 16;
     while (cols > 1 && sizeof(double) * 2 * (size_t)ny * cols > 100 * 1024) cols >>= 1;
     s->dft_cols = cols;
     const size_t dft_smem = sizeof(double) * 2 * (size_t)ny * cols;
-    if (!s->uniform && dft_smem > 48 * 1024) {
-      cudaFuncSetAttribute(k_dft_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dft_smem);
-      cudaFuncSetAttribute(k_dft_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dft_smem);
-    }
+    if (!s->uniform && (cudaSuccess != raise_smem_limit(k_dft_fwd, dft_smem) ||
+                        cudaSuccess != raise_smem_limit(k_dft_inv, dft_smem)))
+      return fail("cudaFuncSetAttribute(k_dft_fwd, k_dft_inv)"), bail();
     if (sizeof(double) * 2 * (size_t)(s->uniform ? nx : ny) > 200 * 1024)
       return fail("svof_create: FFT length too large for one block"), bail();
   }
@@ -654,17 +671,13 @@ int engine_create(const svof_params_t *prm, const double *xf, const double *xc, 
     s->ysolve_kt = pick_kt(nx, bpl);
     const size_t sm = bpl * s->ysolve_kt;
     if (sm > 200 * 1024) return fail("svof_create: ny = %d too large for the y line solver", ny), bail();
-    if (sm > 48 * 1024 &&
-        cudaSuccess != cudaFuncSetAttribute(k_dct_ysolve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))
-      return fail("cudaFuncSetAttribute(k_dct_ysolve)"), bail();
+    if (cudaSuccess != raise_smem_limit(k_dct_ysolve, sm)) return fail("cudaFuncSetAttribute(k_dct_ysolve)"), bail();
   } else {
     const size_t bpl = sizeof(double) * 4 * (size_t)nx;
     s->xsolve_kt = pick_kt(ny / 2 + 1, bpl);
     const size_t sm = bpl * s->xsolve_kt;
     if (sm > 200 * 1024) return fail("svof_create: nx = %d too large for the x line solver", nx), bail();
-    if (sm > 48 * 1024 &&
-        cudaSuccess != cudaFuncSetAttribute(k_dft_xsolve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))
-      return fail("cudaFuncSetAttribute(k_dft_xsolve)"), bail();
+    if (cudaSuccess != raise_smem_limit(k_dft_xsolve, sm)) return fail("cudaFuncSetAttribute(k_dft_xsolve)"), bail();
   }
   // launch plan checks: every dynamic shared-memory size covers what the
   // kernel indexes, every line solve has a thread per line

@@ -21,6 +21,7 @@
 #include "../../include/svof3d_b200.h"
 #include "svof3d_internal.cuh"
 #include "stat_internal.cuh"
+#include "smem_limit.cuh"
 
 using namespace svof3;
 
@@ -584,9 +585,7 @@ int svof3d_create(const svof3d_params_t *prm, const double *xf, const double *xc
       return fail("cudaFuncSetAttribute(Poisson): %s", cudaGetErrorString(cudaGetLastError())), bail();
     const size_t coef_smem = sizeof(double) * 6 * nx;
     if (coef_smem > 200 * 1024) return fail("svof3d_create: nx too large"), bail();
-    if (cudaSuccess !=
-        cudaFuncSetAttribute(k3_tdm_coef, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coef_smem))
-      return fail("cudaFuncSetAttribute(k3_tdm_coef)"), bail();
+    if (cudaSuccess != raise_smem_limit(k3_tdm_coef, coef_smem)) return fail("cudaFuncSetAttribute(k3_tdm_coef)"), bail();
   }
   if (cudaSuccess != cudaMalloc(&s->d_dt, sizeof(double))) return fail("cudaMalloc dt"), bail();
   if (cudaSuccess != cudaMalloc(&s->d_work, sizeof(unsigned) * nx * (ny + 2) * (nz + 2)) ||

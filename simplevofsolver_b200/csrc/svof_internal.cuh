@@ -17,6 +17,15 @@ namespace svof {
 
 constexpr double kDblEpsilon = 2.220446049250313080847e-16;  // DBL_EPSILON
 
+// Programmatic dependent launch: on small grids the step graph launches its
+// kernels with programmatic stream serialisation, so that a kernel is set up
+// while its predecessor drains.  Every step kernel starts here and waits
+// until the preceding kernels of its stream have completed and their memory
+// is visible.  The successor is released when the blocks exit (an explicit
+// early release measured slower from 256^2 cells up).  The wait does nothing
+// for a kernel launched without the attribute.
+__device__ __forceinline__ void pdl_enter() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // reference include/array_macros/**: index maps of the halo'd arrays
 struct Grid2 {
   int nx, ny;
