@@ -90,20 +90,19 @@ ALG_WORDS_3D = {
 }
 # the mixed path's bytes per interior cell and launch: the state (velocities,
 # p, t, vof, vof sources, psi) stays FP64, curvature, forces, momentum
-# sources, increments and spectra are FP32; the Poisson kinds average its
-# two passes (the second also reads psi)
+# sources and increments are FP32; the Poisson solve is the FP64 path's
 ALG_BYTES_3D_MIXED = {
     "dt": 24.0, "geom": 12.0, "force": 24.0, "vof": 48.0 + 16.0 / 3.0,
     "predict": 40.0 + 12.0 + 32.0 / 3.0 + 32.0 + 16.0,
-    "poisson_fwd": 32.0, "poisson_z": 8.0, "poisson_solve": 8.0, "poisson_inv": 16.0, "project": 72.0,
+    "poisson_fwd": 32.0, "poisson_z": 16.0, "poisson_solve": 16.0, "poisson_inv": 16.0, "project": 72.0,
 }
 # dt (2), then per substep: geom + intercept, force, vof, coef + rhs +
-# line solve, 6 Poisson launches (right-hand side, y, z, x, z, y; 12 in the
-# mixed path), project
+# line solve, 6 Poisson launches (right-hand side, y, z, x, z, y), project;
+# the same in both paths
 KERNELS_PER_STEP_3D = 2 + 3 * 14
 # kernels launched per launch of a kind (profile counts kernels)
 KERNELS_PER_KIND_3D = {"dt": 2, "geom": 2, "predict": 3, "poisson_fwd": 2}
-KERNELS_PER_STEP_3D_MIXED = 2 + 3 * 20
+KERNELS_PER_STEP_3D_MIXED = KERNELS_PER_STEP_3D
 
 WORKLOADS3D = {
     # the headline configuration: 512^3, 128 droplets, radii 0.02 .. 0.05
@@ -463,8 +462,9 @@ def run3d(args, wl, ic, env, world, rank, local_rank):
             "data": "synthetic (seeded droplet field, workloads.droplets3d)",
             "config": {"workload": args.workload, "nx": n, "ny": n, "nz": n, "droplets": wl["ndrops"],
                        "radii": list(wl["radii"]), "x_grid": "tanh-stretched (1.5)",
-                       "poisson": "r2c-y + dft-z + thomas-x (mixed: two passes, FP64 residual)",
-                       "precision": "mixed (FP32 intermediates and transforms, FP64 state and x line solves)",
+                       "poisson": "r2c-y + dft-z + thomas-x, FP64 in both paths",
+                       "precision": "mixed (FP32 interface geometry, forces, sources and increments; FP64 state, "
+                                    "stencils, x line solves and Poisson solve)",
                        "l2": "not flushed: inputs larger than L2 (fields of %.1f GB resident)" % (
                            35.5 * cells * 8 / 1e9),
                        "parallelism": f"replicas{world}"},

@@ -53,14 +53,13 @@ typedef struct {
  *   SVOF3_FP64   every array and every operation in FP64 (follows the
  *                restatement's rounding; only exp / log may differ)
  *   SVOF3_MIXED  velocities, pressure, psi, t, vof and the vof sources stay
- *                FP64; curvature, normals, forces, momentum sources, the
- *                predictor's sweep scratch and the Poisson spectra are FP32;
- *                interface geometry, THINC and the y/z transforms compute in
- *                FP32; the momentum stencils, the x line solves and the vof
- *                update in FP64; the projection solves twice (FP64 residual,
- *                defect correction).  Fields stored in FP32 are converted
- *                to FP64 by svof3d_download_field / from FP64 by
- *                svof3d_upload_field. */
+ *                FP64; curvature, normals, forces, momentum sources and the
+ *                predictor's sweep scratch are FP32; interface geometry and
+ *                THINC compute in FP32; the momentum stencils, the x line
+ *                solves, the vof update and the whole Poisson solve (the
+ *                FP64 path's kernels, one pass) in FP64.  Fields stored in
+ *                FP32 are converted to FP64 by svof3d_download_field / from
+ *                FP64 by svof3d_upload_field. */
 enum { SVOF3_FP64 = 0, SVOF3_MIXED = 1 };
 
 enum {

@@ -8,8 +8,7 @@
 // x fastest: every transform reads and writes runs of consecutive i, and the
 // x line solve reads each line contiguously.  No transpose pass exists.
 //
-//   k3_pois_b      the right-hand side of every cell, compact (k3_pois_resid:
-//                  the mixed second pass's residual, in place)
+//   k3_pois_b      the right-hand side of every cell, compact
 //   k3_pois_fwd_y  a block owns COLS consecutive i of one plane k
 //   k3_pois_z      a block owns COLS consecutive i of one ky, both signs
 //                  (in place)
@@ -21,13 +20,10 @@
 //                  with its halo images and Neumann walls
 //
 // Templates on R, the type of the spectrum, the twiddles and the transform
-// arithmetic: R = double is the FP64 path (the restatement's butterflies bit
-// for bit); R = float is the mixed path.  The x line solve is FP64 in both.
-// The mixed path solves twice (defect correction): the second pass
-// transforms the FP64 residual b - A psi of the first solution (k3_pois_resid) and
-// adds its solution to psi (ACCUM); its singular (ky, kz) = (0, 0) line has
-// its gauge pinned (last unknown zero) so that the FP32 round-off of the
-// compatibility condition cannot blow the additive constant up.
+// arithmetic; the x line solve computes in FP64.  Both the FP64 and the mixed
+// path instantiate R = double (the restatement's butterflies bit for bit):
+// one FP64 pass costs less than two FP32 passes of defect correction and
+// leaves the divergence at FP64 round-off.
 #include <cuda_pipeline.h>
 
 #include <type_traits>
@@ -228,52 +224,6 @@ __global__ void __launch_bounds__(256, 4) k3_pois_b(const double *__restrict__ u
   }
 }
 
-// the residual of the mixed path's second pass, in place: b - A psi / (ny nz)
-// from the first pass's right-hand side b (still in the scratch) and the first
-// solution psi, FP64: one thread per (i, j) walking kBPlanes planes, psi at
-// k, k + 1 carried to the next plane
-__global__ void __launch_bounds__(256, 4) k3_pois_resid(const double *__restrict__ psi,
-                                                        const double *__restrict__ pl,
-                                                        const double *__restrict__ pu, double *__restrict__ b,
-                                                        Grid3 g) {
-  const int nx = g.nx, ny = g.ny, nz = g.nz;
-  const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
-  const int k0 = 1 + blockIdx.z * kBPlanes;
-  if (i > nx || j > ny || k0 > nz) return;
-  const double l = ldg(pl + i - 1), u = ldg(pu + i - 1);
-  const double dy2 = g.dy * g.dy, dz2 = g.dz * g.dz, nn = 1. * g.ny * g.nz;
-  double *bo = b + (i - 1) + (size_t)nx * (j - 1);
-  const size_t bplane = (size_t)nx * ny;
-  double pkm = ldg(psi + ix_cc(g, i, j, k0 - 1)), pk = ldg(psi + ix_cc(g, i, j, k0));
-  constexpr int B = 2;
-#pragma unroll
-  for (int kb = 0; kb < kBPlanes; kb += B) {
-    double bb[B], pxm[B], pxp[B], pym[B], pyp[B], pzp[B];
-#pragma unroll
-    for (int h = 0; h < B; h++) {
-      const int k = min(k0 + kb + h, nz);
-      bb[h] = bo[bplane * (k - 1)];
-      pxm[h] = ldg(psi + ix_cc(g, i - 1, j, k));
-      pxp[h] = ldg(psi + ix_cc(g, i + 1, j, k));
-      pym[h] = ldg(psi + ix_cc(g, i, j - 1, k));
-      pyp[h] = ldg(psi + ix_cc(g, i, j + 1, k));
-      pzp[h] = ldg(psi + ix_cc(g, i, j, k + 1));
-    }
-#pragma unroll
-    for (int h = 0; h < B; h++) {
-      const int k = k0 + kb + h;
-      if (k > nz) break;
-      const double c = pk;
-      const double ap = (l * pxm[h] + (-l - u) * c + u * pxp[h]) + (pym[h] - 2. * c + pyp[h]) / dy2 +
-                        (pkm - 2. * c + pzp[h]) / dz2;
-      pkm = pk;
-      pk = pzp[h];
-      bo[bplane * (k - 1)] = bb[h] - ap / nn;
-    }
-  }
-}
-
 // forward transform along y of COLS consecutive i of plane k: the first pass
 // reads the right-hand side b (k3_pois_b), the last one writes the
 // ky = 0 .. N/2 half of the spectrum
@@ -370,7 +320,7 @@ template <class R, int LPB>
 __global__ void __launch_bounds__(LPB) k3_pois_x(R *__restrict__ spec, R *__restrict__ scratch,
                                                  const double *__restrict__ pl, const double *__restrict__ pu,
                                                  const double *__restrict__ evy, const double *__restrict__ evz,
-                                                 int pin_gauge, Grid3 g) {
+                                                 Grid3 g) {
   using C2 = typename Cplx<R>::T;
   using S = XShape<R, LPB>;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -386,11 +336,9 @@ __global__ void __launch_bounds__(LPB) k3_pois_x(R *__restrict__ spec, R *__rest
   const bool live = l0 + t < nlines;
   const int nchunks = (nx + XC - 1) / XC;
   double lam = 0.;
-  bool pinned = false;
   if (live) {
     const long l = l0 + t;
     lam = ldg(evy + l % nky) + ldg(evz + l / nky);
-    pinned = pin_gauge && (0 == l);
   }
   // chunk copies: element e = t + LPB r is point e % XC of line e / XC
   auto copy_in = [&](int p0, bool with_v) {
@@ -452,7 +400,7 @@ __global__ void __launch_bounds__(LPB) k3_pois_x(R *__restrict__ spec, R *__rest
           qi = val * (xi - l * qi);
         } else {
           const double val = c - l * vprev;
-          if (fabs(val) > kDblEpsilon && !pinned) {
+          if (fabs(val) > kDblEpsilon) {
             qr = 1. / val * (xr - l * qr);
             qi = 1. / val * (xi - l * qi);
           } else {
@@ -500,10 +448,10 @@ __global__ void __launch_bounds__(LPB) k3_pois_x(R *__restrict__ spec, R *__rest
 }
 
 // c2r along y (Hermitian extension as FFTW's c2r reads it: Im of X_0 and
-// X_{ny/2} ignored), psi of COLS consecutive i of plane k (ACCUM: psi +=) with
-// the halo images; the Neumann walls take the new neighbour value and hand
+// X_{ny/2} ignored), psi of COLS consecutive i of plane k with the halo
+// images; the Neumann walls take the new neighbour value and hand
 // their old value to the halo images
-template <int L2N, class R, bool ACCUM>
+template <int L2N, class R>
 __global__ void __launch_bounds__(kLineThreads, Line<R, L2N>::MINB)
     k3_pois_inv_y(const R *__restrict__ spec, double *__restrict__ psi, const R *__restrict__ tw, Grid3 g) {
   using L = Line<R, L2N>;
@@ -541,10 +489,7 @@ __global__ void __launch_bounds__(kLineThreads, Line<R, L2N>::MINB)
     const int i = i0 + c;
     double y[G];
 #pragma unroll
-    for (int q = 0; q < G; q++) {
-      y[q] = (double)xr[q];
-      if (ACCUM) y[q] += psi[ix_cc(g, i, base + q * H + 1, k)];
-    }
+    for (int q = 0; q < G; q++) y[q] = (double)xr[q];
 #pragma unroll
     for (int q = 0; q < G; q++) {
       const double v = y[q];
@@ -605,8 +550,7 @@ cudaError_t pois_prepare(int log2ny, int log2nz) {
     constexpr int sm = Line<R, L2>::SMEM;
     cudaError_t r;
     if (cudaSuccess != (r = line_attrs(k3_pois_fwd_y<L2, R>, sm))) return r;
-    if (cudaSuccess != (r = line_attrs(k3_pois_inv_y<L2, R, false>, sm))) return r;
-    return line_attrs(k3_pois_inv_y<L2, R, true>, sm);
+    return line_attrs(k3_pois_inv_y<L2, R>, sm);
   });
   if (cudaSuccess != e) return e;
   e = by_l2n(log2nz, [&](auto c) {
@@ -619,16 +563,10 @@ cudaError_t pois_prepare(int log2ny, int log2nz) {
 }
 
 template <class R>
-cudaError_t pois_fwd_y(bool resid, cudaStream_t st, const double *ux, const double *uy, const double *uz,
-                       const double *psi, const double *pl, const double *pu, double *b, R *spec, const R *tw,
-                       const double *dtp, double gam, int log2n, Grid3 g) {
+cudaError_t pois_fwd_y(cudaStream_t st, const double *ux, const double *uy, const double *uz, double *b, R *spec,
+                       const R *tw, const double *dtp, double gam, int log2n, Grid3 g) {
   const dim3 bb(32, 8), bg((g.nx + 31) / 32, (g.ny + 7) / 8, (g.nz + kBPlanes - 1) / kBPlanes);
-  if (resid) {
-    // the first pass's right-hand side is still in b
-    k3_pois_resid<<<bg, bb, 0, st>>>(psi, pl, pu, b, g);
-  } else {
-    k3_pois_b<<<bg, bb, 0, st>>>(ux, uy, uz, b, dtp, gam, g);
-  }
+  k3_pois_b<<<bg, bb, 0, st>>>(ux, uy, uz, b, dtp, gam, g);
   cudaError_t e = cudaGetLastError();
   if (cudaSuccess != e) return e;
   return by_l2n(log2n, [&](auto c) {
@@ -656,44 +594,38 @@ inline bool pois_x_narrow(long nlines) { return nlines < 148L * 4 * 128; }
 
 template <class R>
 cudaError_t pois_x(cudaStream_t st, R *spec, R *scratch, const double *pl, const double *pu, const double *evy,
-                   const double *evz, int pin_gauge, Grid3 g) {
+                   const double *evz, Grid3 g) {
   const long nlines = (long)(g.ny / 2 + 1) * g.nz;
   if (pois_x_narrow(nlines)) {
     k3_pois_x<R, 64><<<(unsigned)((nlines + 63) / 64), 64, XShape<R, 64>::SMEM, st>>>(spec, scratch, pl, pu, evy,
-                                                                                      evz, pin_gauge, g);
+                                                                                      evz, g);
   } else {
     k3_pois_x<R, 128><<<(unsigned)((nlines + 127) / 128), 128, XShape<R, 128>::SMEM, st>>>(spec, scratch, pl, pu,
-                                                                                          evy, evz, pin_gauge, g);
+                                                                                          evy, evz, g);
   }
   return cudaGetLastError();
 }
 
 template <class R>
-cudaError_t pois_inv_y(bool accum, cudaStream_t st, const R *spec, double *psi, const R *tw, int log2n, Grid3 g) {
+cudaError_t pois_inv_y(cudaStream_t st, const R *spec, double *psi, const R *tw, int log2n, Grid3 g) {
   return by_l2n(log2n, [&](auto c) {
     constexpr int L2 = decltype(c)::value;
     using L = Line<R, L2>;
     dim3 gr((g.nx + L::COLS - 1) / L::COLS, g.nz);
-    if (accum) {
-      k3_pois_inv_y<L2, R, true><<<gr, kLineThreads, L::SMEM, st>>>(spec, psi, tw, g);
-    } else {
-      k3_pois_inv_y<L2, R, false><<<gr, kLineThreads, L::SMEM, st>>>(spec, psi, tw, g);
-    }
+    k3_pois_inv_y<L2, R><<<gr, kLineThreads, L::SMEM, st>>>(spec, psi, tw, g);
     return cudaGetLastError();
   });
 }
 
 #define SVOF3_POISSON_INST(R)                                                                                    \
   template cudaError_t pois_prepare<R>(int, int);                                                                \
-  template cudaError_t pois_fwd_y<R>(bool, cudaStream_t, const double *, const double *, const double *,   \
-                                     const double *, const double *, const double *, double *, R *,             \
+  template cudaError_t pois_fwd_y<R>(cudaStream_t, const double *, const double *, const double *, double *, R *, \
                                      const R *, const double *, double, int, Grid3);                            \
   template cudaError_t pois_z<R>(cudaStream_t, R *, const R *, int, Grid3);                                      \
   template cudaError_t pois_x<R>(cudaStream_t, R *, R *, const double *, const double *, const double *,        \
-                                 const double *, int, Grid3);                                                    \
-  template cudaError_t pois_inv_y<R>(bool, cudaStream_t, const R *, double *, const R *, int, Grid3);
+                                 const double *, Grid3);                                                         \
+  template cudaError_t pois_inv_y<R>(cudaStream_t, const R *, double *, const R *, int, Grid3);
 SVOF3_POISSON_INST(double)
-SVOF3_POISSON_INST(float)
 #undef SVOF3_POISSON_INST
 
 }  // namespace svof3

@@ -83,13 +83,6 @@ int upload(DevBuf &b, const std::vector<double> &h) {
   return 0;
 }
 
-int upload_f(DevBuf &b, const std::vector<double> &h) {
-  std::vector<float> f(h.begin(), h.end());
-  if (dalloc(b, h.size(), 4)) return 1;
-  CK(cudaMemcpy(b.p, f.data(), sizeof(float) * f.size(), cudaMemcpyHostToDevice));
-  return 0;
-}
-
 void dfree(DevBuf &b) {
   if (b.p) cudaFree(b.p);
   b.p = nullptr;
@@ -114,7 +107,6 @@ struct svof3d_solver {
   double lims[4] = {0., 0., 0., 0.};  // explicit diffusive dt limits: m y, m z, t y, t z
   // Poisson
   DevBuf spec, xscratch, twf_y, twb_y, twf_z, twb_z, pl, pu, evy, evz;
-  DevBuf twf_y32, twb_y32, twf_z32, twb_z32;  // FP32 twiddles of the mixed path
   // predictor forward-sweep scratch
   DevBuf fw;
   // time step
@@ -272,40 +264,26 @@ int launch_predict(svof3d_solver *s, int rk) {
 // after each launch
 using Marker = std::function<int(int)>;
 
-template <class R>
-int launch_potential_t(svof3d_solver *s, int rk, const Marker &mark, const R *twfy, const R *twby, const R *twfz,
-                       const R *twbz) {
+// the Poisson solve, FP64 in both paths (one pass)
+int launch_potential(svof3d_solver *s, int rk, const Marker &mark = Marker()) {
   const double gam = RK_A[rk] + RK_B[rk];
   const Grid3 g = s->grid();
   auto m = [&](int kind) { return mark ? mark(kind) : 0; };
-  const int passes = s->mixed ? 2 : 1;
-  for (int pass = 0; pass < passes; pass++) {
-    const bool second = pass > 0;
-    const int cu = s->cur_u;
-    // (the right-hand side goes through the predictor's line scratch, idle
-    // here: 4 nx ny nz elements of 4 or 8 bytes)
-    CK(pois_fwd_y<R>(second, s->stream, s->ux[cu].p, s->uy[cu].p, s->uz[cu].p, s->psi.p, s->pl.p,
-                     s->pu.p, s->fw.as<double>(), s->spec.as<R>(), twfy, s->d_dt, gam, s->log2ny, g));
-    if (m(SVOF3_K_POISSON_FWD)) return 1;
-    CK(pois_z<R>(s->stream, s->spec.as<R>(), twfz, s->log2nz, g));
-    if (m(SVOF3_K_POISSON_Z)) return 1;
-    CK(pois_x<R>(s->stream, s->spec.as<R>(), s->xscratch.as<R>(), s->pl.p, s->pu.p, s->evy.p, s->evz.p,
-                 s->mixed ? 1 : 0, g));
-    if (m(SVOF3_K_POISSON_SOLVE)) return 1;
-    CK(pois_z<R>(s->stream, s->spec.as<R>(), twbz, s->log2nz, g));
-    if (m(SVOF3_K_POISSON_Z)) return 1;
-    CK(pois_inv_y<R>(second, s->stream, s->spec.as<R>(), s->psi.p, twby, s->log2ny, g));
-    if (m(SVOF3_K_POISSON_INV)) return 1;
-  }
+  const int cu = s->cur_u;
+  // (the right-hand side goes through the predictor's line scratch, idle
+  // here: 4 nx ny nz elements of 4 or 8 bytes)
+  CK(pois_fwd_y<double>(s->stream, s->ux[cu].p, s->uy[cu].p, s->uz[cu].p, s->fw.as<double>(), s->spec.p,
+                        s->twf_y.p, s->d_dt, gam, s->log2ny, g));
+  if (m(SVOF3_K_POISSON_FWD)) return 1;
+  CK(pois_z<double>(s->stream, s->spec.p, s->twf_z.p, s->log2nz, g));
+  if (m(SVOF3_K_POISSON_Z)) return 1;
+  CK(pois_x<double>(s->stream, s->spec.p, s->xscratch.p, s->pl.p, s->pu.p, s->evy.p, s->evz.p, g));
+  if (m(SVOF3_K_POISSON_SOLVE)) return 1;
+  CK(pois_z<double>(s->stream, s->spec.p, s->twb_z.p, s->log2nz, g));
+  if (m(SVOF3_K_POISSON_Z)) return 1;
+  CK(pois_inv_y<double>(s->stream, s->spec.p, s->psi.p, s->twb_y.p, s->log2ny, g));
+  if (m(SVOF3_K_POISSON_INV)) return 1;
   return 0;
-}
-
-int launch_potential(svof3d_solver *s, int rk, const Marker &mark = Marker()) {
-  if (s->mixed) {
-    return launch_potential_t<float>(s, rk, mark, s->twf_y32.as<float>(), s->twb_y32.as<float>(),
-                                     s->twf_z32.as<float>(), s->twb_z32.as<float>());
-  }
-  return launch_potential_t<double>(s, rk, mark, s->twf_y.p, s->twb_y.p, s->twf_z.p, s->twb_z.p);
 }
 
 int launch_project(svof3d_solver *s, int rk, int do_vel, int do_p) {
@@ -474,15 +452,6 @@ int build_tables(svof3d_solver *s, const double *xf, const double *xc) {
     return upload(f, twf) || upload(b, twb);
   };
   if (twiddles(ny, s->twf_y, s->twb_y) || twiddles(nz, s->twf_z, s->twb_z)) return 1;
-  // FP32 copies for the mixed path (the FP64 tables rounded once)
-  auto twiddles32 = [&](const DevBuf &src, DevBuf &dst) -> int {
-    std::vector<double> h(src.n);
-    CK(cudaMemcpy(h.data(), src.p, sizeof(double) * src.n, cudaMemcpyDeviceToHost));
-    return upload_f(dst, h);
-  };
-  if (twiddles32(s->twf_y, s->twf_y32) || twiddles32(s->twb_y, s->twb_y32) || twiddles32(s->twf_z, s->twf_z32) ||
-      twiddles32(s->twb_z, s->twb_z32))
-    return 1;
   const int nky = ny / 2 + 1;
   std::vector<double> evy(nky), evz(nz), pl(nx), pu(nx);
   for (size_t j = 0; j < (size_t)nky; j++)
@@ -515,8 +484,7 @@ int svof3d_destroy(svof3d_solver_t *s) {
   }
   DevBuf *bufs[] = {&s->p, &s->psi, &s->curv, &s->normal, &s->ifrcx, &s->ifrcy, &s->ifrcz, &s->dxf, &s->dxc,
                     &s->lap_ux, &s->lap_cc, &s->coef, &s->spec, &s->xscratch, &s->twf_y, &s->twb_y, &s->twf_z,
-                    &s->twb_z, &s->pl, &s->pu, &s->evy, &s->evz, &s->fw, &s->diag, &s->twf_y32, &s->twb_y32,
-                    &s->twf_z32, &s->twb_z32, &s->stat_part};
+                    &s->twb_z, &s->pl, &s->pu, &s->evy, &s->evz, &s->fw, &s->diag, &s->stat_part};
   for (DevBuf *b : bufs) dfree(*b);
   for (DevBuf &b : s->stat) dfree(b);
   if (s->d_dt) cudaFree(s->d_dt);
@@ -575,12 +543,11 @@ int svof3d_create(const svof3d_params_t *prm, const double *xf, const double *xc
   if (build_tables(s, xf, xc)) return bail();
   if (dalloc(s->coef, 9 * nx)) return bail();
   const size_t nky = ny / 2 + 1;
-  if (dalloc(s->spec, 2 * nx * nky * nz, es) || dalloc(s->xscratch, nx * nky * nz, es) ||
+  if (dalloc(s->spec, 2 * nx * nky * nz) || dalloc(s->xscratch, nx * nky * nz) ||
       dalloc(s->fw, 4 * nx * ny * nz, es))
     return bail();
   {
-    const cudaError_t pe = s->mixed ? pois_prepare<float>(s->log2ny, s->log2nz)
-                                    : pois_prepare<double>(s->log2ny, s->log2nz);
+    const cudaError_t pe = pois_prepare<double>(s->log2ny, s->log2nz);
     if (cudaSuccess != pe || cudaSuccess != predict_prepare() || cudaSuccess != interface_prepare())
       return fail("cudaFuncSetAttribute(Poisson): %s", cudaGetErrorString(cudaGetLastError())), bail();
     const size_t coef_smem = sizeof(double) * 6 * nx;

@@ -143,28 +143,24 @@ __global__ void k3_tdm_coef(const double *__restrict__ lap_ux, const double *__r
                             double *__restrict__ coef);
 
 // Poisson: spectral array S[kz][ky][i] (complex, i fastest)
-// Poisson stages (k3_poisson.cu), templates on R = double (FP64 path) or float
-// (mixed path): R is the type of the spectrum, the twiddles and the transform
-// arithmetic; the x line solve is FP64.  The transforms are compiled for each
-// length 2^1 .. 2^11 (log2n outside that range is an invalid value).
-// resid: transform the residual b - A psi of the current psi instead of b,
-// formed in place from the b of the previous (first) pass, which must still
-// be in the scratch; accum: psi += the inverse; pin_gauge: zero the last
-// unknown of the singular (ky, kz) = (0, 0) line.
+// Poisson stages (k3_poisson.cu), templates on R, the type of the spectrum,
+// the twiddles and the transform arithmetic; the FP64 and the mixed path
+// both use R = double.  The x line solve is FP64.  The transforms are
+// compiled for each length 2^1 .. 2^11 (log2n outside that range is an
+// invalid value).
 template <class R>
 cudaError_t pois_prepare(int log2ny, int log2nz);
 // (b: scratch of nx ny nz doubles for the right-hand side)
 template <class R>
-cudaError_t pois_fwd_y(bool resid, cudaStream_t st, const double *ux, const double *uy, const double *uz,
-                       const double *psi, const double *pl, const double *pu, double *b, R *spec, const R *tw,
-                       const double *dtp, double gam, int log2n, Grid3 g);
+cudaError_t pois_fwd_y(cudaStream_t st, const double *ux, const double *uy, const double *uz, double *b, R *spec,
+                       const R *tw, const double *dtp, double gam, int log2n, Grid3 g);
 template <class R>
 cudaError_t pois_z(cudaStream_t st, R *spec, const R *tw, int log2n, Grid3 g);
 template <class R>
 cudaError_t pois_x(cudaStream_t st, R *spec, R *scratch, const double *pl, const double *pu, const double *evy,
-                   const double *evz, int pin_gauge, Grid3 g);
+                   const double *evz, Grid3 g);
 template <class R>
-cudaError_t pois_inv_y(bool accum, cudaStream_t st, const R *spec, double *psi, const R *tw, int log2n, Grid3 g);
+cudaError_t pois_inv_y(cudaStream_t st, const R *spec, double *psi, const R *tw, int log2n, Grid3 g);
 
 // projection and pressure update, in place
 __global__ void k3_project(double *__restrict__ ux, double *__restrict__ uy, double *__restrict__ uz,

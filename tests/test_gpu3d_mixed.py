@@ -2,9 +2,10 @@
 FP64 GPU path.
 
 The mixed path keeps the state (velocities, pressure, psi, t, vof, vof
-sources) in FP64 and runs the interface geometry, THINC and the transforms in
-FP32 with FP32 intermediates; the projection solves twice (FP64 residual,
-defect correction).  Bounds, stated per result: velocity relative L2 error
+sources) in FP64 and runs the interface geometry and THINC in FP32 with FP32
+intermediates (curvature, normals, forces, momentum sources, increments);
+the momentum stencils, the x line solves and the Poisson solve are FP64.
+Bounds, stated per result: velocity relative L2 error
 <= 1e-5 against the FP64 reference after the run, max |div u| <= 1e-10 and
 total-volume drift <= 1e-10.
 """
