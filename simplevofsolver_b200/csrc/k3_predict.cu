@@ -455,10 +455,18 @@ constexpr int PL = kPredLines, PC = kPredChunk;
 // ping-pong pair, halo images included, then the walls.  The tile holds the
 // storage type R (in the mixed path the swept increments are FP32, as in the
 // line array).
+// chunk buffers: the FP32 tile (mixed path) is double-buffered, so that the
+// copies of chunk c + 1 are in flight while chunk c is swept (a 4-byte copy
+// carries half the bytes of an FP64 one); the FP64 tile stays single, within
+// the 48 KB of static shared memory
+template <class R>
+constexpr int kXsBufs = 4 == sizeof(R) ? 2 : 1;
+
 template <class R>
 __global__ void __launch_bounds__(256) k3_xsolve(Predict3Args<R> a) {
-  __shared__ R sd[4][PL][PC + 1];  // the four fields' values of one tile
-  __shared__ double sco[9][PC];         // L, R, V of the three systems, one chunk
+  constexpr int NB = kXsBufs<R>;
+  __shared__ R sd[NB][4][PL][PC + 1];  // the four fields' values of one tile
+  __shared__ double sco[NB][9][PC];    // L, R, V of the three systems, one chunk
   const Grid3 g = a.g;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const long nlines = (long)ny * nz;
@@ -472,15 +480,19 @@ __global__ void __launch_bounds__(256) k3_xsolve(Predict3Args<R> a) {
   const int set = (0 == f) ? 0 : (3 == f ? 2 : 1);
   const int nf = (0 == f) ? nx - 1 : nx;
   const size_t fstride = (size_t)nlines * nx;  // line array per field
-  double carry = 0.;
-
-  // ------------------------------------------------------------ forward
-  for (int c = 0; c < nchunks; c++) {
+  // coefficients of chunk c into buffer b: all nine rows (forward) or the
+  // three V rows (backward)
+  auto load_coef = [&](int c, int b, bool fwd) {
     const int p0 = c * PC;
-    for (int w = tid; w < 9 * PC; w += 256) {
+    for (int w = tid; w < (fwd ? 9 : 3) * PC; w += 256) {
       const int r = w / PC, q = w - r * PC;
-      sco[r][q] = (p0 + q < nx) ? ldg(a.coef + (size_t)r * nx + p0 + q) : 0.;
+      const int row = fwd ? r : 3 * r + 2;
+      sco[b][row][q] = (p0 + q < nx) ? ldg(a.coef + (size_t)row * nx + p0 + q) : 0.;
     }
+  };
+  // the four fields of chunk c of the block's lines into buffer b, one commit group
+  auto load_tile = [&](int c, int b) {
+    const int p0 = c * PC;
 #pragma unroll 1
     for (int m = 0; m < 4; m++) {
       const int ll = ty + 8 * m;
@@ -488,18 +500,42 @@ __global__ void __launch_bounds__(256) k3_xsolve(Predict3Args<R> a) {
       const int p = p0 + tx;
       if (l >= nlines || p >= nx) continue;
       const R *fw = a.fw + (size_t)l * nx + p;
-      if (p < nx - 1) __pipeline_memcpy_async(&sd[0][ll][tx], fw, sizeof(R));
-      else sd[0][ll][tx] = R(0.);
-      __pipeline_memcpy_async(&sd[1][ll][tx], fw + fstride, sizeof(R));
-      __pipeline_memcpy_async(&sd[2][ll][tx], fw + 2 * fstride, sizeof(R));
-      __pipeline_memcpy_async(&sd[3][ll][tx], fw + 3 * fstride, sizeof(R));
+      if (p < nx - 1) __pipeline_memcpy_async(&sd[b][0][ll][tx], fw, sizeof(R));
+      else sd[b][0][ll][tx] = R(0.);
+      __pipeline_memcpy_async(&sd[b][1][ll][tx], fw + fstride, sizeof(R));
+      __pipeline_memcpy_async(&sd[b][2][ll][tx], fw + 2 * fstride, sizeof(R));
+      __pipeline_memcpy_async(&sd[b][3][ll][tx], fw + 3 * fstride, sizeof(R));
     }
     __pipeline_commit();
-    __pipeline_wait_prior(0);
+  };
+  // chunk c (position `it` of the walk) in place: with two buffers the next
+  // chunk of the walk is requested first and one group may stay in flight
+  auto stage = [&](int it, int c, int cnext, bool fwd) {
+    if (NB > 1 && it + 1 < nchunks) {
+      load_coef(cnext, (it + 1) % NB, fwd);
+      load_tile(cnext, (it + 1) % NB);
+      __pipeline_wait_prior(1);
+    } else {
+      if (NB == 1 && it > 0) {
+        load_coef(c, 0, fwd);
+        load_tile(c, 0);
+      }
+      __pipeline_wait_prior(0);
+    }
     __syncthreads();
+  };
+  double carry = 0.;
+
+  // ------------------------------------------------------------ forward
+  load_coef(0, 0, true);
+  load_tile(0, 0);
+  for (int c = 0; c < nchunks; c++) {
+    const int b = c % NB;
+    const int p0 = c * PC;
+    stage(c, c, c + 1, true);
     if (sweeper) {
-      R *q = sd[f][tx];
-      const double *L = sco[3 * set], *Rr = sco[3 * set + 1];
+      R *q = sd[b][f][tx];
+      const double *L = sco[b][3 * set], *Rr = sco[b][3 * set + 1];
       const int smax = min(PC, nf - p0);
 #pragma unroll 4
       for (int s = 0; s < smax; s++) {
@@ -523,41 +559,26 @@ __global__ void __launch_bounds__(256) k3_xsolve(Predict3Args<R> a) {
       const int p = p0 + tx;
       if (l >= nlines || p >= nx) continue;
       R *fw = a.fw + (size_t)l * nx + p;
-      if (p < nx - 1) fw[0] = R(sd[0][ll][tx]);
-      fw[fstride] = R(sd[1][ll][tx]);
-      fw[2 * fstride] = R(sd[2][ll][tx]);
-      fw[3 * fstride] = R(sd[3][ll][tx]);
+      if (p < nx - 1) fw[0] = R(sd[b][0][ll][tx]);
+      fw[fstride] = R(sd[b][1][ll][tx]);
+      fw[2 * fstride] = R(sd[b][2][ll][tx]);
+      fw[3 * fstride] = R(sd[b][3][ll][tx]);
     }
     __syncthreads();
   }
 
   // ------------------------------------------------------------ backward
   double nxt = 0.;
-  for (int c = nchunks - 1; c >= 0; c--) {
+  load_coef(nchunks - 1, 0, false);
+  load_tile(nchunks - 1, 0);
+  for (int it = 0; it < nchunks; it++) {
+    const int c = nchunks - 1 - it;
+    const int b = it % NB;
     const int p0 = c * PC;
-    for (int w = tid; w < 3 * PC; w += 256) {
-      const int r = w / PC, q = w - r * PC;
-      sco[3 * r + 2][q] = (p0 + q < nx) ? ldg(a.coef + (size_t)(3 * r + 2) * nx + p0 + q) : 0.;
-    }
-#pragma unroll 1
-    for (int m = 0; m < 4; m++) {
-      const int ll = ty + 8 * m;
-      const long l = l0 + ll;
-      const int p = p0 + tx;
-      if (l >= nlines || p >= nx) continue;
-      const R *fw = a.fw + (size_t)l * nx + p;
-      if (p < nx - 1) __pipeline_memcpy_async(&sd[0][ll][tx], fw, sizeof(R));
-      else sd[0][ll][tx] = R(0.);
-      __pipeline_memcpy_async(&sd[1][ll][tx], fw + fstride, sizeof(R));
-      __pipeline_memcpy_async(&sd[2][ll][tx], fw + 2 * fstride, sizeof(R));
-      __pipeline_memcpy_async(&sd[3][ll][tx], fw + 3 * fstride, sizeof(R));
-    }
-    __pipeline_commit();
-    __pipeline_wait_prior(0);
-    __syncthreads();
+    stage(it, c, c - 1, false);
     if (sweeper) {
-      R *q = sd[f][tx];
-      const double *V = sco[3 * set + 2];
+      R *q = sd[b][f][tx];
+      const double *V = sco[b][3 * set + 2];
       const int smax = min(PC, nf - p0);
 #pragma unroll 4
       for (int s = smax - 1; s >= 0; s--) {
@@ -580,15 +601,15 @@ __global__ void __launch_bounds__(256) k3_xsolve(Predict3Args<R> a) {
       const int j = 1 + (int)(l % ny), k = 1 + (int)(l / ny);
       if (p < nx - 1) {
         const int i = p + 2;
-        const double v = ldg(a.ux + ix_ux(g, i, j, k)) + sd[0][ll][tx];
+        const double v = ldg(a.ux + ix_ux(g, i, j, k)) + sd[b][0][ll][tx];
         for_images(j, k, ny, nz, true, [&](int jj, int kk) { a.ux_new[ix_ux(g, i, jj, kk)] = v; });
       }
       {
         const int i = p + 1;
         const long ic = ix_cc(g, i, j, k);
-        const double vy = ldg(a.uy + ic) + sd[1][ll][tx];
-        const double vz = ldg(a.uz + ic) + sd[2][ll][tx];
-        const double vt = ldg(a.t + ic) + sd[3][ll][tx];
+        const double vy = ldg(a.uy + ic) + sd[b][1][ll][tx];
+        const double vz = ldg(a.uz + ic) + sd[b][2][ll][tx];
+        const double vt = ldg(a.t + ic) + sd[b][3][ll][tx];
         for_images(j, k, ny, nz, true, [&](int jj, int kk) {
           const long o = ix_cc(g, i, jj, kk);
           a.uy_new[o] = vy;
