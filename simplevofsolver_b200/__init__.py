@@ -123,6 +123,7 @@ def lib() -> ctypes.CDLL:
         L.svof_statistics_count.argtypes = [vp, ctypes.POINTER(sz)]
         L.svof_statistics_reduce.argtypes = [vp, i, dp, sz]
         L.svof_statistics_field.argtypes = [vp, i, dp, sz]
+        L.svof_poisson_dct_noalloc.argtypes = [ctypes.POINTER(Params), dp, dp, dp, dp, sz, d, vp]
         L.svof_synchronize.argtypes = [vp]
         L.svof_profile_step.argtypes = [vp, dp, dp, i]
         L.svof_stream.argtypes = [vp, ctypes.POINTER(vp)]

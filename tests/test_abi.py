@@ -43,6 +43,17 @@ def test_python_host_binds_every_exported_entry():
     assert {n for n in declared if n.startswith("svof3d_")} == set(svof.EXPORTS3D)
 
 
+def test_every_declared_entry_has_argtypes():
+    """the Python host declares the argument types of every C-ABI function
+    (the two error-string getters take none)"""
+    from simplevofsolver_b200.solver3d import lib3
+    L = lib3()
+    for name in declared_functions():
+        if name in ("svof_last_error", "svof3d_last_error"):
+            continue
+        assert getattr(L, name).argtypes is not None, name
+
+
 def test_create_fails_cleanly_without_device():
     """without a GPU, svof_create reports an error instead of crashing"""
     import torch
