@@ -1,10 +1,14 @@
-"""Generates the golden fixtures of tests/test_oracle_pin.py.
+"""Generates the golden fixtures of tests/test_oracle_pin.py and
+tests/test_statistics.py.
 
 Runs the reference's own sources (compiled by oracle/Makefile into
 oracle/_ref/libsvof_ref*.so from the reference tree, against single-rank
 shims) on small seeded droplet cases and stores the fields after 1 and 10
-steps.  Needs the reference tree only to build oracle/_ref; the fixtures are
-then committed so the tests can pin the oracle anywhere.
+steps.  The statistics fixture is the output of the reference's own host
+program (oracle/_ref/svof_main_ref: main.c, statistics.c and the solver
+sources) on a 32 x 32 droplet: the row sums it writes to output/stat and
+its sample count.  Needs the reference tree only to build oracle/_ref; the
+fixtures are then committed so the tests can pin the oracle anywhere.
 
     python tests/golden/make_golden.py
 """
@@ -29,6 +33,46 @@ CASES = {
 }
 NAMES = ("ux", "uy", "p", "psi", "t", "vof")
 
+# the statistics case: the reference's own parameters (src/param/: buoyancy,
+# hot and cold walls), samples every 0.01 from 0.02 to 0.12
+STAT_ENV = {
+    "timemax": "0.12", "wtimemax": "600", "log_rate": "1e9", "save_rate": "1e9", "save_after": "1e9",
+    "stat_rate": "0.01", "stat_after": "0.02", "coef_dt_adv": "0.5", "coef_dt_dif": "0.95",
+    "Ra": "1.0e4", "Pr": "1.0", "We": "10.0",
+}
+STAT_NAMES = ("ux1", "ux2", "uy1", "uy2", "t1", "t2", "uxt")
+
+
+def statistics_case():
+    """the 32 x 32 stretched droplet with a temperature field and a visible
+    velocity"""
+    ic = droplet2d(32, 32, uniform=False, noise=1e-2, seed=4)
+    xc = ic.xc[1:-1]
+    yc = (np.arange(ic.ny) + 0.5) / ic.ny * ic.ly
+    ic.t[:, 1:-1] = 0.4 * (0.5 - xc)[None, :] + 0.1 * np.sin(2 * np.pi * yc)[:, None] * np.sin(np.pi * xc)[None, :]
+    return ic
+
+
+def make_statistics():
+    import glob
+    import subprocess
+    import tempfile
+    from simplevofsolver_b200.workloads import write_npy_dir
+    exe = os.path.join(ROOT, "oracle", "_ref", "svof_main_ref")
+    with tempfile.TemporaryDirectory() as tmp:
+        write_npy_dir(statistics_case(), os.path.join(tmp, "ic"))
+        for d in ("log", "save", "stat"):
+            os.makedirs(os.path.join(tmp, "run", "output", d))
+        env = dict(os.environ)
+        env.update(STAT_ENV)
+        subprocess.run([exe, os.path.join(tmp, "ic")], cwd=os.path.join(tmp, "run"), env=env, check=True,
+                       capture_output=True)
+        (stat,) = glob.glob(os.path.join(tmp, "run", "output", "stat", "step*"))
+        out = {k: np.load(os.path.join(stat, f"{k}.npy")) for k in STAT_NAMES}
+        out["num"] = np.load(os.path.join(stat, "num.npy"))
+    np.savez_compressed(os.path.join(HERE, "statistics_32x32.npz"), **out)
+    print("wrote statistics_32x32")
+
 
 def main():
     for name, (make, env, variant) in CASES.items():
@@ -41,6 +85,7 @@ def main():
                 out[f"{k}_{nsteps}"] = r[k]
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
         print("wrote", name)
+    make_statistics()
 
 
 if __name__ == "__main__":

@@ -7,7 +7,10 @@ run (src/statistics.c; the schedule in src/main.c:137-140).
 - The oracle's restatement (svo_stat_collect / svo_stat_reduce) is pinned
   here against the reference program itself, oracle/_ref/svof_main_ref. Its
   saves and its statistics fire at the same steps, so the restatement applied
-  to the saved states reproduces the statistics it wrote, bit for bit.
+  to the saved states reproduces the statistics it wrote, bit for bit. The
+  program's output for a 32 x 32 case is also committed as a fixture
+  (tests/golden/statistics_32x32.npz), which the oracle reproduces from its
+  own trajectory where the reference cannot be built.
 - The device kernels, given the same fields as the oracle, reproduce its
   sums of ux, uy, (uz,) t and ux t bit for bit. The sums of squares agree
   within 1e-13 relative: the device squares are correctly rounded products,
@@ -80,6 +83,37 @@ def compare(got, ref, names):
             np.testing.assert_allclose(got[k], ref[k], rtol=1e-13, atol=0, err_msg=k)
         else:
             assert np.array_equal(got[k], ref[k]), (k, np.abs(got[k] - ref[k]).max())
+
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "statistics_32x32.npz")
+
+
+def test_oracle_statistics_reproduce_golden():
+    """the oracle runs the reference program's schedule (src/main.c:111-141,
+    src/statistics.c:59-75) and reproduces its statistics output, committed
+    as a fixture by tests/golden/make_golden.py, bit for bit"""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "make_golden", os.path.join(os.path.dirname(GOLDEN), "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    golden = np.load(GOLDEN)
+    env = mg.STAT_ENV
+    o = Oracle(mg.statistics_case(), physical_params(DROPLET2D_ENV), add_buoyancy=True, t_walls=T_WALLS)
+    timemax, rate, after = float(env["timemax"]), float(env["stat_rate"]), float(env["stat_after"])
+    time = 0.0
+    nxt = rate * math.ceil(max(sys.float_info.epsilon, max(time, after)) / rate)
+    while True:
+        time += o.run(1)[0]
+        if timemax < time:
+            break
+        if nxt < time:
+            o.statistics_collect()
+            nxt += rate
+    got = o.statistics_reduced()
+    assert got["num"] == int(golden["num"]) >= 4
+    for k in STAT_NAMES:
+        assert np.array_equal(got[k], golden[k]), (k, np.abs(got[k] - golden[k]).max())
 
 
 @pytest.mark.skipif(not os.path.exists(REF_MAIN), reason="reference host program not built")
