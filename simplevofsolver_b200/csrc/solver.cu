@@ -1061,15 +1061,23 @@ static int stat_width(const svof_solver *s, int q) {
 
 int svof_statistics_collect(svof_solver_t *s) {
   if (!s) return fail("null argument");
-  if (!s->stat[0].p) {
-    for (int q = 0; q < SVOF_NSTATS; q++) {
-      DevBuf &b = s->stat[q];
-      b.n = (size_t)stat_width(s, q) * s->ny;
-      CK(cudaMalloc(&b.p, sizeof(double) * b.n));
-      CK(cudaMemsetAsync(b.p, 0, sizeof(double) * b.n, s->stream));
+  if (!s->stat_part.p) {
+    // all accumulators and the row-sum scratch, or none: a failed allocation
+    // frees what it made, and the next collection tries again
+    DevBuf made[SVOF_NSTATS + 1];
+    cudaError_t e = cudaSuccess;
+    for (int q = 0; q <= SVOF_NSTATS && cudaSuccess == e; q++) {
+      made[q].n = q < SVOF_NSTATS ? (size_t)stat_width(s, q) * s->ny : 2 * (size_t)(s->nx + 2);
+      e = cudaMalloc(&made[q].p, sizeof(double) * made[q].n);
+      if (cudaSuccess == e && q < SVOF_NSTATS)
+        e = cudaMemsetAsync(made[q].p, 0, sizeof(double) * made[q].n, s->stream);
     }
-    s->stat_part.n = 2 * (size_t)(s->nx + 2);
-    CK(cudaMalloc(&s->stat_part.p, sizeof(double) * s->stat_part.n));
+    if (cudaSuccess != e) {
+      for (DevBuf &b : made) dfree(b);
+      return fail("statistics accumulators: %s", cudaGetErrorString(e));
+    }
+    for (int q = 0; q < SVOF_NSTATS; q++) s->stat[q] = made[q];
+    s->stat_part = made[SVOF_NSTATS];
   }
   StatArgs a{s->ux[s->cur_u].p, s->uy[s->cur_u].p, nullptr, s->t[s->cur_u].p,
              s->stat[SVOF_STAT_UX1].p, s->stat[SVOF_STAT_UX2].p, s->stat[SVOF_STAT_UY1].p,
@@ -1102,7 +1110,7 @@ int svof_statistics_reduce(svof_solver_t *s, int quantity, double *out, size_t c
   if (quantity < 0 || quantity >= SVOF_NSTATS) return fail("unknown statistics quantity %d", quantity);
   const int w = stat_width(s, quantity);
   if (count != (size_t)w) return fail("statistics quantity %d has %d columns, got %zu", quantity, w, count);
-  if (!s->stat[0].p) {
+  if (!s->stat_part.p) {
     for (int i = 0; i < w; i++) out[i] = 0.;
     return 0;
   }
@@ -1121,7 +1129,7 @@ int svof_statistics_field(svof_solver_t *s, int quantity, double *out, size_t co
   if (quantity < 0 || quantity >= SVOF_NSTATS) return fail("unknown statistics quantity %d", quantity);
   const size_t n = (size_t)stat_width(s, quantity) * s->ny;
   if (count != n) return fail("statistics quantity %d holds %zu values, got %zu", quantity, n, count);
-  if (!s->stat[0].p) {
+  if (!s->stat_part.p) {
     for (size_t q = 0; q < n; q++) out[q] = 0.;
     return 0;
   }

@@ -373,11 +373,11 @@ int interior_layout(const svof3d_solver *s, int field, int *nh, int *width) {
 int io_slot(svof3d_solver *s, svof3d_solver::IoSlot &q, size_t count) {
   if (!s->io_h2d) CK(cudaStreamCreateWithFlags(&s->io_h2d, cudaStreamNonBlocking));
   if (!s->io_d2h) CK(cudaStreamCreateWithFlags(&s->io_d2h, cudaStreamNonBlocking));
-  if (!q.stage) {
-    CK(cudaMalloc(&q.stage, sizeof(double) * count));
-    CK(cudaEventCreateWithFlags(&q.filled, cudaEventDisableTiming));
-    CK(cudaEventCreateWithFlags(&q.drained, cudaEventDisableTiming));
-  }
+  // the events first and the buffer last, so that a slot with a buffer is
+  // complete (a failure leaves the events for the next attempt)
+  if (!q.filled) CK(cudaEventCreateWithFlags(&q.filled, cudaEventDisableTiming));
+  if (!q.drained) CK(cudaEventCreateWithFlags(&q.drained, cudaEventDisableTiming));
+  if (!q.stage) CK(cudaMalloc(&q.stage, sizeof(double) * count));
   return 0;
 }
 
@@ -904,15 +904,23 @@ static int stat_width(const svof3d_solver *s, int q) {
 
 int svof3d_statistics_collect(svof3d_solver_t *s) {
   if (!s) return fail("null argument");
-  if (!s->stat[0].p) {
-    for (int q = 0; q < SVOF3_NSTATS; q++) {
-      DevBuf &b = s->stat[q];
-      b.n = (size_t)stat_width(s, q) * s->ny * s->nz;
-      CK(cudaMalloc(&b.p, sizeof(double) * b.n));
-      CK(cudaMemsetAsync(b.p, 0, sizeof(double) * b.n, s->stream));
+  if (!s->stat_part.p) {
+    // all accumulators and the row-sum scratch, or none: a failed allocation
+    // frees what it made, and the next collection tries again
+    DevBuf made[SVOF3_NSTATS + 1];
+    cudaError_t e = cudaSuccess;
+    for (int q = 0; q <= SVOF3_NSTATS && cudaSuccess == e; q++) {
+      made[q].n = q < SVOF3_NSTATS ? (size_t)stat_width(s, q) * s->ny * s->nz : (size_t)(s->nz + 1) * (s->nx + 2);
+      e = cudaMalloc(&made[q].p, sizeof(double) * made[q].n);
+      if (cudaSuccess == e && q < SVOF3_NSTATS)
+        e = cudaMemsetAsync(made[q].p, 0, sizeof(double) * made[q].n, s->stream);
     }
-    s->stat_part.n = (size_t)(s->nz + 1) * (s->nx + 2);
-    CK(cudaMalloc(&s->stat_part.p, sizeof(double) * s->stat_part.n));
+    if (cudaSuccess != e) {
+      for (DevBuf &b : made) dfree(b);
+      return fail("statistics accumulators: %s", cudaGetErrorString(e));
+    }
+    for (int q = 0; q < SVOF3_NSTATS; q++) s->stat[q] = made[q];
+    s->stat_part = made[SVOF3_NSTATS];
   }
   StatArgs a{s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->uz[s->cur_u].p, s->t[s->cur_u].p,
              s->stat[SVOF3_STAT_UX1].p, s->stat[SVOF3_STAT_UX2].p, s->stat[SVOF3_STAT_UY1].p,
@@ -946,7 +954,7 @@ int svof3d_statistics_reduce(svof3d_solver_t *s, int quantity, double *out, size
   if (quantity < 0 || quantity >= SVOF3_NSTATS) return fail("unknown statistics quantity %d", quantity);
   const int w = stat_width(s, quantity);
   if (count != (size_t)w) return fail("statistics quantity %d has %d columns, got %zu", quantity, w, count);
-  if (!s->stat[0].p) {
+  if (!s->stat_part.p) {
     for (int i = 0; i < w; i++) out[i] = 0.;
     return 0;
   }
@@ -966,7 +974,7 @@ int svof3d_statistics_field(svof3d_solver_t *s, int quantity, double *out, size_
   if (quantity < 0 || quantity >= SVOF3_NSTATS) return fail("unknown statistics quantity %d", quantity);
   const size_t n = (size_t)stat_width(s, quantity) * s->ny * s->nz;
   if (count != n) return fail("statistics quantity %d holds %zu values, got %zu", quantity, n, count);
-  if (!s->stat[0].p) {
+  if (!s->stat_part.p) {
     for (size_t q = 0; q < n; q++) out[q] = 0.;
     return 0;
   }
