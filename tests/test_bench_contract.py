@@ -1,0 +1,55 @@
+"""bench.py's output contract, checked on CPU through its reference arm (the
+3D restatement on the host cores, which needs no GPU): one JSON line with
+the metric, the whole-host value, the CPU-baseline record and an end-to-end
+record without host-device copies, printed by rank 0 alone when the bench
+runs under torchrun."""
+import json
+import os
+import socket
+import subprocess
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _json_lines(text):
+    out = []
+    for line in text.splitlines():
+        line = line.strip()
+        if line.startswith("{"):
+            out.append(json.loads(line))
+    return out
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def test_reference_arm_line():
+    r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "1", "--warmup", "1"],
+                       cwd=ROOT, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    (line,) = _json_lines(r.stdout)
+    assert line["impl"] == "reference"
+    assert line["metric"] == "Mcell-steps/s" and line["unit"] == "Mcell-steps/s"
+    assert line["value"] > 0 and line["higher_is_better"] is True
+    assert line["steps"] == 1 and line["warmup"] >= 3  # at least three warm-up steps, whatever is asked
+    assert line["config"]["workload"] == "droplets3d_512"
+    cpu = line["cpu_baseline"]
+    assert cpu["value"] == line["value"] and cpu["cores"] >= 1 and cpu["kind"] in ("port", "reference")
+    assert cpu["sample"]
+    e2e = line["e2e"]
+    assert e2e["value"] == line["value"] and e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
+
+
+def test_reference_arm_prints_once_under_torchrun():
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+           "--master-addr", "127.0.0.1", "--master-port", str(_free_port()),
+           "bench.py", "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "1"]
+    r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = _json_lines(r.stdout)
+    assert len(lines) == 1, r.stdout[-2000:]
+    assert lines[0]["impl"] == "reference"
