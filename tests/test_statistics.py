@@ -116,6 +116,29 @@ def test_oracle_statistics_reproduce_golden():
         assert np.array_equal(got[k], golden[k]), (k, np.abs(got[k] - golden[k]).max())
 
 
+def test_oracle3d_statistics_reduce_to_2d():
+    """the 3D statistics restatement on a 2D field repeated along z: each z
+    plane accumulates what the pinned 2D restatement accumulates, and the
+    y-z sum is the sum of those plane sums in z order"""
+    from simplevofsolver_b200.workloads import extrude_z
+    ic2 = lively_droplet(32, 32, uniform=False)
+    nz = 4
+    phys = physical_params(DROPLET2D_ENV)
+    o2 = Oracle(ic2, phys, add_buoyancy=True, t_walls=T_WALLS)
+    o3 = Oracle3D(extrude_z(ic2, nz), phys, add_buoyancy=True, t_walls=T_WALLS)
+    for _ in range(2):
+        o2.statistics_collect()
+        o3.statistics_collect()
+    r2, r3 = o2.statistics_reduced(), o3.statistics_reduced()
+    assert r2["num"] == r3["num"] == 2
+    for k in STAT_NAMES:
+        want = np.zeros_like(r2[k])
+        for _ in range(nz):
+            want = want + r2[k]
+        assert np.array_equal(r3[k], want), k
+    assert not r3["uz1"].any() and not r3["uz2"].any()
+
+
 @pytest.mark.skipif(not os.path.exists(REF_MAIN), reason="reference host program not built")
 def test_oracle_statistics_reproduce_reference_output(tmp_path):
     ic = lively_droplet(32, 32, uniform=False)
