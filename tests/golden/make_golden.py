@@ -4,10 +4,11 @@ tests/test_statistics.py.
 Runs the reference's own sources (compiled by oracle/Makefile into
 oracle/_ref/libsvof_ref*.so from the reference tree, against single-rank
 shims) on small seeded droplet cases and stores the fields after 1 and 10
-steps.  The statistics fixture is the output of the reference's own host
-program (oracle/_ref/svof_main_ref: main.c, statistics.c and the solver
-sources) on a 32 x 32 droplet: the row sums it writes to output/stat and
-its sample count.  Needs the reference tree only to build oracle/_ref; the
+steps.  The statistics and logging fixtures are outputs of the reference's
+own host program (oracle/_ref/svof_main_ref: main.c, statistics.c, logging/
+and the solver sources) on a 32 x 32 droplet: the row sums it writes to
+output/stat with its sample count, and its momentum.dat, energy.dat and
+nusselt.dat.  Needs the reference tree only to build oracle/_ref; the
 fixtures are then committed so the tests can pin the oracle anywhere.
 
     python tests/golden/make_golden.py
@@ -53,21 +54,42 @@ def statistics_case():
     return ic
 
 
-def make_statistics():
-    import glob
+# the logging case: the same droplet, logged every 0.02 up to 0.2
+LOG_ENV = dict(STAT_ENV, timemax="0.2", log_rate="0.02", stat_rate="1e9", stat_after="1e9")
+
+
+def run_reference_program(env, tmp):
+    """the reference's own host program on statistics_case() in tmp; returns its
+    output directory"""
     import subprocess
-    import tempfile
     from simplevofsolver_b200.workloads import write_npy_dir
     exe = os.path.join(ROOT, "oracle", "_ref", "svof_main_ref")
+    write_npy_dir(statistics_case(), os.path.join(tmp, "ic"))
+    for d in ("log", "save", "stat"):
+        os.makedirs(os.path.join(tmp, "run", "output", d))
+    full = dict(os.environ)
+    full.update(env)
+    subprocess.run([exe, os.path.join(tmp, "ic")], cwd=os.path.join(tmp, "run"), env=full, check=True,
+                   capture_output=True)
+    return os.path.join(tmp, "run", "output")
+
+
+def make_logging():
+    import tempfile
     with tempfile.TemporaryDirectory() as tmp:
-        write_npy_dir(statistics_case(), os.path.join(tmp, "ic"))
-        for d in ("log", "save", "stat"):
-            os.makedirs(os.path.join(tmp, "run", "output", d))
-        env = dict(os.environ)
-        env.update(STAT_ENV)
-        subprocess.run([exe, os.path.join(tmp, "ic")], cwd=os.path.join(tmp, "run"), env=env, check=True,
-                       capture_output=True)
-        (stat,) = glob.glob(os.path.join(tmp, "run", "output", "stat", "step*"))
+        out = run_reference_program(LOG_ENV, tmp)
+        logs = {name: np.loadtxt(os.path.join(out, "log", f"{name}.dat"), ndmin=2)
+                for name in ("momentum", "energy", "nusselt")}
+    np.savez_compressed(os.path.join(HERE, "logging_32x32.npz"), **logs)
+    print("wrote logging_32x32")
+
+
+def make_statistics():
+    import glob
+    import tempfile
+    with tempfile.TemporaryDirectory() as tmp:
+        out = run_reference_program(STAT_ENV, tmp)
+        (stat,) = glob.glob(os.path.join(out, "stat", "step*"))
         out = {k: np.load(os.path.join(stat, f"{k}.npy")) for k in STAT_NAMES}
         out["num"] = np.load(os.path.join(stat, "num.npy"))
     np.savez_compressed(os.path.join(HERE, "statistics_32x32.npz"), **out)
@@ -86,6 +108,7 @@ def main():
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
         print("wrote", name)
     make_statistics()
+    make_logging()
 
 
 if __name__ == "__main__":

@@ -6,7 +6,10 @@ GPU fields without moving them to the host (svof_logging_quantities).
 The checker is the oracle's restatement of those loops (svo_logging).  It is
 pinned here against the reference program itself: oracle/_ref/svof_main_ref
 logs and saves at the same steps, and the restatement applied to each saved
-state reproduces the logged values.
+state reproduces the logged values.  The program's logs of a 32 x 32 case
+are also committed as a fixture (tests/golden/logging_32x32.npz), which the
+oracle reproduces from its own trajectory where the reference cannot be
+built.
 """
 import glob
 import os
@@ -72,6 +75,39 @@ def test_oracle_logging_reproduces_reference_logs(tmp_path):
         ref = dict(zip(Oracle.LOGGING_NAMES, np.concatenate([logs["momentum"][n, 1:], logs["energy"][n, 1:],
                                                               logs["nusselt"][n, 1:]])))
         # the logs print 16 significant digits
+        compare(got, ref, 1e-14, {k: 1e-300 for k in ref})
+
+
+def test_oracle_logging_reproduces_golden():
+    """the oracle runs the reference program's schedule (src/main.c:111-141,
+    src/logging/main.c:25-30 and 104) and reproduces its momentum.dat,
+    energy.dat and nusselt.dat, committed as a fixture by
+    tests/golden/make_golden.py, to the 16 digits they print"""
+    import importlib.util
+    import math
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(here, "golden", "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    golden = np.load(os.path.join(here, "golden", "logging_32x32.npz"))
+    env = mg.LOG_ENV
+    o = Oracle(mg.statistics_case(), physical_params(DROPLET2D_ENV), add_buoyancy=True, t_walls=T_WALLS)
+    timemax, rate = float(env["timemax"]), float(env["log_rate"])
+    time = 0.0
+    nxt = rate * math.ceil(max(sys.float_info.epsilon, time) / rate)
+    rows = []
+    while True:
+        time += o.run(1)[0]
+        if timemax < time:
+            break
+        if nxt < time:
+            rows.append(o.logging())
+            nxt += rate
+    assert len(rows) == golden["momentum"].shape[0] >= 5
+    for n, got in enumerate(rows):
+        ref = dict(zip(Oracle.LOGGING_NAMES, np.concatenate([golden["momentum"][n, 1:], golden["energy"][n, 1:],
+                                                              golden["nusselt"][n, 1:]])))
         compare(got, ref, 1e-14, {k: 1e-300 for k in ref})
 
 
