@@ -91,6 +91,13 @@ def _load():
                    "svo_correct", "svo_update_pressure"):
             getattr(L, fn).argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double]
         L.svo_integrate.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+        L.svo_integrate_fixed.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        L.svo_set_gravity.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
+        L.svo_tl_integrate_fixed.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
+        L.svo_tl_curvature_tensor.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.svo_tl_force.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double]
+        L.svo_tl_update_vof.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_double]
+        L.svo_tl_predict.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_double]
         L.svo_run.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
         L.svo_logging.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.svo_stat_collect.argtypes = [ctypes.c_void_p]
@@ -120,6 +127,8 @@ class Oracle:
                      float(t_walls[0]), float(t_walls[1]))
         xf = np.ascontiguousarray(ic.xf, dtype=np.float64)
         xc = np.ascontiguousarray(ic.xc, dtype=np.float64)
+        # kept for tangent contexts on the same grid (wall values zero)
+        self._grid = (pr, xf, xc)
         self._h = L.svo_create(ctypes.byref(pr), xf.ctypes.data, xc.ctypes.data)
         if not self._h:
             raise ValueError("svo_create failed")
@@ -176,6 +185,19 @@ class Oracle:
     def update_pressure(self, rk, dt):
         _load().svo_update_pressure(self._h, rk, dt)
 
+    def integrate_fixed(self, dt: float):
+        """one step with the given dt (no CFL decision)"""
+        _load().svo_integrate_fixed(self._h, float(dt))
+
+    def set_gravity(self, grav_vof: float, vof_ref: float):
+        """the vof buoyancy extension (absent from the reference): srcuy +=
+        grav_vof * (vof at the uy face - vof_ref)"""
+        _load().svo_set_gravity(self._h, float(grav_vof), float(vof_ref))
+
+    def tangent(self) -> "OracleTangent":
+        """a zero tangent of this context (tangent-linear model)"""
+        return OracleTangent(self)
+
     def run(self, nsteps: int) -> np.ndarray:
         dts = np.zeros(max(nsteps, 1))
         if _load().svo_run(self._h, int(nsteps), dts.ctypes.data) != 0:
@@ -211,6 +233,65 @@ class Oracle:
 
 
 # ---------------------------------------------------------------- 3D
+
+class OracleTangent:
+    """Tangents of an :class:`Oracle`'s fields (svof_oracle_tl.inc): a second
+    context on the same grid with zero wall values.  ``step`` advances the
+    primal and the tangent by one step of the tangent-linear model with the
+    time step held fixed."""
+
+    def __init__(self, primal: Oracle):
+        L = _load()
+        pr, xf, xc = primal._grid
+        z = _Params(pr.nx, pr.ny, pr.lx, pr.ly, pr.m_dif, pr.t_dif, pr.tension, pr.coef_dt_adv,
+                    pr.coef_dt_dif, pr.add_buoyancy, 0.0, 0.0, 0.0, 0.0)
+        self.primal = primal
+        self.nx, self.ny = primal.nx, primal.ny
+        self._h = L.svo_create(ctypes.byref(z), xf.ctypes.data, xc.ctypes.data)
+        if not self._h:
+            raise ValueError("svo_create failed")
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            _load().svo_destroy(self._h)
+            self._h = None
+
+    def field(self, name: str) -> np.ndarray:
+        n = ctypes.c_long(0)
+        ptr = _load().svo_field(self._h, name.encode(), ctypes.byref(n))
+        if not ptr:
+            raise KeyError(name)
+        return np.ctypeslib.as_array(ptr, shape=(n.value,)).reshape(storage_shape(name, self.nx, self.ny))
+
+    def init_boundaries(self):
+        _load().svo_init_boundaries(self._h)
+
+    def step(self, dt: float, dtension: float = 0.0):
+        _load().svo_tl_integrate_fixed(self.primal._h, self._h, float(dt), float(dtension))
+
+    # the linearised functions one by one (each before the primal function)
+    def curvature_tensor(self):
+        _load().svo_tl_curvature_tensor(self.primal._h, self._h)
+
+    def force(self, dtension: float = 0.0):
+        _load().svo_tl_force(self.primal._h, self._h, float(dtension))
+
+    def update_vof(self, rk, dt):
+        _load().svo_tl_update_vof(self.primal._h, self._h, int(rk), float(dt))
+
+    def predict(self, rk, dt):
+        _load().svo_tl_predict(self.primal._h, self._h, int(rk), float(dt))
+
+    def potential(self, rk, dt):
+        f = _load().svo_potential_dct if self.primal.uniform() else _load().svo_potential_dft
+        f(self._h, int(rk), float(dt))
+
+    def correct(self, rk, dt):
+        _load().svo_correct(self._h, int(rk), float(dt))
+
+    def update_pressure(self, rk, dt):
+        _load().svo_update_pressure(self._h, int(rk), float(dt))
+
 
 def storage_shape3d(name: str, nx: int, ny: int, nz: int):
     """storage shapes of the 3D restatement (z, y, x[, comps]), x fastest"""

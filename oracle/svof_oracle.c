@@ -63,6 +63,9 @@ struct svo_ctx {
    * t2 uxt, allocated on the first collection */
   double *stat[7];
   long stat_num;
+  /* buoyancy of the volume fraction on uy (an extension, not in the
+   * reference; off while grav_vof == 0): srcuy += grav_vof (vof_face - vof_ref) */
+  double grav_vof, vof_ref;
 };
 
 /* ---------- index maps (reference include/array_macros/) ---------- */
@@ -469,6 +472,8 @@ static double indicator(const double *n, const double x0, const double x1) {
   return 1. / (1. + exp(-2. * VOFBETA * (+n[0] * x0 + n[1] * x1 + n[2])));
 }
 
+static void vof_rhs_advect(svo_ctx_t *c, int rkstep, double dt);
+
 int svo_update_vof(svo_ctx_t *c, int rkstep, double dt) {
   /* reset_srcs, update/main.c:28-45 */
   if (0 != rkstep) {
@@ -513,6 +518,14 @@ int svo_update_vof(svo_ctx_t *c, int rkstep, double dt) {
       FLXY(i, j) = vel * flux;
     }
   }
+  vof_rhs_advect(c, rkstep, dt);
+  return 0;
+}
+
+/* interface_compute_rhs + interface_advect_vof + the boundary update
+ * (update/main.c:47-110, boundary.c:7-39): linear in the fluxes, src_b and
+ * vof, so the tangent-linear model runs it on its own context as well */
+static void vof_rhs_advect(svo_ctx_t *c, int rkstep, double dt) {
   /* interface_compute_rhs, update/main.c:47-78 */
   double *src = c->src[0];
   for (int j = 1; j <= NY; j++) {
@@ -540,7 +553,6 @@ int svo_update_vof(svo_ctx_t *c, int rkstep, double dt) {
     }
   }
   bc_vof(c);
-  return 0;
 }
 
 /* ---------------- Thomas solvers: src/tdm.c ---------------- */
@@ -734,6 +746,18 @@ static void rhs_uy(svo_ctx_t *c) {
   for (int j = 1; j <= NY; j++) {
     for (int i = 1; i <= NX; i++, cnt++) srca[cnt] += c->ifrcy[cnt];
   }
+  /* extension: Boussinesq buoyancy of the volume fraction along y, the
+   * face value of vof averaged from the two cells beside the uy face; absent
+   * from the reference, whose only body force is the temperature buoyancy
+   * along x (ux.c:181-197) */
+  if (0. != c->grav_vof) {
+    cnt = 0;
+    for (int j = 1; j <= NY; j++) {
+      for (int i = 1; i <= NX; i++, cnt++) {
+        srca[cnt] += c->grav_vof * (0.5 * VOF(i, j - 1) + 0.5 * VOF(i, j) - c->vof_ref);
+      }
+    }
+  }
 }
 
 static void rhs_t(svo_ctx_t *c) {
@@ -788,6 +812,8 @@ static void increments(svo_ctx_t *c, double *const *s, const long nitems, const 
   }
 }
 
+static void predict_tail(svo_ctx_t *c, int rkstep, double dt);
+
 int svo_predict(svo_ctx_t *c, int rkstep, double dt) {
   /* fluid_predict_field, src/fluid/predict/main.c:62-79 */
   reset_srcs3(c, c->srcux, c->n_srcux, rkstep);
@@ -796,6 +822,14 @@ int svo_predict(svo_ctx_t *c, int rkstep, double dt) {
   rhs_ux(c);
   rhs_uy(c);
   rhs_t(c);
+  predict_tail(c, rkstep, dt);
+  return 0;
+}
+
+/* increments, x-implicit solves, updates and boundary updates of
+ * predict_{ux,uy,t}: linear in the sources and fields, so the tangent-linear
+ * model runs it on its own context as well */
+static void predict_tail(svo_ctx_t *c, int rkstep, double dt) {
   /* predict_ux, ux.c:306-388 */
   {
     increments(c, c->srcux, c->n_srcux, rkstep, dt);
@@ -829,7 +863,6 @@ int svo_predict(svo_ctx_t *c, int rkstep, double dt) {
     }
     bc_t(c);
   }
-  return 0;
 }
 
 /* ---------------- Poisson: src/fluid/compute_potential/{dct,dft}.c ---------------- */
@@ -992,6 +1025,31 @@ int svo_integrate(svo_ctx_t *c, double *dt) {
     svo_correct(c, rkstep, *dt);
     svo_update_pressure(c, rkstep, *dt);
   }
+  return 0;
+}
+
+/* one step with a given dt (the time-step sequence of a differentiated run
+ * is held fixed) */
+int svo_integrate_fixed(svo_ctx_t *c, double dt) {
+  for (int rkstep = 0; rkstep < 3; rkstep++) {
+    svo_curvature_tensor(c);
+    svo_force(c);
+    svo_update_vof(c, rkstep, dt);
+    svo_predict(c, rkstep, dt);
+    if (c->uniform) {
+      svo_potential_dct(c, rkstep, dt);
+    } else {
+      svo_potential_dft(c, rkstep, dt);
+    }
+    svo_correct(c, rkstep, dt);
+    svo_update_pressure(c, rkstep, dt);
+  }
+  return 0;
+}
+
+int svo_set_gravity(svo_ctx_t *c, double grav_vof, double vof_ref) {
+  c->grav_vof = grav_vof;
+  c->vof_ref = vof_ref;
   return 0;
 }
 
@@ -1193,3 +1251,5 @@ int svo_stat_reduce(const svo_ctx_t *c, int q, double *out) {
 }
 
 long svo_stat_num(const svo_ctx_t *c) { return c->stat_num; }
+
+#include "svof_oracle_tl.inc"

@@ -61,6 +61,29 @@ int svo_correct(svo_ctx_t *ctx, int rkstep, double dt);
 int svo_update_pressure(svo_ctx_t *ctx, int rkstep, double dt);
 int svo_integrate(svo_ctx_t *ctx, double *dt);
 int svo_run(svo_ctx_t *ctx, int nsteps, double *dts);
+/* one step with a given dt (no CFL decision) */
+int svo_integrate_fixed(svo_ctx_t *ctx, double dt);
+/* extension absent from the reference: buoyancy of the volume fraction on uy,
+ * srcuy_a += grav_vof * (vof at the uy face - vof_ref); grav_vof = g_y (1 -
+ * density ratio) in the Boussinesq form, vof_ref the domain-mean volume
+ * fraction (zero net force).  Off (the reference's physics) while grav_vof is 0. */
+int svo_set_gravity(svo_ctx_t *ctx, double grav_vof, double vof_ref);
+
+/* Tangent-linear model of one step (linearisation of every function above
+ * about the current state of `c`).  `d` is a second context on the same grid
+ * and parameters, with zero wall values, whose arrays hold the tangents
+ * (directional derivatives) of c's fields; `dtension` is the tangent of the
+ * surface tension coefficient 1/We.  The time step is held fixed.  Advances
+ * both contexts by one step. */
+int svo_tl_integrate_fixed(svo_ctx_t *c, svo_ctx_t *d, double dt, double dtension);
+/* the linearised functions one by one: each reads the primal state of c at
+ * the function's input, so it runs before the primal function of the same
+ * name; the linear functions (potential, correct, update_pressure) are the
+ * primal functions applied to d */
+int svo_tl_curvature_tensor(svo_ctx_t *c, svo_ctx_t *d);
+int svo_tl_force(svo_ctx_t *c, svo_ctx_t *d, double dtension);
+int svo_tl_update_vof(svo_ctx_t *c, svo_ctx_t *d, int rkstep, double dt);
+int svo_tl_predict(svo_ctx_t *c, svo_ctx_t *d, int rkstep, double dt);
 /* logging reductions of the current fields (src/logging/momentum.c,
  * energy.c, nusselt/ sources): out = {momentum x, y; energy ux, uy, t; Nusselt from
  * the wall heat flux, kinetic energy injection, kinetic and thermal energy

@@ -33,7 +33,10 @@ def test_reference_arm_line():
     assert r.returncode == 0, r.stderr[-2000:]
     (line,) = _json_lines(r.stdout)
     assert line["impl"] == "reference"
-    assert line["metric"] == "Mcell-steps/s" and line["unit"] == "Mcell-steps/s"
+    # the same metric string as our arm's line on this workload (bench.METRIC3D)
+    import bench
+    assert line["metric"] == bench.METRIC3D and line["unit"] == "Mcell-steps/s"
+    assert line["config"]["same_config"] is False and "restatement" in line["config"]["implementation"]
     assert line["value"] > 0 and line["higher_is_better"] is True
     assert line["steps"] == 1 and line["warmup"] >= 3  # at least three warm-up steps, whatever is asked
     assert line["config"]["workload"] == "droplets3d_512"
