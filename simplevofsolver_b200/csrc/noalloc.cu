@@ -12,16 +12,23 @@
 // Every GPU that loads this library holds that array (about 2.2 MB) until the
 // process exits.
 //
-// Limits: nx and ny powers of two, nx * ny <= 65536,
-// nx, ny <= 1024.  The array is shared by all calls and keeps the last call's
-// contents (the tables are reused while the grid is unchanged; the spectrum is
-// overwritten by every call), so calls that overlap on the GPU race.
+// Limits: nx a power of two, nx * ny <= 65536, 4 <= nx, ny <= 1024.  The
+// array is shared by all calls and keeps the last call's contents (the tables
+// are reused while the grid is unchanged; dt and the spectrum are overwritten
+// by every call), so calls that overlap on the GPU race.  The host part of a
+// call (grid metrics, tables, their upload) holds a process-wide lock, so
+// host threads may call concurrently; their GPU work must still not overlap.
+// A call on a grid other than the previous call's on that device builds and
+// uploads new tables and waits for the stream; any other call only enqueues
+// work (dt is written into the array by a one-thread kernel in stream order).
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 
 #include "../../include/svof_b200.h"
+#include "smem_limit.cuh"
 #include "svof_internal.cuh"
 
 using namespace svof;
@@ -58,11 +65,16 @@ struct DeviceState {
 };
 DeviceState g_dev[kMaxDevices];
 
+// guards g_dev and the host staging below (the host part of every call)
+std::mutex g_mu;
+
 // host staging of the tables (static: no allocation on the call path)
 double h_vt[kMaxCells], h_rvt[kMaxCells], h_q1t[kMaxCells];
 double h_ck[kMaxN], h_den[kMaxN], h_lastf[kMaxN], h_dxf[kMaxN], h_twf[kMaxN], h_twb[kMaxN], h_cs[2 * kMaxN];
 double h_l[kMaxN], h_c[kMaxN], h_u[kMaxN], h_v[kMaxN], h_q1[kMaxN];
-double h_dt;
+
+// dt of this call, written in stream order (no host staging, no wait)
+__global__ void k_noalloc_set_dt(double *dst, double dt) { *dst = dt; }
 
 // failures are reported on stderr (the reference's convention) and by the
 // non-zero return value
@@ -157,6 +169,7 @@ extern "C" int svof_poisson_dct_noalloc(const svof_params_t *prm, const double *
   const int log2n = ilog2_exact(nx);
   if (log2n < 1) return nfail("nx must be a power of two");
   if (rkstep > 2) return nfail("rkstep out of range");
+  std::lock_guard<std::mutex> lock(g_mu);
   // grid metrics as src/domain.c:107-121 and the uniformity test :75-98
   double mn = 1.7976931348623157e308, mx = -1.7976931348623157e308;
   for (int i = 1; i <= nx; i++) {
@@ -185,6 +198,7 @@ extern "C" int svof_poisson_dct_noalloc(const svof_params_t *prm, const double *
   // tables: rebuilt and uploaded only when the grid changes
   const uint64_t hsh = fnv1a(h_dxf, sizeof(double) * nx);
   if (st.nx != nx || st.ny != ny || st.lx != prm->lx || st.ly != prm->ly || st.dxf_hash != hsh) {
+    st.nx = 0;  // the array holds no valid tables until the upload has completed
     build_tables(nx, ny, prm->lx, dy);
     const size_t nn = (size_t)nx * ny;
     struct { size_t off; const double *src; size_t n; } up[] = {
@@ -203,11 +217,7 @@ extern "C" int svof_poisson_dct_noalloc(const svof_params_t *prm, const double *
     st.ly = prm->ly;
     st.dxf_hash = hsh;
   }
-  h_dt = dt;
-  e = cudaMemcpyAsync(S + kDt, &h_dt, sizeof(double), cudaMemcpyHostToDevice, s);
-  if (cudaSuccess != e) return nfail("dt upload", e);
-  e = cudaStreamSynchronize(s);
-  if (cudaSuccess != e) return nfail("dt upload", e);
+  k_noalloc_set_dt<<<1, 1, 0, s>>>(S + kDt, dt);
   // the three kernels of the DCT path, on the scratch array
   const double gam = (rkstep == 0 ? 32. / 60. + 0. / 60.
                                   : rkstep == 1 ? 25. / 60. + -17. / 60. : 45. / 60. + -25. / 60.);
@@ -218,6 +228,10 @@ extern "C" int svof_poisson_dct_noalloc(const svof_params_t *prm, const double *
   int kt = 32;
   while (kt > 4 && nx / kt < 148) kt >>= 1;
   while (kt > 1 && sizeof(double) * 3 * (size_t)ny * kt > 48 * 1024) kt >>= 1;
+  // the default 48 KB limit counts the kernel's static shared memory as well:
+  // raise the dynamic limit for every size, as the allocating solver does
+  e = raise_smem_limit(k_dct_ysolve, sizeof(double) * 3 * kt * ny);
+  if (cudaSuccess != e) return nfail("shared-memory limit of the y solve", e);
   k_dct_ysolve<<<(nx + kt - 1) / kt, 128, sizeof(double) * 3 * kt * ny, s>>>(
       S + kSpec, S + kVt, S + kRvt, S + kQ1t, S + kCk, S + kLastf, S + kDen, 1. / dy / dy, nx, ny, kt);
   k_dct_inv<<<ny, nthr, sizeof(double) * 2 * nx, s>>>(S + kSpec, psi, S + kTwb, S + kCs, log2n, g);
