@@ -311,6 +311,78 @@ def _timed_steps(solver, steps, world, local_rank, flush=None):
     return total_ms, clk.summary()
 
 
+def adjoint_cost(steps: int = 200, K: int = 20):
+    """Cost of the differentiation form on its workload (falling droplet,
+    256 x 256, vof buoyancy Fr = 1, density ratio 0.1, Re = 200, We = 20):
+    device time per step of the forward (svof_integrate_fixed, the time
+    steps held fixed) and of the backward pass (the segment recompute with
+    tapes plus the step adjoints, svof_adjoint_step), CUDA events on the
+    solver's stream.  adjoint_over_forward = backward / forward per step; the
+    forward's checkpoint copies are not counted on either side."""
+    import torch
+    from simplevofsolver_b200 import Solver
+    from simplevofsolver_b200.adjoint import Rollout
+    from simplevofsolver_b200.workloads import (FALLING2D_ENV, falling_droplet2d, falling_gravity,
+                                                physical_params)
+    n = 256
+    ic = falling_droplet2d(n)
+    phys = physical_params(FALLING2D_ENV)
+    s = Solver(ic, phys)
+    s.set_gravity(*falling_gravity(ic))
+    dts = s.run(steps)
+    r = Rollout(s, dts, K)
+    dev = dict(dtype=torch.float64, device="cuda")
+    x = (torch.tensor(ic.ux[:, 1:n], **dev), torch.tensor(ic.uy[:, 1:n + 1], **dev),
+         torch.tensor(ic.vof[:, 1:n + 1], **dev), phys["tension"])
+    stream = torch.cuda.ExternalStream(s.stream())
+    tapes = [torch.empty(s.tape_count(), **dev) for _ in range(K)]
+
+    def fwd():
+        r.load(*x)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            for dt in dts:
+                s.integrate_fixed(dt)
+            e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    def bwd():
+        # checkpoints of the forward (not timed), then the timed backward
+        r.forward(*x)
+        s.adjoint_reset()
+        s.synchronize()
+        ms = 0.0
+        for seg in reversed(range(len(r.checkpoints))):
+            n0, n1 = seg * K, min(steps, seg * K + K)
+            r._restore_state(r.checkpoints[seg])
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                e0.record(stream)
+                for k in range(n0, n1):
+                    s.integrate_fixed(dts[k], tapes[k - n0].data_ptr())
+                for k in reversed(range(n0, n1)):
+                    s.adjoint_step(tapes[k - n0].data_ptr(), dts[k])
+                e1.record(stream)
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+        return ms
+
+    fwd()
+    bwd()
+    f_ms = min(fwd() for _ in range(3))
+    b_ms = min(bwd() for _ in range(3))
+    s.close()
+    return {"workload": f"falling_droplet2d_{n} (vof buoyancy Fr=1, density ratio 0.1, Re=200, We=20)",
+            "steps": steps, "checkpoint_every": K, "dtype": "f64",
+            "forward_ms_per_step": f_ms / steps, "backward_ms_per_step": b_ms / steps,
+            "adjoint_over_forward": b_ms / f_ms,
+            "backward": "segment recompute with tapes + step adjoints (svof_adjoint_step)",
+            "forward": "svof_integrate_fixed (time steps held fixed)"}
+
+
 def _profile(solver, nprof):
     """per-kernel-kind device time of `nprof` steps launched kernel by kernel;
     a long memset ahead lets the host enqueue the whole step first"""
@@ -502,6 +574,12 @@ def run3d(args, wl, ic, env, world, rank, local_rank):
             "cpu_baseline": cpu,
             "clocks": m["clocks"],
         }
+        if world == 1 and not args.no_adjoint:
+            try:
+                line["adjoint"] = adjoint_cost()
+                line["adjoint_over_forward"] = line["adjoint"]["adjoint_over_forward"]
+            except Exception as e:  # reported, never silently dropped
+                line["adjoint"] = {"error": str(e)}
         print(json.dumps(line))
 
 
@@ -513,6 +591,7 @@ def main():
     ap.add_argument("--workload", default="droplets3d_512", choices=sorted(WORKLOADS) + sorted(WORKLOADS3D))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample-steps", type=int, default=None)
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiation form's cost")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     three_d = args.workload in WORKLOADS3D

@@ -235,10 +235,94 @@ int svof_profile_step(svof_solver_t *solver, double *ms, int *launches, int nkin
  * 4 <= nx, ny <= 1024, nx * ny <= 65536; larger grids are refused with a
  * non-zero return and a message on stderr.  The first call on a device looks
  * up that device's address of the array (cudaGetSymbolAddress) and should
- * come before any stream capture.  All calls share the array, which keeps the
- * last call's tables and spectrum: calls that overlap on the GPU race. */
+ * come before any stream capture.  A call whose grid differs from the previous
+ * call's on that device builds the line-solve tables on the host, uploads them
+ * and waits for `stream`; other calls only enqueue work.  All calls share the
+ * array, which keeps the last call's tables, dt and spectrum: calls that
+ * overlap on the GPU race.  The host part of a call holds a process-wide lock,
+ * so host threads may call at the same time, but their GPU work must not
+ * overlap. */
 int svof_poisson_dct_noalloc(const svof_params_t *params, const double *xf, const double *ux,
                              const double *uy, double *psi, size_t rkstep, double dt, void *stream);
+
+/* ---------------------------------------------------------------------
+ * Differentiation form (FP64).  No counterpart in the reference: the adjoint
+ * of one time step, for gradients of an objective of the final state with
+ * respect to the initial velocities and vof and the surface-tension
+ * coefficient 1/We.  The time-step sequence of a differentiated run is held
+ * fixed (svof_integrate_fixed); branches of the method (upwind side of a face,
+ * interfacial-cell test, clamps of vanishing gradients) follow the primal
+ * state.  Requires add_buoyancy = 0: the temperature is not differentiated.
+ * -------------------------------------------------------------------- */
+
+/* Extension absent from the reference (whose only body force is the
+ * temperature buoyancy along x): Boussinesq buoyancy of the volume fraction
+ * on uy, srcuy_a += grav_vof * (vof at the uy face - vof_ref), with vof after
+ * the substep's advection.  grav_vof = g_y (1 - density ratio) with g_y =
+ * -1/Fr^2 for gravity along -y; vof_ref = the domain-mean volume fraction
+ * (zero net force in the periodic direction).  0 (the default) is the
+ * reference's physics, bit for bit. */
+int svof_set_gravity(svof_solver_t *solver, double grav_vof, double vof_ref);
+
+/* replaces the run-time parameters (same grid), for example the surface
+ * tension 1/We of a differentiated run; waits for the solver's stream */
+int svof_set_params(svof_solver_t *solver, const svof_params_t *params);
+
+/* doubles of one step's tape: the inputs ux, uy, vof (storage layouts) of the
+ * three Runge-Kutta substeps */
+int svof_tape_count(const svof_solver_t *solver, size_t *count);
+/* one time step with the given dt (no CFL decision), enqueued on the solver's
+ * stream (svof_synchronize waits for it); when tape (device memory,
+ * svof_tape_count doubles) is not NULL it records the step's substep inputs.
+ * Replaces integrate() (include/integrate.h:5-10) in a differentiated run. */
+int svof_integrate_fixed(svof_solver_t *solver, double dt, double *tape);
+
+/* adjoint fields, device memory owned by the solver (made on first use),
+ * compact layouts: SVOF_ADJ_UX and SVOF_ADJ_IFRCX ny rows x (nx-1) (faces
+ * i = 2..nx), SVOF_ADJ_NORMAL ny x nx x 3, the others ny x nx.  The adjoint of
+ * a step's output is written into UX, UY, P, VOF; svof_adjoint_step turns it
+ * into the adjoint of the step's input in place.  TENSION holds per-cell
+ * contributions to the adjoint of 1/We (svof_adjoint_tension sums them).  The
+ * pointer of SVOF_ADJ_VOF and SVOF_ADJ_SRC_A changes after each interface
+ * adjoint (they alternate between two buffers): ask again. */
+enum {
+  SVOF_ADJ_UX = 0,
+  SVOF_ADJ_UY = 1,
+  SVOF_ADJ_P = 2,
+  SVOF_ADJ_VOF = 3,
+  SVOF_ADJ_PSI = 4,
+  SVOF_ADJ_IFRCX = 5,
+  SVOF_ADJ_IFRCY = 6,
+  SVOF_ADJ_CURV = 7,
+  SVOF_ADJ_NORMAL = 8,     /* (nx, ny, intercept) of the cell normal */
+  SVOF_ADJ_SRCUX_A = 9,    /* pending adjoints of the substep's src_a (from the next substep's beta term) */
+  SVOF_ADJ_SRCUY_A = 10,
+  SVOF_ADJ_SRC_A = 11,
+  SVOF_ADJ_TENSION = 12
+};
+int svof_adjoint_field(svof_solver_t *solver, int which, double **dptr, size_t *count);
+/* zero every adjoint field (enqueued) */
+int svof_adjoint_reset(svof_solver_t *solver);
+/* the adjoint of one svof_integrate_fixed(dt, tape) step, enqueued: (UX, UY,
+ * P, VOF) of the step's output -> of its input, TENSION += its contribution.
+ * Per substep in reverse: the projection and pressure update, the Poisson
+ * solve (its adjoint is a second Poisson solve of psi_bar / dxf: the x grid's
+ * metric weights), the implicit-x line solves, the momentum right-hand sides,
+ * the THINC/QQ fluxes and vof update, the CSF force, the intercepts (implicit
+ * function theorem), the normals and the curvature. */
+int svof_adjoint_step(svof_solver_t *solver, const double *tape, double dt);
+/* the same pieces one by one, each the adjoint of the reference function of
+ * the same name about the primal state in the solver's current fields (that
+ * function's input), in place on the adjoint fields; each waits for its work */
+int svof_adjoint_fluid_update_pressure(svof_solver_t *solver, size_t rkstep, double dt);
+int svof_adjoint_fluid_correct_velocity(svof_solver_t *solver, size_t rkstep, double dt);
+int svof_adjoint_fluid_compute_potential(svof_solver_t *solver, size_t rkstep, double dt);
+int svof_adjoint_fluid_predict_field(svof_solver_t *solver, size_t rkstep, double dt);
+int svof_adjoint_interface_update_vof(svof_solver_t *solver, size_t rkstep, double dt);
+int svof_adjoint_interface_compute_force(svof_solver_t *solver);
+int svof_adjoint_interface_compute_curvature_tensor(svof_solver_t *solver);
+/* the accumulated adjoint of 1/We (waits) */
+int svof_adjoint_tension(svof_solver_t *solver, double *out);
 
 /* wait for all work of the solver's stream */
 int svof_synchronize(svof_solver_t *solver);

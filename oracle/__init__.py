@@ -283,7 +283,7 @@ class OracleTangent:
         _load().svo_tl_predict(self.primal._h, self._h, int(rk), float(dt))
 
     def potential(self, rk, dt):
-        f = _load().svo_potential_dct if self.primal.uniform() else _load().svo_potential_dft
+        f = _load().svo_potential_dct if self.primal.uniform else _load().svo_potential_dft
         f(self._h, int(rk), float(dt))
 
     def correct(self, rk, dt):

@@ -57,7 +57,34 @@ EXPORTS = ["svof_create", "svof_destroy", "svof_field_count", "svof_upload_field
            "svof_enqueue_steps", "svof_last_dt",
            "svof_diagnostics", "svof_profile_step", "svof_synchronize", "svof_stream", "svof_last_error",
            "svof_logging_quantities", "svof_statistics_collect", "svof_statistics_reset",
-           "svof_statistics_count", "svof_statistics_reduce", "svof_statistics_field"]
+           "svof_statistics_count", "svof_statistics_reduce", "svof_statistics_field",
+           "svof_set_gravity", "svof_set_params", "svof_tape_count", "svof_integrate_fixed",
+           "svof_adjoint_field", "svof_adjoint_reset", "svof_adjoint_step", "svof_adjoint_fluid_update_pressure",
+           "svof_adjoint_fluid_correct_velocity", "svof_adjoint_fluid_compute_potential",
+           "svof_adjoint_fluid_predict_field", "svof_adjoint_interface_update_vof",
+           "svof_adjoint_interface_compute_force", "svof_adjoint_interface_compute_curvature_tensor",
+           "svof_adjoint_tension", "svof_poisson_dct_noalloc"]
+
+# adjoint fields (SVOF_ADJ_*); compact layouts: ux faces (ny, nx-1), cells (ny, nx)
+ADJ_FIELDS = {"ux": 0, "uy": 1, "p": 2, "vof": 3, "psi": 4, "ifrcx": 5, "ifrcy": 6, "curv": 7, "normal": 8,
+              "srcux_a": 9, "srcuy_a": 10, "src_a": 11, "tension": 12}
+
+
+def adjoint_shape(name: str, nx: int, ny: int):
+    if name in ("ux", "ifrcx", "srcux_a"):
+        return (ny, nx - 1)
+    if name == "normal":
+        return (ny, nx, 3)
+    return (ny, nx)
+
+
+class _DeviceArray:
+    """__cuda_array_interface__ of a float64 device buffer (a zero-copy view
+    for torch.as_tensor)"""
+
+    def __init__(self, ptr: int, shape):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": "<f8", "data": (int(ptr), False),
+                                         "version": 3, "strides": None}
 
 # statistics quantities (SVOF_STAT_*), in the reference's order (src/statistics.c:41-47)
 STAT_NAMES = ["ux1", "ux2", "uy1", "uy2", "t1", "t2", "uxt"]
@@ -128,6 +155,21 @@ def lib() -> ctypes.CDLL:
         L.svof_profile_step.argtypes = [vp, dp, dp, i]
         L.svof_stream.argtypes = [vp, ctypes.POINTER(vp)]
         L.svof_last_error.restype = ctypes.c_char_p
+        # differentiation form
+        L.svof_set_gravity.argtypes = [vp, d, d]
+        L.svof_set_params.argtypes = [vp, ctypes.POINTER(Params)]
+        L.svof_tape_count.argtypes = [vp, ctypes.POINTER(sz)]
+        L.svof_integrate_fixed.argtypes = [vp, d, vp]
+        L.svof_adjoint_field.argtypes = [vp, i, ctypes.POINTER(vp), ctypes.POINTER(sz)]
+        L.svof_adjoint_reset.argtypes = [vp]
+        L.svof_adjoint_step.argtypes = [vp, vp, d]
+        for fn in ("svof_adjoint_fluid_update_pressure", "svof_adjoint_fluid_correct_velocity",
+                   "svof_adjoint_fluid_compute_potential", "svof_adjoint_fluid_predict_field",
+                   "svof_adjoint_interface_update_vof"):
+            getattr(L, fn).argtypes = [vp, sz, d]
+        L.svof_adjoint_interface_compute_force.argtypes = [vp]
+        L.svof_adjoint_interface_compute_curvature_tensor.argtypes = [vp]
+        L.svof_adjoint_tension.argtypes = [vp, pd]
         _lib = L
     return _lib
 
@@ -381,6 +423,73 @@ class Solver:
 
     def synchronize(self):
         _check(lib().svof_synchronize(self._h))
+
+    # ------------------------------------------------------------ differentiation form
+    def device_view(self, name: str):
+        """zero-copy torch view of a field's current device storage (valid
+        until the next call that swaps its buffers; synchronise the solver's
+        stream and torch's around its use)"""
+        import torch
+        return torch.as_tensor(_DeviceArray(self.device_ptr(name), storage_shape(name, self.nx, self.ny)),
+                               device="cuda")
+
+    def adjoint_view(self, name: str):
+        """zero-copy torch view of an adjoint field (compact layout)"""
+        import torch
+        p = ctypes.c_void_p()
+        n = ctypes.c_size_t(0)
+        _check(lib().svof_adjoint_field(self._h, ADJ_FIELDS[name], ctypes.byref(p), ctypes.byref(n)))
+        return torch.as_tensor(_DeviceArray(p.value, adjoint_shape(name, self.nx, self.ny)), device="cuda")
+
+    def set_gravity(self, grav_vof: float, vof_ref: float):
+        """the vof buoyancy extension on uy (absent from the reference; 0 = off)"""
+        _check(lib().svof_set_gravity(self._h, float(grav_vof), float(vof_ref)))
+
+    def set_tension(self, tension: float):
+        self.params.tension = float(tension)
+        _check(lib().svof_set_params(self._h, ctypes.byref(self.params)))
+
+    def tape_count(self) -> int:
+        n = ctypes.c_size_t(0)
+        _check(lib().svof_tape_count(self._h, ctypes.byref(n)))
+        return int(n.value)
+
+    def integrate_fixed(self, dt: float, tape_ptr: int = 0):
+        """one step with the given dt, enqueued; records the substep inputs at
+        tape_ptr (device memory, tape_count() doubles) when non-zero"""
+        _check(lib().svof_integrate_fixed(self._h, float(dt), ctypes.c_void_p(tape_ptr or None)))
+
+    def adjoint_reset(self):
+        _check(lib().svof_adjoint_reset(self._h))
+
+    def adjoint_step(self, tape_ptr: int, dt: float):
+        _check(lib().svof_adjoint_step(self._h, ctypes.c_void_p(tape_ptr), float(dt)))
+
+    def adjoint_tension(self) -> float:
+        out = ctypes.c_double(0.0)
+        _check(lib().svof_adjoint_tension(self._h, ctypes.byref(out)))
+        return out.value
+
+    def adjoint_fluid_update_pressure(self, rk: int, dt: float):
+        _check(lib().svof_adjoint_fluid_update_pressure(self._h, rk, dt))
+
+    def adjoint_fluid_correct_velocity(self, rk: int, dt: float):
+        _check(lib().svof_adjoint_fluid_correct_velocity(self._h, rk, dt))
+
+    def adjoint_fluid_compute_potential(self, rk: int, dt: float):
+        _check(lib().svof_adjoint_fluid_compute_potential(self._h, rk, dt))
+
+    def adjoint_fluid_predict_field(self, rk: int, dt: float):
+        _check(lib().svof_adjoint_fluid_predict_field(self._h, rk, dt))
+
+    def adjoint_interface_update_vof(self, rk: int, dt: float):
+        _check(lib().svof_adjoint_interface_update_vof(self._h, rk, dt))
+
+    def adjoint_interface_compute_force(self):
+        _check(lib().svof_adjoint_interface_compute_force(self._h))
+
+    def adjoint_interface_compute_curvature_tensor(self):
+        _check(lib().svof_adjoint_interface_compute_curvature_tensor(self._h))
 
 
 # the 3D path (include/svof3d_b200.h)

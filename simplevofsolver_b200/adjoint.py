@@ -1,0 +1,196 @@
+"""Differentiation form of the 2D FP64 path: gradients through a rollout.
+
+``Rollout`` runs ``len(dts)`` time steps of the CUDA solver with the time-step
+sequence held fixed (``svof_integrate_fixed``) and is differentiable with
+respect to the initial velocities, the initial volume fraction and the
+surface-tension coefficient 1/We through :class:`RolloutFunction`, a
+``torch.autograd.Function`` whose backward pass runs the hand-written CUDA
+adjoint of each step (``svof_adjoint_step``, ``csrc/k_adjoint.cu``).
+
+Memory is bounded by recompute-from-checkpoint: the forward pass keeps the
+full state every ``K`` steps only; the backward pass walks the segments in
+reverse, re-runs each segment forward from its checkpoint while recording the
+substep inputs of its K steps on a tape (K tapes of ``tape_count()`` doubles),
+and applies the K step adjoints in reverse.  Device memory: N / K
+checkpoints + K tapes.
+
+Tensors live on the GPU in compact layouts: ux on the interior faces
+(ny, nx-1), uy, vof and p on the cells (ny, nx).  The temperature is not
+differentiated (buoyancy of t must be off); the vof buoyancy extension
+(``Solver.set_gravity``) is.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import Solver, SvofError
+
+
+def _to_interior(name, a, nx, ny):
+    """compact (device tensor) -> restart-file layout (numpy)"""
+    a = a.detach().to("cpu").double().numpy()
+    out = np.zeros((ny, nx + 1) if name == "ux" else (ny, nx + 2))
+    if name == "ux":
+        out[:, 1:nx] = a
+    else:
+        out[:, 1:nx + 1] = a
+    return out
+
+
+class Rollout:
+    """``nsteps = len(dts)`` steps of one solver from a given initial state.
+
+    ``solver`` is a :class:`Solver` (its p and t at construction are the
+    initial p and t of every rollout); ``dts`` the fixed time steps;
+    ``checkpoint_every`` = K."""
+
+    STATE = ("ux", "uy", "p", "t", "vof")
+
+    def __init__(self, solver: Solver, dts, checkpoint_every: int = 20):
+        import torch
+        if checkpoint_every < 1:
+            raise ValueError("checkpoint_every must be at least 1")
+        self.s = solver
+        self.dts = [float(x) for x in dts]
+        self.K = int(checkpoint_every)
+        self.nx, self.ny = solver.nx, solver.ny
+        self.p0 = solver.interior("p")
+        self.t0 = solver.interior("t")
+        self.tapes = None
+        self.checkpoints = []
+        self._torch = torch
+
+    # -- state transfer (the solver's stream and torch's are synchronised around each)
+    def _sync(self):
+        self.s.synchronize()
+        self._torch.cuda.synchronize()
+
+    def load(self, ux0, uy0, vof0, tension):
+        s = self.s
+        s.set_tension(float(tension))
+        s.load_interior("ux", _to_interior("ux", ux0, self.nx, self.ny))
+        s.load_interior("uy", _to_interior("uy", uy0, self.nx, self.ny))
+        s.load_interior("vof", _to_interior("vof", vof0, self.nx, self.ny))
+        s.load_interior("p", self.p0)
+        s.load_interior("t", self.t0)
+
+    def _save_state(self):
+        self._sync()
+        return {k: self.s.device_view(k).clone() for k in self.STATE}
+
+    def _restore_state(self, st):
+        self._sync()
+        for k in self.STATE:
+            self.s.device_view(k).copy_(st[k])
+        self._torch.cuda.synchronize()
+
+    def outputs(self):
+        self._sync()
+        nx, ny = self.nx, self.ny
+        ux = self.s.device_view("ux")[1:ny + 1, 1:nx].clone()
+        uy = self.s.device_view("uy")[1:ny + 1, 1:nx + 1].clone()
+        p = self.s.device_view("p")[1:ny + 1, 1:nx + 1].clone()
+        vof = self.s.device_view("vof")[2:ny + 2, 1:nx + 1].clone()
+        return ux, uy, vof, p
+
+    # -- forward: no tapes, checkpoints every K steps
+    def forward(self, ux0, uy0, vof0, tension, keep_checkpoints=True):
+        self.load(ux0, uy0, vof0, tension)
+        self.checkpoints = []
+        for n, dt in enumerate(self.dts):
+            if keep_checkpoints and n % self.K == 0:
+                self.checkpoints.append(self._save_state())
+            self.s.integrate_fixed(dt)
+        return self.outputs()
+
+    # -- backward: recompute each segment with tapes, then its step adjoints in reverse
+    def backward(self, gux, guy, gvof, gp):
+        torch = self._torch
+        s = self.s
+        nx, ny = self.nx, self.ny
+        if self.tapes is None:
+            self.tapes = [torch.empty(s.tape_count(), dtype=torch.float64, device="cuda") for _ in range(self.K)]
+        s.adjoint_reset()
+        self._sync()
+        zeros = torch.zeros
+        seeds = {"ux": gux if gux is not None else zeros((ny, nx - 1), dtype=torch.float64, device="cuda"),
+                 "uy": guy if guy is not None else zeros((ny, nx), dtype=torch.float64, device="cuda"),
+                 "vof": gvof if gvof is not None else zeros((ny, nx), dtype=torch.float64, device="cuda"),
+                 "p": gp if gp is not None else zeros((ny, nx), dtype=torch.float64, device="cuda")}
+        # the pressure's additive constant is fixed by round-off: only its
+        # zero-mean part has a meaningful adjoint
+        seeds["p"] = seeds["p"] - seeds["p"].mean()
+        for k, v in seeds.items():
+            s.adjoint_view(k).copy_(v.double())
+        torch.cuda.synchronize()
+        N = len(self.dts)
+        for seg in reversed(range(len(self.checkpoints))):
+            n0 = seg * self.K
+            n1 = min(N, n0 + self.K)
+            self._restore_state(self.checkpoints[seg])
+            for n in range(n0, n1):
+                s.integrate_fixed(self.dts[n], self.tapes[n - n0].data_ptr())
+            for n in reversed(range(n0, n1)):
+                s.adjoint_step(self.tapes[n - n0].data_ptr(), self.dts[n])
+        self._sync()
+        g_ux = s.adjoint_view("ux").clone()
+        g_uy = s.adjoint_view("uy").clone()
+        g_vof = s.adjoint_view("vof").clone()
+        g_ten = s.adjoint_tension()
+        return g_ux, g_uy, g_vof, g_ten
+
+
+def _function():
+    import torch
+
+    class RolloutFunction(torch.autograd.Function):
+        """(ux0, uy0, vof0, tension) -> (ux, uy, vof, p) after the rollout's
+        steps; backward through the CUDA step adjoints with recompute from
+        checkpoints."""
+
+        @staticmethod
+        def forward(ctx, ux0, uy0, vof0, tension, rollout):
+            ctx.rollout = rollout
+            ctx.tension_like = tension
+            return rollout.forward(ux0, uy0, vof0, float(tension))
+
+        @staticmethod
+        def backward(ctx, gux, guy, gvof, gp):
+            r = ctx.rollout
+            g_ux, g_uy, g_vof, g_ten = r.backward(gux, guy, gvof, gp)
+            gt = torch.tensor(g_ten, dtype=torch.float64, device=ctx.tension_like.device)
+            return g_ux, g_uy, g_vof, gt, None
+
+    return RolloutFunction
+
+
+_RF = None
+
+
+def rollout(ux0, uy0, vof0, tension, r: Rollout):
+    """differentiable rollout: returns (ux, uy, vof, p) after len(r.dts) steps"""
+    global _RF
+    if _RF is None:
+        _RF = _function()
+    return _RF.apply(ux0, uy0, vof0, tension, r)
+
+
+def falling_objective(ux, uy, vof, xf, ly: float = 1.0):
+    """the differentiation workload's objective: the vof-weighted centroid y
+    of the droplet plus 0.1 times the kinetic energy (the reference's energy
+    weights, src/logging/energy.c:41-65: ux on dxc dy, uy on dxf dy)"""
+    import torch
+    ny, nx = vof.shape
+    dy = ly / ny
+    xf = torch.as_tensor(np.asarray(xf), dtype=torch.float64, device=vof.device)
+    dxf = xf[1:] - xf[:-1]
+    xc = torch.cat([xf[:1], 0.5 * (xf[1:] + xf[:-1]), xf[-1:]])
+    dxc = xc[1:] - xc[:-1]                              # nx + 1 face spacings
+    yc = (torch.arange(ny, dtype=torch.float64, device=vof.device) + 0.5) * dy
+    w = vof * dxf[None, :] * dy
+    centroid = torch.sum(w * yc[:, None]) / torch.sum(w)
+    ke = 0.5 * torch.sum(ux * ux * dxc[None, 1:nx] * dy) + 0.5 * torch.sum(uy * uy * dxf[None, :] * dy)
+    return centroid + 0.1 * ke
+
+
+__all__ = ["Rollout", "rollout", "falling_objective", "SvofError"]

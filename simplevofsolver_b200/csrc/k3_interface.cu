@@ -25,10 +25,26 @@
 #include "svof3d_internal.cuh"
 #include "smem_limit.cuh"
 
+// Precision split of this translation unit: built twice, once with
+// SVOF3_PRECISION=64 (the FP64 instantiations and the shared non-template
+// code, FMA contraction off as for every FP64 kernel) and once with
+// SVOF3_PRECISION=32 (the mixed path's FP32 instantiations only, FMA on).
+// Without the macro both are built in one pass.
+#if !defined(SVOF3_PRECISION) || SVOF3_PRECISION == 64
+#define SVOF3_WITH_F64 1
+#else
+#define SVOF3_WITH_F64 0
+#endif
+#if !defined(SVOF3_PRECISION) || SVOF3_PRECISION == 32
+#define SVOF3_WITH_F32 1
+#else
+#define SVOF3_WITH_F32 0
+#endif
+
 namespace svof3 {
 
-__constant__ double c3_gauss_p[2] = {-0.2886751345948129, +0.2886751345948129};
-__constant__ double c3_gauss_w[2] = {+0.5, +0.5};
+static __constant__ double c3_gauss_p[2] = {-0.2886751345948129, +0.2886751345948129};
+static __constant__ double c3_gauss_w[2] = {+0.5, +0.5};
 constexpr double kVofBeta = 1.;
 constexpr double kVofMin = 1.e-8;
 
@@ -38,6 +54,7 @@ constexpr double kVofMin = 1.e-8;
 // halo planes, then assigns the x wall values of the interior rows; vof walls
 // are zero in every row.  A halo row therefore holds the values its source
 // row had before the wall assignment.
+#if SVOF3_WITH_F64
 __global__ void k3_halo_bc(double *a, int width, int nh, int ny, int nz, int kind, double lo, double hi) {
   const long w = width;
   const long tot = w * ny * nz;
@@ -73,6 +90,7 @@ __global__ void k3_halo_bc(double *a, int width, int nh, int ny, int nz, int kin
     }
   at(r, q) = val;
 }
+#endif
 
 template <class T>
 __device__ __forceinline__ T plane_dx(T v00, T v10, T v01, T v11) {
@@ -646,10 +664,9 @@ cudaError_t interface_advect(cudaStream_t st, const double *vof, double *vof_new
   return cudaGetLastError();
 }
 
-cudaError_t interface_prepare() {
-  cudaError_t e = raise_smem_limit(k3_vof_advect<double>, kAdvectSmem);
-  if (cudaSuccess != e) return e;
-  return raise_smem_limit(k3_vof_advect<float>, kAdvectSmem);
+template <class R>
+cudaError_t interface_prepare_t() {
+  return raise_smem_limit(k3_vof_advect<R>, kAdvectSmem);
 }
 
 #define SVOF3_INTERFACE_INST(R)                                                                                \
@@ -658,8 +675,25 @@ cudaError_t interface_prepare() {
   template cudaError_t interface_advect<R>(cudaStream_t, const double *, double *, const double *, const double *, \
                                            const double *, const R *, double *, const double *, const double *,   \
                                            RK, int, Grid3);
+#if SVOF3_WITH_F64
 SVOF3_INTERFACE_INST(double)
+template cudaError_t interface_prepare_t<double>();
+#endif
+#if SVOF3_WITH_F32
 SVOF3_INTERFACE_INST(float)
+template cudaError_t interface_prepare_t<float>();
+#endif
 #undef SVOF3_INTERFACE_INST
+
+#if SVOF3_WITH_F64
+#if !SVOF3_WITH_F32
+extern template cudaError_t interface_prepare_t<float>();
+#endif
+cudaError_t interface_prepare() {
+  cudaError_t e = interface_prepare_t<double>();
+  if (cudaSuccess != e) return e;
+  return interface_prepare_t<float>();
+}
+#endif
 
 }  // namespace svof3

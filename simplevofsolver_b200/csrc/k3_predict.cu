@@ -23,11 +23,26 @@
 #include "svof3d_internal.cuh"
 #include "smem_limit.cuh"
 
+// Precision split as in k3_interface.cu: SVOF3_PRECISION=64 builds the FP64
+// instantiations and the shared code (no FMA contraction), =32 the FP32
+// instantiations only (FMA on); unset builds both.
+#if !defined(SVOF3_PRECISION) || SVOF3_PRECISION == 64
+#define SVOF3_WITH_F64 1
+#else
+#define SVOF3_WITH_F64 0
+#endif
+#if !defined(SVOF3_PRECISION) || SVOF3_PRECISION == 32
+#define SVOF3_WITH_F32 1
+#else
+#define SVOF3_WITH_F32 0
+#endif
+
 namespace svof3 {
 
 // Layout per system s at coef + 3 s nx:  L[i] = tdm_l[i];  R[0] = tdm_c[0],
 // R[i] = 1 / (c_i - l_i v_{i-1}) for 0 < i < n-1, R[n-1] = 1 / (c - l v) of
 // the last row or 0 when that row is zeroed (src/tdm.c:17-50);  V[i] = v_i.
+#if SVOF3_WITH_F64
 __global__ void k3_tdm_coef(const double *__restrict__ lap_ux, const double *__restrict__ lap_cc,
                             const double *__restrict__ dtp, double gam, double m_dif, double t_dif, int nx,
                             double *__restrict__ coef) {
@@ -70,6 +85,7 @@ __global__ void k3_tdm_coef(const double *__restrict__ lap_ux, const double *__r
     R[n - 1] = fabs(val) > kDblEpsilon ? 1. / val : 0.;
   }
 }
+#endif
 
 // The stencil values one cell's right-hand sides read: uy, uz, t at cell i
 // and ux at the face iu = i + 1 (names: u = ux, v = uy, w = uz, t, p; 0 / 1
@@ -665,12 +681,28 @@ cudaError_t predict_launch(cudaStream_t st, const Predict3Args<R> &a) {
   return cudaGetLastError();
 }
 
-cudaError_t predict_prepare() {
-  cudaError_t e = raise_smem_limit(k3_rhs<double>, kRhsSmem<double>);
-  if (cudaSuccess != e) return e;
-  return raise_smem_limit(k3_rhs<float>, kRhsSmem<float>);
+template <class R>
+cudaError_t predict_prepare_t() {
+  return raise_smem_limit(k3_rhs<R>, kRhsSmem<R>);
 }
+#if SVOF3_WITH_F64
 template cudaError_t predict_launch<double>(cudaStream_t, const Predict3Args<double> &);
+template cudaError_t predict_prepare_t<double>();
+#endif
+#if SVOF3_WITH_F32
 template cudaError_t predict_launch<float>(cudaStream_t, const Predict3Args<float> &);
+template cudaError_t predict_prepare_t<float>();
+#endif
+
+#if SVOF3_WITH_F64
+#if !SVOF3_WITH_F32
+extern template cudaError_t predict_prepare_t<float>();
+#endif
+cudaError_t predict_prepare() {
+  cudaError_t e = predict_prepare_t<double>();
+  if (cudaSuccess != e) return e;
+  return predict_prepare_t<float>();
+}
+#endif
 
 }  // namespace svof3

@@ -40,23 +40,38 @@ __device__ __forceinline__ double poisson_rhs(const double *__restrict__ ux, con
   return prefactor * (+(ux_xp - ux_xm) / dx + (uy_yp - uy_ym) / g.dy);
 }
 
+// the right-hand side of the forward solve (assign_input): the divergence of
+// the predicted velocity times the substep's prefactor
+struct DivRhs {
+  const double *ux, *uy;
+  Grid2 g;
+  double prefactor;
+  __device__ __forceinline__ double operator()(int i, int j) const { return poisson_rhs(ux, uy, g, i, j, prefactor); }
+};
+
+// a right-hand side given as an array [j-1][i-1] divided by the cell widths
+// dxf (the adjoint's solve with the grid-metric weights of the x grid)
+struct ArrayRhs {
+  const double *r;
+  const double *dxf;
+  int nx;
+  __device__ __forceinline__ double operator()(int i, int j) const {
+    return r[(size_t)(j - 1) * nx + (i - 1)] / dxf[i - 1];
+  }
+};
+
 // ---------------------------------------------------------------- DCT path
-// one block per row j; dynamic shared memory 2 nx doubles
-__global__ void k_dct_fwd(const double *__restrict__ ux, const double *__restrict__ uy,
-                          double *__restrict__ spec, const double *__restrict__ tw,
-                          const double *__restrict__ cs, const double *__restrict__ dtp,
-                          double gam, int log2n, Grid2 g) {
-  pdl_enter();
+// row j of the right-hand side, FFTW_REDFT10 along x into spec; the block's
+// dynamic shared memory holds 2 nx doubles
+template <class Rhs>
+__device__ __forceinline__ void dct_fwd_row(const Rhs &rhs, double *__restrict__ spec, const double *__restrict__ tw,
+                                            const double *__restrict__ cs, int log2n, int n, int j) {
   extern __shared__ double z[];
-  const int n = g.nx;
-  const int j = 1 + blockIdx.x;
-  const double dt = *dtp;
-  const double prefactor = 1. / (gam * dt) / (2. * n);
   // Makhoul reordering v_m = x_{2m}, v_{n-1-m} = x_{2m+1}, stored bit-reversed
   for (int q = threadIdx.x; q < n; q += blockDim.x) {
     const int m = bitrev(q, log2n);
     const int src = (m < n / 2) ? 2 * m : 2 * (n - 1 - m) + 1;
-    z[2 * q] = poisson_rhs(ux, uy, g, src + 1, j, prefactor);
+    z[2 * q] = rhs(src + 1, j);
     z[2 * q + 1] = 0.;
   }
   __syncthreads();
@@ -66,6 +81,23 @@ __global__ void k_dct_fwd(const double *__restrict__ ux, const double *__restric
     const double c = cs[2 * k], s = cs[2 * k + 1];
     out[k] = 2.0 * (c * z[2 * k] + s * z[2 * k + 1]);
   }
+}
+
+// one block per row j; dynamic shared memory 2 nx doubles
+__global__ void k_dct_fwd(const double *__restrict__ ux, const double *__restrict__ uy,
+                          double *__restrict__ spec, const double *__restrict__ tw,
+                          const double *__restrict__ cs, const double *__restrict__ dtp,
+                          double gam, int log2n, Grid2 g) {
+  pdl_enter();
+  const int n = g.nx;
+  const double dt = *dtp;
+  const double prefactor = 1. / (gam * dt) / (2. * n);
+  dct_fwd_row(DivRhs{ux, uy, g, prefactor}, spec, tw, cs, log2n, n, 1 + blockIdx.x);
+}
+
+__global__ void k_dct_fwd_rhs(const double *__restrict__ r, double *__restrict__ spec, const double *__restrict__ tw,
+                              const double *__restrict__ cs, int log2n, Grid2 g) {
+  dct_fwd_row(ArrayRhs{r, g.dxf, g.nx}, spec, tw, cs, log2n, g.nx, 1 + blockIdx.x);
 }
 
 // periodic tri-diagonal solve along y per wavenumber k (src/tdm.c:78-99 with
@@ -192,24 +224,19 @@ __global__ void k_dct_inv(const double *__restrict__ spec, double *__restrict__ 
 }
 
 // ---------------------------------------------------------------- DFT path
-// a block owns `cols` consecutive columns i0 .. i0+cols-1 and all ny rows;
-// dynamic shared memory cols * 2 ny doubles
-__global__ void k_dft_fwd(const double *__restrict__ ux, const double *__restrict__ uy,
-                          double *__restrict__ spec, const double *__restrict__ tw,
-                          const double *__restrict__ dtp, double gam, int log2n, int cols, Grid2 g) {
-  pdl_enter();
+// columns i0 .. i0+cols-1 of the right-hand side, r2c along y into spec; the
+// block's dynamic shared memory holds cols * 2 ny doubles
+template <class Rhs>
+__device__ __forceinline__ void dft_fwd_cols(const Rhs &rhs, double *__restrict__ spec, const double *__restrict__ tw,
+                                             int log2n, int cols, int nx, int n, int i0) {
   extern __shared__ double z[];
-  const int n = g.ny, nx = g.nx;
   const int nky = n / 2 + 1;
-  const int i0 = 1 + blockIdx.x * cols;
   const int nc = min(cols, nx - i0 + 1);
-  const double dt = *dtp;
-  const double prefactor = 1. / (gam * dt) / (1. * n);
   for (int w = threadIdx.x; w < cols * n; w += blockDim.x) {
     const int q = w / cols, col = w % cols;
     const int m = bitrev(q, log2n);
     double v = 0.;
-    if (col < nc) v = poisson_rhs(ux, uy, g, i0 + col, m + 1, prefactor);
+    if (col < nc) v = rhs(i0 + col, m + 1);
     z[2 * (col * n + q)] = v;
     z[2 * (col * n + q) + 1] = 0.;
   }
@@ -221,6 +248,23 @@ __global__ void k_dft_fwd(const double *__restrict__ ux, const double *__restric
     spec[o] = z[2 * (col * n + k)];
     spec[o + 1] = z[2 * (col * n + k) + 1];
   }
+}
+
+// a block owns `cols` consecutive columns i0 .. i0+cols-1 and all ny rows;
+// dynamic shared memory cols * 2 ny doubles
+__global__ void k_dft_fwd(const double *__restrict__ ux, const double *__restrict__ uy,
+                          double *__restrict__ spec, const double *__restrict__ tw,
+                          const double *__restrict__ dtp, double gam, int log2n, int cols, Grid2 g) {
+  pdl_enter();
+  const int n = g.ny;
+  const double dt = *dtp;
+  const double prefactor = 1. / (gam * dt) / (1. * n);
+  dft_fwd_cols(DivRhs{ux, uy, g, prefactor}, spec, tw, log2n, cols, g.nx, n, 1 + blockIdx.x * cols);
+}
+
+__global__ void k_dft_fwd_rhs(const double *__restrict__ r, double *__restrict__ spec, const double *__restrict__ tw,
+                              int log2n, int cols, Grid2 g) {
+  dft_fwd_cols(ArrayRhs{r, g.dxf, g.nx}, spec, tw, log2n, cols, g.nx, g.ny, 1 + blockIdx.x * cols);
 }
 
 // complex Neumann Thomas along x per ky (dft.c:364-395); spec layout [i][ky],

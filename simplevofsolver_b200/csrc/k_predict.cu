@@ -169,6 +169,10 @@ __global__ void __launch_bounds__(256) k_predict(PredictArgs a) {
       sg -= 1. / dy * (-p[ix_cc(nx, i, j - 1)] + p[ix_cc(nx, i, j)]);
       // surface, uy.c:176-187
       sa += a.ifrcy[ix_src(nx, i, j)];
+      // extension: buoyancy of the volume fraction (not in the reference)
+      if (0. != a.grav_vof) {
+        sa += a.grav_vof * (0.5 * a.vof[ix_vof(nx, i, j - 1)] + 0.5 * a.vof[ix_vof(nx, i, j)] - a.vof_ref);
+      }
       a.suy_a[ix_src(nx, i, j)] = sa;
       const double sb = a.use_b ? cb * a.suy_b[ix_src(nx, i, j)] : 0.;
       sd[(1 * R + jj) * ld + (i - 1)] = +ca * sa + sb + cg * sg;

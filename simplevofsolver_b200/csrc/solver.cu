@@ -23,35 +23,14 @@
 #include "svof_internal.cuh"
 #include "stat_internal.cuh"
 #include "smem_limit.cuh"
+#include "solver_state.cuh"
 
 using namespace svof;
 
 namespace {
 
-thread_local std::string g_err;
-
-int fail(const char *fmt, ...) {
-  char buf[512];
-  va_list ap;
-  va_start(ap, fmt);
-  vsnprintf(buf, sizeof(buf), fmt, ap);
-  va_end(ap);
-  g_err = buf;
-  return 1;
-}
-
-#define CK(x)                                                                  \
-  do {                                                                         \
-    cudaError_t e_ = (x);                                                      \
-    if (cudaSuccess != e_) return fail("%s: %s", #x, cudaGetErrorString(e_));  \
-  } while (0)
-
-#define CK_LAUNCH() CK(cudaGetLastError())
-
 constexpr double kPi = 3.14159265358979323846;        // oracle/svof_fft.c
 constexpr double kGPi = 3.14159265358979324;          // src/fluid/compute_potential/dct.c:20
-constexpr double RK_A[3] = {32. / 60., 25. / 60., 45. / 60.};
-constexpr double RK_B[3] = {0. / 60., -17. / 60., -25. / 60.};
 
 int ilog2_exact(int n) {
   int l = 0;
@@ -77,75 +56,27 @@ void host_gtsv(int n, const double *l, const double *c, const double *u, double 
   for (int i = n - 2; i >= 0; i--) q[i] -= v[i] * q[i + 1];
 }
 
-struct DevBuf {
-  double *p = nullptr;
-  size_t n = 0;
-};
 
 }  // namespace
 
-struct svof_solver {
-  svof_params_t prm{};
-  bool managed = false;     // field buffers in CUDA managed memory
-  int nx = 0, ny = 0;
-  double dy = 0.;
-  bool uniform = false;
-  int log2fft = 0;          // log2 of the FFT length (nx for DCT, ny for DFT)
-  cudaStream_t stream = nullptr;
-  // fields (two buffers where a kernel writes a new copy)
-  DevBuf ux[2], uy[2], t[2], vof[2];
-  DevBuf p, psi, curv, normal, ifrcx, ifrcy;
-  DevBuf sux[2], suy[2], st[2], svof[2];
-  int cur_u = 0;   // which of ux/uy/t[] is current
-  int cur_v = 0;   // which of vof[] is current
-  int sa_f = 0;    // which of sux/suy/st[] is src[rk_a]
-  int sa_v = 0;    // which of svof[] is src[rk_a]
-  // grid tables
-  DevBuf dxf, dxc, lap_ux, lap_uy, lap_t;
-  double lapy[3] = {0., 0., 0.};
-  double dif_m_y = 0., dif_t_y = 0.;
-  // Poisson
-  DevBuf spec, twf, twb, cs, vt, rvt, q1t, ck, lastf, den, pl, pu, evals;
-  int ysolve_kt = 32;       // wavenumber lines per block of the DCT y solve
-  // predictor Thomas coefficients of the current substep (k_tdm_coef)
-  DevBuf coef;
-  // side stream of the step graph: the coefficient kernel runs beside the
-  // interface kernels
-  cudaStream_t side = nullptr;
-  cudaEvent_t ev_fork[3] = {nullptr, nullptr, nullptr}, ev_join[3] = {nullptr, nullptr, nullptr};
-  cudaEvent_t ev_geom[3] = {nullptr, nullptr, nullptr};
-  // predict launch shape
-  int pred_rows = 1;
-  int pred_threads = 256;
-  size_t pred_smem = 0;
-  int xsolve_kt = 8;        // ky lines per block of the DFT x solve
-  int dft_cols = 1;
-  // time step
-  double *d_dt = nullptr;
-  unsigned long long *d_minbits = nullptr;
-  double *h_dt = nullptr;   // pinned, many slots for svof_run
-  int h_dt_slots = 0;
-  DevBuf diag;
-  // set while the step graph of a small grid is captured: its kernels are
-  // launched with programmatic stream serialisation (each starts with
-  // pdl_enter)
-  bool pdl = false;
-  // time-averaged statistics: accumulators (made on the first collection),
-  // row-sum scratch, samples so far
-  DevBuf stat[SVOF_NSTATS], stat_part;
-  size_t stat_num = 0;
-  std::vector<double> xf, xc, dxf_h, dxc_h;
-  // graphs keyed by the buffer state at the start of a step
-  std::map<int, cudaGraphExec_t> graphs;
 
-  Grid2 grid() const { return Grid2{nx, ny, dy, dxf.p, dxc.p}; }
-};
+namespace svof {
 
-namespace {
+thread_local std::string g_err;
+
+int fail(const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return 1;
+}
 
 // managed: CUDA managed memory, so that a host program holding the pointer
 // (the reference's logging and save code read the fields directly) can read it
-int dalloc(DevBuf &b, size_t n, bool managed = false) {
+int dalloc(DevBuf &b, size_t n, bool managed) {
   b.n = n;
   if (managed) {
     CK(cudaMallocManaged(&b.p, sizeof(double) * (n ? n : 1)));
@@ -170,27 +101,6 @@ void dfree(DevBuf &b) {
 
 // ---- launch helpers: each issues the kernels of one reference function ----
 
-// launch k on st; with pdl, as a programmatic dependent of the stream's
-// previous kernel
-template <typename... KArgs, typename... Args>
-cudaError_t launch_k(bool pdl, void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
-                     Args... args) {
-  if (!pdl) {
-    k<<<grid, block, smem, st>>>(args...);
-    return cudaGetLastError();
-  }
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = grid;
-  cfg.blockDim = block;
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = st;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = at;
-  cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k, args...);
-}
 
 int launch_halo_bc(svof_solver *s, double *a, int field) {
   const int nx = s->nx, ny = s->ny;
@@ -227,7 +137,7 @@ int launch_geom(svof_solver *s) {
   return 0;
 }
 
-int launch_force(svof_solver *s, cudaStream_t st = nullptr) {
+int launch_force(svof_solver *s, cudaStream_t st) {
   dim3 b(32, 8), gr((s->nx + 31) / 32, (s->ny + 7) / 8);
   CK(launch_k(s->pdl, k_force, gr, b, 0, st ? st : s->stream, (const double *)s->vof[s->cur_v].p,
               (const double *)s->curv.p, s->ifrcx.p, s->ifrcy.p, s->prm.tension, s->grid()));
@@ -255,7 +165,7 @@ int launch_coef(svof_solver *s, int rk, cudaStream_t st) {
 
 // with_coef: launch k_tdm_coef first on the same stream (the step graph
 // launches it on the side stream instead)
-int launch_predict(svof_solver *s, int rk, bool with_coef = true) {
+int launch_predict(svof_solver *s, int rk, bool with_coef) {
   if (with_coef && launch_coef(s, rk, s->stream)) return 1;
   if (0 != rk) s->sa_f ^= 1;  // reset_srcs, src/fluid/predict/main.c:9-29
   PredictArgs a{};
@@ -292,6 +202,9 @@ int launch_predict(svof_solver *s, int rk, bool with_coef = true) {
   a.uy_xp = s->prm.uy_xp;
   a.t_xm = s->prm.t_xm;
   a.t_xp = s->prm.t_xp;
+  a.vof = s->vof[s->cur_v].p;
+  a.grav_vof = s->grav_vof;
+  a.vof_ref = s->vof_ref;
   a.rows_per_block = s->pred_rows;
   a.g = s->grid();
   const int blocks = (s->ny + s->pred_rows - 1) / s->pred_rows;
@@ -739,6 +652,7 @@ extern "C" {
 int svof_destroy(svof_solver_t *s) {
   if (!s) return 0;
   if (s->stream) cudaStreamSynchronize(s->stream);
+  adjoint_free(s);
   for (auto &kv : s->graphs) cudaGraphExecDestroy(kv.second);
   s->graphs.clear();
   for (int k = 0; k < 2; k++) {

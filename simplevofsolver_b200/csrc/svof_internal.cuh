@@ -84,6 +84,11 @@ struct PredictArgs {
   int use_b;
   int add_buoyancy;
   double uy_xm, uy_xp, t_xm, t_xp;
+  // vof buoyancy on uy (an extension, absent from the reference; skipped
+  // while grav_vof is 0): srcuy_a += grav_vof (vof at the uy face - vof_ref),
+  // vof the field after this substep's advection
+  const double *vof;
+  double grav_vof, vof_ref;
   int rows_per_block;
   Grid2 g;
 };
@@ -115,6 +120,14 @@ __global__ void k_dft_xsolve(double *__restrict__ spec, const double *__restrict
                              int nky, int kt);
 __global__ void k_dft_inv(const double *__restrict__ spec, double *__restrict__ psi,
                           const double *__restrict__ tw, int log2n, int cols, Grid2 g);
+
+// the forward transforms of the two paths on a right-hand side r[j-1][i-1] /
+// dxf[i-1] (the adjoint's second Poisson solve, with the grid-metric weights
+// of the x grid); same launch shapes
+__global__ void k_dct_fwd_rhs(const double *__restrict__ r, double *__restrict__ spec, const double *__restrict__ tw,
+                              const double *__restrict__ cs, int log2n, Grid2 g);
+__global__ void k_dft_fwd_rhs(const double *__restrict__ r, double *__restrict__ spec, const double *__restrict__ tw,
+                              int log2n, int cols, Grid2 g);
 
 // projection and pressure update, in place (src/fluid/correct_velocity/*.c,
 // src/fluid/update_pressure.c); do_vel / do_p select the two halves

@@ -308,6 +308,52 @@ DROPLETS3D_ENV = {"Ra": 2.5e5, "Pr": 1.0, "We": 20.0, "coef_dt_adv": 0.5, "coef_
 DROPLET2D_ENV = {"Ra": 1.0e4, "Pr": 1.0, "We": 10.0, "coef_dt_adv": 0.5, "coef_dt_dif": 0.95}
 
 
+# the falling droplet of the differentiation workload: Re = 200 (Ra = Re^2 with
+# Pr = 1 gives m_dif = 1 / Re), We = 20; gravity Fr = 1 and the density ratio
+# 0.1 enter as the vof buoyancy coefficient grav_vof = -(1 - 0.1) / Fr^2
+FALLING2D_ENV = {"Ra": 4.0e4, "Pr": 1.0, "We": 20.0, "coef_dt_adv": 0.5, "coef_dt_dif": 0.95}
+FALLING2D_FROUDE = 1.0
+FALLING2D_DENSITY_RATIO = 0.1
+
+
+def falling_droplet2d(n: int = 256, radius: float = 0.15, centre=(0.5, 0.7), rms: float = 0.05,
+                      kmax: int = 3, seed: int = 0, uniform: bool = True) -> InitialCondition:
+    """One circular droplet (radius 0.15 at (0.5, 0.7)) in the unit box, and a
+    seeded divergence-free random velocity of the given rms: the staggered
+    curl of the stream function sin^2(pi x) sum_k (a_k cos 2 pi k y + b_k
+    sin 2 pi k y), 1 <= k <= kmax, evaluated at the cell corners, so that the
+    discrete divergence vanishes and ux vanishes at the walls.  vof as
+    droplet2d (tanh profile of one-third-cell width, sub-cell integration)."""
+    ic = droplet2d(n, n, 1.0, 1.0, uniform=uniform, centre=centre, semi_axes=(radius, radius), noise=0.0,
+                   seed=seed)
+    rng = np.random.default_rng(seed)
+    a = rng.standard_normal(kmax)
+    b = rng.standard_normal(kmax)
+    yf = np.arange(n + 1) * (1.0 / n)                                 # corner rows y_{j-1/2}
+    xf = ic.xf
+    k = np.arange(1, kmax + 1)[:, None]
+    fy = (a[:, None] * np.cos(2 * np.pi * k * yf[None, :]) + b[:, None] * np.sin(2 * np.pi * k * yf[None, :])).sum(0)
+    psi = (np.sin(np.pi * xf) ** 2)[None, :] * fy[:, None]            # (n+1 corners in y, n+1 in x)
+    dy = 1.0 / n
+    dxf = np.diff(xf)
+    ux = (psi[1:, :] - psi[:-1, :]) / dy                              # (n, n+1) faces, rows j
+    uy = -(psi[:, 1:] - psi[:, :-1]) / dxf[None, :]                   # (n+1, n) rows j-1/2
+    scale = rms / np.sqrt(0.5 * (np.mean(ux[:, 1:-1] ** 2) + np.mean(uy ** 2)))
+    ic.ux[:, 1:-1] = scale * ux[:, 1:-1]
+    ic.uy[:, 1:-1] = scale * uy[:-1, :]
+    return ic
+
+
+def falling_gravity(ic: InitialCondition, froude: float = FALLING2D_FROUDE,
+                    density_ratio: float = FALLING2D_DENSITY_RATIO):
+    """(grav_vof, vof_ref) of the vof buoyancy extension: gravity -1/Fr^2
+    along y on the density difference (1 - ratio) vof, relative to the
+    domain-mean volume fraction (no net force along the periodic y)"""
+    dxf = np.diff(ic.xf)
+    vof_ref = float(np.sum(ic.vof[:, 1:-1] * dxf[None, :]) / (ic.ly * ic.lx) * (ic.ly / ic.ny))
+    return -(1.0 - density_ratio) / froude ** 2, vof_ref
+
+
 def physical_params(env: dict):
     """Diffusivities and surface tension as the reference derives them."""
     Ra, Pr, We = float(env["Ra"]), float(env["Pr"]), float(env["We"])
