@@ -22,6 +22,12 @@ throughput on a bounded sample, and the SM clocks seen during the timed
 region.  The path does not shard (one domain per GPU): with N GPUs every rank
 runs an independent replica ("weak" scaling, no collective on the data path).
 
+The 3D line also carries the differentiation form's cost ("adjoint",
+"adjoint_over_forward"): on its workload (falling droplet, 256 x 256, 200
+steps, checkpoints every 20) the device time per step of the backward pass
+(segment recompute with tapes plus the CUDA step adjoints) over that of the
+forward (--no-adjoint skips it).
+
 --impl reference times the reference's own C implementation (its src/*.c
 compiled against single-rank shims, oracle/_ref) on all host cores: one
 single-rank process per core, each a replica of the same workload.  The

@@ -58,6 +58,20 @@ def gradient(ic, r, x):
     return float(J), {k: xs[k].grad.clone() for k in ("ux", "uy", "ten")}
 
 
+def solenoidal_direction(rng, nx, ny, xf):
+    """a random divergence-free velocity perturbation: the discrete curl of a
+    random stream function at the cell corners, zero on the walls (the
+    perturbed initial field stays admissible: divergence-free to round-off,
+    no flow through the walls)"""
+    psi = np.zeros((ny, nx + 1))
+    psi[:, 1:nx] = rng.standard_normal((ny, nx - 1))
+    dy = 1.0 / ny
+    dxf = np.diff(xf)
+    ux = (np.roll(psi, -1, 0) - psi)[:, 1:nx] / dy
+    uy = -(psi[:, 1:] - psi[:, :-1]) / dxf[None, :]
+    return ux, uy
+
+
 def test_gradient_matches_central_differences(gpu_available):
     import torch
     ic, phys, r, x = make()
@@ -68,8 +82,9 @@ def test_gradient_matches_central_differences(gpu_available):
     eps = 1e-6
     worst_norm, worst_rel = 0.0, 0.0
     for _ in range(16):
-        v = {k: torch.tensor(rng.standard_normal(tuple(x[k].shape)), dtype=torch.float64, device="cuda")
-             for k in ("ux", "uy", "ten")}
+        dux, duy = solenoidal_direction(rng, ic.nx, ic.ny, ic.xf)
+        v = {k: torch.tensor(a, dtype=torch.float64, device="cuda")
+             for k, a in (("ux", dux), ("uy", duy), ("ten", np.array(rng.standard_normal())))}
         nrm = float(torch.sqrt(sum(torch.sum(a * a) for a in v.values())))
         v = {k: a / nrm for k, a in v.items()}
         d_adj = float(sum(torch.sum(grad[k] * v[k]) for k in v))
