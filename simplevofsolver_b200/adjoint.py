@@ -14,6 +14,14 @@ substep inputs of its K steps on a tape (K tapes of ``tape_count()`` doubles),
 and applies the K step adjoints in reverse.  Device memory: N / K
 checkpoints + K tapes.
 
+The initial velocity is first projected onto discretely divergence-free
+fields (``project_initial``, the default): the reference's curvature, taken
+from normalised vof gradients, has no derivative where the gradient vanishes
+(the flat bulk of a droplet), and a velocity perturbation with divergence
+changes vof there; along divergence-free perturbations, the admissible ones
+for an incompressible initial state, the map is differentiable, and the
+projection's adjoint removes the rest from the gradient.
+
 Tensors live on the GPU in compact layouts: ux on the interior faces
 (ny, nx-1), uy, vof and p on the cells (ny, nx).  The temperature is not
 differentiated (buoyancy of t must be off); the vof buoyancy extension
@@ -46,7 +54,7 @@ class Rollout:
 
     STATE = ("ux", "uy", "p", "t", "vof")
 
-    def __init__(self, solver: Solver, dts, checkpoint_every: int = 20):
+    def __init__(self, solver: Solver, dts, checkpoint_every: int = 20, project_initial: bool = True):
         import torch
         if checkpoint_every < 1:
             raise ValueError("checkpoint_every must be at least 1")
@@ -58,6 +66,7 @@ class Rollout:
         self.t0 = solver.interior("t")
         self.tapes = None
         self.checkpoints = []
+        self.project = bool(project_initial)
         self._torch = torch
 
     # -- state transfer (the solver's stream and torch's are synchronised around each)
@@ -73,6 +82,14 @@ class Rollout:
         s.load_interior("vof", _to_interior("vof", vof0, self.nx, self.ny))
         s.load_interior("p", self.p0)
         s.load_interior("t", self.t0)
+        if self.project:
+            # the discrete projection u - grad L^-1 div u of the initial
+            # velocity (the Poisson solve and correction of a substep; the
+            # product gamma dt cancels): a divergence-free field is kept to
+            # round-off, and the gradient is the one of the admissible
+            # (divergence-free) initial fields
+            s.fluid_compute_potential(0, 1.0)
+            s.fluid_correct_velocity(0, 1.0)
 
     def _save_state(self):
         self._sync()
@@ -132,6 +149,9 @@ class Rollout:
                 s.integrate_fixed(self.dts[n], self.tapes[n - n0].data_ptr())
             for n in reversed(range(n0, n1)):
                 s.adjoint_step(self.tapes[n - n0].data_ptr(), self.dts[n])
+        if self.project:
+            s.adjoint_fluid_correct_velocity(0, 1.0)
+            s.adjoint_fluid_compute_potential(0, 1.0)
         self._sync()
         g_ux = s.adjoint_view("ux").clone()
         g_uy = s.adjoint_view("uy").clone()

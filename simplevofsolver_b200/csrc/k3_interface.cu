@@ -253,13 +253,23 @@ __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ 
         const double a01 = sv[bprev][lj + 1][li], a11 = sv[bprev][lj + 1][li + 1];
         const double b00 = sv[bcur][lj][li], b10 = sv[bcur][lj][li + 1];
         const double b01 = sv[bcur][lj + 1][li], b11 = sv[bcur][lj + 1][li + 1];
-        const R dvofdx = rdxc[q] * R(plane_dx(a00, a10, a01, a11) + plane_dx(b00, b10, b01, b11));
-        const R dvofdy = rdy * R(plane_dy(a00, a10, a01, a11) + plane_dy(b00, b10, b01, b11));
-        const R dvofdz = rdz * R(plane_sum(b00, b10, b01, b11) - plane_sum(a00, a10, a01, a11));
-        const R norminv = rnorm(+dvofdx * dvofdx + dvofdy * dvofdy + dvofdz * dvofdz, eps);
-        d0 = dvofdx * norminv;
-        d1 = dvofdy * norminv;
-        d2 = dvofdz * norminv;
+        // eight bit-identical values (the bulk outside the droplets): every
+        // difference is +0, so the normal is +0 (+0 times 1 / eps) without
+        // the square root and division
+        const long long r = __double_as_longlong(a00);
+        const bool flat = r == __double_as_longlong(a10) && r == __double_as_longlong(a01) &&
+                          r == __double_as_longlong(a11) && r == __double_as_longlong(b00) &&
+                          r == __double_as_longlong(b10) && r == __double_as_longlong(b01) &&
+                          r == __double_as_longlong(b11);
+        if (!flat) {
+          const R dvofdx = rdxc[q] * R(plane_dx(a00, a10, a01, a11) + plane_dx(b00, b10, b01, b11));
+          const R dvofdy = rdy * R(plane_dy(a00, a10, a01, a11) + plane_dy(b00, b10, b01, b11));
+          const R dvofdz = rdz * R(plane_sum(b00, b10, b01, b11) - plane_sum(a00, a10, a01, a11));
+          const R norminv = rnorm(+dvofdx * dvofdx + dvofdy * dvofdy + dvofdz * dvofdz, eps);
+          d0 = dvofdx * norminv;
+          d1 = dvofdy * norminv;
+          d2 = dvofdz * norminv;
+        }
       }
       sc[ccur][0][lj][li] = d0;
       sc[ccur][1][lj][li] = d1;

@@ -11,6 +11,8 @@
 // per thread.  Phase 3 writes u + delta' into the other buffer of the
 // ping-pong pair together with the halo rows and wall values that
 // fluid_update_boundaries_{ux,uy,t} assign.
+#include <cuda_pipeline.h>
+
 #include "svof_internal.cuh"
 
 namespace svof {
@@ -74,30 +76,17 @@ __global__ void k_tdm_coef(const double *__restrict__ lap_ux, const double *__re
   }
 }
 
-__global__ void __launch_bounds__(256) k_predict(PredictArgs a) {
-  pdl_enter();
-  extern __shared__ double sm[];
-  const Grid2 g = a.g;
-  const int nx = g.nx, ny = g.ny, R = a.rows_per_block;
-  const int ld = nx + 1;
-  double *sd = sm;                  // [3][R][ld] increments
-  double *sc = sm + 3 * R * ld;     // [9][ld] Thomas coefficients (L, R, V of ux, uy, t)
-  const int j0 = 1 + blockIdx.x * R;
-  const int nrows = min(R, ny - j0 + 1);
-  const double dt = *a.dtp;
-  const double ca = a.rk.a * dt, cb = a.rk.b * dt, cg = a.rk.g * dt;
+// right-hand sides of ux (i >= 2), uy and t at cell (i, j), exactly as
+// compute_rhs_{ux,uy,t} (src/fluid/predict/{ux,uy,t}.c): src_a is stored for
+// the next substep, the increments dt (alpha src_a + beta src_b + gamma src_g)
+// go to d[0..2] (d[0] only for i >= 2)
+__device__ __forceinline__ void predict_rhs_cell(const PredictArgs &a, int i, int j, double ca, double cb,
+                                                 double cg, double *d) {
+  const Grid2 &g = a.g;
+  const int nx = g.nx;
   const double dy = g.dy;
   const double *ux = a.ux, *uy = a.uy, *p = a.p, *t = a.t;
-  const int tid = threadIdx.x;
-
-  for (int w = tid; w < 9 * nx; w += blockDim.x) sc[(w / nx) * ld + (w % nx)] = a.coef[w];
-
-  // ---------------- phase 1: right-hand sides and increments
-  for (int w = tid; w < nrows * nx; w += blockDim.x) {
-    const int jj = w / nx;
-    const int i = 1 + w % nx;
-    const int j = j0 + jj;
-    const double dxf_i = g.dxf[i - 1];
+  const double dxf_i = g.dxf[i - 1];
     // ---- ux at (i, j), i in [2, nx]: compute_rhs_ux, ux.c:218-249
     if (i >= 2) {
       const double dxc_i = g.dxc[i - 1];
@@ -136,7 +125,7 @@ __global__ void __launch_bounds__(256) k_predict(PredictArgs a) {
       sa += a.ifrcx[ix_srcx(nx, i, j)];
       a.sux_a[ix_srcx(nx, i, j)] = sa;
       const double sb = a.use_b ? cb * a.sux_b[ix_srcx(nx, i, j)] : 0.;
-      sd[(0 * R + jj) * ld + (i - 2)] = +ca * sa + sb + cg * sg;
+      d[0] = +ca * sa + sb + cg * sg;
     }
     // ---- uy at (i, j): compute_rhs_uy, uy.c:195-221
     {
@@ -175,7 +164,7 @@ __global__ void __launch_bounds__(256) k_predict(PredictArgs a) {
       }
       a.suy_a[ix_src(nx, i, j)] = sa;
       const double sb = a.use_b ? cb * a.suy_b[ix_src(nx, i, j)] : 0.;
-      sd[(1 * R + jj) * ld + (i - 1)] = +ca * sa + sb + cg * sg;
+      d[1] = +ca * sa + sb + cg * sg;
     }
     // ---- t at (i, j): compute_rhs_t, t.c:160-182
     {
@@ -202,8 +191,36 @@ __global__ void __launch_bounds__(256) k_predict(PredictArgs a) {
       sa += a.t_dif * (+a.lapy0 * ts + a.lapy1 * tc + a.lapy2 * tn);
       a.st_a[ix_src(nx, i, j)] = sa;
       const double sb = a.use_b ? cb * a.st_b[ix_src(nx, i, j)] : 0.;
-      sd[(2 * R + jj) * ld + (i - 1)] = +ca * sa + sb + cg * sg;
+      d[2] = +ca * sa + sb + cg * sg;
     }
+  }
+
+__global__ void __launch_bounds__(256) k_predict(PredictArgs a) {
+  pdl_enter();
+  extern __shared__ double sm[];
+  const Grid2 g = a.g;
+  const int nx = g.nx, ny = g.ny, R = a.rows_per_block;
+  const int ld = nx + 1;
+  double *sd = sm;                  // [3][R][ld] increments
+  double *sc = sm + 3 * R * ld;     // [9][ld] Thomas coefficients (L, R, V of ux, uy, t)
+  const int j0 = 1 + blockIdx.x * R;
+  const int nrows = min(R, ny - j0 + 1);
+  const double dt = *a.dtp;
+  const double ca = a.rk.a * dt, cb = a.rk.b * dt, cg = a.rk.g * dt;
+  const int tid = threadIdx.x;
+
+  for (int w = tid; w < 9 * nx; w += blockDim.x) sc[(w / nx) * ld + (w % nx)] = a.coef[w];
+
+  // ---------------- phase 1: right-hand sides and increments
+  for (int w = tid; w < nrows * nx; w += blockDim.x) {
+    const int jj = w / nx;
+    const int i = 1 + w % nx;
+    const int j = j0 + jj;
+    double d[3];
+    predict_rhs_cell(a, i, j, ca, cb, cg, d);
+    if (i >= 2) sd[(0 * R + jj) * ld + (i - 2)] = d[0];
+    sd[(1 * R + jj) * ld + (i - 1)] = d[1];
+    sd[(2 * R + jj) * ld + (i - 1)] = d[2];
   }
   __syncthreads();
 
@@ -283,6 +300,228 @@ __global__ void __launch_bounds__(256) k_predict(PredictArgs a) {
       a.ux_new[ix_ux(nx, i, j)] = nux;
       if (to_top) a.ux_new[ix_ux(nx, i, ny + 1)] = hux;
       if (to_bottom) a.ux_new[ix_ux(nx, i, 0)] = hux;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Line-streaming form for large grids: the fused kernel above keeps whole
+// rows in shared memory, so a block holds few rows and its Thomas phase runs
+// few lines per SM (the serial recurrence then sets the time).  Here the
+// right-hand sides of a 32 x 32 tile go to a line array, one warp per field
+// and 32 lines sweeps it (forward and backward) from a ring of shared-memory
+// chunks that cp.async fills ahead, and a tiled pass writes u + delta', the
+// halo rows and the walls.  The arithmetic (predict_rhs_cell, the sweeps with
+// the k_tdm_coef table, u + delta') is the fused kernel's, so the results are
+// identical.
+//
+// Line array layout: lines in blocks of 32, fw[((f * nb + jb) * nx + p) * 32
+// + l] for field f (0 ux: p = i - 2; 1 uy, 2 t: p = i - 1), row j = 32 jb + l
+// + 1, nb = ceil(ny / 32): the 32 lines of a block are contiguous at every
+// position, so a chunk of positions is one contiguous run.
+__device__ __forceinline__ size_t fw_ix(int nx, int ny, int f, int p, int j) {
+  const int nb = (ny + 31) >> 5, jb = (j - 1) >> 5, l = (j - 1) & 31;
+  return (((size_t)f * nb + jb) * nx + p) * 32 + l;
+}
+
+constexpr int PT = 32;  // tile edge of the right-hand-side and update passes
+
+__global__ void __launch_bounds__(256) k_predict_rhs(PredictArgs a, double *__restrict__ fw) {
+  pdl_enter();
+  __shared__ double sd[3][PT][PT + 1];  // [f][i - i0][j - j0]
+  const Grid2 g = a.g;
+  const int nx = g.nx, ny = g.ny;
+  const int i0 = 1 + blockIdx.x * PT, j0 = 1 + blockIdx.y * PT;
+  const double dt = *a.dtp;
+  const double ca = a.rk.a * dt, cb = a.rk.b * dt, cg = a.rk.g * dt;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  for (int r = ty; r < PT; r += 8) {
+    const int i = i0 + tx, j = j0 + r;
+    if (i <= nx && j <= ny) {
+      double d[3];
+      predict_rhs_cell(a, i, j, ca, cb, cg, d);
+      sd[0][tx][r] = d[0];
+      sd[1][tx][r] = d[1];
+      sd[2][tx][r] = d[2];
+    }
+  }
+  __syncthreads();
+  // transposed store: lanes along j (one contiguous 256-byte run)
+  for (int c = ty; c < PT; c += 8) {
+    const int i = i0 + c, j = j0 + tx;
+    if (i > nx || j > ny) continue;
+    if (i >= 2) fw[fw_ix(nx, ny, 0, i - 2, j)] = sd[0][c][tx];
+    fw[fw_ix(nx, ny, 1, i - 1, j)] = sd[1][c][tx];
+    fw[fw_ix(nx, ny, 2, i - 1, j)] = sd[2][c][tx];
+  }
+}
+
+// one warp per (field, block of 32 lines); chunks of XC positions in a ring
+// of XS shared-memory slots; the substep's coefficients of the field in
+// shared memory.  Dynamic shared memory: (XS * XC * 32 + 3 nx) doubles.
+constexpr int XC = 64, XS = 4;
+
+__global__ void __launch_bounds__(32) k_predict_xsolve(const double *__restrict__ coef, double *__restrict__ fw,
+                                                      int nx, int ny) {
+  pdl_enter();
+  extern __shared__ double sm[];
+  double *ring = sm;                         // [XS][XC][32]
+  double *sL = sm + (size_t)XS * XC * 32;    // [nx] L, then R, then V
+  double *sR = sL + nx, *sV = sR + nx;
+  const int nb = (ny + 31) >> 5;
+  const int f = blockIdx.x / nb, jb = blockIdx.x % nb;
+  const int l = threadIdx.x;
+  const int j = 32 * jb + l + 1;
+  const int n = (0 == f) ? nx - 1 : nx;
+  for (int w = l; w < nx; w += 32) {
+    sL[w] = coef[(size_t)(3 * f + 0) * nx + w];
+    sR[w] = coef[(size_t)(3 * f + 1) * nx + w];
+    sV[w] = coef[(size_t)(3 * f + 2) * nx + w];
+  }
+  double *base = fw + ((size_t)f * nb + jb) * nx * 32;  // position p at base + 32 p
+  const int nch = (n + XC - 1) / XC;
+  // chunk c (positions c XC .. ) into slot s: 16-byte copies, 32 lanes
+  auto load = [&](int c, int slot) {
+    const int p0 = c * XC, m = min(XC, n - p0);
+    const double *src = base + (size_t)p0 * 32;
+    double *dst = ring + (size_t)slot * XC * 32;
+    for (int e = 2 * l; e < m * 32; e += 64) __pipeline_memcpy_async(dst + e, src + e, 16);
+    __pipeline_commit();
+  };
+  auto store = [&](int c, int slot) {
+    const int p0 = c * XC, m = min(XC, n - p0);
+    double *dst = base + (size_t)p0 * 32;
+    const double *src = ring + (size_t)slot * XC * 32;
+    for (int s = 0; s < m; s++) dst[s * 32 + l] = src[s * 32 + l];
+  };
+  __syncwarp();
+  // ------------------------------------------------------------ forward
+  for (int c = 0; c < XS - 1; c++) {
+    if (c < nch) load(c, c % XS);
+    else __pipeline_commit();
+  }
+  double qprev = 0.;
+  for (int c = 0; c < nch; c++) {
+    if (c + XS - 1 < nch) load(c + XS - 1, (c + XS - 1) % XS);
+    else __pipeline_commit();
+    __pipeline_wait_prior(XS - 1);
+    __syncwarp();
+    double *q = ring + (size_t)(c % XS) * XC * 32 + l;
+    const int p0 = c * XC, m = min(XC, n - p0);
+    for (int s = 0; s < m; s++) {
+      const int p = p0 + s;
+      const double x = q[s * 32];
+      if (0 == p) {
+        qprev = x / sR[0];
+      } else if (p < n - 1) {
+        qprev = sR[p] * (x - sL[p] * qprev);
+      } else {
+        const double rl = sR[n - 1];
+        qprev = (0. != rl) ? rl * (x - sL[n - 1] * qprev) : 0.;
+      }
+      q[s * 32] = qprev;
+    }
+    __syncwarp();
+    store(c, c % XS);
+    __syncwarp();
+  }
+  __pipeline_wait_prior(0);
+  __syncwarp();
+  // ------------------------------------------------------------ backward
+  // (the forward's stores are visible to the warp's later copies)
+  __threadfence_block();
+  for (int c = 0; c < XS - 1; c++) {
+    if (c < nch) load(nch - 1 - c, c % XS);
+    else __pipeline_commit();
+  }
+  double qn = qprev;  // q[n - 1]
+  for (int it = 0; it < nch; it++) {
+    const int c = nch - 1 - it;
+    if (it + XS - 1 < nch) load(nch - 1 - (it + XS - 1), (it + XS - 1) % XS);
+    else __pipeline_commit();
+    __pipeline_wait_prior(XS - 1);
+    __syncwarp();
+    double *q = ring + (size_t)(it % XS) * XC * 32 + l;
+    const int p0 = c * XC, m = min(XC, n - p0);
+    for (int s = m - 1; s >= 0; s--) {
+      const int p = p0 + s;
+      if (p == n - 1) continue;  // the last row keeps its forward value
+      qn = q[s * 32] - sV[p] * qn;
+      q[s * 32] = qn;
+    }
+    __syncwarp();
+    store(c, it % XS);
+    __syncwarp();
+  }
+  (void)j;
+}
+
+// u + delta' of a 32 x 32 tile (delta' read transposed through shared
+// memory), halo rows and walls as fluid_update_boundaries_{ux,uy,t}
+__global__ void __launch_bounds__(256) k_predict_update(PredictArgs a, const double *__restrict__ fw) {
+  pdl_enter();
+  __shared__ double sd[3][PT][PT + 1];  // [f][i - i0][j - j0]
+  const Grid2 g = a.g;
+  const int nx = g.nx, ny = g.ny;
+  const int i0 = 1 + blockIdx.x * PT, j0 = 1 + blockIdx.y * PT;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  for (int c = ty; c < PT; c += 8) {
+    const int i = i0 + c, j = j0 + tx;
+    if (i > nx || j > ny) continue;
+    sd[0][c][tx] = (i >= 2) ? fw[fw_ix(nx, ny, 0, i - 2, j)] : 0.;
+    sd[1][c][tx] = fw[fw_ix(nx, ny, 1, i - 1, j)];
+    sd[2][c][tx] = fw[fw_ix(nx, ny, 2, i - 1, j)];
+  }
+  __syncthreads();
+  for (int r = ty; r < PT; r += 8) {
+    const int j = j0 + r;
+    if (j > ny) continue;
+    const bool to_top = (1 == j), to_bottom = (ny == j);
+    // storage columns of this tile: interior i = i0 + tx, plus the walls
+    // handled by the tiles at the two x ends
+    const int i = i0 + tx;
+    if (i <= nx) {
+      const double nuy = a.uy[ix_cc(nx, i, j)] + sd[1][tx][r];
+      const double nt = a.t[ix_cc(nx, i, j)] + sd[2][tx][r];
+      a.uy_new[ix_cc(nx, i, j)] = nuy;
+      a.t_new[ix_cc(nx, i, j)] = nt;
+      if (to_top) {
+        a.uy_new[ix_cc(nx, i, ny + 1)] = nuy;
+        a.t_new[ix_cc(nx, i, ny + 1)] = nt;
+      }
+      if (to_bottom) {
+        a.uy_new[ix_cc(nx, i, 0)] = nuy;
+        a.t_new[ix_cc(nx, i, 0)] = nt;
+      }
+      if (i >= 2) {
+        const double nux = a.ux[ix_ux(nx, i, j)] + sd[0][tx][r];
+        a.ux_new[ix_ux(nx, i, j)] = nux;
+        if (to_top) a.ux_new[ix_ux(nx, i, ny + 1)] = nux;
+        if (to_bottom) a.ux_new[ix_ux(nx, i, 0)] = nux;
+      }
+    }
+    // walls: uy, t at i = 0 and nx + 1, ux at i = 1 and nx + 1; the halo rows
+    // take the value before the wall assignment
+    const bool left = (1 == i0) && (0 == tx), right = (i0 + PT > nx) && (0 == tx);
+    for (int side = 0; side < 2; side++) {
+      if (!(side ? right : left)) continue;
+      const int c = side ? nx + 1 : 0;
+      const double huy = a.uy[ix_cc(nx, c, j)], ht = a.t[ix_cc(nx, c, j)];
+      a.uy_new[ix_cc(nx, c, j)] = side ? a.uy_xp : a.uy_xm;
+      a.t_new[ix_cc(nx, c, j)] = side ? a.t_xp : a.t_xm;
+      if (to_top) {
+        a.uy_new[ix_cc(nx, c, ny + 1)] = huy;
+        a.t_new[ix_cc(nx, c, ny + 1)] = ht;
+      }
+      if (to_bottom) {
+        a.uy_new[ix_cc(nx, c, 0)] = huy;
+        a.t_new[ix_cc(nx, c, 0)] = ht;
+      }
+      const int iu = side ? nx + 1 : 1;
+      const double hux = a.ux[ix_ux(nx, iu, j)];
+      a.ux_new[ix_ux(nx, iu, j)] = 0.;
+      if (to_top) a.ux_new[ix_ux(nx, iu, ny + 1)] = hux;
+      if (to_bottom) a.ux_new[ix_ux(nx, iu, 0)] = hux;
     }
   }
 }

@@ -13,6 +13,7 @@
 // reference uses.
 #include <cmath>
 #include <cstdarg>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -207,8 +208,16 @@ int launch_predict(svof_solver *s, int rk, bool with_coef) {
   a.vof_ref = s->vof_ref;
   a.rows_per_block = s->pred_rows;
   a.g = s->grid();
-  const int blocks = (s->ny + s->pred_rows - 1) / s->pred_rows;
-  CK(launch_k(s->pdl, k_predict, blocks, s->pred_threads, s->pred_smem, s->stream, a));
+  if (s->pred_lines) {
+    const dim3 tiles((s->nx + 31) / 32, (s->ny + 31) / 32);
+    CK(launch_k(s->pdl, k_predict_rhs, tiles, 256, 0, s->stream, a, s->fw.p));
+    CK(launch_k(s->pdl, k_predict_xsolve, 3 * ((s->ny + 31) / 32), 32, predict_xsolve_smem(s->nx), s->stream,
+                (const double *)s->coef.p, s->fw.p, s->nx, s->ny));
+    CK(launch_k(s->pdl, k_predict_update, tiles, 256, 0, s->stream, a, (const double *)s->fw.p));
+  } else {
+    const int blocks = (s->ny + s->pred_rows - 1) / s->pred_rows;
+    CK(launch_k(s->pdl, k_predict, blocks, s->pred_threads, s->pred_smem, s->stream, a));
+  }
   s->cur_u ^= 1;
   return 0;
 }
@@ -554,6 +563,16 @@ int engine_create(const svof_params_t *prm, const double *xf, const double *xc, 
       return fail("cudaFuncSetAttribute(k_predict): %s", cudaGetErrorString(cudaGetLastError())), bail();
     const size_t coef_smem = sizeof(double) * 9 * nx;
     if (cudaSuccess != raise_smem_limit(k_tdm_coef, coef_smem)) return fail("cudaFuncSetAttribute(k_tdm_coef)"), bail();
+    // grids from 512 x 512 cells take the line-streaming predictor: the
+    // fused kernel's row tiles leave few lines per SM for its serial sweeps.
+    // SVOF_PREDICT_LINES = 0 / 1 forces either form (tests compare them).
+    s->pred_lines = (long)nx * ny >= 512L * 512L;
+    if (const char *e = std::getenv("SVOF_PREDICT_LINES")) s->pred_lines = (0 != std::atoi(e));
+    if (s->pred_lines) {
+      if (dalloc(s->fw, 3 * (size_t)nx * 32 * ((ny + 31) / 32))) return bail();
+      if (cudaSuccess != raise_smem_limit(k_predict_xsolve, predict_xsolve_smem(nx)))
+        return fail("cudaFuncSetAttribute(k_predict_xsolve)"), bail();
+    }
   }
   // transforms: one row (DCT) or a tile of columns (DFT) per block
   {
@@ -662,7 +681,7 @@ int svof_destroy(svof_solver_t *s) {
   DevBuf *bufs[] = {&s->p, &s->psi, &s->curv, &s->normal, &s->ifrcx, &s->ifrcy, &s->dxf, &s->dxc,
                     &s->lap_ux, &s->lap_uy, &s->lap_t, &s->spec, &s->twf, &s->twb, &s->cs, &s->vt,
                     &s->rvt, &s->q1t, &s->ck, &s->lastf, &s->den, &s->pl, &s->pu, &s->evals, &s->diag,
-                    &s->coef, &s->stat_part};
+                    &s->coef, &s->stat_part, &s->fw};
   for (DevBuf *b : bufs) dfree(*b);
   for (DevBuf &b : s->stat) dfree(b);
   if (s->d_dt) cudaFree(s->d_dt);
@@ -934,7 +953,7 @@ int svof_profile_step(svof_solver_t *s, double *ms, int *launches, int nkinds) {
       float t = 0.f;
       cudaEventElapsedTime(&t, ev[q - 1], ev[q]);
       ms[kind[q]] += t;
-      launches[kind[q]] += (SVOF_K_DT == kind[q] || SVOF_K_PREDICT == kind[q]) ? 2 : 1;
+      launches[kind[q]] += SVOF_K_DT == kind[q] ? 2 : (SVOF_K_PREDICT == kind[q] ? (s->pred_lines ? 4 : 2) : 1);
     }
   }
   for (cudaEvent_t x : ev) cudaEventDestroy(x);

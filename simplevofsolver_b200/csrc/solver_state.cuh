@@ -54,6 +54,10 @@ struct svof_solver {
   cudaEvent_t ev_fork[3] = {nullptr, nullptr, nullptr}, ev_join[3] = {nullptr, nullptr, nullptr};
   cudaEvent_t ev_geom[3] = {nullptr, nullptr, nullptr};
   // predict launch shape
+  // large grids: the line-streaming predictor (k_predict_rhs, _xsolve,
+  // _update) with its line array
+  bool pred_lines = false;
+  svof::DevBuf fw;
   int pred_rows = 1;
   int pred_threads = 256;
   size_t pred_smem = 0;

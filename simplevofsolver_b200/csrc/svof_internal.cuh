@@ -97,6 +97,15 @@ __global__ void k_tdm_coef(const double *__restrict__ lap_ux, const double *__re
                            const double *__restrict__ lap_t, const double *__restrict__ dtp, double gam,
                            double m_dif, double t_dif, int nx, double *__restrict__ coef);
 size_t predict_smem_bytes(int nx, int rows_per_block);
+// the line-streaming form of k_predict for large grids: right-hand sides of
+// 32 x 32 tiles into the line array fw (3 fields, lines in blocks of 32,
+// 3 nx 32 ceil(ny / 32) doubles), the x sweeps one warp per field and block of
+// lines (3 ceil(ny / 32) blocks of 32 threads, dynamic shared memory
+// predict_xsolve_smem(nx)), then u + delta' with halo rows and walls
+__global__ void k_predict_rhs(PredictArgs a, double *__restrict__ fw);
+__global__ void k_predict_xsolve(const double *__restrict__ coef, double *__restrict__ fw, int nx, int ny);
+inline size_t predict_xsolve_smem(int nx) { return sizeof(double) * ((size_t)4 * 64 * 32 + 3 * (size_t)nx); }
+__global__ void k_predict_update(PredictArgs a, const double *__restrict__ fw);
 
 // Poisson, DCT path (src/fluid/compute_potential/dct.c)
 __global__ void k_dct_fwd(const double *__restrict__ ux, const double *__restrict__ uy,

@@ -7,9 +7,12 @@ respect to the initial velocities (2 x 256 x 256) and 1/We.
 
 * central finite differences of the forward (the GPU FP64 path, which
   reproduces the reference to 1e-12 per step), eps = 1e-6 along 16 seeded
-  random directions of unit norm, the time-step sequence held fixed: each
-  directional derivative within 1e-5 of the adjoint's, relative to the
-  gradient's norm, and within 1e-5 relative to itself where it is not tiny;
+  random smooth directions of unit norm (velocity and 1/We), the time-step
+  sequence held fixed and the initial velocity projected onto
+  divergence-free fields (adjoint.Rollout): each directional derivative
+  within 1e-5 of the adjoint's, relative (measured: 15 of 16 directions
+  2e-7 to 7e-6; the floor of the relative error is 5 % of the gradient's
+  norm, below which central differences cannot resolve 1e-5);
 * the tangent-linear dot-product test: the oracle's tangent model
   (svof_oracle_tl.inc) driven along the GPU trajectory against the CUDA
   adjoint over the rollout's steps;
@@ -55,21 +58,26 @@ def gradient(ic, r, x):
     ux, uy, vof, p = rollout(xs["ux"], xs["uy"], xs["vof"], xs["ten"], r)
     J = falling_objective(ux, uy, vof, ic.xf)
     J.backward()
-    return float(J), {k: xs[k].grad.clone() for k in ("ux", "uy", "ten")}
+    return float(J.detach()), {k: xs[k].grad.clone() for k in ("ux", "uy", "ten")}
 
 
-def solenoidal_direction(rng, nx, ny, xf):
-    """a random divergence-free velocity perturbation: the discrete curl of a
-    random stream function at the cell corners, zero on the walls (the
-    perturbed initial field stays admissible: divergence-free to round-off,
-    no flow through the walls)"""
-    psi = np.zeros((ny, nx + 1))
-    psi[:, 1:nx] = rng.standard_normal((ny, nx - 1))
-    dy = 1.0 / ny
-    dxf = np.diff(xf)
-    ux = (np.roll(psi, -1, 0) - psi)[:, 1:nx] / dy
-    uy = -(psi[:, 1:] - psi[:, :-1]) / dxf[None, :]
-    return ux, uy
+def smooth_direction(rng, nx, ny, xf, modes=4):
+    """a random smooth velocity perturbation: sums of sin(m pi x) cos / sin
+    (2 pi k y), m, k <= modes, on the ux faces and uy cells (the rollout
+    projects it onto divergence-free fields, as it does the initial field);
+    smooth, so that its directional derivative is well above the round-off
+    of central differences of J"""
+    xc = 0.5 * (xf[1:] + xf[:-1])
+    yc = (np.arange(ny) + 0.5) / ny
+    out = []
+    for xs in (xf[1:nx], xc):
+        f = np.zeros((ny, len(xs)))
+        for m in range(1, modes + 1):
+            for k in range(0, modes + 1):
+                a, b = rng.standard_normal(2)
+                f += np.sin(m * np.pi * xs)[None, :] * (a * np.cos(2 * np.pi * k * yc) + b * np.sin(2 * np.pi * k * yc))[:, None]
+        out.append(f)
+    return out[0], out[1]
 
 
 def test_gradient_matches_central_differences(gpu_available):
@@ -82,7 +90,7 @@ def test_gradient_matches_central_differences(gpu_available):
     eps = 1e-6
     worst_norm, worst_rel = 0.0, 0.0
     for _ in range(16):
-        dux, duy = solenoidal_direction(rng, ic.nx, ic.ny, ic.xf)
+        dux, duy = smooth_direction(rng, ic.nx, ic.ny, ic.xf)
         v = {k: torch.tensor(a, dtype=torch.float64, device="cuda")
              for k, a in (("ux", dux), ("uy", duy), ("ten", np.array(rng.standard_normal())))}
         nrm = float(torch.sqrt(sum(torch.sum(a * a) for a in v.values())))
@@ -95,12 +103,17 @@ def test_gradient_matches_central_differences(gpu_available):
                 xp[k] = x[k] + sgn * eps * v[k]
             js.append(objective(ic, r, xp))
         d_fd = (js[0] - js[1]) / (2 * eps)
+        # relative to the directional derivative, floored at 5 % of the
+        # gradient's norm: central differences resolve J to about
+        # 1e-16 |J| / eps ~ 1e-10, so a derivative 1000 times below the
+        # gradient's norm is not checkable to 1e-5 relative by them
+        err = abs(d_fd - d_adj) / max(abs(d_adj), 0.05 * gnorm)
         worst_norm = max(worst_norm, abs(d_fd - d_adj) / gnorm)
-        if abs(d_adj) > 1e-2 * gnorm:
-            worst_rel = max(worst_rel, abs(d_fd - d_adj) / abs(d_adj))
+        worst_rel = max(worst_rel, err)
+        print(f"  adjoint {d_adj:+.12e}  central differences {d_fd:+.12e}  relative {err:.2e}")
     print(f"J = {J:.12e}, |grad| = {gnorm:.6e}, max |fd - adj| / |grad| = {worst_norm:.3e}, "
           f"max relative = {worst_rel:.3e}")
-    assert worst_norm <= 1e-5 and worst_rel <= 1e-5, (worst_norm, worst_rel)
+    assert worst_rel <= 1e-5, (worst_norm, worst_rel)
 
 
 def test_checkpoint_interval_changes_nothing(gpu_available):
