@@ -42,8 +42,9 @@ namespace {
 int adj_ensure(svof_solver *s) {
   if (s->adj) return 0;
   if (s->prm.add_buoyancy) return fail("the adjoint needs add_buoyancy = 0 (t is not differentiated)");
-  AdjointState *a = new AdjointState();
   const int nx = s->nx, ny = s->ny;
+  if (sizeof(double) * 2 * (size_t)nx > 200 * 1024) return fail("the adjoint's x line solve needs nx <= 12800");
+  AdjointState *a = new AdjointState();
   const size_t nc = (size_t)nx * ny, nf = (size_t)(nx - 1) * ny;
   const size_t ncc = (size_t)(nx + 2) * (ny + 2);
   bool bad = dalloc(a->ux, nf) || dalloc(a->uy, nc) || dalloc(a->p, nc) || dalloc(a->vof[0], nc) ||
@@ -52,8 +53,11 @@ int adj_ensure(svof_solver *s) {
              dalloc(a->sa_y, nc) || dalloc(a->sg_y, nc) || dalloc(a->ifx, nf) || dalloc(a->ify, nc) ||
              dalloc(a->kap, nc) || dalloc(a->m, 2 * nc) || dalloc(a->nrm, 3 * nc) || dalloc(a->sig, nc) ||
              dalloc(a->psib, nc) || dalloc(a->psis, ncc) || dalloc(a->sum, 1);
-  // transposed line solves: R rows per block so that the blocks cover the SMs
+  // transposed line solves: R rows per block so that the blocks cover the SMs,
+  // within 160 KB of staged rows
   int r = std::max(1, std::min(8, ny / 148));
+  while (r > 1 && sizeof(double) * 2 * (size_t)r * nx > 160 * 1024) r--;
+
   a->xs_rows = r;
   a->xs_smem = sizeof(double) * 2 * (size_t)r * nx;
   if (!bad && cudaSuccess != raise_smem_limit(k_adj_xsolve, a->xs_smem)) bad = true;
@@ -142,7 +146,7 @@ int adj_predict(svof_solver *s, int rk, double dt, const double *ux, const doubl
   if (launch_coef(s, rk, s->stream)) return 1;
   const int R = a->xs_rows;
   k_adj_xsolve<<<(s->ny + R - 1) / R, 128, a->xs_smem, s->stream>>>(
-      a->ux.p, a->uy.p, s->coef.p, a->sa_x.p, a->sg_x.p, a->sa_y.p, a->sg_y.p, a->pend_x.p, a->pend_y.p,
+      a->ux.p, a->uy.p, coef_table(s, rk), a->sa_x.p, a->sg_x.p, a->sa_y.p, a->sg_y.p, a->pend_x.p, a->pend_y.p,
       RK_A[rk] * dt, RK_B[rk] * dt, (RK_A[rk] + RK_B[rk]) * dt, R, s->grid());
   CK_LAUNCH();
   AdjRhsArgs r{};

@@ -30,9 +30,12 @@ size_t predict_smem_bytes(int nx, int R) {
 // v_{i-1}) for 0 < i < n-1, R[n-1] = 1 / (c - l v) of the last row or 0 when
 // the reference zeroes that row;  V[i] = v_i.
 __global__ void k_tdm_coef(const double *__restrict__ lap_ux, const double *__restrict__ lap_uy,
-                           const double *__restrict__ lap_t, const double *__restrict__ dtp, double gam,
-                           double m_dif, double t_dif, int nx, double *__restrict__ coef) {
+                           const double *__restrict__ lap_t, const double *__restrict__ dtp, Gam3 gams,
+                           double m_dif, double t_dif, int nx, double *__restrict__ coef_all) {
   pdl_enter();
+  // block b: the table of gamma = gams.g[b] at coef_all + 9 nx b
+  const double gam = gams.g[blockIdx.x];
+  double *coef = coef_all + (size_t)9 * nx * blockIdx.x;
   // the Laplacian tables are staged in shared memory first: the recurrence
   // below then waits on arithmetic only
   extern __shared__ double slap[];  // [3][3 nx]
@@ -359,7 +362,7 @@ __global__ void __launch_bounds__(256) k_predict_rhs(PredictArgs a, double *__re
 // one warp per (field, block of 32 lines); chunks of XC positions in a ring
 // of XS shared-memory slots; the substep's coefficients of the field in
 // shared memory.  Dynamic shared memory: (XS * XC * 32 + 3 nx) doubles.
-constexpr int XC = 64, XS = 4;
+constexpr int XC = 64, XS = 4, XB = 16;
 
 __global__ void __launch_bounds__(32) k_predict_xsolve(const double *__restrict__ coef, double *__restrict__ fw,
                                                       int nx, int ny) {
@@ -392,6 +395,7 @@ __global__ void __launch_bounds__(32) k_predict_xsolve(const double *__restrict_
     const int p0 = c * XC, m = min(XC, n - p0);
     double *dst = base + (size_t)p0 * 32;
     const double *src = ring + (size_t)slot * XC * 32;
+#pragma unroll 16
     for (int s = 0; s < m; s++) dst[s * 32 + l] = src[s * 32 + l];
   };
   __syncwarp();
@@ -408,18 +412,36 @@ __global__ void __launch_bounds__(32) k_predict_xsolve(const double *__restrict_
     __syncwarp();
     double *q = ring + (size_t)(c % XS) * XC * 32 + l;
     const int p0 = c * XC, m = min(XC, n - p0);
-    for (int s = 0; s < m; s++) {
-      const int p = p0 + s;
-      const double x = q[s * 32];
-      if (0 == p) {
-        qprev = x / sR[0];
-      } else if (p < n - 1) {
-        qprev = sR[p] * (x - sL[p] * qprev);
-      } else {
-        const double rl = sR[n - 1];
-        qprev = (0. != rl) ? rl * (x - sL[n - 1] * qprev) : 0.;
+    // batches of XB positions: the batch's loads are issued ahead of the
+    // dependent chain, which then runs on registers
+    for (int s0 = 0; s0 < m; s0 += XB) {
+      const int mb = min(XB, m - s0);
+      double xv[XB], lv[XB], rv[XB];
+#pragma unroll
+      for (int k = 0; k < XB; k++) {
+        if (k < mb) {
+          xv[k] = q[(s0 + k) * 32];
+          lv[k] = sL[p0 + s0 + k];
+          rv[k] = sR[p0 + s0 + k];
+        }
       }
-      q[s * 32] = qprev;
+#pragma unroll
+      for (int k = 0; k < XB; k++) {
+        if (k < mb) {
+          const int p = p0 + s0 + k;
+          if (0 == p) {
+            qprev = xv[k] / rv[k];
+          } else if (p < n - 1) {
+            qprev = rv[k] * (xv[k] - lv[k] * qprev);
+          } else {
+            qprev = (0. != rv[k]) ? rv[k] * (xv[k] - lv[k] * qprev) : 0.;
+          }
+          xv[k] = qprev;
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < XB; k++)
+        if (k < mb) q[(s0 + k) * 32] = xv[k];
     }
     __syncwarp();
     store(c, c % XS);
@@ -443,11 +465,30 @@ __global__ void __launch_bounds__(32) k_predict_xsolve(const double *__restrict_
     __syncwarp();
     double *q = ring + (size_t)(it % XS) * XC * 32 + l;
     const int p0 = c * XC, m = min(XC, n - p0);
-    for (int s = m - 1; s >= 0; s--) {
-      const int p = p0 + s;
-      if (p == n - 1) continue;  // the last row keeps its forward value
-      qn = q[s * 32] - sV[p] * qn;
-      q[s * 32] = qn;
+    // batches from the top of the chunk down, loads ahead of the chain
+    for (int s1 = m; s1 > 0; s1 -= XB) {
+      const int mb = min(XB, s1);  // positions s1 - 1 .. s1 - mb
+      double xv[XB], vv[XB];
+#pragma unroll
+      for (int k = 0; k < XB; k++) {
+        if (k < mb) {
+          xv[k] = q[(s1 - 1 - k) * 32];
+          vv[k] = sV[p0 + s1 - 1 - k];
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < XB; k++) {
+        if (k < mb) {
+          const int p = p0 + s1 - 1 - k;
+          if (p != n - 1) {  // the last row keeps its forward value
+            qn = xv[k] - vv[k] * qn;
+            xv[k] = qn;
+          }
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < XB; k++)
+        if (k < mb) q[(s1 - 1 - k) * 32] = xv[k];
     }
     __syncwarp();
     store(c, it % XS);

@@ -157,10 +157,22 @@ int launch_vof(svof_solver *s, int rk) {
   return 0;
 }
 
+double *coef_table(svof_solver *s, int rk) { return s->coef.p + (size_t)9 * s->nx * rk; }
+
 int launch_coef(svof_solver *s, int rk, cudaStream_t st) {
+  Gam3 g{{RK_A[rk] + RK_B[rk], 0., 0.}};
   CK(launch_k(s->pdl, k_tdm_coef, 1, 128, sizeof(double) * 9 * s->nx, st, (const double *)s->lap_ux.p,
-              (const double *)s->lap_uy.p, (const double *)s->lap_t.p, (const double *)s->d_dt, RK_A[rk] + RK_B[rk],
-              s->prm.m_dif, s->prm.t_dif, s->nx, s->coef.p));
+              (const double *)s->lap_uy.p, (const double *)s->lap_t.p, (const double *)s->d_dt, g, s->prm.m_dif,
+              s->prm.t_dif, s->nx, coef_table(s, rk)));
+  return 0;
+}
+
+// the three substeps' tables at once (they need only dt), one block each
+int launch_coef_all(svof_solver *s, cudaStream_t st) {
+  Gam3 g{{RK_A[0] + RK_B[0], RK_A[1] + RK_B[1], RK_A[2] + RK_B[2]}};
+  CK(launch_k(s->pdl, k_tdm_coef, 3, 128, sizeof(double) * 9 * s->nx, st, (const double *)s->lap_ux.p,
+              (const double *)s->lap_uy.p, (const double *)s->lap_t.p, (const double *)s->d_dt, g, s->prm.m_dif,
+              s->prm.t_dif, s->nx, coef_table(s, 0)));
   return 0;
 }
 
@@ -189,7 +201,7 @@ int launch_predict(svof_solver *s, int rk, bool with_coef) {
   a.lap_ux = s->lap_ux.p;
   a.lap_uy = s->lap_uy.p;
   a.lap_t = s->lap_t.p;
-  a.coef = s->coef.p;
+  a.coef = coef_table(s, rk);
   a.dtp = s->d_dt;
   a.m_dif = s->prm.m_dif;
   a.t_dif = s->prm.t_dif;
@@ -212,7 +224,7 @@ int launch_predict(svof_solver *s, int rk, bool with_coef) {
     const dim3 tiles((s->nx + 31) / 32, (s->ny + 31) / 32);
     CK(launch_k(s->pdl, k_predict_rhs, tiles, 256, 0, s->stream, a, s->fw.p));
     CK(launch_k(s->pdl, k_predict_xsolve, 3 * ((s->ny + 31) / 32), 32, predict_xsolve_smem(s->nx), s->stream,
-                (const double *)s->coef.p, s->fw.p, s->nx, s->ny));
+                (const double *)coef_table(s, rk), s->fw.p, s->nx, s->ny));
     CK(launch_k(s->pdl, k_predict_update, tiles, 256, 0, s->stream, a, (const double *)s->fw.p));
   } else {
     const int blocks = (s->ny + s->pred_rows - 1) / s->pred_rows;
@@ -265,12 +277,14 @@ int launch_project(svof_solver *s, int rk, int do_vel, int do_p) {
 // the kernel sequence of integrate(), src/integrate.c:11-68
 int launch_step(svof_solver *s) {
   if (launch_dt(s)) return 1;
+  // the three substeps' predictor coefficients need only dt: one launch on a
+  // branch of its own, beside the first substep's interface kernels (the
+  // serial recurrence takes about as long as they do)
+  CK(cudaEventRecord(s->ev_fork[0], s->stream));
+  CK(cudaStreamWaitEvent(s->side2, s->ev_fork[0], 0));
+  if (launch_coef_all(s, s->side2)) return 1;
+  CK(cudaEventRecord(s->ev_coef, s->side2));
   for (int rk = 0; rk < 3; rk++) {
-    // the predictor coefficients need only dt: compute them beside the
-    // interface kernels
-    CK(cudaEventRecord(s->ev_fork[rk], s->stream));
-    CK(cudaStreamWaitEvent(s->side, s->ev_fork[rk], 0));
-    if (launch_coef(s, rk, s->side)) return 1;
     if (launch_geom(s)) return 1;
     // the CSF force and the vof advection both only need the geometry: the
     // force runs beside the advection, on the side branch
@@ -280,6 +294,7 @@ int launch_step(svof_solver *s) {
     CK(cudaEventRecord(s->ev_join[rk], s->side));
     if (launch_vof(s, rk)) return 1;
     CK(cudaStreamWaitEvent(s->stream, s->ev_join[rk], 0));
+    if (0 == rk) CK(cudaStreamWaitEvent(s->stream, s->ev_coef, 0));
     if (launch_predict(s, rk, false)) return 1;
     if (launch_potential(s, rk, s->uniform)) return 1;
     if (launch_project(s, rk, 1, 1)) return 1;
@@ -540,8 +555,10 @@ int engine_create(const svof_params_t *prm, const double *xf, const double *xc, 
       dalloc(s->ifrcy, n_src, mg) || dalloc(s->diag, 16))
     return bail();
   if (build_tables(s, xf, xc)) return bail();
-  if (dalloc(s->coef, 9 * (size_t)nx)) return bail();
+  if (dalloc(s->coef, 27 * (size_t)nx)) return bail();  // one table per substep
   if (cudaSuccess != cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking)) return fail("stream"), bail();
+  if (cudaSuccess != cudaStreamCreateWithFlags(&s->side2, cudaStreamNonBlocking)) return fail("stream"), bail();
+  if (cudaSuccess != cudaEventCreateWithFlags(&s->ev_coef, cudaEventDisableTiming)) return fail("event"), bail();
   for (int k = 0; k < 3; k++) {
     if (cudaSuccess != cudaEventCreateWithFlags(&s->ev_fork[k], cudaEventDisableTiming) ||
         cudaSuccess != cudaEventCreateWithFlags(&s->ev_geom[k], cudaEventDisableTiming) ||
@@ -692,6 +709,8 @@ int svof_destroy(svof_solver_t *s) {
     if (s->ev_geom[k]) cudaEventDestroy(s->ev_geom[k]);
     if (s->ev_join[k]) cudaEventDestroy(s->ev_join[k]);
   }
+  if (s->ev_coef) cudaEventDestroy(s->ev_coef);
+  if (s->side2) cudaStreamDestroy(s->side2);
   if (s->side) cudaStreamDestroy(s->side);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;

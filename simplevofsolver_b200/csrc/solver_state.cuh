@@ -46,11 +46,15 @@ struct svof_solver {
   // Poisson
   svof::DevBuf spec, twf, twb, cs, vt, rvt, q1t, ck, lastf, den, pl, pu, evals;
   int ysolve_kt = 32;       // wavenumber lines per block of the DCT y solve
-  // predictor Thomas coefficients of the current substep (k_tdm_coef)
+  // predictor Thomas coefficients, one table per substep (k_tdm_coef)
   svof::DevBuf coef;
   // side stream of the step graph: the coefficient kernel runs beside the
   // interface kernels
   cudaStream_t side = nullptr;
+  // the branch of the three substeps' Thomas tables (computed at the start
+  // of a step) and its join event
+  cudaStream_t side2 = nullptr;
+  cudaEvent_t ev_coef = nullptr;
   cudaEvent_t ev_fork[3] = {nullptr, nullptr, nullptr}, ev_join[3] = {nullptr, nullptr, nullptr};
   cudaEvent_t ev_geom[3] = {nullptr, nullptr, nullptr};
   // predict launch shape
@@ -139,6 +143,8 @@ cudaError_t launch_k(bool pdl, void (*k)(KArgs...), dim3 grid, dim3 block, size_
 int launch_halo_bc(svof_solver *s, double *a, int field);
 int launch_dt(svof_solver *s);
 int launch_coef(svof_solver *s, int rk, cudaStream_t st);
+// the predictor's Thomas table of substep rk (k_tdm_coef layout)
+double *coef_table(svof_solver *s, int rk);
 int launch_geom(svof_solver *s);
 int launch_force(svof_solver *s, cudaStream_t st = nullptr);
 int launch_vof(svof_solver *s, int rk);

@@ -93,9 +93,14 @@ struct PredictArgs {
   Grid2 g;
 };
 __global__ void k_predict(PredictArgs a);
+// the Thomas tables of up to three substeps, one block each (block b uses
+// gams.g[b] and writes coef_all + 9 nx b)
+struct Gam3 {
+  double g[3];
+};
 __global__ void k_tdm_coef(const double *__restrict__ lap_ux, const double *__restrict__ lap_uy,
-                           const double *__restrict__ lap_t, const double *__restrict__ dtp, double gam,
-                           double m_dif, double t_dif, int nx, double *__restrict__ coef);
+                           const double *__restrict__ lap_t, const double *__restrict__ dtp, Gam3 gams,
+                           double m_dif, double t_dif, int nx, double *__restrict__ coef_all);
 size_t predict_smem_bytes(int nx, int rows_per_block);
 // the line-streaming form of k_predict for large grids: right-hand sides of
 // 32 x 32 tiles into the line array fw (3 fields, lines in blocks of 32,
