@@ -62,7 +62,7 @@ int adj_ensure(svof_solver *s) {
   a->xs_smem = sizeof(double) * 2 * (size_t)r * nx;
   if (!bad && cudaSuccess != raise_smem_limit(k_adj_xsolve, a->xs_smem)) bad = true;
   // the forward transforms on an array right-hand side share the forward's shapes
-  if (!bad && s->uniform && cudaSuccess != raise_smem_limit(k_dct_fwd_rhs, sizeof(double) * 2 * nx)) bad = true;
+  if (!bad && s->uniform && cudaSuccess != raise_smem_limit(k_dct_fwd_rhs, dct_row_smem(nx))) bad = true;
   if (!bad && !s->uniform &&
       cudaSuccess != raise_smem_limit(k_dft_fwd_rhs, sizeof(double) * 2 * (size_t)ny * s->dft_cols))
     bad = true;
@@ -108,7 +108,7 @@ int adj_potential(svof_solver *s, int rk, double dt) {
   double pre_p;
   if (s->uniform) {
     const int nthr = std::min(256, std::max(32, s->nx / 2));
-    const size_t smem = sizeof(double) * 2 * s->nx;
+    const size_t smem = dct_row_smem(s->nx);
     k_dct_fwd_rhs<<<s->ny, nthr, smem, s->stream>>>(a->psib.p, s->spec.p, s->twf.p, s->cs.p, s->log2fft, g);
     CK_LAUNCH();
     const int kt = s->ysolve_kt;

@@ -66,16 +66,23 @@ struct ArrayRhs {
 template <class Rhs>
 __device__ __forceinline__ void dct_fwd_row(const Rhs &rhs, double *__restrict__ spec, const double *__restrict__ tw,
                                             const double *__restrict__ cs, int log2n, int n, int j) {
-  extern __shared__ double z[];
+  extern __shared__ double z[];  // [2n] transform, [n] right-hand side, [n] twiddles (n/2 pairs)
+  double *r = z + 2 * n, *stw = r + n;
+  // the row's right-hand side and the twiddles, read in order (coalesced)
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    r[i] = rhs(i + 1, j);
+    stw[i] = tw[i];
+  }
+  __syncthreads();
   // Makhoul reordering v_m = x_{2m}, v_{n-1-m} = x_{2m+1}, stored bit-reversed
   for (int q = threadIdx.x; q < n; q += blockDim.x) {
     const int m = bitrev(q, log2n);
     const int src = (m < n / 2) ? 2 * m : 2 * (n - 1 - m) + 1;
-    z[2 * q] = rhs(src + 1, j);
+    z[2 * q] = r[src];
     z[2 * q + 1] = 0.;
   }
   __syncthreads();
-  fft_stages(z, log2n, 1, tw);
+  fft_stages(z, log2n, 1, stw);
   double *out = spec + (size_t)(j - 1) * n;
   for (int k = threadIdx.x; k < n; k += blockDim.x) {
     const double c = cs[2 * k], s = cs[2 * k + 1];
@@ -181,16 +188,23 @@ __global__ void k_dct_inv(const double *__restrict__ spec, double *__restrict__ 
                           const double *__restrict__ tw, const double *__restrict__ cs,
                           int log2n, Grid2 g) {
   pdl_enter();
-  extern __shared__ double z[];
+  extern __shared__ double z[];  // [2n] transform, [n] spectrum row, [n] twiddles (n/2 pairs)
   const int n = g.nx, nx = g.nx, ny = g.ny;
   const int j = 1 + blockIdx.x;
-  const double *in = spec + (size_t)(j - 1) * n;
+  double *in = z + 2 * n, *stw = in + n;
   // old wall values of the rows that feed the halo (read before any write)
   double wl = 0., wr = 0.;
   if (0 == threadIdx.x && (1 == j || ny == j)) {
     wl = psi[ix_cc(nx, 0, j)];
     wr = psi[ix_cc(nx, nx + 1, j)];
   }
+  // the spectrum row and the twiddles, read in order (coalesced)
+  const double *row = spec + (size_t)(j - 1) * n;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    in[i] = row[i];
+    stw[i] = tw[i];
+  }
+  __syncthreads();
   for (int q = threadIdx.x; q < n; q += blockDim.x) {
     const int m = bitrev(q, log2n);
     const double a = in[m];
@@ -200,7 +214,7 @@ __global__ void k_dct_inv(const double *__restrict__ spec, double *__restrict__ 
     z[2 * q + 1] = s * a - c * b;
   }
   __syncthreads();
-  fft_stages(z, log2n, 1, tw);
+  fft_stages(z, log2n, 1, stw);
   for (int o = threadIdx.x; o < n; o += blockDim.x) {
     const double y = (0 == (o & 1)) ? z[2 * (o >> 1)] : z[2 * (n - 1 - (o >> 1))];
     const int i = o + 1;

@@ -373,8 +373,7 @@ __global__ void __launch_bounds__(32) k_predict_xsolve(const double *__restrict_
   double *sR = sL + nx, *sV = sR + nx;
   const int nb = (ny + 31) >> 5;
   const int f = blockIdx.x / nb, jb = blockIdx.x % nb;
-  const int l = threadIdx.x;
-  const int j = 32 * jb + l + 1;
+  const int l = threadIdx.x;  // line 32 jb + l + 1 (lanes past ny sweep zeros)
   const int n = (0 == f) ? nx - 1 : nx;
   for (int w = l; w < nx; w += 32) {
     sL[w] = coef[(size_t)(3 * f + 0) * nx + w];
@@ -494,7 +493,6 @@ __global__ void __launch_bounds__(32) k_predict_xsolve(const double *__restrict_
     store(c, it % XS);
     __syncwarp();
   }
-  (void)j;
 }
 
 // u + delta' of a 32 x 32 tile (delta' read transposed through shared

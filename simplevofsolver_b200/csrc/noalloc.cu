@@ -223,7 +223,7 @@ extern "C" int svof_poisson_dct_noalloc(const svof_params_t *prm, const double *
                                   : rkstep == 1 ? 25. / 60. + -17. / 60. : 45. / 60. + -25. / 60.);
   const Grid2 g{nx, ny, dy, S + kDxf, S + kDxf};
   const int nthr = nx / 2 < 32 ? 32 : (nx / 2 > 256 ? 256 : nx / 2);
-  k_dct_fwd<<<ny, nthr, sizeof(double) * 2 * nx, s>>>(ux, uy, S + kSpec, S + kTwf, S + kCs, S + kDt, gam, log2n,
+  k_dct_fwd<<<ny, nthr, dct_row_smem(nx), s>>>(ux, uy, S + kSpec, S + kTwf, S + kCs, S + kDt, gam, log2n,
                                                       g);
   int kt = 32;
   while (kt > 4 && nx / kt < 148) kt >>= 1;
@@ -234,7 +234,7 @@ extern "C" int svof_poisson_dct_noalloc(const svof_params_t *prm, const double *
   if (cudaSuccess != e) return nfail("shared-memory limit of the y solve", e);
   k_dct_ysolve<<<(nx + kt - 1) / kt, 128, sizeof(double) * 3 * kt * ny, s>>>(
       S + kSpec, S + kVt, S + kRvt, S + kQ1t, S + kCk, S + kLastf, S + kDen, 1. / dy / dy, nx, ny, kt);
-  k_dct_inv<<<ny, nthr, sizeof(double) * 2 * nx, s>>>(S + kSpec, psi, S + kTwb, S + kCs, log2n, g);
+  k_dct_inv<<<ny, nthr, dct_row_smem(nx), s>>>(S + kSpec, psi, S + kTwb, S + kCs, log2n, g);
   e = cudaGetLastError();
   if (cudaSuccess != e) return nfail("kernel launch", e);
   return 0;

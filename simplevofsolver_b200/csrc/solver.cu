@@ -242,7 +242,7 @@ int launch_potential(svof_solver *s, int rk, int want_dct) {
   }
   if (s->uniform) {
     const int nthr = std::min(256, std::max(32, s->nx / 2));
-    const size_t smem = sizeof(double) * 2 * s->nx;
+    const size_t smem = dct_row_smem(s->nx);
     CK(launch_k(s->pdl, k_dct_fwd, s->ny, nthr, smem, s->stream, s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->spec.p,
                 s->twf.p, s->cs.p, s->d_dt, gam, s->log2fft, g));
     const int kt = s->ysolve_kt;
@@ -593,7 +593,7 @@ int engine_create(const svof_params_t *prm, const double *xf, const double *xc, 
   }
   // transforms: one row (DCT) or a tile of columns (DFT) per block
   {
-    const size_t dct_smem = sizeof(double) * 2 * nx;
+    const size_t dct_smem = dct_row_smem(nx);
     if (s->uniform && (cudaSuccess != raise_smem_limit(k_dct_fwd, dct_smem) ||
                        cudaSuccess != raise_smem_limit(k_dct_inv, dct_smem)))
       return fail("cudaFuncSetAttribute(k_dct_fwd, k_dct_inv)"), bail();
@@ -604,7 +604,7 @@ int engine_create(const svof_params_t *prm, const double *xf, const double *xc, 
     if (!s->uniform && (cudaSuccess != raise_smem_limit(k_dft_fwd, dft_smem) ||
                         cudaSuccess != raise_smem_limit(k_dft_inv, dft_smem)))
       return fail("cudaFuncSetAttribute(k_dft_fwd, k_dft_inv)"), bail();
-    if (sizeof(double) * 2 * (size_t)(s->uniform ? nx : ny) > 200 * 1024)
+    if ((s->uniform ? dct_row_smem(nx) : sizeof(double) * 2 * (size_t)ny) > 200 * 1024)
       return fail("svof_create: FFT length too large for one block"), bail();
   }
   // line solves: lines per block so that the blocks cover the SMs, within
@@ -936,7 +936,7 @@ int svof_profile_step(svof_solver_t *s, double *ms, int *launches, int nkinds) {
       const Grid2 g = s->grid();
       if (s->uniform) {
         const int nthr = std::min(256, std::max(32, s->nx / 2));
-        const size_t smem = sizeof(double) * 2 * s->nx;
+        const size_t smem = dct_row_smem(s->nx);
         k_dct_fwd<<<s->ny, nthr, smem, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->spec.p, s->twf.p,
                                                     s->cs.p, s->d_dt, gam, s->log2fft, g);
         rc = rc || mark(SVOF_K_POISSON_FWD);

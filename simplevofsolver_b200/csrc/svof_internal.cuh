@@ -112,7 +112,10 @@ __global__ void k_predict_xsolve(const double *__restrict__ coef, double *__rest
 inline size_t predict_xsolve_smem(int nx) { return sizeof(double) * ((size_t)4 * 64 * 32 + 3 * (size_t)nx); }
 __global__ void k_predict_update(PredictArgs a, const double *__restrict__ fw);
 
-// Poisson, DCT path (src/fluid/compute_potential/dct.c)
+// Poisson, DCT path (src/fluid/compute_potential/dct.c); k_dct_fwd,
+// k_dct_fwd_rhs and k_dct_inv take dct_row_smem(nx) bytes of dynamic shared
+// memory (the transform, the row and the twiddles)
+inline size_t dct_row_smem(int nx) { return sizeof(double) * 4 * (size_t)nx; }
 __global__ void k_dct_fwd(const double *__restrict__ ux, const double *__restrict__ uy,
                           double *__restrict__ spec, const double *__restrict__ tw,
                           const double *__restrict__ cs, const double *__restrict__ dtp,
