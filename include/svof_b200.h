@@ -248,8 +248,8 @@ int svof_poisson_dct_noalloc(const svof_params_t *params, const double *xf, cons
 /* ---------------------------------------------------------------------
  * Differentiation form (FP64).  No counterpart in the reference: the adjoint
  * of one time step, for gradients of an objective of the final state with
- * respect to the initial velocities and vof and the surface-tension
- * coefficient 1/We.  The time-step sequence of a differentiated run is held
+ * respect to the initial velocities and vof, the surface-tension
+ * coefficient 1/We and the vof buoyancy coefficient grav_vof.  The time-step sequence of a differentiated run is held
  * fixed (svof_integrate_fixed); branches of the method (upwind side of a face,
  * interfacial-cell test, clamps of vanishing gradients) follow the primal
  * state.  Requires add_buoyancy = 0: the temperature is not differentiated.
@@ -269,11 +269,12 @@ int svof_set_gravity(svof_solver_t *solver, double grav_vof, double vof_ref);
 int svof_set_params(svof_solver_t *solver, const svof_params_t *params);
 
 /* doubles of one step's tape: the inputs ux, uy, vof (storage layouts) of the
- * three Runge-Kutta substeps */
+ * three Runge-Kutta substeps, then the step's final vof */
 int svof_tape_count(const svof_solver_t *solver, size_t *count);
 /* one time step with the given dt (no CFL decision), enqueued on the solver's
  * stream (svof_synchronize waits for it); when tape (device memory,
- * svof_tape_count doubles) is not NULL it records the step's substep inputs.
+ * svof_tape_count doubles) is not NULL it records the step's substep inputs
+ * and final vof.
  * Replaces integrate() (include/integrate.h:5-10) in a differentiated run. */
 int svof_integrate_fixed(svof_solver_t *solver, double dt, double *tape);
 
@@ -282,7 +283,8 @@ int svof_integrate_fixed(svof_solver_t *solver, double dt, double *tape);
  * i = 2..nx), SVOF_ADJ_NORMAL ny x nx x 3, the others ny x nx.  The adjoint of
  * a step's output is written into UX, UY, P, VOF; svof_adjoint_step turns it
  * into the adjoint of the step's input in place.  TENSION holds per-cell
- * contributions to the adjoint of 1/We (svof_adjoint_tension sums them).  The
+ * contributions to the adjoint of 1/We (svof_adjoint_tension sums them),
+ * GRAVITY those to the adjoint of grav_vof (svof_adjoint_gravity).  The
  * pointer of SVOF_ADJ_VOF and SVOF_ADJ_SRC_A changes after each interface
  * adjoint (they alternate between two buffers): ask again. */
 enum {
@@ -298,13 +300,15 @@ enum {
   SVOF_ADJ_SRCUX_A = 9,    /* pending adjoints of the substep's src_a (from the next substep's beta term) */
   SVOF_ADJ_SRCUY_A = 10,
   SVOF_ADJ_SRC_A = 11,
-  SVOF_ADJ_TENSION = 12
+  SVOF_ADJ_TENSION = 12,
+  SVOF_ADJ_GRAVITY = 13
 };
 int svof_adjoint_field(svof_solver_t *solver, int which, double **dptr, size_t *count);
 /* zero every adjoint field (enqueued) */
 int svof_adjoint_reset(svof_solver_t *solver);
 /* the adjoint of one svof_integrate_fixed(dt, tape) step, enqueued: (UX, UY,
- * P, VOF) of the step's output -> of its input, TENSION += its contribution.
+ * P, VOF) of the step's output -> of its input, TENSION and GRAVITY += their
+ * contributions.
  * Per substep in reverse: the projection and pressure update, the Poisson
  * solve (its adjoint is a second Poisson solve of psi_bar / dxf: the x grid's
  * metric weights), the implicit-x line solves, the momentum right-hand sides,
@@ -323,6 +327,9 @@ int svof_adjoint_interface_compute_force(svof_solver_t *solver);
 int svof_adjoint_interface_compute_curvature_tensor(svof_solver_t *solver);
 /* the accumulated adjoint of 1/We (waits) */
 int svof_adjoint_tension(svof_solver_t *solver, double *out);
+/* the accumulated adjoint of grav_vof (waits); for a density ratio r and
+ * Froude number Fr, d/dr = grav_bar / Fr^2 (grav_vof = -(1 - r) / Fr^2) */
+int svof_adjoint_gravity(svof_solver_t *solver, double *out);
 
 /* wait for all work of the solver's stream */
 int svof_synchronize(svof_solver_t *solver);

@@ -93,11 +93,12 @@ def _load():
         L.svo_integrate.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
         L.svo_integrate_fixed.argtypes = [ctypes.c_void_p, ctypes.c_double]
         L.svo_set_gravity.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
-        L.svo_tl_integrate_fixed.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
+        L.svo_tl_integrate_fixed.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_double,
+                                             ctypes.c_double]
         L.svo_tl_curvature_tensor.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.svo_tl_force.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double]
         L.svo_tl_update_vof.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_double]
-        L.svo_tl_predict.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_double]
+        L.svo_tl_predict.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_double]
         L.svo_run.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
         L.svo_logging.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.svo_stat_collect.argtypes = [ctypes.c_void_p]
@@ -266,8 +267,8 @@ class OracleTangent:
     def init_boundaries(self):
         _load().svo_init_boundaries(self._h)
 
-    def step(self, dt: float, dtension: float = 0.0):
-        _load().svo_tl_integrate_fixed(self.primal._h, self._h, float(dt), float(dtension))
+    def step(self, dt: float, dtension: float = 0.0, dgrav: float = 0.0):
+        _load().svo_tl_integrate_fixed(self.primal._h, self._h, float(dt), float(dtension), float(dgrav))
 
     # the linearised functions one by one (each before the primal function)
     def curvature_tensor(self):
@@ -279,8 +280,8 @@ class OracleTangent:
     def update_vof(self, rk, dt):
         _load().svo_tl_update_vof(self.primal._h, self._h, int(rk), float(dt))
 
-    def predict(self, rk, dt):
-        _load().svo_tl_predict(self.primal._h, self._h, int(rk), float(dt))
+    def predict(self, rk, dt, dgrav: float = 0.0):
+        _load().svo_tl_predict(self.primal._h, self._h, int(rk), float(dt), float(dgrav))
 
     def potential(self, rk, dt):
         f = _load().svo_potential_dct if self.primal.uniform else _load().svo_potential_dft

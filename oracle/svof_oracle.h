@@ -73,9 +73,10 @@ int svo_set_gravity(svo_ctx_t *ctx, double grav_vof, double vof_ref);
  * about the current state of `c`).  `d` is a second context on the same grid
  * and parameters, with zero wall values, whose arrays hold the tangents
  * (directional derivatives) of c's fields; `dtension` is the tangent of the
- * surface tension coefficient 1/We.  The time step is held fixed.  Advances
+ * surface tension coefficient 1/We, `dgrav` that of the vof buoyancy
+ * coefficient grav_vof.  The time step is held fixed.  Advances
  * both contexts by one step. */
-int svo_tl_integrate_fixed(svo_ctx_t *c, svo_ctx_t *d, double dt, double dtension);
+int svo_tl_integrate_fixed(svo_ctx_t *c, svo_ctx_t *d, double dt, double dtension, double dgrav);
 /* the linearised functions one by one: each reads the primal state of c at
  * the function's input, so it runs before the primal function of the same
  * name; the linear functions (potential, correct, update_pressure) are the
@@ -83,7 +84,7 @@ int svo_tl_integrate_fixed(svo_ctx_t *c, svo_ctx_t *d, double dt, double dtensio
 int svo_tl_curvature_tensor(svo_ctx_t *c, svo_ctx_t *d);
 int svo_tl_force(svo_ctx_t *c, svo_ctx_t *d, double dtension);
 int svo_tl_update_vof(svo_ctx_t *c, svo_ctx_t *d, int rkstep, double dt);
-int svo_tl_predict(svo_ctx_t *c, svo_ctx_t *d, int rkstep, double dt);
+int svo_tl_predict(svo_ctx_t *c, svo_ctx_t *d, int rkstep, double dt, double dgrav);
 /* logging reductions of the current fields (src/logging/momentum.c,
  * energy.c, nusselt/ sources): out = {momentum x, y; energy ux, uy, t; Nusselt from
  * the wall heat flux, kinetic energy injection, kinetic and thermal energy

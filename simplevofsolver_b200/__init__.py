@@ -63,11 +63,11 @@ EXPORTS = ["svof_create", "svof_destroy", "svof_field_count", "svof_upload_field
            "svof_adjoint_fluid_correct_velocity", "svof_adjoint_fluid_compute_potential",
            "svof_adjoint_fluid_predict_field", "svof_adjoint_interface_update_vof",
            "svof_adjoint_interface_compute_force", "svof_adjoint_interface_compute_curvature_tensor",
-           "svof_adjoint_tension", "svof_poisson_dct_noalloc"]
+           "svof_adjoint_tension", "svof_adjoint_gravity", "svof_poisson_dct_noalloc"]
 
 # adjoint fields (SVOF_ADJ_*); compact layouts: ux faces (ny, nx-1), cells (ny, nx)
 ADJ_FIELDS = {"ux": 0, "uy": 1, "p": 2, "vof": 3, "psi": 4, "ifrcx": 5, "ifrcy": 6, "curv": 7, "normal": 8,
-              "srcux_a": 9, "srcuy_a": 10, "src_a": 11, "tension": 12}
+              "srcux_a": 9, "srcuy_a": 10, "src_a": 11, "tension": 12, "gravity": 13}
 
 
 def adjoint_shape(name: str, nx: int, ny: int):
@@ -170,6 +170,7 @@ def lib() -> ctypes.CDLL:
         L.svof_adjoint_interface_compute_force.argtypes = [vp]
         L.svof_adjoint_interface_compute_curvature_tensor.argtypes = [vp]
         L.svof_adjoint_tension.argtypes = [vp, pd]
+        L.svof_adjoint_gravity.argtypes = [vp, pd]
         _lib = L
     return _lib
 
@@ -203,6 +204,7 @@ class Solver:
         self._h = ctypes.c_void_p()
         xf, xc = _c(ic.xf), _c(ic.xc)
         self._grid = (float(ic.lx), float(ic.ly), xf.copy(), xc.copy())
+        self.gravity = (0.0, 0.0)  # (grav_vof, vof_ref) of the vof buoyancy extension
         _check(L.svof_create(ctypes.byref(self.params), xf.ctypes.data, xc.ctypes.data, ctypes.byref(self._h)))
         for k, v in ic.fields().items():
             self.load_interior(k, v)
@@ -444,6 +446,7 @@ class Solver:
     def set_gravity(self, grav_vof: float, vof_ref: float):
         """the vof buoyancy extension on uy (absent from the reference; 0 = off)"""
         _check(lib().svof_set_gravity(self._h, float(grav_vof), float(vof_ref)))
+        self.gravity = (float(grav_vof), float(vof_ref))
 
     def set_tension(self, tension: float):
         self.params.tension = float(tension)
@@ -468,6 +471,11 @@ class Solver:
     def adjoint_tension(self) -> float:
         out = ctypes.c_double(0.0)
         _check(lib().svof_adjoint_tension(self._h, ctypes.byref(out)))
+        return out.value
+
+    def adjoint_gravity(self) -> float:
+        out = ctypes.c_double(0.0)
+        _check(lib().svof_adjoint_gravity(self._h, ctypes.byref(out)))
         return out.value
 
     def adjoint_fluid_update_pressure(self, rk: int, dt: float):

@@ -2,8 +2,10 @@
 
 ``Rollout`` runs ``len(dts)`` time steps of the CUDA solver with the time-step
 sequence held fixed (``svof_integrate_fixed``) and is differentiable with
-respect to the initial velocities, the initial volume fraction and the
-surface-tension coefficient 1/We through :class:`RolloutFunction`, a
+respect to the initial velocities, the initial volume fraction, the
+surface-tension coefficient 1/We and the coefficient grav_vof of the vof
+buoyancy extension (through it the density ratio r: grav_vof =
+-(1 - r) / Fr^2) through :class:`RolloutFunction`, a
 ``torch.autograd.Function`` whose backward pass runs the hand-written CUDA
 adjoint of each step (``svof_adjoint_step``, ``csrc/k_adjoint.cu``).
 
@@ -74,9 +76,11 @@ class Rollout:
         self.s.synchronize()
         self._torch.cuda.synchronize()
 
-    def load(self, ux0, uy0, vof0, tension):
+    def load(self, ux0, uy0, vof0, tension, grav=None):
         s = self.s
         s.set_tension(float(tension))
+        if grav is not None:
+            s.set_gravity(float(grav), s.gravity[1])
         s.load_interior("ux", _to_interior("ux", ux0, self.nx, self.ny))
         s.load_interior("uy", _to_interior("uy", uy0, self.nx, self.ny))
         s.load_interior("vof", _to_interior("vof", vof0, self.nx, self.ny))
@@ -111,8 +115,8 @@ class Rollout:
         return ux, uy, vof, p
 
     # -- forward: no tapes, checkpoints every K steps
-    def forward(self, ux0, uy0, vof0, tension, keep_checkpoints=True):
-        self.load(ux0, uy0, vof0, tension)
+    def forward(self, ux0, uy0, vof0, tension, grav=None, keep_checkpoints=True):
+        self.load(ux0, uy0, vof0, tension, grav)
         self.checkpoints = []
         for n, dt in enumerate(self.dts):
             if keep_checkpoints and n % self.K == 0:
@@ -157,29 +161,34 @@ class Rollout:
         g_uy = s.adjoint_view("uy").clone()
         g_vof = s.adjoint_view("vof").clone()
         g_ten = s.adjoint_tension()
-        return g_ux, g_uy, g_vof, g_ten
+        g_grav = s.adjoint_gravity()
+        return g_ux, g_uy, g_vof, g_ten, g_grav
 
 
 def _function():
     import torch
 
     class RolloutFunction(torch.autograd.Function):
-        """(ux0, uy0, vof0, tension) -> (ux, uy, vof, p) after the rollout's
-        steps; backward through the CUDA step adjoints with recompute from
-        checkpoints."""
+        """(ux0, uy0, vof0, tension, grav) -> (ux, uy, vof, p) after the
+        rollout's steps; backward through the CUDA step adjoints with
+        recompute from checkpoints.  grav None keeps the solver's
+        coefficient (and has no gradient)."""
 
         @staticmethod
-        def forward(ctx, ux0, uy0, vof0, tension, rollout):
+        def forward(ctx, ux0, uy0, vof0, tension, grav, rollout):
             ctx.rollout = rollout
             ctx.tension_like = tension
-            return rollout.forward(ux0, uy0, vof0, float(tension))
+            ctx.has_grav = grav is not None
+            return rollout.forward(ux0, uy0, vof0, float(tension), None if grav is None else float(grav))
 
         @staticmethod
         def backward(ctx, gux, guy, gvof, gp):
             r = ctx.rollout
-            g_ux, g_uy, g_vof, g_ten = r.backward(gux, guy, gvof, gp)
-            gt = torch.tensor(g_ten, dtype=torch.float64, device=ctx.tension_like.device)
-            return g_ux, g_uy, g_vof, gt, None
+            g_ux, g_uy, g_vof, g_ten, g_grav = r.backward(gux, guy, gvof, gp)
+            dev = ctx.tension_like.device
+            gt = torch.tensor(g_ten, dtype=torch.float64, device=dev)
+            gg = torch.tensor(g_grav, dtype=torch.float64, device=dev) if ctx.has_grav else None
+            return g_ux, g_uy, g_vof, gt, gg, None
 
     return RolloutFunction
 
@@ -187,12 +196,13 @@ def _function():
 _RF = None
 
 
-def rollout(ux0, uy0, vof0, tension, r: Rollout):
-    """differentiable rollout: returns (ux, uy, vof, p) after len(r.dts) steps"""
+def rollout(ux0, uy0, vof0, tension, r: Rollout, grav=None):
+    """differentiable rollout: returns (ux, uy, vof, p) after len(r.dts)
+    steps; grav (a 0-d tensor, optional) sets the vof buoyancy coefficient"""
     global _RF
     if _RF is None:
         _RF = _function()
-    return _RF.apply(ux0, uy0, vof0, tension, r)
+    return _RF.apply(ux0, uy0, vof0, tension, grav, r)
 
 
 def falling_objective(ux, uy, vof, xf, ly: float = 1.0):

@@ -3,13 +3,14 @@
 //
 // A differentiated run holds the time-step sequence fixed: svof_integrate_fixed
 // takes one step with a given dt and, when asked, records the primal inputs of
-// its three substeps (ux, uy, vof, storage layouts) on a tape in device
-// memory.  svof_adjoint_step maps the adjoint of a step's outputs (ux, uy, p,
-// vof) to the adjoint of its inputs in place, and accumulates the adjoint of
-// the surface-tension coefficient 1/We; per substep, in reverse: the
-// projection and pressure update, the Poisson solve (a second solve with the
-// x grid's metric weights), the implicit-x line solves, the momentum
-// right-hand sides, the vof fluxes and update, the CSF force, the intercept
+// its three substeps (ux, uy, vof, storage layouts) and its final vof on a
+// tape in device memory.  svof_adjoint_step maps the adjoint of a step's
+// outputs (ux, uy, p, vof) to the adjoint of its inputs in place, and
+// accumulates the adjoints of the surface-tension coefficient 1/We and of the
+// vof buoyancy coefficient; per substep, in reverse: the projection and
+// pressure update, the Poisson solve (a second solve with the x grid's metric
+// weights), the implicit-x line solves, the momentum right-hand sides, the
+// vof fluxes and update, the CSF force, the intercept
 // and normals (k_adjoint.cu).  The per-function entry points expose the same
 // pieces one by one, each reading the primal state from the solver's current
 // fields, for tests and for callers that drive the reference's functions
@@ -30,7 +31,7 @@ namespace svof {
 struct AdjointState {
   // adjoint fields (compact: ux faces [ny][nx-1], cells [ny][nx])
   DevBuf ux, uy, p, vof[2], pend_v[2];
-  DevBuf pend_x, pend_y, sa_x, sg_x, sa_y, sg_y, ifx, ify, kap, m, nrm, sig, psib, psis, sum;
+  DevBuf pend_x, pend_y, sa_x, sg_x, sa_y, sg_y, ifx, ify, kap, m, nrm, sig, grv, psib, psis, sum;
   int cv = 0;  // current buffer of vof_bar
   int cp = 0;  // current buffer of the vof source's pending adjoint
   int xs_rows = 1;
@@ -52,7 +53,7 @@ int adj_ensure(svof_solver *s) {
              dalloc(a->pend_x, nf) || dalloc(a->pend_y, nc) || dalloc(a->sa_x, nf) || dalloc(a->sg_x, nf) ||
              dalloc(a->sa_y, nc) || dalloc(a->sg_y, nc) || dalloc(a->ifx, nf) || dalloc(a->ify, nc) ||
              dalloc(a->kap, nc) || dalloc(a->m, 2 * nc) || dalloc(a->nrm, 3 * nc) || dalloc(a->sig, nc) ||
-             dalloc(a->psib, nc) || dalloc(a->psis, ncc) || dalloc(a->sum, 1);
+             dalloc(a->grv, nc) || dalloc(a->psib, nc) || dalloc(a->psis, ncc) || dalloc(a->sum, 1);
   // transposed line solves: R rows per block so that the blocks cover the SMs,
   // within 160 KB of staged rows
   int r = std::max(1, std::min(8, ny / 148));
@@ -70,7 +71,7 @@ int adj_ensure(svof_solver *s) {
     std::string e = g_err;
     DevBuf *bufs[] = {&a->ux, &a->uy, &a->p, &a->vof[0], &a->vof[1], &a->pend_v[0], &a->pend_v[1],
                       &a->pend_x, &a->pend_y, &a->sa_x, &a->sg_x, &a->sa_y, &a->sg_y, &a->ifx, &a->ify,
-                      &a->kap, &a->m, &a->nrm, &a->sig, &a->psib, &a->psis, &a->sum};
+                      &a->kap, &a->m, &a->nrm, &a->sig, &a->grv, &a->psib, &a->psis, &a->sum};
     for (DevBuf *b : bufs) dfree(*b);
     delete a;
     g_err = e.empty() ? "adjoint set-up failed" : e;
@@ -139,9 +140,9 @@ int adj_potential(svof_solver *s, int rk, double dt) {
   return 0;
 }
 
-// fluid_predict_field about the primal velocities ux, uy (storage layouts);
-// d_dt must hold dt
-int adj_predict(svof_solver *s, int rk, double dt, const double *ux, const double *uy) {
+// fluid_predict_field about the primal velocities ux, uy and the vof after
+// the substep's advection (storage layouts); d_dt must hold dt
+int adj_predict(svof_solver *s, int rk, double dt, const double *ux, const double *uy, const double *vof_post) {
   AdjointState *a = s->adj;
   if (launch_coef(s, rk, s->stream)) return 1;
   const int R = a->xs_rows;
@@ -169,6 +170,9 @@ int adj_predict(svof_solver *s, int rk, double dt, const double *ux, const doubl
   r.lapy1 = s->lapy[1];
   r.lapy2 = s->lapy[2];
   r.grav_vof = s->grav_vof;
+  r.vof_ref = s->vof_ref;
+  r.vof_post = vof_post;
+  r.agrv = a->grv.p;
   r.g = s->grid();
   k_adj_rhs<<<cell_grid(s), dim3(32, 8), 0, s->stream>>>(r);
   CK_LAUNCH();
@@ -220,10 +224,13 @@ int adj_corners(svof_solver *s, const double *vof) {
   return 0;
 }
 
+size_t vof_count(const svof_solver *s) { return (size_t)(s->nx + 2) * (s->ny + 4); }
+
+// one substep's part of a tape: ux, uy, vof; the tape holds three of them and
+// the step's final vof
 size_t tape_stride(const svof_solver *s) {
   const size_t n_ux = (size_t)(s->nx + 1) * (s->ny + 2), n_cc = (size_t)(s->nx + 2) * (s->ny + 2);
-  const size_t n_vof = (size_t)(s->nx + 2) * (s->ny + 4);
-  return n_ux + n_cc + n_vof;
+  return n_ux + n_cc + vof_count(s);
 }
 
 int check_prim(svof_solver *s) {
@@ -262,7 +269,7 @@ int svof_set_params(svof_solver_t *s, const svof_params_t *prm) {
 
 int svof_tape_count(const svof_solver_t *s, size_t *count) {
   if (!s || !count) return fail("null argument");
-  *count = 3 * tape_stride(s);
+  *count = 3 * tape_stride(s) + vof_count(s);
   return 0;
 }
 
@@ -284,6 +291,9 @@ int svof_integrate_fixed(svof_solver_t *s, double dt, double *tape) {
         launch_predict(s, rk, false) || launch_potential(s, rk, s->uniform) || launch_project(s, rk, 1, 1))
       return 1;
   }
+  if (tape)
+    CK(cudaMemcpyAsync(tape + 3 * st, s->vof[s->cur_v].p, sizeof(double) * n_vof, cudaMemcpyDeviceToDevice,
+                       s->stream));
   return 0;
 }
 
@@ -308,6 +318,7 @@ int svof_adjoint_field(svof_solver_t *s, int which, double **dptr, size_t *count
     case SVOF_ADJ_SRCUY_A: b = &a->pend_y; break;
     case SVOF_ADJ_SRC_A: b = &a->pend_v[a->cp]; break;
     case SVOF_ADJ_TENSION: b = &a->sig; break;
+    case SVOF_ADJ_GRAVITY: b = &a->grv; break;
     default: return fail("unknown adjoint field %d", which);
   }
   *dptr = b->p;
@@ -320,7 +331,7 @@ int svof_adjoint_reset(svof_solver_t *s) {
   AdjointState *a = s->adj;
   DevBuf *bufs[] = {&a->ux, &a->uy, &a->p, &a->vof[0], &a->vof[1], &a->pend_v[0], &a->pend_v[1],
                     &a->pend_x, &a->pend_y, &a->sa_x, &a->sg_x, &a->sa_y, &a->sg_y, &a->ifx, &a->ify,
-                    &a->kap, &a->m, &a->nrm, &a->sig, &a->psib, &a->psis};
+                    &a->kap, &a->m, &a->nrm, &a->sig, &a->grv, &a->psib, &a->psis};
   for (DevBuf *b : bufs) CK(cudaMemsetAsync(b->p, 0, sizeof(double) * b->n, s->stream));
   return 0;
 }
@@ -339,11 +350,12 @@ int svof_adjoint_step(svof_solver_t *s, const double *tape, double dt) {
   if (adj_set_dt(s, dt)) return 1;
   for (int rk = 2; rk >= 0; rk--) {
     const double *ux = tape + rk * st, *uy = ux + n_ux, *vof = uy + n_cc;
+    const double *vof_post = tape + (rk + 1) * st + (rk < 2 ? n_ux + n_cc : 0);
     // the substep's geometry from its vof (normals, intercepts, curvature)
     k_geom<<<dim3((s->nx + 31) / 32, (s->ny + 2 + 7) / 8), dim3(32, 8), 0, s->stream>>>(vof, s->normal.p,
                                                                                          s->curv.p, s->grid());
     CK_LAUNCH();
-    if (adj_project(s, rk, dt, 3) || adj_potential(s, rk, dt) || adj_predict(s, rk, dt, ux, uy) ||
+    if (adj_project(s, rk, dt, 3) || adj_potential(s, rk, dt) || adj_predict(s, rk, dt, ux, uy, vof_post) ||
         adj_interface(s, rk, dt, 7, ux, uy, vof) || adj_corners(s, vof))
       return 1;
   }
@@ -371,7 +383,8 @@ int svof_adjoint_fluid_compute_potential(svof_solver_t *s, size_t rk, double dt)
 int svof_adjoint_fluid_predict_field(svof_solver_t *s, size_t rk, double dt) {
   if (check_prim(s)) return 1;
   if (rk > 2) return fail("rkstep out of range");
-  return adj_set_dt(s, dt) || adj_predict(s, (int)rk, dt, s->ux[s->cur_u].p, s->uy[s->cur_u].p) || sync(s);
+  return adj_set_dt(s, dt) ||
+         adj_predict(s, (int)rk, dt, s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->vof[s->cur_v].p) || sync(s);
 }
 
 int svof_adjoint_interface_update_vof(svof_solver_t *s, size_t rk, double dt) {
@@ -391,15 +404,26 @@ int svof_adjoint_interface_compute_curvature_tensor(svof_solver_t *s) {
   return adj_interface(s, 0, 0., 4, s->ux[s->cur_u].p, s->uy[s->cur_u].p, vof) || adj_corners(s, vof) || sync(s);
 }
 
-int svof_adjoint_tension(svof_solver_t *s, double *out) {
-  if (check_prim(s)) return 1;
-  if (!out) return fail("null argument");
+// the deterministic sum of a per-cell accumulator, copied to the host
+static int adj_total(svof_solver *s, const DevBuf &b, double *out) {
   AdjointState *a = s->adj;
-  k_adj_sum<<<1, 256, 0, s->stream>>>(a->sig.p, (long)a->sig.n, a->sum.p);
+  k_adj_sum<<<1, 256, 0, s->stream>>>(b.p, (long)b.n, a->sum.p);
   CK_LAUNCH();
   CK(cudaMemcpyAsync(out, a->sum.p, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   return 0;
+}
+
+int svof_adjoint_tension(svof_solver_t *s, double *out) {
+  if (check_prim(s)) return 1;
+  if (!out) return fail("null argument");
+  return adj_total(s, s->adj->sig, out);
+}
+
+int svof_adjoint_gravity(svof_solver_t *s, double *out) {
+  if (check_prim(s)) return 1;
+  if (!out) return fail("null argument");
+  return adj_total(s, s->adj->grv, out);
 }
 
 }  // extern "C"
@@ -412,7 +436,7 @@ void adjoint_free(svof_solver *s) {
   AdjointState *a = s->adj;
   DevBuf *bufs[] = {&a->ux, &a->uy, &a->p, &a->vof[0], &a->vof[1], &a->pend_v[0], &a->pend_v[1],
                     &a->pend_x, &a->pend_y, &a->sa_x, &a->sg_x, &a->sa_y, &a->sg_y, &a->ifx, &a->ify,
-                    &a->kap, &a->m, &a->nrm, &a->sig, &a->psib, &a->psis, &a->sum};
+                    &a->kap, &a->m, &a->nrm, &a->sig, &a->grv, &a->psib, &a->psis, &a->sum};
   for (DevBuf *b : bufs) dfree(*b);
   delete a;
   s->adj = nullptr;

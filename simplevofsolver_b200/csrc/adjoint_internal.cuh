@@ -26,7 +26,9 @@ struct AdjRhsArgs {
   double *aux, *auy, *ap, *avof, *aifx, *aify;
   const double *lap_ux, *lap_uy;
   double m_dif, lapy0, lapy1, lapy2;
-  double grav_vof;
+  double grav_vof, vof_ref;
+  const double *vof_post;                    // primal vof after the substep's advection (storage layout)
+  double *agrv;                              // buoyancy coefficient adjoint, per cell, +=
   Grid2 g;
 };
 __global__ void k_adj_rhs(AdjRhsArgs a);

@@ -205,10 +205,11 @@ __global__ void k_adj_xsolve(const double *__restrict__ aux, const double *__res
 // k_adj_rhs: transposes of compute_rhs_ux (ux.c:71-249) and compute_rhs_uy
 // (uy.c:70-221): u_bar = u_bar* + (d src / d u)^T src_bar, p_bar +=
 // (d src_g / d p)^T src_g_bar, ifrc_bar = src_a_bar, vof_bar += the vof
-// buoyancy's transpose.  The energy-consistent advection term l a + c b + u e
-// with l = k (a + b), u = -k (b + e), c = -l - u equals k (a^2 - e^2): its
-// derivatives are 2 k a, 0, -2 k e.  One thread per cell (i, j) writes ux
-// face i (i >= 2), uy (i, j), p (i, j), vof (i, j), the two forces.
+// buoyancy's transpose, grv_bar += its derivative in the coefficient.  The
+// energy-consistent advection term l a + c b + u e with l = k (a + b),
+// u = -k (b + e), c = -l - u equals k (a^2 - e^2): its derivatives are
+// 2 k a, 0, -2 k e.  One thread per cell (i, j) writes ux face i (i >= 2),
+// uy (i, j), p (i, j), vof (i, j), grv (i, j), the two forces.
 
 __global__ void k_adj_rhs(AdjRhsArgs a) {
   const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
@@ -303,8 +304,10 @@ __global__ void k_adj_rhs(AdjRhsArgs a) {
     if (i >= 2) pb -= SGX(i, j) / g.dxc[i - 1];
     if (i + 1 <= nx) pb += SGX(i + 1, j) / g.dxc[i];
     a.ap[o] += pb;
-    // vof buoyancy: grav_vof (0.5 vof(i, j-1) + 0.5 vof(i, j) - vof_ref) on uy (i, j)
+    // vof buoyancy: grav_vof (0.5 vof(i, j-1) + 0.5 vof(i, j) - vof_ref) on uy (i, j);
+    // its derivative in grav_vof is the bracket, for any grav_vof
     if (0. != a.grav_vof) a.avof[o] += a.grav_vof * 0.5 * (SAY(i, j) + SAY(i, jp));
+    a.agrv[o] += SAY(i, j) * (0.5 * a.vof_post[ix_vof(nx, i, j - 1)] + 0.5 * a.vof_post[ix_vof(nx, i, j)] - a.vof_ref);
   }
 }
 

@@ -223,8 +223,7 @@ extern "C" int svof_poisson_dct_noalloc(const svof_params_t *prm, const double *
                                   : rkstep == 1 ? 25. / 60. + -17. / 60. : 45. / 60. + -25. / 60.);
   const Grid2 g{nx, ny, dy, S + kDxf, S + kDxf};
   const int nthr = nx / 2 < 32 ? 32 : (nx / 2 > 256 ? 256 : nx / 2);
-  k_dct_fwd<<<ny, nthr, dct_row_smem(nx), s>>>(ux, uy, S + kSpec, S + kTwf, S + kCs, S + kDt, gam, log2n,
-                                                      g);
+  k_dct_fwd<<<ny, nthr, dct_row_smem(nx), s>>>(ux, uy, S + kSpec, S + kTwf, S + kCs, S + kDt, gam, log2n, g);
   int kt = 32;
   while (kt > 4 && nx / kt < 148) kt >>= 1;
   while (kt > 1 && sizeof(double) * 3 * (size_t)ny * kt > 48 * 1024) kt >>= 1;

@@ -158,7 +158,8 @@ def test_predict_field(gpu_available, uniform, rk):
     # src_b of this substep is the current src_a (moved by reset_srcs)
     tan.field("srcux0")[...] = d["sbx"]
     tan.field("srcuy0")[...] = d["sby"]
-    tan.predict(rk, dt)
+    dgrav = 0.23    # tangent of the vof buoyancy coefficient
+    tan.predict(rk, dt, dgrav)
     lhs = (np.sum(cx(tan.field("ux"), nx, ny) * b["ux"]) + np.sum(cc(tan.field("uy"), nx, ny) * b["uy"])
            + np.sum(tan.field("srcux0") * b["sax"]) + np.sum(tan.field("srcuy0") * b["say"]))
     put(g, "ux", b["ux"])
@@ -168,7 +169,7 @@ def test_predict_field(gpu_available, uniform, rk):
     g.adjoint_fluid_predict_field(rk, dt)
     rhs = (np.sum(d["ux"] * get(g, "ux")) + np.sum(d["uy"] * get(g, "uy")) + np.sum(d["p"] * get(g, "p"))
            + np.sum(d["vof"] * get(g, "vof")) + np.sum(d["ifrcx"] * get(g, "ifrcx"))
-           + np.sum(d["ifrcy"] * get(g, "ifrcy")))
+           + np.sum(d["ifrcy"] * get(g, "ifrcy")) + dgrav * g.adjoint_gravity())
     if rk != 0:
         rhs += np.sum(d["sbx"] * get(g, "srcux_a")) + np.sum(d["sby"] * get(g, "srcuy_a"))
     assert rel(lhs, rhs) <= TOL, (lhs, rhs)
@@ -259,9 +260,10 @@ def test_curvature_tensor(gpu_available, uniform):
     assert rel(lhs, rhs) <= TOL, (lhs, rhs)
 
 
-def tangent_step_along(o, tan, tape, rk_fields, dt, dten):
+def tangent_step_along(o, tan, tape, rk_fields, dt, dten, dgrav=0.0):
     """one step of the oracle's tangent model linearised about the GPU's taped
-    substep inputs (ux, uy, vof of each substep)"""
+    substep inputs (ux, uy, vof of each substep; the predictor's vof is the
+    one after the substep's advection: the next entry's)"""
     for rk in range(3):
         for k in ("ux", "uy", "vof"):
             o.field(k)[...] = rk_fields[rk][k]
@@ -269,19 +271,22 @@ def tangent_step_along(o, tan, tape, rk_fields, dt, dten):
         tan.curvature_tensor()
         tan.force(dten)
         tan.update_vof(rk, dt)
-        tan.predict(rk, dt)
+        o.field("vof")[...] = rk_fields[rk + 1]["vof"]
+        tan.predict(rk, dt, dgrav)
         tan.potential(rk, dt)
         tan.correct(rk, dt)
         tan.update_pressure(rk, dt)
 
 
 def taped_fields(g, tape):
-    """split one step's tape into the substep inputs (storage layouts)"""
+    """split one step's tape into the substep inputs (storage layouts) and,
+    as a fourth entry, the step's final vof"""
     from simplevofsolver_b200 import storage_shape
     nx, ny = g.nx, g.ny
     t = tape.cpu().numpy()
     sizes = [np.prod(storage_shape(k, nx, ny)) for k in ("ux", "uy", "vof")]
     st = sum(sizes)
+    assert t.size == 3 * st + sizes[2]
     out = []
     for rk in range(3):
         base = rk * st
@@ -290,6 +295,7 @@ def taped_fields(g, tape):
             d[k] = t[base:base + n].reshape(storage_shape(k, nx, ny))
             base += n
         out.append(d)
+    out.append({"vof": t[3 * st:].reshape(storage_shape("vof", nx, ny))})
     return out
 
 
@@ -307,7 +313,7 @@ def test_step_dot_product(gpu_available, uniform, gravity, steps):
     rng = np.random.default_rng(7)
     d0 = {"ux": rnd(rng, (ny, nx - 1)), "uy": rnd(rng, (ny, nx)), "p": rnd(rng, (ny, nx)),
           "vof": rnd(rng, (ny, nx)) * interfacial_mask(o, nx, ny)}
-    dten = 0.21
+    dten, dgrav = 0.21, -0.17
     b = {"ux": rnd(rng, (ny, nx - 1)), "uy": rnd(rng, (ny, nx)), "p": zero_mean(rnd(rng, (ny, nx))),
          "vof": rnd(rng, (ny, nx))}
     # tangent model along the GPU trajectory
@@ -317,7 +323,7 @@ def test_step_dot_product(gpu_available, uniform, gravity, steps):
     cc(tan.field("vof"), nx, ny, 2)[...] = d0["vof"]
     tan.init_boundaries()
     for k in range(steps):
-        tangent_step_along(o, tan, tapes[k], taped_fields(g, tapes[k]), dt, dten)
+        tangent_step_along(o, tan, tapes[k], taped_fields(g, tapes[k]), dt, dten, dgrav)
     lhs = (np.sum(cx(tan.field("ux"), nx, ny) * b["ux"]) + np.sum(cc(tan.field("uy"), nx, ny) * b["uy"])
            + np.sum(cc(tan.field("p"), nx, ny) * b["p"]) + np.sum(cc(tan.field("vof"), nx, ny, 2) * b["vof"]))
     # adjoint
@@ -325,6 +331,7 @@ def test_step_dot_product(gpu_available, uniform, gravity, steps):
         put(g, k, b[k])
     for k in reversed(range(steps)):
         g.adjoint_step(tapes[k].data_ptr(), dt)
-    rhs = sum(np.sum(d0[k] * get(g, k)) for k in ("ux", "uy", "p", "vof")) + dten * g.adjoint_tension()
+    rhs = (sum(np.sum(d0[k] * get(g, k)) for k in ("ux", "uy", "p", "vof")) + dten * g.adjoint_tension()
+           + dgrav * g.adjoint_gravity())
     assert rel(lhs, rhs) <= 1e-10, (lhs, rhs)
     g.close()

@@ -3,11 +3,12 @@ differentiation form): 256 x 256 on the unit box, one droplet of radius 0.15
 at (0.5, 0.7) falling under gravity (Fr = 1, density ratio 0.1 as vof
 buoyancy), Re = 200, We = 20, 200 steps with checkpoints every 20, objective
 = final vof-weighted centroid y + 0.1 x final kinetic energy, gradient with
-respect to the initial velocities (2 x 256 x 256) and 1/We.
+respect to the initial velocities (2 x 256 x 256), 1/We and the vof
+buoyancy coefficient grav_vof = -(1 - r) / Fr^2 (r the density ratio).
 
 * central finite differences of the forward (the GPU FP64 path, which
   reproduces the reference to 1e-12 per step), eps = 1e-6 along 16 seeded
-  random smooth directions of unit norm (velocity and 1/We), the time-step
+  random smooth directions of unit norm (velocity, 1/We, grav_vof), the time-step
   sequence held fixed and the initial velocity projected onto
   divergence-free fields (adjoint.Rollout): each directional derivative
   within 1e-5 of the adjoint's, relative (measured: 15 of 16 directions
@@ -42,23 +43,25 @@ def make(n=256, steps=200, K=20):
     r = Rollout(s, dts, K)
     dev = dict(dtype=torch.float64, device="cuda")
     x = {"ux": torch.tensor(ic.ux[:, 1:n], **dev), "uy": torch.tensor(ic.uy[:, 1:n + 1], **dev),
-         "vof": torch.tensor(ic.vof[:, 1:n + 1], **dev), "ten": torch.tensor(phys["tension"], **dev)}
+         "vof": torch.tensor(ic.vof[:, 1:n + 1], **dev), "ten": torch.tensor(phys["tension"], **dev),
+         "grav": torch.tensor(falling_gravity(ic)[0], **dev)}
     return ic, phys, r, x
 
 
 def objective(ic, r, x):
     from simplevofsolver_b200.adjoint import falling_objective
-    ux, uy, vof, p = r.forward(x["ux"], x["uy"], x["vof"], float(x["ten"]), keep_checkpoints=False)
+    ux, uy, vof, p = r.forward(x["ux"], x["uy"], x["vof"], float(x["ten"]), float(x["grav"]),
+                               keep_checkpoints=False)
     return float(falling_objective(ux, uy, vof, ic.xf))
 
 
 def gradient(ic, r, x):
     from simplevofsolver_b200.adjoint import falling_objective, rollout
     xs = {k: v.clone().requires_grad_(k != "vof") for k, v in x.items()}
-    ux, uy, vof, p = rollout(xs["ux"], xs["uy"], xs["vof"], xs["ten"], r)
+    ux, uy, vof, p = rollout(xs["ux"], xs["uy"], xs["vof"], xs["ten"], r, grav=xs["grav"])
     J = falling_objective(ux, uy, vof, ic.xf)
     J.backward()
-    return float(J.detach()), {k: xs[k].grad.clone() for k in ("ux", "uy", "ten")}
+    return float(J.detach()), {k: xs[k].grad.clone() for k in ("ux", "uy", "ten", "grav")}
 
 
 def smooth_direction(rng, nx, ny, xf, modes=4):
@@ -92,7 +95,8 @@ def test_gradient_matches_central_differences(gpu_available):
     for _ in range(16):
         dux, duy = smooth_direction(rng, ic.nx, ic.ny, ic.xf)
         v = {k: torch.tensor(a, dtype=torch.float64, device="cuda")
-             for k, a in (("ux", dux), ("uy", duy), ("ten", np.array(rng.standard_normal())))}
+             for k, a in (("ux", dux), ("uy", duy), ("ten", np.array(rng.standard_normal())),
+                          ("grav", np.array(rng.standard_normal())))}
         nrm = float(torch.sqrt(sum(torch.sum(a * a) for a in v.values())))
         v = {k: a / nrm for k, a in v.items()}
         d_adj = float(sum(torch.sum(grad[k] * v[k]) for k in v))
@@ -143,11 +147,11 @@ def test_tangent_dot_product_along_rollout(gpu_available):
     tan = o.tangent()
     rng = np.random.default_rng(11)
     d0 = {"ux": rng.standard_normal((ny, nx - 1)), "uy": rng.standard_normal((ny, nx))}
-    dten = 0.3
+    dten, dgrav = 0.3, 0.4
     b = {"ux": rng.standard_normal((ny, nx - 1)), "uy": rng.standard_normal((ny, nx)),
          "p": zero_mean(rng.standard_normal((ny, nx))), "vof": rng.standard_normal((ny, nx))}
     # forward with tapes
-    r.load(x["ux"], x["uy"], x["vof"], float(x["ten"]))
+    r.load(x["ux"], x["uy"], x["vof"], float(x["ten"]), float(x["grav"]))
     tapes = [torch.empty(s.tape_count(), dtype=torch.float64, device="cuda") for _ in r.dts]
     torch.cuda.synchronize()
     for k, dt in enumerate(r.dts):
@@ -157,7 +161,7 @@ def test_tangent_dot_product_along_rollout(gpu_available):
     cc(tan.field("uy"), nx, ny)[...] = d0["uy"]
     tan.init_boundaries()
     for k, dt in enumerate(r.dts):
-        tangent_step_along(o, tan, tapes[k], taped_fields(s, tapes[k]), dt, dten)
+        tangent_step_along(o, tan, tapes[k], taped_fields(s, tapes[k]), dt, dten, dgrav)
     lhs = (np.sum(cx(tan.field("ux"), nx, ny) * b["ux"]) + np.sum(cc(tan.field("uy"), nx, ny) * b["uy"])
            + np.sum(cc(tan.field("p"), nx, ny) * b["p"]) + np.sum(cc(tan.field("vof"), nx, ny, 2) * b["vof"]))
     s.adjoint_reset()
@@ -170,7 +174,7 @@ def test_tangent_dot_product_along_rollout(gpu_available):
     s.synchronize()
     rhs = (float(torch.sum(s.adjoint_view("ux").cpu() * torch.as_tensor(d0["ux"])))
            + float(torch.sum(s.adjoint_view("uy").cpu() * torch.as_tensor(d0["uy"])))
-           + dten * s.adjoint_tension())
+           + dten * s.adjoint_tension() + dgrav * s.adjoint_gravity())
     rel = abs(lhs - rhs) / max(abs(lhs), abs(rhs))
     print(f"dot product over {len(r.dts)} steps: {lhs:.15e} vs {rhs:.15e}, relative {rel:.2e}")
     assert rel <= 1e-9, (lhs, rhs)

@@ -7,7 +7,8 @@ linearises.  The time step is held fixed in both.  A random weight w defines
 J(x) = <w, F(x)> over the final ux, uy, p and vof (the weights of p sum to
 zero: its additive constant is fixed by round-off); the directional derivative
 of J along a random direction of unit norm (initial velocities, vof of
-interfacial cells, surface tension) from the tangent model must match
+interfacial cells, surface tension, the vof buoyancy coefficient where it is
+on) from the tangent model must match
 (J(x + eps v) - J(x - eps v)) / (2 eps), eps = 1e-6, to 1e-7 relative.
 """
 import numpy as np
@@ -33,10 +34,10 @@ def make(ic, phys, gravity=None):
     return o
 
 
-def perturbed(ic, phys, v, eps, gravity=None, dtension=0.0):
+def perturbed(ic, phys, v, eps, gravity=None, dtension=0.0, dgrav=0.0):
     p = dict(phys)
     p["tension"] = phys["tension"] + eps * dtension
-    o = make(ic, p, gravity)
+    o = make(ic, p, (gravity[0] + eps * dgrav, gravity[1]) if gravity else None)
     for k in ("ux", "uy", "vof"):
         interior(k, o.field(k), o.nx, o.ny)[...] += eps * v[k]
     import oracle
@@ -77,19 +78,20 @@ def test_tangent_matches_central_differences(uniform, gravity, steps):
     dt = base.decide_dt()
     v, w = directions(ic, base, 7)
     dten = 0.3
+    dgrav = 0.4 if gravity else 0.0
     # tangent: primal and tangent advanced together
     tan = base.tangent()
     for k in ("ux", "uy", "vof"):
         interior(k, tan.field(k), tan.nx, tan.ny)[...] = v[k]
     tan.init_boundaries()
     for _ in range(steps):
-        tan.step(dt, dten)
+        tan.step(dt, dten, dgrav)
     dj_tl = sum(float(np.sum(w[k] * interior(k, tan.field(k), tan.nx, tan.ny))) for k in w)
     # central differences of the primal
     eps = 1e-6
     js = []
     for sgn in (+1, -1):
-        o = perturbed(ic, phys, v, sgn * eps, gravity, dten)
+        o = perturbed(ic, phys, v, sgn * eps, gravity, dten, dgrav)
         for _ in range(steps):
             o.integrate_fixed(dt)
         js.append(objective(o, w))
