@@ -183,16 +183,17 @@ __device__ __forceinline__ void load_normal(const float *__restrict__ normal, lo
 // ---------------------------------------------------------------------------
 // k3_geom: cells i in [1, nx], j in [0, ny+1], k in [0, nz+1] (halo cells
 // included, as the restatement computes them).  Block: 32 x 4 cells of one
-// plane, marching over G3Z planes; shared memory holds two vof planes
-// (34 x 6, FP64) and two planes of corner normals (33 x 5 x 3, R).  The vof
-// differences are taken in FP64 and then carried in R.
-constexpr int G3X = 32, G3Y = 4, G3Z = 32;
+// plane, marching over G3Z planes; shared memory holds a ring of vof planes
+// (34 x 6, FP64), G3D planes in flight ahead of the two being read, and two
+// planes of corner normals (33 x 5 x 3, R).  The vof differences are taken
+// in FP64 and then carried in R.
+constexpr int G3X = 32, G3Y = 4, G3Z = 32, G3D = 4, G3S = G3D + 2;
 
 template <class R>
 __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ vof, R *__restrict__ normal,
                                                     R *__restrict__ curv, unsigned *__restrict__ work,
                                                     unsigned *__restrict__ nwork, Grid3 g) {
-  __shared__ double sv[3][G3Y + 2][G3X + 2];  // vof planes, plane p in slot (p - k0 + 1) % 3
+  __shared__ double sv[G3S][G3Y + 2][G3X + 2];  // vof planes, plane p in slot (p - k0 + 1) % G3S
   __shared__ R sc[2][3][G3Y + 1][G3X + 1];
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int i0 = 1 + blockIdx.x * G3X;
@@ -203,9 +204,11 @@ __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ 
   const int tx = tid % G3X, ty = tid / G3X;
   const R eps = R(kDblEpsilon);
   const R rdy = R(1.) / R(g.dy), rdz = R(1.) / R(g.dz);
-  // cp.async: the next plane arrives while the current one is processed; the
-  // window elements a thread copies are the same on every plane, their
-  // in-plane offsets computed once (-1: zero fill, -2: no element)
+  // cp.async: planes arrive G3D ahead of the one being processed; the window
+  // elements a thread copies are the same on every plane, their in-plane
+  // offsets computed once (-1: zero fill, -2: no element).  Every thread
+  // commits one group per plane slot (empty past the block's last plane), so
+  // that a plane's group is always a fixed number of groups behind the newest
   constexpr int NT = G3X * G3Y, NW = ((G3X + 2) * (G3Y + 2) + NT - 1) / NT;
   const long vplane = (long)(nx + 2) * (ny + 4);
   int woff[NW];
@@ -216,7 +219,7 @@ __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ 
     woff[q] = (t >= (G3X + 2) * (G3Y + 2)) ? -2 : ((i <= nx + 1 && j <= ny + 2) ? i + (nx + 2) * (j + 1) : -1);
   }
   auto load_plane = [&](int k) {
-    const int buf = (k - k0 + 1) % 3;
+    const int buf = (k - k0 + 1) % G3S;
     const double *vp = vof + vplane * (k + 1);
     double *d = &sv[buf][0][0];
 #pragma unroll
@@ -226,8 +229,10 @@ __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ 
     }
     __pipeline_commit();
   };
-  load_plane(k0 - 1);
-  load_plane(k0);
+  for (int p = k0 - 1; p < k0 + G3D; p++) {
+    if (p <= kend) load_plane(p);
+    else __pipeline_commit();
+  }
   // 1 / dxc of the (up to two) corner columns this thread handles and 1 / dxf
   // of its cell column, once (the same values as per corner / cell)
   R rdxc[2] = {R(0.), R(0.)};
@@ -236,46 +241,68 @@ __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ 
     if (ic <= nx + 1) rdxc[q] = R(1.) / R(ldg(g.dxc + ic - 1));
   }
   const R rdxf = (i0 + tx <= nx) ? R(1.) / R(ldg(g.dxf + i0 + tx - 1)) : R(0.);
-  __pipeline_wait_prior(0);
-  __syncthreads();
+  // whether this thread's window elements of a plane (its own copies and zero
+  // fills, complete after its wait) are all +0: the block's vote, taken at a
+  // barrier, tells whether the whole window of the plane is +0
+  auto my_zero = [&](int buf) {
+    const double *d = &sv[buf][0][0];
+    int z = 1;
+#pragma unroll
+    for (int q = 0; q < NW; q++)
+      if (woff[q] >= -1 && 0 != __double_as_longlong(d[tid + NT * q])) z = 0;
+    return z;
+  };
+  __pipeline_wait_prior(G3D - 1);             // planes k0 - 1 and k0
+  int z_lo = __syncthreads_and(my_zero(0));  // plane kc - 1 all +0
+  int z_hi = __syncthreads_and(my_zero(1));  // plane kc all +0
   R l_dx0 = R(0.), l_dy1 = R(0.), l_s0 = R(0.), l_s1 = R(0.), l_s2 = R(0.);  // lower corner plane
   for (int kc = k0; kc <= kend; kc++) {
-    const int bcur = (kc - k0 + 1) % 3, bprev = (kc - k0) % 3;
+    const int bcur = (kc - k0 + 1) % G3S, bprev = (kc - k0) % G3S;
     const int ccur = (kc - k0) & 1;
-    if (kc + 1 <= kend) load_plane(kc + 1);
+    // plane kc + G3D into the slot of plane kc - 2 (read last in the
+    // previous iteration, before its closing barrier)
+    if (kc + G3D <= kend) load_plane(kc + G3D);
+    else __pipeline_commit();
+    // both vof planes of the corner plane kc all +0 (the gas bulk, most of
+    // the domain): every corner is flat, every corner normal +0 and so every
+    // 2 x 2 stencil sum below; the corner pass and its barrier are skipped
+    // (block-uniform), the cells take the +0 sums
+    const bool flat_tile = z_lo && z_hi;
     // compute_gradient at corners (ic, jc, kc): planes kc-1 (bprev) and kc (bcur)
-    for (int t = tid, q = 0; t < (G3X + 1) * (G3Y + 1); t += G3X * G3Y, q++) {
-      const int li = t % (G3X + 1), lj = t / (G3X + 1);
-      const int ic = i0 + li, jc = j0 + lj;
-      R d0 = R(0.), d1 = R(0.), d2 = R(0.);
-      if (ic <= nx + 1 && jc <= ny + 2) {
-        const double a00 = sv[bprev][lj][li], a10 = sv[bprev][lj][li + 1];
-        const double a01 = sv[bprev][lj + 1][li], a11 = sv[bprev][lj + 1][li + 1];
-        const double b00 = sv[bcur][lj][li], b10 = sv[bcur][lj][li + 1];
-        const double b01 = sv[bcur][lj + 1][li], b11 = sv[bcur][lj + 1][li + 1];
-        // eight bit-identical values (the bulk outside the droplets): every
-        // difference is +0, so the normal is +0 (+0 times 1 / eps) without
-        // the square root and division
-        const long long r = __double_as_longlong(a00);
-        const bool flat = r == __double_as_longlong(a10) && r == __double_as_longlong(a01) &&
-                          r == __double_as_longlong(a11) && r == __double_as_longlong(b00) &&
-                          r == __double_as_longlong(b10) && r == __double_as_longlong(b01) &&
-                          r == __double_as_longlong(b11);
-        if (!flat) {
-          const R dvofdx = rdxc[q] * R(plane_dx(a00, a10, a01, a11) + plane_dx(b00, b10, b01, b11));
-          const R dvofdy = rdy * R(plane_dy(a00, a10, a01, a11) + plane_dy(b00, b10, b01, b11));
-          const R dvofdz = rdz * R(plane_sum(b00, b10, b01, b11) - plane_sum(a00, a10, a01, a11));
-          const R norminv = rnorm(+dvofdx * dvofdx + dvofdy * dvofdy + dvofdz * dvofdz, eps);
-          d0 = dvofdx * norminv;
-          d1 = dvofdy * norminv;
-          d2 = dvofdz * norminv;
+    if (!flat_tile) {
+      for (int t = tid, q = 0; t < (G3X + 1) * (G3Y + 1); t += G3X * G3Y, q++) {
+        const int li = t % (G3X + 1), lj = t / (G3X + 1);
+        const int ic = i0 + li, jc = j0 + lj;
+        R d0 = R(0.), d1 = R(0.), d2 = R(0.);
+        if (ic <= nx + 1 && jc <= ny + 2) {
+          const double a00 = sv[bprev][lj][li], a10 = sv[bprev][lj][li + 1];
+          const double a01 = sv[bprev][lj + 1][li], a11 = sv[bprev][lj + 1][li + 1];
+          const double b00 = sv[bcur][lj][li], b10 = sv[bcur][lj][li + 1];
+          const double b01 = sv[bcur][lj + 1][li], b11 = sv[bcur][lj + 1][li + 1];
+          // eight bit-identical values (the bulk outside the droplets): every
+          // difference is +0, so the normal is +0 (+0 times 1 / eps) without
+          // the square root and division
+          const long long r = __double_as_longlong(a00);
+          const bool flat = r == __double_as_longlong(a10) && r == __double_as_longlong(a01) &&
+                            r == __double_as_longlong(a11) && r == __double_as_longlong(b00) &&
+                            r == __double_as_longlong(b10) && r == __double_as_longlong(b01) &&
+                            r == __double_as_longlong(b11);
+          if (!flat) {
+            const R dvofdx = rdxc[q] * R(plane_dx(a00, a10, a01, a11) + plane_dx(b00, b10, b01, b11));
+            const R dvofdy = rdy * R(plane_dy(a00, a10, a01, a11) + plane_dy(b00, b10, b01, b11));
+            const R dvofdz = rdz * R(plane_sum(b00, b10, b01, b11) - plane_sum(a00, a10, a01, a11));
+            const R norminv = rnorm(+dvofdx * dvofdx + dvofdy * dvofdy + dvofdz * dvofdz, eps);
+            d0 = dvofdx * norminv;
+            d1 = dvofdy * norminv;
+            d2 = dvofdz * norminv;
+          }
         }
+        sc[ccur][0][lj][li] = d0;
+        sc[ccur][1][lj][li] = d1;
+        sc[ccur][2][lj][li] = d2;
       }
-      sc[ccur][0][lj][li] = d0;
-      sc[ccur][1][lj][li] = d1;
-      sc[ccur][2][lj][li] = d2;
+      __syncthreads();
     }
-    __syncthreads();
     // the corner plane kc's 2 x 2 stencils of this thread's cell column: the
     // upper plane of cell k = kc - 1 now, the lower plane of cell kc next
     // (carried in registers, so each is formed once, with the same operands
@@ -283,7 +310,7 @@ __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ 
     const int i = i0 + tx, j = j0 + ty;
     const bool cell = i <= nx && j <= ny + 1;
     R u_dx0 = R(0.), u_dy1 = R(0.), u_s0 = R(0.), u_s1 = R(0.), u_s2 = R(0.);
-    if (cell) {
+    if (cell && !flat_tile) {
 #define CU(m, a, b) sc[ccur][m][ty + (b)][tx + (a)]
       u_dx0 = plane_dx(CU(0, 0, 0), CU(0, 1, 0), CU(0, 0, 1), CU(0, 1, 1));
       u_dy1 = plane_dy(CU(1, 0, 0), CU(1, 1, 0), CU(1, 0, 1), CU(1, 1, 1));
@@ -337,8 +364,10 @@ __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ 
     l_s0 = u_s0;
     l_s1 = u_s1;
     l_s2 = u_s2;
-    __pipeline_wait_prior(0);
-    __syncthreads();
+    __pipeline_wait_prior(G3D - 1);  // plane kc + 1
+    const int zn = __syncthreads_and(kc + 1 <= kend ? my_zero((kc - k0 + 2) % G3S) : 1);
+    z_lo = z_hi;
+    z_hi = zn;
   }
 }
 
@@ -638,7 +667,7 @@ __global__ void __launch_bounds__(AX * AY, 4) k3_vof_advect(const double *__rest
       }
     }
     fz_lo = fz_hi;
-    __pipeline_wait_prior(0);
+    __pipeline_wait_prior(1);  // plane k + 2
     __syncthreads();
   }
 #undef VR
