@@ -63,7 +63,7 @@ int adj_ensure(svof_solver *s) {
   a->xs_smem = sizeof(double) * 2 * (size_t)r * nx;
   if (!bad && cudaSuccess != raise_smem_limit(k_adj_xsolve, a->xs_smem)) bad = true;
   // the forward transforms on an array right-hand side share the forward's shapes
-  if (!bad && s->uniform && cudaSuccess != raise_smem_limit(k_dct_fwd_rhs, dct_row_smem(nx))) bad = true;
+  if (!bad && s->uniform && cudaSuccess != dct_prepare(s->log2fft)) bad = true;
   if (!bad && !s->uniform &&
       cudaSuccess != raise_smem_limit(k_dft_fwd_rhs, sizeof(double) * 2 * (size_t)ny * s->dft_cols))
     bad = true;
@@ -108,16 +108,18 @@ int adj_potential(svof_solver *s, int rk, double dt) {
   const Grid2 g = s->grid();
   double pre_p;
   if (s->uniform) {
-    const int nthr = std::min(256, std::max(32, s->nx / 2));
-    const size_t smem = dct_row_smem(s->nx);
-    k_dct_fwd_rhs<<<s->ny, nthr, smem, s->stream>>>(a->psib.p, s->spec.p, s->twf.p, s->cs.p, s->log2fft, g);
+    const int L = s->log2fft;
+    const dim3 rows_grid((s->ny + dct_rows(L) - 1) / dct_rows(L));
+    dct_fwd_rhs_kernel(L)<<<rows_grid, dct_threads(L), dct_smem(L, false), s->stream>>>(a->psib.p, s->spec.p, s->twf.p,
+                                                                                    s->cs.p, g);
     CK_LAUNCH();
     const int kt = s->ysolve_kt;
     k_dct_ysolve<<<(s->nx + kt - 1) / kt, 128, sizeof(double) * 3 * kt * s->ny, s->stream>>>(
         s->spec.p, s->vt.p, s->rvt.p, s->q1t.p, s->ck.p, s->lastf.p, s->den.p, 1. / s->dy / s->dy, s->nx, s->ny,
         kt);
     CK_LAUNCH();
-    k_dct_inv<<<s->ny, nthr, smem, s->stream>>>(s->spec.p, a->psis.p, s->twb.p, s->cs.p, s->log2fft, g);
+    dct_inv_kernel(L)<<<rows_grid, dct_threads(L), dct_smem(L, true), s->stream>>>(s->spec.p, a->psis.p, s->twb.p,
+                                                                                 s->cs.p, g);
     CK_LAUNCH();
     pre_p = 1. / (gam * dt) / (2. * s->nx);
   } else {

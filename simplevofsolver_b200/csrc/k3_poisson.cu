@@ -19,11 +19,15 @@
 //   k3_pois_inv_y  a block owns COLS consecutive i of one plane k; writes psi
 //                  with its halo images and Neumann walls
 //
+//   k3_pois_resid  the FP64 residual b - L psi of a solve (the defect of an
+//                  FP32 pass), into a compact array
+//
 // Templates on R, the type of the spectrum, the twiddles and the transform
-// arithmetic; the x line solve computes in FP64.  Both the FP64 and the mixed
-// path instantiate R = double (the restatement's butterflies bit for bit):
-// one FP64 pass costs less than two FP32 passes of defect correction and
-// leaves the divergence at FP64 round-off.
+// arithmetic; the x line solve computes in FP64.  The FP64 and the mixed path
+// instantiate R = double (the restatement's butterflies bit for bit); the
+// defect-corrected form (SVOF3_MIXED_DC) instantiates R = float: an FP32
+// pass, the FP64 residual of its psi, a second FP32 pass on the residual,
+// accumulated into psi.
 #include <cuda_pipeline.h>
 
 #include <type_traits>
@@ -35,33 +39,16 @@
 namespace svof3 {
 
 using svof_fft_dev::bitrev;
+using svof_fft_dev::Cplx;
+using svof_fft_dev::fft_lines;
+using svof_fft_dev::fpad;
 
-template <class R>
-struct Cplx;
-template <>
-struct Cplx<double> {
-  using T = double2;
-  static __device__ __forceinline__ T make(double a, double b) { return make_double2(a, b); }
-};
-template <>
-struct Cplx<float> {
-  using T = float2;
-  static __device__ __forceinline__ T make(float a, float b) { return make_float2(a, b); }
-};
 
-// The transforms.  A block owns COLS lines of N = 2^L2N points (N a
-// compile-time constant): consecutive i of one plane k for y, of one ky for z.
-// The transform is the oracle's radix-2 decimation in time (same butterfly
-// pairs, same twiddles, same association) run in passes of up to three
-// stages.  In a pass a thread takes (line, group) pairs, lines fastest across
-// the lanes, loads the 2^NS points of its group, runs their butterflies in
-// registers and stores them.  The first pass reads its points (in bit-reversed
-// order) from global memory and the last one writes its results there, so a
-// warp's global accesses are runs of consecutive i; the passes between go
-// through shared memory, re / im separately, point p of line c at
-// c LD + p + p / 8 with LD = N + N / 8 + 1 odd, so the lanes of a half warp,
-// on distinct lines, fall on distinct banks.
-__device__ __forceinline__ int fpad(int p) { return p + (p >> 3); }
+// The transforms (the register-blocked passes of fft_device.cuh).  A block
+// owns COLS lines of N = 2^L2N points: consecutive i of one plane k for y, of
+// one ky for z.  The first pass reads its points from global memory and the
+// last one writes its results there, so a warp's global accesses are runs of
+// consecutive i.
 
 constexpr int kLineThreads = 256;
 // COLS: the widest of 16 / 8 / 4 lines whose shared memory stays within 80 KB
@@ -78,110 +65,14 @@ constexpr int line_minb(int smem) {
 template <class R, int L2N>
 struct Line {
   static constexpr int N = 1 << L2N;
-  static constexpr int LD = N + (N >> 3) + 1;
+  static constexpr int LD = svof_fft_dev::fft_ld(L2N);
   static constexpr int COL_BYTES = 2 * (int)sizeof(R) * LD;
   static constexpr int COLS = line_cols(COL_BYTES);
   static constexpr int SMEM = COLS * COL_BYTES;
   static constexpr int MINB = line_minb(SMEM);
 };
 
-// twiddle loads: read-only path, kept in L1 ahead of the streaming data
-__device__ __forceinline__ double2 tw_ld(const double2 *p) {
-  double2 v;
-  asm("ld.global.nc.L1::evict_last.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
-  return v;
-}
-__device__ __forceinline__ float2 tw_ld(const float2 *p) {
-  float2 v;
-  asm("ld.global.nc.L1::evict_last.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p));
-  return v;
-}
 
-// the butterflies of stages S0 .. S0 + NS - 1 of group gi, in registers
-template <class R, int L2N, int S0, int NS>
-__device__ __forceinline__ void butterflies(int gi, R *xr, R *xi, const R *__restrict__ tw) {
-  using C2 = typename Cplx<R>::T;
-  constexpr int G = 1 << NS, H = 1 << (S0 - 1);
-#pragma unroll
-  for (int t = 0; t < NS; t++) {
-    const int st_ = S0 + t, dist = 1 << t;
-#pragma unroll
-    for (int m = 0; m < G; m++) {
-      if (m & dist) continue;
-      // twiddle of the pair (base + m H, base + (m + dist) H) at stage st_
-      const int kk = (gi & (H - 1)) + (m & (dist - 1)) * H;
-      const C2 w = tw_ld(reinterpret_cast<const C2 *>(tw) + (kk << (L2N - st_)));
-      const R br = xr[m + dist], bi = xi[m + dist];
-      const R tr = w.x * br - w.y * bi;
-      const R ti = w.x * bi + w.y * br;
-      const R ur = xr[m], ui = xi[m];
-      xr[m] = ur + tr;
-      xi[m] = ui + ti;
-      xr[m + dist] = ur - tr;
-      xi[m + dist] = ui - ti;
-    }
-  }
-}
-
-// stages S0 .. S0 + NS - 1 of the block's COLS lines: ld(c, base, G, H, re,
-// im) fetches the G points base + m H (m < G) of line c into re[m], im[m],
-// st(c, base, G, H, re, im) stores them (G and H as integral constants)
-template <class R, int L2N, int COLS, int S0, int NS, class LdF, class StF>
-__device__ __forceinline__ void fft_pass(const R *__restrict__ tw, LdF ld, StF st) {
-  constexpr int G = 1 << NS, H = 1 << (S0 - 1), NG = (1 << L2N) >> NS, PAIRS = COLS * NG;
-  using GC = std::integral_constant<int, G>;
-  using HC = std::integral_constant<int, H>;
-#pragma unroll
-  for (int p0 = 0; p0 < PAIRS; p0 += kLineThreads) {
-    const int pr = p0 + (int)threadIdx.x;
-    if (0 == PAIRS % kLineThreads || pr < PAIRS) {
-      const int c = pr % COLS, gi = pr / COLS;
-      const int base = (gi & (H - 1)) + ((gi >> (S0 - 1)) << (S0 - 1 + NS));
-      R xr[G], xi[G];
-      ld(c, base, GC(), HC(), xr, xi);
-      butterflies<R, L2N, S0, NS>(gi, xr, xi, tw);
-      st(c, base, GC(), HC(), xr, xi);
-    }
-  }
-}
-
-// all passes: the first reads through `first`, the last writes through `last`
-template <class R, int L2N, int COLS, int S0 = 1, class FirstF, class LastF>
-__device__ __forceinline__ void fft_lines(R *__restrict__ re, R *__restrict__ im, const R *__restrict__ tw,
-                                          FirstF first, LastF last) {
-  constexpr int LD = Line<R, L2N>::LD;
-  constexpr int NS = (L2N - S0 + 1) < 3 ? (L2N - S0 + 1) : 3;
-  constexpr bool IS_FIRST = (1 == S0), IS_LAST = (S0 + NS > L2N);
-  auto lds = [&](int c, int base, auto gc, auto hc, R *xr, R *xi) {
-    constexpr int G = decltype(gc)::value, H = decltype(hc)::value;
-#pragma unroll
-    for (int m = 0; m < G; m++) {
-      xr[m] = re[c * LD + fpad(base + m * H)];
-      xi[m] = im[c * LD + fpad(base + m * H)];
-    }
-  };
-  auto sts = [&](int c, int base, auto gc, auto hc, const R *xr, const R *xi) {
-    constexpr int G = decltype(gc)::value, H = decltype(hc)::value;
-#pragma unroll
-    for (int m = 0; m < G; m++) {
-      re[c * LD + fpad(base + m * H)] = xr[m];
-      im[c * LD + fpad(base + m * H)] = xi[m];
-    }
-  };
-  if constexpr (IS_FIRST && IS_LAST) {
-    fft_pass<R, L2N, COLS, S0, NS>(tw, first, last);
-  } else if constexpr (IS_FIRST) {
-    fft_pass<R, L2N, COLS, S0, NS>(tw, first, sts);
-  } else if constexpr (IS_LAST) {
-    fft_pass<R, L2N, COLS, S0, NS>(tw, lds, last);
-  } else {
-    fft_pass<R, L2N, COLS, S0, NS>(tw, lds, sts);
-  }
-  if constexpr (!IS_LAST) {
-    __syncthreads();
-    fft_lines<R, L2N, COLS, S0 + NS>(re, im, tw, first, last);
-  }
-}
 
 // the right-hand side b = div u / (gamma dt ny nz) of every interior cell,
 // FP64, into a compact array (x fastest, nx ny per plane), with the
@@ -221,6 +112,34 @@ __global__ void __launch_bounds__(256, 4) k3_pois_b(const double *__restrict__ u
     const double div = +(x1[h] - x0[h]) / dx + (y1[h] - y0[h]) / g.dy + (zp[h] - uzk) / g.dz;
     uzk = zp[h];
     bo[bplane * (k - 1)] = prefactor * div;
+  }
+}
+
+// the residual r = b - L psi / (ny nz) of every interior cell, FP64, into a
+// compact array like b: L the operator the spectral solve inverts (x:
+// pl (psi(i-1) - psi) + pu (psi(i+1) - psi), the wall cells holding their
+// neighbour's value (Neumann); y, z: the periodic second differences over
+// the halo images); 1 / (ny nz) undoes the unnormalised transforms' scale
+// that b carries.  One thread per (i, j), kBPlanes planes.
+__global__ void __launch_bounds__(256, 4) k3_pois_resid(const double *__restrict__ b, const double *__restrict__ psi,
+                                                        double *__restrict__ r, const double *__restrict__ pl,
+                                                        const double *__restrict__ pu, Grid3 g) {
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k0 = 1 + blockIdx.z * kBPlanes;
+  if (i > nx || j > ny || k0 > nz) return;
+  const double l = ldg(pl + i - 1), u = ldg(pu + i - 1);
+  const double ry = 1. / (g.dy * g.dy), rz = 1. / (g.dz * g.dz);
+  const double scale = 1. / ((double)ny * (double)nz);
+  const size_t o = (i - 1) + (size_t)nx * (j - 1), bplane = (size_t)nx * ny;
+  for (int k = k0; k < min(k0 + kBPlanes, nz + 1); k++) {
+    const double pc = ldg(psi + ix_cc(g, i, j, k));
+    const double lx = l * (ldg(psi + ix_cc(g, i - 1, j, k)) - pc) + u * (ldg(psi + ix_cc(g, i + 1, j, k)) - pc);
+    const double lyy = ry * (ldg(psi + ix_cc(g, i, j - 1, k)) - 2. * pc + ldg(psi + ix_cc(g, i, j + 1, k)));
+    const double lzz = rz * (ldg(psi + ix_cc(g, i, j, k - 1)) - 2. * pc + ldg(psi + ix_cc(g, i, j, k + 1)));
+    const size_t q = o + bplane * (k - 1);
+    r[q] = ldg(b + q) - scale * (lx + lyy + lzz);
   }
 }
 
@@ -451,7 +370,10 @@ __global__ void __launch_bounds__(LPB) k3_pois_x(R *__restrict__ spec, R *__rest
 // X_{ny/2} ignored), psi of COLS consecutive i of plane k with the halo
 // images; the Neumann walls take the new neighbour value and hand
 // their old value to the halo images
-template <int L2N, class R>
+// ACC (the correction pass of the defect-corrected form): psi += the result,
+// the walls take their neighbour's new total and their halo images keep what
+// the first pass gave them
+template <int L2N, class R, bool ACC>
 __global__ void __launch_bounds__(kLineThreads, Line<R, L2N>::MINB)
     k3_pois_inv_y(const R *__restrict__ spec, double *__restrict__ psi, const R *__restrict__ tw, Grid3 g) {
   using L = Line<R, L2N>;
@@ -493,7 +415,10 @@ __global__ void __launch_bounds__(kLineThreads, Line<R, L2N>::MINB)
 #pragma unroll
     for (int q = 0; q < G; q++) {
       const double v = y[q];
-      for_images(base + q * H + 1, k, ny, nz, true, [&](int jj, int kk) { psi[ix_cc(g, i, jj, kk)] = v; });
+      for_images(base + q * H + 1, k, ny, nz, true, [&](int jj, int kk) {
+        if (ACC) psi[ix_cc(g, i, jj, kk)] += v;
+        else psi[ix_cc(g, i, jj, kk)] = v;
+      });
     }
   };
   fft_lines<R, L2N, COLS>(re, im, tw, first, last);
@@ -508,6 +433,10 @@ __global__ void __launch_bounds__(kLineThreads, Line<R, L2N>::MINB)
     if ((0 == side && !has_left) || (1 == side && !has_right)) continue;
     const int iw = side ? nx + 1 : 0;
     const double nv = psi[ix_cc(g, side ? nx : 1, j, k)];
+    if (ACC) {
+      psi[ix_cc(g, iw, j, k)] = nv;
+      continue;
+    }
     const double old = psi[ix_cc(g, iw, j, k)];
     psi[ix_cc(g, iw, j, k)] = nv;
     for_images(j, k, ny, nz, false, [&](int jj, int kk) { psi[ix_cc(g, iw, jj, kk)] = old; });
@@ -550,7 +479,8 @@ cudaError_t pois_prepare(int log2ny, int log2nz) {
     constexpr int sm = Line<R, L2>::SMEM;
     cudaError_t r;
     if (cudaSuccess != (r = line_attrs(k3_pois_fwd_y<L2, R>, sm))) return r;
-    return line_attrs(k3_pois_inv_y<L2, R>, sm);
+    if (cudaSuccess != (r = line_attrs(k3_pois_inv_y<L2, R, true>, sm))) return r;
+    return line_attrs(k3_pois_inv_y<L2, R, false>, sm);
   });
   if (cudaSuccess != e) return e;
   e = by_l2n(log2nz, [&](auto c) {
@@ -607,14 +537,33 @@ cudaError_t pois_x(cudaStream_t st, R *spec, R *scratch, const double *pl, const
 }
 
 template <class R>
-cudaError_t pois_inv_y(cudaStream_t st, const R *spec, double *psi, const R *tw, int log2n, Grid3 g) {
+cudaError_t pois_inv_y(cudaStream_t st, const R *spec, double *psi, const R *tw, int log2n, Grid3 g, bool acc) {
   return by_l2n(log2n, [&](auto c) {
     constexpr int L2 = decltype(c)::value;
     using L = Line<R, L2>;
     dim3 gr((g.nx + L::COLS - 1) / L::COLS, g.nz);
-    k3_pois_inv_y<L2, R><<<gr, kLineThreads, L::SMEM, st>>>(spec, psi, tw, g);
+    if (acc) k3_pois_inv_y<L2, R, true><<<gr, kLineThreads, L::SMEM, st>>>(spec, psi, tw, g);
+    else k3_pois_inv_y<L2, R, false><<<gr, kLineThreads, L::SMEM, st>>>(spec, psi, tw, g);
     return cudaGetLastError();
   });
+}
+
+template <class R>
+cudaError_t pois_fwd_y_array(cudaStream_t st, const double *b, R *spec, const R *tw, int log2n, Grid3 g) {
+  return by_l2n(log2n, [&](auto c) {
+    constexpr int L2 = decltype(c)::value;
+    using L = Line<R, L2>;
+    dim3 gr((g.nx + L::COLS - 1) / L::COLS, g.nz);
+    k3_pois_fwd_y<L2, R><<<gr, kLineThreads, L::SMEM, st>>>(b, spec, tw, g);
+    return cudaGetLastError();
+  });
+}
+
+cudaError_t pois_resid(cudaStream_t st, const double *b, const double *psi, double *r, const double *pl,
+                       const double *pu, Grid3 g) {
+  const dim3 bb(32, 8), bg((g.nx + 31) / 32, (g.ny + 7) / 8, (g.nz + kBPlanes - 1) / kBPlanes);
+  k3_pois_resid<<<bg, bb, 0, st>>>(b, psi, r, pl, pu, g);
+  return cudaGetLastError();
 }
 
 #define SVOF3_POISSON_INST(R)                                                                                    \
@@ -624,8 +573,10 @@ cudaError_t pois_inv_y(cudaStream_t st, const R *spec, double *psi, const R *tw,
   template cudaError_t pois_z<R>(cudaStream_t, R *, const R *, int, Grid3);                                      \
   template cudaError_t pois_x<R>(cudaStream_t, R *, R *, const double *, const double *, const double *,        \
                                  const double *, Grid3);                                                         \
-  template cudaError_t pois_inv_y<R>(cudaStream_t, const R *, double *, const R *, int, Grid3);
+  template cudaError_t pois_inv_y<R>(cudaStream_t, const R *, double *, const R *, int, Grid3, bool);          \
+  template cudaError_t pois_fwd_y_array<R>(cudaStream_t, const double *, R *, const R *, int, Grid3);
 SVOF3_POISSON_INST(double)
+SVOF3_POISSON_INST(float)
 #undef SVOF3_POISSON_INST
 
 }  // namespace svof3

@@ -19,8 +19,11 @@
 // The transforms are the radix-2 decimation-in-time FFT of the oracle
 // (oracle/svof_fft.c) with the same butterflies and the same twiddle tables,
 // so with FMA contraction disabled they agree with it bit for bit.  Lengths
-// must be powers of two.
+// must be powers of two (the DCT path's row transforms: 4 .. 4096 points).
+#include <type_traits>
+
 #include "fft_device.cuh"
+#include "smem_limit.cuh"
 #include "svof_internal.cuh"
 
 namespace svof {
@@ -61,50 +64,86 @@ struct ArrayRhs {
 };
 
 // ---------------------------------------------------------------- DCT path
-// row j of the right-hand side, FFTW_REDFT10 along x into spec; the block's
-// dynamic shared memory holds 2 nx doubles
-template <class Rhs>
-__device__ __forceinline__ void dct_fwd_row(const Rhs &rhs, double *__restrict__ spec, const double *__restrict__ tw,
-                                            const double *__restrict__ cs, int log2n, int n, int j) {
-  extern __shared__ double z[];  // [2n] transform, [n] right-hand side, [n] twiddles (n/2 pairs)
-  double *r = z + 2 * n, *stw = r + n;
-  // the row's right-hand side and the twiddles, read in order (coalesced)
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    r[i] = rhs(i + 1, j);
-    stw[i] = tw[i];
+// A block owns DctShape<L2N>::ROWS consecutive rows j (N = nx = 2^L2N points
+// each; THREADS threads, pairs of (row, butterfly group) across the lanes)
+// and runs their transforms as the register-blocked passes of fft_device.cuh:
+// the same butterflies, twiddles and stage order as the oracle, three stages
+// per pass between shared-memory round trips.  Dynamic shared memory: re / im
+// (ROWS fft_ld(L2N) each), the rows' input (ROWS N) and, for the inverse, the
+// rows' output (ROWS N).
+// ROWS: one row up to 256 points (those grids have few rows: one block per
+// row keeps the SMs busy), then 2048 / N; THREADS: the first pass's pairs,
+// 32 .. 256
+template <int L2N>
+struct DctShape {
+  static constexpr int N = 1 << L2N;
+  static constexpr int ROWS = (L2N <= 8 || (2048 >> L2N) < 1) ? 1 : (2048 >> L2N);
+  static constexpr int PAIRS = ROWS * (N >> (L2N < 3 ? L2N : 3));
+  static constexpr int THREADS = PAIRS < 32 ? 32 : (PAIRS > 256 ? 256 : (PAIRS + 31) / 32 * 32);
+  static constexpr int LD = svof_fft_dev::fft_ld(L2N);
+  static constexpr size_t SMEM_FWD = sizeof(double) * ROWS * (2 * (size_t)LD + N);
+  static constexpr size_t SMEM_INV = sizeof(double) * ROWS * (2 * (size_t)LD + 2 * N);
+};
+
+// rows j0 .. j0 + ROWS - 1 of the right-hand side, FFTW_REDFT10 along x into
+// spec (Makhoul: v_m = x_{2m}, v_{n-1-m} = x_{2m+1}, an FFT of v, then
+// 2 Re(w_k V_k) with the pre/post twiddles cs)
+template <int L2N, class Rhs>
+__device__ __forceinline__ void dct_fwd_rows(const Rhs &rhs, double *__restrict__ spec,
+                                             const double *__restrict__ tw, const double *__restrict__ cs, int ny) {
+  using S = DctShape<L2N>;
+  constexpr int N = S::N, ROWS = S::ROWS, LD = S::LD;
+  extern __shared__ double dsm[];
+  double *re = dsm, *im = re + ROWS * LD, *rr = im + ROWS * LD;  // rr [ROWS][N]
+  const int j0 = 1 + blockIdx.x * ROWS;
+  const int nr = min(ROWS, ny - j0 + 1);
+  // the rows' right-hand sides, read in order (coalesced)
+  for (int w = threadIdx.x; w < ROWS * N; w += S::THREADS) {
+    const int c = w >> L2N, i = w & (N - 1);
+    rr[w] = (c < nr) ? rhs(i + 1, j0 + c) : 0.;
   }
   __syncthreads();
-  // Makhoul reordering v_m = x_{2m}, v_{n-1-m} = x_{2m+1}, stored bit-reversed
-  for (int q = threadIdx.x; q < n; q += blockDim.x) {
-    const int m = bitrev(q, log2n);
-    const int src = (m < n / 2) ? 2 * m : 2 * (n - 1 - m) + 1;
-    z[2 * q] = r[src];
-    z[2 * q + 1] = 0.;
-  }
-  __syncthreads();
-  fft_stages(z, log2n, 1, stw);
-  double *out = spec + (size_t)(j - 1) * n;
-  for (int k = threadIdx.x; k < n; k += blockDim.x) {
-    const double c = cs[2 * k], s = cs[2 * k + 1];
-    out[k] = 2.0 * (c * z[2 * k] + s * z[2 * k + 1]);
-  }
+  // point p of the bit-reversed FFT input holds v_m, m = bitrev(p)
+  auto first = [&](int c, int base, auto gc, auto hc, double *xr, double *xi) {
+    constexpr int G = decltype(gc)::value, H = decltype(hc)::value;
+#pragma unroll
+    for (int q = 0; q < G; q++) {
+      const int m = bitrev(base + q * H, L2N);
+      const int src = (m < N / 2) ? 2 * m : 2 * (N - 1 - m) + 1;
+      xr[q] = rr[c * N + src];
+      xi[q] = 0.;
+    }
+  };
+  auto last = [&](int c, int base, auto gc, auto hc, const double *xr, const double *xi) {
+    constexpr int G = decltype(gc)::value, H = decltype(hc)::value;
+    if (c >= nr) return;
+    double *out = spec + (size_t)(j0 + c - 1) * N;
+#pragma unroll
+    for (int q = 0; q < G; q++) {
+      const int k = base + q * H;
+      const double2 w = __ldg(reinterpret_cast<const double2 *>(cs) + k);
+      out[k] = 2.0 * (w.x * xr[q] + w.y * xi[q]);
+    }
+  };
+  svof_fft_dev::fft_lines<double, L2N, ROWS, 1, S::THREADS>(re, im, tw, first, last);
 }
 
-// one block per row j; dynamic shared memory 2 nx doubles
-__global__ void k_dct_fwd(const double *__restrict__ ux, const double *__restrict__ uy,
-                          double *__restrict__ spec, const double *__restrict__ tw,
-                          const double *__restrict__ cs, const double *__restrict__ dtp,
-                          double gam, int log2n, Grid2 g) {
+template <int L2N>
+__global__ void __launch_bounds__(DctShape<L2N>::THREADS) k_dct_fwd(const double *__restrict__ ux, const double *__restrict__ uy,
+                                                        double *__restrict__ spec, const double *__restrict__ tw,
+                                                        const double *__restrict__ cs, const double *__restrict__ dtp,
+                                                        double gam, Grid2 g) {
   pdl_enter();
-  const int n = g.nx;
   const double dt = *dtp;
-  const double prefactor = 1. / (gam * dt) / (2. * n);
-  dct_fwd_row(DivRhs{ux, uy, g, prefactor}, spec, tw, cs, log2n, n, 1 + blockIdx.x);
+  const double prefactor = 1. / (gam * dt) / (2. * (1 << L2N));
+  dct_fwd_rows<L2N>(DivRhs{ux, uy, g, prefactor}, spec, tw, cs, g.ny);
 }
 
-__global__ void k_dct_fwd_rhs(const double *__restrict__ r, double *__restrict__ spec, const double *__restrict__ tw,
-                              const double *__restrict__ cs, int log2n, Grid2 g) {
-  dct_fwd_row(ArrayRhs{r, g.dxf, g.nx}, spec, tw, cs, log2n, g.nx, 1 + blockIdx.x);
+template <int L2N>
+__global__ void __launch_bounds__(DctShape<L2N>::THREADS) k_dct_fwd_rhs(const double *__restrict__ r, double *__restrict__ spec,
+                                                            const double *__restrict__ tw,
+                                                            const double *__restrict__ cs, Grid2 g) {
+  dct_fwd_rows<L2N>(ArrayRhs{r, g.dxf, g.nx}, spec, tw, cs, g.ny);
 }
 
 // periodic tri-diagonal solve along y per wavenumber k (src/tdm.c:78-99 with
@@ -183,58 +222,129 @@ __global__ void k_dct_ysolve(double *__restrict__ spec, const double *__restrict
   }
 }
 
-// one block per row j: REDFT01 then extract_output + fluid_update_boundaries_psi
-__global__ void k_dct_inv(const double *__restrict__ spec, double *__restrict__ psi,
-                          const double *__restrict__ tw, const double *__restrict__ cs,
-                          int log2n, Grid2 g) {
+// rows j0 .. j0 + ROWS - 1: REDFT01 then extract_output +
+// fluid_update_boundaries_psi (the pre-twiddle pairs spectrum k and n - k;
+// FFT point p is output position 2p below n/2, 2(n-1-p)+1 above)
+template <int L2N>
+__global__ void __launch_bounds__(DctShape<L2N>::THREADS) k_dct_inv(const double *__restrict__ spec, double *__restrict__ psi,
+                                                        const double *__restrict__ tw, const double *__restrict__ cs,
+                                                        Grid2 g) {
   pdl_enter();
-  extern __shared__ double z[];  // [2n] transform, [n] spectrum row, [n] twiddles (n/2 pairs)
-  const int n = g.nx, nx = g.nx, ny = g.ny;
-  const int j = 1 + blockIdx.x;
-  double *in = z + 2 * n, *stw = in + n;
-  // old wall values of the rows that feed the halo (read before any write)
-  double wl = 0., wr = 0.;
-  if (0 == threadIdx.x && (1 == j || ny == j)) {
-    wl = psi[ix_cc(nx, 0, j)];
-    wr = psi[ix_cc(nx, nx + 1, j)];
+  using S = DctShape<L2N>;
+  constexpr int N = S::N, ROWS = S::ROWS, LD = S::LD;
+  extern __shared__ double dsm[];
+  double *re = dsm, *im = re + ROWS * LD, *in = im + ROWS * LD, *ro = in + ROWS * N;  // in, ro [ROWS][N]
+  __shared__ double wold[4];  // old wall values of rows 1 and ny (left, right)
+  const int nx = g.nx, ny = g.ny;
+  const int j0 = 1 + blockIdx.x * ROWS;
+  const int nr = min(ROWS, ny - j0 + 1);
+  // old wall values of the rows that feed the halo, read before any write
+  if (threadIdx.x < 4) {
+    const int row = (threadIdx.x < 2) ? 1 : ny, side = threadIdx.x & 1;
+    if (row >= j0 && row < j0 + nr) wold[threadIdx.x] = psi[ix_cc(nx, side ? nx + 1 : 0, row)];
   }
-  // the spectrum row and the twiddles, read in order (coalesced)
-  const double *row = spec + (size_t)(j - 1) * n;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    in[i] = row[i];
-    stw[i] = tw[i];
-  }
-  __syncthreads();
-  for (int q = threadIdx.x; q < n; q += blockDim.x) {
-    const int m = bitrev(q, log2n);
-    const double a = in[m];
-    const double b = (0 == m) ? 0. : in[n - m];
-    const double c = cs[2 * m], s = cs[2 * m + 1];
-    z[2 * q] = c * a + s * b;
-    z[2 * q + 1] = s * a - c * b;
+  // the spectrum rows, read in order (coalesced)
+  for (int w = threadIdx.x; w < ROWS * N; w += S::THREADS) {
+    const int c = w >> L2N;
+    in[w] = (c < nr) ? spec[(size_t)(j0 - 1) * N + w] : 0.;
   }
   __syncthreads();
-  fft_stages(z, log2n, 1, stw);
-  for (int o = threadIdx.x; o < n; o += blockDim.x) {
-    const double y = (0 == (o & 1)) ? z[2 * (o >> 1)] : z[2 * (n - 1 - (o >> 1))];
-    const int i = o + 1;
+  auto first = [&](int c, int base, auto gc, auto hc, double *xr, double *xi) {
+    constexpr int G = decltype(gc)::value, H = decltype(hc)::value;
+#pragma unroll
+    for (int q = 0; q < G; q++) {
+      const int m = bitrev(base + q * H, L2N);
+      const double a = in[c * N + m];
+      const double b = (0 == m) ? 0. : in[c * N + N - m];
+      const double2 w = __ldg(reinterpret_cast<const double2 *>(cs) + m);
+      xr[q] = w.x * a + w.y * b;
+      xi[q] = w.y * a - w.x * b;
+    }
+  };
+  auto last = [&](int c, int base, auto gc, auto hc, const double *xr, const double *) {
+    constexpr int G = decltype(gc)::value, H = decltype(hc)::value;
+#pragma unroll
+    for (int q = 0; q < G; q++) {
+      const int p = base + q * H;
+      const int o = (p < N / 2) ? 2 * p : 2 * (N - 1 - p) + 1;
+      ro[c * N + o] = xr[q];
+    }
+  };
+  svof_fft_dev::fft_lines<double, L2N, ROWS, 1, S::THREADS>(re, im, tw, first, last);
+  __syncthreads();
+  // psi rows with their halo images, written in order (coalesced)
+  for (int w = threadIdx.x; w < nr * N; w += S::THREADS) {
+    const int c = w >> L2N, i = (w & (N - 1)) + 1, j = j0 + c;
+    const double y = ro[w];
     psi[ix_cc(nx, i, j)] = y;
     if (ny == j) psi[ix_cc(nx, i, 0)] = y;
     if (1 == j) psi[ix_cc(nx, i, ny + 1)] = y;
   }
-  if (0 == threadIdx.x) {
+  // Neumann walls, psi.c:7-20 (the wall takes its neighbour), and the halo
+  // rows' wall cells, which take the walls' old values
+  for (int c = threadIdx.x; c < nr; c += S::THREADS) {
+    const int j = j0 + c;
+    psi[ix_cc(nx, 0, j)] = ro[c * N];
+    psi[ix_cc(nx, nx + 1, j)] = ro[c * N + N - 1];
     if (ny == j) {
-      psi[ix_cc(nx, 0, 0)] = wl;
-      psi[ix_cc(nx, nx + 1, 0)] = wr;
+      psi[ix_cc(nx, 0, 0)] = wold[2];
+      psi[ix_cc(nx, nx + 1, 0)] = wold[3];
     }
     if (1 == j) {
-      psi[ix_cc(nx, 0, ny + 1)] = wl;
-      psi[ix_cc(nx, nx + 1, ny + 1)] = wr;
+      psi[ix_cc(nx, 0, ny + 1)] = wold[0];
+      psi[ix_cc(nx, nx + 1, ny + 1)] = wold[1];
     }
-    // Neumann walls, psi.c:7-20
-    psi[ix_cc(nx, 0, j)] = z[0];
-    psi[ix_cc(nx, nx + 1, j)] = z[2 * (n - 1 - ((n - 1) >> 1))];
   }
+}
+
+// ---- launch plans of the DCT row transforms, by length
+namespace {
+template <class F>
+auto by_log2n(int l2n, F f) {
+  switch (l2n) {
+    case 2: return f(std::integral_constant<int, 2>());
+    case 3: return f(std::integral_constant<int, 3>());
+    case 4: return f(std::integral_constant<int, 4>());
+    case 5: return f(std::integral_constant<int, 5>());
+    case 6: return f(std::integral_constant<int, 6>());
+    case 7: return f(std::integral_constant<int, 7>());
+    case 8: return f(std::integral_constant<int, 8>());
+    case 9: return f(std::integral_constant<int, 9>());
+    case 10: return f(std::integral_constant<int, 10>());
+    case 11: return f(std::integral_constant<int, 11>());
+    default: return f(std::integral_constant<int, 12>());
+  }
+}
+}  // namespace
+
+bool dct_length_ok(int log2n) { return log2n >= kDctMinL2N && log2n <= kDctMaxL2N; }
+int dct_rows(int log2n) {
+  return by_log2n(log2n, [](auto c) { return DctShape<decltype(c)::value>::ROWS; });
+}
+int dct_threads(int log2n) {
+  return by_log2n(log2n, [](auto c) { return DctShape<decltype(c)::value>::THREADS; });
+}
+size_t dct_smem(int log2n, bool inverse) {
+  return by_log2n(log2n, [&](auto c) {
+    using S = DctShape<decltype(c)::value>;
+    return inverse ? S::SMEM_INV : S::SMEM_FWD;
+  });
+}
+DctFwdKernel dct_fwd_kernel(int log2n) {
+  return by_log2n(log2n, [](auto c) { return (DctFwdKernel)&k_dct_fwd<decltype(c)::value>; });
+}
+DctFwdRhsKernel dct_fwd_rhs_kernel(int log2n) {
+  return by_log2n(log2n, [](auto c) { return (DctFwdRhsKernel)&k_dct_fwd_rhs<decltype(c)::value>; });
+}
+DctInvKernel dct_inv_kernel(int log2n) {
+  return by_log2n(log2n, [](auto c) { return (DctInvKernel)&k_dct_inv<decltype(c)::value>; });
+}
+cudaError_t dct_prepare(int log2n) {
+  if (!dct_length_ok(log2n)) return cudaErrorInvalidValue;
+  cudaError_t e = raise_smem_limit(dct_fwd_kernel(log2n), dct_smem(log2n, false));
+  if (cudaSuccess == e) e = raise_smem_limit(dct_fwd_rhs_kernel(log2n), dct_smem(log2n, false));
+  if (cudaSuccess == e) e = raise_smem_limit(dct_inv_kernel(log2n), dct_smem(log2n, true));
+  return e;
 }
 
 // ---------------------------------------------------------------- DFT path

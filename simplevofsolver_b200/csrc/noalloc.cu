@@ -222,8 +222,13 @@ extern "C" int svof_poisson_dct_noalloc(const svof_params_t *prm, const double *
   const double gam = (rkstep == 0 ? 32. / 60. + 0. / 60.
                                   : rkstep == 1 ? 25. / 60. + -17. / 60. : 45. / 60. + -25. / 60.);
   const Grid2 g{nx, ny, dy, S + kDxf, S + kDxf};
-  const int nthr = nx / 2 < 32 ? 32 : (nx / 2 > 256 ? 256 : nx / 2);
-  k_dct_fwd<<<ny, nthr, dct_row_smem(nx), s>>>(ux, uy, S + kSpec, S + kTwf, S + kCs, S + kDt, gam, log2n, g);
+  // (the row transforms' shared-memory limits: raised once per length, as the
+  // allocating solver does)
+  e = dct_prepare(log2n);
+  if (cudaSuccess != e) return nfail("shared-memory limit of the row transforms", e);
+  const dim3 rows_grid((ny + dct_rows(log2n) - 1) / dct_rows(log2n));
+  dct_fwd_kernel(log2n)<<<rows_grid, dct_threads(log2n), dct_smem(log2n, false), s>>>(ux, uy, S + kSpec, S + kTwf, S + kCs,
+                                                                              S + kDt, gam, g);
   int kt = 32;
   while (kt > 4 && nx / kt < 148) kt >>= 1;
   while (kt > 1 && sizeof(double) * 3 * (size_t)ny * kt > 48 * 1024) kt >>= 1;
@@ -233,7 +238,7 @@ extern "C" int svof_poisson_dct_noalloc(const svof_params_t *prm, const double *
   if (cudaSuccess != e) return nfail("shared-memory limit of the y solve", e);
   k_dct_ysolve<<<(nx + kt - 1) / kt, 128, sizeof(double) * 3 * kt * ny, s>>>(
       S + kSpec, S + kVt, S + kRvt, S + kQ1t, S + kCk, S + kLastf, S + kDen, 1. / dy / dy, nx, ny, kt);
-  k_dct_inv<<<ny, nthr, dct_row_smem(nx), s>>>(S + kSpec, psi, S + kTwb, S + kCs, log2n, g);
+  dct_inv_kernel(log2n)<<<rows_grid, dct_threads(log2n), dct_smem(log2n, true), s>>>(S + kSpec, psi, S + kTwb, S + kCs, g);
   e = cudaGetLastError();
   if (cudaSuccess != e) return nfail("kernel launch", e);
   return 0;

@@ -241,16 +241,17 @@ int launch_potential(svof_solver *s, int rk, int want_dct) {
     return fail(want_dct ? "DCT Poisson path needs a uniform x grid" : "DFT path requested on a uniform grid");
   }
   if (s->uniform) {
-    const int nthr = std::min(256, std::max(32, s->nx / 2));
-    const size_t smem = dct_row_smem(s->nx);
-    CK(launch_k(s->pdl, k_dct_fwd, s->ny, nthr, smem, s->stream, s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->spec.p,
-                s->twf.p, s->cs.p, s->d_dt, gam, s->log2fft, g));
+    const int L = s->log2fft;
+    const dim3 rows_grid((s->ny + dct_rows(L) - 1) / dct_rows(L));
+    CK(launch_k(s->pdl, dct_fwd_kernel(L), rows_grid, dct_threads(L), dct_smem(L, false), s->stream,
+                (const double *)s->ux[s->cur_u].p, (const double *)s->uy[s->cur_u].p, s->spec.p,
+                (const double *)s->twf.p, (const double *)s->cs.p, (const double *)s->d_dt, gam, g));
     const int kt = s->ysolve_kt;
     CK(launch_k(s->pdl, k_dct_ysolve, (s->nx + kt - 1) / kt, 128, sizeof(double) * 3 * kt * s->ny, s->stream,
                 s->spec.p, s->vt.p, s->rvt.p, s->q1t.p, s->ck.p, s->lastf.p, s->den.p, 1. / s->dy / s->dy, s->nx,
                 s->ny, kt));
-    CK(launch_k(s->pdl, k_dct_inv, s->ny, nthr, smem, s->stream, s->spec.p, s->psi.p, s->twb.p, s->cs.p,
-                s->log2fft, g));
+    CK(launch_k(s->pdl, dct_inv_kernel(L), rows_grid, dct_threads(L), dct_smem(L, true), s->stream,
+                (const double *)s->spec.p, s->psi.p, (const double *)s->twb.p, (const double *)s->cs.p, g));
   } else {
     const int cols = s->dft_cols;
     const int blocks = (s->nx + cols - 1) / cols;
@@ -591,11 +592,11 @@ int engine_create(const svof_params_t *prm, const double *xf, const double *xc, 
         return fail("cudaFuncSetAttribute(k_predict_xsolve)"), bail();
     }
   }
-  // transforms: one row (DCT) or a tile of columns (DFT) per block
+  // transforms: rows (DCT) or a tile of columns (DFT) per block
   {
-    const size_t dct_smem = dct_row_smem(nx);
-    if (s->uniform && (cudaSuccess != raise_smem_limit(k_dct_fwd, dct_smem) ||
-                       cudaSuccess != raise_smem_limit(k_dct_inv, dct_smem)))
+    if (s->uniform && !dct_length_ok(s->log2fft))
+      return fail("svof_create: the DCT path takes nx = 4 .. 4096 (got %d)", nx), bail();
+    if (s->uniform && cudaSuccess != dct_prepare(s->log2fft))
       return fail("cudaFuncSetAttribute(k_dct_fwd, k_dct_inv)"), bail();
     int cols = 16;
     while (cols > 1 && sizeof(double) * 2 * (size_t)ny * cols > 100 * 1024) cols >>= 1;
@@ -604,7 +605,7 @@ int engine_create(const svof_params_t *prm, const double *xf, const double *xc, 
     if (!s->uniform && (cudaSuccess != raise_smem_limit(k_dft_fwd, dft_smem) ||
                         cudaSuccess != raise_smem_limit(k_dft_inv, dft_smem)))
       return fail("cudaFuncSetAttribute(k_dft_fwd, k_dft_inv)"), bail();
-    if ((s->uniform ? dct_row_smem(nx) : sizeof(double) * 2 * (size_t)ny) > 200 * 1024)
+    if (!s->uniform && sizeof(double) * 2 * (size_t)ny > 200 * 1024)
       return fail("svof_create: FFT length too large for one block"), bail();
   }
   // line solves: lines per block so that the blocks cover the SMs, within
@@ -935,17 +936,18 @@ int svof_profile_step(svof_solver_t *s, double *ms, int *launches, int nkinds) {
       const double gam = RK_A[rk] + RK_B[rk];
       const Grid2 g = s->grid();
       if (s->uniform) {
-        const int nthr = std::min(256, std::max(32, s->nx / 2));
-        const size_t smem = dct_row_smem(s->nx);
-        k_dct_fwd<<<s->ny, nthr, smem, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->spec.p, s->twf.p,
-                                                    s->cs.p, s->d_dt, gam, s->log2fft, g);
+        const int L = s->log2fft;
+        const dim3 rows_grid((s->ny + dct_rows(L) - 1) / dct_rows(L));
+        dct_fwd_kernel(L)<<<rows_grid, dct_threads(L), dct_smem(L, false), s->stream>>>(
+            s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->spec.p, s->twf.p, s->cs.p, s->d_dt, gam, g);
         rc = rc || mark(SVOF_K_POISSON_FWD);
         const int kt = s->ysolve_kt;
         k_dct_ysolve<<<(s->nx + kt - 1) / kt, 128, sizeof(double) * 3 * kt * s->ny, s->stream>>>(
             s->spec.p, s->vt.p, s->rvt.p, s->q1t.p, s->ck.p, s->lastf.p, s->den.p, 1. / s->dy / s->dy, s->nx,
             s->ny, kt);
         rc = rc || mark(SVOF_K_POISSON_SOLVE);
-        k_dct_inv<<<s->ny, nthr, smem, s->stream>>>(s->spec.p, s->psi.p, s->twb.p, s->cs.p, s->log2fft, g);
+        dct_inv_kernel(L)<<<rows_grid, dct_threads(L), dct_smem(L, true), s->stream>>>(s->spec.p, s->psi.p, s->twb.p,
+                                                                                     s->cs.p, g);
         rc = rc || mark(SVOF_K_POISSON_INV);
       } else {
         const int cols = s->dft_cols;

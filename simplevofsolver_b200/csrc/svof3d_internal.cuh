@@ -145,9 +145,9 @@ __global__ void k3_tdm_coef(const double *__restrict__ lap_ux, const double *__r
 // Poisson: spectral array S[kz][ky][i] (complex, i fastest)
 // Poisson stages (k3_poisson.cu), templates on R, the type of the spectrum,
 // the twiddles and the transform arithmetic; the FP64 and the mixed path
-// both use R = double.  The x line solve is FP64.  The transforms are
-// compiled for each length 2^1 .. 2^11 (log2n outside that range is an
-// invalid value).
+// use R = double, the defect-corrected mixed form R = float.  The x line
+// solve is FP64.  The transforms are compiled for each length 2^1 .. 2^11
+// (log2n outside that range is an invalid value).
 template <class R>
 cudaError_t pois_prepare(int log2ny, int log2nz);
 // (b: scratch of nx ny nz doubles for the right-hand side)
@@ -159,8 +159,16 @@ cudaError_t pois_z(cudaStream_t st, R *spec, const R *tw, int log2n, Grid3 g);
 template <class R>
 cudaError_t pois_x(cudaStream_t st, R *spec, R *scratch, const double *pl, const double *pu, const double *evy,
                    const double *evz, Grid3 g);
+// acc: psi += the result (the correction pass), the walls' halo images kept
 template <class R>
-cudaError_t pois_inv_y(cudaStream_t st, const R *spec, double *psi, const R *tw, int log2n, Grid3 g);
+cudaError_t pois_inv_y(cudaStream_t st, const R *spec, double *psi, const R *tw, int log2n, Grid3 g,
+                       bool acc = false);
+// the forward y transform of a right-hand side given as a compact array
+template <class R>
+cudaError_t pois_fwd_y_array(cudaStream_t st, const double *b, R *spec, const R *tw, int log2n, Grid3 g);
+// r = b - L psi / (ny nz), compact arrays of nx ny nz doubles (FP64)
+cudaError_t pois_resid(cudaStream_t st, const double *b, const double *psi, double *r, const double *pl,
+                       const double *pu, Grid3 g);
 
 // projection and pressure update, in place
 __global__ void k3_project(double *__restrict__ ux, double *__restrict__ uy, double *__restrict__ uz,

@@ -112,21 +112,31 @@ __global__ void k_predict_xsolve(const double *__restrict__ coef, double *__rest
 inline size_t predict_xsolve_smem(int nx) { return sizeof(double) * ((size_t)4 * 64 * 32 + 3 * (size_t)nx); }
 __global__ void k_predict_update(PredictArgs a, const double *__restrict__ fw);
 
-// Poisson, DCT path (src/fluid/compute_potential/dct.c); k_dct_fwd,
-// k_dct_fwd_rhs and k_dct_inv take dct_row_smem(nx) bytes of dynamic shared
-// memory (the transform, the row and the twiddles)
-inline size_t dct_row_smem(int nx) { return sizeof(double) * 4 * (size_t)nx; }
-__global__ void k_dct_fwd(const double *__restrict__ ux, const double *__restrict__ uy,
-                          double *__restrict__ spec, const double *__restrict__ tw,
-                          const double *__restrict__ cs, const double *__restrict__ dtp,
-                          double gam, int log2n, Grid2 g);
+// Poisson, DCT path (src/fluid/compute_potential/dct.c).  The row transforms
+// (k_dct_fwd: divergence right-hand side + REDFT10; k_dct_fwd_rhs: the same
+// on an array right-hand side r[j-1][i-1] / dxf[i-1], the adjoint's second
+// solve; k_dct_inv: REDFT01 + psi rows with halo and walls) are compiled per
+// length nx = 2^log2n, log2n in [kDctMinL2N, kDctMaxL2N]: dct_threads(log2n)
+// threads, dct_rows(log2n) rows per block (grid ceil(ny / rows)),
+// dct_smem(log2n, inverse) bytes of dynamic shared memory; dct_prepare raises
+// those limits.
+constexpr int kDctMinL2N = 2, kDctMaxL2N = 12;
+using DctFwdKernel = void (*)(const double *, const double *, double *, const double *, const double *,
+                              const double *, double, Grid2);
+using DctFwdRhsKernel = void (*)(const double *, double *, const double *, const double *, Grid2);
+using DctInvKernel = void (*)(const double *, double *, const double *, const double *, Grid2);
+bool dct_length_ok(int log2n);
+int dct_rows(int log2n);
+int dct_threads(int log2n);
+size_t dct_smem(int log2n, bool inverse);
+DctFwdKernel dct_fwd_kernel(int log2n);
+DctFwdRhsKernel dct_fwd_rhs_kernel(int log2n);
+DctInvKernel dct_inv_kernel(int log2n);
+cudaError_t dct_prepare(int log2n);
 __global__ void k_dct_ysolve(double *__restrict__ spec, const double *__restrict__ vt,
                              const double *__restrict__ rvt, const double *__restrict__ q1t,
                              const double *__restrict__ ck, const double *__restrict__ lastf,
                              const double *__restrict__ den, double lap, int nx, int ny, int kt);
-__global__ void k_dct_inv(const double *__restrict__ spec, double *__restrict__ psi,
-                          const double *__restrict__ tw, const double *__restrict__ cs,
-                          int log2n, Grid2 g);
 // Poisson, DFT path (src/fluid/compute_potential/dft.c)
 __global__ void k_dft_fwd(const double *__restrict__ ux, const double *__restrict__ uy,
                           double *__restrict__ spec, const double *__restrict__ tw,
@@ -138,11 +148,9 @@ __global__ void k_dft_xsolve(double *__restrict__ spec, const double *__restrict
 __global__ void k_dft_inv(const double *__restrict__ spec, double *__restrict__ psi,
                           const double *__restrict__ tw, int log2n, int cols, Grid2 g);
 
-// the forward transforms of the two paths on a right-hand side r[j-1][i-1] /
+// the DFT path's forward transform on a right-hand side r[j-1][i-1] /
 // dxf[i-1] (the adjoint's second Poisson solve, with the grid-metric weights
-// of the x grid); same launch shapes
-__global__ void k_dct_fwd_rhs(const double *__restrict__ r, double *__restrict__ spec, const double *__restrict__ tw,
-                              const double *__restrict__ cs, int log2n, Grid2 g);
+// of the x grid); k_dft_fwd's launch shape
 __global__ void k_dft_fwd_rhs(const double *__restrict__ r, double *__restrict__ spec, const double *__restrict__ tw,
                               int log2n, int cols, Grid2 g);
 
