@@ -26,7 +26,9 @@ The 3D line also carries the differentiation form's cost ("adjoint",
 "adjoint_over_forward"): on its workload (falling droplet, 256 x 256, 200
 steps, checkpoints every 20) the device time per step of the backward pass
 (segment recompute with tapes plus the CUDA step adjoints) over that of the
-forward (--no-adjoint skips it).
+forward (--no-adjoint skips it), and the defect-corrected mixed form
+("mixed_dc": the Poisson solve as two FP32 passes with an FP64 residual,
+its throughput and its error against the FP64 path; --no-dc skips it).
 
 --impl reference times the reference's own C implementation (its src/*.c
 compiled against single-rank shims, oracle/_ref) on all host cores: one
@@ -447,7 +449,8 @@ def run3d(args, wl, ic, env, world, rank, local_rank):
     dxf = np.diff(ic.xf)
     vol0 = float(np.sum(ic.vof[:, :, 1:-1] * dxf)) * (ic.ly / ic.ny) * (ic.lz / ic.nz)
     res = {}
-    for prec in ("fp64", "mixed"):
+    precs = ("fp64", "mixed") if args.no_dc else ("fp64", "mixed", "mixed_dc")
+    for prec in precs:
         solver = svof.Solver3D(ic, phys, precision=prec)
         solver.run(args.warmup)
         torch.cuda.synchronize()
@@ -455,7 +458,7 @@ def run3d(args, wl, ic, env, world, rank, local_rank):
         diag = solver.diagnostics()
         fields = {k: solver.interior(k) for k in ("ux", "uy", "uz", "p", "vof")}
         prof = _profile(solver, 3)
-        alg = ALG_BYTES_3D_MIXED if prec == "mixed" else {k: 8.0 * v for k, v in ALG_WORDS_3D.items()}
+        alg = ALG_BYTES_3D_MIXED if prec != "fp64" else {k: 8.0 * v for k, v in ALG_WORDS_3D.items()}
         step_alg = sum(alg[k] * (v[1] / 3) / KERNELS_PER_KIND_3D.get(k, 1) for k, v in prof.items())
         res[prec] = dict(total_ms=total_ms, clocks=clocks, diag=diag, fields=fields, prof=prof,
                          value=_aggregate(cells, args.steps, world, total_ms),
@@ -513,24 +516,38 @@ def run3d(args, wl, ic, env, world, rank, local_rank):
         solver.close()
         torch.cuda.synchronize()
     m, f = res["mixed"], res["fp64"]
-    err = {}
     w = dxf[None, None, :]  # cell volumes up to the uniform dy * dz
-    for k in ("ux", "uy", "uz", "p", "vof"):
-        a, b = m["fields"][k][:, :, 1:-1], f["fields"][k][:, :, 1:-1]
-        if k == "p":
-            # the pressure's additive constant is fixed by round-off in both
-            # paths: compare modulo the volume-weighted mean
-            a = a - float(np.sum(a * w) / (np.sum(w) * a.shape[0] * a.shape[1]))
-            b = b - float(np.sum(b * w) / (np.sum(w) * b.shape[0] * b.shape[1]))
-        d = a - b
-        err[f"{k}_rel_l2"] = float(np.linalg.norm(d.ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
-        err[f"{k}_max_rel"] = float(np.abs(d).max() / max(np.abs(b).max(), 1e-300))
-        del a, b, d
-    err["divmax"] = m["diag"]["divmax"]
-    err["volume_drift"] = abs(m["diag"]["volume"] - vol0) / vol0
-    err["fp64_divmax"] = f["diag"]["divmax"]
-    err["fp64_volume_drift"] = abs(f["diag"]["volume"] - vol0) / vol0
-    err["after_steps"] = args.warmup + args.steps
+
+    def error_vs_fp64(m):
+        err = {}
+        for k in ("ux", "uy", "uz", "p", "vof"):
+            a, b = m["fields"][k][:, :, 1:-1], f["fields"][k][:, :, 1:-1]
+            if k == "p":
+                # the pressure's additive constant is fixed by round-off in
+                # both paths: compare modulo the volume-weighted mean
+                a = a - float(np.sum(a * w) / (np.sum(w) * a.shape[0] * a.shape[1]))
+                b = b - float(np.sum(b * w) / (np.sum(w) * b.shape[0] * b.shape[1]))
+            d = a - b
+            err[f"{k}_rel_l2"] = float(np.linalg.norm(d.ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+            err[f"{k}_max_rel"] = float(np.abs(d).max() / max(np.abs(b).max(), 1e-300))
+            del a, b, d
+        err["divmax"] = m["diag"]["divmax"]
+        err["volume_drift"] = abs(m["diag"]["volume"] - vol0) / vol0
+        err["fp64_divmax"] = f["diag"]["divmax"]
+        err["fp64_volume_drift"] = abs(f["diag"]["volume"] - vol0) / vol0
+        err["after_steps"] = args.warmup + args.steps
+        return err
+
+    err = error_vs_fp64(m)
+    dc = None
+    if "mixed_dc" in res:
+        d_ = res["mixed_dc"]
+        dc = {"value": d_["value"], "unit": METRIC, "ms_per_step": d_["total_ms"] / args.steps,
+              "over_fp64": d_["value"] / f["value"], "over_mixed": d_["value"] / m["value"],
+              "poisson": "two FP32 passes (r2c-y, dft-z, FP32 spectrum; x line solve computing in FP64) with "
+                         "the FP64 residual of the first as the second's right-hand side",
+              "error": error_vs_fp64(d_),
+              "kernel_ms_per_step": {k: v[0] / 3 for k, v in d_["prof"].items()}, "clocks": d_["clocks"]}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -569,6 +586,7 @@ def run3d(args, wl, ic, env, world, rank, local_rank):
                      "clocks": f["clocks"]},
             "mixed_over_fp64": m["value"] / f["value"],
             "mixed_error": err,
+            "mixed_dc": dc,
             "e2e": m["e2e"],
             "gpu_launches": KERNELS_PER_STEP_3D_MIXED * args.steps,
             "roofline": dict(m["roofline"], traffic=_traffic(args.workload, "mixed", m["roofline"]["kernel"]),
@@ -598,6 +616,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample-steps", type=int, default=None)
     ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiation form's cost")
+    ap.add_argument("--no-dc", action="store_true",
+                    help="skip the defect-corrected mixed form (FP32 Poisson passes) in the 3D workloads")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     three_d = args.workload in WORKLOADS3D

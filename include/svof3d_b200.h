@@ -46,7 +46,7 @@ typedef struct {
   double uy_xm, uy_xp;          /* wall values of uy at x = 0, lx */
   double uz_xm, uz_xp;          /* wall values of uz */
   double t_xm, t_xp;            /* wall values of t */
-  int precision;                /* SVOF3_FP64 or SVOF3_MIXED */
+  int precision;                /* SVOF3_FP64, SVOF3_MIXED or SVOF3_MIXED_DC */
 } svof3d_params_t;
 
 /* precision of svof3d_params_t:
@@ -59,8 +59,14 @@ typedef struct {
  *                solves, the vof update and the whole Poisson solve (the
  *                FP64 path's kernels, one pass) in FP64.  Fields stored in
  *                FP32 are converted to FP64 by svof3d_download_field / from
- *                FP64 by svof3d_upload_field. */
-enum { SVOF3_FP64 = 0, SVOF3_MIXED = 1 };
+ *                FP64 by svof3d_upload_field.
+ *   SVOF3_MIXED_DC as SVOF3_MIXED, with the Poisson solve in the form of a
+ *                defect correction: an FP32 pass (FP32 spectrum, twiddles
+ *                and transforms; the x line solve computing in FP64), the
+ *                FP64 residual of its psi against the operator the solve
+ *                inverts, and a second FP32 pass on the residual added to
+ *                psi. */
+enum { SVOF3_FP64 = 0, SVOF3_MIXED = 1, SVOF3_MIXED_DC = 2 };
 
 enum {
   SVOF3_UX = 0,

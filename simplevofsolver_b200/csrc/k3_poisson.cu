@@ -227,6 +227,12 @@ __global__ void __launch_bounds__(kLineThreads, Line<R, L2N>::MINB)
 // cp.async (a warp's copies are runs of XC consecutive points of two lines):
 // forward (values back into S, v into scratch), then back substitution in
 // reverse chunk order.  The spectrum and the scratch of v are R.
+// gauge0 (the FP32 passes of the defect-corrected solve): the line of the
+// mode ky = kz = 0, whose Neumann system is singular, takes the gauge
+// psi_hat(last) = 0 instead of the quotient by its round-off-sized last
+// pivot (the FP64 path's choice, the reference's, whose solution then
+// carries a large constant that FP32 storage of the line cannot resolve);
+// psi changes by a constant only.
 constexpr int XC = 16;
 template <class R, int LPB>
 struct XShape {
@@ -239,7 +245,7 @@ template <class R, int LPB>
 __global__ void __launch_bounds__(LPB) k3_pois_x(R *__restrict__ spec, R *__restrict__ scratch,
                                                  const double *__restrict__ pl, const double *__restrict__ pu,
                                                  const double *__restrict__ evy, const double *__restrict__ evz,
-                                                 Grid3 g) {
+                                                 Grid3 g, int gauge0) {
   using C2 = typename Cplx<R>::T;
   using S = XShape<R, LPB>;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -319,7 +325,7 @@ __global__ void __launch_bounds__(LPB) k3_pois_x(R *__restrict__ spec, R *__rest
           qi = val * (xi - l * qi);
         } else {
           const double val = c - l * vprev;
-          if (fabs(val) > kDblEpsilon) {
+          if (fabs(val) > kDblEpsilon && !(gauge0 && 0 == l0 + t)) {
             qr = 1. / val * (xr - l * qr);
             qi = 1. / val * (xi - l * qi);
           } else {
@@ -524,14 +530,15 @@ inline bool pois_x_narrow(long nlines) { return nlines < 148L * 4 * 128; }
 
 template <class R>
 cudaError_t pois_x(cudaStream_t st, R *spec, R *scratch, const double *pl, const double *pu, const double *evy,
-                   const double *evz, Grid3 g) {
+                   const double *evz, Grid3 g, bool gauge0) {
   const long nlines = (long)(g.ny / 2 + 1) * g.nz;
+  const int gz = gauge0 ? 1 : 0;
   if (pois_x_narrow(nlines)) {
     k3_pois_x<R, 64><<<(unsigned)((nlines + 63) / 64), 64, XShape<R, 64>::SMEM, st>>>(spec, scratch, pl, pu, evy,
-                                                                                      evz, g);
+                                                                                      evz, g, gz);
   } else {
     k3_pois_x<R, 128><<<(unsigned)((nlines + 127) / 128), 128, XShape<R, 128>::SMEM, st>>>(spec, scratch, pl, pu,
-                                                                                          evy, evz, g);
+                                                                                          evy, evz, g, gz);
   }
   return cudaGetLastError();
 }
@@ -572,7 +579,7 @@ cudaError_t pois_resid(cudaStream_t st, const double *b, const double *psi, doub
                                      const R *, const double *, double, int, Grid3);                            \
   template cudaError_t pois_z<R>(cudaStream_t, R *, const R *, int, Grid3);                                      \
   template cudaError_t pois_x<R>(cudaStream_t, R *, R *, const double *, const double *, const double *,        \
-                                 const double *, Grid3);                                                         \
+                                 const double *, Grid3, bool);                                                         \
   template cudaError_t pois_inv_y<R>(cudaStream_t, const R *, double *, const R *, int, Grid3, bool);          \
   template cudaError_t pois_fwd_y_array<R>(cudaStream_t, const double *, R *, const R *, int, Grid3);
 SVOF3_POISSON_INST(double)

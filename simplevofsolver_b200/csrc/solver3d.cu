@@ -93,7 +93,8 @@ void dfree(DevBuf &b) {
 
 struct svof3d_solver {
   svof3d_params_t prm{};
-  bool mixed = false;  // SVOF3_MIXED: FP32 intermediates (see svof3d_b200.h)
+  bool mixed = false;  // SVOF3_MIXED or SVOF3_MIXED_DC: FP32 intermediates (see svof3d_b200.h)
+  bool dc = false;     // SVOF3_MIXED_DC: FP32 Poisson passes with an FP64 defect correction
   int nx = 0, ny = 0, nz = 0;
   double dy = 0., dz = 0.;
   int log2ny = 0, log2nz = 0;
@@ -107,6 +108,7 @@ struct svof3d_solver {
   double lims[4] = {0., 0., 0., 0.};  // explicit diffusive dt limits: m y, m z, t y, t z
   // Poisson
   DevBuf spec, xscratch, twf_y, twb_y, twf_z, twb_z, pl, pu, evy, evz;
+  DevBuf twf_y32, twb_y32, twf_z32, twb_z32;  // FP32 twiddles (SVOF3_MIXED_DC)
   // predictor forward-sweep scratch
   DevBuf fw;
   // time step
@@ -264,8 +266,41 @@ int launch_predict(svof3d_solver *s, int rk) {
 // after each launch
 using Marker = std::function<int(int)>;
 
-// the Poisson solve, FP64 in both paths (one pass)
+// the defect-corrected form (SVOF3_MIXED_DC): an FP32 pass on b, the FP64
+// residual r = b - L psi1, an FP32 pass on r accumulated into psi (b and r in
+// the predictor's idle line scratch, the spectrum and the x scratch in their
+// FP64 buffers' first halves)
+int launch_potential_dc(svof3d_solver *s, int rk, const Marker &mark) {
+  const double gam = RK_A[rk] + RK_B[rk];
+  const Grid3 g = s->grid();
+  auto m = [&](int kind) { return mark ? mark(kind) : 0; };
+  const int cu = s->cur_u;
+  double *b = s->fw.as<double>(), *r = b + (size_t)s->nx * s->ny * s->nz;
+  float *sp = s->spec.as<float>(), *xs = s->xscratch.as<float>();
+  for (int pass = 0; pass < 2; pass++) {
+    if (0 == pass) {
+      CK(pois_fwd_y<float>(s->stream, s->ux[cu].p, s->uy[cu].p, s->uz[cu].p, b, sp, s->twf_y32.as<float>(),
+                           s->d_dt, gam, s->log2ny, g));
+    } else {
+      CK(pois_resid(s->stream, b, s->psi.p, r, s->pl.p, s->pu.p, g));
+      CK(pois_fwd_y_array<float>(s->stream, r, sp, s->twf_y32.as<float>(), s->log2ny, g));
+    }
+    if (m(SVOF3_K_POISSON_FWD)) return 1;
+    CK(pois_z<float>(s->stream, sp, s->twf_z32.as<float>(), s->log2nz, g));
+    if (m(SVOF3_K_POISSON_Z)) return 1;
+    CK(pois_x<float>(s->stream, sp, xs, s->pl.p, s->pu.p, s->evy.p, s->evz.p, g, true));
+    if (m(SVOF3_K_POISSON_SOLVE)) return 1;
+    CK(pois_z<float>(s->stream, sp, s->twb_z32.as<float>(), s->log2nz, g));
+    if (m(SVOF3_K_POISSON_Z)) return 1;
+    CK(pois_inv_y<float>(s->stream, sp, s->psi.p, s->twb_y32.as<float>(), s->log2ny, g, 1 == pass));
+    if (m(SVOF3_K_POISSON_INV)) return 1;
+  }
+  return 0;
+}
+
+// the Poisson solve, FP64 in the FP64 and mixed paths (one pass)
 int launch_potential(svof3d_solver *s, int rk, const Marker &mark = Marker()) {
+  if (s->dc) return launch_potential_dc(s, rk, mark);
   const double gam = RK_A[rk] + RK_B[rk];
   const Grid3 g = s->grid();
   auto m = [&](int kind) { return mark ? mark(kind) : 0; };
@@ -452,6 +487,20 @@ int build_tables(svof3d_solver *s, const double *xf, const double *xc) {
     return upload(f, twf) || upload(b, twb);
   };
   if (twiddles(ny, s->twf_y, s->twb_y) || twiddles(nz, s->twf_z, s->twb_z)) return 1;
+  if (s->dc) {
+    // FP32 copies of the same tables (the FP64 values rounded once)
+    auto to32 = [&](const DevBuf &d, DevBuf &f) -> int {
+      std::vector<double> h(d.n);
+      CK(cudaMemcpy(h.data(), d.p, sizeof(double) * d.n, cudaMemcpyDeviceToHost));
+      std::vector<float> hf(h.begin(), h.end());
+      if (dalloc(f, d.n, sizeof(float))) return 1;
+      CK(cudaMemcpy(f.p, hf.data(), sizeof(float) * d.n, cudaMemcpyHostToDevice));
+      return 0;
+    };
+    if (to32(s->twf_y, s->twf_y32) || to32(s->twb_y, s->twb_y32) || to32(s->twf_z, s->twf_z32) ||
+        to32(s->twb_z, s->twb_z32))
+      return 1;
+  }
   const int nky = ny / 2 + 1;
   std::vector<double> evy(nky), evz(nz), pl(nx), pu(nx);
   for (size_t j = 0; j < (size_t)nky; j++)
@@ -484,7 +533,8 @@ int svof3d_destroy(svof3d_solver_t *s) {
   }
   DevBuf *bufs[] = {&s->p, &s->psi, &s->curv, &s->normal, &s->ifrcx, &s->ifrcy, &s->ifrcz, &s->dxf, &s->dxc,
                     &s->lap_ux, &s->lap_cc, &s->coef, &s->spec, &s->xscratch, &s->twf_y, &s->twb_y, &s->twf_z,
-                    &s->twb_z, &s->pl, &s->pu, &s->evy, &s->evz, &s->fw, &s->diag, &s->stat_part};
+                    &s->twb_z, &s->pl, &s->pu, &s->evy, &s->evz, &s->fw, &s->diag, &s->stat_part,
+                    &s->twf_y32, &s->twb_y32, &s->twf_z32, &s->twb_z32};
   for (DevBuf *b : bufs) dfree(*b);
   for (DevBuf &b : s->stat) dfree(b);
   if (s->d_dt) cudaFree(s->d_dt);
@@ -505,11 +555,13 @@ int svof3d_create(const svof3d_params_t *prm, const double *xf, const double *xc
   if (prm->ny > 2048 || prm->nz > 2048) return fail("svof3d_create: ny and nz must be at most 2048");
   if ((double)prm->nx * (prm->ny + 4) * (prm->nz + 4) > 4.0e9)
     return fail("svof3d_create: %d x %d x %d cells exceed the 32-bit cell index", prm->nx, prm->ny, prm->nz);
-  if (SVOF3_FP64 != prm->precision && SVOF3_MIXED != prm->precision)
-    return fail("svof3d_create: precision must be SVOF3_FP64 or SVOF3_MIXED (got %d)", prm->precision);
+  if (SVOF3_FP64 != prm->precision && SVOF3_MIXED != prm->precision && SVOF3_MIXED_DC != prm->precision)
+    return fail("svof3d_create: precision must be SVOF3_FP64, SVOF3_MIXED or SVOF3_MIXED_DC (got %d)",
+                prm->precision);
   svof3d_solver *s = new svof3d_solver();
   s->prm = *prm;
-  s->mixed = SVOF3_MIXED == prm->precision;
+  s->mixed = SVOF3_FP64 != prm->precision;
+  s->dc = SVOF3_MIXED_DC == prm->precision;
   s->nx = prm->nx;
   s->ny = prm->ny;
   s->nz = prm->nz;
@@ -547,7 +599,8 @@ int svof3d_create(const svof3d_params_t *prm, const double *xf, const double *xc
       dalloc(s->fw, 4 * nx * ny * nz, es))
     return bail();
   {
-    const cudaError_t pe = pois_prepare<double>(s->log2ny, s->log2nz);
+    const cudaError_t pe =
+        s->dc ? pois_prepare<float>(s->log2ny, s->log2nz) : pois_prepare<double>(s->log2ny, s->log2nz);
     if (cudaSuccess != pe || cudaSuccess != predict_prepare() || cudaSuccess != interface_prepare())
       return fail("cudaFuncSetAttribute(Poisson): %s", cudaGetErrorString(cudaGetLastError())), bail();
     const size_t coef_smem = sizeof(double) * 6 * nx;

@@ -157,8 +157,9 @@ cudaError_t pois_fwd_y(cudaStream_t st, const double *ux, const double *uy, cons
 template <class R>
 cudaError_t pois_z(cudaStream_t st, R *spec, const R *tw, int log2n, Grid3 g);
 template <class R>
+// (gauge0: the ky = kz = 0 line takes the gauge psi_hat(last) = 0, for FP32 storage)
 cudaError_t pois_x(cudaStream_t st, R *spec, R *scratch, const double *pl, const double *pu, const double *evy,
-                   const double *evz, Grid3 g);
+                   const double *evz, Grid3 g, bool gauge0 = false);
 // acc: psi += the result (the correction pass), the walls' halo images kept
 template <class R>
 cudaError_t pois_inv_y(cudaStream_t st, const R *spec, double *psi, const R *tw, int log2n, Grid3 g,

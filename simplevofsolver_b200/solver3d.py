@@ -30,7 +30,8 @@ class Params3D(ctypes.Structure):
                 ("precision", ctypes.c_int)]
 
 
-FP64, MIXED = 0, 1
+FP64, MIXED, MIXED_DC = 0, 1, 2
+PRECISIONS = {"fp64": FP64, "mixed": MIXED, "mixed_dc": MIXED_DC}
 
 FIELDS3D = {"ux": 0, "uy": 1, "uz": 2, "p": 3, "t": 4, "vof": 5, "psi": 6, "curv": 7, "normal": 8,
             "ifrcx": 9, "ifrcy": 10, "ifrcz": 11, "srcux_a": 12, "srcux_b": 13, "srcuy_a": 14, "srcuy_b": 15,
@@ -129,9 +130,9 @@ class Solver3D:
 
     def __init__(self, ic: InitialCondition3D, physical: dict, add_buoyancy: bool = False,
                  uy_walls=(0.0, 0.0), uz_walls=(0.0, 0.0), t_walls=(0.0, 0.0), precision: str = "fp64"):
-        """precision: "fp64" or "mixed" (see svof3d_b200.h)"""
-        if precision not in ("fp64", "mixed"):
-            raise ValueError(f"precision must be 'fp64' or 'mixed', not {precision!r}")
+        """precision: "fp64", "mixed" or "mixed_dc" (see svof3d_b200.h)"""
+        if precision not in PRECISIONS:
+            raise ValueError(f"precision must be 'fp64', 'mixed' or 'mixed_dc', not {precision!r}")
         L = lib3()
         self.precision = precision
         self.nx, self.ny, self.nz = int(ic.nx), int(ic.ny), int(ic.nz)
@@ -139,7 +140,7 @@ class Solver3D:
                                physical["m_dif"], physical["t_dif"], physical["tension"],
                                physical["coef_dt_adv"], physical["coef_dt_dif"], int(bool(add_buoyancy)),
                                float(uy_walls[0]), float(uy_walls[1]), float(uz_walls[0]), float(uz_walls[1]),
-                               float(t_walls[0]), float(t_walls[1]), MIXED if precision == "mixed" else FP64)
+                               float(t_walls[0]), float(t_walls[1]), PRECISIONS[precision])
         self._h = ctypes.c_void_p()
         self._io_held = []
         xf, xc = _c(ic.xf), _c(ic.xc)
