@@ -24,6 +24,13 @@
  * except the host copies of the queued loads and stores, which run on two
  * copy streams the solver makes for them.
  * A solver is not reentrant: one host thread drives it at a time.
+ *
+ * Failure detection as in svof_b200.h: a non-finite velocity met by the CFL
+ * reduction, or a time step that is not a positive finite number, makes the
+ * next call that waits for the solver's stream (svof3d_fluid_decide_dt,
+ * svof3d_run, svof3d_integrate, svof3d_last_dt, svof3d_io_wait,
+ * svof3d_synchronize) return non-zero; SVOF_FAIL_ALLOC=N fails the N-th
+ * device buffer allocation of svof3d_create.
  */
 #ifndef SVOF3D_B200_H
 #define SVOF3D_B200_H

@@ -6,6 +6,15 @@
  * non-zero code on failure (the reference's convention, src/main.c:66-99);
  * svof_last_error() describes the last failure of the calling thread.
  *
+ * Failure detection (absent from the reference, whose dt ignores NaN): the
+ * CFL reduction of every step sets a device status word when it meets a
+ * non-finite velocity (NaN or Inf) or yields a time step that is not a
+ * positive finite number; the calls that wait for the solver's stream
+ * (svof_fluid_decide_dt, svof_run, svof_integrate, svof_last_dt,
+ * svof_synchronize) then return non-zero with that message, and clear the
+ * word.  SVOF_FAIL_ALLOC=N in the environment makes the N-th device buffer
+ * allocation of svof_create fail (a test hook: no allocation happens).
+ *
  * Data layout: every field is stored on the device exactly as the reference
  * stores it in memory (reference include/array_macros/**): float64, x
  * fastest, x ghost cells and y halo rows included.  For nx x ny interior

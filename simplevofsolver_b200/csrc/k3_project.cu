@@ -136,16 +136,18 @@ __device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v)
 // maximum |u| (NaN velocities are skipped by fmax, as by the fmin of the
 // per-face form): three divisions a thread instead of three a cell.  All
 // candidates are positive, so the minimum of their IEEE bit patterns as
-// unsigned integers is the bit pattern of the minimum.
+// unsigned integers is the bit pattern of the minimum.  A non-finite
+// velocity (NaN or Inf) sets bit 0 of *status for the host to report.
 __global__ void __launch_bounds__(256) k3_cfl(const double *__restrict__ ux, const double *__restrict__ uy,
                                               const double *__restrict__ uz, unsigned long long *__restrict__ minbits,
-                                              Grid3 g) {
+                                              unsigned *__restrict__ status, Grid3 g) {
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
   const int k0 = 1 + blockIdx.z * kCflPlanes;
   const double small = 1.e-8;
   unsigned long long best = 0x7ff0000000000000ull;
+  bool bad = false;
   if (i <= nx && j <= ny) {
     double vy[kCflPlanes], vz[kCflPlanes], vx[kCflPlanes];
 #pragma unroll
@@ -162,6 +164,7 @@ __global__ void __launch_bounds__(256) k3_cfl(const double *__restrict__ ux, con
       my = fmax(my, fabs(vy[h]));
       mz = fmax(mz, fabs(vz[h]));
       if (i >= 2) mx = fmax(mx, fabs(vx[h]));
+      bad |= !(fabs(vy[h]) <= kDblMax && fabs(vz[h]) <= kDblMax && fabs(vx[h]) <= kDblMax);
     }
     double cand = __longlong_as_double(0x7ff0000000000000ll);
     if (my >= 0.) cand = fmin(cand, g.dy / (my + small));
@@ -169,6 +172,7 @@ __global__ void __launch_bounds__(256) k3_cfl(const double *__restrict__ ux, con
     if (mx >= 0.) cand = fmin(cand, ldg(g.dxc + i - 1) / (mx + small));
     best = (unsigned long long)__double_as_longlong(cand);
   }
+  if (__any_sync(0xffffffffu, bad) && 0 == ((threadIdx.x + blockDim.x * threadIdx.y) & 31)) atomicOr(status, 1u);
   best = warp_min_u64(best);
   __shared__ unsigned long long sbest[8];
   const int tid = threadIdx.x + blockDim.x * threadIdx.y;
@@ -183,9 +187,10 @@ __global__ void __launch_bounds__(256) k3_cfl(const double *__restrict__ ux, con
 }
 
 // dt = min(coef_adv min(1, advective minimum), the four explicit diffusive
-// limits); resets the accumulator to the bit pattern of 1.0
+// limits); resets the accumulator to the bit pattern of 1.0; a time step
+// that is not a positive finite number sets bit 1 of *status
 __global__ void k3_dt_final(unsigned long long *minbits, double *dt, double coef_adv, double l0, double l1,
-                            double l2, double l3) {
+                            double l2, double l3, unsigned *status) {
   double dta = fmin(1., __longlong_as_double((long long)*minbits));
   dta *= coef_adv;
   double r = dta;
@@ -194,6 +199,7 @@ __global__ void k3_dt_final(unsigned long long *minbits, double *dt, double coef
   r = fmin(r, l2);
   r = fmin(r, l3);
   *dt = r;
+  if (!(r > 0. && r <= kDblMax)) atomicOr(status, 2u);
   *minbits = (unsigned long long)__double_as_longlong(1.);
 }
 

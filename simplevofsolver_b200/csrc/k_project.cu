@@ -106,7 +106,9 @@ __global__ void k_project(double *__restrict__ ux, double *__restrict__ uy, doub
 // i in [1, nx] of rows 1..ny.  All candidates are positive, so the minimum
 // of their IEEE bit patterns (as unsigned integers) is the bit pattern of
 // the minimum; NaN candidates sort above every finite value and are ignored,
-// like fmin ignores them in the reference.
+// like fmin ignores them in the reference.  A non-finite velocity (NaN or
+// Inf) sets bit 0 of *status (the failure detection the reference lacks:
+// the host reports it at its next synchronisation).
 __device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -117,11 +119,12 @@ __device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v)
 }
 
 __global__ void k_cfl(const double *__restrict__ ux, const double *__restrict__ uy,
-                      unsigned long long *__restrict__ minbits, Grid2 g) {
+                      unsigned long long *__restrict__ minbits, unsigned *__restrict__ status, Grid2 g) {
   pdl_enter();
   const int nx = g.nx, ny = g.ny;
   const double small = 1.e-8;
   unsigned long long best = 0x7ff0000000000000ull;  // +inf
+  bool bad = false;
   const long nfx = (long)(nx - 1) * ny, nfy = (long)nx * ny;
   const long stride = (long)gridDim.x * blockDim.x;
   for (long w = (long)blockIdx.x * blockDim.x + threadIdx.x; w < nfx + nfy; w += stride) {
@@ -130,18 +133,23 @@ __global__ void k_cfl(const double *__restrict__ ux, const double *__restrict__ 
       const int i = 2 + (int)(w % (nx - 1));
       const int j = 1 + (int)(w / (nx - 1));
       const double dx = g.dxc[i - 1];
-      const double vel = fabs(ux[ix_ux(nx, i, j)]) + small;
+      const double au = fabs(ux[ix_ux(nx, i, j)]);
+      bad |= !(au <= kDblMax);
+      const double vel = au + small;
       cand = dx / vel;
     } else {
       const long v = w - nfx;
       const int i = 1 + (int)(v % nx);
       const int j = 1 + (int)(v / nx);
-      const double vel = fabs(uy[ix_cc(nx, i, j)]) + small;
+      const double av = fabs(uy[ix_cc(nx, i, j)]);
+      bad |= !(av <= kDblMax);
+      const double vel = av + small;
       cand = g.dy / vel;
     }
     const unsigned long long b = (unsigned long long)__double_as_longlong(cand);
     best = b < best ? b : best;
   }
+  if (__any_sync(0xffffffffu, bad) && 0 == (threadIdx.x & 31)) atomicOr(status, 1u);
   best = warp_min_u64(best);
   __shared__ unsigned long long sbest[32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -157,8 +165,9 @@ __global__ void k_cfl(const double *__restrict__ ux, const double *__restrict__ 
 // decide_dt_adv tail and fluid_decide_dt (src/fluid/decide_dt.c:61-63, 129-143);
 // dif_m_y, dif_t_y are decide_dt_dif's y limits, computed on the host.
 // Resets the accumulator to the bit pattern of 1.0 (the initial *dt = 1.).
+// A time step that is not a positive finite number sets bit 1 of *status.
 __global__ void k_dt_final(unsigned long long *minbits, double *dt, double coef_adv, double dif_m_y,
-                           double dif_t_y) {
+                           double dif_t_y, unsigned *status) {
   pdl_enter();
   double dta = fmin(1., __longlong_as_double((long long)*minbits));
   dta *= coef_adv;
@@ -166,6 +175,7 @@ __global__ void k_dt_final(unsigned long long *minbits, double *dt, double coef_
   r = fmin(r, dif_m_y);
   r = fmin(r, dif_t_y);
   *dt = r;
+  if (!(r > 0. && r <= kDblMax)) atomicOr(status, 2u);
   *minbits = (unsigned long long)__double_as_longlong(1.);
 }
 

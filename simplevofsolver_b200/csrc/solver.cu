@@ -24,6 +24,7 @@
 #include "svof_internal.cuh"
 #include "stat_internal.cuh"
 #include "smem_limit.cuh"
+#include "fault_hook.cuh"
 #include "solver_state.cuh"
 
 using namespace svof;
@@ -78,6 +79,7 @@ int fail(const char *fmt, ...) {
 // managed: CUDA managed memory, so that a host program holding the pointer
 // (the reference's logging and save code read the fields directly) can read it
 int dalloc(DevBuf &b, size_t n, bool managed) {
+  if (svof_fault::next_alloc_fails()) return fail("cudaMalloc: out of memory (injected by SVOF_FAIL_ALLOC)");
   b.n = n;
   if (managed) {
     CK(cudaMallocManaged(&b.p, sizeof(double) * (n ? n : 1)));
@@ -121,13 +123,28 @@ int launch_halo_bc(svof_solver *s, double *a, int field) {
   return 0;
 }
 
+// reads and clears the device status word (after the stream's work is
+// done): a set bit is reported as a failure of `who`
+int check_status(svof_solver *s, const char *who) {
+  unsigned st = 0;
+  CK(cudaMemcpyAsync(&st, s->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  if (0 == st) return 0;
+  CK(cudaMemsetAsync(s->d_status, 0, sizeof(unsigned), s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  if (st & 1u)
+    return fail("%s: the CFL reduction met a non-finite velocity (NaN or Inf): the fields hold non-finite values",
+                who);
+  return fail("%s: the time step is not a positive finite number", who);
+}
+
 int launch_dt(svof_solver *s) {
   const long nf = (long)(s->nx - 1) * s->ny + (long)s->nx * s->ny;
   int blocks = (int)std::min<long>((nf + 255) / 256, 148L * 8);
   CK(launch_k(s->pdl, k_cfl, blocks, 256, 0, s->stream, (const double *)s->ux[s->cur_u].p,
-              (const double *)s->uy[s->cur_u].p, s->d_minbits, s->grid()));
+              (const double *)s->uy[s->cur_u].p, s->d_minbits, s->d_status, s->grid()));
   CK(launch_k(s->pdl, k_dt_final, 1, 1, 0, s->stream, s->d_minbits, s->d_dt, s->prm.coef_dt_adv, s->dif_m_y,
-              s->dif_t_y));
+              s->dif_t_y, s->d_status));
   return 0;
 }
 
@@ -522,6 +539,7 @@ int engine_create(const svof_params_t *prm, const double *xf, const double *xc, 
                   svof_solver_t **out) {
   if (!prm || !xf || !xc || !out) return fail("svof_create: null argument");
   *out = nullptr;
+  svof_fault::begin_creation();
   if (prm->nx < 4 || prm->ny < 4) return fail("svof_create: nx and ny must be at least 4");
   if (!(prm->m_dif > 0.) || !(prm->t_dif > 0.)) return fail("svof_create: diffusivities must be positive");
   svof_solver *s = new svof_solver();
@@ -642,6 +660,9 @@ int engine_create(const svof_params_t *prm, const double *xf, const double *xc, 
   }
   if (cudaSuccess != cudaMalloc(&s->d_dt, sizeof(double))) return fail("cudaMalloc dt"), bail();
   if (cudaSuccess != cudaMalloc(&s->d_minbits, sizeof(unsigned long long))) return fail("cudaMalloc"), bail();
+  if (cudaSuccess != cudaMalloc(&s->d_status, sizeof(unsigned)) ||
+      cudaSuccess != cudaMemset(s->d_status, 0, sizeof(unsigned)))
+    return fail("cudaMalloc status"), bail();
   {
     const double one = 1.;
     unsigned long long bits;
@@ -704,6 +725,7 @@ int svof_destroy(svof_solver_t *s) {
   for (DevBuf &b : s->stat) dfree(b);
   if (s->d_dt) cudaFree(s->d_dt);
   if (s->d_minbits) cudaFree(s->d_minbits);
+  if (s->d_status) cudaFree(s->d_status);
   if (s->h_dt) cudaFreeHost(s->h_dt);
   for (int k = 0; k < 3; k++) {
     if (s->ev_fork[k]) cudaEventDestroy(s->ev_fork[k]);
@@ -792,7 +814,7 @@ int svof_fluid_decide_dt(svof_solver_t *s, double *dt) {
   CK(cudaMemcpyAsync(s->h_dt, s->d_dt, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   *dt = s->h_dt[0];
-  return 0;
+  return check_status(s, "svof_fluid_decide_dt");
 }
 
 static int set_dt(svof_solver_t *s, double dt) {
@@ -877,7 +899,7 @@ int svof_run(svof_solver_t *s, int nsteps, double *dts) {
     const int done = ((nsteps - 1) / s->h_dt_slots) * s->h_dt_slots;
     std::memcpy(dts + done, s->h_dt, sizeof(double) * (nsteps - done));
   }
-  return 0;
+  return check_status(s, "svof_run");
 }
 
 int svof_enqueue_steps(svof_solver_t *s, int nsteps) {
@@ -896,7 +918,7 @@ int svof_last_dt(svof_solver_t *s, double *dt) {
   if (!s || !dt) return fail("null argument");
   CK(cudaStreamSynchronize(s->stream));
   *dt = s->h_dt[0];
-  return 0;
+  return check_status(s, "svof_last_dt");
 }
 
 int svof_integrate(svof_solver_t *s, double *dt) {
@@ -1095,7 +1117,7 @@ int svof_statistics_field(svof_solver_t *s, int quantity, double *out, size_t co
 int svof_synchronize(svof_solver_t *s) {
   if (!s) return fail("null argument");
   CK(cudaStreamSynchronize(s->stream));
-  return 0;
+  return check_status(s, "svof_synchronize");
 }
 
 int svof_stream(svof_solver_t *s, void **stream) {

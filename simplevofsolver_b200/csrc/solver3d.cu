@@ -22,6 +22,7 @@
 #include "svof3d_internal.cuh"
 #include "stat_internal.cuh"
 #include "smem_limit.cuh"
+#include "fault_hook.cuh"
 
 using namespace svof3;
 
@@ -70,6 +71,7 @@ struct DevBuf {
 };
 
 int dalloc(DevBuf &b, size_t n, size_t es = 8) {
+  if (svof_fault::next_alloc_fails()) return fail("cudaMalloc: out of memory (injected by SVOF_FAIL_ALLOC)");
   b.n = n;
   b.es = es;
   CK(cudaMalloc(&b.p, es * (n ? n : 1)));
@@ -114,6 +116,10 @@ struct svof3d_solver {
   // time step
   double *d_dt = nullptr;
   unsigned long long *d_minbits = nullptr;
+  // failure detection: bits set by k3_cfl (a non-finite velocity) and
+  // k3_dt_final (a time step that is not a positive finite number), read and
+  // cleared by the host at its synchronisations (check_status)
+  unsigned *d_status = nullptr;
   double *h_dt = nullptr;
   int h_dt_slots = 0;
   DevBuf diag;
@@ -159,13 +165,28 @@ int launch_halo_bc(svof3d_solver *s, double *a, int field) {
   return 0;
 }
 
+// reads and clears the device status word (after the stream's work is
+// done): a set bit is reported as a failure of `who`
+int check_status(svof3d_solver *s, const char *who) {
+  unsigned st = 0;
+  CK(cudaMemcpyAsync(&st, s->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  if (0 == st) return 0;
+  CK(cudaMemsetAsync(s->d_status, 0, sizeof(unsigned), s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  if (st & 1u)
+    return fail("%s: the CFL reduction met a non-finite velocity (NaN or Inf): the fields hold non-finite values",
+                who);
+  return fail("%s: the time step is not a positive finite number", who);
+}
+
 int launch_dt(svof3d_solver *s) {
   const dim3 cb(32, 8), cg((s->nx + 31) / 32, (s->ny + 7) / 8, (s->nz + kCflPlanes - 1) / kCflPlanes);
   k3_cfl<<<cg, cb, 0, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->uz[s->cur_u].p, s->d_minbits,
-                                        s->grid());
+                                        s->d_status, s->grid());
   CK_LAUNCH();
   k3_dt_final<<<1, 1, 0, s->stream>>>(s->d_minbits, s->d_dt, s->prm.coef_dt_adv, s->lims[0], s->lims[1],
-                                      s->lims[2], s->lims[3]);
+                                      s->lims[2], s->lims[3], s->d_status);
   CK_LAUNCH();
   return 0;
 }
@@ -539,6 +560,7 @@ int svof3d_destroy(svof3d_solver_t *s) {
   for (DevBuf &b : s->stat) dfree(b);
   if (s->d_dt) cudaFree(s->d_dt);
   if (s->d_minbits) cudaFree(s->d_minbits);
+  if (s->d_status) cudaFree(s->d_status);
   if (s->d_work) cudaFree(s->d_work);
   if (s->d_nwork) cudaFree(s->d_nwork);
   if (s->h_dt) cudaFreeHost(s->h_dt);
@@ -550,6 +572,7 @@ int svof3d_destroy(svof3d_solver_t *s) {
 int svof3d_create(const svof3d_params_t *prm, const double *xf, const double *xc, svof3d_solver_t **out) {
   if (!prm || !xf || !xc || !out) return fail("svof3d_create: null argument");
   *out = nullptr;
+  svof_fault::begin_creation();
   if (prm->nx < 4 || prm->ny < 4 || prm->nz < 4) return fail("svof3d_create: nx, ny and nz must be at least 4");
   if (!(prm->m_dif > 0.) || !(prm->t_dif > 0.)) return fail("svof3d_create: diffusivities must be positive");
   if (prm->ny > 2048 || prm->nz > 2048) return fail("svof3d_create: ny and nz must be at most 2048");
@@ -612,6 +635,9 @@ int svof3d_create(const svof3d_params_t *prm, const double *xf, const double *xc
       cudaSuccess != cudaMalloc(&s->d_nwork, sizeof(unsigned)))
     return fail("cudaMalloc worklist"), bail();
   if (cudaSuccess != cudaMalloc(&s->d_minbits, sizeof(unsigned long long))) return fail("cudaMalloc"), bail();
+  if (cudaSuccess != cudaMalloc(&s->d_status, sizeof(unsigned)) ||
+      cudaSuccess != cudaMemset(s->d_status, 0, sizeof(unsigned)))
+    return fail("cudaMalloc status"), bail();
   {
     const double one = 1.;
     unsigned long long bits;
@@ -769,7 +795,7 @@ int svof3d_io_wait(svof3d_solver_t *s) {
   if (s->io_h2d) CK(cudaStreamSynchronize(s->io_h2d));
   CK(cudaStreamSynchronize(s->stream));
   if (s->io_d2h) CK(cudaStreamSynchronize(s->io_d2h));
-  return 0;
+  return check_status(s, "svof3d_io_wait");
 }
 
 int svof3d_fluid_decide_dt(svof3d_solver_t *s, double *dt) {
@@ -778,7 +804,7 @@ int svof3d_fluid_decide_dt(svof3d_solver_t *s, double *dt) {
   CK(cudaMemcpyAsync(s->h_dt, s->d_dt, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   *dt = s->h_dt[0];
-  return 0;
+  return check_status(s, "svof3d_fluid_decide_dt");
 }
 
 static int set_dt(svof3d_solver_t *s, double dt) {
@@ -857,7 +883,7 @@ int svof3d_run(svof3d_solver_t *s, int nsteps, double *dts) {
     const int done = ((nsteps - 1) / s->h_dt_slots) * s->h_dt_slots;
     std::memcpy(dts + done, s->h_dt, sizeof(double) * (nsteps - done));
   }
-  return 0;
+  return check_status(s, "svof3d_run");
 }
 
 int svof3d_enqueue_steps(svof3d_solver_t *s, int nsteps) {
@@ -876,7 +902,7 @@ int svof3d_last_dt(svof3d_solver_t *s, double *dt) {
   if (!s || !dt) return fail("null argument");
   CK(cudaStreamSynchronize(s->stream));
   *dt = s->h_dt[0];
-  return 0;
+  return check_status(s, "svof3d_last_dt");
 }
 
 int svof3d_integrate(svof3d_solver_t *s, double *dt) {
@@ -1039,7 +1065,7 @@ int svof3d_statistics_field(svof3d_solver_t *s, int quantity, double *out, size_
 int svof3d_synchronize(svof3d_solver_t *s) {
   if (!s) return fail("null argument");
   CK(cudaStreamSynchronize(s->stream));
-  return 0;
+  return check_status(s, "svof3d_synchronize");
 }
 
 int svof3d_stream(svof3d_solver_t *s, void **stream) {

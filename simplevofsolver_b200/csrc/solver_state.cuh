@@ -70,6 +70,10 @@ struct svof_solver {
   // time step
   double *d_dt = nullptr;
   unsigned long long *d_minbits = nullptr;
+  // failure detection: bits set on the device (k_cfl: a non-finite velocity;
+  // k_dt_final: a time step that is not a positive finite number), read and
+  // cleared by the host at its synchronisations (check_status)
+  unsigned *d_status = nullptr;
   double *h_dt = nullptr;   // pinned, many slots for svof_run
   int h_dt_slots = 0;
   svof::DevBuf diag;
@@ -142,6 +146,7 @@ cudaError_t launch_k(bool pdl, void (*k)(KArgs...), dim3 grid, dim3 block, size_
 // each issues the kernels of one reference function on the solver's stream
 int launch_halo_bc(svof_solver *s, double *a, int field);
 int launch_dt(svof_solver *s);
+int check_status(svof_solver *s, const char *who);
 int launch_coef(svof_solver *s, int rk, cudaStream_t st);
 // the predictor's Thomas table of substep rk (k_tdm_coef layout)
 double *coef_table(svof_solver *s, int rk);

@@ -13,6 +13,7 @@
 namespace svof3 {
 
 constexpr double kDblEpsilon = 2.220446049250313080847e-16;  // DBL_EPSILON
+constexpr double kDblMax = 1.7976931348623157e308;          // DBL_MAX
 
 struct Grid3 {
   int nx, ny, nz;
@@ -177,11 +178,12 @@ __global__ void k3_project(double *__restrict__ ux, double *__restrict__ uy, dou
                            double gam, double m_dif, double uy_xm, double uy_xp, double uz_xm, double uz_xp,
                            int do_vel, int do_p, Grid3 g);
 
-// time step
+// time step (status: bit 0 a non-finite velocity, bit 1 a time step that is
+// not a positive finite number)
 __global__ void k3_cfl(const double *__restrict__ ux, const double *__restrict__ uy, const double *__restrict__ uz,
-                       unsigned long long *__restrict__ minbits, Grid3 g);
+                       unsigned long long *__restrict__ minbits, unsigned *__restrict__ status, Grid3 g);
 __global__ void k3_dt_final(unsigned long long *minbits, double *dt, double coef_adv, double l0, double l1,
-                            double l2, double l3);
+                            double l2, double l3, unsigned *status);
 // diagnostics, deterministic two-stage reduction: blocks of 32 x 8 threads
 // over kDiagPlanes planes write 5 partials each; out = {max |div u|, vof min,
 // vof max, sum vof dx dy dz (compensated)}

@@ -16,6 +16,7 @@
 namespace svof {
 
 constexpr double kDblEpsilon = 2.220446049250313080847e-16;  // DBL_EPSILON
+constexpr double kDblMax = 1.7976931348623157e308;          // DBL_MAX
 
 // Programmatic dependent launch: on small grids the step graph launches its
 // kernels with programmatic stream serialisation, so that a kernel is set up
@@ -161,10 +162,12 @@ __global__ void k_project(double *__restrict__ ux, double *__restrict__ uy, doub
                           double m_dif, double uy_xm, double uy_xp, int do_vel, int do_p, Grid2 g);
 
 // time step (src/fluid/decide_dt.c)
+// (status: bit 0 a non-finite velocity, bit 1 a time step that is not a
+// positive finite number)
 __global__ void k_cfl(const double *__restrict__ ux, const double *__restrict__ uy,
-                      unsigned long long *__restrict__ minbits, Grid2 g);
+                      unsigned long long *__restrict__ minbits, unsigned *__restrict__ status, Grid2 g);
 __global__ void k_dt_final(unsigned long long *minbits, double *dt, double coef_adv, double dif_m_y,
-                           double dif_t_y);
+                           double dif_t_y, unsigned *status);
 // diagnostics (src/logging/divergence.c, src/logging/interface.c)
 __global__ void k_diag(const double *__restrict__ ux, const double *__restrict__ uy,
                        const double *__restrict__ vof, double *__restrict__ out, Grid2 g);

@@ -383,16 +383,46 @@ def write_npy_dir(ic, dirname: str, step: int = 0, time: float = 0.0):
         np.save(os.path.join(dirname, f"{k}.npy"), np.ascontiguousarray(v, dtype=np.float64))
 
 
+def _load_npy(dirname: str, name: str, shape=None, dtype=np.float64):
+    """one array of a restart directory, checked against the reference's
+    layout (little-endian, C order, the given dtype and shape); a file that
+    is not a readable NPY v1/v2 array, or that differs, raises ValueError
+    naming the file"""
+    path = os.path.join(dirname, f"{name}.npy")
+    try:
+        a = np.load(path, allow_pickle=False)
+    except (ValueError, OSError, EOFError) as e:
+        raise ValueError(f"{path}: not a readable NPY array ({e})") from None
+    want = np.dtype(dtype).newbyteorder("<")
+    if a.dtype != want:
+        raise ValueError(f"{path}: dtype {a.dtype.str}, expected {want.str}")
+    if a.ndim > 1 and not a.flags.c_contiguous:
+        raise ValueError(f"{path}: Fortran order, expected C order")
+    if shape is not None and tuple(a.shape) != tuple(shape):
+        raise ValueError(f"{path}: shape {tuple(a.shape)}, expected {tuple(shape)}")
+    return a
+
+
 def read_npy_dir(dirname: str):
     """the restart directory written by write_npy_dir or by the reference's
-    save: InitialCondition (2D) or InitialCondition3D (glsizes of 3 items)"""
-    ld = lambda k: np.load(os.path.join(dirname, f"{k}.npy"))
-    gl = ld("glsizes")
-    ln = ld("lengths")
+    save: InitialCondition (2D) or InitialCondition3D (glsizes of 3 items).
+    Every array is checked against the reference's layout (float64 fields
+    with the x ghost cells: ux (.., nx + 1), the others (.., nx + 2); xf of
+    nx + 1, xc of nx + 2 values; uint64 glsizes): ValueError otherwise."""
+    gl = _load_npy(dirname, "glsizes", None, np.uint64)
+    if gl.ndim != 1 or len(gl) not in (2, 3) or np.any(gl < 1):
+        raise ValueError(f"{dirname}: glsizes {gl.tolist()} is not a 2D or 3D grid size")
+    ln = _load_npy(dirname, "lengths", (len(gl),))
+    nx = int(gl[0])
+    xf = _load_npy(dirname, "xf", (nx + 1,))
+    xc = _load_npy(dirname, "xc", (nx + 2,))
+    rows = tuple(int(v) for v in gl[1:][::-1])  # (ny,) or (nz, ny)
+    fx, fc = rows + (nx + 1,), rows + (nx + 2,)
+    ld = lambda k: _load_npy(dirname, k, fx if k == "ux" else fc)
     if 3 == len(gl):
-        nx, ny, nz = (int(v) for v in gl)
-        return InitialCondition3D(nx, ny, nz, float(ln[0]), float(ln[1]), float(ln[2]), ld("xf"), ld("xc"),
+        ny, nz = int(gl[1]), int(gl[2])
+        return InitialCondition3D(nx, ny, nz, float(ln[0]), float(ln[1]), float(ln[2]), xf, xc,
                                   ld("ux"), ld("uy"), ld("uz"), ld("p"), ld("t"), ld("vof"))
-    nx, ny = int(gl[0]), int(gl[1])
-    return InitialCondition(nx, ny, float(ln[0]), float(ln[1]), ld("xf"), ld("xc"),
+    ny = int(gl[1])
+    return InitialCondition(nx, ny, float(ln[0]), float(ln[1]), xf, xc,
                             ld("ux"), ld("uy"), ld("p"), ld("t"), ld("vof"))
