@@ -23,6 +23,7 @@
 
 #include "../../include/svof_b200.h"
 #include "adjoint_internal.cuh"
+#include "trace.cuh"
 #include "smem_limit.cuh"
 #include "solver_state.cuh"
 
@@ -276,6 +277,7 @@ int svof_tape_count(const svof_solver_t *s, size_t *count) {
 }
 
 int svof_integrate_fixed(svof_solver_t *s, double dt, double *tape) {
+  SVOF_RANGE();
   if (!s) return fail("null argument");
   if (!(dt > 0.)) return fail("svof_integrate_fixed: dt must be positive");
   if (adj_set_dt(s, dt)) return 1;
@@ -339,6 +341,7 @@ int svof_adjoint_reset(svof_solver_t *s) {
 }
 
 int svof_adjoint_step(svof_solver_t *s, const double *tape, double dt) {
+  SVOF_RANGE();
   if (check_prim(s)) return 1;
   if (!tape) return fail("svof_adjoint_step: null tape");
   if (!(dt > 0.)) return fail("svof_adjoint_step: dt must be positive");
@@ -365,24 +368,28 @@ int svof_adjoint_step(svof_solver_t *s, const double *tape, double dt) {
 }
 
 int svof_adjoint_fluid_update_pressure(svof_solver_t *s, size_t rk, double dt) {
+  SVOF_RANGE();
   if (check_prim(s)) return 1;
   if (rk > 2) return fail("rkstep out of range");
   return adj_project(s, (int)rk, dt, 1) || sync(s);
 }
 
 int svof_adjoint_fluid_correct_velocity(svof_solver_t *s, size_t rk, double dt) {
+  SVOF_RANGE();
   if (check_prim(s)) return 1;
   if (rk > 2) return fail("rkstep out of range");
   return adj_project(s, (int)rk, dt, 2) || sync(s);
 }
 
 int svof_adjoint_fluid_compute_potential(svof_solver_t *s, size_t rk, double dt) {
+  SVOF_RANGE();
   if (check_prim(s)) return 1;
   if (rk > 2) return fail("rkstep out of range");
   return adj_potential(s, (int)rk, dt) || sync(s);
 }
 
 int svof_adjoint_fluid_predict_field(svof_solver_t *s, size_t rk, double dt) {
+  SVOF_RANGE();
   if (check_prim(s)) return 1;
   if (rk > 2) return fail("rkstep out of range");
   return adj_set_dt(s, dt) ||
@@ -390,17 +397,20 @@ int svof_adjoint_fluid_predict_field(svof_solver_t *s, size_t rk, double dt) {
 }
 
 int svof_adjoint_interface_update_vof(svof_solver_t *s, size_t rk, double dt) {
+  SVOF_RANGE();
   if (check_prim(s)) return 1;
   if (rk > 2) return fail("rkstep out of range");
   return adj_interface(s, (int)rk, dt, 1, s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->vof[s->cur_v].p) || sync(s);
 }
 
 int svof_adjoint_interface_compute_force(svof_solver_t *s) {
+  SVOF_RANGE();
   if (check_prim(s)) return 1;
   return adj_interface(s, 0, 0., 2, s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->vof[s->cur_v].p) || sync(s);
 }
 
 int svof_adjoint_interface_compute_curvature_tensor(svof_solver_t *s) {
+  SVOF_RANGE();
   if (check_prim(s)) return 1;
   const double *vof = s->vof[s->cur_v].p;
   return adj_interface(s, 0, 0., 4, s->ux[s->cur_u].p, s->uy[s->cur_u].p, vof) || adj_corners(s, vof) || sync(s);

@@ -23,6 +23,7 @@
 #include "../../include/svof_b200.h"
 #include "svof_internal.cuh"
 #include "stat_internal.cuh"
+#include "trace.cuh"
 #include "smem_limit.cuh"
 #include "fault_hook.cuh"
 #include "solver_state.cuh"
@@ -778,6 +779,7 @@ int svof_device_field(svof_solver_t *s, int field, double **dptr) {
 }
 
 int svof_load_interior(svof_solver_t *s, int field, const double *host, size_t count) {
+  SVOF_RANGE();
   int nh, width;
   DevBuf *b;
   if (!s || !host) return fail("null argument");
@@ -791,6 +793,7 @@ int svof_load_interior(svof_solver_t *s, int field, const double *host, size_t c
 }
 
 int svof_store_interior(svof_solver_t *s, int field, double *host, size_t count) {
+  SVOF_RANGE();
   int nh, width;
   DevBuf *b;
   if (!s || !host) return fail("null argument");
@@ -809,6 +812,7 @@ int svof_x_grid_is_uniform(const svof_solver_t *s, int *u) {
 }
 
 int svof_fluid_decide_dt(svof_solver_t *s, double *dt) {
+  SVOF_RANGE();
   if (!s || !dt) return fail("null argument");
   if (launch_dt(s)) return 1;
   CK(cudaMemcpyAsync(s->h_dt, s->d_dt, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
@@ -831,54 +835,63 @@ static int finish(svof_solver_t *s) {
 }
 
 int svof_interface_compute_curvature_tensor(svof_solver_t *s) {
+  SVOF_RANGE();
   if (!s) return fail("null argument");
   if (launch_geom(s)) return 1;
   return finish(s);
 }
 
 int svof_interface_compute_force(svof_solver_t *s) {
+  SVOF_RANGE();
   if (!s) return fail("null argument");
   if (launch_force(s)) return 1;
   return finish(s);
 }
 
 int svof_interface_update_vof(svof_solver_t *s, size_t rk, double dt) {
+  SVOF_RANGE();
   if (!s) return fail("null argument");
   if (check_rk(rk) || set_dt(s, dt) || launch_vof(s, (int)rk)) return 1;
   return finish(s);
 }
 
 int svof_fluid_predict_field(svof_solver_t *s, size_t rk, double dt) {
+  SVOF_RANGE();
   if (!s) return fail("null argument");
   if (check_rk(rk) || set_dt(s, dt) || launch_predict(s, (int)rk)) return 1;
   return finish(s);
 }
 
 int svof_fluid_compute_potential_dct(svof_solver_t *s, size_t rk, double dt) {
+  SVOF_RANGE();
   if (!s) return fail("null argument");
   if (check_rk(rk) || set_dt(s, dt) || launch_potential(s, (int)rk, 1)) return 1;
   return finish(s);
 }
 
 int svof_fluid_compute_potential_dft(svof_solver_t *s, size_t rk, double dt) {
+  SVOF_RANGE();
   if (!s) return fail("null argument");
   if (check_rk(rk) || set_dt(s, dt) || launch_potential(s, (int)rk, 0)) return 1;
   return finish(s);
 }
 
 int svof_fluid_correct_velocity(svof_solver_t *s, size_t rk, double dt) {
+  SVOF_RANGE();
   if (!s) return fail("null argument");
   if (check_rk(rk) || set_dt(s, dt) || launch_project(s, (int)rk, 1, 0)) return 1;
   return finish(s);
 }
 
 int svof_fluid_update_pressure(svof_solver_t *s, size_t rk, double dt) {
+  SVOF_RANGE();
   if (!s) return fail("null argument");
   if (check_rk(rk) || set_dt(s, dt) || launch_project(s, (int)rk, 0, 1)) return 1;
   return finish(s);
 }
 
 int svof_run(svof_solver_t *s, int nsteps, double *dts) {
+  SVOF_RANGE();
   if (!s) return fail("null argument");
   if (nsteps < 0) return fail("nsteps must be non-negative");
   for (int n = 0; n < nsteps; n++) {
@@ -903,6 +916,7 @@ int svof_run(svof_solver_t *s, int nsteps, double *dts) {
 }
 
 int svof_enqueue_steps(svof_solver_t *s, int nsteps) {
+  SVOF_RANGE();
   if (!s) return fail("null argument");
   if (nsteps < 0) return fail("nsteps must be non-negative");
   for (int n = 0; n < nsteps; n++) {
@@ -922,6 +936,7 @@ int svof_last_dt(svof_solver_t *s, double *dt) {
 }
 
 int svof_integrate(svof_solver_t *s, double *dt) {
+  SVOF_RANGE();
   double d = 0.;
   if (svof_run(s, 1, &d)) return 1;
   if (dt) *dt = d;
@@ -932,6 +947,7 @@ int svof_integrate(svof_solver_t *s, double *dt) {
 // the launches; ms[k] and launches[k] accumulate per kernel kind k (see
 // svof_b200.h).  Advances the solution exactly as svof_integrate does.
 int svof_profile_step(svof_solver_t *s, double *ms, int *launches, int nkinds) {
+  SVOF_RANGE();
   if (!s || !ms || !launches || nkinds < SVOF_NKINDS) return fail("svof_profile_step: bad arguments");
   for (int k = 0; k < nkinds; k++) {
     ms[k] = 0.;
@@ -1006,6 +1022,7 @@ int svof_profile_step(svof_solver_t *s, double *ms, int *launches, int nkinds) {
 }
 
 int svof_diagnostics(svof_solver_t *s, double *divmax, double *vofmin, double *vofmax, double *vofmean) {
+  SVOF_RANGE();
   if (!s) return fail("null argument");
   k_diag<<<1, 1024, 0, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->vof[s->cur_v].p, s->diag.p,
                                     s->grid());
@@ -1115,6 +1132,7 @@ int svof_statistics_field(svof_solver_t *s, int quantity, double *out, size_t co
 }
 
 int svof_synchronize(svof_solver_t *s) {
+  SVOF_RANGE();
   if (!s) return fail("null argument");
   CK(cudaStreamSynchronize(s->stream));
   return check_status(s, "svof_synchronize");

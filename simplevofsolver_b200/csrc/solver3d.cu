@@ -21,6 +21,7 @@
 #include "../../include/svof3d_b200.h"
 #include "svof3d_internal.cuh"
 #include "stat_internal.cuh"
+#include "trace.cuh"
 #include "smem_limit.cuh"
 #include "fault_hook.cuh"
 
@@ -706,6 +707,7 @@ int svof3d_device_field(svof3d_solver_t *s, int field, double **dptr) {
 // the restart layout is nz x ny x width; in storage each interior plane k has
 // nh halo rows below and above, so the copy is one 2D memcpy of nz planes
 int svof3d_load_interior(svof3d_solver_t *s, int field, const double *host, size_t count) {
+  SVOF_RANGE();
   int nh, width;
   DevBuf *b;
   if (!s || !host) return fail("null argument");
@@ -723,6 +725,7 @@ int svof3d_load_interior(svof3d_solver_t *s, int field, const double *host, size
 }
 
 int svof3d_store_interior(svof3d_solver_t *s, int field, double *host, size_t count) {
+  SVOF_RANGE();
   int nh, width;
   DevBuf *b;
   if (!s || !host) return fail("null argument");
@@ -742,6 +745,7 @@ int svof3d_store_interior(svof3d_solver_t *s, int field, double *host, size_t co
 // then staging -> storage and the halo update on the solver's stream, in
 // order with the steps queued around it
 int svof3d_load_interior_async(svof3d_solver_t *s, int field, const double *host, size_t count) {
+  SVOF_RANGE();
   int nh, width;
   DevBuf *b;
   if (!s || !host) return fail("null argument");
@@ -768,6 +772,7 @@ int svof3d_load_interior_async(svof3d_solver_t *s, int field, const double *host
 // queued store: storage -> staging on the solver's stream, then staging ->
 // host on the copy-out stream (one contiguous copy)
 int svof3d_store_interior_async(svof3d_solver_t *s, int field, double *host, size_t count) {
+  SVOF_RANGE();
   int nh, width;
   DevBuf *b;
   if (!s || !host) return fail("null argument");
@@ -791,6 +796,7 @@ int svof3d_store_interior_async(svof3d_solver_t *s, int field, double *host, siz
 }
 
 int svof3d_io_wait(svof3d_solver_t *s) {
+  SVOF_RANGE();
   if (!s) return fail("null argument");
   if (s->io_h2d) CK(cudaStreamSynchronize(s->io_h2d));
   CK(cudaStreamSynchronize(s->stream));
@@ -799,6 +805,7 @@ int svof3d_io_wait(svof3d_solver_t *s) {
 }
 
 int svof3d_fluid_decide_dt(svof3d_solver_t *s, double *dt) {
+  SVOF_RANGE();
   if (!s || !dt) return fail("null argument");
   if (launch_dt(s)) return 1;
   CK(cudaMemcpyAsync(s->h_dt, s->d_dt, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
@@ -821,48 +828,56 @@ static int finish(svof3d_solver_t *s) {
 }
 
 int svof3d_interface_compute_curvature_tensor(svof3d_solver_t *s) {
+  SVOF_RANGE();
   if (!s) return fail("null argument");
   if (launch_geom(s)) return 1;
   return finish(s);
 }
 
 int svof3d_interface_compute_force(svof3d_solver_t *s) {
+  SVOF_RANGE();
   if (!s) return fail("null argument");
   if (launch_force(s)) return 1;
   return finish(s);
 }
 
 int svof3d_interface_update_vof(svof3d_solver_t *s, size_t rk, double dt) {
+  SVOF_RANGE();
   if (!s) return fail("null argument");
   if (check_rk(rk) || set_dt(s, dt) || launch_vof(s, (int)rk)) return 1;
   return finish(s);
 }
 
 int svof3d_fluid_predict_field(svof3d_solver_t *s, size_t rk, double dt) {
+  SVOF_RANGE();
   if (!s) return fail("null argument");
   if (check_rk(rk) || set_dt(s, dt) || launch_predict(s, (int)rk)) return 1;
   return finish(s);
 }
 
 int svof3d_fluid_compute_potential_dft(svof3d_solver_t *s, size_t rk, double dt) {
+  SVOF_RANGE();
   if (!s) return fail("null argument");
   if (check_rk(rk) || set_dt(s, dt) || launch_potential(s, (int)rk)) return 1;
   return finish(s);
 }
 
 int svof3d_fluid_correct_velocity(svof3d_solver_t *s, size_t rk, double dt) {
+  SVOF_RANGE();
   if (!s) return fail("null argument");
   if (check_rk(rk) || set_dt(s, dt) || launch_project(s, (int)rk, 1, 0)) return 1;
   return finish(s);
 }
 
 int svof3d_fluid_update_pressure(svof3d_solver_t *s, size_t rk, double dt) {
+  SVOF_RANGE();
   if (!s) return fail("null argument");
   if (check_rk(rk) || set_dt(s, dt) || launch_project(s, (int)rk, 0, 1)) return 1;
   return finish(s);
 }
 
 int svof3d_run(svof3d_solver_t *s, int nsteps, double *dts) {
+  SVOF_RANGE();
   if (!s) return fail("null argument");
   if (nsteps < 0) return fail("nsteps must be non-negative");
   for (int n = 0; n < nsteps; n++) {
@@ -887,6 +902,7 @@ int svof3d_run(svof3d_solver_t *s, int nsteps, double *dts) {
 }
 
 int svof3d_enqueue_steps(svof3d_solver_t *s, int nsteps) {
+  SVOF_RANGE();
   if (!s) return fail("null argument");
   if (nsteps < 0) return fail("nsteps must be non-negative");
   for (int n = 0; n < nsteps; n++) {
@@ -906,6 +922,7 @@ int svof3d_last_dt(svof3d_solver_t *s, double *dt) {
 }
 
 int svof3d_integrate(svof3d_solver_t *s, double *dt) {
+  SVOF_RANGE();
   double d = 0.;
   if (svof3d_run(s, 1, &d)) return 1;
   if (dt) *dt = d;
@@ -913,6 +930,7 @@ int svof3d_integrate(svof3d_solver_t *s, double *dt) {
 }
 
 int svof3d_profile_step(svof3d_solver_t *s, double *ms, int *launches, int nkinds) {
+  SVOF_RANGE();
   if (!s || !ms || !launches || nkinds < SVOF3_NKINDS) return fail("svof3d_profile_step: bad arguments");
   for (int k = 0; k < nkinds; k++) {
     ms[k] = 0.;
@@ -959,6 +977,7 @@ int svof3d_profile_step(svof3d_solver_t *s, double *ms, int *launches, int nkind
 }
 
 int svof3d_diagnostics(svof3d_solver_t *s, double *divmax, double *vofmin, double *vofmax, double *volume) {
+  SVOF_RANGE();
   if (!s) return fail("null argument");
   const dim3 db(32, 8), dg((s->nx + 31) / 32, (s->ny + 7) / 8, (s->nz + kDiagPlanes - 1) / kDiagPlanes);
   k3_diag_part<<<dg, db, 0, s->stream>>>(s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->uz[s->cur_u].p,
@@ -1063,6 +1082,7 @@ int svof3d_statistics_field(svof3d_solver_t *s, int quantity, double *out, size_
 }
 
 int svof3d_synchronize(svof3d_solver_t *s) {
+  SVOF_RANGE();
   if (!s) return fail("null argument");
   CK(cudaStreamSynchronize(s->stream));
   return check_status(s, "svof3d_synchronize");
