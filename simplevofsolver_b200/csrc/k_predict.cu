@@ -329,7 +329,7 @@ __device__ __forceinline__ size_t fw_ix(int nx, int ny, int f, int p, int j) {
 
 constexpr int PT = 32;  // tile edge of the right-hand-side and update passes
 
-__global__ void __launch_bounds__(256) k_predict_rhs(PredictArgs a, double *__restrict__ fw) {
+__global__ void __launch_bounds__(256, 3) k_predict_rhs(PredictArgs a, double *__restrict__ fw) {
   pdl_enter();
   __shared__ double sd[3][PT][PT + 1];  // [f][i - i0][j - j0]
   const Grid2 g = a.g;
@@ -338,6 +338,8 @@ __global__ void __launch_bounds__(256) k_predict_rhs(PredictArgs a, double *__re
   const double dt = *a.dtp;
   const double ca = a.rk.a * dt, cb = a.rk.b * dt, cg = a.rk.g * dt;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  // the thread's four cells unrolled, so that their loads overlap
+#pragma unroll
   for (int r = ty; r < PT; r += 8) {
     const int i = i0 + tx, j = j0 + r;
     if (i <= nx && j <= ny) {
