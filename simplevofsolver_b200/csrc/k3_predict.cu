@@ -15,10 +15,13 @@
 //              updated fields with their halo images and walls
 //
 // The Thomas coefficients depend on the substep only (k3_tdm_coef: three
-// distinct systems, ux, uy/uz, t).  The arithmetic is FP64 with the
-// restatement's association in both precisions, so the FP64 path matches it
-// bit for bit; R is the storage type of forces, sources and increments.
+// distinct systems, ux, uy/uz, t).  The right-hand sides compute in FP64
+// with the restatement's association in both precisions, the x sweeps in FP64
+// (FP64 path: bit for bit) or FP32 (mixed path, whose increments are stored
+// in FP32); R is the storage type of forces, sources and increments.
 #include <cuda_pipeline.h>
+
+#include <type_traits>
 
 #include "svof3d_internal.cuh"
 #include "smem_limit.cuh"
@@ -479,11 +482,18 @@ constexpr int PL = kPredLines, PC = kPredChunk;
 template <class R>
 constexpr int kXsBufs = 4 == sizeof(R) ? 2 : 1;
 
+// the arithmetic type of the sweeps: FP64 in the FP64 path (the restatement's
+// roundings, bit for bit), FP32 in the mixed path (its increments are FP32
+// already; an FP32 chain is a tenth of the FP64 one's latency)
+template <class R>
+using SweepT = typename std::conditional<4 == sizeof(R), float, double>::type;
+
 template <class R>
 __global__ void __launch_bounds__(256) k3_xsolve(Predict3Args<R> a) {
   constexpr int NB = kXsBufs<R>;
+  using T = SweepT<R>;
   __shared__ R sd[NB][4][PL][PC + 1];  // the four fields' values of one tile
-  __shared__ double sco[NB][9][PC];    // L, R, V of the three systems, one chunk
+  __shared__ T sco[NB][9][PC];         // L, R, V of the three systems, one chunk
   const Grid3 g = a.g;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const long nlines = (long)ny * nz;
@@ -504,7 +514,7 @@ __global__ void __launch_bounds__(256) k3_xsolve(Predict3Args<R> a) {
     for (int w = tid; w < (fwd ? 9 : 3) * PC; w += 256) {
       const int r = w / PC, q = w - r * PC;
       const int row = fwd ? r : 3 * r + 2;
-      sco[b][row][q] = (p0 + q < nx) ? ldg(a.coef + (size_t)row * nx + p0 + q) : 0.;
+      sco[b][row][q] = (p0 + q < nx) ? T(ldg(a.coef + (size_t)row * nx + p0 + q)) : T(0.);
     }
   };
   // the four fields of chunk c of the block's lines into buffer b, one commit group
@@ -541,7 +551,7 @@ __global__ void __launch_bounds__(256) k3_xsolve(Predict3Args<R> a) {
     }
     __syncthreads();
   };
-  double carry = 0.;
+  T carry = T(0.);
 
   // ------------------------------------------------------------ forward
   load_coef(0, 0, true);
@@ -552,18 +562,18 @@ __global__ void __launch_bounds__(256) k3_xsolve(Predict3Args<R> a) {
     stage(c, c, c + 1, true);
     if (sweeper) {
       R *q = sd[b][f][tx];
-      const double *L = sco[b][3 * set], *Rr = sco[b][3 * set + 1];
+      const T *L = sco[b][3 * set], *Rr = sco[b][3 * set + 1];
       const int smax = min(PC, nf - p0);
 #pragma unroll 4
       for (int s = 0; s < smax; s++) {
         const int pp = p0 + s;
-        const double x = q[s];
+        const T x = T(q[s]);
         if (0 == pp) {
           carry = x / Rr[s];
         } else if (pp < nf - 1) {
           carry = Rr[s] * (x - L[s] * carry);
         } else {
-          carry = (0. != Rr[s]) ? Rr[s] * (x - L[s] * carry) : 0.;
+          carry = (T(0.) != Rr[s]) ? Rr[s] * (x - L[s] * carry) : T(0.);
         }
         q[s] = R(carry);
       }
@@ -585,7 +595,7 @@ __global__ void __launch_bounds__(256) k3_xsolve(Predict3Args<R> a) {
   }
 
   // ------------------------------------------------------------ backward
-  double nxt = 0.;
+  T nxt = T(0.);
   load_coef(nchunks - 1, 0, false);
   load_tile(nchunks - 1, 0);
   for (int it = 0; it < nchunks; it++) {
@@ -595,15 +605,15 @@ __global__ void __launch_bounds__(256) k3_xsolve(Predict3Args<R> a) {
     stage(it, c, c - 1, false);
     if (sweeper) {
       R *q = sd[b][f][tx];
-      const double *V = sco[b][3 * set + 2];
+      const T *V = sco[b][3 * set + 2];
       const int smax = min(PC, nf - p0);
 #pragma unroll 4
       for (int s = smax - 1; s >= 0; s--) {
         const int pp = p0 + s;
         if (nf - 1 == pp) {
-          nxt = q[s];
+          nxt = T(q[s]);
         } else {
-          nxt = q[s] - V[s] * nxt;
+          nxt = T(q[s]) - V[s] * nxt;
           q[s] = R(nxt);
         }
       }
