@@ -206,6 +206,62 @@ int svof3d_statistics_reduce(svof3d_solver_t *s, int quantity, double *out, size
 /* the accumulated array itself */
 int svof3d_statistics_field(svof3d_solver_t *s, int quantity, double *out, size_t count);
 
+/* ---- differentiation form (FP64 path; no counterpart in the reference) ----
+ * The 2D form of svof_b200.h carried to 3D.  A differentiated run holds the
+ * time-step sequence fixed: svof3d_integrate_fixed takes one step with the
+ * given dt (no decide_dt) and, when tape is not NULL, records the primal
+ * inputs of its three substeps (ux, uy, uz, vof in storage layouts) there:
+ * svof3d_tape_count() doubles of device memory.  svof3d_adjoint_step maps
+ * the adjoint of a step's outputs to the adjoint of its inputs, in place in
+ * the adjoint fields, and accumulates the adjoint of the surface-tension
+ * coefficient.  The per-function entry points apply one function's
+ * transpose about the solver's current fields (the adjoint of its outputs in,
+ * of its inputs out; the adjoints of fields a function does not read pass
+ * through): update_pressure (p', psi -> p, psi), correct_velocity (u', psi
+ * -> u, psi), compute_potential_dft (psi -> u; psi_bar cleared),
+ * predict_field (u', src_a of the next substep -> u, p, the forces, src_a of
+ * the previous substep), update_vof (vof', src of the next substep -> u,
+ * vof, the normals, src of the previous substep), compute_force (the forces
+ * -> vof, curvature, tension), compute_curvature_tensor (normals, curvature
+ * -> vof).  Adjoint fields are compact: ux faces nz x ny x (nx-1), cells
+ * nz x ny x nx, normal nz x ny x nx x 4, tension one value per cell (summed
+ * by svof3d_adjoint_tension).  Requires precision SVOF3_FP64 and
+ * add_buoyancy 0; the temperature is not differentiated. */
+enum {
+  SVOF3_ADJ_UX = 0,
+  SVOF3_ADJ_UY,
+  SVOF3_ADJ_UZ,
+  SVOF3_ADJ_P,
+  SVOF3_ADJ_VOF,
+  SVOF3_ADJ_PSI,
+  SVOF3_ADJ_IFRCX,
+  SVOF3_ADJ_IFRCY,
+  SVOF3_ADJ_IFRCZ,
+  SVOF3_ADJ_CURV,
+  SVOF3_ADJ_NORMAL,
+  SVOF3_ADJ_SRCUX_A,  /* momentum sources' adjoints (between substeps) */
+  SVOF3_ADJ_SRCUY_A,
+  SVOF3_ADJ_SRCUZ_A,
+  SVOF3_ADJ_SRC_A,    /* vof source's adjoint */
+  SVOF3_ADJ_TENSION
+};
+/* the surface-tension coefficient 1/We of the following steps */
+int svof3d_set_tension(svof3d_solver_t *s, double tension);
+int svof3d_tape_count(const svof3d_solver_t *s, size_t *count);
+int svof3d_integrate_fixed(svof3d_solver_t *s, double dt, double *tape);
+/* device pointer and element count of an adjoint field (made on first use) */
+int svof3d_adjoint_field(svof3d_solver_t *s, int which, double **dptr, size_t *count);
+int svof3d_adjoint_reset(svof3d_solver_t *s);
+int svof3d_adjoint_step(svof3d_solver_t *s, const double *tape, double dt);
+int svof3d_adjoint_fluid_update_pressure(svof3d_solver_t *s, size_t rkstep, double dt);
+int svof3d_adjoint_fluid_correct_velocity(svof3d_solver_t *s, size_t rkstep, double dt);
+int svof3d_adjoint_fluid_compute_potential_dft(svof3d_solver_t *s, size_t rkstep, double dt);
+int svof3d_adjoint_fluid_predict_field(svof3d_solver_t *s, size_t rkstep, double dt);
+int svof3d_adjoint_interface_update_vof(svof3d_solver_t *s, size_t rkstep, double dt);
+int svof3d_adjoint_interface_compute_force(svof3d_solver_t *s);
+int svof3d_adjoint_interface_compute_curvature_tensor(svof3d_solver_t *s);
+int svof3d_adjoint_tension(svof3d_solver_t *s, double *out);
+
 /* one step launched kernel by kernel with events between; ms[k], launches[k] per kind */
 int svof3d_profile_step(svof3d_solver_t *s, double *ms, int *launches, int nkinds);
 int svof3d_synchronize(svof3d_solver_t *s);

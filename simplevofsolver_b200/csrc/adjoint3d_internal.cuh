@@ -1,0 +1,62 @@
+// adjoint3d_internal.cuh -- kernels of the 3D step's adjoint (k3_adjoint.cu)
+// and their argument blocks, used by the host code in solver3d.cu.
+#pragma once
+
+#include "svof3d_internal.cuh"
+
+namespace svof3 {
+
+// psi_bar += (d p' / d psi)^T p_bar' (mode & 1), (d u' / d psi)^T u_bar' (mode & 2)
+__global__ void k3_adj_project(const double *__restrict__ aux, const double *__restrict__ auy,
+                               const double *__restrict__ auz, const double *__restrict__ ap,
+                               double *__restrict__ apsi, double gdt, double pre, int mode, Grid3 g);
+// b = psi_bar / dxf (compact)
+__global__ void k3_adj_scale(const double *__restrict__ apsi, double *__restrict__ b, Grid3 g);
+// u_bar += the divergence's transpose of pre_p dxf s; psi_bar = 0
+__global__ void k3_adj_div(double *__restrict__ aux, double *__restrict__ auy, double *__restrict__ auz,
+                           const double *__restrict__ s, double *__restrict__ apsi, double pre_p, Grid3 g);
+// transposed implicit-x solves and the RK split; dynamic shared memory 3 R nx doubles
+__global__ void k3_adj_xsolve(const double *__restrict__ aux, const double *__restrict__ auy,
+                              const double *__restrict__ auz, const double *__restrict__ coef,
+                              double *__restrict__ sa_x, double *__restrict__ sg_x, double *__restrict__ sa_y,
+                              double *__restrict__ sg_y, double *__restrict__ sa_z, double *__restrict__ sg_z,
+                              double *__restrict__ pend_x, double *__restrict__ pend_y, double *__restrict__ pend_z,
+                              double adt, double bdt, double gdt, int R, Grid3 g);
+
+struct Adj3RhsArgs {
+  const double *ux, *uy, *uz;                               // primal, storage layouts
+  const double *sa_x, *sg_x, *sa_y, *sg_y, *sa_z, *sg_z;    // src_a_bar, src_g_bar
+  double *aux, *auy, *auz, *ap, *aifx, *aify, *aifz;
+  const double *lap_ux, *lap_cc;
+  double m_dif, ly0, ly1, ly2, lz0, lz1, lz2;
+  Grid3 g;
+};
+__global__ void k3_adj_rhs(Adj3RhsArgs a);
+
+struct Adj3IfaceArgs {
+  const double *ux, *uy, *uz, *vof, *normal, *curv;  // primal, storage layouts
+  const double *avof_in, *pend_in;                   // vof_bar' and pend (compact)
+  double *avof_out, *pend_out;
+  double *aux, *auy, *auz;                           // += flux terms of owned faces
+  const double *aifx, *aify, *aifz;                  // force adjoints
+  double *anrm;                                      // [4] per cell
+  double *am;                                        // [3] per cell, m_bar
+  double *akap;                                      // kappa_bar
+  double *asig;                                      // tension adjoint, per cell, +=
+  double adt, bdt, tension;
+  int mode;
+  Grid3 g;
+};
+__global__ void k3_adj_interface(Adj3IfaceArgs a);
+
+// corner gradients' adjoints ([3] per corner, (nx + 1) ny nz corners)
+__global__ void k3_adj_cgrad(const double *__restrict__ vof, const double *__restrict__ am,
+                             const double *__restrict__ akap, double *__restrict__ gbar, Grid3 g);
+// vof_bar += the corner gradients' transposes
+__global__ void k3_adj_cvof(const double *__restrict__ gbar, double *__restrict__ avof, Grid3 g);
+// deterministic sum (one block of 256 threads)
+__global__ void k3_adj_sum(const double *__restrict__ x, long n, double *__restrict__ out);
+// *dst = v in stream order
+__global__ void k3_adj_set(double *dst, double v);
+
+}  // namespace svof3

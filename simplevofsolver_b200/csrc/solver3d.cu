@@ -9,6 +9,7 @@
 // 8-byte dt.  Tables the reference recomputes on every call (Laplacian
 // coefficients, eigenvalues, FFT twiddles) are computed here once, on the
 // host, with the restatement's expressions.
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -24,6 +25,7 @@
 #include "trace.cuh"
 #include "smem_limit.cuh"
 #include "fault_hook.cuh"
+#include "adjoint3d_internal.cuh"
 
 using namespace svof3;
 
@@ -94,6 +96,9 @@ void dfree(DevBuf &b) {
 
 }  // namespace
 
+struct Adjoint3State;  // the differentiation form's buffers (made on first use)
+void adjoint3_free(struct svof3d_solver *s);
+
 struct svof3d_solver {
   svof3d_params_t prm{};
   bool mixed = false;  // SVOF3_MIXED or SVOF3_MIXED_DC: FP32 intermediates (see svof3d_b200.h)
@@ -141,6 +146,8 @@ struct svof3d_solver {
   // row-sum scratch (one partial row per z plane, then the result), samples
   DevBuf stat[SVOF3_NSTATS], stat_part;
   size_t stat_num = 0;
+
+  Adjoint3State *adj = nullptr;
 
   Grid3 grid() const { return Grid3{nx, ny, nz, dy, dz, dxf.p, dxc.p}; }
 };
@@ -547,6 +554,7 @@ int svof3d_destroy(svof3d_solver_t *s) {
   if (!s) return 0;
   if (s->stream) cudaStreamSynchronize(s->stream);
   io_free(s);
+  adjoint3_free(s);
   for (auto &kv : s->graphs) cudaGraphExecDestroy(kv.second);
   s->graphs.clear();
   for (int k = 0; k < 2; k++) {
@@ -1091,6 +1099,394 @@ int svof3d_synchronize(svof3d_solver_t *s) {
 int svof3d_stream(svof3d_solver_t *s, void **stream) {
   if (!s || !stream) return fail("null argument");
   *stream = (void *)s->stream;
+  return 0;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// The differentiation form of the 3D FP64 path (no counterpart in the
+// reference), the 2D form (adjoint.cu) carried to the third direction: a
+// differentiated run holds the time-step sequence fixed; svof3d_integrate_fixed
+// takes one step with a given dt and, when asked, records the primal inputs
+// of its three substeps (ux, uy, uz, vof, storage layouts) on a tape in device
+// memory; svof3d_adjoint_step maps the adjoint of a step's outputs (ux, uy,
+// uz, p, vof) to the adjoint of its inputs in place and accumulates the
+// adjoint of the surface-tension coefficient 1/We.  Per substep, in reverse:
+// the projection and pressure update, the Poisson solve (a second solve, of
+// psi_bar / dxf, by the forward's own transforms and line solves), the
+// implicit-x line solves, the momentum right-hand sides, the vof fluxes and
+// update, the CSF force, the intercept and normals, the corner gradients
+// (k3_adjoint.cu).  The per-function entry points expose the same pieces one
+// by one about the solver's current fields.  The temperature is not
+// differentiated (add_buoyancy must be 0); the mixed paths have no adjoint.
+
+struct Adjoint3State {
+  // compact: ux faces nz x ny x (nx-1), cells nz x ny x nx
+  DevBuf ux, uy, uz, p, vof[2], pend_v[2];
+  DevBuf pend_x, pend_y, pend_z, sa_x, sg_x, sa_y, sg_y, sa_z, sg_z, ifx, ify, ifz, kap, m, nrm, sig;
+  DevBuf psib, b, psis, gbar, sum;
+  int cv = 0;  // current buffer of vof_bar
+  int cp = 0;  // current buffer of the vof source's pending adjoint
+  int xs_rows = 1;
+  size_t xs_smem = 0;
+  DevBuf *all(int q) {
+    DevBuf *l[] = {&ux, &uy, &uz, &p, &vof[0], &vof[1], &pend_v[0], &pend_v[1], &pend_x, &pend_y, &pend_z,
+                   &sa_x, &sg_x, &sa_y, &sg_y, &sa_z, &sg_z, &ifx, &ify, &ifz, &kap, &m, &nrm, &sig,
+                   &psib, &b, &psis, &gbar, &sum};
+    return q < (int)(sizeof(l) / sizeof(l[0])) ? l[q] : nullptr;
+  }
+};
+
+void adjoint3_free(svof3d_solver *s) {
+  if (!s || !s->adj) return;
+  for (int q = 0; DevBuf *b = s->adj->all(q); q++) dfree(*b);
+  delete s->adj;
+  s->adj = nullptr;
+}
+
+namespace {
+
+int adj3_ensure(svof3d_solver *s) {
+  if (s->adj) return 0;
+  if (s->mixed) return fail("the adjoint needs the FP64 path (precision SVOF3_FP64)");
+  if (s->prm.add_buoyancy) return fail("the adjoint needs add_buoyancy = 0 (t is not differentiated)");
+  const size_t nx = s->nx, ny = s->ny, nz = s->nz;
+  if (sizeof(double) * 3 * nx > 160 * 1024) return fail("the adjoint's x line solve needs nx <= 6826");
+  Adjoint3State *a = new Adjoint3State();
+  const size_t nc = nx * ny * nz, nf = (nx - 1) * ny * nz, ncc = (nx + 2) * (ny + 2) * (nz + 2);
+  bool bad = dalloc(a->ux, nf) || dalloc(a->uy, nc) || dalloc(a->uz, nc) || dalloc(a->p, nc) ||
+             dalloc(a->vof[0], nc) || dalloc(a->vof[1], nc) || dalloc(a->pend_v[0], nc) ||
+             dalloc(a->pend_v[1], nc) || dalloc(a->pend_x, nf) || dalloc(a->pend_y, nc) || dalloc(a->pend_z, nc) ||
+             dalloc(a->sa_x, nf) || dalloc(a->sg_x, nf) || dalloc(a->sa_y, nc) || dalloc(a->sg_y, nc) ||
+             dalloc(a->sa_z, nc) || dalloc(a->sg_z, nc) || dalloc(a->ifx, nf) || dalloc(a->ify, nc) ||
+             dalloc(a->ifz, nc) || dalloc(a->kap, nc) || dalloc(a->m, 3 * nc) || dalloc(a->nrm, 4 * nc) ||
+             dalloc(a->sig, nc) || dalloc(a->psib, nc) || dalloc(a->b, nc) || dalloc(a->psis, ncc) ||
+             dalloc(a->gbar, 3 * (nx + 1) * ny * nz) || dalloc(a->sum, 1);
+  // transposed line solves: R lines (j, k) per block, 3 R threads at most
+  // 128, blocks covering the SMs twice where the lines allow, within 160 KB
+  const long lines = (long)ny * nz;
+  int r = (int)std::max(1L, std::min(42L, lines / (148L * 2)));
+  while (r > 1 && sizeof(double) * 3 * (size_t)r * nx > 160 * 1024) r--;
+  a->xs_rows = r;
+  a->xs_smem = sizeof(double) * 3 * (size_t)r * nx;
+  if (!bad && cudaSuccess != raise_smem_limit(k3_adj_xsolve, a->xs_smem)) bad = fail("cudaFuncSetAttribute(k3_adj_xsolve)");
+  if (bad) {
+    std::string e = g_err3;
+    s->adj = a;
+    adjoint3_free(s);
+    g_err3 = e.empty() ? "adjoint set-up failed" : e;
+    return 1;
+  }
+  s->adj = a;
+  return 0;
+}
+
+dim3 adj3_cells(const svof3d_solver *s) { return dim3((s->nx + 31) / 32, (s->ny + 7) / 8, s->nz); }
+
+int adj3_set_dt(svof3d_solver *s, double dt) {
+  k3_adj_set<<<1, 1, 0, s->stream>>>(s->d_dt, dt);
+  CK_LAUNCH();
+  return 0;
+}
+
+// fluid_update_pressure (mode 1) and fluid_correct_velocity (mode 2)
+int adj3_project(svof3d_solver *s, int rk, double dt, int mode) {
+  Adjoint3State *a = s->adj;
+  const double gam = RK_A[rk] + RK_B[rk];
+  k3_adj_project<<<adj3_cells(s), dim3(32, 8), 0, s->stream>>>(a->ux.p, a->uy.p, a->uz.p, a->p.p, a->psib.p,
+                                                               gam * dt, 0.5 * gam * dt * s->prm.m_dif, mode,
+                                                               s->grid());
+  CK_LAUNCH();
+  return 0;
+}
+
+// fluid_compute_potential_dft: s = the forward solve of psi_bar / dxf, then
+// the divergence's transpose of pre_p dxf s (the Poisson operator is dxf^-1
+// times a symmetric matrix, so its inverse's transpose is dxf L^-1 dxf^-1)
+int adj3_potential(svof3d_solver *s, int rk, double dt) {
+  Adjoint3State *a = s->adj;
+  const double gam = RK_A[rk] + RK_B[rk];
+  const Grid3 g = s->grid();
+  k3_adj_scale<<<adj3_cells(s), dim3(32, 8), 0, s->stream>>>(a->psib.p, a->b.p, g);
+  CK_LAUNCH();
+  CK(pois_fwd_y_array<double>(s->stream, a->b.p, s->spec.p, s->twf_y.p, s->log2ny, g));
+  CK(pois_z<double>(s->stream, s->spec.p, s->twf_z.p, s->log2nz, g));
+  CK(pois_x<double>(s->stream, s->spec.p, s->xscratch.p, s->pl.p, s->pu.p, s->evy.p, s->evz.p, g, false));
+  CK(pois_z<double>(s->stream, s->spec.p, s->twb_z.p, s->log2nz, g));
+  CK(pois_inv_y<double>(s->stream, s->spec.p, a->psis.p, s->twb_y.p, s->log2ny, g, false));
+  const double pre_p = 1. / (gam * dt) / (1. * s->ny * s->nz);
+  k3_adj_div<<<adj3_cells(s), dim3(32, 8), 0, s->stream>>>(a->ux.p, a->uy.p, a->uz.p, a->psis.p, a->psib.p, pre_p,
+                                                           g);
+  CK_LAUNCH();
+  return 0;
+}
+
+// fluid_predict_field about the primal velocities (storage layouts); d_dt must hold dt
+int adj3_predict(svof3d_solver *s, int rk, double dt, const double *ux, const double *uy, const double *uz) {
+  Adjoint3State *a = s->adj;
+  k3_tdm_coef<<<1, 128, sizeof(double) * 6 * s->nx, s->stream>>>(s->lap_ux.p, s->lap_cc.p, s->d_dt,
+                                                                 RK_A[rk] + RK_B[rk], s->prm.m_dif, s->prm.t_dif,
+                                                                 s->nx, s->coef.p);
+  CK_LAUNCH();
+  const int R = a->xs_rows;
+  const long lines = (long)s->ny * s->nz;
+  k3_adj_xsolve<<<(unsigned)((lines + R - 1) / R), 128, a->xs_smem, s->stream>>>(
+      a->ux.p, a->uy.p, a->uz.p, s->coef.p, a->sa_x.p, a->sg_x.p, a->sa_y.p, a->sg_y.p, a->sa_z.p, a->sg_z.p,
+      a->pend_x.p, a->pend_y.p, a->pend_z.p, RK_A[rk] * dt, RK_B[rk] * dt, (RK_A[rk] + RK_B[rk]) * dt, R,
+      s->grid());
+  CK_LAUNCH();
+  Adj3RhsArgs r{};
+  r.ux = ux;
+  r.uy = uy;
+  r.uz = uz;
+  r.sa_x = a->sa_x.p;
+  r.sg_x = a->sg_x.p;
+  r.sa_y = a->sa_y.p;
+  r.sg_y = a->sg_y.p;
+  r.sa_z = a->sa_z.p;
+  r.sg_z = a->sg_z.p;
+  r.aux = a->ux.p;
+  r.auy = a->uy.p;
+  r.auz = a->uz.p;
+  r.ap = a->p.p;
+  r.aifx = a->ifx.p;
+  r.aify = a->ify.p;
+  r.aifz = a->ifz.p;
+  r.lap_ux = s->lap_ux.p;
+  r.lap_cc = s->lap_cc.p;
+  r.m_dif = s->prm.m_dif;
+  r.ly0 = s->lapy[0];
+  r.ly1 = s->lapy[1];
+  r.ly2 = s->lapy[2];
+  r.lz0 = s->lapz[0];
+  r.lz1 = s->lapz[1];
+  r.lz2 = s->lapz[2];
+  r.g = s->grid();
+  k3_adj_rhs<<<adj3_cells(s), dim3(32, 8), 0, s->stream>>>(r);
+  CK_LAUNCH();
+  return 0;
+}
+
+// interface_update_vof (mode 1), interface_compute_force (2), the intercept
+// and normal part of interface_compute_curvature_tensor (4), about the primal
+// velocities and vof (storage layouts) and the solver's normal and curv
+int adj3_interface(svof3d_solver *s, int rk, double dt, int mode, const double *ux, const double *uy,
+                   const double *uz, const double *vof) {
+  Adjoint3State *a = s->adj;
+  Adj3IfaceArgs f{};
+  f.ux = ux;
+  f.uy = uy;
+  f.uz = uz;
+  f.vof = vof;
+  f.normal = s->normal.p;
+  f.curv = s->curv.p;
+  f.avof_in = a->vof[a->cv].p;
+  f.avof_out = a->vof[1 - a->cv].p;
+  f.pend_in = a->pend_v[a->cp].p;
+  f.pend_out = a->pend_v[1 - a->cp].p;
+  f.aux = a->ux.p;
+  f.auy = a->uy.p;
+  f.auz = a->uz.p;
+  f.aifx = a->ifx.p;
+  f.aify = a->ify.p;
+  f.aifz = a->ifz.p;
+  f.anrm = a->nrm.p;
+  f.am = a->m.p;
+  f.akap = a->kap.p;
+  f.asig = a->sig.p;
+  f.adt = RK_A[rk] * dt;
+  f.bdt = RK_B[rk] * dt;
+  f.tension = s->prm.tension;
+  f.mode = mode;
+  f.g = s->grid();
+  k3_adj_interface<<<adj3_cells(s), dim3(32, 8), 0, s->stream>>>(f);
+  CK_LAUNCH();
+  a->cv ^= 1;
+  if (mode & 1) a->cp ^= 1;
+  return 0;
+}
+
+// the corner normals and curvature part of interface_compute_curvature_tensor
+int adj3_corners(svof3d_solver *s, const double *vof) {
+  Adjoint3State *a = s->adj;
+  const Grid3 g = s->grid();
+  k3_adj_cgrad<<<dim3((s->nx + 1 + 31) / 32, (s->ny + 7) / 8, s->nz), dim3(32, 8), 0, s->stream>>>(
+      vof, a->m.p, a->kap.p, a->gbar.p, g);
+  CK_LAUNCH();
+  k3_adj_cvof<<<adj3_cells(s), dim3(32, 8), 0, s->stream>>>(a->gbar.p, a->vof[a->cv].p, g);
+  CK_LAUNCH();
+  return 0;
+}
+
+size_t n_ux3(const svof3d_solver *s) { return (size_t)(s->nx + 1) * (s->ny + 2) * (s->nz + 2); }
+size_t n_cc3(const svof3d_solver *s) { return (size_t)(s->nx + 2) * (s->ny + 2) * (s->nz + 2); }
+size_t n_vof3(const svof3d_solver *s) { return (size_t)(s->nx + 2) * (s->ny + 4) * (s->nz + 4); }
+// one substep's part of a tape: ux, uy, uz, vof
+size_t tape_stride3(const svof3d_solver *s) { return n_ux3(s) + 2 * n_cc3(s) + n_vof3(s); }
+
+int adj3_check(svof3d_solver *s) {
+  if (!s) return fail("null argument");
+  return adj3_ensure(s);
+}
+
+}  // namespace
+
+extern "C" {
+
+int svof3d_set_tension(svof3d_solver_t *s, double tension) {
+  if (!s) return fail("null argument");
+  CK(cudaStreamSynchronize(s->stream));
+  s->prm.tension = tension;
+  for (auto &kv : s->graphs) cudaGraphExecDestroy(kv.second);
+  s->graphs.clear();
+  return 0;
+}
+
+int svof3d_tape_count(const svof3d_solver_t *s, size_t *count) {
+  if (!s || !count) return fail("null argument");
+  *count = 3 * tape_stride3(s);
+  return 0;
+}
+
+int svof3d_integrate_fixed(svof3d_solver_t *s, double dt, double *tape) {
+  SVOF_RANGE();
+  if (!s) return fail("null argument");
+  if (!(dt > 0.)) return fail("svof3d_integrate_fixed: dt must be positive");
+  if (adj3_set_dt(s, dt)) return 1;
+  const size_t nu = n_ux3(s), nc = n_cc3(s), nv = n_vof3(s), st = tape_stride3(s);
+  for (int rk = 0; rk < 3; rk++) {
+    if (tape) {
+      double *t = tape + rk * st;
+      const int cu = s->cur_u;
+      CK(cudaMemcpyAsync(t, s->ux[cu].p, sizeof(double) * nu, cudaMemcpyDeviceToDevice, s->stream));
+      CK(cudaMemcpyAsync(t + nu, s->uy[cu].p, sizeof(double) * nc, cudaMemcpyDeviceToDevice, s->stream));
+      CK(cudaMemcpyAsync(t + nu + nc, s->uz[cu].p, sizeof(double) * nc, cudaMemcpyDeviceToDevice, s->stream));
+      CK(cudaMemcpyAsync(t + nu + 2 * nc, s->vof[s->cur_v].p, sizeof(double) * nv, cudaMemcpyDeviceToDevice,
+                         s->stream));
+    }
+    if (launch_geom(s) || launch_force(s) || launch_vof(s, rk) || launch_predict(s, rk) ||
+        launch_potential(s, rk) || launch_project(s, rk, 1, 1))
+      return 1;
+  }
+  return 0;
+}
+
+int svof3d_adjoint_field(svof3d_solver_t *s, int which, double **dptr, size_t *count) {
+  if (!s || !dptr) return fail("null argument");
+  if (adj3_ensure(s)) return 1;
+  Adjoint3State *a = s->adj;
+  const size_t nc = (size_t)s->nx * s->ny * s->nz, nf = (size_t)(s->nx - 1) * s->ny * s->nz;
+  DevBuf *b = nullptr;
+  size_t n = nc;
+  switch (which) {
+    case SVOF3_ADJ_UX: b = &a->ux; n = nf; break;
+    case SVOF3_ADJ_UY: b = &a->uy; break;
+    case SVOF3_ADJ_UZ: b = &a->uz; break;
+    case SVOF3_ADJ_P: b = &a->p; break;
+    case SVOF3_ADJ_VOF: b = &a->vof[a->cv]; break;
+    case SVOF3_ADJ_PSI: b = &a->psib; break;
+    case SVOF3_ADJ_IFRCX: b = &a->ifx; n = nf; break;
+    case SVOF3_ADJ_IFRCY: b = &a->ify; break;
+    case SVOF3_ADJ_IFRCZ: b = &a->ifz; break;
+    case SVOF3_ADJ_CURV: b = &a->kap; break;
+    case SVOF3_ADJ_NORMAL: b = &a->nrm; n = 4 * nc; break;
+    case SVOF3_ADJ_SRCUX_A: b = &a->pend_x; n = nf; break;
+    case SVOF3_ADJ_SRCUY_A: b = &a->pend_y; break;
+    case SVOF3_ADJ_SRCUZ_A: b = &a->pend_z; break;
+    case SVOF3_ADJ_SRC_A: b = &a->pend_v[a->cp]; break;
+    case SVOF3_ADJ_TENSION: b = &a->sig; break;
+    default: return fail("unknown adjoint field %d", which);
+  }
+  *dptr = b->p;
+  if (count) *count = n;
+  return 0;
+}
+
+int svof3d_adjoint_reset(svof3d_solver_t *s) {
+  if (adj3_check(s)) return 1;
+  for (int q = 0; DevBuf *b = s->adj->all(q); q++) CK(cudaMemsetAsync(b->p, 0, sizeof(double) * b->n, s->stream));
+  return 0;
+}
+
+int svof3d_adjoint_step(svof3d_solver_t *s, const double *tape, double dt) {
+  SVOF_RANGE();
+  if (adj3_check(s)) return 1;
+  if (!tape) return fail("svof3d_adjoint_step: null tape");
+  if (!(dt > 0.)) return fail("svof3d_adjoint_step: dt must be positive");
+  Adjoint3State *a = s->adj;
+  const size_t nu = n_ux3(s), nc = n_cc3(s), st = tape_stride3(s);
+  // no substep follows the last one: its sources' pending adjoints are zero
+  DevBuf *pend[] = {&a->pend_x, &a->pend_y, &a->pend_z, &a->pend_v[a->cp]};
+  for (DevBuf *b : pend) CK(cudaMemsetAsync(b->p, 0, sizeof(double) * b->n, s->stream));
+  if (adj3_set_dt(s, dt)) return 1;
+  for (int rk = 2; rk >= 0; rk--) {
+    const double *ux = tape + rk * st, *uy = ux + nu, *uz = uy + nc, *vof = uz + nc;
+    // the substep's geometry (normals, intercepts, curvature) from its vof
+    CK(interface_geom<double>(s->stream, vof, s->normal.as<double>(), s->curv.as<double>(), s->d_work, s->d_nwork,
+                              s->grid()));
+    if (adj3_project(s, rk, dt, 3) || adj3_potential(s, rk, dt) || adj3_predict(s, rk, dt, ux, uy, uz) ||
+        adj3_interface(s, rk, dt, 7, ux, uy, uz, vof) || adj3_corners(s, vof))
+      return 1;
+  }
+  return 0;
+}
+
+#define ADJ3_PRIMAL s->ux[s->cur_u].p, s->uy[s->cur_u].p, s->uz[s->cur_u].p
+
+int svof3d_adjoint_fluid_update_pressure(svof3d_solver_t *s, size_t rk, double dt) {
+  SVOF_RANGE();
+  if (adj3_check(s) || check_rk(rk)) return 1;
+  return adj3_project(s, (int)rk, dt, 1) || finish(s);
+}
+
+int svof3d_adjoint_fluid_correct_velocity(svof3d_solver_t *s, size_t rk, double dt) {
+  SVOF_RANGE();
+  if (adj3_check(s) || check_rk(rk)) return 1;
+  return adj3_project(s, (int)rk, dt, 2) || finish(s);
+}
+
+int svof3d_adjoint_fluid_compute_potential_dft(svof3d_solver_t *s, size_t rk, double dt) {
+  SVOF_RANGE();
+  if (adj3_check(s) || check_rk(rk)) return 1;
+  return adj3_potential(s, (int)rk, dt) || finish(s);
+}
+
+int svof3d_adjoint_fluid_predict_field(svof3d_solver_t *s, size_t rk, double dt) {
+  SVOF_RANGE();
+  if (adj3_check(s) || check_rk(rk)) return 1;
+  return adj3_set_dt(s, dt) || adj3_predict(s, (int)rk, dt, ADJ3_PRIMAL) || finish(s);
+}
+
+int svof3d_adjoint_interface_update_vof(svof3d_solver_t *s, size_t rk, double dt) {
+  SVOF_RANGE();
+  if (adj3_check(s) || check_rk(rk)) return 1;
+  return adj3_interface(s, (int)rk, dt, 1, ADJ3_PRIMAL, s->vof[s->cur_v].p) || finish(s);
+}
+
+int svof3d_adjoint_interface_compute_force(svof3d_solver_t *s) {
+  SVOF_RANGE();
+  if (adj3_check(s)) return 1;
+  return adj3_interface(s, 0, 0., 2, ADJ3_PRIMAL, s->vof[s->cur_v].p) || finish(s);
+}
+
+int svof3d_adjoint_interface_compute_curvature_tensor(svof3d_solver_t *s) {
+  SVOF_RANGE();
+  if (adj3_check(s)) return 1;
+  const double *vof = s->vof[s->cur_v].p;
+  return adj3_interface(s, 0, 0., 4, ADJ3_PRIMAL, vof) || adj3_corners(s, vof) || finish(s);
+}
+
+#undef ADJ3_PRIMAL
+
+int svof3d_adjoint_tension(svof3d_solver_t *s, double *out) {
+  if (adj3_check(s)) return 1;
+  if (!out) return fail("null argument");
+  Adjoint3State *a = s->adj;
+  k3_adj_sum<<<1, 256, 0, s->stream>>>(a->sig.p, (long)a->sig.n, a->sum.p);
+  CK_LAUNCH();
+  CK(cudaMemcpyAsync(out, a->sum.p, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
   return 0;
 }
 

@@ -46,7 +46,25 @@ EXPORTS3D = ["svof3d_create", "svof3d_destroy", "svof3d_field_count", "svof3d_up
              "svof3d_fluid_update_pressure", "svof3d_integrate", "svof3d_run", "svof3d_enqueue_steps",
              "svof3d_last_dt", "svof3d_diagnostics", "svof3d_profile_step", "svof3d_synchronize",
              "svof3d_stream", "svof3d_last_error", "svof3d_statistics_collect", "svof3d_statistics_reset",
-             "svof3d_statistics_count", "svof3d_statistics_reduce", "svof3d_statistics_field"]
+             "svof3d_statistics_count", "svof3d_statistics_reduce", "svof3d_statistics_field",
+             "svof3d_set_tension", "svof3d_tape_count", "svof3d_integrate_fixed", "svof3d_adjoint_field",
+             "svof3d_adjoint_reset", "svof3d_adjoint_step", "svof3d_adjoint_fluid_update_pressure",
+             "svof3d_adjoint_fluid_correct_velocity", "svof3d_adjoint_fluid_compute_potential_dft",
+             "svof3d_adjoint_fluid_predict_field", "svof3d_adjoint_interface_update_vof",
+             "svof3d_adjoint_interface_compute_force", "svof3d_adjoint_interface_compute_curvature_tensor",
+             "svof3d_adjoint_tension"]
+
+# adjoint fields (SVOF3_ADJ_*); compact layouts: ux faces (nz, ny, nx-1), cells (nz, ny, nx)
+ADJ_FIELDS3D = {"ux": 0, "uy": 1, "uz": 2, "p": 3, "vof": 4, "psi": 5, "ifrcx": 6, "ifrcy": 7, "ifrcz": 8,
+                "curv": 9, "normal": 10, "srcux_a": 11, "srcuy_a": 12, "srcuz_a": 13, "src_a": 14, "tension": 15}
+
+
+def adjoint_shape3d(name: str, nx: int, ny: int, nz: int):
+    if name in ("ux", "ifrcx", "srcux_a"):
+        return (nz, ny, nx - 1)
+    if name == "normal":
+        return (nz, ny, nx, 4)
+    return (nz, ny, nx)
 
 # statistics quantities (SVOF3_STAT_*)
 STAT_NAMES3D = ["ux1", "ux2", "uy1", "uy2", "uz1", "uz2", "t1", "t2", "uxt"]
@@ -109,6 +127,19 @@ def lib3() -> ctypes.CDLL:
         L.svof3d_synchronize.argtypes = [vp]
         L.svof3d_stream.argtypes = [vp, ctypes.POINTER(vp)]
         L.svof3d_last_error.restype = ctypes.c_char_p
+        L.svof3d_set_tension.argtypes = [vp, d]
+        L.svof3d_tape_count.argtypes = [vp, ctypes.POINTER(sz)]
+        L.svof3d_integrate_fixed.argtypes = [vp, d, vp]
+        L.svof3d_adjoint_field.argtypes = [vp, i, ctypes.POINTER(vp), ctypes.POINTER(sz)]
+        L.svof3d_adjoint_reset.argtypes = [vp]
+        L.svof3d_adjoint_step.argtypes = [vp, vp, d]
+        for fn in ("svof3d_adjoint_fluid_update_pressure", "svof3d_adjoint_fluid_correct_velocity",
+                   "svof3d_adjoint_fluid_compute_potential_dft", "svof3d_adjoint_fluid_predict_field",
+                   "svof3d_adjoint_interface_update_vof"):
+            getattr(L, fn).argtypes = [vp, sz, d]
+        L.svof3d_adjoint_interface_compute_force.argtypes = [vp]
+        L.svof3d_adjoint_interface_compute_curvature_tensor.argtypes = [vp]
+        L.svof3d_adjoint_tension.argtypes = [vp, pd]
         _bound = True
     return L
 
@@ -358,3 +389,69 @@ class Solver3D:
 
     def synchronize(self):
         _check(lib3().svof3d_synchronize(self._h))
+
+    # ------------------------------------------------------------ differentiation form
+    def device_view(self, name: str):
+        """zero-copy torch view of a field's current device storage (valid
+        until the next call that swaps its buffers; synchronise the solver's
+        stream and torch's around its use)"""
+        import torch
+        from . import _DeviceArray
+        return torch.as_tensor(_DeviceArray(self.device_ptr(name), storage_shape3d(name, self.nx, self.ny, self.nz)),
+                               device="cuda")
+
+    def adjoint_view(self, name: str):
+        """zero-copy torch view of an adjoint field (compact layout)"""
+        import torch
+        from . import _DeviceArray
+        p = ctypes.c_void_p()
+        n = ctypes.c_size_t(0)
+        _check(lib3().svof3d_adjoint_field(self._h, ADJ_FIELDS3D[name], ctypes.byref(p), ctypes.byref(n)))
+        return torch.as_tensor(_DeviceArray(p.value, adjoint_shape3d(name, self.nx, self.ny, self.nz)),
+                               device="cuda")
+
+    def set_tension(self, tension: float):
+        _check(lib3().svof3d_set_tension(self._h, float(tension)))
+        self.params.tension = float(tension)
+
+    def tape_count(self) -> int:
+        n = ctypes.c_size_t(0)
+        _check(lib3().svof3d_tape_count(self._h, ctypes.byref(n)))
+        return int(n.value)
+
+    def integrate_fixed(self, dt: float, tape_ptr: int = 0):
+        """one step with the given dt, enqueued; records the substep inputs at
+        tape_ptr (device memory, tape_count() doubles) when non-zero"""
+        _check(lib3().svof3d_integrate_fixed(self._h, float(dt), ctypes.c_void_p(tape_ptr or None)))
+
+    def adjoint_reset(self):
+        _check(lib3().svof3d_adjoint_reset(self._h))
+
+    def adjoint_step(self, tape_ptr: int, dt: float):
+        _check(lib3().svof3d_adjoint_step(self._h, ctypes.c_void_p(tape_ptr), float(dt)))
+
+    def adjoint_tension(self) -> float:
+        out = ctypes.c_double(0.0)
+        _check(lib3().svof3d_adjoint_tension(self._h, ctypes.byref(out)))
+        return out.value
+
+    def adjoint_fluid_update_pressure(self, rk: int, dt: float):
+        _check(lib3().svof3d_adjoint_fluid_update_pressure(self._h, rk, dt))
+
+    def adjoint_fluid_correct_velocity(self, rk: int, dt: float):
+        _check(lib3().svof3d_adjoint_fluid_correct_velocity(self._h, rk, dt))
+
+    def adjoint_fluid_compute_potential_dft(self, rk: int, dt: float):
+        _check(lib3().svof3d_adjoint_fluid_compute_potential_dft(self._h, rk, dt))
+
+    def adjoint_fluid_predict_field(self, rk: int, dt: float):
+        _check(lib3().svof3d_adjoint_fluid_predict_field(self._h, rk, dt))
+
+    def adjoint_interface_update_vof(self, rk: int, dt: float):
+        _check(lib3().svof3d_adjoint_interface_update_vof(self._h, rk, dt))
+
+    def adjoint_interface_compute_force(self):
+        _check(lib3().svof3d_adjoint_interface_compute_force(self._h))
+
+    def adjoint_interface_compute_curvature_tensor(self):
+        _check(lib3().svof3d_adjoint_interface_compute_curvature_tensor(self._h))

@@ -1,0 +1,393 @@
+"""The CUDA adjoint of the 3D step (FP64 path) against central differences of
+the CUDA forward.
+
+The 3D path has no tangent model in the oracle; its forward is pinned to the
+3D restatement function by function (test_gpu3d_parity.py), so each
+transpose is checked against the forward it transposes: for inputs x, a
+tangent d and an adjoint seed y_bar, <y_bar, (F(x + e d) - F(x - e d)) / 2e>
+(the GPU forward through the C ABI) must equal <d, F^T y_bar> (the GPU
+adjoint).  The linear functions (projection, pressure update, Poisson solve)
+and the quadratic ones (momentum right-hand sides and x solves, CSF force)
+have exact central differences, so those tests take e = 1 and round-off
+tolerances; the THINC fluxes and the geometry are smooth but not
+polynomial and take a small e, with the vof tangent confined to interfacial
+cells away from the 1e-8 thresholds (the branch sets do not change).  The
+step test differentiates two full steps with respect to a discretely
+divergence-free initial velocity direction and the surface-tension
+coefficient.
+"""
+import numpy as np
+import pytest
+
+from simplevofsolver_b200 import DROPLETS3D_ENV, Solver3D, droplets3d, physical_params
+
+pytestmark = pytest.mark.gpu
+
+TOL_LINEAR = 1e-10
+
+
+def make(seed=3):
+    ic = droplets3d(32, 16, 16, ndrops=3, radii=(0.12, 0.2), seed=seed)
+    phys = physical_params(DROPLETS3D_ENV)
+    g = Solver3D(ic, phys)
+    return ic, phys, g
+
+
+def rel(a, b):
+    return abs(a - b) / max(abs(a), abs(b), 1e-300)
+
+
+# ---- layouts: compact (adjoint) <-> restart interior (load_interior) and storage
+def embed(name, c, nx):
+    """compact (nz, ny, nx-1 | nx) -> restart interior with zero x ghosts"""
+    nz, ny = c.shape[:2]
+    out = np.zeros((nz, ny, nx + 1 if name == "ux" else nx + 2))
+    if name == "ux":
+        out[..., 1:nx] = c
+    else:
+        out[..., 1:nx + 1] = c
+    return out
+
+
+def compact(name, a, nx):
+    return a[..., 1:nx] if name == "ux" else a[..., 1:nx + 1]
+
+
+def fill_periodic(a):
+    """the one-deep y and z halos of a storage array (axes 0 = z, 1 = y)"""
+    nz, ny = a.shape[0] - 2, a.shape[1] - 2
+    a[:, 0] = a[:, ny]
+    a[:, ny + 1] = a[:, 1]
+    a[0] = a[nz]
+    a[nz + 1] = a[1]
+
+
+def set_storage_interior(g, name, c):
+    """writes the interior of a halo'd storage field (curv: (nz, ny, nx);
+    normal: (nz, ny, nx, 4)) with periodic halo copies"""
+    s = g.field(name)
+    if name == "normal":
+        s[1:-1, 1:-1] = c
+    else:
+        s[1:-1, 1:-1, 1:g.nx + 1] = c
+    fill_periodic(s)
+    g.set_field(name, s)
+
+
+def storage_interior(g, name):
+    s = g.field(name)
+    return s[1:-1, 1:-1].copy() if name == "normal" else s[1:-1, 1:-1, 1:g.nx + 1].copy()
+
+
+def put_adj(g, name, x):
+    import torch
+    g.synchronize()
+    g.adjoint_view(name).copy_(torch.as_tensor(np.ascontiguousarray(x), device="cuda"))
+    torch.cuda.synchronize()
+
+
+def get_adj(g, name):
+    import torch
+    g.synchronize()
+    torch.cuda.synchronize()
+    return g.adjoint_view(name).cpu().numpy().copy()
+
+
+def shapes(g):
+    nx, ny, nz = g.nx, g.ny, g.nz
+    return (nz, ny, nx - 1), (nz, ny, nx)
+
+
+class State:
+    """a base state (restart interiors, storage interiors, compact arrays)
+    and its loading with a tangent scaled by e"""
+
+    INTERIOR = ("ux", "uy", "uz", "p", "psi", "vof", "t")
+    STORAGE = ("curv", "normal")
+
+    def __init__(self, g, names):
+        self.g = g
+        self.base = {}
+        for n in names:
+            if n in self.INTERIOR:
+                self.base[n] = g.interior(n)
+            elif n in self.STORAGE:
+                self.base[n] = storage_interior(g, n)
+            else:
+                self.base[n] = g.field(n)
+
+    def load(self, d=None, e=0.0):
+        g = self.g
+        for n, b in self.base.items():
+            x = b.copy()
+            if d is not None and n in d:
+                x = x + e * (embed(n, d[n], g.nx) if n in self.INTERIOR else d[n])
+            if n in self.INTERIOR:
+                g.load_interior(n, x)
+            elif n in self.STORAGE:
+                set_storage_interior(g, n, x)
+            else:
+                g.set_field(n, x)
+        g.synchronize()
+
+
+def read(g, n):
+    return compact(n, g.interior(n), g.nx) if n in State.INTERIOR else (
+        storage_interior(g, n) if n in State.STORAGE else g.field(n))
+
+
+def central(state, d, e, run, outs, seeds):
+    """<seeds, (F(x + e d) - F(x - e d)) / 2e> over the outputs outs"""
+    vals = []
+    for sgn in (+1.0, -1.0):
+        state.load(d, sgn * e)
+        run()
+        vals.append({n: read(state.g, n) for n in outs})
+    return sum(float(np.sum(seeds[n] * (vals[0][n] - vals[1][n]) / (2.0 * e))) for n in outs)
+
+
+def interfacial_cells(g, lo=1e-4):
+    v = compact("vof", g.interior("vof"), g.nx)
+    return (v > lo) & (v < 1.0 - lo)
+
+
+@pytest.mark.parametrize("rk", [0, 2])
+def test_update_pressure_and_correct_velocity(gpu_available, rk):
+    ic, phys, g = make()
+    dt = 1.3e-3
+    rng = np.random.default_rng(1)
+    fs, cs = shapes(g)
+    d = {"ux": rng.standard_normal(fs), "uy": rng.standard_normal(cs), "uz": rng.standard_normal(cs),
+         "p": rng.standard_normal(cs), "psi": rng.standard_normal(cs)}
+    g.load_interior("psi", embed("psi", rng.standard_normal(cs), g.nx))
+    st = State(g, ("ux", "uy", "uz", "p", "psi"))
+    seeds = {"ux": rng.standard_normal(fs), "uy": rng.standard_normal(cs), "uz": rng.standard_normal(cs),
+             "p": rng.standard_normal(cs)}
+
+    def run():
+        g.fluid_correct_velocity(rk, dt)
+        g.fluid_update_pressure(rk, dt)
+
+    lhs = central(st, d, 1.0, run, ("ux", "uy", "uz", "p"), seeds)
+    st.load()
+    g.adjoint_reset()
+    for n, v in seeds.items():
+        put_adj(g, n, v)
+    g.adjoint_fluid_update_pressure(rk, dt)
+    g.adjoint_fluid_correct_velocity(rk, dt)
+    rhs = sum(float(np.sum(d[n] * get_adj(g, n))) for n in ("ux", "uy", "uz", "p", "psi"))
+    assert rel(lhs, rhs) <= TOL_LINEAR, (lhs, rhs)
+
+
+@pytest.mark.parametrize("rk", [0, 1])
+def test_compute_potential(gpu_available, rk):
+    ic, phys, g = make()
+    dt = 1.1e-3
+    rng = np.random.default_rng(2)
+    fs, cs = shapes(g)
+    d = {"ux": rng.standard_normal(fs), "uy": rng.standard_normal(cs), "uz": rng.standard_normal(cs)}
+    st = State(g, ("ux", "uy", "uz"))
+    psib = rng.standard_normal(cs)
+    psib -= psib.mean()
+    vals = []
+    for sgn in (+1.0, -1.0):
+        st.load(d, sgn)
+        g.fluid_compute_potential_dft(rk, dt)
+        vals.append(read(g, "psi"))
+    dpsi = (vals[0] - vals[1]) / 2.0
+    # psi is fixed up to a constant (the singular mode's round-off)
+    lhs = float(np.sum(psib * (dpsi - dpsi.mean())))
+    st.load()
+    g.adjoint_reset()
+    put_adj(g, "psi", psib)
+    g.adjoint_fluid_compute_potential_dft(rk, dt)
+    rhs = sum(float(np.sum(d[n] * get_adj(g, n))) for n in ("ux", "uy", "uz"))
+    assert rel(lhs, rhs) <= TOL_LINEAR, (lhs, rhs)
+    assert np.all(get_adj(g, "psi") == 0.0)
+
+
+@pytest.mark.parametrize("rk", [0, 2])
+def test_predict_field(gpu_available, rk):
+    ic, phys, g = make()
+    dt = 1.2e-3
+    rng = np.random.default_rng(3)
+    fs, cs = shapes(g)
+    # src_b of this substep is the current src_a (the call swaps them first)
+    for n, sh in (("srcux_a", fs), ("srcuy_a", cs), ("srcuz_a", cs)):
+        g.set_field(n, rng.standard_normal(sh))
+    for n, sh in (("ifrcx", fs), ("ifrcy", cs), ("ifrcz", cs)):
+        g.set_field(n, rng.standard_normal(sh))
+    names = ("ux", "uy", "uz", "p", "ifrcx", "ifrcy", "ifrcz", "srcux_a", "srcuy_a", "srcuz_a")
+    st = State(g, names)
+    d = {n: rng.standard_normal(st.base[n].shape if n not in State.INTERIOR else
+                                (fs if n == "ux" else cs)) for n in names}
+    seeds = {n: rng.standard_normal(fs if n in ("ux", "srcux_a") else cs)
+             for n in ("ux", "uy", "uz", "srcux_a", "srcuy_a", "srcuz_a")}
+
+    def run():
+        g.fluid_predict_field(rk, dt)
+
+    lhs = central(st, d, 1.0, run, tuple(seeds), seeds)
+    st.load()
+    g.adjoint_reset()
+    for n, v in seeds.items():
+        put_adj(g, n, v)
+    g.adjoint_fluid_predict_field(rk, dt)
+    rhs = 0.0
+    for n in ("ux", "uy", "uz", "p", "ifrcx", "ifrcy", "ifrcz"):
+        rhs += float(np.sum(d[n] * get_adj(g, n)))
+    if rk != 0:
+        for n in ("srcux_a", "srcuy_a", "srcuz_a"):
+            rhs += float(np.sum(d[n] * get_adj(g, n)))
+    assert rel(lhs, rhs) <= 1e-9, (lhs, rhs)
+
+
+@pytest.mark.parametrize("rk", [0, 1])
+def test_update_vof(gpu_available, rk):
+    ic, phys, g = make()
+    dt = 1.0e-3
+    rng = np.random.default_rng(4)
+    fs, cs = shapes(g)
+    g.interface_compute_curvature_tensor()
+    g.set_field("src_a", rng.standard_normal(cs))
+    mask = interfacial_cells(g)
+    assert mask.sum() > 50
+    names = ("ux", "uy", "uz", "vof", "normal", "src_a")
+    st = State(g, names)
+    d = {"ux": rng.standard_normal(fs), "uy": rng.standard_normal(cs), "uz": rng.standard_normal(cs),
+         "vof": rng.standard_normal(cs) * mask, "normal": rng.standard_normal(cs + (4,)) * mask[..., None],
+         "src_a": rng.standard_normal(cs)}
+    seeds = {"vof": rng.standard_normal(cs), "src_a": rng.standard_normal(cs)}
+
+    def run():
+        g.interface_update_vof(rk, dt)
+
+    lhs = central(st, d, 1e-6, run, ("vof", "src_a"), seeds)
+    st.load()
+    g.adjoint_reset()
+    put_adj(g, "vof", seeds["vof"])
+    put_adj(g, "src_a", seeds["src_a"])
+    g.adjoint_interface_update_vof(rk, dt)
+    rhs = sum(float(np.sum(d[n] * get_adj(g, n))) for n in ("ux", "uy", "uz", "vof", "normal"))
+    if rk != 0:
+        rhs += float(np.sum(d["src_a"] * get_adj(g, "src_a")))
+    assert rel(lhs, rhs) <= 1e-7, (lhs, rhs)
+
+
+def test_compute_force(gpu_available):
+    ic, phys, g = make()
+    rng = np.random.default_rng(5)
+    fs, cs = shapes(g)
+    g.interface_compute_curvature_tensor()
+    st = State(g, ("vof", "curv"))
+    d = {"vof": rng.standard_normal(cs), "curv": rng.standard_normal(cs)}
+    dten = 0.37
+    seeds = {"ifrcx": rng.standard_normal(fs), "ifrcy": rng.standard_normal(cs), "ifrcz": rng.standard_normal(cs)}
+    ten = phys["tension"]
+    # the force is trilinear in (tension, vof, curv): central differences
+    # are exact along (vof, curv) at fixed tension and along the tension alone
+    lhs = 0.0
+    for dd, dt_ in ((d, 0.0), (None, dten)):
+        vals = []
+        for sgn in (+1.0, -1.0):
+            st.load(dd, sgn)
+            g.set_tension(ten + sgn * dt_)
+            g.interface_compute_force()
+            vals.append({n: g.field(n) for n in seeds})
+        lhs += sum(float(np.sum(seeds[n] * (vals[0][n] - vals[1][n]) / 2.0)) for n in seeds)
+    g.set_tension(ten)
+    st.load()
+    g.adjoint_reset()
+    for n, v in seeds.items():
+        put_adj(g, n, v)
+    g.adjoint_interface_compute_force()
+    rhs = (float(np.sum(d["vof"] * get_adj(g, "vof"))) + float(np.sum(d["curv"] * get_adj(g, "curv")))
+           + dten * g.adjoint_tension())
+    assert rel(lhs, rhs) <= TOL_LINEAR, (lhs, rhs)
+
+
+def test_compute_curvature_tensor(gpu_available):
+    ic, phys, g = make()
+    rng = np.random.default_rng(6)
+    fs, cs = shapes(g)
+    mask = interfacial_cells(g)
+    inter = interfacial_cells(g, 1e-8)
+    st = State(g, ("vof",))
+    d = {"vof": rng.standard_normal(cs) * mask}
+    seeds = {"normal": rng.standard_normal(cs + (4,)) * inter[..., None], "curv": rng.standard_normal(cs)}
+
+    def run():
+        g.interface_compute_curvature_tensor()
+
+    lhs = central(st, d, 1e-7, run, ("normal", "curv"), seeds)
+    st.load()
+    g.interface_compute_curvature_tensor()
+    g.adjoint_reset()
+    put_adj(g, "normal", seeds["normal"])
+    put_adj(g, "curv", seeds["curv"])
+    g.adjoint_interface_compute_curvature_tensor()
+    rhs = float(np.sum(d["vof"] * get_adj(g, "vof")))
+    assert rel(lhs, rhs) <= 1e-6, (lhs, rhs)
+
+
+def test_two_steps(gpu_available):
+    """two full steps (fixed dt): the directional derivative along a
+    divergence-free velocity and the tension against the adjoint"""
+    import torch
+    ic, phys, g = make()
+    nx = g.nx
+    fs, cs = shapes(g)
+    dt = g.fluid_decide_dt()
+    rng = np.random.default_rng(7)
+    # a discretely divergence-free direction: the generator's velocity of another seed
+    dirn = droplets3d(32, 16, 16, ndrops=1, radii=(0.12, 0.13), seed=11)
+    d = {"ux": compact("ux", dirn.ux, nx), "uy": compact("uy", dirn.uy, nx), "uz": compact("uz", dirn.uz, nx)}
+    dten = 0.3 * phys["tension"]
+    seeds = {"ux": rng.standard_normal(fs), "uy": rng.standard_normal(cs), "uz": rng.standard_normal(cs),
+             "p": rng.standard_normal(cs)}
+    seeds["p"] -= seeds["p"].mean()
+    yc = (np.arange(g.ny) + 0.5) / g.ny
+    seeds["vof"] = np.broadcast_to(yc[None, :, None], cs).copy()
+    nsteps = 2
+
+    def J(e):
+        for n, v in ic.fields().items():
+            x = v.copy()
+            if n in d:
+                x = x + e * embed(n, d[n], nx)
+            g.load_interior(n, x)
+        g.set_tension(phys["tension"] + e * dten)
+        for _ in range(nsteps):
+            g.integrate_fixed(dt)
+        g.synchronize()
+        return sum(float(np.sum(seeds[n] * read(g, n))) for n in seeds)
+
+    e = 1e-6
+    lhs = (J(e) - J(-e)) / (2 * e)
+    # the adjoint: recorded forward, then the step adjoints in reverse
+    for n, v in ic.fields().items():
+        g.load_interior(n, v)
+    g.set_tension(phys["tension"])
+    tapes = [torch.empty(g.tape_count(), dtype=torch.float64, device="cuda") for _ in range(nsteps)]
+    for t in tapes:
+        g.integrate_fixed(dt, t.data_ptr())
+    g.synchronize()
+    g.adjoint_reset()
+    for n, v in seeds.items():
+        put_adj(g, n, v)
+    for t in reversed(tapes):
+        g.adjoint_step(t.data_ptr(), dt)
+    rhs = sum(float(np.sum(d[n] * get_adj(g, n))) for n in d) + dten * g.adjoint_tension()
+    assert rel(lhs, rhs) <= 1e-5, (lhs, rhs)
+
+
+def test_adjoint_needs_fp64():
+    """the mixed paths have no adjoint (host check, no kernel runs)"""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from simplevofsolver_b200 import SvofError
+    ic = droplets3d(32, 16, 16, ndrops=3, radii=(0.12, 0.2), seed=3)
+    g = Solver3D(ic, physical_params(DROPLETS3D_ENV), precision="mixed")
+    with pytest.raises(SvofError, match="FP64"):
+        g.adjoint_reset()
