@@ -1,4 +1,6 @@
-"""Differentiation form of the 2D FP64 path: gradients through a rollout.
+"""Differentiation form of the FP64 paths: gradients through a rollout
+(2D: :class:`Rollout`; 3D: :class:`Rollout3D`, the same design with uz and
+without the vof buoyancy extension).
 
 ``Rollout`` runs ``len(dts)`` time steps of the CUDA solver with the time-step
 sequence held fixed (``svof_integrate_fixed``) and is differentiable with
@@ -205,6 +207,160 @@ def rollout(ux0, uy0, vof0, tension, r: Rollout, grav=None):
     return _RF.apply(ux0, uy0, vof0, tension, grav, r)
 
 
+def _to_interior3(name, a, nx):
+    """compact (device tensor, (nz, ny, nx-1 | nx)) -> restart interior (numpy)"""
+    a = a.detach().to("cpu").double().numpy()
+    nz, ny = a.shape[:2]
+    out = np.zeros((nz, ny, nx + 1) if name == "ux" else (nz, ny, nx + 2))
+    if name == "ux":
+        out[..., 1:nx] = a
+    else:
+        out[..., 1:nx + 1] = a
+    return out
+
+
+class Rollout3D:
+    """The 3D form of :class:`Rollout`: ``len(dts)`` steps of a
+    :class:`simplevofsolver_b200.solver3d.Solver3D` (precision "fp64") with
+    the time steps held fixed (``svof3d_integrate_fixed``), differentiable
+    with respect to the initial ux, uy, uz, vof and 1/We through
+    :func:`rollout3d`; the backward pass recomputes each segment of K steps
+    from its checkpoint with tapes and applies the CUDA step adjoints
+    (``svof3d_adjoint_step``, ``csrc/k3_adjoint.cu``) in reverse.  The
+    initial velocity is projected onto discretely divergence-free fields
+    first (``project_initial``), as in 2D.  Compact layouts: ux (nz, ny,
+    nx-1), cells (nz, ny, nx)."""
+
+    STATE = ("ux", "uy", "uz", "p", "t", "vof")
+
+    def __init__(self, solver, dts, checkpoint_every: int = 20, project_initial: bool = True):
+        import torch
+        if checkpoint_every < 1:
+            raise ValueError("checkpoint_every must be at least 1")
+        self.s = solver
+        self.dts = [float(x) for x in dts]
+        self.K = int(checkpoint_every)
+        self.nx, self.ny, self.nz = solver.nx, solver.ny, solver.nz
+        self.p0 = solver.interior("p")
+        self.t0 = solver.interior("t")
+        self.tapes = None
+        self.checkpoints = []
+        self.project = bool(project_initial)
+        self._torch = torch
+
+    def _sync(self):
+        self.s.synchronize()
+        self._torch.cuda.synchronize()
+
+    def load(self, ux0, uy0, uz0, vof0, tension):
+        s = self.s
+        s.set_tension(float(tension))
+        for name, a in (("ux", ux0), ("uy", uy0), ("uz", uz0), ("vof", vof0)):
+            s.load_interior(name, _to_interior3(name, a, self.nx))
+        s.load_interior("p", self.p0)
+        s.load_interior("t", self.t0)
+        if self.project:
+            s.fluid_compute_potential_dft(0, 1.0)
+            s.fluid_correct_velocity(0, 1.0)
+
+    def _save_state(self):
+        self._sync()
+        return {k: self.s.device_view(k).clone() for k in self.STATE}
+
+    def _restore_state(self, st):
+        self._sync()
+        for k in self.STATE:
+            self.s.device_view(k).copy_(st[k])
+        self._torch.cuda.synchronize()
+
+    def outputs(self):
+        self._sync()
+        nx, ny, nz = self.nx, self.ny, self.nz
+        ux = self.s.device_view("ux")[1:nz + 1, 1:ny + 1, 1:nx].clone()
+        uy = self.s.device_view("uy")[1:nz + 1, 1:ny + 1, 1:nx + 1].clone()
+        uz = self.s.device_view("uz")[1:nz + 1, 1:ny + 1, 1:nx + 1].clone()
+        p = self.s.device_view("p")[1:nz + 1, 1:ny + 1, 1:nx + 1].clone()
+        vof = self.s.device_view("vof")[2:nz + 2, 2:ny + 2, 1:nx + 1].clone()
+        return ux, uy, uz, vof, p
+
+    def forward(self, ux0, uy0, uz0, vof0, tension, keep_checkpoints=True):
+        self.load(ux0, uy0, uz0, vof0, tension)
+        self.checkpoints = []
+        for n, dt in enumerate(self.dts):
+            if keep_checkpoints and n % self.K == 0:
+                self.checkpoints.append(self._save_state())
+            self.s.integrate_fixed(dt)
+        return self.outputs()
+
+    def backward(self, gux, guy, guz, gvof, gp):
+        torch = self._torch
+        s = self.s
+        nx, ny, nz = self.nx, self.ny, self.nz
+        if self.tapes is None:
+            self.tapes = [torch.empty(s.tape_count(), dtype=torch.float64, device="cuda") for _ in range(self.K)]
+        s.adjoint_reset()
+        self._sync()
+        dev = dict(dtype=torch.float64, device="cuda")
+        seeds = {"ux": gux if gux is not None else torch.zeros((nz, ny, nx - 1), **dev),
+                 "uy": guy if guy is not None else torch.zeros((nz, ny, nx), **dev),
+                 "uz": guz if guz is not None else torch.zeros((nz, ny, nx), **dev),
+                 "vof": gvof if gvof is not None else torch.zeros((nz, ny, nx), **dev),
+                 "p": gp if gp is not None else torch.zeros((nz, ny, nx), **dev)}
+        seeds["p"] = seeds["p"] - seeds["p"].mean()
+        for k, v in seeds.items():
+            s.adjoint_view(k).copy_(v.double())
+        torch.cuda.synchronize()
+        N = len(self.dts)
+        for seg in reversed(range(len(self.checkpoints))):
+            n0 = seg * self.K
+            n1 = min(N, n0 + self.K)
+            self._restore_state(self.checkpoints[seg])
+            for n in range(n0, n1):
+                s.integrate_fixed(self.dts[n], self.tapes[n - n0].data_ptr())
+            for n in reversed(range(n0, n1)):
+                s.adjoint_step(self.tapes[n - n0].data_ptr(), self.dts[n])
+        if self.project:
+            s.adjoint_fluid_correct_velocity(0, 1.0)
+            s.adjoint_fluid_compute_potential_dft(0, 1.0)
+        self._sync()
+        return (s.adjoint_view("ux").clone(), s.adjoint_view("uy").clone(), s.adjoint_view("uz").clone(),
+                s.adjoint_view("vof").clone(), s.adjoint_tension())
+
+
+def _function3d():
+    import torch
+
+    class Rollout3DFunction(torch.autograd.Function):
+        """(ux0, uy0, uz0, vof0, tension) -> (ux, uy, uz, vof, p) after the
+        rollout's steps; backward through the CUDA step adjoints"""
+
+        @staticmethod
+        def forward(ctx, ux0, uy0, uz0, vof0, tension, rollout):
+            ctx.rollout = rollout
+            ctx.tension_like = tension
+            return rollout.forward(ux0, uy0, uz0, vof0, float(tension))
+
+        @staticmethod
+        def backward(ctx, gux, guy, guz, gvof, gp):
+            g_ux, g_uy, g_uz, g_vof, g_ten = ctx.rollout.backward(gux, guy, guz, gvof, gp)
+            gt = torch.tensor(g_ten, dtype=torch.float64, device=ctx.tension_like.device)
+            return g_ux, g_uy, g_uz, g_vof, gt, None
+
+    return Rollout3DFunction
+
+
+_RF3 = None
+
+
+def rollout3d(ux0, uy0, uz0, vof0, tension, r: Rollout3D):
+    """differentiable 3D rollout: returns (ux, uy, uz, vof, p) after
+    len(r.dts) steps"""
+    global _RF3
+    if _RF3 is None:
+        _RF3 = _function3d()
+    return _RF3.apply(ux0, uy0, uz0, vof0, tension, r)
+
+
 def falling_objective(ux, uy, vof, xf, ly: float = 1.0):
     """the differentiation workload's objective: the vof-weighted centroid y
     of the droplet plus 0.1 times the kinetic energy (the reference's energy
@@ -223,4 +379,4 @@ def falling_objective(ux, uy, vof, xf, ly: float = 1.0):
     return centroid + 0.1 * ke
 
 
-__all__ = ["Rollout", "rollout", "falling_objective", "SvofError"]
+__all__ = ["Rollout", "rollout", "Rollout3D", "rollout3d", "falling_objective", "SvofError"]
