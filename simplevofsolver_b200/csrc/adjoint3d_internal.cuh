@@ -6,22 +6,39 @@
 
 namespace svof3 {
 
+// the grid with the reciprocal spacings the adjoint kernels multiply by (the
+// adjoint follows no reference rounding: no divisions in its kernels)
+struct AGrid3 {
+  Grid3 g;
+  const double *rxf;  // [nx]   1 / dxf
+  const double *rxc;  // [nx+1] 1 / dxc
+  double rdy, rdz;
+};
+
+// lines per block and points per shared-memory chunk of k3_adj_xsolve
+constexpr int kAdjXLines = 128;
+constexpr int kAdjXChunk = 16;
+
 // psi_bar += (d p' / d psi)^T p_bar' (mode & 1), (d u' / d psi)^T u_bar' (mode & 2)
 __global__ void k3_adj_project(const double *__restrict__ aux, const double *__restrict__ auy,
                                const double *__restrict__ auz, const double *__restrict__ ap,
-                               double *__restrict__ apsi, double gdt, double pre, int mode, Grid3 g);
+                               double *__restrict__ apsi, double gdt, double pre, int mode, AGrid3 ag);
 // b = psi_bar / dxf (compact)
-__global__ void k3_adj_scale(const double *__restrict__ apsi, double *__restrict__ b, Grid3 g);
+__global__ void k3_adj_scale(const double *__restrict__ apsi, double *__restrict__ b, AGrid3 ag);
 // u_bar += the divergence's transpose of pre_p dxf s; psi_bar = 0
 __global__ void k3_adj_div(double *__restrict__ aux, double *__restrict__ auy, double *__restrict__ auz,
-                           const double *__restrict__ s, double *__restrict__ apsi, double pre_p, Grid3 g);
-// transposed implicit-x solves and the RK split; dynamic shared memory 3 R nx doubles
+                           const double *__restrict__ s, double *__restrict__ apsi, double pre_p, AGrid3 ag);
+// transposed implicit-x solves and the RK split: grid (lines / kAdjXLines,
+// 3 fields), kAdjXLines threads, dynamic shared memory adj_xsolve_smem(nx)
 __global__ void k3_adj_xsolve(const double *__restrict__ aux, const double *__restrict__ auy,
                               const double *__restrict__ auz, const double *__restrict__ coef,
                               double *__restrict__ sa_x, double *__restrict__ sg_x, double *__restrict__ sa_y,
                               double *__restrict__ sg_y, double *__restrict__ sa_z, double *__restrict__ sg_z,
                               double *__restrict__ pend_x, double *__restrict__ pend_y, double *__restrict__ pend_z,
-                              double adt, double bdt, double gdt, int R, Grid3 g);
+                              double adt, double bdt, double gdt, Grid3 g);
+inline size_t adj_xsolve_smem(int nx) {
+  return sizeof(double) * (3 * (size_t)nx + (size_t)kAdjXLines * (kAdjXChunk + 1));
+}
 
 struct Adj3RhsArgs {
   const double *ux, *uy, *uz;                               // primal, storage layouts
@@ -29,7 +46,7 @@ struct Adj3RhsArgs {
   double *aux, *auy, *auz, *ap, *aifx, *aify, *aifz;
   const double *lap_ux, *lap_cc;
   double m_dif, ly0, ly1, ly2, lz0, lz1, lz2;
-  Grid3 g;
+  AGrid3 ag;
 };
 __global__ void k3_adj_rhs(Adj3RhsArgs a);
 
@@ -45,15 +62,15 @@ struct Adj3IfaceArgs {
   double *asig;                                      // tension adjoint, per cell, +=
   double adt, bdt, tension;
   int mode;
-  Grid3 g;
+  AGrid3 ag;
 };
 __global__ void k3_adj_interface(Adj3IfaceArgs a);
 
 // corner gradients' adjoints ([3] per corner, (nx + 1) ny nz corners)
 __global__ void k3_adj_cgrad(const double *__restrict__ vof, const double *__restrict__ am,
-                             const double *__restrict__ akap, double *__restrict__ gbar, Grid3 g);
+                             const double *__restrict__ akap, double *__restrict__ gbar, AGrid3 ag);
 // vof_bar += the corner gradients' transposes
-__global__ void k3_adj_cvof(const double *__restrict__ gbar, double *__restrict__ avof, Grid3 g);
+__global__ void k3_adj_cvof(const double *__restrict__ gbar, double *__restrict__ avof, AGrid3 ag);
 // deterministic sum (one block of 256 threads)
 __global__ void k3_adj_sum(const double *__restrict__ x, long n, double *__restrict__ out);
 // *dst = v in stream order

@@ -28,6 +28,7 @@
 // storage layouts, halos included.  Branches follow the primal state
 // (upwind side, interfacial test, eps clamps).  Every kernel gathers (each
 // thread owns its outputs): no atomics, results independent of scheduling.
+// Spacings enter as reciprocals (AGrid3): no divisions but the normalisations'.
 // The temperature is not differentiated (the adjoint needs add_buoyancy = 0).
 #include "adjoint3d_internal.cuh"
 
@@ -39,6 +40,7 @@ __constant__ double a3_gauss_p[2] = {-0.2886751345948129, +0.2886751345948129};
 __constant__ double a3_gauss_w[2] = {+0.5, +0.5};
 constexpr double kBeta3 = 1.;
 constexpr double kVofMin3 = 1.e-8;
+constexpr double kInvEps = 4503599627370496.;  // 1 / DBL_EPSILON = 2^52
 
 __device__ __forceinline__ int wrap(int j, int n) { return j < 1 ? j + n : (j > n ? j - n : j); }
 __device__ __forceinline__ bool interfacial3(double v) { return !(v < kVofMin3 || 1. - kVofMin3 < v); }
@@ -54,33 +56,36 @@ __device__ __forceinline__ void unit_adj3(double gx, double gy, double gz, doubl
                                           double &ox, double &oy, double &oz) {
   const double norm = sqrt(gx * gx + gy * gy + gz * gz);
   if (norm > kDblEpsilon) {
-    const double nx_ = gx / norm, ny_ = gy / norm, nz_ = gz / norm;
+    const double rn = 1. / norm;
+    const double nx_ = gx * rn, ny_ = gy * rn, nz_ = gz * rn;
     const double pr = nx_ * bx + ny_ * by + nz_ * bz;
-    ox = (bx - nx_ * pr) / norm;
-    oy = (by - ny_ * pr) / norm;
-    oz = (bz - nz_ * pr) / norm;
+    ox = (bx - nx_ * pr) * rn;
+    oy = (by - ny_ * pr) * rn;
+    oz = (bz - nz_ * pr) * rn;
   } else {
-    ox = bx / kDblEpsilon;
-    oy = by / kDblEpsilon;
-    oz = bz / kDblEpsilon;
+    ox = bx * kInvEps;
+    oy = by * kInvEps;
+    oz = bz * kInvEps;
   }
 }
 
 // the unnormalised corner gradient of compute_gradient at corner (ic, jc, kc)
 // (storage rows jc - 1, jc and planes kc - 1, kc)
-__device__ __forceinline__ void corner_grad3(const double *__restrict__ vof, const Grid3 &g, int ic, int jc, int kc,
-                                             double &gx, double &gy, double &gz) {
+__device__ __forceinline__ void corner_grad3(const double *__restrict__ vof, const AGrid3 &ag, int ic, int jc,
+                                             int kc, double &gx, double &gy, double &gz) {
+  const Grid3 &g = ag.g;
   double a[2][4];
   for (int q = 0; q < 2; q++) {
-    const int kk = kc - 1 + q;
-    a[q][0] = vof[ix_vof(g, ic - 1, jc - 1, kk)];
-    a[q][1] = vof[ix_vof(g, ic, jc - 1, kk)];
-    a[q][2] = vof[ix_vof(g, ic - 1, jc, kk)];
-    a[q][3] = vof[ix_vof(g, ic, jc, kk)];
+    const long o = ix_vof(g, ic - 1, jc - 1, kc - 1 + q);
+    const long r = g.nx + 2;
+    a[q][0] = vof[o];
+    a[q][1] = vof[o + 1];
+    a[q][2] = vof[o + r];
+    a[q][3] = vof[o + r + 1];
   }
-  gx = 1. / g.dxc[ic - 1] * ((-a[0][0] + a[0][1] - a[0][2] + a[0][3]) + (-a[1][0] + a[1][1] - a[1][2] + a[1][3]));
-  gy = 1. / g.dy * ((-a[0][0] - a[0][1] + a[0][2] + a[0][3]) + (-a[1][0] - a[1][1] + a[1][2] + a[1][3]));
-  gz = 1. / g.dz * ((+a[1][0] + a[1][1] + a[1][2] + a[1][3]) - (+a[0][0] + a[0][1] + a[0][2] + a[0][3]));
+  gx = ag.rxc[ic - 1] * ((-a[0][0] + a[0][1] - a[0][2] + a[0][3]) + (-a[1][0] + a[1][1] - a[1][2] + a[1][3]));
+  gy = ag.rdy * ((-a[0][0] - a[0][1] + a[0][2] + a[0][3]) + (-a[1][0] - a[1][1] + a[1][2] + a[1][3]));
+  gz = ag.rdz * ((+a[1][0] + a[1][1] + a[1][2] + a[1][3]) - (+a[0][0] + a[0][1] + a[0][2] + a[0][3]));
 }
 
 __device__ __forceinline__ bool cell3(const Grid3 &g, int &i, int &j, int &k) {
@@ -89,6 +94,22 @@ __device__ __forceinline__ bool cell3(const Grid3 &g, int &i, int &j, int &k) {
   k = 1 + blockIdx.z;
   return i <= g.nx && j <= g.ny && k <= g.nz;
 }
+
+// offsets of the periodic neighbours of row j / plane k in a compact array of
+// rows of w values (a row step s = w, a plane step p = w ny)
+struct Wrap3 {
+  long jp, jm, kp, km;
+  __device__ __forceinline__ Wrap3(int j, int k, int ny, int nz, long w) {
+    const long p = w * ny;
+    jp = (j == ny) ? -(long)(ny - 1) * w : w;
+    jm = (j == 1) ? (long)(ny - 1) * w : -w;
+    kp = (k == nz) ? -(long)(nz - 1) * p : p;
+    km = (k == 1) ? (long)(nz - 1) * p : -p;
+  }
+  __device__ __forceinline__ long at(int dj, int dk) const {
+    return (dj == 0 ? 0L : (dj > 0 ? jp : jm)) + (dk == 0 ? 0L : (dk > 0 ? kp : km));
+  }
+};
 
 }  // namespace
 
@@ -100,121 +121,156 @@ __device__ __forceinline__ bool cell3(const Grid3 &g, int &i, int &j, int &k) {
 // grad psi, y and z periodic.
 __global__ void k3_adj_project(const double *__restrict__ aux, const double *__restrict__ auy,
                                const double *__restrict__ auz, const double *__restrict__ ap,
-                               double *__restrict__ apsi, double gdt, double pre, int mode, Grid3 g) {
+                               double *__restrict__ apsi, double gdt, double pre, int mode, AGrid3 ag) {
   int i, j, k;
+  const Grid3 &g = ag.g;
   if (!cell3(g, i, j, k)) return;
-  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int nx = g.nx;
+  const long oc = ix_src(g, i, j, k);
   double acc = 0.;
   if (mode & 1) {
-    const double pb = ap[ix_src(g, i, j, k)];
-    const double ci = pre / g.dxf[i - 1];
+    const double pb = ap[oc];
+    const double ci = pre * ag.rxf[i - 1];
     double diag = 0.;
-    if (i > 1) diag += 1. / g.dxc[i - 1];
-    if (i < nx) diag += 1. / g.dxc[i];
+    if (i > 1) diag += ag.rxc[i - 1];
+    if (i < nx) diag += ag.rxc[i];
     acc += pb + pb * ci * diag;
-    if (i > 1) acc -= ap[ix_src(g, i - 1, j, k)] * (pre / g.dxf[i - 2]) / g.dxc[i - 1];
-    if (i < nx) acc -= ap[ix_src(g, i + 1, j, k)] * (pre / g.dxf[i]) / g.dxc[i];
+    if (i > 1) acc -= ap[oc - 1] * (pre * ag.rxf[i - 2]) * ag.rxc[i - 1];
+    if (i < nx) acc -= ap[oc + 1] * (pre * ag.rxf[i]) * ag.rxc[i];
   }
   if (mode & 2) {
-    if (i >= 2) acc -= gdt / g.dxc[i - 1] * aux[ix_srcx(g, i, j, k)];
-    if (i + 1 <= nx) acc += gdt / g.dxc[i] * aux[ix_srcx(g, i + 1, j, k)];
-    acc -= gdt / g.dy * auy[ix_src(g, i, j, k)];
-    acc += gdt / g.dy * auy[ix_src(g, i, wrap(j + 1, ny), k)];
-    acc -= gdt / g.dz * auz[ix_src(g, i, j, k)];
-    acc += gdt / g.dz * auz[ix_src(g, i, j, wrap(k + 1, nz))];
+    const Wrap3 w(j, k, g.ny, g.nz, nx);
+    const long of = ix_srcx(g, i, j, k);
+    if (i >= 2) acc -= gdt * ag.rxc[i - 1] * aux[of];
+    if (i + 1 <= nx) acc += gdt * ag.rxc[i] * aux[of + 1];
+    acc -= gdt * ag.rdy * auy[oc];
+    acc += gdt * ag.rdy * auy[oc + w.jp];
+    acc -= gdt * ag.rdz * auz[oc];
+    acc += gdt * ag.rdz * auz[oc + w.kp];
   }
-  apsi[ix_src(g, i, j, k)] += acc;
+  apsi[oc] += acc;
 }
 
 // b = psi_bar / dxf into the compact right-hand-side layout of the forward
 // transforms (x fastest, nx ny per plane: the same as ix_src)
-__global__ void k3_adj_scale(const double *__restrict__ apsi, double *__restrict__ b, Grid3 g) {
+__global__ void k3_adj_scale(const double *__restrict__ apsi, double *__restrict__ b, AGrid3 ag) {
   int i, j, k;
-  if (!cell3(g, i, j, k)) return;
-  const long o = ix_src(g, i, j, k);
-  b[o] = apsi[o] / g.dxf[i - 1];
+  if (!cell3(ag.g, i, j, k)) return;
+  const long o = ix_src(ag.g, i, j, k);
+  b[o] = apsi[o] * ag.rxf[i - 1];
 }
 
 // the transpose of the divergence right-hand side b = pre (dux/dxf + duy/dy +
 // duz/dz) applied to the adjoint solve's output s (psi layout): b_bar =
 // dxf s; also clears psi_bar (the forward overwrites psi)
 __global__ void k3_adj_div(double *__restrict__ aux, double *__restrict__ auy, double *__restrict__ auz,
-                           const double *__restrict__ s, double *__restrict__ apsi, double pre_p, Grid3 g) {
+                           const double *__restrict__ s, double *__restrict__ apsi, double pre_p, AGrid3 ag) {
   int i, j, k;
+  const Grid3 &g = ag.g;
   if (!cell3(g, i, j, k)) return;
-  const int ny = g.ny, nz = g.nz;
-  const double sc = s[ix_cc(g, i, j, k)];
-  if (i >= 2) aux[ix_srcx(g, i, j, k)] += pre_p * (s[ix_cc(g, i - 1, j, k)] - sc);
-  auy[ix_src(g, i, j, k)] += pre_p * (g.dxf[i - 1] / g.dy) * (s[ix_cc(g, i, wrap(j - 1, ny), k)] - sc);
-  auz[ix_src(g, i, j, k)] += pre_p * (g.dxf[i - 1] / g.dz) * (s[ix_cc(g, i, j, wrap(k - 1, nz))] - sc);
-  apsi[ix_src(g, i, j, k)] = 0.;
+  const long oc = ix_src(g, i, j, k);
+  const long q = ix_cc(g, i, j, k);  // psi layout: halos hold the periodic copies
+  const double sc = s[q];
+  if (i >= 2) aux[ix_srcx(g, i, j, k)] += pre_p * (s[q - 1] - sc);
+  const double dxf = g.dxf[i - 1];
+  auy[oc] += pre_p * (dxf * ag.rdy) * (s[q - (g.nx + 2)] - sc);
+  auz[oc] += pre_p * (dxf * ag.rdz) * (s[q - (long)(g.nx + 2) * (g.ny + 2)] - sc);
+  apsi[oc] = 0.;
 }
 
 // ---------------------------------------------------------------------------
 // delta_bar = T^-T u_bar* for every x line of ux, uy, uz, T = L U the
 // forward's factorisation (k3_tdm_coef: per system s at coef + 3 s nx, L[i],
 // R[i] = 1 / d_i (R[0] = d_0), V[i] = v_i; systems 0 ux, 1 uy and uz):
-// U^T z = b (z_i = b_i - v_{i-1} z_{i-1}), then L^T y = z (y_i = (z_i -
-// l_{i+1} y_{i+1}) / d_i).  Then the RK weights: src_a_bar = a dt delta_bar +
-// pend, src_g_bar = g dt delta_bar, pend = b dt delta_bar.  A block owns R
-// lines (j, k), staged in shared memory [3][R][nx].
-__global__ void k3_adj_xsolve(const double *__restrict__ aux, const double *__restrict__ auy,
-                              const double *__restrict__ auz, const double *__restrict__ coef,
-                              double *__restrict__ sa_x, double *__restrict__ sg_x, double *__restrict__ sa_y,
-                              double *__restrict__ sg_y, double *__restrict__ sa_z, double *__restrict__ sg_z,
-                              double *__restrict__ pend_x, double *__restrict__ pend_y, double *__restrict__ pend_z,
-                              double adt, double bdt, double gdt, int R, Grid3 g) {
-  extern __shared__ double sm3[];
-  const int nx = g.nx, ny = g.ny;
-  const long nlines = (long)ny * g.nz;
-  const long l0 = (long)blockIdx.x * R;
-  const int nr = (int)min((long)R, nlines - l0);
-  double *sq[3] = {sm3, sm3 + (size_t)R * nx, sm3 + 2 * (size_t)R * nx};
-  const double *src[3] = {aux, auy, auz};
-  for (int w = threadIdx.x; w < 3 * nr * nx; w += blockDim.x) {
-    const int f = w / (nr * nx), rem = w - f * nr * nx, r = rem / nx, p = rem - r * nx;
-    const long l = l0 + r;
-    const int j = 1 + (int)(l % ny), k = 1 + (int)(l / ny);
-    double v;
-    if (0 == f) v = (p < nx - 1) ? src[0][ix_srcx(g, p + 2, j, k)] : 0.;
-    else v = src[f][ix_src(g, p + 1, j, k)];
-    sq[f][(size_t)r * nx + p] = v;
-  }
-  __syncthreads();
+// U^T z = b (z_0 = b_0, z_i = b_i - v_{i-1} z_{i-1}), then L^T y = z
+// (y_{n-1} = R_{n-1} z_{n-1}, y_i = R_i (z_i - l_{i+1} y_{i+1}), y_0 = (z_0 -
+// l_1 y_1) / d_0).  Then the RK weights: src_a_bar = a dt delta_bar + pend,
+// src_g_bar = g dt delta_bar, pend = b dt delta_bar.
+// A block owns kAdjXLines consecutive lines (j, k) of one field (blockIdx.y),
+// one per thread, the recurrences carried in registers; the lines (rows of
+// the compact arrays, contiguous) pass through a shared tile kAdjXChunk
+// points at a time, loaded and stored in runs of consecutive points.  The
+// forward sweep leaves z in src_g_bar, which the backward sweep reads and
+// overwrites.
+__global__ void __launch_bounds__(kAdjXLines) k3_adj_xsolve(
+    const double *__restrict__ aux, const double *__restrict__ auy, const double *__restrict__ auz,
+    const double *__restrict__ coef, double *__restrict__ sa_x, double *__restrict__ sg_x, double *__restrict__ sa_y,
+    double *__restrict__ sg_y, double *__restrict__ sa_z, double *__restrict__ sg_z, double *__restrict__ pend_x,
+    double *__restrict__ pend_y, double *__restrict__ pend_z, double adt, double bdt, double gdt, Grid3 g) {
+  extern __shared__ double smx[];
+  constexpr int NL = kAdjXLines, XC = kAdjXChunk, LD = kAdjXChunk + 1;
+  const int nx = g.nx;
+  const int f = blockIdx.y;  // 0 ux, 1 uy, 2 uz
+  const int n = (0 == f) ? nx - 1 : nx;
+  const double *src = (0 == f) ? aux : (1 == f ? auy : auz);
+  double *sa = (0 == f) ? sa_x : (1 == f ? sa_y : sa_z);
+  double *sg = (0 == f) ? sg_x : (1 == f ? sg_y : sg_z);
+  double *pend = (0 == f) ? pend_x : (1 == f ? pend_y : pend_z);
+  const int set = (0 == f) ? 0 : 1;
+  double *sL = smx, *sR = smx + nx, *sV = smx + 2 * nx, *tile = smx + 3 * nx;
+  for (int w = threadIdx.x; w < 3 * nx; w += NL) smx[w] = coef[(size_t)3 * set * nx + w];
+  const long nlines = (long)g.ny * g.nz;
+  const long l0 = (long)blockIdx.x * NL;
+  const int nr = (int)min((long)NL, nlines - l0);
   const int t = threadIdx.x;
-  if (t < 3 * nr) {
-    const int f = t / nr, r = t - f * nr;
-    const int set = (0 == f) ? 0 : 1;
-    const int n = (0 == f) ? nx - 1 : nx;
-    double *q = sq[f] + (size_t)r * nx;
-    const double *L = coef + (size_t)(3 * set + 0) * nx;
-    const double *Rv = coef + (size_t)(3 * set + 1) * nx;
-    const double *V = coef + (size_t)(3 * set + 2) * nx;
-    double z = q[0];
-    for (int p = 1; p < n; p++) {
-      z = q[p] - V[p - 1] * z;
-      q[p] = z;
-    }
-    double y = q[n - 1] * Rv[n - 1];
-    q[n - 1] = y;
-    for (int p = n - 2; p >= 1; p--) {
-      y = Rv[p] * (q[p] - L[p + 1] * y);
-      q[p] = y;
-    }
-    if (n > 1) q[0] = (q[0] - L[1] * y) / Rv[0];
-  }
+  const size_t base = (size_t)l0 * n;  // row l at base + (l - l0) n
   __syncthreads();
-  double *sa[3] = {sa_x, sa_y, sa_z}, *sg[3] = {sg_x, sg_y, sg_z}, *pd[3] = {pend_x, pend_y, pend_z};
-  for (int w = threadIdx.x; w < 3 * nr * nx; w += blockDim.x) {
-    const int f = w / (nr * nx), rem = w - f * nr * nx, r = rem / nx, p = rem - r * nx;
-    if (0 == f && p >= nx - 1) continue;
-    const long l = l0 + r;
-    const int j = 1 + (int)(l % ny), k = 1 + (int)(l / ny);
-    const long o = (0 == f) ? ix_srcx(g, p + 2, j, k) : ix_src(g, p + 1, j, k);
-    const double d = sq[f][(size_t)r * nx + p];
-    sa[f][o] = adt * d + pd[f][o];
-    sg[f][o] = gdt * d;
-    pd[f][o] = bdt * d;
+  // forward sweep
+  double z = 0.;
+  for (int c0 = 0; c0 < n; c0 += XC) {
+    const int cw = min(XC, n - c0);
+    for (int w = t; w < nr * XC; w += NL) {
+      const int r = w / XC, q = w - r * XC;
+      if (q < cw) tile[r * LD + q] = src[base + (size_t)r * n + c0 + q];
+    }
+    __syncthreads();
+    if (t < nr) {
+      for (int q = 0; q < cw; q++) {
+        const int p = c0 + q;
+        const double b = tile[t * LD + q];
+        z = (0 == p) ? b : b - sV[p - 1] * z;
+        tile[t * LD + q] = z;
+      }
+    }
+    __syncthreads();
+    for (int w = t; w < nr * XC; w += NL) {
+      const int r = w / XC, q = w - r * XC;
+      if (q < cw) sg[base + (size_t)r * n + c0 + q] = tile[r * LD + q];
+    }
+    __syncthreads();
+  }
+  // backward sweep, chunks in reverse
+  double y = 0.;
+  const double rd0 = 1. / sR[0];
+  for (int c0 = ((n - 1) / XC) * XC; c0 >= 0; c0 -= XC) {
+    const int cw = min(XC, n - c0);
+    for (int w = t; w < nr * XC; w += NL) {
+      const int r = w / XC, q = w - r * XC;
+      if (q < cw) tile[r * LD + q] = sg[base + (size_t)r * n + c0 + q];
+    }
+    __syncthreads();
+    if (t < nr) {
+      for (int q = cw - 1; q >= 0; q--) {
+        const int p = c0 + q;
+        const double zz = tile[t * LD + q];
+        if (p == n - 1) y = zz * sR[n - 1];
+        else if (p > 0) y = sR[p] * (zz - sL[p + 1] * y);
+        else y = (zz - sL[1] * y) * rd0;
+        tile[t * LD + q] = y;
+      }
+    }
+    __syncthreads();
+    for (int w = t; w < nr * XC; w += NL) {
+      const int r = w / XC, q = w - r * XC;
+      if (q < cw) {
+        const size_t o = base + (size_t)r * n + c0 + q;
+        const double d = tile[r * LD + q];
+        sa[o] = adt * d + pend[o];
+        sg[o] = gdt * d;
+        pend[o] = bdt * d;
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -227,158 +283,161 @@ __global__ void k3_adj_xsolve(const double *__restrict__ aux, const double *__re
 // derivatives h ul, h (uu - ul), -h uu in (a, b, e) and h (a - b), -h (e - b)
 // in its advecting velocities ul, uu.  One thread per cell (i, j, k) writes
 // ux face i (i >= 2), uy, uz and p of the cell, and the three forces.
-
+// Neighbours are addressed by offsets (di, dj, dk) from the cell: compact
+// arrays with periodic wraps (Wrap3), primal storage arrays through their
+// halos.
 __global__ void k3_adj_rhs(Adj3RhsArgs a) {
   int i, j, k;
-  const Grid3 g = a.g;
+  const AGrid3 &ag = a.ag;
+  const Grid3 &g = ag.g;
   if (!cell3(g, i, j, k)) return;
-  const int nx = g.nx, ny = g.ny, nz = g.nz;
-  const double dy = g.dy, dz = g.dz, nu = a.m_dif;
-  const int jm = wrap(j - 1, ny), jp = wrap(j + 1, ny), km = wrap(k - 1, nz), kp = wrap(k + 1, nz);
-  auto UX = [&](int ii, int jj, int kk) { return a.ux[ix_ux(g, ii, jj, kk)]; };
-  auto V = [&](int ii, int jj, int kk) { return a.uy[ix_cc(g, ii, jj, kk)]; };
-  auto W = [&](int ii, int jj, int kk) { return a.uz[ix_cc(g, ii, jj, kk)]; };
-  // (jj, kk wrapped by the callers)
-  auto SAX = [&](int ii, int jj, int kk) { return (ii >= 2 && ii <= nx) ? a.sa_x[ix_srcx(g, ii, jj, kk)] : 0.; };
-  auto SGX = [&](int ii, int jj, int kk) { return (ii >= 2 && ii <= nx) ? a.sg_x[ix_srcx(g, ii, jj, kk)] : 0.; };
-  auto SAY = [&](int ii, int jj, int kk) { return (ii >= 1 && ii <= nx) ? a.sa_y[ix_src(g, ii, jj, kk)] : 0.; };
-  auto SGY = [&](int ii, int jj, int kk) { return (ii >= 1 && ii <= nx) ? a.sg_y[ix_src(g, ii, jj, kk)] : 0.; };
-  auto SAZ = [&](int ii, int jj, int kk) { return (ii >= 1 && ii <= nx) ? a.sa_z[ix_src(g, ii, jj, kk)] : 0.; };
-  auto SGZ = [&](int ii, int jj, int kk) { return (ii >= 1 && ii <= nx) ? a.sg_z[ix_src(g, ii, jj, kk)] : 0.; };
+  const int nx = g.nx;
+  const double rdy = ag.rdy, rdz = ag.rdz, nu = a.m_dif;
+  const Wrap3 wc(j, k, g.ny, g.nz, nx), wf(j, k, g.ny, g.nz, nx - 1);
   const long oc = ix_src(g, i, j, k);
+  const long of = ix_srcx(g, i, j, k);  // (face i; a face i + di at of + di)
+  const long pu = ix_ux(g, i, j, k), pc = ix_cc(g, i, j, k);
+  const long uj = nx + 1, uk = (long)(nx + 1) * (g.ny + 2), cj = nx + 2, ck = (long)(nx + 2) * (g.ny + 2);
+  auto UX = [&](int di, int dj, int dk) { return a.ux[pu + di + dj * uj + dk * uk]; };
+  auto V = [&](int di, int dj, int dk) { return a.uy[pc + di + dj * cj + dk * ck]; };
+  auto W = [&](int di, int dj, int dk) { return a.uz[pc + di + dj * cj + dk * ck]; };
+  auto SAX = [&](int di, int dj, int dk) { return (i + di >= 2 && i + di <= nx) ? a.sa_x[of + di + wf.at(dj, dk)] : 0.; };
+  auto SGX = [&](int di, int dj, int dk) { return (i + di >= 2 && i + di <= nx) ? a.sg_x[of + di + wf.at(dj, dk)] : 0.; };
+  auto SAY = [&](int di, int dj, int dk) { return (i + di >= 1 && i + di <= nx) ? a.sa_y[oc + di + wc.at(dj, dk)] : 0.; };
+  auto SGY = [&](int di, int dj, int dk) { return (i + di >= 1 && i + di <= nx) ? a.sg_y[oc + di + wc.at(dj, dk)] : 0.; };
+  auto SAZ = [&](int di, int dj, int dk) { return (i + di >= 1 && i + di <= nx) ? a.sa_z[oc + di + wc.at(dj, dk)] : 0.; };
+  auto SGZ = [&](int di, int dj, int dk) { return (i + di >= 1 && i + di <= nx) ? a.sg_z[oc + di + wc.at(dj, dk)] : 0.; };
+  const double rxf_i = ag.rxf[i - 1];
+  const double rxf_m = (i >= 2) ? ag.rxf[i - 2] : 0., rxf_p = (i < nx) ? ag.rxf[i] : 0.;
+  const double rxc_i = ag.rxc[i - 1], rxc_p = ag.rxc[i];
   // ---- ux face (i, j, k), i = 2..nx
   if (i >= 2) {
-    const long o = ix_srcx(g, i, j, k);
-    double acc = a.aux[o];
-    const double uxc = UX(i, j, k);
+    double acc = a.aux[of];
+    const double uxc = UX(0, 0, 0);
     // advection x of ux: (0.25 / dxc_f) (ux(f-1)^2 - ux(f+1)^2) at faces f = i -+ 1
-    if (i + 1 <= nx) acc += 2. * (0.25 / g.dxc[i]) * uxc * SAX(i + 1, j, k);
-    if (i - 1 >= 2) acc -= 2. * (0.25 / g.dxc[i - 2]) * uxc * SAX(i - 1, j, k);
-    const double w_xm = 0.5 * g.dxf[i - 2] / g.dxc[i - 1];
-    const double w_xp = 0.5 * g.dxf[i - 1] / g.dxc[i - 1];
+    if (i + 1 <= nx) acc += 2. * (0.25 * rxc_p) * uxc * SAX(1, 0, 0);
+    if (i - 1 >= 2) acc -= 2. * (0.25 * ag.rxc[i - 2]) * uxc * SAX(-1, 0, 0);
+    const double w_xm = 0.5 * g.dxf[i - 2] * rxc_i;
+    const double w_xp = 0.5 * g.dxf[i - 1] * rxc_i;
     {  // advection y of ux at rows j, j -+ 1, V(row) = w_xm uy(i-1, row) + w_xp uy(i, row)
-      const double vj = w_xm * V(i - 1, j, k) + w_xp * V(i, j, k);
-      const double vj1 = w_xm * V(i - 1, j + 1, k) + w_xp * V(i, j + 1, k);
-      acc += (0.5 / dy) * (vj1 * SAX(i, jp, k) + (vj1 - vj) * SAX(i, j, k) - vj * SAX(i, jm, k));
+      const double vj = w_xm * V(-1, 0, 0) + w_xp * V(0, 0, 0);
+      const double vj1 = w_xm * V(-1, 1, 0) + w_xp * V(0, 1, 0);
+      acc += (0.5 * rdy) * (vj1 * SAX(0, 1, 0) + (vj1 - vj) * SAX(0, 0, 0) - vj * SAX(0, -1, 0));
     }
     {  // advection z of ux
-      const double wk = w_xm * W(i - 1, j, k) + w_xp * W(i, j, k);
-      const double wk1 = w_xm * W(i - 1, j, k + 1) + w_xp * W(i, j, k + 1);
-      acc += (0.5 / dz) * (wk1 * SAX(i, j, kp) + (wk1 - wk) * SAX(i, j, k) - wk * SAX(i, j, km));
+      const double wk = w_xm * W(-1, 0, 0) + w_xp * W(0, 0, 0);
+      const double wk1 = w_xm * W(-1, 0, 1) + w_xp * W(0, 0, 1);
+      acc += (0.5 * rdz) * (wk1 * SAX(0, 0, 1) + (wk1 - wk) * SAX(0, 0, 0) - wk * SAX(0, 0, -1));
     }
     // diffusion y, z (src_a) and x (src_g)
-    acc += nu * (a.ly0 * SAX(i, jp, k) + a.ly1 * SAX(i, j, k) + a.ly2 * SAX(i, jm, k));
-    acc += nu * (a.lz0 * SAX(i, j, kp) + a.lz1 * SAX(i, j, k) + a.lz2 * SAX(i, j, km));
+    acc += nu * (a.ly0 * SAX(0, 1, 0) + a.ly1 * SAX(0, 0, 0) + a.ly2 * SAX(0, -1, 0));
+    acc += nu * (a.lz0 * SAX(0, 0, 1) + a.lz1 * SAX(0, 0, 0) + a.lz2 * SAX(0, 0, -1));
     {
-      double d = a.lap_ux[3 * (i - 2) + 1] * SGX(i, j, k);
-      if (i - 1 >= 2) d += a.lap_ux[3 * (i - 3) + 2] * SGX(i - 1, j, k);
-      if (i + 1 <= nx) d += a.lap_ux[3 * (i - 1) + 0] * SGX(i + 1, j, k);
+      double d = a.lap_ux[3 * (i - 2) + 1] * SGX(0, 0, 0);
+      if (i - 1 >= 2) d += a.lap_ux[3 * (i - 3) + 2] * SGX(-1, 0, 0);
+      if (i + 1 <= nx) d += a.lap_ux[3 * (i - 1) + 0] * SGX(1, 0, 0);
       acc += nu * d;
     }
     // advection x of uy and of uz: ux(i, j, k) is half of U_l of cell i and of
     // U_u of cell i - 1 at rows j, j + 1 (uy) and planes k, k + 1 (uz)
     for (int s = 0; s < 2; s++) {
-      const int jq = j + s, jw = wrap(jq, ny);
-      const double du = V(i - 1, jq, k) - V(i, jq, k);
-      acc += 0.25 * du * (SAY(i, jw, k) / g.dxf[i - 1] + SAY(i - 1, jw, k) / g.dxf[i - 2]);
-      const int kq = k + s, kw = wrap(kq, nz);
-      const double dw = W(i - 1, j, kq) - W(i, j, kq);
-      acc += 0.25 * dw * (SAZ(i, j, kw) / g.dxf[i - 1] + SAZ(i - 1, j, kw) / g.dxf[i - 2]);
+      const double du = V(-1, s, 0) - V(0, s, 0);
+      acc += 0.25 * du * (SAY(0, s, 0) * rxf_i + SAY(-1, s, 0) * rxf_m);
+      const double dw = W(-1, 0, s) - W(0, 0, s);
+      acc += 0.25 * dw * (SAZ(0, 0, s) * rxf_i + SAZ(-1, 0, s) * rxf_m);
     }
-    a.aux[o] = acc;
-    a.aifx[o] = SAX(i, j, k);
+    a.aux[of] = acc;
+    a.aifx[of] = SAX(0, 0, 0);
   }
   const double dxf = g.dxf[i - 1];
   // ---- uy cell (i, j, k)
   {
     double acc = a.auy[oc];
-    const double uyc = V(i, j, k);
-    acc += 2. * (0.25 / dy) * uyc * (SAY(i, jp, k) - SAY(i, jm, k));
+    const double uyc = V(0, 0, 0);
+    acc += 2. * (0.25 * rdy) * uyc * (SAY(0, 1, 0) - SAY(0, -1, 0));
     {  // advection x of uy (U of cells i, i -+ 1)
-      const double ul = 0.5 * UX(i, j - 1, k) + 0.5 * UX(i, j, k);
-      const double uu = 0.5 * UX(i + 1, j - 1, k) + 0.5 * UX(i + 1, j, k);
-      acc += (0.5 / dxf) * (uu - ul) * SAY(i, j, k);
-      if (i + 1 <= nx) acc += (0.5 / g.dxf[i]) * uu * SAY(i + 1, j, k);
-      if (i - 1 >= 1) acc -= (0.5 / g.dxf[i - 2]) * ul * SAY(i - 1, j, k);
+      const double ul = 0.5 * UX(0, -1, 0) + 0.5 * UX(0, 0, 0);
+      const double uu = 0.5 * UX(1, -1, 0) + 0.5 * UX(1, 0, 0);
+      acc += (0.5 * rxf_i) * (uu - ul) * SAY(0, 0, 0);
+      if (i + 1 <= nx) acc += (0.5 * rxf_p) * uu * SAY(1, 0, 0);
+      if (i - 1 >= 1) acc -= (0.5 * rxf_m) * ul * SAY(-1, 0, 0);
     }
     {  // advection z of uy (W(plane) = 0.5 uz(i, j-1, plane) + 0.5 uz(i, j, plane))
-      const double wz = 0.5 * W(i, j - 1, k) + 0.5 * W(i, j, k);
-      const double wz1 = 0.5 * W(i, j - 1, k + 1) + 0.5 * W(i, j, k + 1);
-      acc += (0.5 / dz) * (wz1 * SAY(i, j, kp) + (wz1 - wz) * SAY(i, j, k) - wz * SAY(i, j, km));
+      const double wz = 0.5 * W(0, -1, 0) + 0.5 * W(0, 0, 0);
+      const double wz1 = 0.5 * W(0, -1, 1) + 0.5 * W(0, 0, 1);
+      acc += (0.5 * rdz) * (wz1 * SAY(0, 0, 1) + (wz1 - wz) * SAY(0, 0, 0) - wz * SAY(0, 0, -1));
     }
     // advection y of ux (V of faces i, i + 1 holds uy(i, j, k))
     for (int s = 0; s < 2; s++) {
       const int ip = i + s;
       if (ip < 2 || ip > nx) continue;
-      const double w = 0.5 * dxf / g.dxc[ip - 1];
-      const double du = UX(ip, j - 1, k) - UX(ip, j, k);
-      acc += w * (0.5 / dy) * du * (SAX(ip, j, k) + SAX(ip, jm, k));
+      const double w = 0.5 * dxf * ag.rxc[ip - 1];
+      const double du = UX(s, -1, 0) - UX(s, 0, 0);
+      acc += w * (0.5 * rdy) * du * (SAX(s, 0, 0) + SAX(s, -1, 0));
     }
     // advection y of uz (V(plane) = 0.5 uy(i, j, plane-1) + 0.5 uy(i, j, plane)
     // of uz cells (i, j, k), (i, j, k+1) and U_u of (i, j-1, .))
     for (int s = 0; s < 2; s++) {
-      const int kq = k + s, kw = wrap(kq, nz);
-      const double dw = W(i, j - 1, kq) - W(i, j, kq);
-      acc += (0.25 / dy) * dw * (SAZ(i, j, kw) + SAZ(i, jm, kw));
+      const double dw = W(0, -1, s) - W(0, 0, s);
+      acc += (0.25 * rdy) * dw * (SAZ(0, 0, s) + SAZ(0, -1, s));
     }
-    acc += nu * (a.ly0 * SAY(i, jp, k) + a.ly1 * SAY(i, j, k) + a.ly2 * SAY(i, jm, k));
-    acc += nu * (a.lz0 * SAY(i, j, kp) + a.lz1 * SAY(i, j, k) + a.lz2 * SAY(i, j, km));
+    acc += nu * (a.ly0 * SAY(0, 1, 0) + a.ly1 * SAY(0, 0, 0) + a.ly2 * SAY(0, -1, 0));
+    acc += nu * (a.lz0 * SAY(0, 0, 1) + a.lz1 * SAY(0, 0, 0) + a.lz2 * SAY(0, 0, -1));
     {
-      double d = a.lap_cc[3 * (i - 1) + 1] * SGY(i, j, k);
-      if (i - 1 >= 1) d += a.lap_cc[3 * (i - 2) + 2] * SGY(i - 1, j, k);
-      if (i + 1 <= nx) d += a.lap_cc[3 * i + 0] * SGY(i + 1, j, k);
+      double d = a.lap_cc[3 * (i - 1) + 1] * SGY(0, 0, 0);
+      if (i - 1 >= 1) d += a.lap_cc[3 * (i - 2) + 2] * SGY(-1, 0, 0);
+      if (i + 1 <= nx) d += a.lap_cc[3 * i + 0] * SGY(1, 0, 0);
       acc += nu * d;
     }
     a.auy[oc] = acc;
-    a.aify[oc] = SAY(i, j, k);
+    a.aify[oc] = SAY(0, 0, 0);
   }
   // ---- uz cell (i, j, k)
   {
     double acc = a.auz[oc];
-    const double uzc = W(i, j, k);
-    acc += 2. * (0.25 / dz) * uzc * (SAZ(i, j, kp) - SAZ(i, j, km));
+    const double uzc = W(0, 0, 0);
+    acc += 2. * (0.25 * rdz) * uzc * (SAZ(0, 0, 1) - SAZ(0, 0, -1));
     {  // advection x of uz
-      const double ul = 0.5 * UX(i, j, k - 1) + 0.5 * UX(i, j, k);
-      const double uu = 0.5 * UX(i + 1, j, k - 1) + 0.5 * UX(i + 1, j, k);
-      acc += (0.5 / dxf) * (uu - ul) * SAZ(i, j, k);
-      if (i + 1 <= nx) acc += (0.5 / g.dxf[i]) * uu * SAZ(i + 1, j, k);
-      if (i - 1 >= 1) acc -= (0.5 / g.dxf[i - 2]) * ul * SAZ(i - 1, j, k);
+      const double ul = 0.5 * UX(0, 0, -1) + 0.5 * UX(0, 0, 0);
+      const double uu = 0.5 * UX(1, 0, -1) + 0.5 * UX(1, 0, 0);
+      acc += (0.5 * rxf_i) * (uu - ul) * SAZ(0, 0, 0);
+      if (i + 1 <= nx) acc += (0.5 * rxf_p) * uu * SAZ(1, 0, 0);
+      if (i - 1 >= 1) acc -= (0.5 * rxf_m) * ul * SAZ(-1, 0, 0);
     }
     {  // advection y of uz (V(row) = 0.5 uy(i, row, k-1) + 0.5 uy(i, row, k))
-      const double vy = 0.5 * V(i, j, k - 1) + 0.5 * V(i, j, k);
-      const double vy1 = 0.5 * V(i, j + 1, k - 1) + 0.5 * V(i, j + 1, k);
-      acc += (0.5 / dy) * (vy1 * SAZ(i, jp, k) + (vy1 - vy) * SAZ(i, j, k) - vy * SAZ(i, jm, k));
+      const double vy = 0.5 * V(0, 0, -1) + 0.5 * V(0, 0, 0);
+      const double vy1 = 0.5 * V(0, 1, -1) + 0.5 * V(0, 1, 0);
+      acc += (0.5 * rdy) * (vy1 * SAZ(0, 1, 0) + (vy1 - vy) * SAZ(0, 0, 0) - vy * SAZ(0, -1, 0));
     }
     // advection z of ux (W of faces i, i + 1 holds uz(i, j, k))
     for (int s = 0; s < 2; s++) {
       const int ip = i + s;
       if (ip < 2 || ip > nx) continue;
-      const double w = 0.5 * dxf / g.dxc[ip - 1];
-      const double du = UX(ip, j, k - 1) - UX(ip, j, k);
-      acc += w * (0.5 / dz) * du * (SAX(ip, j, k) + SAX(ip, j, km));
+      const double w = 0.5 * dxf * ag.rxc[ip - 1];
+      const double du = UX(s, 0, -1) - UX(s, 0, 0);
+      acc += w * (0.5 * rdz) * du * (SAX(s, 0, 0) + SAX(s, 0, -1));
     }
     // advection z of uy (W(row) = 0.5 uz(i, row-1, k) + 0.5 uz(i, row, k) of
     // uy cells (i, j, k), (i, j+1, k) and U_u of (., ., k-1))
     for (int s = 0; s < 2; s++) {
-      const int jq = j + s, jw = wrap(jq, ny);
-      const double dv = V(i, jq, k - 1) - V(i, jq, k);
-      acc += (0.25 / dz) * dv * (SAY(i, jw, k) + SAY(i, jw, km));
+      const double dv = V(0, s, -1) - V(0, s, 0);
+      acc += (0.25 * rdz) * dv * (SAY(0, s, 0) + SAY(0, s, -1));
     }
-    acc += nu * (a.ly0 * SAZ(i, jp, k) + a.ly1 * SAZ(i, j, k) + a.ly2 * SAZ(i, jm, k));
-    acc += nu * (a.lz0 * SAZ(i, j, kp) + a.lz1 * SAZ(i, j, k) + a.lz2 * SAZ(i, j, km));
+    acc += nu * (a.ly0 * SAZ(0, 1, 0) + a.ly1 * SAZ(0, 0, 0) + a.ly2 * SAZ(0, -1, 0));
+    acc += nu * (a.lz0 * SAZ(0, 0, 1) + a.lz1 * SAZ(0, 0, 0) + a.lz2 * SAZ(0, 0, -1));
     {
-      double d = a.lap_cc[3 * (i - 1) + 1] * SGZ(i, j, k);
-      if (i - 1 >= 1) d += a.lap_cc[3 * (i - 2) + 2] * SGZ(i - 1, j, k);
-      if (i + 1 <= nx) d += a.lap_cc[3 * i + 0] * SGZ(i + 1, j, k);
+      double d = a.lap_cc[3 * (i - 1) + 1] * SGZ(0, 0, 0);
+      if (i - 1 >= 1) d += a.lap_cc[3 * (i - 2) + 2] * SGZ(-1, 0, 0);
+      if (i + 1 <= nx) d += a.lap_cc[3 * i + 0] * SGZ(1, 0, 0);
       acc += nu * d;
     }
     a.auz[oc] = acc;
-    a.aifz[oc] = SAZ(i, j, k);
+    a.aifz[oc] = SAZ(0, 0, 0);
   }
   // ---- pressure gradients of the three src_g
-  double pb = -SGY(i, j, k) / dy + SGY(i, jp, k) / dy - SGZ(i, j, k) / dz + SGZ(i, j, kp) / dz;
-  if (i >= 2) pb -= SGX(i, j, k) / g.dxc[i - 1];
-  if (i + 1 <= nx) pb += SGX(i + 1, j, k) / g.dxc[i];
+  double pb = (SGY(0, 1, 0) - SGY(0, 0, 0)) * rdy + (SGZ(0, 0, 1) - SGZ(0, 0, 0)) * rdz;
+  if (i >= 2) pb -= SGX(0, 0, 0) * rxc_i;
+  if (i + 1 <= nx) pb += SGX(1, 0, 0) * rxc_p;
   a.ap[oc] += pb;
 }
 
@@ -397,29 +456,30 @@ __global__ void k3_adj_rhs(Adj3RhsArgs a) {
 //    vof_bar(c) and the adjoint m_bar of the unnormalised mean normal.
 // With mode & 1 but not & 4, n_bar goes to anrm; with & 4 but not & 1 it is
 // read from there.
-
 __global__ void k3_adj_interface(Adj3IfaceArgs a) {
   int i, j, k;
-  const Grid3 g = a.g;
+  const AGrid3 &ag = a.ag;
+  const Grid3 &g = ag.g;
   if (!cell3(g, i, j, k)) return;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
-  const double dy = g.dy, dz = g.dz;
-  const int jm = wrap(j - 1, ny), jp = wrap(j + 1, ny), km = wrap(k - 1, nz), kp = wrap(k + 1, nz);
+  const double rdy = ag.rdy, rdz = ag.rdz;
+  const Wrap3 wc(j, k, ny, nz, nx);
   const long oc = ix_src(g, i, j, k);
   const double vofc = a.vof[ix_vof(g, i, j, k)];
   const bool inter = interfacial3(vofc);
   double vacc = a.avof_in[oc];
   double nb[4] = {0., 0., 0., 0.};
   if (a.mode & 1) {
-    auto SRC = [&](int ii, int jj, int kk) {  // src_bar of cell (ii, jj, kk), 0 outside x
-      if (ii < 1 || ii > nx) return 0.;
-      const long q = ix_src(g, ii, jj, kk);
+    auto SRC = [&](int di, int dj, int dk) {  // src_bar of a neighbour, 0 outside x
+      if (i + di < 1 || i + di > nx) return 0.;
+      const long q = oc + di + wc.at(dj, dk);
       return a.adt * a.avof_in[q] + a.pend_in[q];
     };
-    const double sc = SRC(i, j, k);
-    auto FX = [&](int f) { return SRC(f, j, k) / g.dxf[f - 1] - SRC(f - 1, j, k) / g.dxf[f - 2]; };
-    const double fy_j = (sc - SRC(i, jm, k)) / dy, fy_jp = (SRC(i, jp, k) - sc) / dy;
-    const double fz_k = (sc - SRC(i, j, km)) / dz, fz_kp = (SRC(i, j, kp) - sc) / dz;
+    const double sc = SRC(0, 0, 0);
+    const double fx_i = (i >= 2) ? sc * ag.rxf[i - 1] - SRC(-1, 0, 0) * ag.rxf[i - 2] : 0.;
+    const double fx_ip = (i + 1 <= nx) ? SRC(1, 0, 0) * ag.rxf[i] - sc * ag.rxf[i - 1] : 0.;
+    const double fy_j = (sc - SRC(0, -1, 0)) * rdy, fy_jp = (SRC(0, 1, 0) - sc) * rdy;
+    const double fz_k = (sc - SRC(0, 0, -1)) * rdz, fz_kp = (SRC(0, 0, 1) - sc) * rdz;
     a.pend_out[oc] = a.bdt * a.avof_in[oc];
     // the indicator sum of a face whose upwind cell (ii, jj, kk) is interfacial,
     // or its vof; axis 0 / 1 / 2 and the face coordinate xf
@@ -443,7 +503,7 @@ __global__ void k3_adj_interface(Adj3IfaceArgs a) {
     if (i >= 2) {
       const double vel = a.ux[ix_ux(g, i, j, k)];
       const bool neg = vel < 0.;
-      a.aux[ix_srcx(g, i, j, k)] += phi_of(neg ? i : i - 1, j, k, 0, neg ? -0.5 : +0.5) * FX(i);
+      a.aux[ix_srcx(g, i, j, k)] += phi_of(neg ? i : i - 1, j, k, 0, neg ? -0.5 : +0.5) * fx_i;
     }
     {
       const double vel = a.uy[ix_cc(g, i, j, k)];
@@ -478,11 +538,11 @@ __global__ void k3_adj_interface(Adj3IfaceArgs a) {
     };
     if (i >= 2) {
       const double vel = a.ux[ix_ux(g, i, j, k)];
-      if (vel < 0.) upwind(vel, FX(i), 0, -0.5);
+      if (vel < 0.) upwind(vel, fx_i, 0, -0.5);
     }
     if (i + 1 <= nx) {
       const double vel = a.ux[ix_ux(g, i + 1, j, k)];
-      if (!(vel < 0.)) upwind(vel, FX(i + 1), 0, +0.5);
+      if (!(vel < 0.)) upwind(vel, fx_ip, 0, +0.5);
     }
     {
       const double vel = a.uy[ix_cc(g, i, j, k)];
@@ -512,30 +572,30 @@ __global__ void k3_adj_interface(Adj3IfaceArgs a) {
       const int f = i + s;
       if (f < 2 || f > nx) continue;
       const double ib = a.aifx[ix_srcx(g, f, j, k)];
-      const double dx = g.dxc[f - 1];
-      const double grad = 1. / dx * (-vof[ix_vof(g, f - 1, j, k)] + vof[ix_vof(g, f, j, k)]);
+      const double rx = ag.rxc[f - 1];
+      const double grad = rx * (-vof[ix_vof(g, f - 1, j, k)] + vof[ix_vof(g, f, j, k)]);
       const double kap = 0.5 * (+curv[ix_cc(g, f - 1, j, k)] + curv[ix_cc(g, f, j, k)]);
-      vacc += (0 == s ? 1. : -1.) * sig * kap / dx * ib;
+      vacc += (0 == s ? 1. : -1.) * sig * kap * rx * ib;
       kb += sig * grad * 0.5 * ib;
       if (0 == s) sb += grad * kap * ib;
     }
     // y faces j (c above) and j + 1 (c below)
     for (int s = 0; s < 2; s++) {
       const int r = j + s;  // storage row of the face's upper cell
-      const double ib = a.aify[ix_src(g, i, 0 == s ? j : jp, k)];
-      const double grad = 1. / dy * (-vof[ix_vof(g, i, r - 1, k)] + vof[ix_vof(g, i, r, k)]);
+      const double ib = a.aify[oc + wc.at(s, 0)];
+      const double grad = rdy * (-vof[ix_vof(g, i, r - 1, k)] + vof[ix_vof(g, i, r, k)]);
       const double kap = 0.5 * (+curv[ix_cc(g, i, wrap(r - 1, ny), k)] + curv[ix_cc(g, i, wrap(r, ny), k)]);
-      vacc += (0 == s ? 1. : -1.) * sig * kap / dy * ib;
+      vacc += (0 == s ? 1. : -1.) * sig * kap * rdy * ib;
       kb += sig * grad * 0.5 * ib;
       if (0 == s) sb += grad * kap * ib;
     }
     // z faces k (c above) and k + 1 (c below)
     for (int s = 0; s < 2; s++) {
       const int r = k + s;
-      const double ib = a.aifz[ix_src(g, i, j, 0 == s ? k : kp)];
-      const double grad = 1. / dz * (-vof[ix_vof(g, i, j, r - 1)] + vof[ix_vof(g, i, j, r)]);
+      const double ib = a.aifz[oc + wc.at(0, s)];
+      const double grad = rdz * (-vof[ix_vof(g, i, j, r - 1)] + vof[ix_vof(g, i, j, r)]);
       const double kap = 0.5 * (+curv[ix_cc(g, i, j, wrap(r - 1, nz))] + curv[ix_cc(g, i, j, wrap(r, nz))]);
-      vacc += (0 == s ? 1. : -1.) * sig * kap / dz * ib;
+      vacc += (0 == s ? 1. : -1.) * sig * kap * rdz * ib;
       kb += sig * grad * 0.5 * ib;
       if (0 == s) sb += grad * kap * ib;
     }
@@ -568,16 +628,16 @@ __global__ void k3_adj_interface(Adj3IfaceArgs a) {
       for (int q = 0; q < 8; q++) {
         const int ic = i + (q & 1), jc = j + ((q >> 1) & 1), kc = k + (q >> 2);
         double gx, gy, gz;
-        corner_grad3(a.vof, g, ic, jc, kc, gx, gy, gz);
+        corner_grad3(a.vof, ag, ic, jc, kc, gx, gy, gz);
         const double norm = sqrt(+gx * gx + gy * gy + gz * gz);
         const double ninv = 1. / fmax(norm, kDblEpsilon);
         mv[0] += gx * ninv;
         mv[1] += gy * ninv;
         mv[2] += gz * ninv;
       }
-      mv[0] /= g.dxf[i - 1];
-      mv[1] /= dy;
-      mv[2] /= dz;
+      mv[0] *= ag.rxf[i - 1];
+      mv[1] *= rdy;
+      mv[2] *= rdz;
       unit_adj3(mv[0], mv[1], mv[2], nb[0], nb[1], nb[2], mb[0], mb[1], mb[2]);
     }
     for (int m = 0; m < 3; m++) a.am[3 * oc + m] = mb[m];
@@ -594,7 +654,8 @@ __global__ void k3_adj_interface(Adj3IfaceArgs a) {
 // the normalisation's transpose; gbar[3 corner] = the corner gradient's
 // adjoint, corner = (ic - 1) + (nx + 1) ((jc - 1) + ny (kc - 1)).
 __global__ void k3_adj_cgrad(const double *__restrict__ vof, const double *__restrict__ am,
-                             const double *__restrict__ akap, double *__restrict__ gbar, Grid3 g) {
+                             const double *__restrict__ akap, double *__restrict__ gbar, AGrid3 ag) {
+  const Grid3 &g = ag.g;
   const int ic = 1 + blockIdx.x * blockDim.x + threadIdx.x;
   const int jc = 1 + blockIdx.y * blockDim.y + threadIdx.y;
   const int kc = 1 + blockIdx.z;
@@ -607,14 +668,14 @@ __global__ void k3_adj_cgrad(const double *__restrict__ vof, const double *__res
         const int p = ic - 1 + dp;
         if (p < 1 || p > nx) continue;
         const long o = ix_src(g, p, wrap(jc - 1 + dq, ny), wrap(kc - 1 + dr, nz));
-        const double kap = akap[o];
-        const double dxp = g.dxf[p - 1];
-        b[0] += am[3 * o + 0] / dxp + (dp ? 1. : -1.) * kap * 0.25 / dxp;
-        b[1] += am[3 * o + 1] / g.dy + (dq ? 1. : -1.) * kap * 0.25 / g.dy;
-        b[2] += am[3 * o + 2] / g.dz + (dr ? 1. : -1.) * kap * 0.25 / g.dz;
+        const double kap = 0.25 * akap[o];
+        const double rxp = ag.rxf[p - 1];
+        b[0] += (am[3 * o + 0] + (dp ? kap : -kap)) * rxp;
+        b[1] += (am[3 * o + 1] + (dq ? kap : -kap)) * ag.rdy;
+        b[2] += (am[3 * o + 2] + (dr ? kap : -kap)) * ag.rdz;
       }
   double gx, gy, gz;
-  corner_grad3(vof, g, ic, jc, kc, gx, gy, gz);
+  corner_grad3(vof, ag, ic, jc, kc, gx, gy, gz);
   double o0, o1, o2;
   unit_adj3(gx, gy, gz, b[0], b[1], b[2], o0, o1, o2);
   const long q = (long)(ic - 1) + (long)(nx + 1) * ((long)(jc - 1) + (long)ny * (kc - 1));
@@ -627,22 +688,24 @@ __global__ void k3_adj_cgrad(const double *__restrict__ vof, const double *__res
 // transposes of its eight corners (ic in {i, i+1}, jc, kc wrapped): the cell is
 // the corner's (ic-1+dp, jc-1+dq, kc-1+dr) cell, with coefficients
 // -+1 / dxc(ic), -+1 / dy, -+1 / dz (+ for dp, dq, dr = 1)
-__global__ void k3_adj_cvof(const double *__restrict__ gbar, double *__restrict__ avof, Grid3 g) {
+__global__ void k3_adj_cvof(const double *__restrict__ gbar, double *__restrict__ avof, AGrid3 ag) {
   int i, j, k;
+  const Grid3 &g = ag.g;
   if (!cell3(g, i, j, k)) return;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
-  double acc = 0.;
+  double sx = 0., sy = 0., sz = 0.;
   for (int sr = 0; sr < 2; sr++)
     for (int sq = 0; sq < 2; sq++)
       for (int sp = 0; sp < 2; sp++) {
         const int ic = i + sp, jc = wrap(j + sq, ny), kc = wrap(k + sr, nz);
-        const int dp = 1 - sp, dq = 1 - sq, dr = 1 - sr;  // the cell's place in the corner's stencil
         const long q = (long)(ic - 1) + (long)(nx + 1) * ((long)(jc - 1) + (long)ny * (kc - 1));
-        acc += gbar[3 * q + 0] * (dp ? 1. : -1.) / g.dxc[ic - 1];
-        acc += gbar[3 * q + 1] * (dq ? 1. : -1.) / g.dy;
-        acc += gbar[3 * q + 2] * (dr ? 1. : -1.) / g.dz;
+        // the cell's place in the corner's stencil: dp = 1 - sp, dq = 1 - sq, dr = 1 - sr
+        const double gxv = gbar[3 * q + 0] * ag.rxc[ic - 1];
+        sx += sp ? -gxv : gxv;
+        sy += sq ? -gbar[3 * q + 1] : gbar[3 * q + 1];
+        sz += sr ? -gbar[3 * q + 2] : gbar[3 * q + 2];
       }
-  avof[ix_src(g, i, j, k)] += acc;
+  avof[ix_src(g, i, j, k)] += sx + sy * ag.rdy + sz * ag.rdz;
 }
 
 // deterministic sum of n values (one block of 256 threads)

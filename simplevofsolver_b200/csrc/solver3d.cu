@@ -1126,10 +1126,11 @@ struct Adjoint3State {
   DevBuf ux, uy, uz, p, vof[2], pend_v[2];
   DevBuf pend_x, pend_y, pend_z, sa_x, sg_x, sa_y, sg_y, sa_z, sg_z, ifx, ify, ifz, kap, m, nrm, sig;
   DevBuf psib, b, psis, gbar, sum;
+  DevBuf rxf, rxc;  // 1 / dxf, 1 / dxc
   int cv = 0;  // current buffer of vof_bar
   int cp = 0;  // current buffer of the vof source's pending adjoint
-  int xs_rows = 1;
   size_t xs_smem = 0;
+  // the adjoint fields and scratch (zeroed by svof3d_adjoint_reset)
   DevBuf *all(int q) {
     DevBuf *l[] = {&ux, &uy, &uz, &p, &vof[0], &vof[1], &pend_v[0], &pend_v[1], &pend_x, &pend_y, &pend_z,
                    &sa_x, &sg_x, &sa_y, &sg_y, &sa_z, &sg_z, &ifx, &ify, &ifz, &kap, &m, &nrm, &sig,
@@ -1141,6 +1142,8 @@ struct Adjoint3State {
 void adjoint3_free(svof3d_solver *s) {
   if (!s || !s->adj) return;
   for (int q = 0; DevBuf *b = s->adj->all(q); q++) dfree(*b);
+  dfree(s->adj->rxf);
+  dfree(s->adj->rxc);
   delete s->adj;
   s->adj = nullptr;
 }
@@ -1152,7 +1155,7 @@ int adj3_ensure(svof3d_solver *s) {
   if (s->mixed) return fail("the adjoint needs the FP64 path (precision SVOF3_FP64)");
   if (s->prm.add_buoyancy) return fail("the adjoint needs add_buoyancy = 0 (t is not differentiated)");
   const size_t nx = s->nx, ny = s->ny, nz = s->nz;
-  if (sizeof(double) * 3 * nx > 160 * 1024) return fail("the adjoint's x line solve needs nx <= 6826");
+  if (adj_xsolve_smem((int)nx) > 200 * 1024) return fail("the adjoint's x line solve needs nx <= 7800");
   Adjoint3State *a = new Adjoint3State();
   const size_t nc = nx * ny * nz, nf = (nx - 1) * ny * nz, ncc = (nx + 2) * (ny + 2) * (nz + 2);
   bool bad = dalloc(a->ux, nf) || dalloc(a->uy, nc) || dalloc(a->uz, nc) || dalloc(a->p, nc) ||
@@ -1163,14 +1166,19 @@ int adj3_ensure(svof3d_solver *s) {
              dalloc(a->ifz, nc) || dalloc(a->kap, nc) || dalloc(a->m, 3 * nc) || dalloc(a->nrm, 4 * nc) ||
              dalloc(a->sig, nc) || dalloc(a->psib, nc) || dalloc(a->b, nc) || dalloc(a->psis, ncc) ||
              dalloc(a->gbar, 3 * (nx + 1) * ny * nz) || dalloc(a->sum, 1);
-  // transposed line solves: R lines (j, k) per block, 3 R threads at most
-  // 128, blocks covering the SMs twice where the lines allow, within 160 KB
-  const long lines = (long)ny * nz;
-  int r = (int)std::max(1L, std::min(42L, lines / (148L * 2)));
-  while (r > 1 && sizeof(double) * 3 * (size_t)r * nx > 160 * 1024) r--;
-  a->xs_rows = r;
-  a->xs_smem = sizeof(double) * 3 * (size_t)r * nx;
+  a->xs_smem = adj_xsolve_smem((int)nx);
   if (!bad && cudaSuccess != raise_smem_limit(k3_adj_xsolve, a->xs_smem)) bad = fail("cudaFuncSetAttribute(k3_adj_xsolve)");
+  if (!bad) {
+    // reciprocal spacings from the device tables
+    std::vector<double> h(nx + 1);
+    bad = cudaSuccess != cudaMemcpy(h.data(), s->dxf.p, sizeof(double) * nx, cudaMemcpyDeviceToHost);
+    for (size_t q = 0; !bad && q < nx; q++) h[q] = 1. / h[q];
+    bad = bad || upload(a->rxf, std::vector<double>(h.begin(), h.begin() + nx));
+    bad = bad || cudaSuccess != cudaMemcpy(h.data(), s->dxc.p, sizeof(double) * (nx + 1), cudaMemcpyDeviceToHost);
+    for (size_t q = 0; !bad && q <= nx; q++) h[q] = 1. / h[q];
+    bad = bad || upload(a->rxc, h);
+    if (bad && g_err3.empty()) fail("adjoint set-up: spacing tables");
+  }
   if (bad) {
     std::string e = g_err3;
     s->adj = a;
@@ -1184,6 +1192,10 @@ int adj3_ensure(svof3d_solver *s) {
 
 dim3 adj3_cells(const svof3d_solver *s) { return dim3((s->nx + 31) / 32, (s->ny + 7) / 8, s->nz); }
 
+AGrid3 agrid(const svof3d_solver *s) {
+  return AGrid3{s->grid(), s->adj->rxf.p, s->adj->rxc.p, 1. / s->dy, 1. / s->dz};
+}
+
 int adj3_set_dt(svof3d_solver *s, double dt) {
   k3_adj_set<<<1, 1, 0, s->stream>>>(s->d_dt, dt);
   CK_LAUNCH();
@@ -1196,7 +1208,7 @@ int adj3_project(svof3d_solver *s, int rk, double dt, int mode) {
   const double gam = RK_A[rk] + RK_B[rk];
   k3_adj_project<<<adj3_cells(s), dim3(32, 8), 0, s->stream>>>(a->ux.p, a->uy.p, a->uz.p, a->p.p, a->psib.p,
                                                                gam * dt, 0.5 * gam * dt * s->prm.m_dif, mode,
-                                                               s->grid());
+                                                               agrid(s));
   CK_LAUNCH();
   return 0;
 }
@@ -1208,7 +1220,7 @@ int adj3_potential(svof3d_solver *s, int rk, double dt) {
   Adjoint3State *a = s->adj;
   const double gam = RK_A[rk] + RK_B[rk];
   const Grid3 g = s->grid();
-  k3_adj_scale<<<adj3_cells(s), dim3(32, 8), 0, s->stream>>>(a->psib.p, a->b.p, g);
+  k3_adj_scale<<<adj3_cells(s), dim3(32, 8), 0, s->stream>>>(a->psib.p, a->b.p, agrid(s));
   CK_LAUNCH();
   CK(pois_fwd_y_array<double>(s->stream, a->b.p, s->spec.p, s->twf_y.p, s->log2ny, g));
   CK(pois_z<double>(s->stream, s->spec.p, s->twf_z.p, s->log2nz, g));
@@ -1217,7 +1229,7 @@ int adj3_potential(svof3d_solver *s, int rk, double dt) {
   CK(pois_inv_y<double>(s->stream, s->spec.p, a->psis.p, s->twb_y.p, s->log2ny, g, false));
   const double pre_p = 1. / (gam * dt) / (1. * s->ny * s->nz);
   k3_adj_div<<<adj3_cells(s), dim3(32, 8), 0, s->stream>>>(a->ux.p, a->uy.p, a->uz.p, a->psis.p, a->psib.p, pre_p,
-                                                           g);
+                                                           agrid(s));
   CK_LAUNCH();
   return 0;
 }
@@ -1229,11 +1241,10 @@ int adj3_predict(svof3d_solver *s, int rk, double dt, const double *ux, const do
                                                                  RK_A[rk] + RK_B[rk], s->prm.m_dif, s->prm.t_dif,
                                                                  s->nx, s->coef.p);
   CK_LAUNCH();
-  const int R = a->xs_rows;
   const long lines = (long)s->ny * s->nz;
-  k3_adj_xsolve<<<(unsigned)((lines + R - 1) / R), 128, a->xs_smem, s->stream>>>(
+  k3_adj_xsolve<<<dim3((unsigned)((lines + kAdjXLines - 1) / kAdjXLines), 3), kAdjXLines, a->xs_smem, s->stream>>>(
       a->ux.p, a->uy.p, a->uz.p, s->coef.p, a->sa_x.p, a->sg_x.p, a->sa_y.p, a->sg_y.p, a->sa_z.p, a->sg_z.p,
-      a->pend_x.p, a->pend_y.p, a->pend_z.p, RK_A[rk] * dt, RK_B[rk] * dt, (RK_A[rk] + RK_B[rk]) * dt, R,
+      a->pend_x.p, a->pend_y.p, a->pend_z.p, RK_A[rk] * dt, RK_B[rk] * dt, (RK_A[rk] + RK_B[rk]) * dt,
       s->grid());
   CK_LAUNCH();
   Adj3RhsArgs r{};
@@ -1262,7 +1273,7 @@ int adj3_predict(svof3d_solver *s, int rk, double dt, const double *ux, const do
   r.lz0 = s->lapz[0];
   r.lz1 = s->lapz[1];
   r.lz2 = s->lapz[2];
-  r.g = s->grid();
+  r.ag = agrid(s);
   k3_adj_rhs<<<adj3_cells(s), dim3(32, 8), 0, s->stream>>>(r);
   CK_LAUNCH();
   return 0;
@@ -1299,7 +1310,7 @@ int adj3_interface(svof3d_solver *s, int rk, double dt, int mode, const double *
   f.bdt = RK_B[rk] * dt;
   f.tension = s->prm.tension;
   f.mode = mode;
-  f.g = s->grid();
+  f.ag = agrid(s);
   k3_adj_interface<<<adj3_cells(s), dim3(32, 8), 0, s->stream>>>(f);
   CK_LAUNCH();
   a->cv ^= 1;
@@ -1310,11 +1321,11 @@ int adj3_interface(svof3d_solver *s, int rk, double dt, int mode, const double *
 // the corner normals and curvature part of interface_compute_curvature_tensor
 int adj3_corners(svof3d_solver *s, const double *vof) {
   Adjoint3State *a = s->adj;
-  const Grid3 g = s->grid();
+  const AGrid3 ag = agrid(s);
   k3_adj_cgrad<<<dim3((s->nx + 1 + 31) / 32, (s->ny + 7) / 8, s->nz), dim3(32, 8), 0, s->stream>>>(
-      vof, a->m.p, a->kap.p, a->gbar.p, g);
+      vof, a->m.p, a->kap.p, a->gbar.p, ag);
   CK_LAUNCH();
-  k3_adj_cvof<<<adj3_cells(s), dim3(32, 8), 0, s->stream>>>(a->gbar.p, a->vof[a->cv].p, g);
+  k3_adj_cvof<<<adj3_cells(s), dim3(32, 8), 0, s->stream>>>(a->gbar.p, a->vof[a->cv].p, ag);
   CK_LAUNCH();
   return 0;
 }
