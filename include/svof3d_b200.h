@@ -223,7 +223,9 @@ int svof3d_statistics_field(svof3d_solver_t *s, int quantity, double *out, size_
  * the previous substep), update_vof (vof', src of the next substep -> u,
  * vof, the normals, src of the previous substep), compute_force (the forces
  * -> vof, curvature, tension), compute_curvature_tensor (normals, curvature
- * -> vof).  Adjoint fields are compact: ux faces nz x ny x (nx-1), cells
+ * -> vof); predict_field also maps to vof and the vof buoyancy coefficient
+ * while the extension is on.  A tape (svof3d_tape_count() doubles) holds the
+ * three substeps' inputs and the step's final vof.  Adjoint fields are compact: ux faces nz x ny x (nx-1), cells
  * nz x ny x nx, normal nz x ny x nx x 4, tension one value per cell (summed
  * by svof3d_adjoint_tension).  Requires precision SVOF3_FP64 and
  * add_buoyancy 0; the temperature is not differentiated. */
@@ -243,10 +245,17 @@ enum {
   SVOF3_ADJ_SRCUY_A,
   SVOF3_ADJ_SRCUZ_A,
   SVOF3_ADJ_SRC_A,    /* vof source's adjoint */
-  SVOF3_ADJ_TENSION
+  SVOF3_ADJ_TENSION,
+  SVOF3_ADJ_GRAVITY   /* the vof buoyancy coefficient's adjoint, per cell */
 };
 /* the surface-tension coefficient 1/We of the following steps */
 int svof3d_set_tension(svof3d_solver_t *s, double tension);
+/* extension (absent from the reference; 0 = off, the default): Boussinesq
+ * buoyancy of the volume fraction along y, src_a of uy += grav_vof
+ * (0.5 vof(j-1) + 0.5 vof(j) - vof_ref), vof after the substep's advection;
+ * with grav_vof = -(1 - r) / Fr^2 it models a density ratio r under gravity
+ * along -y (the 2D svof_set_gravity carried to 3D) */
+int svof3d_set_gravity(svof3d_solver_t *s, double grav_vof, double vof_ref);
 int svof3d_tape_count(const svof3d_solver_t *s, size_t *count);
 int svof3d_integrate_fixed(svof3d_solver_t *s, double dt, double *tape);
 /* device pointer and element count of an adjoint field (made on first use) */
@@ -261,6 +270,7 @@ int svof3d_adjoint_interface_update_vof(svof3d_solver_t *s, size_t rkstep, doubl
 int svof3d_adjoint_interface_compute_force(svof3d_solver_t *s);
 int svof3d_adjoint_interface_compute_curvature_tensor(svof3d_solver_t *s);
 int svof3d_adjoint_tension(svof3d_solver_t *s, double *out);
+int svof3d_adjoint_gravity(svof3d_solver_t *s, double *out);
 
 /* one step launched kernel by kernel with events between; ms[k], launches[k] per kind */
 int svof3d_profile_step(svof3d_solver_t *s, double *ms, int *launches, int nkinds);

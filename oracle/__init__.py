@@ -353,6 +353,7 @@ def _load3():
             getattr(L, fn).argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double]
         L.svo3_integrate.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
         L.svo3_run.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        L.svo3_set_gravity.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
         L.svo3_stat_collect.argtypes = [ctypes.c_void_p]
         L.svo3_stat_reduce.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
         L.svo3_stat_num.argtypes = [ctypes.c_void_p]
@@ -428,6 +429,10 @@ class Oracle3D:
 
     def update_pressure(self, rk, dt):
         _load3().svo3_update_pressure(self._h, rk, dt)
+
+    def set_gravity(self, grav_vof: float, vof_ref: float):
+        """the vof buoyancy extension on uy (0 = off)"""
+        _load3().svo3_set_gravity(self._h, float(grav_vof), float(vof_ref))
 
     def substeps(self, dt):
         """one step's three Runge-Kutta substeps with a given dt"""

@@ -46,6 +46,10 @@ struct svo3_ctx {
    * first collection */
   double *stat[9];
   long stat_num;
+  /* extension (absent from the reference; off while grav_vof == 0): the
+   * Boussinesq buoyancy of the volume fraction along y, srcuy += grav_vof
+   * (vof_face - vof_ref), as the 2D restatement's svo_set_gravity */
+  double grav_vof, vof_ref;
 };
 
 #define NX (c->nx)
@@ -645,6 +649,10 @@ static void rhs_all(svo3_ctx_t *c) {
           sa += md * (+lz[0] * zs + lz[1] * xc + lz[2] * zn);
           sg -= 1. / dy * (-CC(p, i, j - 1, k) + CC(p, i, j, k));
           sa += SRC(c->ifrcy, i, j, k);
+          /* extension: buoyancy of the volume fraction, the face value of
+           * vof averaged from the two cells beside the uy face (the vof
+           * after this substep's advection, as in 2D) */
+          if (0. != c->grav_vof) sa += c->grav_vof * (0.5 * VOF(i, j - 1, k) + 0.5 * VOF(i, j, k) - c->vof_ref);
           SRC(c->srcuy[0], i, j, k) = sa;
           SRC(c->srcuy[2], i, j, k) = sg;
         }
@@ -874,6 +882,12 @@ int svo3_integrate(svo3_ctx_t *c, double *dt) {
     svo3_correct(c, rk, *dt);
     svo3_update_pressure(c, rk, *dt);
   }
+  return 0;
+}
+
+int svo3_set_gravity(svo3_ctx_t *c, double grav_vof, double vof_ref) {
+  c->grav_vof = grav_vof;
+  c->vof_ref = vof_ref;
   return 0;
 }
 

@@ -46,6 +46,8 @@ int svo3_correct(svo3_ctx_t *ctx, int rkstep, double dt);
 int svo3_update_pressure(svo3_ctx_t *ctx, int rkstep, double dt);
 int svo3_integrate(svo3_ctx_t *ctx, double *dt);
 int svo3_run(svo3_ctx_t *ctx, int nsteps, double *dts);
+/* extension: vof buoyancy on uy, srcuy += grav_vof (vof_face - vof_ref) (0 = off) */
+int svo3_set_gravity(svo3_ctx_t *ctx, double grav_vof, double vof_ref);
 /* time-averaged statistics: one sample of ux1 ux2 uy1 uy2 uz1 uz2 t1 t2 uxt
  * (q = 0 .. 8), the y-z sum of one quantity (nx+1 values for ux1 ux2 uxt,
  * nx+2 for the others), the number of samples */

@@ -223,7 +223,8 @@ class Rollout3D:
     """The 3D form of :class:`Rollout`: ``len(dts)`` steps of a
     :class:`simplevofsolver_b200.solver3d.Solver3D` (precision "fp64") with
     the time steps held fixed (``svof3d_integrate_fixed``), differentiable
-    with respect to the initial ux, uy, uz, vof and 1/We through
+    with respect to the initial ux, uy, uz, vof, 1/We and the vof buoyancy
+    coefficient (``Solver3D.set_gravity``) through
     :func:`rollout3d`; the backward pass recomputes each segment of K steps
     from its checkpoint with tapes and applies the CUDA step adjoints
     (``svof3d_adjoint_step``, ``csrc/k3_adjoint.cu``) in reverse.  The
@@ -252,9 +253,11 @@ class Rollout3D:
         self.s.synchronize()
         self._torch.cuda.synchronize()
 
-    def load(self, ux0, uy0, uz0, vof0, tension):
+    def load(self, ux0, uy0, uz0, vof0, tension, grav=None):
         s = self.s
         s.set_tension(float(tension))
+        if grav is not None:
+            s.set_gravity(float(grav), s.gravity[1])
         for name, a in (("ux", ux0), ("uy", uy0), ("uz", uz0), ("vof", vof0)):
             s.load_interior(name, _to_interior3(name, a, self.nx))
         s.load_interior("p", self.p0)
@@ -283,8 +286,8 @@ class Rollout3D:
         vof = self.s.device_view("vof")[2:nz + 2, 2:ny + 2, 1:nx + 1].clone()
         return ux, uy, uz, vof, p
 
-    def forward(self, ux0, uy0, uz0, vof0, tension, keep_checkpoints=True):
-        self.load(ux0, uy0, uz0, vof0, tension)
+    def forward(self, ux0, uy0, uz0, vof0, tension, grav=None, keep_checkpoints=True):
+        self.load(ux0, uy0, uz0, vof0, tension, grav)
         self.checkpoints = []
         for n, dt in enumerate(self.dts):
             if keep_checkpoints and n % self.K == 0:
@@ -324,27 +327,31 @@ class Rollout3D:
             s.adjoint_fluid_compute_potential_dft(0, 1.0)
         self._sync()
         return (s.adjoint_view("ux").clone(), s.adjoint_view("uy").clone(), s.adjoint_view("uz").clone(),
-                s.adjoint_view("vof").clone(), s.adjoint_tension())
+                s.adjoint_view("vof").clone(), s.adjoint_tension(), s.adjoint_gravity())
 
 
 def _function3d():
     import torch
 
     class Rollout3DFunction(torch.autograd.Function):
-        """(ux0, uy0, uz0, vof0, tension) -> (ux, uy, uz, vof, p) after the
-        rollout's steps; backward through the CUDA step adjoints"""
+        """(ux0, uy0, uz0, vof0, tension, grav) -> (ux, uy, uz, vof, p) after
+        the rollout's steps; backward through the CUDA step adjoints.  grav
+        None keeps the solver's vof buoyancy coefficient (no gradient)."""
 
         @staticmethod
-        def forward(ctx, ux0, uy0, uz0, vof0, tension, rollout):
+        def forward(ctx, ux0, uy0, uz0, vof0, tension, grav, rollout):
             ctx.rollout = rollout
             ctx.tension_like = tension
-            return rollout.forward(ux0, uy0, uz0, vof0, float(tension))
+            ctx.has_grav = grav is not None
+            return rollout.forward(ux0, uy0, uz0, vof0, float(tension), None if grav is None else float(grav))
 
         @staticmethod
         def backward(ctx, gux, guy, guz, gvof, gp):
-            g_ux, g_uy, g_uz, g_vof, g_ten = ctx.rollout.backward(gux, guy, guz, gvof, gp)
-            gt = torch.tensor(g_ten, dtype=torch.float64, device=ctx.tension_like.device)
-            return g_ux, g_uy, g_uz, g_vof, gt, None
+            g_ux, g_uy, g_uz, g_vof, g_ten, g_grav = ctx.rollout.backward(gux, guy, guz, gvof, gp)
+            dev = ctx.tension_like.device
+            gt = torch.tensor(g_ten, dtype=torch.float64, device=dev)
+            gg = torch.tensor(g_grav, dtype=torch.float64, device=dev) if ctx.has_grav else None
+            return g_ux, g_uy, g_uz, g_vof, gt, gg, None
 
     return Rollout3DFunction
 
@@ -352,13 +359,14 @@ def _function3d():
 _RF3 = None
 
 
-def rollout3d(ux0, uy0, uz0, vof0, tension, r: Rollout3D):
+def rollout3d(ux0, uy0, uz0, vof0, tension, r: Rollout3D, grav=None):
     """differentiable 3D rollout: returns (ux, uy, uz, vof, p) after
-    len(r.dts) steps"""
+    len(r.dts) steps; grav (a 0-d tensor, optional) sets the vof buoyancy
+    coefficient"""
     global _RF3
     if _RF3 is None:
         _RF3 = _function3d()
-    return _RF3.apply(ux0, uy0, uz0, vof0, tension, r)
+    return _RF3.apply(ux0, uy0, uz0, vof0, tension, grav, r)
 
 
 def falling_objective(ux, uy, vof, xf, ly: float = 1.0):

@@ -46,6 +46,12 @@ struct Adj3RhsArgs {
   double *aux, *auy, *auz, *ap, *aifx, *aify, *aifz;
   const double *lap_ux, *lap_cc;
   double m_dif, ly0, ly1, ly2, lz0, lz1, lz2;
+  // the vof buoyancy extension (skipped while grav_vof == 0): vof_post the
+  // primal vof after the substep's advection (storage layout), avof its
+  // adjoint (+=), agrv the coefficient's adjoint per cell (+=)
+  double grav_vof, vof_ref;
+  const double *vof_post;
+  double *avof, *agrv;
   AGrid3 ag;
 };
 __global__ void k3_adj_rhs(Adj3RhsArgs a);

@@ -282,7 +282,8 @@ __global__ void __launch_bounds__(kAdjXLines) k3_adj_xsolve(
 // derivatives h a, 0, -h e; a cross term h [ul (a - b) - uu (e - b)] has
 // derivatives h ul, h (uu - ul), -h uu in (a, b, e) and h (a - b), -h (e - b)
 // in its advecting velocities ul, uu.  One thread per cell (i, j, k) writes
-// ux face i (i >= 2), uy, uz and p of the cell, and the three forces.
+// ux face i (i >= 2), uy, uz and p of the cell, the three forces, and with
+// the vof buoyancy extension on, vof_bar and the coefficient's adjoint.
 // Neighbours are addressed by offsets (di, dj, dk) from the cell: compact
 // arrays with periodic wraps (Wrap3), primal storage arrays through their
 // halos.
@@ -391,6 +392,14 @@ __global__ void k3_adj_rhs(Adj3RhsArgs a) {
     }
     a.auy[oc] = acc;
     a.aify[oc] = SAY(0, 0, 0);
+    // the vof buoyancy grav (0.5 vof(j-1) + 0.5 vof(j) - vof_ref) of the uy
+    // faces j and j + 1
+    if (0. != a.grav_vof) {
+      const long v0 = ix_vof(g, i, j, k);
+      const double face = 0.5 * a.vof_post[v0 - (nx + 2)] + 0.5 * a.vof_post[v0] - a.vof_ref;
+      a.agrv[oc] += SAY(0, 0, 0) * face;
+      a.avof[oc] += a.grav_vof * 0.5 * (SAY(0, 0, 0) + SAY(0, 1, 0));
+    }
   }
   // ---- uz cell (i, j, k)
   {

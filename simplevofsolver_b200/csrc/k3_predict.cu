@@ -98,6 +98,7 @@ struct Stencil4 {
   double vc, vxm, vxp, vs, vn, vb, vt, vnb, v1n;
   double wc, wxm, wxp, ws, wn, wb, wt, wst, w1t;
   double tc, txm, txp, ts, tn, tb, tt;
+  double gv;  // the vof buoyancy's face value (used while grav_vof != 0)
   double pc, ps, pb, pxp;
   double ifx, ify, ifz;
   double dxf_i, dxf_i1, dxc_i1;
@@ -209,6 +210,8 @@ __device__ __forceinline__ void rhs4_values(const Predict3Args<R> &a, const Grid
     ra += md * (+lz[0] * zs + lz[1] * xc + lz[2] * zn);
     rg -= K.rdy * (-ps + pc);
     ra += ify;
+    // extension: buoyancy of the volume fraction (not in the reference)
+    if (0. != a.grav_vof) ra += a.grav_vof * (S.gv - a.vof_ref);
     sa[1] = ra;
     sg[1] = rg;
   }
@@ -418,6 +421,9 @@ __global__ void __launch_bounds__(RX * RY, 2) k3_rhs(Predict3Args<R> a) {
       S.pc = RING(4, s0, ty + 1, tx + 1);
       S.ps = RING(4, s0, ty, tx + 1);
       S.pb = RING(4, sm, ty + 1, tx + 1);
+      S.gv = (0. != a.grav_vof)
+                 ? 0.5 * ldg(a.vof + ix_vof(g, i, j - 1, k)) + 0.5 * ldg(a.vof + ix_vof(g, i, j, k))
+                 : 0.;
       S.pxp = RING(4, s0, ty + 1, tx + 2);
 #undef RING
       const long is = ix_src(g, i, j, k);

@@ -148,6 +148,8 @@ struct svof3d_solver {
   size_t stat_num = 0;
 
   Adjoint3State *adj = nullptr;
+  // vof buoyancy extension (svof3d_set_gravity; 0 = off)
+  double grav_vof = 0., vof_ref = 0.;
 
   Grid3 grid() const { return Grid3{nx, ny, nz, dy, dz, dxf.p, dxc.p}; }
 };
@@ -274,6 +276,9 @@ int launch_predict_t(svof3d_solver *s, int rk) {
   a.uz_xp = s->prm.uz_xp;
   a.t_xm = s->prm.t_xm;
   a.t_xp = s->prm.t_xp;
+  a.vof = s->vof[s->cur_v].p;  // after this substep's advection
+  a.grav_vof = s->grav_vof;
+  a.vof_ref = s->vof_ref;
   a.g = s->grid();
   CK(predict_launch<R>(s->stream, a));
   return 0;
@@ -1125,7 +1130,7 @@ struct Adjoint3State {
   // compact: ux faces nz x ny x (nx-1), cells nz x ny x nx
   DevBuf ux, uy, uz, p, vof[2], pend_v[2];
   DevBuf pend_x, pend_y, pend_z, sa_x, sg_x, sa_y, sg_y, sa_z, sg_z, ifx, ify, ifz, kap, m, nrm, sig;
-  DevBuf psib, b, psis, gbar, sum;
+  DevBuf psib, b, psis, gbar, grv, sum;
   DevBuf rxf, rxc;  // 1 / dxf, 1 / dxc
   int cv = 0;  // current buffer of vof_bar
   int cp = 0;  // current buffer of the vof source's pending adjoint
@@ -1134,7 +1139,7 @@ struct Adjoint3State {
   DevBuf *all(int q) {
     DevBuf *l[] = {&ux, &uy, &uz, &p, &vof[0], &vof[1], &pend_v[0], &pend_v[1], &pend_x, &pend_y, &pend_z,
                    &sa_x, &sg_x, &sa_y, &sg_y, &sa_z, &sg_z, &ifx, &ify, &ifz, &kap, &m, &nrm, &sig,
-                   &psib, &b, &psis, &gbar, &sum};
+                   &psib, &b, &psis, &gbar, &grv, &sum};
     return q < (int)(sizeof(l) / sizeof(l[0])) ? l[q] : nullptr;
   }
 };
@@ -1165,7 +1170,7 @@ int adj3_ensure(svof3d_solver *s) {
              dalloc(a->sa_z, nc) || dalloc(a->sg_z, nc) || dalloc(a->ifx, nf) || dalloc(a->ify, nc) ||
              dalloc(a->ifz, nc) || dalloc(a->kap, nc) || dalloc(a->m, 3 * nc) || dalloc(a->nrm, 4 * nc) ||
              dalloc(a->sig, nc) || dalloc(a->psib, nc) || dalloc(a->b, nc) || dalloc(a->psis, ncc) ||
-             dalloc(a->gbar, 3 * (nx + 1) * ny * nz) || dalloc(a->sum, 1);
+             dalloc(a->gbar, 3 * (nx + 1) * ny * nz) || dalloc(a->grv, nc) || dalloc(a->sum, 1);
   a->xs_smem = adj_xsolve_smem((int)nx);
   if (!bad && cudaSuccess != raise_smem_limit(k3_adj_xsolve, a->xs_smem)) bad = fail("cudaFuncSetAttribute(k3_adj_xsolve)");
   if (!bad) {
@@ -1234,8 +1239,10 @@ int adj3_potential(svof3d_solver *s, int rk, double dt) {
   return 0;
 }
 
-// fluid_predict_field about the primal velocities (storage layouts); d_dt must hold dt
-int adj3_predict(svof3d_solver *s, int rk, double dt, const double *ux, const double *uy, const double *uz) {
+// fluid_predict_field about the primal velocities and the vof after the
+// substep's advection (storage layouts); d_dt must hold dt
+int adj3_predict(svof3d_solver *s, int rk, double dt, const double *ux, const double *uy, const double *uz,
+                 const double *vof_post) {
   Adjoint3State *a = s->adj;
   k3_tdm_coef<<<1, 128, sizeof(double) * 6 * s->nx, s->stream>>>(s->lap_ux.p, s->lap_cc.p, s->d_dt,
                                                                  RK_A[rk] + RK_B[rk], s->prm.m_dif, s->prm.t_dif,
@@ -1273,6 +1280,11 @@ int adj3_predict(svof3d_solver *s, int rk, double dt, const double *ux, const do
   r.lz0 = s->lapz[0];
   r.lz1 = s->lapz[1];
   r.lz2 = s->lapz[2];
+  r.grav_vof = s->grav_vof;
+  r.vof_ref = s->vof_ref;
+  r.vof_post = vof_post;
+  r.avof = a->vof[a->cv].p;
+  r.agrv = a->grv.p;
   r.ag = agrid(s);
   k3_adj_rhs<<<adj3_cells(s), dim3(32, 8), 0, s->stream>>>(r);
   CK_LAUNCH();
@@ -1333,7 +1345,8 @@ int adj3_corners(svof3d_solver *s, const double *vof) {
 size_t n_ux3(const svof3d_solver *s) { return (size_t)(s->nx + 1) * (s->ny + 2) * (s->nz + 2); }
 size_t n_cc3(const svof3d_solver *s) { return (size_t)(s->nx + 2) * (s->ny + 2) * (s->nz + 2); }
 size_t n_vof3(const svof3d_solver *s) { return (size_t)(s->nx + 2) * (s->ny + 4) * (s->nz + 4); }
-// one substep's part of a tape: ux, uy, uz, vof
+// one substep's part of a tape: ux, uy, uz, vof; a tape holds three of
+// them and the step's final vof
 size_t tape_stride3(const svof3d_solver *s) { return n_ux3(s) + 2 * n_cc3(s) + n_vof3(s); }
 
 int adj3_check(svof3d_solver *s) {
@@ -1354,9 +1367,19 @@ int svof3d_set_tension(svof3d_solver_t *s, double tension) {
   return 0;
 }
 
+int svof3d_set_gravity(svof3d_solver_t *s, double grav_vof, double vof_ref) {
+  if (!s) return fail("null argument");
+  CK(cudaStreamSynchronize(s->stream));
+  s->grav_vof = grav_vof;
+  s->vof_ref = vof_ref;
+  for (auto &kv : s->graphs) cudaGraphExecDestroy(kv.second);
+  s->graphs.clear();
+  return 0;
+}
+
 int svof3d_tape_count(const svof3d_solver_t *s, size_t *count) {
   if (!s || !count) return fail("null argument");
-  *count = 3 * tape_stride3(s);
+  *count = 3 * tape_stride3(s) + n_vof3(s);
   return 0;
 }
 
@@ -1380,6 +1403,9 @@ int svof3d_integrate_fixed(svof3d_solver_t *s, double dt, double *tape) {
         launch_potential(s, rk) || launch_project(s, rk, 1, 1))
       return 1;
   }
+  if (tape)
+    CK(cudaMemcpyAsync(tape + 3 * st, s->vof[s->cur_v].p, sizeof(double) * nv, cudaMemcpyDeviceToDevice,
+                       s->stream));
   return 0;
 }
 
@@ -1407,6 +1433,7 @@ int svof3d_adjoint_field(svof3d_solver_t *s, int which, double **dptr, size_t *c
     case SVOF3_ADJ_SRCUZ_A: b = &a->pend_z; break;
     case SVOF3_ADJ_SRC_A: b = &a->pend_v[a->cp]; break;
     case SVOF3_ADJ_TENSION: b = &a->sig; break;
+    case SVOF3_ADJ_GRAVITY: b = &a->grv; break;
     default: return fail("unknown adjoint field %d", which);
   }
   *dptr = b->p;
@@ -1433,10 +1460,11 @@ int svof3d_adjoint_step(svof3d_solver_t *s, const double *tape, double dt) {
   if (adj3_set_dt(s, dt)) return 1;
   for (int rk = 2; rk >= 0; rk--) {
     const double *ux = tape + rk * st, *uy = ux + nu, *uz = uy + nc, *vof = uz + nc;
+    const double *vof_post = tape + (rk + 1) * st + (rk < 2 ? nu + 2 * nc : 0);
     // the substep's geometry (normals, intercepts, curvature) from its vof
     CK(interface_geom<double>(s->stream, vof, s->normal.as<double>(), s->curv.as<double>(), s->d_work, s->d_nwork,
                               s->grid()));
-    if (adj3_project(s, rk, dt, 3) || adj3_potential(s, rk, dt) || adj3_predict(s, rk, dt, ux, uy, uz) ||
+    if (adj3_project(s, rk, dt, 3) || adj3_potential(s, rk, dt) || adj3_predict(s, rk, dt, ux, uy, uz, vof_post) ||
         adj3_interface(s, rk, dt, 7, ux, uy, uz, vof) || adj3_corners(s, vof))
       return 1;
   }
@@ -1466,7 +1494,7 @@ int svof3d_adjoint_fluid_compute_potential_dft(svof3d_solver_t *s, size_t rk, do
 int svof3d_adjoint_fluid_predict_field(svof3d_solver_t *s, size_t rk, double dt) {
   SVOF_RANGE();
   if (adj3_check(s) || check_rk(rk)) return 1;
-  return adj3_set_dt(s, dt) || adj3_predict(s, (int)rk, dt, ADJ3_PRIMAL) || finish(s);
+  return adj3_set_dt(s, dt) || adj3_predict(s, (int)rk, dt, ADJ3_PRIMAL, s->vof[s->cur_v].p) || finish(s);
 }
 
 int svof3d_adjoint_interface_update_vof(svof3d_solver_t *s, size_t rk, double dt) {
@@ -1490,15 +1518,26 @@ int svof3d_adjoint_interface_compute_curvature_tensor(svof3d_solver_t *s) {
 
 #undef ADJ3_PRIMAL
 
-int svof3d_adjoint_tension(svof3d_solver_t *s, double *out) {
-  if (adj3_check(s)) return 1;
-  if (!out) return fail("null argument");
+// the deterministic sum of a per-cell accumulator, copied to the host
+static int adj3_total(svof3d_solver *s, const DevBuf &b, double *out) {
   Adjoint3State *a = s->adj;
-  k3_adj_sum<<<1, 256, 0, s->stream>>>(a->sig.p, (long)a->sig.n, a->sum.p);
+  k3_adj_sum<<<1, 256, 0, s->stream>>>(b.p, (long)b.n, a->sum.p);
   CK_LAUNCH();
   CK(cudaMemcpyAsync(out, a->sum.p, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   return 0;
+}
+
+int svof3d_adjoint_tension(svof3d_solver_t *s, double *out) {
+  if (adj3_check(s)) return 1;
+  if (!out) return fail("null argument");
+  return adj3_total(s, s->adj->sig, out);
+}
+
+int svof3d_adjoint_gravity(svof3d_solver_t *s, double *out) {
+  if (adj3_check(s)) return 1;
+  if (!out) return fail("null argument");
+  return adj3_total(s, s->adj->grv, out);
 }
 
 }  // extern "C"

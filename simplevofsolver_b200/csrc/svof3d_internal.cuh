@@ -132,6 +132,10 @@ struct Predict3Args {
   RK rk;
   int use_b, add_buoyancy;
   double uy_xm, uy_xp, uz_xm, uz_xp, t_xm, t_xp;
+  // extension (off while grav_vof == 0): srcuy += grav_vof (vof_face -
+  // vof_ref), vof the field after this substep's advection (storage layout)
+  const double *vof;
+  double grav_vof, vof_ref;
   Grid3 g;
 };
 template <class R>

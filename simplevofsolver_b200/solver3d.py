@@ -52,11 +52,12 @@ EXPORTS3D = ["svof3d_create", "svof3d_destroy", "svof3d_field_count", "svof3d_up
              "svof3d_adjoint_fluid_correct_velocity", "svof3d_adjoint_fluid_compute_potential_dft",
              "svof3d_adjoint_fluid_predict_field", "svof3d_adjoint_interface_update_vof",
              "svof3d_adjoint_interface_compute_force", "svof3d_adjoint_interface_compute_curvature_tensor",
-             "svof3d_adjoint_tension"]
+             "svof3d_adjoint_tension", "svof3d_set_gravity", "svof3d_adjoint_gravity"]
 
 # adjoint fields (SVOF3_ADJ_*); compact layouts: ux faces (nz, ny, nx-1), cells (nz, ny, nx)
 ADJ_FIELDS3D = {"ux": 0, "uy": 1, "uz": 2, "p": 3, "vof": 4, "psi": 5, "ifrcx": 6, "ifrcy": 7, "ifrcz": 8,
-                "curv": 9, "normal": 10, "srcux_a": 11, "srcuy_a": 12, "srcuz_a": 13, "src_a": 14, "tension": 15}
+                "curv": 9, "normal": 10, "srcux_a": 11, "srcuy_a": 12, "srcuz_a": 13, "src_a": 14, "tension": 15,
+                "gravity": 16}
 
 
 def adjoint_shape3d(name: str, nx: int, ny: int, nz: int):
@@ -140,6 +141,8 @@ def lib3() -> ctypes.CDLL:
         L.svof3d_adjoint_interface_compute_force.argtypes = [vp]
         L.svof3d_adjoint_interface_compute_curvature_tensor.argtypes = [vp]
         L.svof3d_adjoint_tension.argtypes = [vp, pd]
+        L.svof3d_set_gravity.argtypes = [vp, d, d]
+        L.svof3d_adjoint_gravity.argtypes = [vp, pd]
         _bound = True
     return L
 
@@ -172,6 +175,7 @@ class Solver3D:
                                physical["coef_dt_adv"], physical["coef_dt_dif"], int(bool(add_buoyancy)),
                                float(uy_walls[0]), float(uy_walls[1]), float(uz_walls[0]), float(uz_walls[1]),
                                float(t_walls[0]), float(t_walls[1]), PRECISIONS[precision])
+        self.gravity = (0.0, 0.0)
         self._h = ctypes.c_void_p()
         self._io_held = []
         xf, xc = _c(ic.xf), _c(ic.xc)
@@ -414,6 +418,11 @@ class Solver3D:
         _check(lib3().svof3d_set_tension(self._h, float(tension)))
         self.params.tension = float(tension)
 
+    def set_gravity(self, grav_vof: float, vof_ref: float):
+        """the vof buoyancy extension on uy (absent from the reference; 0 = off)"""
+        _check(lib3().svof3d_set_gravity(self._h, float(grav_vof), float(vof_ref)))
+        self.gravity = (float(grav_vof), float(vof_ref))
+
     def tape_count(self) -> int:
         n = ctypes.c_size_t(0)
         _check(lib3().svof3d_tape_count(self._h, ctypes.byref(n)))
@@ -433,6 +442,11 @@ class Solver3D:
     def adjoint_tension(self) -> float:
         out = ctypes.c_double(0.0)
         _check(lib3().svof3d_adjoint_tension(self._h, ctypes.byref(out)))
+        return out.value
+
+    def adjoint_gravity(self) -> float:
+        out = ctypes.c_double(0.0)
+        _check(lib3().svof3d_adjoint_gravity(self._h, ctypes.byref(out)))
         return out.value
 
     def adjoint_fluid_update_pressure(self, rk: int, dt: float):

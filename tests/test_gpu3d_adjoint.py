@@ -208,16 +208,20 @@ def test_compute_potential(gpu_available, rk):
 
 @pytest.mark.parametrize("rk", [0, 2])
 def test_predict_field(gpu_available, rk):
+    """with the vof buoyancy extension on: the source is bilinear in (vof,
+    grav), so the vof and grav directions are differenced separately"""
     ic, phys, g = make()
     dt = 1.2e-3
     rng = np.random.default_rng(3)
     fs, cs = shapes(g)
+    grav, dgrav = -0.9, 0.31
+    g.set_gravity(grav, 0.2)
     # src_b of this substep is the current src_a (the call swaps them first)
     for n, sh in (("srcux_a", fs), ("srcuy_a", cs), ("srcuz_a", cs)):
         g.set_field(n, rng.standard_normal(sh))
     for n, sh in (("ifrcx", fs), ("ifrcy", cs), ("ifrcz", cs)):
         g.set_field(n, rng.standard_normal(sh))
-    names = ("ux", "uy", "uz", "p", "ifrcx", "ifrcy", "ifrcz", "srcux_a", "srcuy_a", "srcuz_a")
+    names = ("ux", "uy", "uz", "p", "vof", "ifrcx", "ifrcy", "ifrcz", "srcux_a", "srcuy_a", "srcuz_a")
     st = State(g, names)
     d = {n: rng.standard_normal(st.base[n].shape if n not in State.INTERIOR else
                                 (fs if n == "ux" else cs)) for n in names}
@@ -228,13 +232,21 @@ def test_predict_field(gpu_available, rk):
         g.fluid_predict_field(rk, dt)
 
     lhs = central(st, d, 1.0, run, tuple(seeds), seeds)
+    vals = []
+    for sgn in (+1.0, -1.0):
+        st.load()
+        g.set_gravity(grav + sgn * dgrav, 0.2)
+        run()
+        vals.append({n: read(g, n) for n in seeds})
+    lhs += sum(float(np.sum(seeds[n] * (vals[0][n] - vals[1][n]) / 2.0)) for n in seeds)
+    g.set_gravity(grav, 0.2)
     st.load()
     g.adjoint_reset()
     for n, v in seeds.items():
         put_adj(g, n, v)
     g.adjoint_fluid_predict_field(rk, dt)
-    rhs = 0.0
-    for n in ("ux", "uy", "uz", "p", "ifrcx", "ifrcy", "ifrcz"):
+    rhs = dgrav * g.adjoint_gravity()
+    for n in ("ux", "uy", "uz", "p", "vof", "ifrcx", "ifrcy", "ifrcz"):
         rhs += float(np.sum(d[n] * get_adj(g, n)))
     if rk != 0:
         for n in ("srcux_a", "srcuy_a", "srcuz_a"):
@@ -331,8 +343,9 @@ def test_compute_curvature_tensor(gpu_available):
 
 
 def test_two_steps(gpu_available):
-    """two full steps (fixed dt): the directional derivative along a
-    divergence-free velocity and the tension against the adjoint"""
+    """two full steps (fixed dt), the vof buoyancy extension on: the
+    directional derivative along a divergence-free velocity, the tension and
+    the buoyancy coefficient against the adjoint"""
     import torch
     ic, phys, g = make()
     nx = g.nx
@@ -343,6 +356,7 @@ def test_two_steps(gpu_available):
     dirn = droplets3d(32, 16, 16, ndrops=1, radii=(0.12, 0.13), seed=11)
     d = {"ux": compact("ux", dirn.ux, nx), "uy": compact("uy", dirn.uy, nx), "uz": compact("uz", dirn.uz, nx)}
     dten = 0.3 * phys["tension"]
+    grav, dgrav = -0.9, 0.2
     seeds = {"ux": rng.standard_normal(fs), "uy": rng.standard_normal(cs), "uz": rng.standard_normal(cs),
              "p": rng.standard_normal(cs)}
     seeds["p"] -= seeds["p"].mean()
@@ -357,6 +371,7 @@ def test_two_steps(gpu_available):
                 x = x + e * embed(n, d[n], nx)
             g.load_interior(n, x)
         g.set_tension(phys["tension"] + e * dten)
+        g.set_gravity(grav + e * dgrav, 0.15)
         for _ in range(nsteps):
             g.integrate_fixed(dt)
         g.synchronize()
@@ -368,6 +383,7 @@ def test_two_steps(gpu_available):
     for n, v in ic.fields().items():
         g.load_interior(n, v)
     g.set_tension(phys["tension"])
+    g.set_gravity(grav, 0.15)
     tapes = [torch.empty(g.tape_count(), dtype=torch.float64, device="cuda") for _ in range(nsteps)]
     for t in tapes:
         g.integrate_fixed(dt, t.data_ptr())
@@ -377,7 +393,8 @@ def test_two_steps(gpu_available):
         put_adj(g, n, v)
     for t in reversed(tapes):
         g.adjoint_step(t.data_ptr(), dt)
-    rhs = sum(float(np.sum(d[n] * get_adj(g, n))) for n in d) + dten * g.adjoint_tension()
+    rhs = (sum(float(np.sum(d[n] * get_adj(g, n))) for n in d) + dten * g.adjoint_tension()
+           + dgrav * g.adjoint_gravity())
     assert rel(lhs, rhs) <= 1e-5, (lhs, rhs)
 
 

@@ -193,3 +193,32 @@ def test_generator_is_divergence_free_and_seeded():
             dy = min(abs(y - y2), 1 - abs(y - y2))
             dz = min(abs(z - z2), 1 - abs(z - z2))
             assert (x - x2) ** 2 + dy ** 2 + dz ** 2 >= (r + r2) ** 2
+
+
+def test_vof_buoyancy_term_is_the_last_addition():
+    """the extension adds grav (0.5 vof(j-1) + 0.5 vof(j) - vof_ref) to uy's
+    src_a after every reference term: the source with it on equals the source
+    without it plus the term, bit for bit; grav 0 leaves the step unchanged"""
+    ic = droplets3d(24, 16, 16, ndrops=3, radii=(0.12, 0.2), seed=3)
+    phys = physical_params(DROPLETS3D_ENV)
+    a, b = Oracle3D(ic, phys), Oracle3D(ic, phys)
+    b.set_gravity(-0.9, 0.2)
+    dt = a.decide_dt()
+    for o in (a, b):
+        o.curvature_tensor()
+        o.force()
+        o.update_vof(0, dt)
+        o.predict(0, dt)
+    vof = b.field("vof")                                     # after the advection
+    nz, ny, nx = 16, 16, 24
+    v = vof[2:nz + 2, :, 1:nx + 1]                           # rows j = -1 .. ny+2 at index j + 1
+    face = 0.5 * v[:, 0 + 1:ny + 1] + 0.5 * v[:, 1 + 1:ny + 2] - 0.2
+    expect = a.field("srcuy0") + (-0.9) * face
+    assert np.array_equal(b.field("srcuy0"), expect)
+    c = Oracle3D(ic, phys)
+    c.set_gravity(0.0, 0.7)
+    a2 = Oracle3D(ic, phys)
+    c.run(2)
+    a2.run(2)
+    for k in ("ux", "uy", "uz", "p", "vof"):
+        assert np.array_equal(c.field(k), a2.field(k))
