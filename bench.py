@@ -27,8 +27,9 @@ The 3D line also carries the differentiation form's cost ("adjoint",
 steps, checkpoints every 20) the device time per step of the backward pass
 (segment recompute with tapes plus the CUDA step adjoints) over that of the
 forward (--no-adjoint skips it), the same ratio for the 3D form
-("adjoint3d": droplets3d 256^3, FP64, 20 steps, checkpoints every 10), and
-the defect-corrected mixed form
+("adjoint3d": the 3D differentiation workload, 256^3, 16 droplets, density
+ratio 0.05, 100 steps, mixed and FP64 forwards, checkpoints fitted to a
+60 GB budget), and the defect-corrected mixed form
 ("mixed_dc": the Poisson solve as two FP32 passes with an FP64 residual,
 its throughput and its error against the FP64 path; --no-dc skips it).
 
@@ -393,73 +394,91 @@ def adjoint_cost(steps: int = 200, K: int = 20):
             "forward": "svof_integrate_fixed (time steps held fixed)"}
 
 
-def adjoint_cost3d(n: int = 256, steps: int = 20, K: int = 10):
-    """Cost of the 3D differentiation form (FP64): droplets3d at n^3 (the
-    generator of the 3D workload), the CFL time-step sequence of `steps`
-    steps held fixed; device time per step of the forward
+def adjoint_cost3d(n: int = 256, steps: int = 100, budget: float = 60e9, precisions=("mixed", "fp64")):
+    """Cost of the 3D differentiation form on its workload (diff3d_case:
+    droplets3d at n^3, 16 droplets of radii in [0.05, 0.09], the vof buoyancy
+    extension with density ratio 0.05 at Fr = 1, `steps` steps with the FP64
+    path's CFL time-step sequence held fixed), per forward precision (the
+    adjoint computes in FP64 on both): device time per step of the forward
     (svof3d_integrate_fixed) and of the backward pass (segment recompute with
     tapes plus svof3d_adjoint_step), CUDA events on the solver's stream;
-    adjoint_over_forward = backward / forward per step."""
+    checkpoints every K steps, K the largest whose tapes and checkpoints fit
+    `budget` bytes (adjoint.checkpoint_interval)."""
     import torch
-    from simplevofsolver_b200.adjoint import Rollout3D
+    from simplevofsolver_b200.adjoint import Rollout3D, checkpoint_interval
     from simplevofsolver_b200.solver3d import Solver3D
-    from simplevofsolver_b200.workloads import DROPLETS3D_ENV, droplets3d, physical_params
-    ic = droplets3d(n, n, n, ndrops=32, radii=(0.04, 0.08), seed=1)
+    from simplevofsolver_b200.workloads import DROPLETS3D_ENV, diff3d_case, gravity3d, physical_params
+    ic = diff3d_case(n)
     phys = physical_params(DROPLETS3D_ENV)
+    grav, ref = gravity3d(ic)
     s = Solver3D(ic, phys)
+    s.set_gravity(grav, ref)
     dts = list(s.run(steps))
-    for k, v in ic.fields().items():
-        s.load_interior(k, v)
-    r = Rollout3D(s, dts, K, project_initial=False)
+    s.close()
     dev = dict(dtype=torch.float64, device="cuda")
     x = [torch.tensor(ic.ux[..., 1:n], **dev)] + [torch.tensor(getattr(ic, f)[..., 1:n + 1], **dev)
                                                   for f in ("uy", "uz", "vof")] + [phys["tension"]]
-    stream = torch.cuda.ExternalStream(s.stream())
-    tapes = [torch.empty(s.tape_count(), **dev) for _ in range(K)]
+    out = {"workload": f"diff3d_{n} (droplets3d {n}^3, 16 droplets r 0.05-0.09, density ratio 0.05, Fr 1, "
+                       f"{steps} steps)", "steps": steps, "hbm_budget_gb": budget / 1e9,
+           "adjoint_dtype": "f64",
+           "backward": "segment recompute with tapes + step adjoints (svof3d_adjoint_step)",
+           "forward": "svof3d_integrate_fixed (time steps held fixed)"}
+    for prec in precisions:
+        s = Solver3D(ic, phys, precision=prec)
+        s.set_gravity(grav, ref)
+        K = checkpoint_interval(s, steps, budget)
+        r = Rollout3D(s, dts, K)
+        stream = torch.cuda.ExternalStream(s.stream())
+        tapes = [torch.empty(s.tape_count(), **dev) for _ in range(K)]
 
-    def fwd():
-        r.load(*x)
-        s.synchronize()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        with torch.cuda.stream(stream):
-            e0.record(stream)
-            for dt in dts:
-                s.integrate_fixed(dt)
-            e1.record(stream)
-        torch.cuda.synchronize()
-        return e0.elapsed_time(e1)
-
-    def bwd():
-        r.forward(*x)
-        s.adjoint_reset()
-        s.synchronize()
-        ms = 0.0
-        for seg in reversed(range(len(r.checkpoints))):
-            n0, n1 = seg * K, min(steps, seg * K + K)
-            r._restore_state(r.checkpoints[seg])
+        def fwd():
+            r.load(*x)
+            s.synchronize()
+            torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             with torch.cuda.stream(stream):
                 e0.record(stream)
-                for k in range(n0, n1):
-                    s.integrate_fixed(dts[k], tapes[k - n0].data_ptr())
-                for k in reversed(range(n0, n1)):
-                    s.adjoint_step(tapes[k - n0].data_ptr(), dts[k])
+                for dt in dts:
+                    s.integrate_fixed(dt)
                 e1.record(stream)
             torch.cuda.synchronize()
-            ms += e0.elapsed_time(e1)
-        return ms
+            return e0.elapsed_time(e1)
 
-    fwd()
-    bwd()
-    f_ms = min(fwd() for _ in range(3))
-    b_ms = min(bwd() for _ in range(3))
-    s.close()
-    return {"workload": f"droplets3d_{n} (32 droplets, stretched x)", "steps": steps, "checkpoint_every": K,
-            "dtype": "f64", "forward_ms_per_step": f_ms / steps, "backward_ms_per_step": b_ms / steps,
-            "adjoint_over_forward": b_ms / f_ms,
-            "backward": "segment recompute with tapes + step adjoints (svof3d_adjoint_step)",
-            "forward": "svof3d_integrate_fixed (time steps held fixed)"}
+        def bwd():
+            r.forward(*x)
+            s.adjoint_reset()
+            s.synchronize()
+            ms = 0.0
+            for seg in reversed(range(len(r.checkpoints))):
+                n0, n1 = seg * K, min(steps, seg * K + K)
+                r._restore_state(r.checkpoints[seg])
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                with torch.cuda.stream(stream):
+                    e0.record(stream)
+                    for k in range(n0, n1):
+                        s.integrate_fixed(dts[k], tapes[k - n0].data_ptr())
+                    for k in reversed(range(n0, n1)):
+                        s.adjoint_step(tapes[k - n0].data_ptr(), dts[k])
+                    e1.record(stream)
+                torch.cuda.synchronize()
+                ms += e0.elapsed_time(e1)
+            return ms
+
+        fwd()
+        bwd()
+        f_ms = min(fwd() for _ in range(2))
+        b_ms = min(bwd() for _ in range(2))
+        state_gb = sum(v.numel() for v in r.checkpoints[0].values()) * 8 / 1e9
+        out[prec] = {"forward_ms_per_step": f_ms / steps, "backward_ms_per_step": b_ms / steps,
+                     "adjoint_over_forward": b_ms / f_ms, "checkpoint_every": K,
+                     "tapes_gb": K * s.tape_count() * 8 / 1e9,
+                     "checkpoints_gb": len(r.checkpoints) * state_gb}
+        del tapes
+        r.checkpoints = []
+        s.close()
+        torch.cuda.empty_cache()
+    out["adjoint_over_forward"] = out[precisions[0]]["adjoint_over_forward"]
+    return out
 
 
 def _profile(solver, nprof):

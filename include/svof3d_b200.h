@@ -227,8 +227,11 @@ int svof3d_statistics_field(svof3d_solver_t *s, int quantity, double *out, size_
  * while the extension is on.  A tape (svof3d_tape_count() doubles) holds the
  * three substeps' inputs and the step's final vof.  Adjoint fields are compact: ux faces nz x ny x (nx-1), cells
  * nz x ny x nx, normal nz x ny x nx x 4, tension one value per cell (summed
- * by svof3d_adjoint_tension).  Requires precision SVOF3_FP64 and
- * add_buoyancy 0; the temperature is not differentiated. */
+ * by svof3d_adjoint_tension).  Requires add_buoyancy 0; the temperature is
+ * not differentiated.  The adjoint computes in FP64 on every precision: with
+ * SVOF3_MIXED / SVOF3_MIXED_DC it is the FP64 step's transpose about the
+ * mixed trajectory (the taped FP64 fields), the interface transposes reading
+ * normals, intercepts and curvature recomputed in FP64 from vof. */
 enum {
   SVOF3_ADJ_UX = 0,
   SVOF3_ADJ_UY,
@@ -261,6 +264,13 @@ int svof3d_integrate_fixed(svof3d_solver_t *s, double dt, double *tape);
 /* device pointer and element count of an adjoint field (made on first use) */
 int svof3d_adjoint_field(svof3d_solver_t *s, int which, double **dptr, size_t *count);
 int svof3d_adjoint_reset(svof3d_solver_t *s);
+/* the adjoint's gradient floor tau: a corner whose vof gradient times its
+ * smallest spacing is below tau (a vof variation below tau across a cell)
+ * counts as flat and its normal's transpose (I - n n^T) / |g| as zero.  0,
+ * the default of SVOF3_FP64, is the exact transpose; the mixed paths default
+ * to 1e-5, below which their FP32 fluxes' vof noise (about 1e-8 beside the
+ * interface) would make those transposes grow without bound over steps. */
+int svof3d_adjoint_set_gradient_floor(svof3d_solver_t *s, double tau);
 int svof3d_adjoint_step(svof3d_solver_t *s, const double *tape, double dt);
 int svof3d_adjoint_fluid_update_pressure(svof3d_solver_t *s, size_t rkstep, double dt);
 int svof3d_adjoint_fluid_correct_velocity(svof3d_solver_t *s, size_t rkstep, double dt);

@@ -369,6 +369,44 @@ def rollout3d(ux0, uy0, uz0, vof0, tension, r: Rollout3D, grav=None):
     return _RF3.apply(ux0, uy0, uz0, vof0, tension, grav, r)
 
 
+def interface_area3d(vof, xf, ly: float = 1.0, lz: float = 1.0, delta: float = 1e-9):
+    """the 3D differentiation workload's objective: the interface area
+    estimated from |grad vof|, sum over cells of |g| dxf dy dz with g the
+    cell-centred central differences of vof (x: over the centres xc(i-1),
+    xc(i+1), the wall values 0 beyond the first and last cells; y, z:
+    periodic) and |g| smoothed as sqrt(|g|^2 + delta^2) - delta, so that
+    cells of uniform vof add exactly 0 and the gradient stays finite there.
+    vof: (nz, ny, nx) tensor."""
+    import torch
+    nz, ny, nx = vof.shape
+    dy, dz = ly / ny, lz / nz
+    xf = torch.as_tensor(np.asarray(xf), dtype=torch.float64, device=vof.device)
+    dxf = xf[1:] - xf[:-1]
+    xc = torch.cat([xf[:1], 0.5 * (xf[1:] + xf[:-1]), xf[-1:]])           # nx + 2, walls included
+    zero = torch.zeros_like(vof[..., :1])
+    vx = torch.cat([zero, vof, zero], dim=-1)
+    gx = (vx[..., 2:] - vx[..., :-2]) / (xc[2:] - xc[:-2])
+    gy = (torch.roll(vof, -1, dims=1) - torch.roll(vof, 1, dims=1)) / (2 * dy)
+    gz = (torch.roll(vof, -1, dims=0) - torch.roll(vof, 1, dims=0)) / (2 * dz)
+    mag = torch.sqrt(gx * gx + gy * gy + gz * gz + delta * delta) - delta
+    return torch.sum(mag * dxf[None, None, :]) * dy * dz
+
+
+def checkpoint_interval(solver, nsteps: int, budget_bytes: float) -> int:
+    """the largest K whose K tapes plus ceil(nsteps / K) checkpoints of the
+    state (ux, uy, uz, p, t, vof) fit in budget_bytes of device memory (the
+    solver's own buffers not counted); at least 1"""
+    nx, ny, nz = solver.nx, solver.ny, solver.nz
+    tape = 8.0 * solver.tape_count()
+    state = 8.0 * ((nx + 1) * (ny + 2) * (nz + 2) + 4 * (nx + 2) * (ny + 2) * (nz + 2)
+                   + (nx + 2) * (ny + 4) * (nz + 4))
+    best = 1
+    for K in range(1, max(1, nsteps) + 1):
+        if K * tape + -(-nsteps // K) * state <= budget_bytes:
+            best = K
+    return best
+
+
 def falling_objective(ux, uy, vof, xf, ly: float = 1.0):
     """the differentiation workload's objective: the vof-weighted centroid y
     of the droplet plus 0.1 times the kinetic energy (the reference's energy
@@ -387,4 +425,5 @@ def falling_objective(ux, uy, vof, xf, ly: float = 1.0):
     return centroid + 0.1 * ke
 
 
-__all__ = ["Rollout", "rollout", "Rollout3D", "rollout3d", "falling_objective", "SvofError"]
+__all__ = ["Rollout", "rollout", "Rollout3D", "rollout3d", "falling_objective", "interface_area3d",
+           "checkpoint_interval", "SvofError"]

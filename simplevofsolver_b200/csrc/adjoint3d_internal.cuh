@@ -13,6 +13,10 @@ struct AGrid3 {
   const double *rxf;  // [nx]   1 / dxf
   const double *rxc;  // [nx+1] 1 / dxc
   double rdy, rdz;
+  // gradient floor tau: a corner whose gradient times its smallest spacing
+  // is below tau (a vof variation below tau across a cell) counts as flat,
+  // its normal's transpose zero; 0 = the exact transpose
+  double tau;
 };
 
 // lines per block and points per shared-memory chunk of k3_adj_xsolve

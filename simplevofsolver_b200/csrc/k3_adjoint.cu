@@ -660,8 +660,9 @@ __global__ void k3_adj_interface(Adj3IfaceArgs a) {
 // adjoint from the eight cells around it, cell (ic-1+dp, jc-1+dq, kc-1+dr):
 // m_bar / (dxf, dy, dz) of the cell's mean normal and -+ kappa_bar / (4 dxf,
 // 4 dy, 4 dz) of its curvature (+ for the cell's left / lower corner), then
-// the normalisation's transpose; gbar[3 corner] = the corner gradient's
-// adjoint, corner = (ic - 1) + (nx + 1) ((jc - 1) + ny (kc - 1)).
+// the normalisation's transpose (zero at a corner flatter than the gradient
+// floor tau); gbar[3 corner] = the corner gradient's adjoint, corner =
+// (ic - 1) + (nx + 1) ((jc - 1) + ny (kc - 1)).
 __global__ void k3_adj_cgrad(const double *__restrict__ vof, const double *__restrict__ am,
                              const double *__restrict__ akap, double *__restrict__ gbar, AGrid3 ag) {
   const Grid3 &g = ag.g;
@@ -687,6 +688,11 @@ __global__ void k3_adj_cgrad(const double *__restrict__ vof, const double *__res
   corner_grad3(vof, ag, ic, jc, kc, gx, gy, gz);
   double o0, o1, o2;
   unit_adj3(gx, gy, gz, b[0], b[1], b[2], o0, o1, o2);
+  if (ag.tau > 0.) {
+    // |g| h < tau with h = min(dxc, dy, dz): a flat corner, no derivative
+    const double rmax = fmax(ag.rxc[ic - 1], fmax(ag.rdy, ag.rdz));
+    if (sqrt(gx * gx + gy * gy + gz * gz) < ag.tau * rmax) o0 = o1 = o2 = 0.;
+  }
   const long q = (long)(ic - 1) + (long)(nx + 1) * ((long)(jc - 1) + (long)ny * (kc - 1));
   gbar[3 * q + 0] = o0;
   gbar[3 * q + 1] = o1;

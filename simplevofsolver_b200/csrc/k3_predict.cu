@@ -98,7 +98,7 @@ struct Stencil4 {
   double vc, vxm, vxp, vs, vn, vb, vt, vnb, v1n;
   double wc, wxm, wxp, ws, wn, wb, wt, wst, w1t;
   double tc, txm, txp, ts, tn, tb, tt;
-  double gv;  // the vof buoyancy's face value (used while grav_vof != 0)
+  double gv;  // the vof buoyancy's face value (the GRAV instantiation only)
   double pc, ps, pb, pxp;
   double ifx, ify, ifz;
   double dxf_i, dxf_i1, dxc_i1;
@@ -138,7 +138,7 @@ __device__ __forceinline__ RhsCoef rhs_coef(double dxf_i, double dxf_i1, double 
 // x-implicit diffusion and the pressure gradient into sg[f], in the
 // restatement's order (advection x, y, z; diffusion x, y, z; pressure;
 // buoyancy; surface).  Fields 0 ux (do_ux: the face exists), 1 uy, 2 uz, 3 t.
-template <class R>
+template <class R, bool GRAV>
 __device__ __forceinline__ void rhs4_values(const Predict3Args<R> &a, const Grid3 &g, const Stencil4 &S,
                                             const RhsCoef &K, bool do_ux, double *sa, double *sg) {
   const double u00 = S.u00, u10 = S.u10, u20 = S.u20, u0s = S.u0s, u1s = S.u1s, u1n = S.u1n, u0b = S.u0b,
@@ -211,7 +211,7 @@ __device__ __forceinline__ void rhs4_values(const Predict3Args<R> &a, const Grid
     rg -= K.rdy * (-ps + pc);
     ra += ify;
     // extension: buoyancy of the volume fraction (not in the reference)
-    if (0. != a.grav_vof) ra += a.grav_vof * (S.gv - a.vof_ref);
+    if (GRAV) ra += a.grav_vof * (S.gv - a.vof_ref);
     sa[1] = ra;
     sg[1] = rg;
   }
@@ -291,7 +291,9 @@ template <class R>
 constexpr size_t kRhsSmem =
     sizeof(double) * NFLD * NSLOT * WY * WX + (kRhsDirect<R> ? 0 : sizeof(R) * NCEN * NSLOT * RY * RX);
 
-template <class R>
+// GRAV: the instantiation with the vof buoyancy extension (grav_vof != 0);
+// the other one is the reference's right-hand side alone
+template <class R, bool GRAV>
 __global__ void __launch_bounds__(RX * RY, 2) k3_rhs(Predict3Args<R> a) {
   extern __shared__ double ring[];  // [NFLD][NSLOT][WY][WX]
   const Grid3 g = a.g;
@@ -421,9 +423,8 @@ __global__ void __launch_bounds__(RX * RY, 2) k3_rhs(Predict3Args<R> a) {
       S.pc = RING(4, s0, ty + 1, tx + 1);
       S.ps = RING(4, s0, ty, tx + 1);
       S.pb = RING(4, sm, ty + 1, tx + 1);
-      S.gv = (0. != a.grav_vof)
-                 ? 0.5 * ldg(a.vof + ix_vof(g, i, j - 1, k)) + 0.5 * ldg(a.vof + ix_vof(g, i, j, k))
-                 : 0.;
+      S.gv = 0.;
+      if (GRAV) S.gv = 0.5 * ldg(a.vof + ix_vof(g, i, j - 1, k)) + 0.5 * ldg(a.vof + ix_vof(g, i, j, k));
       S.pxp = RING(4, s0, ty + 1, tx + 2);
 #undef RING
       const long is = ix_src(g, i, j, k);
@@ -447,7 +448,7 @@ __global__ void __launch_bounds__(RX * RY, 2) k3_rhs(Predict3Args<R> a) {
       S.lc1 = lc1;
       S.lc2 = lc2;
       double sa[4], sg[4];
-      rhs4_values(a, g, S, K, do_ux, sa, sg);
+      rhs4_values<R, GRAV>(a, g, S, K, do_ux, sa, sg);
       const size_t line = (size_t)(j - 1) + (size_t)ny * (k - 1);
       R *dl = a.fw + line * nx + (i - 1);
       if (do_ux) {
@@ -689,7 +690,8 @@ template <class R>
 cudaError_t predict_launch(cudaStream_t st, const Predict3Args<R> &a) {
   const Grid3 &g = a.g;
   dim3 gr((g.nx + RX - 1) / RX, (g.ny + RY - 1) / RY, (g.nz + RZ - 1) / RZ);
-  k3_rhs<R><<<gr, RX * RY, kRhsSmem<R>, st>>>(a);
+  if (0. != a.grav_vof) k3_rhs<R, true><<<gr, RX * RY, kRhsSmem<R>, st>>>(a);
+  else k3_rhs<R, false><<<gr, RX * RY, kRhsSmem<R>, st>>>(a);
   cudaError_t e = cudaGetLastError();
   if (cudaSuccess != e) return e;
   const long nlines = (long)g.ny * g.nz;
@@ -699,7 +701,9 @@ cudaError_t predict_launch(cudaStream_t st, const Predict3Args<R> &a) {
 
 template <class R>
 cudaError_t predict_prepare_t() {
-  return raise_smem_limit(k3_rhs<R>, kRhsSmem<R>);
+  const cudaError_t e = raise_smem_limit(k3_rhs<R, false>, kRhsSmem<R>);
+  if (cudaSuccess != e) return e;
+  return raise_smem_limit(k3_rhs<R, true>, kRhsSmem<R>);
 }
 #if SVOF3_WITH_F64
 template cudaError_t predict_launch<double>(cudaStream_t, const Predict3Args<double> &);

@@ -1124,7 +1124,11 @@ int svof3d_stream(svof3d_solver_t *s, void **stream) {
 // update, the CSF force, the intercept and normals, the corner gradients
 // (k3_adjoint.cu).  The per-function entry points expose the same pieces one
 // by one about the solver's current fields.  The temperature is not
-// differentiated (add_buoyancy must be 0); the mixed paths have no adjoint.
+// differentiated (add_buoyancy must be 0).  The adjoint computes in FP64 on
+// every path: with the mixed paths (FP32 geometry, FP32 sources) it is the
+// FP64 step's transpose about the mixed trajectory, its geometry (normals,
+// intercepts, curvature) recomputed in FP64 from the taped vof into buffers
+// of its own.
 
 struct Adjoint3State {
   // compact: ux faces nz x ny x (nx-1), cells nz x ny x nx
@@ -1132,9 +1136,11 @@ struct Adjoint3State {
   DevBuf pend_x, pend_y, pend_z, sa_x, sg_x, sa_y, sg_y, sa_z, sg_z, ifx, ify, ifz, kap, m, nrm, sig;
   DevBuf psib, b, psis, gbar, grv, sum;
   DevBuf rxf, rxc;  // 1 / dxf, 1 / dxc
+  DevBuf nrm64, curv64;  // FP64 geometry of the mixed paths (storage layouts)
   int cv = 0;  // current buffer of vof_bar
   int cp = 0;  // current buffer of the vof source's pending adjoint
   size_t xs_smem = 0;
+  double tau = 0.;  // gradient floor (svof3d_adjoint_set_gradient_floor)
   // the adjoint fields and scratch (zeroed by svof3d_adjoint_reset)
   DevBuf *all(int q) {
     DevBuf *l[] = {&ux, &uy, &uz, &p, &vof[0], &vof[1], &pend_v[0], &pend_v[1], &pend_x, &pend_y, &pend_z,
@@ -1149,15 +1155,22 @@ void adjoint3_free(svof3d_solver *s) {
   for (int q = 0; DevBuf *b = s->adj->all(q); q++) dfree(*b);
   dfree(s->adj->rxf);
   dfree(s->adj->rxc);
+  dfree(s->adj->nrm64);
+  dfree(s->adj->curv64);
   delete s->adj;
   s->adj = nullptr;
 }
 
 namespace {
 
+// the mixed paths' default gradient floor: their FP32 fluxes leave vof noise
+// of order 1e-8 beside the interface, where corners with such tiny gradients
+// would make the normals' transposes (I - n n^T) / |g| grow without bound
+// from step to step
+constexpr double kAdjMixedTau = 1e-5;
+
 int adj3_ensure(svof3d_solver *s) {
   if (s->adj) return 0;
-  if (s->mixed) return fail("the adjoint needs the FP64 path (precision SVOF3_FP64)");
   if (s->prm.add_buoyancy) return fail("the adjoint needs add_buoyancy = 0 (t is not differentiated)");
   const size_t nx = s->nx, ny = s->ny, nz = s->nz;
   if (adj_xsolve_smem((int)nx) > 200 * 1024) return fail("the adjoint's x line solve needs nx <= 7800");
@@ -1171,7 +1184,11 @@ int adj3_ensure(svof3d_solver *s) {
              dalloc(a->ifz, nc) || dalloc(a->kap, nc) || dalloc(a->m, 3 * nc) || dalloc(a->nrm, 4 * nc) ||
              dalloc(a->sig, nc) || dalloc(a->psib, nc) || dalloc(a->b, nc) || dalloc(a->psis, ncc) ||
              dalloc(a->gbar, 3 * (nx + 1) * ny * nz) || dalloc(a->grv, nc) || dalloc(a->sum, 1);
+  if (!bad && s->mixed)
+    bad = dalloc(a->nrm64, 4 * nx * (ny + 2) * (nz + 2)) || dalloc(a->curv64, ncc) ||
+          (s->dc && cudaSuccess != pois_prepare<double>(s->log2ny, s->log2nz));
   a->xs_smem = adj_xsolve_smem((int)nx);
+  a->tau = s->mixed ? kAdjMixedTau : 0.;
   if (!bad && cudaSuccess != raise_smem_limit(k3_adj_xsolve, a->xs_smem)) bad = fail("cudaFuncSetAttribute(k3_adj_xsolve)");
   if (!bad) {
     // reciprocal spacings from the device tables
@@ -1198,7 +1215,17 @@ int adj3_ensure(svof3d_solver *s) {
 dim3 adj3_cells(const svof3d_solver *s) { return dim3((s->nx + 31) / 32, (s->ny + 7) / 8, s->nz); }
 
 AGrid3 agrid(const svof3d_solver *s) {
-  return AGrid3{s->grid(), s->adj->rxf.p, s->adj->rxc.p, 1. / s->dy, 1. / s->dz};
+  return AGrid3{s->grid(), s->adj->rxf.p, s->adj->rxc.p, 1. / s->dy, 1. / s->dz, s->adj->tau};
+}
+
+// the geometry the interface transposes read: the solver's own (FP64 path)
+// or, on the mixed paths, an FP64 recomputation from vof into the adjoint's
+// buffers (adj3_geometry recomputes it from vof)
+double *adj3_normal(svof3d_solver *s) { return s->mixed ? s->adj->nrm64.p : s->normal.p; }
+double *adj3_curv(svof3d_solver *s) { return s->mixed ? s->adj->curv64.p : s->curv.p; }
+int adj3_geometry(svof3d_solver *s, const double *vof) {
+  CK(interface_geom<double>(s->stream, vof, adj3_normal(s), adj3_curv(s), s->d_work, s->d_nwork, s->grid()));
+  return 0;
 }
 
 int adj3_set_dt(svof3d_solver *s, double dt) {
@@ -1302,8 +1329,8 @@ int adj3_interface(svof3d_solver *s, int rk, double dt, int mode, const double *
   f.uy = uy;
   f.uz = uz;
   f.vof = vof;
-  f.normal = s->normal.p;
-  f.curv = s->curv.p;
+  f.normal = adj3_normal(s);
+  f.curv = adj3_curv(s);
   f.avof_in = a->vof[a->cv].p;
   f.avof_out = a->vof[1 - a->cv].p;
   f.pend_in = a->pend_v[a->cp].p;
@@ -1353,6 +1380,7 @@ int adj3_check(svof3d_solver *s) {
   if (!s) return fail("null argument");
   return adj3_ensure(s);
 }
+
 
 }  // namespace
 
@@ -1441,6 +1469,13 @@ int svof3d_adjoint_field(svof3d_solver_t *s, int which, double **dptr, size_t *c
   return 0;
 }
 
+int svof3d_adjoint_set_gradient_floor(svof3d_solver_t *s, double tau) {
+  if (adj3_check(s)) return 1;
+  if (!(tau >= 0.)) return fail("svof3d_adjoint_set_gradient_floor: tau must be non-negative");
+  s->adj->tau = tau;
+  return 0;
+}
+
 int svof3d_adjoint_reset(svof3d_solver_t *s) {
   if (adj3_check(s)) return 1;
   for (int q = 0; DevBuf *b = s->adj->all(q); q++) CK(cudaMemsetAsync(b->p, 0, sizeof(double) * b->n, s->stream));
@@ -1462,8 +1497,7 @@ int svof3d_adjoint_step(svof3d_solver_t *s, const double *tape, double dt) {
     const double *ux = tape + rk * st, *uy = ux + nu, *uz = uy + nc, *vof = uz + nc;
     const double *vof_post = tape + (rk + 1) * st + (rk < 2 ? nu + 2 * nc : 0);
     // the substep's geometry (normals, intercepts, curvature) from its vof
-    CK(interface_geom<double>(s->stream, vof, s->normal.as<double>(), s->curv.as<double>(), s->d_work, s->d_nwork,
-                              s->grid()));
+    if (adj3_geometry(s, vof)) return 1;
     if (adj3_project(s, rk, dt, 3) || adj3_potential(s, rk, dt) || adj3_predict(s, rk, dt, ux, uy, uz, vof_post) ||
         adj3_interface(s, rk, dt, 7, ux, uy, uz, vof) || adj3_corners(s, vof))
       return 1;
@@ -1500,20 +1534,23 @@ int svof3d_adjoint_fluid_predict_field(svof3d_solver_t *s, size_t rk, double dt)
 int svof3d_adjoint_interface_update_vof(svof3d_solver_t *s, size_t rk, double dt) {
   SVOF_RANGE();
   if (adj3_check(s) || check_rk(rk)) return 1;
-  return adj3_interface(s, (int)rk, dt, 1, ADJ3_PRIMAL, s->vof[s->cur_v].p) || finish(s);
+  const double *vof = s->vof[s->cur_v].p;
+  return (s->mixed && adj3_geometry(s, vof)) || adj3_interface(s, (int)rk, dt, 1, ADJ3_PRIMAL, vof) || finish(s);
 }
 
 int svof3d_adjoint_interface_compute_force(svof3d_solver_t *s) {
   SVOF_RANGE();
   if (adj3_check(s)) return 1;
-  return adj3_interface(s, 0, 0., 2, ADJ3_PRIMAL, s->vof[s->cur_v].p) || finish(s);
+  const double *vof = s->vof[s->cur_v].p;
+  return (s->mixed && adj3_geometry(s, vof)) || adj3_interface(s, 0, 0., 2, ADJ3_PRIMAL, vof) || finish(s);
 }
 
 int svof3d_adjoint_interface_compute_curvature_tensor(svof3d_solver_t *s) {
   SVOF_RANGE();
   if (adj3_check(s)) return 1;
   const double *vof = s->vof[s->cur_v].p;
-  return adj3_interface(s, 0, 0., 4, ADJ3_PRIMAL, vof) || adj3_corners(s, vof) || finish(s);
+  return (s->mixed && adj3_geometry(s, vof)) || adj3_interface(s, 0, 0., 4, ADJ3_PRIMAL, vof) ||
+         adj3_corners(s, vof) || finish(s);
 }
 
 #undef ADJ3_PRIMAL

@@ -52,7 +52,8 @@ EXPORTS3D = ["svof3d_create", "svof3d_destroy", "svof3d_field_count", "svof3d_up
              "svof3d_adjoint_fluid_correct_velocity", "svof3d_adjoint_fluid_compute_potential_dft",
              "svof3d_adjoint_fluid_predict_field", "svof3d_adjoint_interface_update_vof",
              "svof3d_adjoint_interface_compute_force", "svof3d_adjoint_interface_compute_curvature_tensor",
-             "svof3d_adjoint_tension", "svof3d_set_gravity", "svof3d_adjoint_gravity"]
+             "svof3d_adjoint_tension", "svof3d_set_gravity", "svof3d_adjoint_gravity",
+             "svof3d_adjoint_set_gradient_floor"]
 
 # adjoint fields (SVOF3_ADJ_*); compact layouts: ux faces (nz, ny, nx-1), cells (nz, ny, nx)
 ADJ_FIELDS3D = {"ux": 0, "uy": 1, "uz": 2, "p": 3, "vof": 4, "psi": 5, "ifrcx": 6, "ifrcy": 7, "ifrcz": 8,
@@ -143,6 +144,7 @@ def lib3() -> ctypes.CDLL:
         L.svof3d_adjoint_tension.argtypes = [vp, pd]
         L.svof3d_set_gravity.argtypes = [vp, d, d]
         L.svof3d_adjoint_gravity.argtypes = [vp, pd]
+        L.svof3d_adjoint_set_gradient_floor.argtypes = [vp, d]
         _bound = True
     return L
 
@@ -435,6 +437,12 @@ class Solver3D:
 
     def adjoint_reset(self):
         _check(lib3().svof3d_adjoint_reset(self._h))
+
+    def adjoint_set_gradient_floor(self, tau: float):
+        """corners flatter than tau (vof variation across a cell) have no
+        normal derivative in the adjoint; 0 = exact (the FP64 default), 1e-5
+        the mixed paths' default"""
+        _check(lib3().svof3d_adjoint_set_gradient_floor(self._h, float(tau)))
 
     def adjoint_step(self, tape_ptr: int, dt: float):
         _check(lib3().svof3d_adjoint_step(self._h, ctypes.c_void_p(tape_ptr), float(dt)))

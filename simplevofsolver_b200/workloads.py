@@ -354,6 +354,29 @@ def falling_gravity(ic: InitialCondition, froude: float = FALLING2D_FROUDE,
     return -(1.0 - density_ratio) / froude ** 2, vof_ref
 
 
+# The 3D differentiation workload: the 3D generator at n^3 (stretched x) with
+# 16 droplets of radii in [0.05, 0.09], the 3D environment (Re = 500, We =
+# 20), the vof buoyancy extension with density ratio 0.05 at Fr = 1 (gravity
+# along -y), 100 steps.
+DIFF3D_DENSITY_RATIO = 0.05
+DIFF3D_FROUDE = 1.0
+
+
+def diff3d_case(n: int = 256, seed: int = 1) -> InitialCondition3D:
+    return droplets3d(n, n, n, ndrops=16, radii=(0.05, 0.09), seed=seed)
+
+
+def gravity3d(ic: InitialCondition3D, froude: float = DIFF3D_FROUDE,
+              density_ratio: float = DIFF3D_DENSITY_RATIO):
+    """(grav_vof, vof_ref) of the 3D vof buoyancy extension: gravity -1/Fr^2
+    along y on the density difference (1 - ratio) vof, relative to the
+    domain-mean volume fraction (no net force along the periodic y);
+    d grav_vof / d ratio = 1 / Fr^2"""
+    dxf = np.diff(ic.xf)
+    vof_ref = float(np.sum(ic.vof[..., 1:-1] * dxf) / (ic.lx * ic.ny * ic.nz))
+    return -(1.0 - density_ratio) / froude ** 2, vof_ref
+
+
 def physical_params(env: dict):
     """Diffusivities and surface tension as the reference derives them."""
     Ra, Pr, We = float(env["Ra"]), float(env["Pr"]), float(env["We"])

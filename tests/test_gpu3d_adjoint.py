@@ -238,14 +238,16 @@ def test_predict_field(gpu_available, rk):
         g.set_gravity(grav + sgn * dgrav, 0.2)
         run()
         vals.append({n: read(g, n) for n in seeds})
-    lhs += sum(float(np.sum(seeds[n] * (vals[0][n] - vals[1][n]) / 2.0)) for n in seeds)
+    lhs_g = sum(float(np.sum(seeds[n] * (vals[0][n] - vals[1][n]) / 2.0)) for n in seeds)
     g.set_gravity(grav, 0.2)
     st.load()
     g.adjoint_reset()
     for n, v in seeds.items():
         put_adj(g, n, v)
     g.adjoint_fluid_predict_field(rk, dt)
-    rhs = dgrav * g.adjoint_gravity()
+    rhs_g = dgrav * g.adjoint_gravity()
+    assert rel(lhs_g, rhs_g) <= 1e-9, ("gravity", lhs_g, rhs_g)
+    rhs = 0.0
     for n in ("ux", "uy", "uz", "p", "vof", "ifrcx", "ifrcy", "ifrcz"):
         rhs += float(np.sum(d[n] * get_adj(g, n)))
     if rk != 0:
@@ -342,10 +344,11 @@ def test_compute_curvature_tensor(gpu_available):
     assert rel(lhs, rhs) <= 1e-6, (lhs, rhs)
 
 
-def test_two_steps(gpu_available):
+@pytest.mark.parametrize("direction", ["velocity", "tension", "gravity"])
+def test_two_steps(gpu_available, direction):
     """two full steps (fixed dt), the vof buoyancy extension on: the
     directional derivative along a divergence-free velocity, the tension and
-    the buoyancy coefficient against the adjoint"""
+    the buoyancy coefficient, each against the adjoint"""
     import torch
     ic, phys, g = make()
     nx = g.nx
@@ -355,8 +358,10 @@ def test_two_steps(gpu_available):
     # a discretely divergence-free direction: the generator's velocity of another seed
     dirn = droplets3d(32, 16, 16, ndrops=1, radii=(0.12, 0.13), seed=11)
     d = {"ux": compact("ux", dirn.ux, nx), "uy": compact("uy", dirn.uy, nx), "uz": compact("uz", dirn.uz, nx)}
-    dten = 0.3 * phys["tension"]
-    grav, dgrav = -0.9, 0.2
+    if direction != "velocity":
+        d = {k: 0.0 * v for k, v in d.items()}
+    dten = 0.3 * phys["tension"] if direction == "tension" else 0.0
+    grav, dgrav = -0.9, (0.2 if direction == "gravity" else 0.0)
     seeds = {"ux": rng.standard_normal(fs), "uy": rng.standard_normal(cs), "uz": rng.standard_normal(cs),
              "p": rng.standard_normal(cs)}
     seeds["p"] -= seeds["p"].mean()
@@ -398,16 +403,26 @@ def test_two_steps(gpu_available):
     assert rel(lhs, rhs) <= 1e-5, (lhs, rhs)
 
 
-def test_adjoint_needs_fp64():
-    """the mixed paths have no adjoint (host check, no kernel runs)"""
-    import torch
-    if not torch.cuda.is_available():
-        pytest.skip("no CUDA device")
-    from simplevofsolver_b200 import SvofError
+def test_mixed_path_transposes_use_fp64_geometry(gpu_available):
+    """on the mixed path the adjoint computes in FP64 about FP64 geometry
+    recomputed from vof: the force transpose of the same state and seeds is
+    the FP64 path's, bit for bit"""
+    from simplevofsolver_b200 import physical_params
     ic = droplets3d(32, 16, 16, ndrops=3, radii=(0.12, 0.2), seed=3)
-    g = Solver3D(ic, physical_params(DROPLETS3D_ENV), precision="mixed")
-    with pytest.raises(SvofError, match="FP64"):
+    rng = np.random.default_rng(8)
+    seeds = {"ifrcx": rng.standard_normal((16, 16, 31)), "ifrcy": rng.standard_normal((16, 16, 32)),
+             "ifrcz": rng.standard_normal((16, 16, 32))}
+    out = []
+    for prec in ("fp64", "mixed"):
+        g = Solver3D(ic, physical_params(DROPLETS3D_ENV), precision=prec)
+        g.interface_compute_curvature_tensor()
         g.adjoint_reset()
+        for n, v in seeds.items():
+            put_adj(g, n, v)
+        g.adjoint_interface_compute_force()
+        out.append((get_adj(g, "vof"), get_adj(g, "curv"), g.adjoint_tension()))
+    for a_, b_ in zip(out[0], out[1]):
+        assert np.array_equal(a_, b_)
 
 
 def test_rollout3d_gradient_and_checkpoints(gpu_available):
