@@ -481,6 +481,35 @@ def adjoint_cost3d(n: int = 256, steps: int = 100, budget: float = 60e9, precisi
     return out
 
 
+def adjoint3d_profile_run(n: int, steps: int = 2):
+    """the launches of the 3D differentiation form for a launch list: the
+    differentiation workload at n^3 (FP64, vof buoyancy on), `steps` taped
+    steps (svof3d_integrate_fixed) and their step adjoints
+    (svof3d_adjoint_step) in reverse, seeded by the interface-area objective"""
+    import torch
+    from simplevofsolver_b200.adjoint import interface_area3d
+    from simplevofsolver_b200.solver3d import Solver3D
+    from simplevofsolver_b200.workloads import DROPLETS3D_ENV, diff3d_case, gravity3d, physical_params
+    ic = diff3d_case(n)
+    s = Solver3D(ic, physical_params(DROPLETS3D_ENV))
+    s.set_gravity(*gravity3d(ic))
+    dt = s.fluid_decide_dt()
+    tapes = [torch.empty(s.tape_count(), dtype=torch.float64, device="cuda") for _ in range(steps)]
+    for t in tapes:
+        s.integrate_fixed(dt, t.data_ptr())
+    s.synchronize()
+    vof = s.device_view("vof")[2:n + 2, 2:n + 2, 1:n + 1].clone().requires_grad_(True)
+    interface_area3d(vof, ic.xf, ic.ly, ic.lz).backward()
+    s.adjoint_reset()
+    s.synchronize()
+    s.adjoint_view("vof").copy_(vof.grad)
+    torch.cuda.synchronize()
+    for t in reversed(tapes):
+        s.adjoint_step(t.data_ptr(), dt)
+    s.synchronize()
+    s.close()
+
+
 def _profile(solver, nprof):
     """per-kernel-kind device time of `nprof` steps launched kernel by kernel;
     a long memset ahead lets the host enqueue the whole step first"""
@@ -713,7 +742,13 @@ def main():
     ap.add_argument("--no-dc", action="store_true",
                     help="skip the defect-corrected mixed form (FP32 Poisson passes) in the 3D workloads")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--adjoint3d-profile", type=int, default=0, metavar="N",
+                    help="profiling mode: two taped FP64 steps and their step adjoints of the 3D "
+                         "differentiation workload at N^3, then exit (no JSON line)")
     args = ap.parse_args()
+    if args.adjoint3d_profile:
+        adjoint3d_profile_run(args.adjoint3d_profile)
+        return
     three_d = args.workload in WORKLOADS3D
     if args.steps is None:
         args.steps = 20 if three_d else 200
