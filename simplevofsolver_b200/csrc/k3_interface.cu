@@ -667,7 +667,10 @@ __global__ void __launch_bounds__(AX * AY, 4) k3_vof_advect(const double *__rest
       }
     }
     fz_lo = fz_hi;
-    __pipeline_wait_prior(1);  // plane k + 2
+    // plane k + 2 (issued at the top of this iteration) complete: the next
+    // iteration reads it as its upper plane sp (the z-face flux above each
+    // cell); waiting for all but the newest group would leave it in flight
+    __pipeline_wait_prior(0);
     __syncthreads();
   }
 #undef VR
