@@ -48,3 +48,21 @@ def test_steps_repeat_bit_for_bit(gpu_available, precision, steps):
     a, b = _hashes(precision, 128, steps)
     first = next((n for n, (x, y) in enumerate(zip(a, b)) if x != y), None)
     assert first is None, f"{precision}: the runs differ from step {first}"
+
+
+def test_2d_steps_repeat_bit_for_bit(gpu_available):
+    """the 2D path (its line-streaming predictor keeps a per-warp cp.async
+    ring): 30 steps at 1024^2, twice, the same fields bit for bit"""
+    from simplevofsolver_b200 import DROPLET2D_ENV, Solver, droplet2d, physical_params
+    ic = droplet2d(1024, 1024, uniform=True)
+    phys = physical_params(DROPLET2D_ENV)
+    runs = []
+    for _ in range(2):
+        s = Solver(ic, phys)
+        dts = s.run(30)
+        h = hashlib.sha1(np.asarray(dts).tobytes())
+        for k in ("ux", "uy", "p", "vof", "src_a", "srcuy_a"):
+            h.update(np.ascontiguousarray(s.field(k)).tobytes())
+        runs.append(h.hexdigest())
+        s.close()
+    assert runs[0] == runs[1]
