@@ -58,7 +58,7 @@ struct Adj3RhsArgs {
   double *avof, *agrv;
   AGrid3 ag;
 };
-__global__ void k3_adj_rhs(Adj3RhsArgs a);
+__global__ void __launch_bounds__(256, 3) k3_adj_rhs(Adj3RhsArgs a);
 
 struct Adj3IfaceArgs {
   const double *ux, *uy, *uz, *vof, *normal, *curv;  // primal, storage layouts
@@ -74,7 +74,7 @@ struct Adj3IfaceArgs {
   int mode;
   AGrid3 ag;
 };
-__global__ void k3_adj_interface(Adj3IfaceArgs a);
+__global__ void __launch_bounds__(256, 4) k3_adj_interface(Adj3IfaceArgs a);
 
 // corner gradients' adjoints ([3] per corner, (nx + 1) ny nz corners)
 __global__ void k3_adj_cgrad(const double *__restrict__ vof, const double *__restrict__ am,

@@ -287,7 +287,9 @@ __global__ void __launch_bounds__(kAdjXLines) k3_adj_xsolve(
 // Neighbours are addressed by offsets (di, dj, dk) from the cell: compact
 // arrays with periodic wraps (Wrap3), primal storage arrays through their
 // halos.
-__global__ void k3_adj_rhs(Adj3RhsArgs a) {
+// (80 registers, no spill: three blocks of 256 threads per SM; the kernel
+// is bound by memory latency, so resident warps set its speed)
+__global__ void __launch_bounds__(256, 3) k3_adj_rhs(Adj3RhsArgs a) {
   int i, j, k;
   const AGrid3 &ag = a.ag;
   const Grid3 &g = ag.g;
@@ -465,7 +467,8 @@ __global__ void k3_adj_rhs(Adj3RhsArgs a) {
 //    vof_bar(c) and the adjoint m_bar of the unnormalised mean normal.
 // With mode & 1 but not & 4, n_bar goes to anrm; with & 4 but not & 1 it is
 // read from there.
-__global__ void k3_adj_interface(Adj3IfaceArgs a) {
+// (64 registers, no spill: four blocks of 256 threads per SM)
+__global__ void __launch_bounds__(256, 4) k3_adj_interface(Adj3IfaceArgs a) {
   int i, j, k;
   const AGrid3 &ag = a.ag;
   const Grid3 &g = ag.g;
