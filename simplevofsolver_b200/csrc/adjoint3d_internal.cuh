@@ -41,7 +41,7 @@ __global__ void k3_adj_xsolve(const double *__restrict__ aux, const double *__re
                               double *__restrict__ pend_x, double *__restrict__ pend_y, double *__restrict__ pend_z,
                               double adt, double bdt, double gdt, Grid3 g);
 inline size_t adj_xsolve_smem(int nx) {
-  return sizeof(double) * (3 * (size_t)nx + (size_t)kAdjXLines * (kAdjXChunk + 1));
+  return sizeof(double) * (3 * (size_t)nx + 2 * (size_t)kAdjXLines * (kAdjXChunk + 1));
 }
 
 struct Adj3RhsArgs {

@@ -30,6 +30,8 @@
 // thread owns its outputs): no atomics, results independent of scheduling.
 // Spacings enter as reciprocals (AGrid3): no divisions but the normalisations'.
 // The temperature is not differentiated (the adjoint needs add_buoyancy = 0).
+#include <cuda_pipeline.h>
+
 #include "adjoint3d_internal.cuh"
 
 namespace svof3 {
@@ -188,17 +190,17 @@ __global__ void k3_adj_div(double *__restrict__ aux, double *__restrict__ auy, d
 // src_g_bar = g dt delta_bar, pend = b dt delta_bar.
 // A block owns kAdjXLines consecutive lines (j, k) of one field (blockIdx.y),
 // one per thread, the recurrences carried in registers; the lines (rows of
-// the compact arrays, contiguous) pass through a shared tile kAdjXChunk
-// points at a time, loaded and stored in runs of consecutive points.  The
-// forward sweep leaves z in src_g_bar, which the backward sweep reads and
-// overwrites.
+// the compact arrays, contiguous) pass through two shared tiles kAdjXChunk
+// points at a time: cp.async brings chunk c + 1 (runs of consecutive points)
+// while chunk c is swept.  The forward sweep leaves z in src_g_bar, which the
+// backward sweep reads and overwrites.
 __global__ void __launch_bounds__(kAdjXLines) k3_adj_xsolve(
     const double *__restrict__ aux, const double *__restrict__ auy, const double *__restrict__ auz,
     const double *__restrict__ coef, double *__restrict__ sa_x, double *__restrict__ sg_x, double *__restrict__ sa_y,
     double *__restrict__ sg_y, double *__restrict__ sa_z, double *__restrict__ sg_z, double *__restrict__ pend_x,
     double *__restrict__ pend_y, double *__restrict__ pend_z, double adt, double bdt, double gdt, Grid3 g) {
   extern __shared__ double smx[];
-  constexpr int NL = kAdjXLines, XC = kAdjXChunk, LD = kAdjXChunk + 1;
+  constexpr int NL = kAdjXLines, XC = kAdjXChunk, LD = kAdjXChunk + 1, PER = NL * XC / kAdjXLines;
   const int nx = g.nx;
   const int f = blockIdx.y;  // 0 ux, 1 uy, 2 uz
   const int n = (0 == f) ? nx - 1 : nx;
@@ -207,65 +209,98 @@ __global__ void __launch_bounds__(kAdjXLines) k3_adj_xsolve(
   double *sg = (0 == f) ? sg_x : (1 == f ? sg_y : sg_z);
   double *pend = (0 == f) ? pend_x : (1 == f ? pend_y : pend_z);
   const int set = (0 == f) ? 0 : 1;
-  double *sL = smx, *sR = smx + nx, *sV = smx + 2 * nx, *tile = smx + 3 * nx;
+  double *sL = smx, *sR = smx + nx, *sV = smx + 2 * nx;
+  double *tiles = smx + 3 * nx;  // [2][NL][LD]
   for (int w = threadIdx.x; w < 3 * nx; w += NL) smx[w] = coef[(size_t)3 * set * nx + w];
   const long nlines = (long)g.ny * g.nz;
   const long l0 = (long)blockIdx.x * NL;
   const int nr = (int)min((long)NL, nlines - l0);
   const int t = threadIdx.x;
   const size_t base = (size_t)l0 * n;  // row l at base + (l - l0) n
-  __syncthreads();
+  const int nch = (n + XC - 1) / XC;
+  // element m of a thread's share of a chunk: row w / XC, point w % XC
+  auto fetch = [&](const double *from, int c, int buf) {
+    const int c0 = c * XC, cw = min(XC, n - c0);
+    double *tl = tiles + (size_t)buf * NL * LD;
+#pragma unroll
+    for (int m = 0; m < PER; m++) {
+      const int w = t + NL * m, r = w / XC, q = w - r * XC;
+      if (r < nr && q < cw) __pipeline_memcpy_async(tl + r * LD + q, from + base + (size_t)r * n + c0 + q, 8);
+    }
+    __pipeline_commit();
+  };
   // forward sweep
   double z = 0.;
-  for (int c0 = 0; c0 < n; c0 += XC) {
-    const int cw = min(XC, n - c0);
-    for (int w = t; w < nr * XC; w += NL) {
-      const int r = w / XC, q = w - r * XC;
-      if (q < cw) tile[r * LD + q] = src[base + (size_t)r * n + c0 + q];
+  fetch(src, 0, 0);
+  __syncthreads();  // (the coefficients)
+  for (int c = 0; c < nch; c++) {
+    const int c0 = c * XC, cw = min(XC, n - c0), buf = c & 1;
+    double *tl = tiles + (size_t)buf * NL * LD;
+    if (c + 1 < nch) {
+      fetch(src, c + 1, buf ^ 1);
+      __pipeline_wait_prior(1);
+    } else {
+      __pipeline_wait_prior(0);
     }
     __syncthreads();
     if (t < nr) {
       for (int q = 0; q < cw; q++) {
         const int p = c0 + q;
-        const double b = tile[t * LD + q];
+        const double b = tl[t * LD + q];
         z = (0 == p) ? b : b - sV[p - 1] * z;
-        tile[t * LD + q] = z;
+        tl[t * LD + q] = z;
       }
     }
     __syncthreads();
-    for (int w = t; w < nr * XC; w += NL) {
-      const int r = w / XC, q = w - r * XC;
-      if (q < cw) sg[base + (size_t)r * n + c0 + q] = tile[r * LD + q];
+#pragma unroll
+    for (int m = 0; m < PER; m++) {
+      const int w = t + NL * m, r = w / XC, q = w - r * XC;
+      if (r < nr && q < cw) sg[base + (size_t)r * n + c0 + q] = tl[r * LD + q];
     }
-    __syncthreads();
+    __syncthreads();  // the tile is refilled two chunks on
   }
+  // the forward sweep's stores are read back by this block's copies
+  __threadfence_block();
+  __syncthreads();
   // backward sweep, chunks in reverse
   double y = 0.;
   const double rd0 = 1. / sR[0];
-  for (int c0 = ((n - 1) / XC) * XC; c0 >= 0; c0 -= XC) {
-    const int cw = min(XC, n - c0);
-    for (int w = t; w < nr * XC; w += NL) {
-      const int r = w / XC, q = w - r * XC;
-      if (q < cw) tile[r * LD + q] = sg[base + (size_t)r * n + c0 + q];
+  fetch(sg, nch - 1, 0);
+  for (int it = 0; it < nch; it++) {
+    const int c = nch - 1 - it, c0 = c * XC, cw = min(XC, n - c0), buf = it & 1;
+    double *tl = tiles + (size_t)buf * NL * LD;
+    if (c - 1 >= 0) {
+      fetch(sg, c - 1, buf ^ 1);
+      __pipeline_wait_prior(1);
+    } else {
+      __pipeline_wait_prior(0);
     }
     __syncthreads();
     if (t < nr) {
       for (int q = cw - 1; q >= 0; q--) {
         const int p = c0 + q;
-        const double zz = tile[t * LD + q];
+        const double zz = tl[t * LD + q];
         if (p == n - 1) y = zz * sR[n - 1];
         else if (p > 0) y = sR[p] * (zz - sL[p + 1] * y);
         else y = (zz - sL[1] * y) * rd0;
-        tile[t * LD + q] = y;
+        tl[t * LD + q] = y;
       }
     }
     __syncthreads();
-    for (int w = t; w < nr * XC; w += NL) {
-      const int r = w / XC, q = w - r * XC;
-      if (q < cw) {
+    // the RK split: the pending terms' loads issued together, then the stores
+    double pv[PER];
+#pragma unroll
+    for (int m = 0; m < PER; m++) {
+      const int w = t + NL * m, r = w / XC, q = w - r * XC;
+      pv[m] = (r < nr && q < cw) ? pend[base + (size_t)r * n + c0 + q] : 0.;
+    }
+#pragma unroll
+    for (int m = 0; m < PER; m++) {
+      const int w = t + NL * m, r = w / XC, q = w - r * XC;
+      if (r < nr && q < cw) {
         const size_t o = base + (size_t)r * n + c0 + q;
-        const double d = tile[r * LD + q];
-        sa[o] = adt * d + pend[o];
+        const double d = tl[r * LD + q];
+        sa[o] = adt * d + pv[m];
         sg[o] = gdt * d;
         pend[o] = bdt * d;
       }
