@@ -449,6 +449,122 @@ __global__ void __launch_bounds__(kLineThreads, Line<R, L2N>::MINB)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Packed y transforms (the mixed path's single FP64 pass; not the FP64
+// path's, whose transforms follow the restatement's rounding): two adjacent
+// columns i, i + 1 travel as the real and imaginary parts of one complex
+// line, so each transform carries two real lines instead of one real line
+// with a zero imaginary part, and a block covers 2 COLS columns.
+// Forward: Z = FFT(b_i + i b_{i+1}), then X_p = (Z_p + conj Z_{N-p}) / 2 and
+// Y_p = (Z_p - conj Z_{N-p}) / 2i for p <= N/2 (a pass through shared memory
+// after the last stage).  Inverse: Z_m = X_m + i Y_m from the two half
+// spectra (conjugates above N/2, Im of X_0, X_{N/2} and Y_0, Y_{N/2} dropped
+// as the c2r transform drops them), then Re -> psi_i, Im -> psi_{i+1}.
+template <int L2N>
+__global__ void __launch_bounds__(kLineThreads, Line<double, L2N>::MINB)
+    k3_pois_fwd_y_pk(const double *__restrict__ b, double *__restrict__ spec, const double *__restrict__ tw,
+                     Grid3 g) {
+  using L = Line<double, L2N>;
+  using C2 = typename Cplx<double>::T;
+  constexpr int N = L::N, COLS = L::COLS, NKY = N / 2 + 1, LD = L::LD;
+  extern __shared__ unsigned char smraw[];
+  double *re = reinterpret_cast<double *>(smraw);
+  double *im = re + COLS * LD;
+  const int nx = g.nx;
+  const int i0 = 1 + blockIdx.x * 2 * COLS;  // columns i0 .. i0 + 2 COLS - 1
+  const int k = 1 + blockIdx.y;
+  const int ncol = min(2 * COLS, nx - i0 + 1);
+  const double *bp = b + (size_t)nx * N * (k - 1) + (i0 - 1);
+  C2 *out = reinterpret_cast<C2 *>(spec) + (size_t)(k - 1) * NKY * nx + (i0 - 1);
+  auto first = [&](int c, int base, auto gc, auto hc, double *xr, double *xi) {
+    constexpr int G = decltype(gc)::value, H = decltype(hc)::value;
+#pragma unroll
+    for (int m = 0; m < G; m++) {
+      const size_t row = (size_t)nx * bitrev(base + m * H, L2N);
+      xr[m] = (2 * c < ncol) ? ldg(bp + row + 2 * c) : 0.;
+      xi[m] = (2 * c + 1 < ncol) ? ldg(bp + row + 2 * c + 1) : 0.;
+    }
+  };
+  auto last = [&](int c, int base, auto gc, auto hc, const double *xr, const double *xi) {
+    constexpr int G = decltype(gc)::value, H = decltype(hc)::value;
+#pragma unroll
+    for (int m = 0; m < G; m++) {
+      re[c * LD + svof_fft_dev::fpad(base + m * H)] = xr[m];
+      im[c * LD + svof_fft_dev::fpad(base + m * H)] = xi[m];
+    }
+  };
+  svof_fft_dev::fft_lines<double, L2N, COLS>(re, im, tw, first, last);
+  __syncthreads();
+  // split: (p, column pair c) with c fastest, two adjacent outputs per thread
+  for (int w = threadIdx.x; w < NKY * COLS; w += kLineThreads) {
+    const int c = w % COLS, p = w / COLS;
+    if (2 * c >= ncol) continue;
+    const int q = (N - p) & (N - 1);
+    const double a = re[c * LD + svof_fft_dev::fpad(p)], bb = im[c * LD + svof_fft_dev::fpad(p)];
+    const double cr = re[c * LD + svof_fft_dev::fpad(q)], d = im[c * LD + svof_fft_dev::fpad(q)];
+    out[(size_t)p * nx + 2 * c] = Cplx<double>::make(0.5 * (a + cr), 0.5 * (bb - d));
+    if (2 * c + 1 < ncol) out[(size_t)p * nx + 2 * c + 1] = Cplx<double>::make(0.5 * (bb + d), -0.5 * (a - cr));
+  }
+}
+
+template <int L2N>
+__global__ void __launch_bounds__(kLineThreads, Line<double, L2N>::MINB)
+    k3_pois_inv_y_pk(const double *__restrict__ spec, double *__restrict__ psi, const double *__restrict__ tw,
+                     Grid3 g) {
+  using L = Line<double, L2N>;
+  using C2 = typename Cplx<double>::T;
+  constexpr int N = L::N, COLS = L::COLS, NKY = N / 2 + 1;
+  extern __shared__ unsigned char smraw[];
+  double *re = reinterpret_cast<double *>(smraw);
+  double *im = re + COLS * L::LD;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int i0 = 1 + blockIdx.x * 2 * COLS;
+  const int k = 1 + blockIdx.y;
+  const int ncol = min(2 * COLS, nx - i0 + 1);
+  const C2 *sp = reinterpret_cast<const C2 *>(spec) + (size_t)(k - 1) * NKY * nx + (i0 - 1);
+  auto first = [&](int c, int base, auto gc, auto hc, double *xr, double *xi) {
+    constexpr int G = decltype(gc)::value, H = decltype(hc)::value;
+#pragma unroll
+    for (int q = 0; q < G; q++) {
+      const int m = bitrev(base + q * H, L2N);
+      const int row = (2 * m <= N) ? m : N - m;
+      const bool edge = (0 == m || 2 * m == N);
+      const double sgn = (2 * m < N) ? 1. : -1.;
+      C2 x = Cplx<double>::make(0., 0.), y = Cplx<double>::make(0., 0.);
+      if (2 * c < ncol) x = __ldg(&sp[(size_t)row * nx + 2 * c]);
+      if (2 * c + 1 < ncol) y = __ldg(&sp[(size_t)row * nx + 2 * c + 1]);
+      const double xi_ = edge ? 0. : sgn * x.y, yi_ = edge ? 0. : sgn * y.y;
+      xr[q] = x.x - yi_;  // Re (X + i Y)
+      xi[q] = xi_ + y.x;  // Im (X + i Y)
+    }
+  };
+  auto last = [&](int c, int base, auto gc, auto hc, const double *xr, const double *xi) {
+    constexpr int G = decltype(gc)::value, H = decltype(hc)::value;
+#pragma unroll
+    for (int q = 0; q < G; q++) {
+      const double ve = xr[q], vo = xi[q];
+      for_images(base + q * H + 1, k, ny, nz, true, [&](int jj, int kk) {
+        if (2 * c < ncol) psi[ix_cc(g, i0 + 2 * c, jj, kk)] = ve;
+        if (2 * c + 1 < ncol) psi[ix_cc(g, i0 + 2 * c + 1, jj, kk)] = vo;
+      });
+    }
+  };
+  svof_fft_dev::fft_lines<double, L2N, COLS>(re, im, tw, first, last);
+  // Neumann walls, as k3_pois_inv_y
+  const bool has_left = (1 == i0), has_right = (i0 + ncol - 1 == nx);
+  if (!has_left && !has_right) return;
+  __syncthreads();
+  for (int w = threadIdx.x; w < 2 * N; w += kLineThreads) {
+    const int side = w / N, j = 1 + (w - side * N);
+    if ((0 == side && !has_left) || (1 == side && !has_right)) continue;
+    const int iw = side ? nx + 1 : 0;
+    const double nv = psi[ix_cc(g, side ? nx : 1, j, k)];
+    const double old = psi[ix_cc(g, iw, j, k)];
+    psi[ix_cc(g, iw, j, k)] = nv;
+    for_images(j, k, ny, nz, false, [&](int jj, int kk) { psi[ix_cc(g, iw, jj, kk)] = old; });
+  }
+}
+
 // ---- host-side launchers (the templates stay in this translation unit)
 namespace {
 constexpr int kMinL2N = 1, kMaxL2N = 11;
@@ -486,6 +602,10 @@ cudaError_t pois_prepare(int log2ny, int log2nz) {
     cudaError_t r;
     if (cudaSuccess != (r = line_attrs(k3_pois_fwd_y<L2, R>, sm))) return r;
     if (cudaSuccess != (r = line_attrs(k3_pois_inv_y<L2, R, true>, sm))) return r;
+    if constexpr (std::is_same<R, double>::value) {
+      if (cudaSuccess != (r = line_attrs(k3_pois_fwd_y_pk<L2>, sm))) return r;
+      if (cudaSuccess != (r = line_attrs(k3_pois_inv_y_pk<L2>, sm))) return r;
+    }
     return line_attrs(k3_pois_inv_y<L2, R, false>, sm);
   });
   if (cudaSuccess != e) return e;
@@ -562,6 +682,32 @@ cudaError_t pois_fwd_y_array(cudaStream_t st, const double *b, R *spec, const R 
     using L = Line<R, L2>;
     dim3 gr((g.nx + L::COLS - 1) / L::COLS, g.nz);
     k3_pois_fwd_y<L2, R><<<gr, kLineThreads, L::SMEM, st>>>(b, spec, tw, g);
+    return cudaGetLastError();
+  });
+}
+
+cudaError_t pois_fwd_y_packed(cudaStream_t st, const double *ux, const double *uy, const double *uz, double *b,
+                              double *spec, const double *tw, const double *dtp, double gam, int log2n, Grid3 g) {
+  const dim3 bb(32, 8), bg((g.nx + 31) / 32, (g.ny + 7) / 8, (g.nz + kBPlanes - 1) / kBPlanes);
+  k3_pois_b<<<bg, bb, 0, st>>>(ux, uy, uz, b, dtp, gam, g);
+  cudaError_t e = cudaGetLastError();
+  if (cudaSuccess != e) return e;
+  return by_l2n(log2n, [&](auto c) {
+    constexpr int L2 = decltype(c)::value;
+    using L = Line<double, L2>;
+    dim3 gr((g.nx + 2 * L::COLS - 1) / (2 * L::COLS), g.nz);
+    k3_pois_fwd_y_pk<L2><<<gr, kLineThreads, L::SMEM, st>>>(b, spec, tw, g);
+    return cudaGetLastError();
+  });
+}
+
+cudaError_t pois_inv_y_packed(cudaStream_t st, const double *spec, double *psi, const double *tw, int log2n,
+                              Grid3 g) {
+  return by_l2n(log2n, [&](auto c) {
+    constexpr int L2 = decltype(c)::value;
+    using L = Line<double, L2>;
+    dim3 gr((g.nx + 2 * L::COLS - 1) / (2 * L::COLS), g.nz);
+    k3_pois_inv_y_pk<L2><<<gr, kLineThreads, L::SMEM, st>>>(spec, psi, tw, g);
     return cudaGetLastError();
   });
 }

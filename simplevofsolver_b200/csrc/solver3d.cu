@@ -340,9 +340,16 @@ int launch_potential(svof3d_solver *s, int rk, const Marker &mark = Marker()) {
   auto m = [&](int kind) { return mark ? mark(kind) : 0; };
   const int cu = s->cur_u;
   // (the right-hand side goes through the predictor's line scratch, idle
-  // here: 4 nx ny nz elements of 4 or 8 bytes)
-  CK(pois_fwd_y<double>(s->stream, s->ux[cu].p, s->uy[cu].p, s->uz[cu].p, s->fw.as<double>(), s->spec.p,
-                        s->twf_y.p, s->d_dt, gam, s->log2ny, g));
+  // here: 4 nx ny nz elements of 4 or 8 bytes).  The mixed path's y
+  // transforms carry two columns per complex line; the FP64 path's follow
+  // the restatement's rounding with one real line per transform.
+  if (s->mixed) {
+    CK(pois_fwd_y_packed(s->stream, s->ux[cu].p, s->uy[cu].p, s->uz[cu].p, s->fw.as<double>(), s->spec.p,
+                         s->twf_y.p, s->d_dt, gam, s->log2ny, g));
+  } else {
+    CK(pois_fwd_y<double>(s->stream, s->ux[cu].p, s->uy[cu].p, s->uz[cu].p, s->fw.as<double>(), s->spec.p,
+                          s->twf_y.p, s->d_dt, gam, s->log2ny, g));
+  }
   if (m(SVOF3_K_POISSON_FWD)) return 1;
   CK(pois_z<double>(s->stream, s->spec.p, s->twf_z.p, s->log2nz, g));
   if (m(SVOF3_K_POISSON_Z)) return 1;
@@ -350,7 +357,8 @@ int launch_potential(svof3d_solver *s, int rk, const Marker &mark = Marker()) {
   if (m(SVOF3_K_POISSON_SOLVE)) return 1;
   CK(pois_z<double>(s->stream, s->spec.p, s->twb_z.p, s->log2nz, g));
   if (m(SVOF3_K_POISSON_Z)) return 1;
-  CK(pois_inv_y<double>(s->stream, s->spec.p, s->psi.p, s->twb_y.p, s->log2ny, g));
+  if (s->mixed) CK(pois_inv_y_packed(s->stream, s->spec.p, s->psi.p, s->twb_y.p, s->log2ny, g));
+  else CK(pois_inv_y<double>(s->stream, s->spec.p, s->psi.p, s->twb_y.p, s->log2ny, g));
   if (m(SVOF3_K_POISSON_INV)) return 1;
   return 0;
 }

@@ -173,6 +173,12 @@ cudaError_t pois_inv_y(cudaStream_t st, const R *spec, double *psi, const R *tw,
 template <class R>
 cudaError_t pois_fwd_y_array(cudaStream_t st, const double *b, R *spec, const R *tw, int log2n, Grid3 g);
 // r = b - L psi / (ny nz), compact arrays of nx ny nz doubles (FP64)
+// the mixed path's y transforms with two columns packed into one complex
+// line (FP64; the right-hand side as pois_fwd_y; a block covers 2 COLS columns)
+cudaError_t pois_fwd_y_packed(cudaStream_t st, const double *ux, const double *uy, const double *uz, double *b,
+                              double *spec, const double *tw, const double *dtp, double gam, int log2n, Grid3 g);
+cudaError_t pois_inv_y_packed(cudaStream_t st, const double *spec, double *psi, const double *tw, int log2n,
+                              Grid3 g);
 cudaError_t pois_resid(cudaStream_t st, const double *b, const double *psi, double *r, const double *pl,
                        const double *pu, Grid3 g);
 

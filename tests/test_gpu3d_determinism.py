@@ -50,11 +50,13 @@ def test_steps_repeat_bit_for_bit(gpu_available, precision, steps):
     assert first is None, f"{precision}: the runs differ from step {first}"
 
 
-def test_2d_steps_repeat_bit_for_bit(gpu_available):
+@pytest.mark.parametrize("uniform", [True, False])
+def test_2d_steps_repeat_bit_for_bit(gpu_available, uniform):
     """the 2D path (its line-streaming predictor keeps a per-warp cp.async
-    ring): 30 steps at 1024^2, twice, the same fields bit for bit"""
+    ring; uniform x takes the DCT Poisson path, stretched x the DFT one): 30
+    steps at 1024^2, twice, the same fields bit for bit"""
     from simplevofsolver_b200 import DROPLET2D_ENV, Solver, droplet2d, physical_params
-    ic = droplet2d(1024, 1024, uniform=True)
+    ic = droplet2d(1024, 1024, uniform=uniform)
     phys = physical_params(DROPLET2D_ENV)
     runs = []
     for _ in range(2):

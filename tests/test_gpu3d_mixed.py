@@ -124,3 +124,30 @@ def test_defect_correction_reduces_the_residual(gpu_available):
     psi_f = psi_f - psi_f.mean()
     e = rel_l2(psi_dc, psi_f)
     assert e <= 1e-9, e
+
+
+@pytest.mark.parametrize("shape", [(32, 16, 16), (33, 8, 16), (40, 64, 32)])
+def test_packed_y_transforms_match_the_fp64_solve(gpu_available, shape):
+    """the mixed path's Poisson solve carries two columns per complex y
+    transform (real and imaginary parts); from the same velocities its psi
+    equals the FP64 path's (one real line per transform, the restatement's
+    rounding) to round-off, modulo the solve's gauge constant; odd nx (a last
+    block with one column) and an 8-point single-pass transform included"""
+    from simplevofsolver_b200 import DROPLETS3D_ENV, Solver3D, droplets3d, physical_params
+    nx, ny, nz = shape
+    ic = droplets3d(nx, ny, nz, ndrops=2, radii=(0.1, 0.15), seed=4)
+    phys = physical_params(DROPLETS3D_ENV)
+    out = {}
+    for prec in ("fp64", "mixed"):
+        s = Solver3D(ic, phys, precision=prec)
+        rng = np.random.default_rng(9)
+        # a velocity with divergence, so that psi is far from zero
+        s.load_interior("ux", ic.ux + 0.1 * rng.standard_normal(ic.ux.shape))
+        s.load_interior("uy", ic.uy + 0.1 * rng.standard_normal(ic.uy.shape))
+        s.fluid_compute_potential_dft(1, 1.3e-3)
+        psi = s.field("psi")[1:-1, 1:-1, :]
+        out[prec] = psi - psi[:, :, 1:-1].mean()
+        s.close()
+    scale = np.abs(out["fp64"]).max()
+    assert scale > 1e-6
+    assert np.abs(out["mixed"] - out["fp64"]).max() <= 1e-12 * scale
