@@ -64,7 +64,8 @@ typedef struct {
  *                predictor's sweep scratch are FP32; interface geometry and
  *                THINC compute in FP32; the momentum stencils, the x line
  *                solves, the vof update and the whole Poisson solve (the
- *                FP64 path's kernels, one pass) in FP64.  Fields stored in
+ *                FP64 path's kernels, one pass, its y transforms carrying
+ *                two columns per complex line) in FP64.  Fields stored in
  *                FP32 are converted to FP64 by svof3d_download_field / from
  *                FP64 by svof3d_upload_field.
  *   SVOF3_MIXED_DC as SVOF3_MIXED, with the Poisson solve in the form of a
