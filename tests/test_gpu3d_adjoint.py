@@ -473,3 +473,37 @@ def test_rollout3d_gradient_and_checkpoints(gpu_available):
         _, gk = grads(K)
         for n in gr:
             assert torch.equal(gk[n], gr[n]), (K, n)
+
+
+def test_defect_corrected_path_adjoint(gpu_available):
+    """the adjoint on the defect-corrected precision (its forward's Poisson
+    passes FP32; the adjoint's second solve FP64): two taped steps, the
+    directional derivative along a divergence-free velocity equals the mixed
+    path's within their trajectories' difference; a negative gradient floor
+    is refused"""
+    import torch
+    from simplevofsolver_b200 import SvofError, physical_params
+    ic = droplets3d(32, 16, 16, ndrops=3, radii=(0.12, 0.2), seed=3)
+    phys = physical_params(DROPLETS3D_ENV)
+    dirn = droplets3d(32, 16, 16, ndrops=1, radii=(0.12, 0.13), seed=11)
+    d = {n: compact(n, getattr(dirn, n), 32) for n in ("ux", "uy", "uz")}
+    dd = {}
+    for prec in ("mixed", "mixed_dc"):
+        g = Solver3D(ic, phys, precision=prec)
+        dt = 1.0e-3
+        tapes = [torch.empty(g.tape_count(), dtype=torch.float64, device="cuda") for _ in range(2)]
+        for t in tapes:
+            g.integrate_fixed(dt, t.data_ptr())
+        g.synchronize()
+        g.adjoint_reset()
+        rng = np.random.default_rng(12)
+        put_adj(g, "ux", rng.standard_normal((16, 16, 31)))
+        put_adj(g, "uy", rng.standard_normal((16, 16, 32)))
+        for t in reversed(tapes):
+            g.adjoint_step(t.data_ptr(), dt)
+        dd[prec] = sum(float(np.sum(d[n] * get_adj(g, n))) for n in d)
+        with pytest.raises(SvofError, match="non-negative"):
+            g.adjoint_set_gradient_floor(-1.0)
+        g.close()
+    assert np.isfinite(dd["mixed_dc"])
+    assert rel(dd["mixed"], dd["mixed_dc"]) <= 1e-4, dd
