@@ -346,6 +346,19 @@ int svof_synchronize(svof_solver_t *solver);
 int svof_stream(svof_solver_t *solver, void **stream);
 const char *svof_last_error(void);
 
+/* Guard zones (a debugging aid in place of a memory checker).  With
+ * SVOF_GUARD_BYTES=N in the environment when the solvers allocate (N > 0,
+ * rounded up to a multiple of 256), every device buffer of the 2D and 3D
+ * solvers gets N bytes before and after it, filled with a canary byte.
+ * svof_guard_bytes() returns the band in effect (0: off, the default).
+ * svof_guard_check() waits for the device, scans every live guard zone of
+ * the process and returns 0 when all are intact; otherwise non-zero, with
+ * the number of changed bytes in *bad_bytes (may be NULL) and the first
+ * changed zone named in svof_last_error().  Writes outside a buffer are
+ * detected; reads are not. */
+size_t svof_guard_bytes(void);
+int svof_guard_check(size_t *bad_bytes);
+
 #ifdef __cplusplus
 }
 #endif

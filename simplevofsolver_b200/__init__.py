@@ -63,7 +63,8 @@ EXPORTS = ["svof_create", "svof_destroy", "svof_field_count", "svof_upload_field
            "svof_adjoint_fluid_correct_velocity", "svof_adjoint_fluid_compute_potential",
            "svof_adjoint_fluid_predict_field", "svof_adjoint_interface_update_vof",
            "svof_adjoint_interface_compute_force", "svof_adjoint_interface_compute_curvature_tensor",
-           "svof_adjoint_tension", "svof_adjoint_gravity", "svof_poisson_dct_noalloc"]
+           "svof_adjoint_tension", "svof_adjoint_gravity", "svof_poisson_dct_noalloc",
+           "svof_guard_bytes", "svof_guard_check"]
 
 # adjoint fields (SVOF_ADJ_*); compact layouts: ux faces (ny, nx-1), cells (ny, nx)
 ADJ_FIELDS = {"ux": 0, "uy": 1, "p": 2, "vof": 3, "psi": 4, "ifrcx": 5, "ifrcy": 6, "curv": 7, "normal": 8,
@@ -151,6 +152,9 @@ def lib() -> ctypes.CDLL:
         L.svof_statistics_reduce.argtypes = [vp, i, dp, sz]
         L.svof_statistics_field.argtypes = [vp, i, dp, sz]
         L.svof_poisson_dct_noalloc.argtypes = [ctypes.POINTER(Params), dp, dp, dp, dp, sz, d, vp]
+        L.svof_guard_bytes.argtypes = []
+        L.svof_guard_bytes.restype = sz
+        L.svof_guard_check.argtypes = [ctypes.POINTER(sz)]
         L.svof_synchronize.argtypes = [vp]
         L.svof_profile_step.argtypes = [vp, dp, dp, i]
         L.svof_stream.argtypes = [vp, ctypes.POINTER(vp)]
@@ -178,6 +182,24 @@ def lib() -> ctypes.CDLL:
 def _check(rc: int):
     if rc != 0:
         raise SvofError(lib().svof_last_error().decode())
+
+
+def guard_bytes() -> int:
+    """the guard band (bytes) around every device buffer, from SVOF_GUARD_BYTES
+    at allocation time; 0 = off"""
+    return int(lib().svof_guard_bytes())
+
+
+def guard_check() -> int:
+    """scans every live guard zone; returns 0 when intact, else raises
+    SvofError naming the first changed zone"""
+    bad = ctypes.c_size_t(0)
+    rc = lib().svof_guard_check(ctypes.byref(bad))
+    if rc != 0 and bad.value == 0:
+        _check(rc)
+    if bad.value:
+        raise SvofError(f"{bad.value} guard bytes changed: " + lib().svof_last_error().decode())
+    return 0
 
 
 def _c(a: np.ndarray) -> np.ndarray:

@@ -20,6 +20,7 @@
 #include <string>
 #include <vector>
 
+#include "guard.cuh"
 #include "../../include/svof_b200.h"
 #include "svof_internal.cuh"
 #include "stat_internal.cuh"
@@ -82,11 +83,7 @@ int fail(const char *fmt, ...) {
 int dalloc(DevBuf &b, size_t n, bool managed) {
   if (svof_fault::next_alloc_fails()) return fail("cudaMalloc: out of memory (injected by SVOF_FAIL_ALLOC)");
   b.n = n;
-  if (managed) {
-    CK(cudaMallocManaged(&b.p, sizeof(double) * (n ? n : 1)));
-  } else {
-    CK(cudaMalloc(&b.p, sizeof(double) * (n ? n : 1)));
-  }
+  CK(svof_guard::alloc(reinterpret_cast<void **>(&b.p), sizeof(double) * (n ? n : 1), managed));
   CK(cudaMemset(b.p, 0, sizeof(double) * (n ? n : 1)));
   return 0;
 }
@@ -98,7 +95,7 @@ int upload(DevBuf &b, const std::vector<double> &h) {
 }
 
 void dfree(DevBuf &b) {
-  if (b.p) cudaFree(b.p);
+  if (b.p) svof_guard::release(b.p);
   b.p = nullptr;
   b.n = 0;
 }

@@ -26,6 +26,7 @@
 #include "smem_limit.cuh"
 #include "fault_hook.cuh"
 #include "adjoint3d_internal.cuh"
+#include "guard.cuh"
 
 using namespace svof3;
 
@@ -77,7 +78,7 @@ int dalloc(DevBuf &b, size_t n, size_t es = 8) {
   if (svof_fault::next_alloc_fails()) return fail("cudaMalloc: out of memory (injected by SVOF_FAIL_ALLOC)");
   b.n = n;
   b.es = es;
-  CK(cudaMalloc(&b.p, es * (n ? n : 1)));
+  CK(svof_guard::alloc(reinterpret_cast<void **>(&b.p), es * (n ? n : 1), false));
   CK(cudaMemset(b.p, 0, es * (n ? n : 1)));
   return 0;
 }
@@ -89,7 +90,7 @@ int upload(DevBuf &b, const std::vector<double> &h) {
 }
 
 void dfree(DevBuf &b) {
-  if (b.p) cudaFree(b.p);
+  if (b.p) svof_guard::release(b.p);
   b.p = nullptr;
   b.n = 0;
 }
