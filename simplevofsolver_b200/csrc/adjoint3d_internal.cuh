@@ -58,7 +58,7 @@ struct Adj3RhsArgs {
   double *avof, *agrv;
   AGrid3 ag;
 };
-__global__ void __launch_bounds__(256, 3) k3_adj_rhs(Adj3RhsArgs a);
+__global__ void __launch_bounds__(256, 4) k3_adj_rhs(Adj3RhsArgs a);
 
 struct Adj3IfaceArgs {
   const double *ux, *uy, *uz, *vof, *normal, *curv;  // primal, storage layouts

@@ -322,9 +322,12 @@ __global__ void __launch_bounds__(kAdjXLines) k3_adj_xsolve(
 // Neighbours are addressed by offsets (di, dj, dk) from the cell: compact
 // arrays with periodic wraps (Wrap3), primal storage arrays through their
 // halos.
-// (80 registers, no spill: three blocks of 256 threads per SM; the kernel
-// is bound by memory latency, so resident warps set its speed)
-__global__ void __launch_bounds__(256, 3) k3_adj_rhs(Adj3RhsArgs a) {
+// (64 registers and a 76-byte spill: four blocks of 256 threads per SM; the
+// kernel is bound by memory latency, so resident warps set its speed: 2 %
+// faster than three blocks without spill.  A z-marching form with the
+// k -+ 1 planes of seven arrays in a cp.async shared-memory ring, two blocks
+// per SM, was 19 % slower)
+__global__ void __launch_bounds__(256, 4) k3_adj_rhs(Adj3RhsArgs a) {
   int i, j, k;
   const AGrid3 &ag = a.ag;
   const Grid3 &g = ag.g;
