@@ -272,6 +272,17 @@ int svof3d_adjoint_reset(svof3d_solver_t *s);
  * to 1e-5, below which their FP32 fluxes' vof noise (about 1e-8 beside the
  * interface) would make those transposes grow without bound over steps. */
 int svof3d_adjoint_set_gradient_floor(svof3d_solver_t *s, double tau);
+/* fp32 != 0: the adjoint's intermediates (the adjoints of the momentum
+ * sources, forces, curvature, normals and corner gradients, and the sources'
+ * pending terms) stored in FP32; the adjoint fields of the state (u, p, vof,
+ * psi), the tension and gravity accumulators, the arithmetic, the x line
+ * recurrences and the Poisson solve stay FP64.  Default 0.  Changing it
+ * discards the adjoint's buffers (they are made again on the next adjoint
+ * call; set it before svof3d_adjoint_reset).  With fp32 the intermediates
+ * are not readable through svof3d_adjoint_field, and the gradient floor
+ * defaults to 1e-5 on every path (the exact transpose's intermediates reach
+ * ~1e9 at corners of round-off gradients, beyond FP32's resolution). */
+int svof3d_adjoint_set_precision(svof3d_solver_t *s, int fp32);
 int svof3d_adjoint_step(svof3d_solver_t *s, const double *tape, double dt);
 int svof3d_adjoint_fluid_update_pressure(svof3d_solver_t *s, size_t rkstep, double dt);
 int svof3d_adjoint_fluid_correct_velocity(svof3d_solver_t *s, size_t rkstep, double dt);

@@ -32,22 +32,22 @@ __global__ void k3_adj_scale(const double *__restrict__ apsi, double *__restrict
 // u_bar += the divergence's transpose of pre_p dxf s; psi_bar = 0
 __global__ void k3_adj_div(double *__restrict__ aux, double *__restrict__ auy, double *__restrict__ auz,
                            const double *__restrict__ s, double *__restrict__ apsi, double pre_p, AGrid3 ag);
-// transposed implicit-x solves and the RK split: grid (lines / kAdjXLines,
-// 3 fields), kAdjXLines threads, dynamic shared memory adj_xsolve_smem(nx)
-__global__ void k3_adj_xsolve(const double *__restrict__ aux, const double *__restrict__ auy,
-                              const double *__restrict__ auz, const double *__restrict__ coef,
-                              double *__restrict__ sa_x, double *__restrict__ sg_x, double *__restrict__ sa_y,
-                              double *__restrict__ sg_y, double *__restrict__ sa_z, double *__restrict__ sg_z,
-                              double *__restrict__ pend_x, double *__restrict__ pend_y, double *__restrict__ pend_z,
-                              double adt, double bdt, double gdt, Grid3 g);
+// S, the storage type of the adjoint's intermediates (the sources', forces',
+// curvature's, normals' and corner gradients' adjoints): double, or float for
+// the FP32 adjoint; accumulators, arithmetic, line recurrences and the
+// Poisson solve are FP64 in both.
+
+// dynamic shared memory of the x solves (kAdjXLines threads a block)
 inline size_t adj_xsolve_smem(int nx) {
   return sizeof(double) * (3 * (size_t)nx + 2 * (size_t)kAdjXLines * (kAdjXChunk + 1));
 }
 
+template <class S>
 struct Adj3RhsArgs {
   const double *ux, *uy, *uz;                               // primal, storage layouts
-  const double *sa_x, *sg_x, *sa_y, *sg_y, *sa_z, *sg_z;    // src_a_bar, src_g_bar
-  double *aux, *auy, *auz, *ap, *aifx, *aify, *aifz;
+  const S *sa_x, *sg_x, *sa_y, *sg_y, *sa_z, *sg_z;         // src_a_bar, src_g_bar
+  double *aux, *auy, *auz, *ap;
+  S *aifx, *aify, *aifz;
   const double *lap_ux, *lap_cc;
   double m_dif, ly0, ly1, ly2, lz0, lz1, lz2;
   // the vof buoyancy extension (skipped while grav_vof == 0): vof_post the
@@ -58,29 +58,43 @@ struct Adj3RhsArgs {
   double *avof, *agrv;
   AGrid3 ag;
 };
-__global__ void __launch_bounds__(256, 4) k3_adj_rhs(Adj3RhsArgs a);
 
+template <class S>
 struct Adj3IfaceArgs {
   const double *ux, *uy, *uz, *vof, *normal, *curv;  // primal, storage layouts
   const double *avof_in, *pend_in;                   // vof_bar' and pend (compact)
   double *avof_out, *pend_out;
   double *aux, *auy, *auz;                           // += flux terms of owned faces
-  const double *aifx, *aify, *aifz;                  // force adjoints
-  double *anrm;                                      // [4] per cell
-  double *am;                                        // [3] per cell, m_bar
-  double *akap;                                      // kappa_bar
+  const S *aifx, *aify, *aifz;                       // force adjoints
+  S *anrm;                                           // [4] per cell
+  S *am;                                             // [3] per cell, m_bar
+  S *akap;                                           // kappa_bar
   double *asig;                                      // tension adjoint, per cell, +=
   double adt, bdt, tension;
   int mode;
   AGrid3 ag;
 };
-__global__ void __launch_bounds__(256, 4) k3_adj_interface(Adj3IfaceArgs a);
 
-// corner gradients' adjoints ([3] per corner, (nx + 1) ny nz corners)
-__global__ void k3_adj_cgrad(const double *__restrict__ vof, const double *__restrict__ am,
-                             const double *__restrict__ akap, double *__restrict__ gbar, AGrid3 ag);
-// vof_bar += the corner gradients' transposes
-__global__ void k3_adj_cvof(const double *__restrict__ gbar, double *__restrict__ avof, AGrid3 ag);
+// launchers of the templated kernels (defined beside them in k3_adjoint.cu):
+// the x solves and RK split on `lines` lines (z_x, z_y, z_z: FP64 scratch of
+// the forward sweep's values, src_g_bar itself when S is double), the
+// right-hand-side and interface transposes on the cells, and the corner
+// gradients (their normalisation's transpose, then back to vof_bar)
+template <class S>
+cudaError_t adj3_xsolve_launch(cudaStream_t st, long lines, size_t smem, const double *aux, const double *auy,
+                               const double *auz, const double *coef, S *sa_x, S *sg_x, S *sa_y, S *sg_y, S *sa_z,
+                               S *sg_z, S *pend_x, S *pend_y, S *pend_z, double *z_x, double *z_y, double *z_z,
+                               double adt, double bdt, double gdt, Grid3 g);
+template <class S>
+cudaError_t adj3_xsolve_prepare(size_t smem);
+template <class S>
+cudaError_t adj3_rhs_launch(cudaStream_t st, const Adj3RhsArgs<S> &a);
+template <class S>
+cudaError_t adj3_interface_launch(cudaStream_t st, const Adj3IfaceArgs<S> &a);
+template <class S>
+cudaError_t adj3_corners_launch(cudaStream_t st, const double *vof, const S *am, const S *akap, S *gbar,
+                                double *avof, AGrid3 ag);
+
 // deterministic sum (one block of 256 threads)
 __global__ void k3_adj_sum(const double *__restrict__ x, long n, double *__restrict__ out);
 // *dst = v in stream order

@@ -192,22 +192,26 @@ __global__ void k3_adj_div(double *__restrict__ aux, double *__restrict__ auy, d
 // one per thread, the recurrences carried in registers; the lines (rows of
 // the compact arrays, contiguous) pass through two shared tiles kAdjXChunk
 // points at a time: cp.async brings chunk c + 1 (runs of consecutive points)
-// while chunk c is swept.  The forward sweep leaves z in src_g_bar, which the
-// backward sweep reads and overwrites.
+// while chunk c is swept.  The forward sweep parks z in z_f (FP64: src_g_bar
+// itself when S is double, a scratch array otherwise), which the backward
+// sweep reads.
+template <class S>
 __global__ void __launch_bounds__(kAdjXLines) k3_adj_xsolve(
     const double *__restrict__ aux, const double *__restrict__ auy, const double *__restrict__ auz,
-    const double *__restrict__ coef, double *__restrict__ sa_x, double *__restrict__ sg_x, double *__restrict__ sa_y,
-    double *__restrict__ sg_y, double *__restrict__ sa_z, double *__restrict__ sg_z, double *__restrict__ pend_x,
-    double *__restrict__ pend_y, double *__restrict__ pend_z, double adt, double bdt, double gdt, Grid3 g) {
+    const double *__restrict__ coef, S *__restrict__ sa_x, S *__restrict__ sg_x, S *__restrict__ sa_y,
+    S *__restrict__ sg_y, S *__restrict__ sa_z, S *__restrict__ sg_z, S *__restrict__ pend_x,
+    S *__restrict__ pend_y, S *__restrict__ pend_z, double *__restrict__ z_x, double *__restrict__ z_y,
+    double *__restrict__ z_z, double adt, double bdt, double gdt, Grid3 g) {
   extern __shared__ double smx[];
   constexpr int NL = kAdjXLines, XC = kAdjXChunk, LD = kAdjXChunk + 1, PER = NL * XC / kAdjXLines;
   const int nx = g.nx;
   const int f = blockIdx.y;  // 0 ux, 1 uy, 2 uz
   const int n = (0 == f) ? nx - 1 : nx;
   const double *src = (0 == f) ? aux : (1 == f ? auy : auz);
-  double *sa = (0 == f) ? sa_x : (1 == f ? sa_y : sa_z);
-  double *sg = (0 == f) ? sg_x : (1 == f ? sg_y : sg_z);
-  double *pend = (0 == f) ? pend_x : (1 == f ? pend_y : pend_z);
+  S *sa = (0 == f) ? sa_x : (1 == f ? sa_y : sa_z);
+  S *sg = (0 == f) ? sg_x : (1 == f ? sg_y : sg_z);
+  S *pend = (0 == f) ? pend_x : (1 == f ? pend_y : pend_z);
+  double *zp = (0 == f) ? z_x : (1 == f ? z_y : z_z);  // the forward sweep's values
   const int set = (0 == f) ? 0 : 1;
   double *sL = smx, *sR = smx + nx, *sV = smx + 2 * nx;
   double *tiles = smx + 3 * nx;  // [2][NL][LD]
@@ -255,7 +259,7 @@ __global__ void __launch_bounds__(kAdjXLines) k3_adj_xsolve(
 #pragma unroll
     for (int m = 0; m < PER; m++) {
       const int w = t + NL * m, r = w / XC, q = w - r * XC;
-      if (r < nr && q < cw) sg[base + (size_t)r * n + c0 + q] = tl[r * LD + q];
+      if (r < nr && q < cw) zp[base + (size_t)r * n + c0 + q] = tl[r * LD + q];
     }
     __syncthreads();  // the tile is refilled two chunks on
   }
@@ -265,12 +269,12 @@ __global__ void __launch_bounds__(kAdjXLines) k3_adj_xsolve(
   // backward sweep, chunks in reverse
   double y = 0.;
   const double rd0 = 1. / sR[0];
-  fetch(sg, nch - 1, 0);
+  fetch(zp, nch - 1, 0);
   for (int it = 0; it < nch; it++) {
     const int c = nch - 1 - it, c0 = c * XC, cw = min(XC, n - c0), buf = it & 1;
     double *tl = tiles + (size_t)buf * NL * LD;
     if (c - 1 >= 0) {
-      fetch(sg, c - 1, buf ^ 1);
+      fetch(zp, c - 1, buf ^ 1);
       __pipeline_wait_prior(1);
     } else {
       __pipeline_wait_prior(0);
@@ -292,7 +296,7 @@ __global__ void __launch_bounds__(kAdjXLines) k3_adj_xsolve(
 #pragma unroll
     for (int m = 0; m < PER; m++) {
       const int w = t + NL * m, r = w / XC, q = w - r * XC;
-      pv[m] = (r < nr && q < cw) ? pend[base + (size_t)r * n + c0 + q] : 0.;
+      pv[m] = (r < nr && q < cw) ? (double)pend[base + (size_t)r * n + c0 + q] : 0.;
     }
 #pragma unroll
     for (int m = 0; m < PER; m++) {
@@ -300,9 +304,9 @@ __global__ void __launch_bounds__(kAdjXLines) k3_adj_xsolve(
       if (r < nr && q < cw) {
         const size_t o = base + (size_t)r * n + c0 + q;
         const double d = tl[r * LD + q];
-        sa[o] = adt * d + pv[m];
-        sg[o] = gdt * d;
-        pend[o] = bdt * d;
+        sa[o] = S(adt * d + pv[m]);
+        sg[o] = S(gdt * d);
+        pend[o] = S(bdt * d);
       }
     }
     __syncthreads();
@@ -327,7 +331,8 @@ __global__ void __launch_bounds__(kAdjXLines) k3_adj_xsolve(
 // faster than three blocks without spill.  A z-marching form with the
 // k -+ 1 planes of seven arrays in a cp.async shared-memory ring, two blocks
 // per SM, was 19 % slower)
-__global__ void __launch_bounds__(256, 4) k3_adj_rhs(Adj3RhsArgs a) {
+template <class S>
+__global__ void __launch_bounds__(256, 4) k3_adj_rhs(Adj3RhsArgs<S> a) {
   int i, j, k;
   const AGrid3 &ag = a.ag;
   const Grid3 &g = ag.g;
@@ -388,7 +393,7 @@ __global__ void __launch_bounds__(256, 4) k3_adj_rhs(Adj3RhsArgs a) {
       acc += 0.25 * dw * (SAZ(0, 0, s) * rxf_i + SAZ(-1, 0, s) * rxf_m);
     }
     a.aux[of] = acc;
-    a.aifx[of] = SAX(0, 0, 0);
+    a.aifx[of] = S(SAX(0, 0, 0));
   }
   const double dxf = g.dxf[i - 1];
   // ---- uy cell (i, j, k)
@@ -431,7 +436,7 @@ __global__ void __launch_bounds__(256, 4) k3_adj_rhs(Adj3RhsArgs a) {
       acc += nu * d;
     }
     a.auy[oc] = acc;
-    a.aify[oc] = SAY(0, 0, 0);
+    a.aify[oc] = S(SAY(0, 0, 0));
     // the vof buoyancy grav (0.5 vof(j-1) + 0.5 vof(j) - vof_ref) of the uy
     // faces j and j + 1
     if (0. != a.grav_vof) {
@@ -481,7 +486,7 @@ __global__ void __launch_bounds__(256, 4) k3_adj_rhs(Adj3RhsArgs a) {
       acc += nu * d;
     }
     a.auz[oc] = acc;
-    a.aifz[oc] = SAZ(0, 0, 0);
+    a.aifz[oc] = S(SAZ(0, 0, 0));
   }
   // ---- pressure gradients of the three src_g
   double pb = (SGY(0, 1, 0) - SGY(0, 0, 0)) * rdy + (SGZ(0, 0, 1) - SGZ(0, 0, 0)) * rdz;
@@ -506,7 +511,8 @@ __global__ void __launch_bounds__(256, 4) k3_adj_rhs(Adj3RhsArgs a) {
 // With mode & 1 but not & 4, n_bar goes to anrm; with & 4 but not & 1 it is
 // read from there.
 // (64 registers, no spill: four blocks of 256 threads per SM)
-__global__ void __launch_bounds__(256, 4) k3_adj_interface(Adj3IfaceArgs a) {
+template <class S>
+__global__ void __launch_bounds__(256, 4) k3_adj_interface(Adj3IfaceArgs<S> a) {
   int i, j, k;
   const AGrid3 &ag = a.ag;
   const Grid3 &g = ag.g;
@@ -611,7 +617,7 @@ __global__ void __launch_bounds__(256, 4) k3_adj_interface(Adj3IfaceArgs a) {
       if (!(vel < 0.)) upwind(vel, fz_kp, 2, +0.5);
     }
     if (!(a.mode & 4))
-      for (int m = 0; m < 4; m++) a.anrm[4 * oc + m] = nb[m];
+      for (int m = 0; m < 4; m++) a.anrm[4 * oc + m] = S(nb[m]);
   }
   if (a.mode & 2) {
     const double sig = a.tension;
@@ -649,7 +655,7 @@ __global__ void __launch_bounds__(256, 4) k3_adj_interface(Adj3IfaceArgs a) {
       kb += sig * grad * 0.5 * ib;
       if (0 == s) sb += grad * kap * ib;
     }
-    a.akap[oc] = kb;
+    a.akap[oc] = S(kb);
     a.asig[oc] += sb;
   }
   if (a.mode & 4) {
@@ -690,7 +696,7 @@ __global__ void __launch_bounds__(256, 4) k3_adj_interface(Adj3IfaceArgs a) {
       mv[2] *= rdz;
       unit_adj3(mv[0], mv[1], mv[2], nb[0], nb[1], nb[2], mb[0], mb[1], mb[2]);
     }
-    for (int m = 0; m < 3; m++) a.am[3 * oc + m] = mb[m];
+    for (int m = 0; m < 3; m++) a.am[3 * oc + m] = S(mb[m]);
   }
   a.avof_out[oc] = vacc;
 }
@@ -704,8 +710,9 @@ __global__ void __launch_bounds__(256, 4) k3_adj_interface(Adj3IfaceArgs a) {
 // the normalisation's transpose (zero at a corner flatter than the gradient
 // floor tau); gbar[3 corner] = the corner gradient's adjoint, corner =
 // (ic - 1) + (nx + 1) ((jc - 1) + ny (kc - 1)).
-__global__ void k3_adj_cgrad(const double *__restrict__ vof, const double *__restrict__ am,
-                             const double *__restrict__ akap, double *__restrict__ gbar, AGrid3 ag) {
+template <class S>
+__global__ void k3_adj_cgrad(const double *__restrict__ vof, const S *__restrict__ am, const S *__restrict__ akap,
+                             S *__restrict__ gbar, AGrid3 ag) {
   const Grid3 &g = ag.g;
   const int ic = 1 + blockIdx.x * blockDim.x + threadIdx.x;
   const int jc = 1 + blockIdx.y * blockDim.y + threadIdx.y;
@@ -735,16 +742,17 @@ __global__ void k3_adj_cgrad(const double *__restrict__ vof, const double *__res
     if (sqrt(gx * gx + gy * gy + gz * gz) < ag.tau * rmax) o0 = o1 = o2 = 0.;
   }
   const long q = (long)(ic - 1) + (long)(nx + 1) * ((long)(jc - 1) + (long)ny * (kc - 1));
-  gbar[3 * q + 0] = o0;
-  gbar[3 * q + 1] = o1;
-  gbar[3 * q + 2] = o2;
+  gbar[3 * q + 0] = S(o0);
+  gbar[3 * q + 1] = S(o1);
+  gbar[3 * q + 2] = S(o2);
 }
 
 // k3_adj_cvof: one thread per cell: vof_bar += the corner gradients'
 // transposes of its eight corners (ic in {i, i+1}, jc, kc wrapped): the cell is
 // the corner's (ic-1+dp, jc-1+dq, kc-1+dr) cell, with coefficients
 // -+1 / dxc(ic), -+1 / dy, -+1 / dz (+ for dp, dq, dr = 1)
-__global__ void k3_adj_cvof(const double *__restrict__ gbar, double *__restrict__ avof, AGrid3 ag) {
+template <class S>
+__global__ void k3_adj_cvof(const S *__restrict__ gbar, double *__restrict__ avof, AGrid3 ag) {
   int i, j, k;
   const Grid3 &g = ag.g;
   if (!cell3(g, i, j, k)) return;
@@ -756,10 +764,11 @@ __global__ void k3_adj_cvof(const double *__restrict__ gbar, double *__restrict_
         const int ic = i + sp, jc = wrap(j + sq, ny), kc = wrap(k + sr, nz);
         const long q = (long)(ic - 1) + (long)(nx + 1) * ((long)(jc - 1) + (long)ny * (kc - 1));
         // the cell's place in the corner's stencil: dp = 1 - sp, dq = 1 - sq, dr = 1 - sr
-        const double gxv = gbar[3 * q + 0] * ag.rxc[ic - 1];
+        const double gxv = (double)gbar[3 * q + 0] * ag.rxc[ic - 1];
+        const double gyv = gbar[3 * q + 1], gzv = gbar[3 * q + 2];
         sx += sp ? -gxv : gxv;
-        sy += sq ? -gbar[3 * q + 1] : gbar[3 * q + 1];
-        sz += sr ? -gbar[3 * q + 2] : gbar[3 * q + 2];
+        sy += sq ? -gyv : gyv;
+        sz += sr ? -gzv : gzv;
       }
   avof[ix_src(g, i, j, k)] += sx + sy * ag.rdy + sz * ag.rdz;
 }
@@ -779,5 +788,62 @@ __global__ void k3_adj_sum(const double *__restrict__ x, long n, double *__restr
 }
 
 __global__ void k3_adj_set(double *dst, double v) { *dst = v; }
+
+// ---- launchers (the kernels' instantiations stay in this translation unit)
+template <class S>
+cudaError_t adj3_xsolve_launch(cudaStream_t st, long lines, size_t smem, const double *aux, const double *auy,
+                               const double *auz, const double *coef, S *sa_x, S *sg_x, S *sa_y, S *sg_y, S *sa_z,
+                               S *sg_z, S *pend_x, S *pend_y, S *pend_z, double *z_x, double *z_y, double *z_z,
+                               double adt, double bdt, double gdt, Grid3 g) {
+  k3_adj_xsolve<S><<<dim3((unsigned)((lines + kAdjXLines - 1) / kAdjXLines), 3), kAdjXLines, smem, st>>>(
+      aux, auy, auz, coef, sa_x, sg_x, sa_y, sg_y, sa_z, sg_z, pend_x, pend_y, pend_z, z_x, z_y, z_z, adt, bdt, gdt,
+      g);
+  return cudaGetLastError();
+}
+
+template <class S>
+cudaError_t adj3_xsolve_prepare(size_t smem) {
+  return cudaFuncSetAttribute(k3_adj_xsolve<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+template <class S>
+cudaError_t adj3_rhs_launch(cudaStream_t st, const Adj3RhsArgs<S> &a) {
+  const Grid3 &g = a.ag.g;
+  k3_adj_rhs<S><<<dim3((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz), dim3(32, 8), 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <class S>
+cudaError_t adj3_interface_launch(cudaStream_t st, const Adj3IfaceArgs<S> &a) {
+  const Grid3 &g = a.ag.g;
+  k3_adj_interface<S><<<dim3((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz), dim3(32, 8), 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <class S>
+cudaError_t adj3_corners_launch(cudaStream_t st, const double *vof, const S *am, const S *akap, S *gbar,
+                                double *avof, AGrid3 ag) {
+  const Grid3 &g = ag.g;
+  k3_adj_cgrad<S><<<dim3((g.nx + 1 + 31) / 32, (g.ny + 7) / 8, g.nz), dim3(32, 8), 0, st>>>(vof, am, akap, gbar,
+                                                                                            ag);
+  cudaError_t e = cudaGetLastError();
+  if (cudaSuccess != e) return e;
+  k3_adj_cvof<S><<<dim3((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz), dim3(32, 8), 0, st>>>(gbar, avof, ag);
+  return cudaGetLastError();
+}
+
+// the two storage types of the adjoint's intermediates
+#define SVOF3_ADJ_INST(S)                                                                                         \
+  template cudaError_t adj3_xsolve_launch<S>(cudaStream_t, long, size_t, const double *, const double *,           \
+                                             const double *, const double *, S *, S *, S *, S *, S *, S *, S *, S *, \
+                                             S *, double *, double *, double *, double, double, double, Grid3);     \
+  template cudaError_t adj3_xsolve_prepare<S>(size_t);                                                           \
+  template cudaError_t adj3_rhs_launch<S>(cudaStream_t, const Adj3RhsArgs<S> &);                                 \
+  template cudaError_t adj3_interface_launch<S>(cudaStream_t, const Adj3IfaceArgs<S> &);                         \
+  template cudaError_t adj3_corners_launch<S>(cudaStream_t, const double *, const S *, const S *, S *, double *,  \
+                                              AGrid3);
+SVOF3_ADJ_INST(double)
+SVOF3_ADJ_INST(float)
+#undef SVOF3_ADJ_INST
 
 }  // namespace svof3

@@ -149,6 +149,8 @@ struct svof3d_solver {
   size_t stat_num = 0;
 
   Adjoint3State *adj = nullptr;
+  bool adj_f32 = false;  // the adjoint's intermediates in FP32 (svof3d_adjoint_set_precision)
+  double adj_tau = -1.;  // gradient floor set by the caller; < 0: the path's default
   // vof buoyancy extension (svof3d_set_gravity; 0 = off)
   double grav_vof = 0., vof_ref = 0.;
 
@@ -1146,6 +1148,8 @@ struct Adjoint3State {
   DevBuf psib, b, psis, gbar, grv, sum;
   DevBuf rxf, rxc;  // 1 / dxf, 1 / dxc
   DevBuf nrm64, curv64;  // FP64 geometry of the mixed paths (storage layouts)
+  DevBuf zx, zy, zz;     // the x solve's forward values with FP32 intermediates (FP64)
+  bool f32 = false;      // intermediates (sources, forces, curvature, normals, corners) in FP32
   int cv = 0;  // current buffer of vof_bar
   int cp = 0;  // current buffer of the vof source's pending adjoint
   size_t xs_smem = 0;
@@ -1166,6 +1170,9 @@ void adjoint3_free(svof3d_solver *s) {
   dfree(s->adj->rxc);
   dfree(s->adj->nrm64);
   dfree(s->adj->curv64);
+  dfree(s->adj->zx);
+  dfree(s->adj->zy);
+  dfree(s->adj->zz);
   delete s->adj;
   s->adj = nullptr;
 }
@@ -1184,21 +1191,29 @@ int adj3_ensure(svof3d_solver *s) {
   const size_t nx = s->nx, ny = s->ny, nz = s->nz;
   if (adj_xsolve_smem((int)nx) > 200 * 1024) return fail("the adjoint's x line solve needs nx <= 7800");
   Adjoint3State *a = new Adjoint3State();
+  a->f32 = s->adj_f32;
+  const size_t es = a->f32 ? sizeof(float) : sizeof(double);  // the intermediates
   const size_t nc = nx * ny * nz, nf = (nx - 1) * ny * nz, ncc = (nx + 2) * (ny + 2) * (nz + 2);
   bool bad = dalloc(a->ux, nf) || dalloc(a->uy, nc) || dalloc(a->uz, nc) || dalloc(a->p, nc) ||
              dalloc(a->vof[0], nc) || dalloc(a->vof[1], nc) || dalloc(a->pend_v[0], nc) ||
-             dalloc(a->pend_v[1], nc) || dalloc(a->pend_x, nf) || dalloc(a->pend_y, nc) || dalloc(a->pend_z, nc) ||
-             dalloc(a->sa_x, nf) || dalloc(a->sg_x, nf) || dalloc(a->sa_y, nc) || dalloc(a->sg_y, nc) ||
-             dalloc(a->sa_z, nc) || dalloc(a->sg_z, nc) || dalloc(a->ifx, nf) || dalloc(a->ify, nc) ||
-             dalloc(a->ifz, nc) || dalloc(a->kap, nc) || dalloc(a->m, 3 * nc) || dalloc(a->nrm, 4 * nc) ||
+             dalloc(a->pend_v[1], nc) || dalloc(a->pend_x, nf, es) || dalloc(a->pend_y, nc, es) ||
+             dalloc(a->pend_z, nc, es) || dalloc(a->sa_x, nf, es) || dalloc(a->sg_x, nf, es) ||
+             dalloc(a->sa_y, nc, es) || dalloc(a->sg_y, nc, es) || dalloc(a->sa_z, nc, es) ||
+             dalloc(a->sg_z, nc, es) || dalloc(a->ifx, nf, es) || dalloc(a->ify, nc, es) || dalloc(a->ifz, nc, es) ||
+             dalloc(a->kap, nc, es) || dalloc(a->m, 3 * nc, es) || dalloc(a->nrm, 4 * nc, es) ||
              dalloc(a->sig, nc) || dalloc(a->psib, nc) || dalloc(a->b, nc) || dalloc(a->psis, ncc) ||
-             dalloc(a->gbar, 3 * (nx + 1) * ny * nz) || dalloc(a->grv, nc) || dalloc(a->sum, 1);
+             dalloc(a->gbar, 3 * (nx + 1) * ny * nz, es) || dalloc(a->grv, nc) || dalloc(a->sum, 1);
+  if (!bad && a->f32) bad = dalloc(a->zx, nf) || dalloc(a->zy, nc) || dalloc(a->zz, nc);
   if (!bad && s->mixed)
     bad = dalloc(a->nrm64, 4 * nx * (ny + 2) * (nz + 2)) || dalloc(a->curv64, ncc) ||
           (s->dc && cudaSuccess != pois_prepare<double>(s->log2ny, s->log2nz));
   a->xs_smem = adj_xsolve_smem((int)nx);
-  a->tau = s->mixed ? kAdjMixedTau : 0.;
-  if (!bad && cudaSuccess != raise_smem_limit(k3_adj_xsolve, a->xs_smem)) bad = fail("cudaFuncSetAttribute(k3_adj_xsolve)");
+  // (FP32 intermediates take the floor too: the exact transposes carry values
+  // up to ~1e9 at corners of round-off gradients, beyond FP32's resolution)
+  a->tau = s->adj_tau >= 0. ? s->adj_tau : ((s->mixed || a->f32) ? kAdjMixedTau : 0.);
+  if (!bad && (cudaSuccess != adj3_xsolve_prepare<double>(a->xs_smem) ||
+               cudaSuccess != adj3_xsolve_prepare<float>(a->xs_smem)))
+    bad = fail("cudaFuncSetAttribute(k3_adj_xsolve)");
   if (!bad) {
     // reciprocal spacings from the device tables
     std::vector<double> h(nx + 1);
@@ -1276,37 +1291,41 @@ int adj3_potential(svof3d_solver *s, int rk, double dt) {
 }
 
 // fluid_predict_field about the primal velocities and the vof after the
-// substep's advection (storage layouts); d_dt must hold dt
-int adj3_predict(svof3d_solver *s, int rk, double dt, const double *ux, const double *uy, const double *uz,
-                 const double *vof_post) {
+// substep's advection (storage layouts); d_dt must hold dt.  S: the
+// storage type of the adjoint's intermediates
+template <class S>
+int adj3_predict_t(svof3d_solver *s, int rk, double dt, const double *ux, const double *uy, const double *uz,
+                   const double *vof_post) {
   Adjoint3State *a = s->adj;
   k3_tdm_coef<<<1, 128, sizeof(double) * 6 * s->nx, s->stream>>>(s->lap_ux.p, s->lap_cc.p, s->d_dt,
                                                                  RK_A[rk] + RK_B[rk], s->prm.m_dif, s->prm.t_dif,
                                                                  s->nx, s->coef.p);
   CK_LAUNCH();
   const long lines = (long)s->ny * s->nz;
-  k3_adj_xsolve<<<dim3((unsigned)((lines + kAdjXLines - 1) / kAdjXLines), 3), kAdjXLines, a->xs_smem, s->stream>>>(
-      a->ux.p, a->uy.p, a->uz.p, s->coef.p, a->sa_x.p, a->sg_x.p, a->sa_y.p, a->sg_y.p, a->sa_z.p, a->sg_z.p,
-      a->pend_x.p, a->pend_y.p, a->pend_z.p, RK_A[rk] * dt, RK_B[rk] * dt, (RK_A[rk] + RK_B[rk]) * dt,
-      s->grid());
-  CK_LAUNCH();
-  Adj3RhsArgs r{};
+  // the forward sweep's values: src_g_bar itself (FP64 intermediates) or the FP64 scratch
+  double *zx = a->f32 ? a->zx.p : a->sg_x.p, *zy = a->f32 ? a->zy.p : a->sg_y.p;
+  double *zz = a->f32 ? a->zz.p : a->sg_z.p;
+  CK(adj3_xsolve_launch<S>(s->stream, lines, a->xs_smem, a->ux.p, a->uy.p, a->uz.p, s->coef.p, a->sa_x.as<S>(),
+                            a->sg_x.as<S>(), a->sa_y.as<S>(), a->sg_y.as<S>(), a->sa_z.as<S>(), a->sg_z.as<S>(),
+                            a->pend_x.as<S>(), a->pend_y.as<S>(), a->pend_z.as<S>(), zx, zy, zz, RK_A[rk] * dt,
+                            RK_B[rk] * dt, (RK_A[rk] + RK_B[rk]) * dt, s->grid()));
+  Adj3RhsArgs<S> r{};
   r.ux = ux;
   r.uy = uy;
   r.uz = uz;
-  r.sa_x = a->sa_x.p;
-  r.sg_x = a->sg_x.p;
-  r.sa_y = a->sa_y.p;
-  r.sg_y = a->sg_y.p;
-  r.sa_z = a->sa_z.p;
-  r.sg_z = a->sg_z.p;
+  r.sa_x = a->sa_x.as<S>();
+  r.sg_x = a->sg_x.as<S>();
+  r.sa_y = a->sa_y.as<S>();
+  r.sg_y = a->sg_y.as<S>();
+  r.sa_z = a->sa_z.as<S>();
+  r.sg_z = a->sg_z.as<S>();
   r.aux = a->ux.p;
   r.auy = a->uy.p;
   r.auz = a->uz.p;
   r.ap = a->p.p;
-  r.aifx = a->ifx.p;
-  r.aify = a->ify.p;
-  r.aifz = a->ifz.p;
+  r.aifx = a->ifx.as<S>();
+  r.aify = a->ify.as<S>();
+  r.aifz = a->ifz.as<S>();
   r.lap_ux = s->lap_ux.p;
   r.lap_cc = s->lap_cc.p;
   r.m_dif = s->prm.m_dif;
@@ -1322,18 +1341,23 @@ int adj3_predict(svof3d_solver *s, int rk, double dt, const double *ux, const do
   r.avof = a->vof[a->cv].p;
   r.agrv = a->grv.p;
   r.ag = agrid(s);
-  k3_adj_rhs<<<adj3_cells(s), dim3(32, 8), 0, s->stream>>>(r);
-  CK_LAUNCH();
+  CK(adj3_rhs_launch<S>(s->stream, r));
   return 0;
+}
+int adj3_predict(svof3d_solver *s, int rk, double dt, const double *ux, const double *uy, const double *uz,
+                 const double *vof_post) {
+  return s->adj->f32 ? adj3_predict_t<float>(s, rk, dt, ux, uy, uz, vof_post)
+                     : adj3_predict_t<double>(s, rk, dt, ux, uy, uz, vof_post);
 }
 
 // interface_update_vof (mode 1), interface_compute_force (2), the intercept
 // and normal part of interface_compute_curvature_tensor (4), about the primal
 // velocities and vof (storage layouts) and the solver's normal and curv
-int adj3_interface(svof3d_solver *s, int rk, double dt, int mode, const double *ux, const double *uy,
-                   const double *uz, const double *vof) {
+template <class S>
+int adj3_interface_t(svof3d_solver *s, int rk, double dt, int mode, const double *ux, const double *uy,
+                     const double *uz, const double *vof) {
   Adjoint3State *a = s->adj;
-  Adj3IfaceArgs f{};
+  Adj3IfaceArgs<S> f{};
   f.ux = ux;
   f.uy = uy;
   f.uz = uz;
@@ -1347,35 +1371,39 @@ int adj3_interface(svof3d_solver *s, int rk, double dt, int mode, const double *
   f.aux = a->ux.p;
   f.auy = a->uy.p;
   f.auz = a->uz.p;
-  f.aifx = a->ifx.p;
-  f.aify = a->ify.p;
-  f.aifz = a->ifz.p;
-  f.anrm = a->nrm.p;
-  f.am = a->m.p;
-  f.akap = a->kap.p;
+  f.aifx = a->ifx.as<S>();
+  f.aify = a->ify.as<S>();
+  f.aifz = a->ifz.as<S>();
+  f.anrm = a->nrm.as<S>();
+  f.am = a->m.as<S>();
+  f.akap = a->kap.as<S>();
   f.asig = a->sig.p;
   f.adt = RK_A[rk] * dt;
   f.bdt = RK_B[rk] * dt;
   f.tension = s->prm.tension;
   f.mode = mode;
   f.ag = agrid(s);
-  k3_adj_interface<<<adj3_cells(s), dim3(32, 8), 0, s->stream>>>(f);
-  CK_LAUNCH();
+  CK(adj3_interface_launch<S>(s->stream, f));
   a->cv ^= 1;
   if (mode & 1) a->cp ^= 1;
   return 0;
 }
+int adj3_interface(svof3d_solver *s, int rk, double dt, int mode, const double *ux, const double *uy,
+                   const double *uz, const double *vof) {
+  return s->adj->f32 ? adj3_interface_t<float>(s, rk, dt, mode, ux, uy, uz, vof)
+                     : adj3_interface_t<double>(s, rk, dt, mode, ux, uy, uz, vof);
+}
 
 // the corner normals and curvature part of interface_compute_curvature_tensor
-int adj3_corners(svof3d_solver *s, const double *vof) {
+template <class S>
+int adj3_corners_t(svof3d_solver *s, const double *vof) {
   Adjoint3State *a = s->adj;
-  const AGrid3 ag = agrid(s);
-  k3_adj_cgrad<<<dim3((s->nx + 1 + 31) / 32, (s->ny + 7) / 8, s->nz), dim3(32, 8), 0, s->stream>>>(
-      vof, a->m.p, a->kap.p, a->gbar.p, ag);
-  CK_LAUNCH();
-  k3_adj_cvof<<<adj3_cells(s), dim3(32, 8), 0, s->stream>>>(a->gbar.p, a->vof[a->cv].p, ag);
-  CK_LAUNCH();
+  CK(adj3_corners_launch<S>(s->stream, vof, a->m.as<S>(), a->kap.as<S>(), a->gbar.as<S>(), a->vof[a->cv].p,
+                             agrid(s)));
   return 0;
+}
+int adj3_corners(svof3d_solver *s, const double *vof) {
+  return s->adj->f32 ? adj3_corners_t<float>(s, vof) : adj3_corners_t<double>(s, vof);
 }
 
 size_t n_ux3(const svof3d_solver *s) { return (size_t)(s->nx + 1) * (s->ny + 2) * (s->nz + 2); }
@@ -1473,6 +1501,9 @@ int svof3d_adjoint_field(svof3d_solver_t *s, int which, double **dptr, size_t *c
     case SVOF3_ADJ_GRAVITY: b = &a->grv; break;
     default: return fail("unknown adjoint field %d", which);
   }
+  if (b->es != sizeof(double))
+    return fail("svof3d_adjoint_field: field %d holds the FP32 adjoint's intermediates (svof3d_adjoint_set_precision)",
+                which);
   *dptr = b->p;
   if (count) *count = n;
   return 0;
@@ -1481,13 +1512,26 @@ int svof3d_adjoint_field(svof3d_solver_t *s, int which, double **dptr, size_t *c
 int svof3d_adjoint_set_gradient_floor(svof3d_solver_t *s, double tau) {
   if (adj3_check(s)) return 1;
   if (!(tau >= 0.)) return fail("svof3d_adjoint_set_gradient_floor: tau must be non-negative");
+  s->adj_tau = tau;
   s->adj->tau = tau;
+  return 0;
+}
+
+int svof3d_adjoint_set_precision(svof3d_solver_t *s, int fp32) {
+  if (!s) return fail("null argument");
+  const bool f = 0 != fp32;
+  if (s->adj && s->adj->f32 != f) {
+    // the buffers are made again, in the other type, on the next adjoint call
+    CK(cudaStreamSynchronize(s->stream));
+    adjoint3_free(s);
+  }
+  s->adj_f32 = f;
   return 0;
 }
 
 int svof3d_adjoint_reset(svof3d_solver_t *s) {
   if (adj3_check(s)) return 1;
-  for (int q = 0; DevBuf *b = s->adj->all(q); q++) CK(cudaMemsetAsync(b->p, 0, sizeof(double) * b->n, s->stream));
+  for (int q = 0; DevBuf *b = s->adj->all(q); q++) CK(cudaMemsetAsync(b->p, 0, b->es * b->n, s->stream));
   return 0;
 }
 
@@ -1500,7 +1544,7 @@ int svof3d_adjoint_step(svof3d_solver_t *s, const double *tape, double dt) {
   const size_t nu = n_ux3(s), nc = n_cc3(s), st = tape_stride3(s);
   // no substep follows the last one: its sources' pending adjoints are zero
   DevBuf *pend[] = {&a->pend_x, &a->pend_y, &a->pend_z, &a->pend_v[a->cp]};
-  for (DevBuf *b : pend) CK(cudaMemsetAsync(b->p, 0, sizeof(double) * b->n, s->stream));
+  for (DevBuf *b : pend) CK(cudaMemsetAsync(b->p, 0, b->es * b->n, s->stream));
   if (adj3_set_dt(s, dt)) return 1;
   for (int rk = 2; rk >= 0; rk--) {
     const double *ux = tape + rk * st, *uy = ux + nu, *uz = uy + nc, *vof = uz + nc;

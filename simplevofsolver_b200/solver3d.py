@@ -53,7 +53,7 @@ EXPORTS3D = ["svof3d_create", "svof3d_destroy", "svof3d_field_count", "svof3d_up
              "svof3d_adjoint_fluid_predict_field", "svof3d_adjoint_interface_update_vof",
              "svof3d_adjoint_interface_compute_force", "svof3d_adjoint_interface_compute_curvature_tensor",
              "svof3d_adjoint_tension", "svof3d_set_gravity", "svof3d_adjoint_gravity",
-             "svof3d_adjoint_set_gradient_floor"]
+             "svof3d_adjoint_set_gradient_floor", "svof3d_adjoint_set_precision"]
 
 # adjoint fields (SVOF3_ADJ_*); compact layouts: ux faces (nz, ny, nx-1), cells (nz, ny, nx)
 ADJ_FIELDS3D = {"ux": 0, "uy": 1, "uz": 2, "p": 3, "vof": 4, "psi": 5, "ifrcx": 6, "ifrcy": 7, "ifrcz": 8,
@@ -145,6 +145,7 @@ def lib3() -> ctypes.CDLL:
         L.svof3d_set_gravity.argtypes = [vp, d, d]
         L.svof3d_adjoint_gravity.argtypes = [vp, pd]
         L.svof3d_adjoint_set_gradient_floor.argtypes = [vp, d]
+        L.svof3d_adjoint_set_precision.argtypes = [vp, i]
         _bound = True
     return L
 
@@ -437,6 +438,15 @@ class Solver3D:
 
     def adjoint_reset(self):
         _check(lib3().svof3d_adjoint_reset(self._h))
+
+    def adjoint_set_precision(self, precision: str):
+        """"fp64" (default) or "fp32": the storage of the adjoint's
+        intermediates (the state's adjoints, accumulators, arithmetic, line
+        recurrences and Poisson solve stay FP64); discards the adjoint's
+        buffers when it changes"""
+        if precision not in ("fp64", "fp32"):
+            raise ValueError(f"adjoint precision must be 'fp64' or 'fp32', not {precision!r}")
+        _check(lib3().svof3d_adjoint_set_precision(self._h, int(precision == "fp32")))
 
     def adjoint_set_gradient_floor(self, tau: float):
         """corners flatter than tau (vof variation across a cell) have no

@@ -507,3 +507,43 @@ def test_defect_corrected_path_adjoint(gpu_available):
         g.close()
     assert np.isfinite(dd["mixed_dc"])
     assert rel(dd["mixed"], dd["mixed_dc"]) <= 1e-4, dd
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_fp32_intermediates(gpu_available, prec):
+    """the adjoint with FP32 intermediates (svof3d_adjoint_set_precision) against
+    the FP64 intermediates with the same gradient floor: two taped steps, the
+    directional derivatives along a divergence-free velocity, the tension
+    and the buoyancy coefficient agree to FP32 round-off; the FP32
+    intermediates are not exposed as FP64 views"""
+    import torch
+    from simplevofsolver_b200 import SvofError, physical_params
+    ic = droplets3d(32, 16, 16, ndrops=3, radii=(0.12, 0.2), seed=3)
+    phys = physical_params(DROPLETS3D_ENV)
+    dirn = droplets3d(32, 16, 16, ndrops=1, radii=(0.12, 0.13), seed=11)
+    d = {n: compact(n, getattr(dirn, n), 32) for n in ("ux", "uy", "uz")}
+    out = {}
+    for adj in ("fp64", "fp32"):
+        g = Solver3D(ic, phys, precision=prec)
+        g.set_gravity(-0.9, 0.15)
+        g.adjoint_set_precision(adj)
+        g.adjoint_set_gradient_floor(1e-5)
+        dt = 1.0e-3
+        tapes = [torch.empty(g.tape_count(), dtype=torch.float64, device="cuda") for _ in range(2)]
+        for t in tapes:
+            g.integrate_fixed(dt, t.data_ptr())
+        g.synchronize()
+        g.adjoint_reset()
+        rng = np.random.default_rng(13)
+        put_adj(g, "ux", rng.standard_normal((16, 16, 31)))
+        put_adj(g, "uy", rng.standard_normal((16, 16, 32)))
+        put_adj(g, "vof", np.broadcast_to(((np.arange(16) + 0.5) / 16)[None, :, None], (16, 16, 32)).copy())
+        for t in reversed(tapes):
+            g.adjoint_step(t.data_ptr(), dt)
+        out[adj] = (sum(float(np.sum(d[n] * get_adj(g, n))) for n in d), g.adjoint_tension(), g.adjoint_gravity())
+        if adj == "fp32":
+            with pytest.raises(SvofError, match="FP32"):
+                g.adjoint_view("ifrcx")
+        g.close()
+    for a_, b_ in zip(out["fp32"], out["fp64"]):
+        assert np.isfinite(a_) and rel(a_, b_) <= 1e-5, (out, a_, b_)
