@@ -394,12 +394,14 @@ def adjoint_cost(steps: int = 200, K: int = 20):
             "forward": "svof_integrate_fixed (time steps held fixed)"}
 
 
-def adjoint_cost3d(n: int = 256, steps: int = 100, budget: float = 60e9, precisions=("mixed", "fp64")):
+def adjoint_cost3d(n: int = 256, steps: int = 100, budget: float = 60e9,
+                   variants=(("mixed", "fp32"), ("mixed", "fp64"), ("fp64", "fp64"))):
     """Cost of the 3D differentiation form on its workload (diff3d_case:
     droplets3d at n^3, 16 droplets of radii in [0.05, 0.09], the vof buoyancy
     extension with density ratio 0.05 at Fr = 1, `steps` steps with the FP64
-    path's CFL time-step sequence held fixed), per forward precision (the
-    adjoint computes in FP64 on both): device time per step of the forward
+    path's CFL time-step sequence held fixed), per (forward precision,
+    storage of the adjoint's intermediates) -- the adjoint's arithmetic is FP64
+    in all: device time per step of the forward
     (svof3d_integrate_fixed) and of the backward pass (segment recompute with
     tapes plus svof3d_adjoint_step), CUDA events on the solver's stream;
     checkpoints every K steps, K the largest whose tapes and checkpoints fit
@@ -423,9 +425,10 @@ def adjoint_cost3d(n: int = 256, steps: int = 100, budget: float = 60e9, precisi
            "adjoint_dtype": "f64",
            "backward": "segment recompute with tapes + step adjoints (svof3d_adjoint_step)",
            "forward": "svof3d_integrate_fixed (time steps held fixed)"}
-    for prec in precisions:
+    for prec, adj in variants:
         s = Solver3D(ic, phys, precision=prec)
         s.set_gravity(grav, ref)
+        s.adjoint_set_precision(adj)
         K = checkpoint_interval(s, steps, budget)
         r = Rollout3D(s, dts, K)
         stream = torch.cuda.ExternalStream(s.stream())
@@ -469,7 +472,8 @@ def adjoint_cost3d(n: int = 256, steps: int = 100, budget: float = 60e9, precisi
         f_ms = min(fwd() for _ in range(2))
         b_ms = min(bwd() for _ in range(2))
         state_gb = sum(v.numel() for v in r.checkpoints[0].values()) * 8 / 1e9
-        out[prec] = {"forward_ms_per_step": f_ms / steps, "backward_ms_per_step": b_ms / steps,
+        out[prec if adj == "fp64" else prec + "_adjoint_fp32"] = {
+                     "forward_ms_per_step": f_ms / steps, "backward_ms_per_step": b_ms / steps,
                      "adjoint_over_forward": b_ms / f_ms, "checkpoint_every": K,
                      "tapes_gb": K * s.tape_count() * 8 / 1e9,
                      "checkpoints_gb": len(r.checkpoints) * state_gb}
@@ -477,7 +481,7 @@ def adjoint_cost3d(n: int = 256, steps: int = 100, budget: float = 60e9, precisi
         r.checkpoints = []
         s.close()
         torch.cuda.empty_cache()
-    out["adjoint_over_forward"] = out[precisions[0]]["adjoint_over_forward"]
+    out["adjoint_over_forward"] = out["mixed_adjoint_fp32"]["adjoint_over_forward"]
     return out
 
 

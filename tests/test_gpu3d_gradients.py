@@ -59,13 +59,14 @@ def case():
     return ic, phys, grav, ref, dts, dirn
 
 
-def gradient(case, precision):
+def gradient(case, precision, adjoint="fp64"):
     import torch
     from simplevofsolver_b200.adjoint import Rollout3D, checkpoint_interval, interface_area3d, rollout3d
     from simplevofsolver_b200.solver3d import Solver3D
     ic, phys, grav, ref, dts, dirn = case
     s = Solver3D(ic, phys, precision=precision)
     s.set_gravity(grav, ref)
+    s.adjoint_set_precision(adjoint)
     K = checkpoint_interval(s, STEPS, BUDGET)
     r = Rollout3D(s, dts, K)
     dev = dict(dtype=torch.float64, device="cuda")
@@ -132,5 +133,21 @@ def test_c4_gradients(case):
           f"{ref_dir}: max error / max derivative {e_dir:.2e}; density-ratio derivative rel {e_r:.2e}")
     assert all(np.isfinite(mix_dir)) and np.isfinite(float(gm["grav"]))
     assert e_dir <= 2e-3 and e_r <= 1e-3, (e_dir, e_r)
+    r.tapes = None
+    s.close()
+    del r, s
+    torch.cuda.empty_cache()
+    # the same with FP32 intermediates in the adjoint (the 3D differentiation
+    # workload's FP32 forward and adjoint, FP64 Poisson solves)
+    s, r, x, Jf, gf, Kf = gradient(case, "mixed", adjoint="fp32")
+    f_dir = directional(gf)
+    e_dir32 = max(abs(a - b) for a, b in zip(f_dir, ref_dir)) / scale
+    e_r32 = rel(float(gf["grav"]), float(g64["grav"]))
+    e_mix = max(abs(a - b) for a, b in zip(f_dir, mix_dir)) / scale
+    print(f"mixed, FP32 adjoint intermediates: directional {f_dir}: max error / max derivative {e_dir32:.2e} "
+          f"against the FP64 adjoint, {e_mix:.2e} against FP64 intermediates; density-ratio derivative rel "
+          f"{e_r32:.2e}")
+    assert all(np.isfinite(f_dir)) and np.isfinite(float(gf["grav"]))
+    assert e_dir32 <= 2e-3 and e_r32 <= 1e-3 and e_mix <= 1e-4, (e_dir32, e_r32, e_mix)
     r.tapes = None
     s.close()
