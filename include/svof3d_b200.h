@@ -30,7 +30,9 @@
  * next call that waits for the solver's stream (svof3d_fluid_decide_dt,
  * svof3d_run, svof3d_integrate, svof3d_last_dt, svof3d_io_wait,
  * svof3d_synchronize) return non-zero; SVOF_FAIL_ALLOC=N fails the N-th
- * device buffer allocation of svof3d_create.
+ * device buffer allocation of svof3d_create.  Two health counters that are
+ * not failures (the reference carries on silently in both cases) accumulate
+ * on the device and are read by svof3d_health.
  */
 #ifndef SVOF3D_B200_H
 #define SVOF3D_B200_H
@@ -297,6 +299,18 @@ int svof3d_adjoint_gravity(svof3d_solver_t *s, double *out);
 /* one step launched kernel by kernel with events between; ms[k], launches[k] per kind */
 int svof3d_profile_step(svof3d_solver_t *s, double *ms, int *launches, int nkinds);
 int svof3d_synchronize(svof3d_solver_t *s);
+/* health counters since creation or the last reset (waits for the stream;
+ * either output may be NULL; reset != 0 clears both after reading):
+ * newton_unconverged  THINC intercepts (svof3d_interface_compute_curvature_tensor
+ *                     and the steps) whose Newton iteration did not reach the
+ *                     1e-12 residual in 8 iterations (the reference keeps the
+ *                     last iterate: src/interface/curvature_tensor.c:50-92)
+ * small_pivots        Poisson x line solves (svof3d_fluid_compute_potential_dft
+ *                     and the steps) other than the singular ky = kz = 0 line
+ *                     that met a pivot of magnitude <= DBL_EPSILON (the
+ *                     reference zeroes such a last pivot, src/tdm.c:39) */
+int svof3d_health(svof3d_solver_t *s, unsigned long long *newton_unconverged, unsigned long long *small_pivots,
+                  int reset);
 int svof3d_stream(svof3d_solver_t *s, void **stream);
 
 #ifdef __cplusplus

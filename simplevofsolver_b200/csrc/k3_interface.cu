@@ -116,9 +116,10 @@ __device__ __forceinline__ float div_by(float x, float y) { return x * (1.f / y)
 
 // THINC intercept with 2 x 2 x 2 Gauss points (compute_intercept3 of the
 // restatement; src/interface/curvature_tensor.c:50-92 in 2D), Newton
-// tolerance 1e-12.
+// tolerance 1e-12.  `converged` tells whether the residual fell below the
+// tolerance within the 8 iterations (the value is the last iterate either way).
 template <class R>
-__device__ __forceinline__ R thinc_intercept3(const R vof, const R n0, const R n1, const R n2) {
+__device__ __forceinline__ R thinc_intercept3(const R vof, const R n0, const R n1, const R n2, bool &converged) {
   const int cntmax = 8;
   const R resmax = R(1.e-12);
   const R gp0 = R(c3_gauss_p[0]), gp1 = R(c3_gauss_p[1]), gw = R(c3_gauss_w[0]);
@@ -150,7 +151,10 @@ __device__ __forceinline__ R thinc_intercept3(const R vof, const R n0, const R n
       }
     }
     val -= f0 / f1;
-    if (fabs(f0) < resmax) break;
+    if (fabs(f0) < resmax) {
+      converged = true;
+      break;
+    }
   }
   return R(-0.5) / R(kVofBeta) * log(val);
 }
@@ -375,21 +379,30 @@ __global__ void __launch_bounds__(G3X * G3Y) k3_geom(const double *__restrict__ 
 // vector is already stored); one thread per cell, grid-stride over the list.
 // The Newton iteration runs in FP64 in both precisions: near-full cells
 // (1 - vof below FP32 resolution) have no FP32 solution, and the list holds
-// only the interfacial cells.
+// only the interfacial cells.  With `unconverged` given, the cells whose
+// iteration did not converge are added to it (one atomic per warp).
 template <class R>
 __global__ void __launch_bounds__(256) k3_intercept(const double *__restrict__ vof, R *__restrict__ normal,
                                                    const unsigned *__restrict__ work,
-                                                   const unsigned *__restrict__ nwork, Grid3 g) {
+                                                   const unsigned *__restrict__ nwork, Grid3 g,
+                                                   unsigned long long *__restrict__ unconverged) {
   const unsigned n = *nwork;
   const int nx = g.nx, rows = g.ny + 2;
+  unsigned missed = 0;
   for (unsigned w = blockIdx.x * blockDim.x + threadIdx.x; w < n; w += gridDim.x * blockDim.x) {
     const unsigned c = work[w];
     const int i = 1 + (int)(c % (unsigned)nx);
     const unsigned r = c / (unsigned)nx;
     const int j = (int)(r % (unsigned)rows), k = (int)(r / (unsigned)rows);
     R *o = normal + 4L * c;
-    o[3] = R(thinc_intercept3<double>(ldg(vof + ix_vof(g, i, j, k)), (double)o[0], (double)o[1], (double)o[2]));
+    bool converged = false;
+    o[3] = R(thinc_intercept3<double>(ldg(vof + ix_vof(g, i, j, k)), (double)o[0], (double)o[1], (double)o[2],
+                                      converged));
+    missed += converged ? 0u : 1u;
   }
+  // every thread of the block reaches this point (no early return)
+  missed = __reduce_add_sync(0xffffffffu, missed);
+  if (unconverged && missed && 0 == (threadIdx.x & 31)) atomicAdd(unconverged, (unsigned long long)missed);
 }
 
 // ---------------------------------------------------------------------------
@@ -679,13 +692,13 @@ __global__ void __launch_bounds__(AX * AY, 4) k3_vof_advect(const double *__rest
 // ---- host-side launchers
 template <class R>
 cudaError_t interface_geom(cudaStream_t st, const double *vof, R *normal, R *curv, unsigned *work,
-                           unsigned *nwork, Grid3 g) {
+                           unsigned *nwork, Grid3 g, unsigned long long *unconverged) {
   cudaError_t e = cudaMemsetAsync(nwork, 0, sizeof(unsigned), st);
   if (cudaSuccess != e) return e;
   dim3 gr((g.nx + G3X - 1) / G3X, (g.ny + 2 + G3Y - 1) / G3Y, (g.nz + 2 + G3Z - 1) / G3Z);
   k3_geom<R><<<gr, G3X * G3Y, 0, st>>>(vof, normal, curv, work, nwork, g);
   if (cudaSuccess != (e = cudaGetLastError())) return e;
-  k3_intercept<R><<<148 * 8, 256, 0, st>>>(vof, normal, work, nwork, g);
+  k3_intercept<R><<<148 * 8, 256, 0, st>>>(vof, normal, work, nwork, g, unconverged);
   return cudaGetLastError();
 }
 
@@ -712,7 +725,8 @@ cudaError_t interface_prepare_t() {
 }
 
 #define SVOF3_INTERFACE_INST(R)                                                                                \
-  template cudaError_t interface_geom<R>(cudaStream_t, const double *, R *, R *, unsigned *, unsigned *, Grid3); \
+  template cudaError_t interface_geom<R>(cudaStream_t, const double *, R *, R *, unsigned *, unsigned *, Grid3, \
+                                          unsigned long long *);                                         \
   template cudaError_t interface_force<R>(cudaStream_t, const double *, const R *, R *, R *, R *, double, Grid3); \
   template cudaError_t interface_advect<R>(cudaStream_t, const double *, double *, const double *, const double *, \
                                            const double *, const R *, double *, const double *, const double *,   \

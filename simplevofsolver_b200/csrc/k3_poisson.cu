@@ -245,7 +245,7 @@ template <class R, int LPB>
 __global__ void __launch_bounds__(LPB) k3_pois_x(R *__restrict__ spec, R *__restrict__ scratch,
                                                  const double *__restrict__ pl, const double *__restrict__ pu,
                                                  const double *__restrict__ evy, const double *__restrict__ evz,
-                                                 Grid3 g, int gauge0) {
+                                                 Grid3 g, int gauge0, unsigned long long *__restrict__ small_pivots) {
   using C2 = typename Cplx<R>::T;
   using S = XShape<R, LPB>;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -294,6 +294,7 @@ __global__ void __launch_bounds__(LPB) k3_pois_x(R *__restrict__ spec, R *__rest
     }
   };
   double vprev = 0., qr = 0., qi = 0.;
+  bool small = false;  // a pivot of this line at most DBL_EPSILON in magnitude
   // ---------------------------------------------------------- forward
   for (int c = 0; c < nchunks; c++) {
     const int p0 = c * XC;
@@ -315,16 +316,20 @@ __global__ void __launch_bounds__(LPB) k3_pois_x(R *__restrict__ spec, R *__rest
         const C2 x = sq[t][s];
         const double xr = x.x, xi = x.y;
         if (0 == i) {
+          small |= !(fabs(c) > kDblEpsilon);
           vprev = u / c;
           qr = xr / c;
           qi = xi / c;
         } else if (i < nx - 1) {
-          const double val = 1. / (c - l * vprev);
+          const double piv = c - l * vprev;
+          small |= !(fabs(piv) > kDblEpsilon);
+          const double val = 1. / piv;
           vprev = val * (u);
           qr = val * (xr - l * qr);
           qi = val * (xi - l * qi);
         } else {
           const double val = c - l * vprev;
+          small |= !(fabs(val) > kDblEpsilon);
           if (fabs(val) > kDblEpsilon && !(gauge0 && 0 == l0 + t)) {
             qr = 1. / val * (xr - l * qr);
             qi = 1. / val * (xi - l * qi);
@@ -370,6 +375,10 @@ __global__ void __launch_bounds__(LPB) k3_pois_x(R *__restrict__ spec, R *__rest
     copy_out(p0, false);
     __syncthreads();
   }
+  // the ky = kz = 0 line is singular by construction (its last pivot is
+  // round-off sized) and is not counted
+  const unsigned bad = __ballot_sync(0xffffffffu, live && small && 0 != l0 + t);
+  if (small_pivots && bad && 0 == (t & 31)) atomicAdd(small_pivots, (unsigned long long)__popc(bad));
 }
 
 // c2r along y (Hermitian extension as FFTW's c2r reads it: Im of X_0 and
@@ -650,15 +659,16 @@ inline bool pois_x_narrow(long nlines) { return nlines < 148L * 4 * 128; }
 
 template <class R>
 cudaError_t pois_x(cudaStream_t st, R *spec, R *scratch, const double *pl, const double *pu, const double *evy,
-                   const double *evz, Grid3 g, bool gauge0) {
+                   const double *evz, Grid3 g, bool gauge0, unsigned long long *small_pivots) {
   const long nlines = (long)(g.ny / 2 + 1) * g.nz;
   const int gz = gauge0 ? 1 : 0;
   if (pois_x_narrow(nlines)) {
     k3_pois_x<R, 64><<<(unsigned)((nlines + 63) / 64), 64, XShape<R, 64>::SMEM, st>>>(spec, scratch, pl, pu, evy,
-                                                                                      evz, g, gz);
+                                                                                      evz, g, gz, small_pivots);
   } else {
     k3_pois_x<R, 128><<<(unsigned)((nlines + 127) / 128), 128, XShape<R, 128>::SMEM, st>>>(spec, scratch, pl, pu,
-                                                                                          evy, evz, g, gz);
+                                                                                          evy, evz, g, gz,
+                                                                                          small_pivots);
   }
   return cudaGetLastError();
 }
@@ -725,7 +735,7 @@ cudaError_t pois_resid(cudaStream_t st, const double *b, const double *psi, doub
                                      const R *, const double *, double, int, Grid3);                            \
   template cudaError_t pois_z<R>(cudaStream_t, R *, const R *, int, Grid3);                                      \
   template cudaError_t pois_x<R>(cudaStream_t, R *, R *, const double *, const double *, const double *,        \
-                                 const double *, Grid3, bool);                                                         \
+                                 const double *, Grid3, bool, unsigned long long *);                             \
   template cudaError_t pois_inv_y<R>(cudaStream_t, const R *, double *, const R *, int, Grid3, bool);          \
   template cudaError_t pois_fwd_y_array<R>(cudaStream_t, const double *, R *, const R *, int, Grid3);
 SVOF3_POISSON_INST(double)

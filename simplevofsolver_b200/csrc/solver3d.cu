@@ -127,6 +127,10 @@ struct svof3d_solver {
   // k3_dt_final (a time step that is not a positive finite number), read and
   // cleared by the host at its synchronisations (check_status)
   unsigned *d_status = nullptr;
+  // health counters, accumulated until svof3d_health resets them: [0] THINC
+  // intercepts whose Newton iteration did not converge, [1] Poisson x lines
+  // (other than ky = kz = 0) that met a pivot of magnitude <= DBL_EPSILON
+  unsigned long long *d_health = nullptr;
   double *h_dt = nullptr;
   int h_dt_slots = 0;
   DevBuf diag;
@@ -207,7 +211,7 @@ int launch_dt(svof3d_solver *s) {
 template <class R>
 int launch_geom_t(svof3d_solver *s) {
   CK(interface_geom<R>(s->stream, s->vof[s->cur_v].p, s->normal.as<R>(), s->curv.as<R>(), s->d_work, s->d_nwork,
-                       s->grid()));
+                       s->grid(), s->d_health));
   return 0;
 }
 int launch_geom(svof3d_solver *s) { return s->mixed ? launch_geom_t<float>(s) : launch_geom_t<double>(s); }
@@ -325,7 +329,7 @@ int launch_potential_dc(svof3d_solver *s, int rk, const Marker &mark) {
     if (m(SVOF3_K_POISSON_FWD)) return 1;
     CK(pois_z<float>(s->stream, sp, s->twf_z32.as<float>(), s->log2nz, g));
     if (m(SVOF3_K_POISSON_Z)) return 1;
-    CK(pois_x<float>(s->stream, sp, xs, s->pl.p, s->pu.p, s->evy.p, s->evz.p, g, true));
+    CK(pois_x<float>(s->stream, sp, xs, s->pl.p, s->pu.p, s->evy.p, s->evz.p, g, true, s->d_health + 1));
     if (m(SVOF3_K_POISSON_SOLVE)) return 1;
     CK(pois_z<float>(s->stream, sp, s->twb_z32.as<float>(), s->log2nz, g));
     if (m(SVOF3_K_POISSON_Z)) return 1;
@@ -356,7 +360,8 @@ int launch_potential(svof3d_solver *s, int rk, const Marker &mark = Marker()) {
   if (m(SVOF3_K_POISSON_FWD)) return 1;
   CK(pois_z<double>(s->stream, s->spec.p, s->twf_z.p, s->log2nz, g));
   if (m(SVOF3_K_POISSON_Z)) return 1;
-  CK(pois_x<double>(s->stream, s->spec.p, s->xscratch.p, s->pl.p, s->pu.p, s->evy.p, s->evz.p, g));
+  CK(pois_x<double>(s->stream, s->spec.p, s->xscratch.p, s->pl.p, s->pu.p, s->evy.p, s->evz.p, g, false,
+                    s->d_health + 1));
   if (m(SVOF3_K_POISSON_SOLVE)) return 1;
   CK(pois_z<double>(s->stream, s->spec.p, s->twb_z.p, s->log2nz, g));
   if (m(SVOF3_K_POISSON_Z)) return 1;
@@ -586,6 +591,7 @@ int svof3d_destroy(svof3d_solver_t *s) {
   if (s->d_dt) cudaFree(s->d_dt);
   if (s->d_minbits) cudaFree(s->d_minbits);
   if (s->d_status) cudaFree(s->d_status);
+  if (s->d_health) cudaFree(s->d_health);
   if (s->d_work) cudaFree(s->d_work);
   if (s->d_nwork) cudaFree(s->d_nwork);
   if (s->h_dt) cudaFreeHost(s->h_dt);
@@ -661,7 +667,9 @@ int svof3d_create(const svof3d_params_t *prm, const double *xf, const double *xc
     return fail("cudaMalloc worklist"), bail();
   if (cudaSuccess != cudaMalloc(&s->d_minbits, sizeof(unsigned long long))) return fail("cudaMalloc"), bail();
   if (cudaSuccess != cudaMalloc(&s->d_status, sizeof(unsigned)) ||
-      cudaSuccess != cudaMemset(s->d_status, 0, sizeof(unsigned)))
+      cudaSuccess != cudaMemset(s->d_status, 0, sizeof(unsigned)) ||
+      cudaSuccess != cudaMalloc(&s->d_health, 2 * sizeof(unsigned long long)) ||
+      cudaSuccess != cudaMemset(s->d_health, 0, 2 * sizeof(unsigned long long)))
     return fail("cudaMalloc status"), bail();
   {
     const double one = 1.;
@@ -1110,6 +1118,19 @@ int svof3d_synchronize(svof3d_solver_t *s) {
   if (!s) return fail("null argument");
   CK(cudaStreamSynchronize(s->stream));
   return check_status(s, "svof3d_synchronize");
+}
+
+int svof3d_health(svof3d_solver_t *s, unsigned long long *newton_unconverged, unsigned long long *small_pivots,
+                  int reset) {
+  SVOF_RANGE();
+  if (!s) return fail("null argument");
+  unsigned long long h[2] = {0, 0};
+  CK(cudaMemcpyAsync(h, s->d_health, sizeof(h), cudaMemcpyDeviceToHost, s->stream));
+  if (reset) CK(cudaMemsetAsync(s->d_health, 0, sizeof(h), s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  if (newton_unconverged) *newton_unconverged = h[0];
+  if (small_pivots) *small_pivots = h[1];
+  return check_status(s, "svof3d_health");
 }
 
 int svof3d_stream(svof3d_solver_t *s, void **stream) {

@@ -97,9 +97,10 @@ __global__ void k3_halo_bc(double *a, int width, int nh, int ny, int nz, int kin
 // geometry / THINC arithmetic; vof, velocities and vof sources are FP64.
 // geometry: corner normals, cell normals, curvature (clears and fills the
 // interfacial-cell worklist), then the THINC intercepts of the listed cells
+// (unconverged, when given: += the cells whose Newton iteration did not converge)
 template <class R>
 cudaError_t interface_geom(cudaStream_t st, const double *vof, R *normal, R *curv, unsigned *work,
-                           unsigned *nwork, Grid3 g);
+                           unsigned *nwork, Grid3 g, unsigned long long *unconverged = nullptr);
 // CSF force
 template <class R>
 cudaError_t interface_force(cudaStream_t st, const double *vof, const R *curv, R *ifrcx, R *ifrcy, R *ifrcz,
@@ -162,9 +163,11 @@ cudaError_t pois_fwd_y(cudaStream_t st, const double *ux, const double *uy, cons
 template <class R>
 cudaError_t pois_z(cudaStream_t st, R *spec, const R *tw, int log2n, Grid3 g);
 template <class R>
-// (gauge0: the ky = kz = 0 line takes the gauge psi_hat(last) = 0, for FP32 storage)
+// (gauge0: the ky = kz = 0 line takes the gauge psi_hat(last) = 0, for FP32 storage;
+// small_pivots, when given: += the lines other than ky = kz = 0 that met a
+// pivot of magnitude at most DBL_EPSILON)
 cudaError_t pois_x(cudaStream_t st, R *spec, R *scratch, const double *pl, const double *pu, const double *evy,
-                   const double *evz, Grid3 g, bool gauge0 = false);
+                   const double *evz, Grid3 g, bool gauge0 = false, unsigned long long *small_pivots = nullptr);
 // acc: psi += the result (the correction pass), the walls' halo images kept
 template <class R>
 cudaError_t pois_inv_y(cudaStream_t st, const R *spec, double *psi, const R *tw, int log2n, Grid3 g,

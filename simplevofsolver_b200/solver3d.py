@@ -44,7 +44,7 @@ EXPORTS3D = ["svof3d_create", "svof3d_destroy", "svof3d_field_count", "svof3d_up
              "svof3d_interface_compute_force", "svof3d_interface_update_vof", "svof3d_fluid_predict_field",
              "svof3d_fluid_compute_potential_dft", "svof3d_fluid_correct_velocity",
              "svof3d_fluid_update_pressure", "svof3d_integrate", "svof3d_run", "svof3d_enqueue_steps",
-             "svof3d_last_dt", "svof3d_diagnostics", "svof3d_profile_step", "svof3d_synchronize",
+             "svof3d_last_dt", "svof3d_diagnostics", "svof3d_profile_step", "svof3d_synchronize", "svof3d_health",
              "svof3d_stream", "svof3d_last_error", "svof3d_statistics_collect", "svof3d_statistics_reset",
              "svof3d_statistics_count", "svof3d_statistics_reduce", "svof3d_statistics_field",
              "svof3d_set_tension", "svof3d_tape_count", "svof3d_integrate_fixed", "svof3d_adjoint_field",
@@ -127,6 +127,8 @@ def lib3() -> ctypes.CDLL:
         L.svof3d_diagnostics.argtypes = [vp, pd, pd, pd, pd]
         L.svof3d_profile_step.argtypes = [vp, dp, dp, i]
         L.svof3d_synchronize.argtypes = [vp]
+        L.svof3d_health.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(ctypes.c_ulonglong),
+                                    ctypes.c_int]
         L.svof3d_stream.argtypes = [vp, ctypes.POINTER(vp)]
         L.svof3d_last_error.restype = ctypes.c_char_p
         L.svof3d_set_tension.argtypes = [vp, d]
@@ -396,6 +398,15 @@ class Solver3D:
 
     def synchronize(self):
         _check(lib3().svof3d_synchronize(self._h))
+
+    def health(self, reset=False):
+        """the device health counters since creation or the last reset:
+        {"newton_unconverged": THINC intercepts whose Newton iteration missed
+        its tolerance, "small_pivots": Poisson x line solves (other than the
+        singular ky = kz = 0 line) that met a pivot <= DBL_EPSILON}"""
+        a, b = ctypes.c_ulonglong(0), ctypes.c_ulonglong(0)
+        _check(lib3().svof3d_health(self._h, ctypes.byref(a), ctypes.byref(b), 1 if reset else 0))
+        return {"newton_unconverged": a.value, "small_pivots": b.value}
 
     # ------------------------------------------------------------ differentiation form
     def device_view(self, name: str):

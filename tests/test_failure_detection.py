@@ -13,6 +13,11 @@
 * Restart files: a damaged NPY header, a wrong dtype, Fortran order or a
   shape that does not match glsizes raise ValueError naming the file (host
   only, no GPU).
+* Health counters (3D): THINC intercepts whose Newton iteration missed its
+  tolerance and Poisson x lines that met a pivot <= DBL_EPSILON are counted
+  on the device and read with Solver3D.health; both stay 0 on the droplet
+  workload in every precision, and a NaN vof cell (an interfacial cell for
+  the geometry: no comparison holds for it) makes the intercept count grow.
 """
 import os
 
@@ -123,6 +128,27 @@ def test_non_finite_velocity_is_reported_3d(gpu_available, name):
     for k, v in ic.fields().items():
         s.load_interior(k, v)
     s.run(1)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed", "mixed_dc"])
+def test_health_counters_3d(gpu_available, precision):
+    from simplevofsolver_b200 import Solver3D
+    ic = droplets3d(32, 16, 16, ndrops=3, radii=(0.12, 0.2), seed=3)
+    s = Solver3D(ic, physical_params(DROPLETS3D_ENV), precision=precision)
+    s.run(5)
+    assert s.health() == {"newton_unconverged": 0, "small_pivots": 0}
+    v = s.field("vof")
+    v[8, 8, 12] = np.nan
+    s.set_field("vof", v)
+    s.interface_compute_curvature_tensor()
+    h = s.health(reset=True)
+    assert h["newton_unconverged"] >= 1 and h["small_pivots"] == 0, h
+    assert s.health() == {"newton_unconverged": 0, "small_pivots": 0}
+    for k, a in ic.fields().items():
+        s.load_interior(k, a)
+    s.run(2)
+    assert s.health() == {"newton_unconverged": 0, "small_pivots": 0}
 
 
 # ---------------------------------------------------------------- allocation failure (GPU)
