@@ -414,9 +414,31 @@ __global__ void __launch_bounds__(32) k_predict_xsolve(const double *__restrict_
     double *q = ring + (size_t)(c % XS) * XC * 32 + l;
     const int p0 = c * XC, m = min(XC, n - p0);
     // batches of XB positions: the batch's loads are issued ahead of the
-    // dependent chain, which then runs on registers
+    // dependent chain, which then runs on registers.  A full batch inside
+    // the line (neither its first nor its last position) runs the bare
+    // recurrence with no per-position tests: the warp runs nearly alone on
+    // its SM, so every issued instruction counts.  Same expression, same
+    // order, same results as the general path below.
     for (int s0 = 0; s0 < m; s0 += XB) {
       const int mb = min(XB, m - s0);
+      const int pb = p0 + s0;
+      if (XB == mb && pb > 0 && pb + XB < n) {
+        double xv[XB], lv[XB], rv[XB];
+#pragma unroll
+        for (int k = 0; k < XB; k++) {
+          xv[k] = q[(s0 + k) * 32];
+          lv[k] = sL[pb + k];
+          rv[k] = sR[pb + k];
+        }
+#pragma unroll
+        for (int k = 0; k < XB; k++) {
+          qprev = rv[k] * (xv[k] - lv[k] * qprev);
+          xv[k] = qprev;
+        }
+#pragma unroll
+        for (int k = 0; k < XB; k++) q[(s0 + k) * 32] = xv[k];
+        continue;
+      }
       double xv[XB], lv[XB], rv[XB];
 #pragma unroll
       for (int k = 0; k < XB; k++) {
@@ -466,9 +488,27 @@ __global__ void __launch_bounds__(32) k_predict_xsolve(const double *__restrict_
     __syncwarp();
     double *q = ring + (size_t)(it % XS) * XC * 32 + l;
     const int p0 = c * XC, m = min(XC, n - p0);
-    // batches from the top of the chunk down, loads ahead of the chain
+    // batches from the top of the chunk down, loads ahead of the chain; a
+    // full batch below the last row runs the bare recurrence
     for (int s1 = m; s1 > 0; s1 -= XB) {
       const int mb = min(XB, s1);  // positions s1 - 1 .. s1 - mb
+      const int pt = p0 + s1 - 1;  // the batch's top position
+      if (XB == mb && pt < n - 1) {
+        double xv[XB], vv[XB];
+#pragma unroll
+        for (int k = 0; k < XB; k++) {
+          xv[k] = q[(s1 - 1 - k) * 32];
+          vv[k] = sV[pt - k];
+        }
+#pragma unroll
+        for (int k = 0; k < XB; k++) {
+          qn = xv[k] - vv[k] * qn;
+          xv[k] = qn;
+        }
+#pragma unroll
+        for (int k = 0; k < XB; k++) q[(s1 - 1 - k) * 32] = xv[k];
+        continue;
+      }
       double xv[XB], vv[XB];
 #pragma unroll
       for (int k = 0; k < XB; k++) {
