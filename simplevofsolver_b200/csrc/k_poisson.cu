@@ -188,18 +188,52 @@ __global__ void k_dct_ysolve(double *__restrict__ spec, const double *__restrict
 #define Q(jj) q[(size_t)(jj) * kt]
 #define V(jj) v[(size_t)(jj) * kt]
 #define RV(jj) r[(size_t)(jj) * kt]
-    // gtsv of size n-1 on rows 0 .. n-2
+    // gtsv of size n-1 on rows 0 .. n-2.  The interior rows go in batches of
+    // YB: the batch's loads first, then the dependent chain on registers,
+    // then its stores (the same expressions in the same order as one row at
+    // a time, which the remainder rows use).
+    constexpr int YB = 8;
     double qprev = Q(0) / c;
     Q(0) = qprev;
-#pragma unroll 8
-    for (int i = 1; i < n - 2; i++) {
+    int i = 1;
+    for (; i + YB <= n - 2; i += YB) {
+      double xv[YB], rv[YB];
+#pragma unroll
+      for (int k = 0; k < YB; k++) {
+        xv[k] = Q(i + k);
+        rv[k] = RV(i + k);
+      }
+#pragma unroll
+      for (int k = 0; k < YB; k++) {
+        qprev = rv[k] * (xv[k] - l * qprev);
+        xv[k] = qprev;
+      }
+#pragma unroll
+      for (int k = 0; k < YB; k++) Q(i + k) = xv[k];
+    }
+    for (; i < n - 2; i++) {
       qprev = RV(i) * (Q(i) - l * qprev);
       Q(i) = qprev;
     }
     Q(n - 2) = (0. != lf) ? lf * (Q(n - 2) - l * qprev) : 0.;
     double qn = Q(n - 2);
-#pragma unroll 8
-    for (int i = n - 3; i >= 0; i--) {
+    i = n - 3;
+    for (; i - YB + 1 >= 0; i -= YB) {
+      double xv[YB], vv[YB];
+#pragma unroll
+      for (int k = 0; k < YB; k++) {
+        xv[k] = Q(i - k);
+        vv[k] = V(i - k);
+      }
+#pragma unroll
+      for (int k = 0; k < YB; k++) {
+        qn = xv[k] - vv[k] * qn;
+        xv[k] = qn;
+      }
+#pragma unroll
+      for (int k = 0; k < YB; k++) Q(i - k) = xv[k];
+    }
+    for (; i >= 0; i--) {
       qn = Q(i) - V(i) * qn;
       Q(i) = qn;
     }

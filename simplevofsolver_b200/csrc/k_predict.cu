@@ -371,8 +371,9 @@ __global__ void __launch_bounds__(32) k_predict_xsolve(const double *__restrict_
   pdl_enter();
   extern __shared__ double sm[];
   double *ring = sm;                         // [XS][XC][32]
-  double *sL = sm + (size_t)XS * XC * 32;    // [nx] L, then R, then V
-  double *sR = sL + nx, *sV = sR + nx;
+  double *sL = sm + (size_t)XS * XC * 32;    // [nx] L, then R, then V, at even offsets
+  const int nxp = (nx + 1) & ~1;
+  double *sR = sL + nxp, *sV = sR + nxp;
   const int nb = (ny + 31) >> 5;
   const int f = blockIdx.x / nb, jb = blockIdx.x % nb;
   const int l = threadIdx.x;  // line 32 jb + l + 1 (lanes past ny sweep zeros)
@@ -384,20 +385,16 @@ __global__ void __launch_bounds__(32) k_predict_xsolve(const double *__restrict_
   }
   double *base = fw + ((size_t)f * nb + jb) * nx * 32;  // position p at base + 32 p
   const int nch = (n + XC - 1) / XC;
-  // chunk c (positions c XC .. ) into slot s: 16-byte copies, 32 lanes
+  // chunk c (positions c XC .. ) into slot s: 16-byte copies, 32 lanes.
+  // Results go from registers straight to the line array (each lane its own
+  // 8-byte column of a 256-byte row); the slot is only read.
   auto load = [&](int c, int slot) {
     const int p0 = c * XC, m = min(XC, n - p0);
     const double *src = base + (size_t)p0 * 32;
     double *dst = ring + (size_t)slot * XC * 32;
+#pragma unroll 8
     for (int e = 2 * l; e < m * 32; e += 64) __pipeline_memcpy_async(dst + e, src + e, 16);
     __pipeline_commit();
-  };
-  auto store = [&](int c, int slot) {
-    const int p0 = c * XC, m = min(XC, n - p0);
-    double *dst = base + (size_t)p0 * 32;
-    const double *src = ring + (size_t)slot * XC * 32;
-#pragma unroll 16
-    for (int s = 0; s < m; s++) dst[s * 32 + l] = src[s * 32 + l];
   };
   __syncwarp();
   // ------------------------------------------------------------ forward
@@ -411,8 +408,9 @@ __global__ void __launch_bounds__(32) k_predict_xsolve(const double *__restrict_
     else __pipeline_commit();
     __pipeline_wait_prior(XS - 1);
     __syncwarp();
-    double *q = ring + (size_t)(c % XS) * XC * 32 + l;
+    const double *q = ring + (size_t)(c % XS) * XC * 32 + l;
     const int p0 = c * XC, m = min(XC, n - p0);
+    double *gq = base + (size_t)p0 * 32 + l;
     // batches of XB positions: the batch's loads are issued ahead of the
     // dependent chain, which then runs on registers.  A full batch inside
     // the line (neither its first nor its last position) runs the bare
@@ -423,20 +421,27 @@ __global__ void __launch_bounds__(32) k_predict_xsolve(const double *__restrict_
       const int mb = min(XB, m - s0);
       const int pb = p0 + s0;
       if (XB == mb && pb > 0 && pb + XB < n) {
+        // pb is a multiple of XB: the coefficient pairs are 16-byte aligned
         double xv[XB], lv[XB], rv[XB];
+        const double2 *l2 = reinterpret_cast<const double2 *>(sL + pb);
+        const double2 *r2 = reinterpret_cast<const double2 *>(sR + pb);
 #pragma unroll
-        for (int k = 0; k < XB; k++) {
-          xv[k] = q[(s0 + k) * 32];
-          lv[k] = sL[pb + k];
-          rv[k] = sR[pb + k];
+        for (int k = 0; k < XB / 2; k++) {
+          const double2 a = l2[k], b = r2[k];
+          lv[2 * k] = a.x;
+          lv[2 * k + 1] = a.y;
+          rv[2 * k] = b.x;
+          rv[2 * k + 1] = b.y;
         }
+#pragma unroll
+        for (int k = 0; k < XB; k++) xv[k] = q[(s0 + k) * 32];
 #pragma unroll
         for (int k = 0; k < XB; k++) {
           qprev = rv[k] * (xv[k] - lv[k] * qprev);
           xv[k] = qprev;
         }
 #pragma unroll
-        for (int k = 0; k < XB; k++) q[(s0 + k) * 32] = xv[k];
+        for (int k = 0; k < XB; k++) gq[(s0 + k) * 32] = xv[k];
         continue;
       }
       double xv[XB], lv[XB], rv[XB];
@@ -464,10 +469,10 @@ __global__ void __launch_bounds__(32) k_predict_xsolve(const double *__restrict_
       }
 #pragma unroll
       for (int k = 0; k < XB; k++)
-        if (k < mb) q[(s0 + k) * 32] = xv[k];
+        if (k < mb) gq[(s0 + k) * 32] = xv[k];
     }
-    __syncwarp();
-    store(c, c % XS);
+    // every lane done reading the slot (the next load refills it) and its
+    // stores ordered before the other lanes' later copies of them
     __syncwarp();
   }
   __pipeline_wait_prior(0);
@@ -486,8 +491,9 @@ __global__ void __launch_bounds__(32) k_predict_xsolve(const double *__restrict_
     else __pipeline_commit();
     __pipeline_wait_prior(XS - 1);
     __syncwarp();
-    double *q = ring + (size_t)(it % XS) * XC * 32 + l;
+    const double *q = ring + (size_t)(it % XS) * XC * 32 + l;
     const int p0 = c * XC, m = min(XC, n - p0);
+    double *gq = base + (size_t)p0 * 32 + l;
     // batches from the top of the chunk down, loads ahead of the chain; a
     // full batch below the last row runs the bare recurrence
     for (int s1 = m; s1 > 0; s1 -= XB) {
@@ -506,7 +512,7 @@ __global__ void __launch_bounds__(32) k_predict_xsolve(const double *__restrict_
           xv[k] = qn;
         }
 #pragma unroll
-        for (int k = 0; k < XB; k++) q[(s1 - 1 - k) * 32] = xv[k];
+        for (int k = 0; k < XB; k++) gq[(s1 - 1 - k) * 32] = xv[k];
         continue;
       }
       double xv[XB], vv[XB];
@@ -529,10 +535,8 @@ __global__ void __launch_bounds__(32) k_predict_xsolve(const double *__restrict_
       }
 #pragma unroll
       for (int k = 0; k < XB; k++)
-        if (k < mb) q[(s1 - 1 - k) * 32] = xv[k];
+        if (k < mb) gq[(s1 - 1 - k) * 32] = xv[k];
     }
-    __syncwarp();
-    store(c, it % XS);
     __syncwarp();
   }
 }

@@ -624,11 +624,12 @@ int engine_create(const svof_params_t *prm, const double *xf, const double *xc, 
     if (!s->uniform && sizeof(double) * 2 * (size_t)ny > 200 * 1024)
       return fail("svof_create: FFT length too large for one block"), bail();
   }
-  // line solves: lines per block so that the blocks cover the SMs, within
+  // line solves: lines per block so that there are four blocks per SM where
+  // the lines allow (one block's staging overlaps the others' sweeps), within
   // 160 KB of staged shared memory
   auto pick_kt = [](int lines, size_t bytes_per_line) {
     int kt = 32;
-    while (kt > 4 && lines / kt < 148) kt >>= 1;
+    while (kt > 1 && lines / kt < 4 * 148) kt >>= 1;
     while (kt > 1 && bytes_per_line * kt > 160 * 1024) kt >>= 1;
     return kt;
   };

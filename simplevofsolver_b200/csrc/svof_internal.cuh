@@ -110,7 +110,10 @@ size_t predict_smem_bytes(int nx, int rows_per_block);
 // predict_xsolve_smem(nx)), then u + delta' with halo rows and walls
 __global__ void k_predict_rhs(PredictArgs a, double *__restrict__ fw);
 __global__ void k_predict_xsolve(const double *__restrict__ coef, double *__restrict__ fw, int nx, int ny);
-inline size_t predict_xsolve_smem(int nx) { return sizeof(double) * ((size_t)4 * 64 * 32 + 3 * (size_t)nx); }
+// (the three coefficient rows start at even offsets: nx rounded up to even)
+inline size_t predict_xsolve_smem(int nx) {
+  return sizeof(double) * ((size_t)4 * 64 * 32 + 3 * (size_t)((nx + 1) & ~1));
+}
 __global__ void k_predict_update(PredictArgs a, const double *__restrict__ fw);
 
 // Poisson, DCT path (src/fluid/compute_potential/dct.c).  The row transforms
